@@ -1,0 +1,218 @@
+/*
+ * wavetoy_b200.h -- C ABI of the B200 (sm_100a) implementation of
+ * WaveToySecondOrder.jl's 3D SBP-SAT right-hand side and RK4 time step.
+ *
+ * Conventions
+ *   - Every function returns int: 0 = OK, < 0 = error (WT_E*); the message of
+ *     the last error on a context is wt_last_error(ctx).
+ *   - Fields are the reference's Julia arrays: (N,N,N,Ne), column-major, i
+ *     fastest (index i + N*(j + N*(k + N*e)), 0-based).  Connectivity arrays
+ *     given by callers are Julia's MeshConnectivity: (6,Ne), 1-based element
+ *     and face numbers, 0 = no neighbour.  Faces 1..6 = (-x,+x,-y,+y,-z,+z).
+ *   - State pointers passed to wt_rhs_* / wt_step_* are DEVICE pointers owned
+ *     by the caller (CuArray interop), of the context's precision (double for
+ *     WT_F64, float for WT_F32); calls are asynchronous on the context stream.
+ *     Functions ending in _host take host pointers and synchronise.
+ *   - A context owns one CUDA stream.  It is thread-compatible (one context
+ *     per host thread), not thread-safe.
+ *
+ * Boundary-condition kinds (src/boundaries1d.jl:61-64):
+ *   1 = Dirichlet, 2 = Sommerfeld, 3 = excision, 4 = full Dirichlet.
+ * Outer-face tags (src/wave.jl:23, 567-571): 0 interior, 1..6 Dirichlet
+ * against bdry_values[tag], 7 Sommerfeld, 8 excision.
+ */
+#ifndef WAVETOY_B200_H
+#define WAVETOY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  WT_OK = 0,
+  WT_EINVAL = -1,     /* bad argument (ArgumentError in the reference) */
+  WT_ECUDA = -2,      /* CUDA runtime error */
+  WT_ENOMEM = -3,     /* device allocation failed / over budget */
+  WT_ENOTSUP = -4,    /* configuration not supported by this build */
+  WT_ENONFINITE = -5, /* a NaN/Inf was detected (the reference's isfinite assert) */
+  WT_ETIMEOUT = -6    /* a bounded device wait gave up */
+};
+
+enum { WT_F64 = 0, WT_F32 = 1 };
+enum { WT_BC_DIRICHLET = 1, WT_BC_SOMMERFELD = 2, WT_BC_EXCISION = 3, WT_BC_FULL_DIRICHLET = 4 };
+enum { WT_BG_MINKOWSKI = 0, WT_BG_CONSTANT_SHIFT = 1, WT_BG_ADM_PERTURBED = 2, WT_BG_RADIAL_SHIFT = 3 };
+
+typedef struct wt_ctx wt_ctx;
+typedef struct wt_mesh wt_mesh;
+typedef struct wt_coef wt_coef;
+typedef struct wt_ws wt_ws;
+
+/* ---- context ------------------------------------------------------------ */
+/* No reference counterpart (Julia picks the backend per array); owns the
+ * stream that KernelAbstractions' backend queue stands for. */
+int wt_ctx_create(int device, wt_ctx** out);
+int wt_ctx_destroy(wt_ctx* ctx);
+const char* wt_last_error(const wt_ctx* ctx);
+int wt_ctx_synchronize(wt_ctx* ctx);
+/* the context's cudaStream_t, as void* */
+int wt_ctx_get_stream(wt_ctx* ctx, void** stream);
+/* Launch on a caller-owned cudaStream_t instead (e.g. the stream a CuArray or
+ * torch tensor was produced on); NULL restores the context's own stream.  The
+ * context never destroys a caller's stream. */
+int wt_ctx_set_stream(wt_ctx* ctx, void* stream);
+/* number of kernel launches this context has issued (evidence counter) */
+int wt_ctx_launch_count(const wt_ctx* ctx, long long* count);
+/* Read and clear the device non-finite flag that fused RK4 steps set when the
+ * state stops being finite (the reference asserts all(isfinite, ...) per
+ * sample, src/evolve.jl:1344); synchronous. */
+int wt_ctx_nonfinite(wt_ctx* ctx, int* flag);
+
+/* ---- mesh + geometry ------------------------------------------------------ */
+/* Analytic hex builder.  Replaces HexMeshes.make_uniform_hex(T, Mx, My, Mz,
+ * x0, x1; periodic) / make_warped_uniform_hex(T, Mx, My, Mz, x0, x1, A;
+ * periodic) (test/dirichlet_warped_tests.jl:23-40, src/evolve.jl:1174-1175)
+ * followed by HexSBPSAT.make_element/make_operators/make_geometry and, for
+ * curvilinear meshes, make_metric_terms3d (src/evolve.jl:1189-1196).  Warp:
+ * X = s + A P(s), P = sin(2 pi s1) sin(2 pi s2) sin(2 pi s3) for all three
+ * components.  Geometry and curl-form metric terms are computed on the device
+ * in FP64. */
+typedef struct {
+  int N;            /* GLL nodes per axis, 2..8 */
+  int M[3];         /* elements per axis */
+  double x0, x1;    /* the cube [x0,x1]^3 */
+  double warp_A;    /* warp amplitude; 0 = affine uniform hex */
+  int periodic;     /* 1 = periodic connectivity */
+  int outer_tag;    /* 0 = side tags 1..6; else this tag on every outer face */
+  int precision;    /* WT_F64 or WT_F32: type of streamed fields and state */
+} wt_mesh_desc;
+int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* desc, wt_mesh** out);
+
+/* Generic mesh from host arrays mirroring MeshGeometry + MeshConnectivity:
+ * coords (3,N,N,N,Ne), jac (3,3,N,N,N,Ne) = dx_a/dxi_b, neighbour /
+ * neighbour_face (6,Ne) int32 1-based, orientation / bdry (6,Ne) int8.
+ * Replaces HexSBPSAT.to_device(geom, backend) (src/evolve.jl:1191).
+ * Orientation must be 0 in this build (WT_ENOTSUP otherwise). */
+int wt_mesh_create_arrays(wt_ctx* ctx, int N, long long Ne, const double* coords, const double* jac,
+                          const int32_t* neighbour, const int32_t* neighbour_face,
+                          const int8_t* orientation, const int8_t* bdry, int precision, wt_mesh** out);
+int wt_mesh_destroy(wt_mesh* mesh);
+int wt_mesh_info(const wt_mesh* mesh, int* N, long long* Ne, int* precision);
+/* Copy a geometry array to host (FP64): "coords" (3*nn), "jac", "invjac"
+ * (9*nn), "detjac", "Hphys", "Hd", "invdetJ" (nn), "Ja" (9*nn, field-major:
+ * Ja[(al*3+i)*nn + node] = J dxi_al/dx_i), "x","H" (N), "G" (N*N, G[i*N+p]);
+ * int32 arrays: "bdry", "neighbour" (6*Ne, 1-based), "handedness" (Ne). */
+int wt_mesh_get(const wt_mesh* mesh, const char* name, void* host_out);
+/* Override the outer-face tags (6,Ne) int32, e.g. to mark excision faces. */
+int wt_mesh_set_bdry(wt_mesh* mesh, const int32_t* bdry);
+/* _min_node_spacing_3d (src/evolve.jl:60-69); synchronous. */
+int wt_mesh_min_spacing(wt_mesh* mesh, double* h);
+
+/* ---- ADM background --------------------------------------------------------*/
+/* Analytic background sampled on the device: replaces AnalyticBackground3D +
+ * make_coef3d + sample_background3d! (src/wave3d_curved.jl:45-124).
+ *   MINKOWSKI: -   CONSTANT_SHIFT: p[0..2] = beta
+ *   ADM_PERTURBED: alpha = 1 + p0 sin 2pi x, beta^i = p1 cos 2pi x_i,
+ *     gamma_ij = d_ij + p2 exp(-|x-c|^2/p3)(d_ij + 0.5 s_ij), c = p4..p6,
+ *     s = p7..p12 (s11,s12,s13,s22,s23,s33)
+ *   RADIAL_SHIFT: beta_r linear from p0 at r=p2 to p1 at r=p3 (src/evolve.jl:1128-1145) */
+typedef struct {
+  int kind;
+  double p[16];
+} wt_background_desc;
+int wt_background_set(wt_ctx* ctx, wt_mesh* mesh, const wt_background_desc* desc, wt_coef** out);
+/* Host-sampled 11-field bundle (alpha, sqrtg, b1, b2, b3, gu11, gu12, gu13,
+ * gu22, gu23, gu33), each (N,N,N,Ne) FP64 -- the layout sample_background3d!
+ * fills. */
+int wt_background_set_arrays(wt_ctx* ctx, wt_mesh* mesh, const double* coef11, wt_coef** out);
+int wt_coef_get(const wt_coef* coef, double* coef11_host);
+int wt_coef_destroy(wt_coef* coef);
+
+/* ---- workspace ---------------------------------------------------------------*/
+/* Replaces make_wave3d_workspace (src/wave3d_curved.jl:158-178): device
+ * scratch plus mu, the spectral radius of apply_D! along axis 1 from the
+ * reference's 30-step power iteration (alternating-sign start). */
+int wt_workspace_create(wt_ctx* ctx, wt_mesh* mesh, wt_ws** out);
+int wt_workspace_destroy(wt_ws* ws);
+int wt_workspace_mu(wt_ws* ws, double* mu);
+
+/* ---- right-hand sides (device pointers, async) ------------------------------*/
+typedef struct {
+  int kinds[6];       /* BC kind per side (-x,+x,-y,+y,-z,+z); curvilinear uses kinds[0] */
+  double sigma;       /* penalty strength, 1 in the reference */
+  int excision_tag;   /* faces with this tag get no SAT (curvilinear pass) */
+  const void* gPhi;   /* optional data fields (device, NULL = none) */
+  const void* gPi;
+  const void* gDx;
+  const void* gDy;
+  const void* gDz;
+} wt_bc_desc;
+
+/* wave3d_curved_rhs!(Phidot, Pidot, Phi, Pi, coef; geom, ops, ws, eps_KO,
+ * bc3d, metric) (src/wave3d_curved.jl:205-258) with the boundary passes
+ * _apply_bc3d! / _apply_bc3d_curv! (src/boundaries3d.jl:58-232).
+ * use_metric = 0 selects the affine per-axis path (metric === nothing),
+ * 1 the curvilinear split-form path.  bc may be NULL (periodic). */
+int wt_rhs_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi,
+                  void* Phidot, void* Pidot, double eps_ko, const wt_bc_desc* bc, int use_metric);
+/* HexSBPSAT.apply_D!(Du, u, d) (called at src/wave3d_curved.jl:169-170, 184-189, 219-221), d = 1..3. */
+int wt_apply_D(wt_ctx* ctx, wt_ws* ws, const void* u, void* Du, int d);
+/* dst += eps * mu^-5 * sum_d D_d^6 field: the three _ko_axis3! calls of one
+ * field (src/wave3d_curved.jl:182-192, 241-248). */
+int wt_ko_add(wt_ctx* ctx, wt_ws* ws, void* dst, const void* field, double eps_ko);
+/* apply_gradient3d! (src/wave3d_curved.jl:223): split-form curvilinear gradient. */
+int wt_gradient3d(wt_ctx* ctx, wt_ws* ws, const void* u, void* g1, void* g2, void* g3);
+/* apply_divergence3d! (src/wave3d_curved.jl:237). */
+int wt_divergence3d(wt_ctx* ctx, wt_ws* ws, const void* F1, const void* F2, const void* F3, void* out);
+
+/* rhs_wave3d!(utt, u, ut, bdry_values; geom, ops, work, tau, sommerfeld_R)
+ * (src/wave.jl:583-611): SIPG Laplacian (apply_laplacian!, README.md:57-80)
+ * plus the tag-7 Sommerfeld pass (src/wave.jl:453-542).  Affine meshes.
+ * sommerfeld_R <= 0 or infinite = plane-wave BGT-0. */
+int wt_rhs_sipg(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, void* utt, const double bdry_values[6],
+                double tau, double sommerfeld_R);
+/* wave_strong_rhs_mesh!(utt, u, ut, mesh, geom, dinvjac, ops; tau, sommerfeld_R)
+ * (src/wave_strong_rhs.jl:296-341); dinvjac (make_metric_derivs, :376-391)
+ * is built on the device on first use. */
+int wt_rhs_strong(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, void* utt, double tau,
+                  double sommerfeld_R);
+/* wave_lap_strong_conservative_mesh!(Lu, u, mesh, ops, h; tau)
+ * (src/wave_lap_strong.jl:280-308): uniform Cartesian meshes. */
+int wt_lap_strong_cons(wt_ctx* ctx, wt_ws* ws, const void* u, void* Lu, double h, double tau);
+
+/* ---- reductions (FP64 accumulation, synchronous) ----------------------------- */
+/* wave3d_energy (src/wave3d_curved.jl:268-287). */
+int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, int use_metric,
+              double* E);
+/* SIPG Hamiltonian 1/2<ut,ut>_H - 1/2<u, L_SAT u>_H (test/kernels3d_tests.jl:39-47). */
+int wt_energy_sipg(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, double tau, double* E);
+/* sqrt(sum (a-b)^2 H), H = Hphys (use_metric 0) or Hd (1) (src/evolve.jl:1353-1354);
+ * b may be NULL (norm of a). */
+int wt_l2_diff(wt_ctx* ctx, wt_ws* ws, const void* a, const void* b, int use_metric, double* out);
+
+/* ---- time stepping ----------------------------------------------------------- */
+/* nsteps classic RK4 steps (OrdinaryDiffEq RK4(), adaptive=false; in-repo
+ * restatement test/wave3d_tests.jl:32-44) of the conservative system, with
+ * the stage update fused into the RHS kernels (low-storage form).  Phi, Pi
+ * are updated in place.  Sets WT_ENONFINITE if the state became non-finite
+ * (checked at the end; the reference asserts isfinite per sample). */
+int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
+                       double eps_ko, const wt_bc_desc* bc, int use_metric);
+/* RK4 of the SIPG system as first-order (u, ut):
+ * u' = ut + eps mu^-5 sum_d D_d^6 u,  ut' = rhs_wave3d!(u, ut) + eps mu^-5 sum_d D_d^6 ut. */
+int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int nsteps,
+                     const double bdry_values[6], double tau, double sommerfeld_R, double eps_ko);
+/* End-to-end evolve with host buffers, the shape of evolve3d(formulation =
+ * :conservative) (src/evolve.jl:1149-1366): upload Phi/Pi, then nsamples times
+ * run steps_per_sample RK4 steps and copy the state back into
+ * Phi_hist/Pi_hist[s] (host, nsamples*nn each, may be NULL) and the energy
+ * into energy[s] (may be NULL).  Phi_host/Pi_host receive the final state. */
+int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* Phi_host, double* Pi_host,
+                          double dt, int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc,
+                          int use_metric, double* energy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WAVETOY_B200_H */

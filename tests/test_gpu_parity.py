@@ -1,0 +1,317 @@
+"""GPU parity: every kernel of libwavetoy_b200.so against the CPU Float64 oracle.
+
+Bar: the plain FP64 form agrees with the oracle to <= 1e-12 relative L2 (RHS and
+operator calls) and <= 1e-12 after many RK4 steps; the FP32 form to <= 1e-5
+relative L2 on the RHS.  Sizes are ones the oracle finishes in seconds.
+"""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def dev(t, x):
+    import torch
+    return torch.tensor(np.asarray(x), dtype=t, device="cuda")
+
+
+def host(x):
+    return x.detach().double().cpu().numpy()
+
+
+def pair(wt, ctx, O, N, M, A=0.0, periodic=False, outer_tag=0, precision=0):
+    g = wt.Mesh.uniform_hex(ctx, N, M, 0.0, 1.0, periodic=periodic, outer_tag=outer_tag, warp_A=A,
+                            precision=precision)
+    o = O.OracleMesh(N, M, A=A, periodic=periodic, outer_tag=outer_tag)
+    return g, o
+
+
+@pytest.mark.parametrize("A,periodic", [(0.0, False), (0.05, False), (0.05, True)])
+def test_geometry_and_metric_terms(wt, ctx, O, A, periodic):
+    g, o = pair(wt, ctx, O, 5, (3, 2, 4), A=A, periodic=periodic, outer_tag=7)
+    for name in ("coords", "jac", "invjac", "detjac", "Hphys", "Ja", "Hd", "invdetJ"):
+        assert rel(g.get(name), o.get(name)) < 1e-13, name
+    assert np.array_equal(g.get("bdry"), o.get("bdry"))
+    nb = g.get("neighbour")
+    assert np.array_equal(nb - 1, o.get("nbr"))
+
+
+def test_background_sampling(wt, ctx, O):
+    g, o = pair(wt, ctx, O, 4, 3, A=0.05, outer_tag=7)
+    p = wt.workloads.adm_params(11)
+    cg = wt.sample_background3d(g, wt.BG_ADM_PERTURBED, p).get()
+    co = o.background(2, p)
+    assert rel(cg, co) < 1e-14
+
+
+def test_mu_power_iteration(wt, ctx, O):
+    for A, per in ((0.0, True), (0.05, False)):
+        g, o = pair(wt, ctx, O, 4, 3, A=A, periodic=per, outer_tag=7)
+        ws = wt.make_wave3d_workspace(g)
+        assert abs(ws.mu - o.mu()) / o.mu() < 1e-10
+
+
+@pytest.mark.parametrize("A,periodic", [(0.0, True), (0.0, False), (0.05, False)])
+def test_apply_D(wt, ctx, O, A, periodic):
+    import torch
+    g, o = pair(wt, ctx, O, 6, 3, A=A, periodic=periodic, outer_tag=7)
+    ws = wt.make_wave3d_workspace(g)
+    u = np.random.default_rng(3).standard_normal(o.nn)
+    ud = dev(torch.float64, u)
+    out = g.zeros()
+    for d in (1, 2, 3):
+        wt.apply_D(out, ud, d, ws)
+        assert rel(host(out), o.apply_D(u, d - 1)) < TOL64
+
+
+def test_gradient_divergence(wt, ctx, O):
+    import torch
+    g, o = pair(wt, ctx, O, 8, 2, A=0.05, outer_tag=7)
+    ws = wt.make_wave3d_workspace(g)
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal(o.nn)
+    F = [rng.standard_normal(o.nn) for _ in range(3)]
+    gd = [g.zeros() for _ in range(3)]
+    wt.apply_gradient3d(*gd, dev(torch.float64, u), ws)
+    go = o.grad3d(u)
+    for c in range(3):
+        assert rel(host(gd[c]), go[c]) < TOL64
+    out = g.zeros()
+    wt.apply_divergence3d(out, *[dev(torch.float64, f) for f in F], ws)
+    assert rel(host(out), o.div3d(*F)) < TOL64
+
+
+def test_ko(wt, ctx, O):
+    import torch
+    for A, per, N, M in ((0.0, True, 4, 3), (0.05, False, 6, (2, 3, 4))):
+        g, o = pair(wt, ctx, O, N, M, A=A, periodic=per, outer_tag=7)
+        ws = wt.make_wave3d_workspace(g)
+        rng = np.random.default_rng(9)
+        f = rng.standard_normal(o.nn)
+        dst = rng.standard_normal(o.nn)
+        dd = dev(torch.float64, dst)
+        wt.ko_add(dd, dev(torch.float64, f), 0.1, ws)
+        od = dst.copy()
+        o.ko_add(od, f, 0.1 * (1.0 / o.mu()) ** 5)
+        assert rel(host(dd), od) < TOL64
+
+
+CASES = [
+    # (N, M, A, periodic, outer_tag, use_metric, bg_kind, eps, bc kinds or None)
+    (4, 3, 0.0, True, 0, False, 0, 0.1, None),
+    (6, 2, 0.0, False, 7, False, 2, 0.1, [2] * 6),
+    (4, 3, 0.0, False, 0, False, 1, 0.0, [4, 3, 2, 2, 1, 2]),
+    (8, 2, 0.05, False, 7, True, 2, 0.0, [2] * 6),
+    (5, 3, 0.05, False, 7, True, 2, 0.1, [2] * 6),
+    (4, 2, 0.05, True, 0, True, 2, 0.0, None),
+    (4, 3, 0.05, False, 7, True, 0, 0.0, [4] * 6),
+]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_rhs_curved(wt, ctx, O, case):
+    import torch
+    N, M, A, per, tag, um, kind, eps, kinds = case
+    g, o = pair(wt, ctx, O, N, M, A=A, periodic=per, outer_tag=tag)
+    p = wt.workloads.adm_params(4) if kind == 2 else ([0.3, -0.2, 0.1] if kind == 1 else [])
+    cg = wt.sample_background3d(g, kind, p)
+    co = o.background(kind, p)
+    ws = wt.make_wave3d_workspace(g)
+    rng = np.random.default_rng(17)
+    Phi, Pi = rng.standard_normal(o.nn), rng.standard_normal(o.nn)
+    gP, gQ = rng.standard_normal(o.nn), rng.standard_normal(o.nn)
+    bcg = bco = None
+    if kinds is not None:
+        bcg = wt.make_bc3d(kinds, gPhi=dev(torch.float64, gP), gPi=dev(torch.float64, gQ))
+        bco = O.make_bc(kinds, gPhi=gP, gPi=gQ)
+    Pd, Qd = g.zeros(), g.zeros()
+    wt.wave3d_curved_rhs(Pd, Qd, dev(torch.float64, Phi), dev(torch.float64, Pi), cg, ws, eps_KO=eps, bc3d=bcg,
+                         metric=um)
+    Po, Qo = o.rhs_curved(co, Phi, Pi, eps_ko=eps, bc=bco, use_metric=um)
+    assert rel(host(Pd), Po) < TOL64
+    assert rel(host(Qd), Qo) < TOL64
+
+
+def test_rhs_curved_excision_tag(wt, ctx, O):
+    """Curvilinear pass: faces carrying the excision tag get no SAT (src/boundaries3d.jl:180-181)."""
+    import torch
+    g, o = pair(wt, ctx, O, 4, 3, A=0.05, outer_tag=7)
+    bd = o.get("bdry").copy()
+    bd[0::6][bd[0::6] != 0] = 8   # -x faces become excision faces
+    o.set_bdry(bd)
+    g.set_bdry(bd)
+    cg = wt.sample_background3d(g, 2, wt.workloads.adm_params(1))
+    co = o.background(2, wt.workloads.adm_params(1))
+    ws = wt.make_wave3d_workspace(g)
+    rng = np.random.default_rng(2)
+    Phi, Pi = rng.standard_normal(o.nn), rng.standard_normal(o.nn)
+    Pd, Qd = g.zeros(), g.zeros()
+    wt.wave3d_curved_rhs(Pd, Qd, dev(torch.float64, Phi), dev(torch.float64, Pi), cg, ws, eps_KO=0.0,
+                         bc3d=wt.make_bc3d([2] * 6, excision_tag=8), metric=True)
+    Po, Qo = o.rhs_curved(co, Phi, Pi, eps_ko=0.0, bc=O.make_bc([2] * 6, excision_tag=8), use_metric=True)
+    assert rel(host(Pd), Po) < TOL64 and rel(host(Qd), Qo) < TOL64
+
+
+@pytest.mark.parametrize("um", [False, True])
+def test_energy(wt, ctx, O, um):
+    import torch
+    g, o = pair(wt, ctx, O, 6, 2, A=0.05 if um else 0.0, outer_tag=7)
+    p = wt.workloads.adm_params(3)
+    cg, co = wt.sample_background3d(g, 2, p), o.background(2, p)
+    ws = wt.make_wave3d_workspace(g)
+    rng = np.random.default_rng(1)
+    Phi, Pi = rng.standard_normal(o.nn), rng.standard_normal(o.nn)
+    Eg = wt.wave3d_energy(dev(torch.float64, Phi), dev(torch.float64, Pi), cg, ws, metric=um)
+    Eo = o.energy(co, Phi, Pi, use_metric=um)
+    assert abs(Eg - Eo) / abs(Eo) < 1e-12
+
+
+@pytest.mark.parametrize("tags,R", [(0, math.inf), (7, math.inf), (7, 1.5)])
+def test_rhs_sipg(wt, ctx, O, tags, R):
+    import torch
+    g, o = pair(wt, ctx, O, 6, 3, outer_tag=tags)
+    ws = wt.make_wave3d_workspace(g)
+    rng = np.random.default_rng(23)
+    u, ut = rng.standard_normal(o.nn), rng.standard_normal(o.nn)
+    bv = [0.1, -0.2, 0.3, 0.0, 0.5, -0.4]
+    out = g.zeros()
+    wt.rhs_wave3d(out, dev(torch.float64, u), dev(torch.float64, ut), bv, ws, tau=20.0, sommerfeld_R=R)
+    assert rel(host(out), o.rhs_sipg(u, ut, bv, tau=20.0, R=R)) < TOL64
+
+
+@pytest.mark.parametrize("A,tag", [(0.0, 0), (0.05, 0), (0.05, 7)])
+def test_rhs_strong(wt, ctx, O, A, tag):
+    import torch
+    g, o = pair(wt, ctx, O, 5, 3, A=A, outer_tag=tag)
+    ws = wt.make_wave3d_workspace(g)
+    rng = np.random.default_rng(29)
+    u, ut = rng.standard_normal(o.nn), rng.standard_normal(o.nn)
+    out = g.zeros()
+    wt.wave_strong_rhs_mesh(out, dev(torch.float64, u), dev(torch.float64, ut), ws, sommerfeld_R=1.0)
+    assert rel(host(out), o.rhs_strong(u, ut, R=1.0)) < TOL64
+
+
+def test_lap_strong_cons(wt, ctx, O):
+    import torch
+    g, o = pair(wt, ctx, O, 4, 3, periodic=True)
+    ws = wt.make_wave3d_workspace(g)
+    u = np.random.default_rng(31).standard_normal(o.nn)
+    out = g.zeros()
+    wt.wave_lap_strong_conservative_mesh(out, dev(torch.float64, u), 1.0 / 3, ws)
+    assert rel(host(out), o.lap_strong_cons(u, 1.0 / 3)) < TOL64
+
+
+def test_rk4_curved_many_steps(wt, ctx, O):
+    """Fused low-storage RK4 (graph replay) vs the oracle's classic RK4: 40 steps of
+    the warped ADM pulse at N = 8, M = 3 with Sommerfeld faces."""
+    import torch
+    g, o = pair(wt, ctx, O, 8, 3, A=0.05, outer_tag=7)
+    p = wt.workloads.adm_params(2)
+    cg, co = wt.sample_background3d(g, 2, p), o.background(2, p)
+    ws = wt.make_wave3d_workspace(g)
+    x, y, z = o.coords()
+    c, a, w = wt.workloads.pulses(2, 1)
+    Phi = wt.workloads.gaussian_field(x, y, z, c, a, w)
+    Pi = np.zeros_like(Phi)
+    dt = 0.2 * o.min_spacing() / wt.workloads.max_speed(p)
+    Pg, Qg = dev(torch.float64, Phi), dev(torch.float64, Pi)
+    wt.step_rk4_curved(Pg, Qg, cg, ws, dt, 40, eps_KO=0.0, bc3d=wt.make_bc3d([2] * 6), metric=True)
+    Po, Qo = o.evolve_curved(co, Phi, Pi, dt, 40, eps_ko=0.0, bc=O.make_bc([2] * 6), use_metric=True)
+    assert rel(host(Pg), Po) < TOL64 and rel(host(Qg), Qo) < TOL64
+    assert not ctx.nonfinite()
+
+
+def test_rk4_curved_with_ko(wt, ctx, O):
+    import torch
+    g, o = pair(wt, ctx, O, 4, 3, outer_tag=7)
+    cg, co = wt.sample_background3d(g, 0), o.background(0)
+    ws = wt.make_wave3d_workspace(g)
+    rng = np.random.default_rng(8)
+    Phi, Pi = rng.standard_normal(o.nn) * 1e-3, rng.standard_normal(o.nn) * 1e-3
+    dt = 0.1 * o.min_spacing()
+    Pg, Qg = dev(torch.float64, Phi), dev(torch.float64, Pi)
+    wt.step_rk4_curved(Pg, Qg, cg, ws, dt, 10, eps_KO=0.1, bc3d=wt.make_bc3d([2] * 6))
+    Po, Qo = o.evolve_curved(co, Phi, Pi, dt, 10, eps_ko=0.1, bc=O.make_bc([2] * 6))
+    assert rel(host(Pg), Po) < TOL64 and rel(host(Qg), Qo) < TOL64
+
+
+@pytest.mark.parametrize("tau", [37.5, 20.0])
+def test_sipg_standing_wave_100_steps(wt, ctx, O, tau):
+    """The flat SIPG standing-wave workload (4^3 elements, n = 6, KO 0.1, RK4 CFL 0.25,
+    100 steps) against the oracle; tau = 20 (the workload's value, sub-critical at
+    n = 6) and the reference driver's 1.5 (N-1)^2."""
+    import torch
+    g, o = pair(wt, ctx, O, 6, 4, outer_tag=0)
+    ws = wt.make_wave3d_workspace(g)
+    x, y, z = o.coords()
+    u0 = wt.workloads.standing_wave(x, y, z)
+    dt = 0.25 * o.min_spacing()
+    ug, vg = dev(torch.float64, u0), g.zeros()
+    wt.step_rk4_sipg(ug, vg, ws, dt, 100, tau=tau, eps_KO=0.1)
+    uo, vo = o.evolve_sipg(u0, np.zeros_like(u0), dt, 100, tau=tau, eps_ko=0.1)
+    tol = TOL64 if tau > 30 else 1e-10
+    assert rel(host(ug), uo) < tol and rel(host(vg), vo) < tol
+
+
+def test_evolve_host_matches_device_stepping(wt, ctx, O):
+    import torch
+    g, o = pair(wt, ctx, O, 4, 3, A=0.05, outer_tag=7)
+    p = wt.workloads.adm_params(5)
+    cg, co = wt.sample_background3d(g, 2, p), o.background(2, p)
+    ws = wt.make_wave3d_workspace(g)
+    x, y, z = o.coords()
+    Phi = wt.workloads.gaussian_field(x, y, z, *wt.workloads.pulses(5, 1))
+    Pi = np.zeros_like(Phi)
+    dt = 0.2 * o.min_spacing() / wt.workloads.max_speed(p)
+    Ph, Qh = Phi.copy(), Pi.copy()
+    E = np.zeros(3)
+    wt.evolve_curved_host(Ph, Qh, cg, ws, dt, 5, 3, bc3d=wt.make_bc3d([2] * 6), metric=True, energy=E)
+    Po, Qo, Eo = o.evolve_curved(co, Phi, Pi, dt, 15, bc=O.make_bc([2] * 6), use_metric=True, record_energy=True)
+    assert rel(Ph, Po) < TOL64 and rel(Qh, Qo) < TOL64
+    assert abs(E[-1] - Eo[-1]) / Eo[-1] < 1e-11
+    assert E[-1] <= E[0] * (1 + 1e-6)
+
+
+def test_fp32_form_rhs(wt, ctx, O):
+    import torch
+    g, o = pair(wt, ctx, O, 8, 2, A=0.05, outer_tag=7, precision=1)
+    p = wt.workloads.adm_params(6)
+    cg, co = wt.sample_background3d(g, 2, p), o.background(2, p)
+    ws = wt.make_wave3d_workspace(g)
+    x, y, z = o.coords()
+    Phi = wt.workloads.gaussian_field(x, y, z, *wt.workloads.pulses(6, 2))
+    Pi = 0.1 * Phi
+    Pd, Qd = g.zeros(), g.zeros()
+    wt.wave3d_curved_rhs(Pd, Qd, dev(torch.float32, Phi), dev(torch.float32, Pi), cg, ws, eps_KO=0.0,
+                         bc3d=wt.make_bc3d([2] * 6), metric=True)
+    Po, Qo = o.rhs_curved(co, Phi, Pi, eps_ko=0.0, bc=O.make_bc([2] * 6), use_metric=True)
+    assert rel(host(Pd), Po) < TOL32 and rel(host(Qd), Qo) < TOL32
+
+
+def test_errors_are_reported(wt, ctx):
+    with pytest.raises(wt.WaveToyError):
+        wt.Mesh.uniform_hex(ctx, 12, 2)
+    with pytest.raises(wt.WaveToyError):
+        wt.Mesh.uniform_hex(ctx, 4, 0)
+    g = wt.Mesh.uniform_hex(ctx, 4, 2)
+    ws = wt.make_wave3d_workspace(g)
+    cg = wt.sample_background3d(g, 0)
+    a = g.zeros()
+    with pytest.raises(wt.WaveToyError):
+        wt.wave3d_curved_rhs(a, a.clone(), a.clone(), a.clone(), cg, ws, bc3d=wt.BC3D((9,) * 6))
+    with pytest.raises(wt.WaveToyError):
+        wt.apply_D(a, a.clone(), 4, ws)
+    with pytest.raises(wt.WaveToyError):
+        wt.step_rk4_curved(a, a.clone(), cg, ws, -1.0, 3)

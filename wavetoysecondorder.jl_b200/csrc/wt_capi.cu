@@ -1,0 +1,965 @@
+// wt_capi.cu -- host runtime behind the C ABI of include/wavetoy_b200.h.
+//
+// Owns device memory for meshes, background coefficients and workspaces,
+// validates arguments (ArgumentError in the reference -> WT_EINVAL with a
+// message), orders launches on the context stream and replays the RK4 step as
+// a CUDA graph.  No CPU fallback exists: every numeric entry point runs the
+// kernels of wt_cons.cu / wt_second.cu / wt_reduce.cu.
+#include "wt_common.cuh"
+#include "../../include/wavetoy_b200.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+struct wt_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream launches go to
+  cudaStream_t own_stream = nullptr;  // the context's own stream
+  std::string err;
+  long long launches = 0;
+  unsigned int* d_flag = nullptr;
+  double* d_partial = nullptr;
+  int nblocks = 0;
+};
+
+struct wt_mesh {
+  wt_ctx* ctx = nullptr;
+  wt::DevMesh m;
+  std::vector<void*> owned;
+};
+
+struct wt_coef {
+  wt_ctx* ctx = nullptr;
+  wt_mesh* mesh = nullptr;
+  wt::DevCoef c;
+};
+
+struct wt_ws {
+  wt_ctx* ctx = nullptr;
+  wt_mesh* mesh = nullptr;
+  double mu = 0.0, inv_mu5 = 0.0;
+  void* F = nullptr;      // 3 nn
+  void* bbuf = nullptr;   // nbf N^2
+  void* grad = nullptr;   // 3 nn
+  void* kP = nullptr;     // nn (Phidot / u_t slope)
+  void* kQ = nullptr;     // nn
+  void* S0 = nullptr;     // stage buffers
+  void* S1 = nullptr;
+  void* SQ = nullptr;
+  void* accP = nullptr;
+  void* accQ = nullptr;
+  void* trace = nullptr;  // 6 N^2 Ne
+  void* zero = nullptr;   // nn zeros
+  void* Lu = nullptr;     // nn
+};
+
+namespace {
+
+int fail(wt_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int cuda_fail(wt_ctx* ctx, cudaError_t e, const char* where) {
+  return fail(ctx, WT_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+size_t rsize(int precision) { return precision == 0 ? sizeof(double) : sizeof(float); }
+
+template <typename T>
+int dalloc(wt_ctx* ctx, T** p, size_t bytes, std::vector<void*>* owner) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc((void**)p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, WT_ENOMEM, std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
+                                    cudaGetErrorString(e));
+  }
+  if (owner) owner->push_back((void*)*p);
+  return 0;
+}
+
+#define WT_TRY(x)            \
+  do {                       \
+    int _rc = (x);           \
+    if (_rc != 0) return _rc; \
+  } while (0)
+
+int lrc(wt_ctx* ctx, int rc, const char* where) {
+  if (rc == 0) return 0;
+  if (rc == -4) return fail(ctx, WT_ENOTSUP, std::string(where) + ": configuration not supported");
+  if (rc == -3) return fail(ctx, WT_ENOMEM, std::string(where) + ": out of device memory");
+  cudaError_t e = cudaGetLastError();
+  return fail(ctx, WT_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// Boundary-face slots, line tables and device copies of the connectivity.
+int finish_topology(wt_mesh* mh) {
+  wt::DevMesh& m = mh->m;
+  wt_ctx* ctx = mh->ctx;
+  const long long Ne = m.Ne;
+  std::vector<int32_t> slot(6 * Ne, -1);
+  int nbf = 0;
+  for (long long e = 0; e < Ne; ++e)
+    for (int f = 0; f < 6; ++f)
+      if (m.h_bdry[f + 6 * e] != 0) slot[f + 6 * e] = nbf++;
+  m.nbf = nbf;
+  WT_TRY(dalloc(ctx, &m.nbr, 6 * Ne * sizeof(int32_t), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.nbrf, 6 * Ne * sizeof(int32_t), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.bdry, 6 * Ne * sizeof(int32_t), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.bslot, 6 * Ne * sizeof(int32_t), &mh->owned));
+  cudaMemcpyAsync(m.nbr, m.h_nbr.data(), 6 * Ne * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(m.nbrf, m.h_nbrf.data(), 6 * Ne * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(m.bdry, m.h_bdry.data(), 6 * Ne * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(m.bslot, slot.data(), 6 * Ne * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream);
+  // lines along each axis: follow face 2d+1 neighbours whose matching face is 2d
+  for (int d = 0; d < 3; ++d) {
+    std::vector<char> seen(Ne, 0);
+    std::vector<int32_t> all;
+    int len = -1, nl = 0, closed = -1;
+    bool ok = true;
+    auto fwd = [&](long long e) -> long long {
+      int en = m.h_nbr[2 * d + 1 + 6 * e];
+      if (en < 0 || m.h_nbrf[2 * d + 1 + 6 * e] != 2 * d || m.h_bdry[2 * d + 1 + 6 * e] != 0) return -1;
+      return en;
+    };
+    auto has_back = [&](long long e) -> bool {
+      int en = m.h_nbr[2 * d + 6 * e];
+      return en >= 0 && m.h_nbrf[2 * d + 6 * e] == 2 * d + 1 && m.h_bdry[2 * d + 6 * e] == 0;
+    };
+    for (long long e0 = 0; e0 < Ne && ok; ++e0) {
+      if (seen[e0] || has_back(e0)) continue;
+      std::vector<int32_t> ln;
+      for (long long e = e0; e >= 0 && !seen[e]; e = fwd(e)) { seen[e] = 1; ln.push_back((int32_t)e); }
+      if (len < 0) len = (int)ln.size();
+      if ((int)ln.size() != len || closed == 1) ok = false;
+      closed = 0;
+      all.insert(all.end(), ln.begin(), ln.end());
+      ++nl;
+    }
+    for (long long e0 = 0; e0 < Ne && ok; ++e0) {  // periodic (closed) lines
+      if (seen[e0]) continue;
+      std::vector<int32_t> ln;
+      long long e = e0;
+      while (e >= 0 && !seen[e]) { seen[e] = 1; ln.push_back((int32_t)e); e = fwd(e); }
+      if (e != e0) { ok = false; break; }
+      if (len < 0) len = (int)ln.size();
+      if ((int)ln.size() != len || closed == 0) ok = false;
+      closed = 1;
+      all.insert(all.end(), ln.begin(), ln.end());
+      ++nl;
+    }
+    m.line_ok[d] = ok && len > 0 ? 1 : 0;
+    if (m.line_ok[d]) {
+      m.nlines[d] = nl; m.line_len[d] = len; m.line_closed[d] = closed == 1;
+      WT_TRY(dalloc(ctx, &m.lines[d], all.size() * sizeof(int32_t), &mh->owned));
+      cudaMemcpyAsync(m.lines[d], all.data(), all.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream);
+    }
+  }
+  return 0;
+}
+
+int alloc_geometry(wt_mesh* mh) {
+  wt::DevMesh& m = mh->m;
+  wt_ctx* ctx = mh->ctx;
+  const long long nn = m.nn;
+  const int N = m.N;
+  m.ops = wt::gll_operators(N);
+  WT_TRY(dalloc(ctx, &m.G, N * N * sizeof(double), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.H, N * sizeof(double), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.x, N * sizeof(double), &mh->owned));
+  cudaMemcpyAsync(m.G, m.ops.G.data(), N * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(m.H, m.ops.H.data(), N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(m.x, m.ops.x.data(), N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  WT_TRY(dalloc(ctx, &m.coords, 3 * nn * sizeof(double), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.jac, 9 * nn * sizeof(double), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.invjac, 9 * nn * sizeof(double), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.detjac, nn * sizeof(double), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.Hphys, nn * sizeof(double), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.Ja, 9 * nn * sizeof(double), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.invdetJ, nn * sizeof(double), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.Hd, nn * sizeof(double), &mh->owned));
+  WT_TRY(dalloc(ctx, &m.handed, m.Ne * sizeof(int32_t), &mh->owned));
+  const size_t rs = rsize(m.precision);
+  if (m.precision == 0) {
+    m.Ja_r = m.Ja;
+    m.invdetJ_r = m.invdetJ;
+  } else {
+    WT_TRY(dalloc(ctx, &m.Ja_r, 9 * nn * rs, &mh->owned));
+    WT_TRY(dalloc(ctx, &m.invdetJ_r, nn * rs, &mh->owned));
+  }
+  WT_TRY(dalloc(ctx, &m.sdiag, 3 * m.Ne * rs, &mh->owned));
+  WT_TRY(dalloc(ctx, &m.bnorm, (size_t)5 * (m.nbf > 0 ? m.nbf : 1) * N * N * rs, &mh->owned));
+  return 0;
+}
+
+int derive_geometry(wt_mesh* mh) {
+  wt::DevMesh& m = mh->m;
+  cudaStream_t s = mh->ctx->stream;
+  WT_TRY(lrc(mh->ctx, wt::launch_geom_derived(m, s), "geometry"));
+  WT_TRY(lrc(mh->ctx, wt::launch_metric(m, s), "metric terms"));
+  if (m.precision == 0) {
+    // Ja_r aliases Ja; still need sdiag
+  }
+  WT_TRY(lrc(mh->ctx, wt::launch_streamed_geometry(m, s), "streamed geometry"));
+  WT_TRY(lrc(mh->ctx, wt::launch_boundary_normals(m, s), "boundary normals"));
+  mh->ctx->launches += 6;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(mh->ctx, e, "mesh set-up");
+  return 0;
+}
+
+void free_mesh(wt_mesh* mh) {
+  for (void* p : mh->owned) cudaFree(p);
+  mh->owned.clear();
+}
+
+int ensure(wt_ws* ws, void** p, size_t bytes) {
+  if (*p) return 0;
+  return dalloc(ws->ctx, p, bytes, nullptr);
+}
+
+int ws_buffers(wt_ws* ws) {
+  const wt::DevMesh& m = ws->mesh->m;
+  const size_t rs = rsize(m.precision);
+  const size_t nb = (size_t)m.nn * rs;
+  WT_TRY(ensure(ws, &ws->F, 3 * nb));
+  WT_TRY(ensure(ws, &ws->bbuf, (size_t)(m.nbf > 0 ? m.nbf : 1) * m.N * m.N * rs));
+  return 0;
+}
+
+int ws_step_buffers(wt_ws* ws) {
+  const wt::DevMesh& m = ws->mesh->m;
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  WT_TRY(ws_buffers(ws));
+  WT_TRY(ensure(ws, &ws->S0, nb));
+  WT_TRY(ensure(ws, &ws->S1, nb));
+  WT_TRY(ensure(ws, &ws->SQ, nb));
+  WT_TRY(ensure(ws, &ws->accP, nb));
+  WT_TRY(ensure(ws, &ws->accQ, nb));
+  return 0;
+}
+
+int ws_k_buffers(wt_ws* ws) {
+  const wt::DevMesh& m = ws->mesh->m;
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  WT_TRY(ensure(ws, &ws->kP, nb));
+  WT_TRY(ensure(ws, &ws->kQ, nb));
+  return 0;
+}
+
+int reduce_to_host(wt_ctx* ctx, double* out) {
+  std::vector<double> h(ctx->nblocks);
+  cudaMemcpyAsync(h.data(), ctx->d_partial, ctx->nblocks * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "reduction");
+  double s = 0.0;
+  for (double v : h) s += v;
+  *out = s;
+  return 0;
+}
+
+int make_bc(wt_ctx* ctx, const wt_bc_desc* bc, int use_metric, wt::ConsBC& out) {
+  out = wt::ConsBC();
+  if (!bc) return 0;
+  for (int f = 0; f < 6; ++f) {
+    if (bc->kinds[f] < 1 || bc->kinds[f] > 4)
+      return fail(ctx, WT_EINVAL, "unknown boundary condition kind " + std::to_string(bc->kinds[f]) +
+                                      " (expected 1 dirichlet, 2 sommerfeld, 3 excision, 4 full_dirichlet)");
+  }
+  out.on = 1;
+  out.curv = use_metric ? 1 : 0;
+  for (int f = 0; f < 6; ++f) out.kinds[f] = bc->kinds[f];
+  out.sigma = bc->sigma;
+  out.exc_tag = bc->excision_tag;
+  out.gPhi = bc->gPhi; out.gPi = bc->gPi; out.gDx = bc->gDx; out.gDy = bc->gDy; out.gDz = bc->gDz;
+  if (use_metric && bc->kinds[0] == WT_BC_EXCISION && bc->excision_tag == 0) out.on = 0;
+  return 0;
+}
+
+int check_ws(wt_ctx* ctx, wt_ws* ws) {
+  if (!ctx) return WT_EINVAL;
+  if (!ws) return fail(ctx, WT_EINVAL, "workspace is NULL");
+  if (ws->ctx != ctx) return fail(ctx, WT_EINVAL, "workspace belongs to another context");
+  return 0;
+}
+
+// One RHS evaluation of the conservative system (non-fused).
+int rhs_curved_impl(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, void* Phid,
+                    void* Pid, double eps_ko, const wt::ConsBC& bc, int use_metric) {
+  const wt::DevMesh& m = ws->mesh->m;
+  wt::RKStage rk;
+  WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, Phi, Pi, ws->F, Phid, ws->bbuf, nullptr, use_metric, bc, rk,
+                                     ctx->stream), "rhs K1"));
+  WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, Pid, ws->bbuf, use_metric, bc, rk, nullptr, ctx->stream), "rhs K2"));
+  ctx->launches += 2;
+  if (eps_ko != 0.0) {
+    const double koT = eps_ko * ws->inv_mu5;
+    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Phid, Phi, koT, ctx->stream), "Kreiss-Oliger"));
+    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Pid, Pi, koT, ctx->stream), "Kreiss-Oliger"));
+    ctx->launches += 6;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wt_ctx_create(int device, wt_ctx** out) {
+  if (!out) return WT_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return WT_ECUDA;
+  }
+  if (device < 0 || device >= ndev) return WT_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) return WT_ECUDA;
+  auto* c = new wt_ctx();
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return WT_ECUDA; }
+  c->stream = c->own_stream;
+  c->nblocks = wt::reduce_blocks();
+  if (cudaMalloc(&c->d_flag, sizeof(unsigned int)) != cudaSuccess ||
+      cudaMalloc(&c->d_partial, c->nblocks * sizeof(double)) != cudaSuccess) {
+    delete c;
+    return WT_ENOMEM;
+  }
+  cudaMemset(c->d_flag, 0, sizeof(unsigned int));
+  *out = c;
+  return 0;
+}
+
+int wt_ctx_destroy(wt_ctx* ctx) {
+  if (!ctx) return WT_EINVAL;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->d_flag);
+  cudaFree(ctx->d_partial);
+  cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return 0;
+}
+
+const char* wt_last_error(const wt_ctx* ctx) { return ctx ? ctx->err.c_str() : "NULL context"; }
+
+int wt_ctx_synchronize(wt_ctx* ctx) {
+  if (!ctx) return WT_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "synchronize");
+}
+
+int wt_ctx_get_stream(wt_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return WT_EINVAL;
+  *stream = (void*)ctx->stream;
+  return 0;
+}
+
+int wt_ctx_set_stream(wt_ctx* ctx, void* stream) {
+  if (!ctx) return WT_EINVAL;
+  cudaStreamSynchronize(ctx->stream);
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return 0;
+}
+
+int wt_ctx_launch_count(const wt_ctx* ctx, long long* count) {
+  if (!ctx || !count) return WT_EINVAL;
+  *count = ctx->launches;
+  return 0;
+}
+
+int wt_ctx_nonfinite(wt_ctx* ctx, int* flag) {
+  if (!ctx || !flag) return WT_EINVAL;
+  unsigned int h = 0;
+  cudaMemcpyAsync(&h, ctx->d_flag, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemsetAsync(ctx->d_flag, 0, sizeof(unsigned int), ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "nonfinite flag");
+  *flag = h ? 1 : 0;
+  return 0;
+}
+
+// ---- mesh -------------------------------------------------------------------
+int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* d, wt_mesh** out) {
+  if (!ctx) return WT_EINVAL;
+  if (!d || !out) return fail(ctx, WT_EINVAL, "wt_mesh_create: NULL argument");
+  *out = nullptr;
+  if (d->N < 2 || d->N > WT_MAXN) return fail(ctx, WT_EINVAL, "N must be in 2..8, got " + std::to_string(d->N));
+  if (d->M[0] < 1 || d->M[1] < 1 || d->M[2] < 1) return fail(ctx, WT_EINVAL, "element counts must be >= 1");
+  if (d->precision != WT_F64 && d->precision != WT_F32) return fail(ctx, WT_EINVAL, "precision must be WT_F64 or WT_F32");
+  if (!(d->x1 > d->x0)) return fail(ctx, WT_EINVAL, "x1 must exceed x0");
+  cudaSetDevice(ctx->device);
+  auto* mh = new wt_mesh();
+  mh->ctx = ctx;
+  wt::DevMesh& m = mh->m;
+  m.N = d->N;
+  for (int a = 0; a < 3; ++a) m.M[a] = d->M[a];
+  m.Ne = (long long)d->M[0] * d->M[1] * d->M[2];
+  m.nn = m.Ne * d->N * d->N * d->N;
+  m.precision = d->precision;
+  m.affine = d->warp_A == 0.0;
+  m.h_nbr.assign(6 * m.Ne, -1);
+  m.h_nbrf.assign(6 * m.Ne, 0);
+  m.h_bdry.assign(6 * m.Ne, 0);
+  const int Mx = d->M[0], My = d->M[1], Mz = d->M[2];
+  for (long long e = 0; e < m.Ne; ++e) {
+    int c[3] = {(int)(e % Mx), (int)((e / Mx) % My), (int)(e / ((long long)Mx * My))};
+    for (int f = 0; f < 6; ++f) {
+      const int ax = f >> 1;
+      int cc[3] = {c[0], c[1], c[2]};
+      cc[ax] += (f & 1) ? 1 : -1;
+      if (cc[ax] < 0 || cc[ax] >= d->M[ax]) {
+        if (!d->periodic) {
+          m.h_bdry[f + 6 * e] = d->outer_tag == 0 ? f + 1 : d->outer_tag;
+          continue;
+        }
+        cc[ax] = (cc[ax] + d->M[ax]) % d->M[ax];
+      }
+      m.h_nbr[f + 6 * e] = (int32_t)(cc[0] + (long long)Mx * (cc[1] + (long long)My * cc[2]));
+      m.h_nbrf[f + 6 * e] = f ^ 1;
+    }
+  }
+  int rc = finish_topology(mh);
+  if (!rc) rc = alloc_geometry(mh);
+  if (!rc) rc = lrc(ctx, wt::launch_geom_analytic(m, d->x0, d->x1, d->warp_A, ctx->stream), "geometry");
+  if (!rc) rc = derive_geometry(mh);
+  if (rc) { free_mesh(mh); delete mh; return rc; }
+  ctx->launches += 1;
+  *out = mh;
+  return 0;
+}
+
+int wt_mesh_create_arrays(wt_ctx* ctx, int N, long long Ne, const double* coords, const double* jac,
+                          const int32_t* neighbour, const int32_t* neighbour_face, const int8_t* orientation,
+                          const int8_t* bdry, int precision, wt_mesh** out) {
+  if (!ctx) return WT_EINVAL;
+  if (!out || !coords || !jac || !neighbour || !neighbour_face || !bdry)
+    return fail(ctx, WT_EINVAL, "wt_mesh_create_arrays: NULL argument");
+  *out = nullptr;
+  if (N < 2 || N > WT_MAXN) return fail(ctx, WT_EINVAL, "N must be in 2..8");
+  if (Ne < 1) return fail(ctx, WT_EINVAL, "Ne must be >= 1");
+  if (precision != WT_F64 && precision != WT_F32) return fail(ctx, WT_EINVAL, "bad precision");
+  if (orientation)
+    for (long long i = 0; i < 6 * Ne; ++i)
+      if (orientation[i] != 0)
+        return fail(ctx, WT_ENOTSUP, "face orientation != 0 is not supported by this build");
+  cudaSetDevice(ctx->device);
+  auto* mh = new wt_mesh();
+  mh->ctx = ctx;
+  wt::DevMesh& m = mh->m;
+  m.N = N; m.Ne = Ne; m.nn = Ne * N * N * N; m.precision = precision; m.affine = 0;
+  m.h_nbr.resize(6 * Ne); m.h_nbrf.resize(6 * Ne); m.h_bdry.resize(6 * Ne);
+  for (long long i = 0; i < 6 * Ne; ++i) {
+    const int en = neighbour[i];
+    if (en < 0 || en > Ne) { delete mh; return fail(ctx, WT_EINVAL, "neighbour index out of range"); }
+    m.h_nbr[i] = en - 1;
+    const int fn = neighbour_face[i];
+    if (en > 0 && (fn < 1 || fn > 6)) { delete mh; return fail(ctx, WT_EINVAL, "neighbour_face out of range"); }
+    m.h_nbrf[i] = en > 0 ? fn - 1 : 0;
+    m.h_bdry[i] = bdry[i];
+  }
+  int rc = finish_topology(mh);
+  if (!rc) rc = alloc_geometry(mh);
+  if (!rc) {
+    cudaMemcpyAsync(m.coords, coords, 3 * m.nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(m.jac, jac, 9 * m.nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    rc = derive_geometry(mh);
+  }
+  if (rc) { free_mesh(mh); delete mh; return rc; }
+  *out = mh;
+  return 0;
+}
+
+int wt_mesh_destroy(wt_mesh* mh) {
+  if (!mh) return WT_EINVAL;
+  cudaStreamSynchronize(mh->ctx->stream);
+  free_mesh(mh);
+  delete mh;
+  return 0;
+}
+
+int wt_mesh_info(const wt_mesh* mh, int* N, long long* Ne, int* precision) {
+  if (!mh) return WT_EINVAL;
+  if (N) *N = mh->m.N;
+  if (Ne) *Ne = mh->m.Ne;
+  if (precision) *precision = mh->m.precision;
+  return 0;
+}
+
+int wt_mesh_get(const wt_mesh* mh, const char* name, void* host_out) {
+  if (!mh || !name || !host_out) return WT_EINVAL;
+  const wt::DevMesh& m = mh->m;
+  wt_ctx* ctx = mh->ctx;
+  std::string s(name);
+  const void* src = nullptr;
+  size_t bytes = 0;
+  if (s == "coords") { src = m.coords; bytes = 3 * m.nn * sizeof(double); }
+  else if (s == "jac") { src = m.jac; bytes = 9 * m.nn * sizeof(double); }
+  else if (s == "invjac") { src = m.invjac; bytes = 9 * m.nn * sizeof(double); }
+  else if (s == "detjac") { src = m.detjac; bytes = m.nn * sizeof(double); }
+  else if (s == "Hphys") { src = m.Hphys; bytes = m.nn * sizeof(double); }
+  else if (s == "Hd") { src = m.Hd; bytes = m.nn * sizeof(double); }
+  else if (s == "invdetJ") { src = m.invdetJ; bytes = m.nn * sizeof(double); }
+  else if (s == "Ja") { src = m.Ja; bytes = 9 * m.nn * sizeof(double); }
+  else if (s == "x") { std::memcpy(host_out, m.ops.x.data(), m.N * sizeof(double)); return 0; }
+  else if (s == "H") { std::memcpy(host_out, m.ops.H.data(), m.N * sizeof(double)); return 0; }
+  else if (s == "G") { std::memcpy(host_out, m.ops.G.data(), m.N * m.N * sizeof(double)); return 0; }
+  else if (s == "bdry") { std::memcpy(host_out, m.h_bdry.data(), 6 * m.Ne * sizeof(int32_t)); return 0; }
+  else if (s == "neighbour") {
+    int32_t* o = (int32_t*)host_out;
+    for (long long i = 0; i < 6 * m.Ne; ++i) o[i] = m.h_nbr[i] + 1;
+    return 0;
+  } else if (s == "handedness") { src = m.handed; bytes = m.Ne * sizeof(int32_t); }
+  else return fail(ctx, WT_EINVAL, "wt_mesh_get: unknown array '" + s + "'");
+  cudaMemcpyAsync(host_out, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "wt_mesh_get");
+}
+
+int wt_mesh_set_bdry(wt_mesh* mh, const int32_t* bdry) {
+  if (!mh || !bdry) return WT_EINVAL;
+  wt::DevMesh& m = mh->m;
+  // the set of boundary faces must not change (slots and normals are precomputed)
+  for (long long i = 0; i < 6 * m.Ne; ++i)
+    if ((bdry[i] != 0) != (m.h_bdry[i] != 0))
+      return fail(mh->ctx, WT_EINVAL, "wt_mesh_set_bdry may only relabel existing outer faces");
+  std::memcpy(m.h_bdry.data(), bdry, 6 * m.Ne * sizeof(int32_t));
+  cudaMemcpyAsync(m.bdry, m.h_bdry.data(), 6 * m.Ne * sizeof(int32_t), cudaMemcpyHostToDevice, mh->ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(mh->ctx->stream);
+  return e == cudaSuccess ? 0 : cuda_fail(mh->ctx, e, "wt_mesh_set_bdry");
+}
+
+int wt_mesh_min_spacing(wt_mesh* mh, double* h) {
+  if (!mh || !h) return WT_EINVAL;
+  mh->ctx->launches += 1;
+  return lrc(mh->ctx, wt::launch_min_spacing(mh->m, h, mh->ctx->stream), "min spacing");
+}
+
+// ---- background ------------------------------------------------------------------
+static int coef_alloc(wt_ctx* ctx, wt_mesh* mesh, wt_coef** out) {
+  auto* c = new wt_coef();
+  c->ctx = ctx; c->mesh = mesh;
+  c->c.nn = mesh->m.nn;
+  c->c.precision = mesh->m.precision;
+  if (dalloc(ctx, &c->c.c11, 11 * c->c.nn * sizeof(double), nullptr) ||
+      dalloc(ctx, &c->c.c10, 10 * c->c.nn * rsize(c->c.precision), nullptr)) {
+    cudaFree(c->c.c11);
+    delete c;
+    return WT_ENOMEM;
+  }
+  *out = c;
+  return 0;
+}
+
+int wt_background_set(wt_ctx* ctx, wt_mesh* mesh, const wt_background_desc* desc, wt_coef** out) {
+  if (!ctx) return WT_EINVAL;
+  if (!mesh || !desc || !out) return fail(ctx, WT_EINVAL, "wt_background_set: NULL argument");
+  if (desc->kind < 0 || desc->kind > 3) return fail(ctx, WT_EINVAL, "unknown background kind");
+  if (desc->kind == WT_BG_ADM_PERTURBED && !(desc->p[3] > 0))
+    return fail(ctx, WT_EINVAL, "ADM background needs a positive Gaussian width p[3]");
+  wt_coef* c = nullptr;
+  WT_TRY(coef_alloc(ctx, mesh, &c));
+  int rc = lrc(ctx, wt::launch_background(mesh->m, c->c, desc->kind, desc->p, ctx->stream), "background");
+  if (!rc) rc = lrc(ctx, wt::launch_coef_combine(mesh->m, c->c, ctx->stream), "background");
+  ctx->launches += 2;
+  if (!rc) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "background");
+  }
+  if (rc) { wt_coef_destroy(c); return rc; }
+  *out = c;
+  return 0;
+}
+
+int wt_background_set_arrays(wt_ctx* ctx, wt_mesh* mesh, const double* coef11, wt_coef** out) {
+  if (!ctx) return WT_EINVAL;
+  if (!mesh || !coef11 || !out) return fail(ctx, WT_EINVAL, "wt_background_set_arrays: NULL argument");
+  wt_coef* c = nullptr;
+  WT_TRY(coef_alloc(ctx, mesh, &c));
+  cudaMemcpyAsync(c->c.c11, coef11, 11 * c->c.nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  int rc = lrc(ctx, wt::launch_coef_combine(mesh->m, c->c, ctx->stream), "background");
+  ctx->launches += 1;
+  if (!rc) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "background");
+  }
+  if (rc) { wt_coef_destroy(c); return rc; }
+  *out = c;
+  return 0;
+}
+
+int wt_coef_get(const wt_coef* c, double* coef11) {
+  if (!c || !coef11) return WT_EINVAL;
+  cudaMemcpyAsync(coef11, c->c.c11, 11 * c->c.nn * sizeof(double), cudaMemcpyDeviceToHost, c->ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(c->ctx->stream);
+  return e == cudaSuccess ? 0 : cuda_fail(c->ctx, e, "wt_coef_get");
+}
+
+int wt_coef_destroy(wt_coef* c) {
+  if (!c) return WT_EINVAL;
+  cudaStreamSynchronize(c->ctx->stream);
+  cudaFree(c->c.c11);
+  cudaFree(c->c.c10);
+  delete c;
+  return 0;
+}
+
+// ---- workspace ---------------------------------------------------------------------
+int wt_workspace_create(wt_ctx* ctx, wt_mesh* mesh, wt_ws** out) {
+  if (!ctx) return WT_EINVAL;
+  if (!mesh || !out) return fail(ctx, WT_EINVAL, "wt_workspace_create: NULL argument");
+  auto* ws = new wt_ws();
+  ws->ctx = ctx; ws->mesh = mesh;
+  const wt::DevMesh& m = mesh->m;
+  int rc = ws_buffers(ws);
+  if (!rc) rc = ws_k_buffers(ws);
+  if (rc) { wt_workspace_destroy(ws); return rc; }
+  // mu: 30 power-iteration steps v <- D_1^2 v / ||D_1^2 v|| (src/wave3d_curved.jl:163-175)
+  cudaStream_t s = ctx->stream;
+  rc = lrc(ctx, wt::launch_alt_sign(m, ws->kP, s), "mu");
+  double mu2 = 0.0;
+  for (int it = 0; it < 30 && !rc; ++it) {
+    rc = lrc(ctx, wt::launch_apply_D(m, ws->kP, ws->kQ, 0, s), "mu");
+    if (!rc) rc = lrc(ctx, wt::launch_apply_D(m, ws->kQ, ws->kP, 0, s), "mu");
+    if (!rc) rc = lrc(ctx, wt::launch_sumsq(m.nn, m.precision, ws->kP, ctx->d_partial, ctx->nblocks, s), "mu");
+    double ss = 0.0;
+    if (!rc) rc = reduce_to_host(ctx, &ss);
+    ctx->launches += 3;
+    if (rc) break;
+    mu2 = std::sqrt(ss);
+    if (!(mu2 > 0)) break;
+    rc = lrc(ctx, wt::launch_scale(m.nn, m.precision, ws->kP, mu2, s), "mu");
+    ctx->launches += 1;
+  }
+  if (rc) { wt_workspace_destroy(ws); return rc; }
+  ws->mu = std::sqrt(mu2);
+  ws->inv_mu5 = ws->mu > 0 ? std::pow(1.0 / ws->mu, 5) : 0.0;
+  *out = ws;
+  return 0;
+}
+
+int wt_workspace_destroy(wt_ws* ws) {
+  if (!ws) return WT_EINVAL;
+  cudaStreamSynchronize(ws->ctx->stream);
+  void* bufs[] = {ws->F, ws->bbuf, ws->grad, ws->kP, ws->kQ, ws->S0, ws->S1, ws->SQ, ws->accP, ws->accQ,
+                  ws->trace, ws->zero, ws->Lu};
+  for (void* p : bufs)
+    if (p) cudaFree(p);
+  delete ws;
+  return 0;
+}
+
+int wt_workspace_mu(wt_ws* ws, double* mu) {
+  if (!ws || !mu) return WT_EINVAL;
+  *mu = ws->mu;
+  return 0;
+}
+
+// ---- RHS ----------------------------------------------------------------------------
+int wt_rhs_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, void* Phidot,
+                  void* Pidot, double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!coef || !Phi || !Pi || !Phidot || !Pidot) return fail(ctx, WT_EINVAL, "wt_rhs_curved: NULL argument");
+  if (coef->mesh != ws->mesh) return fail(ctx, WT_EINVAL, "coefficients belong to another mesh");
+  wt::ConsBC b;
+  WT_TRY(make_bc(ctx, bc, use_metric, b));
+  return rhs_curved_impl(ctx, ws, coef, Phi, Pi, Phidot, Pidot, eps_ko, b, use_metric);
+}
+
+int wt_apply_D(wt_ctx* ctx, wt_ws* ws, const void* u, void* Du, int d) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!u || !Du) return fail(ctx, WT_EINVAL, "wt_apply_D: NULL argument");
+  if (d < 1 || d > 3) return fail(ctx, WT_EINVAL, "wt_apply_D: d must be 1, 2 or 3");
+  ctx->launches += 1;
+  return lrc(ctx, wt::launch_apply_D(ws->mesh->m, u, Du, d - 1, ctx->stream), "apply_D");
+}
+
+int wt_ko_add(wt_ctx* ctx, wt_ws* ws, void* dst, const void* field, double eps_ko) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!dst || !field) return fail(ctx, WT_EINVAL, "wt_ko_add: NULL argument");
+  ctx->launches += 3;
+  return lrc(ctx, wt::launch_ko_add(ws->mesh->m, dst, field, eps_ko * ws->inv_mu5, ctx->stream), "Kreiss-Oliger");
+}
+
+int wt_gradient3d(wt_ctx* ctx, wt_ws* ws, const void* u, void* g1, void* g2, void* g3) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!u || !g1 || !g2 || !g3) return fail(ctx, WT_EINVAL, "wt_gradient3d: NULL argument");
+  const wt::DevMesh& m = ws->mesh->m;
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  WT_TRY(ensure(ws, &ws->grad, 3 * nb));
+  wt::DevCoef nocoef;
+  wt::ConsBC bc;
+  wt::RKStage rk;
+  WT_TRY(lrc(ctx, wt::launch_cons_k1(m, nocoef, u, nullptr, nullptr, nullptr, nullptr, ws->grad, 1, bc, rk,
+                                     ctx->stream), "gradient3d"));
+  cudaMemcpyAsync(g1, ws->grad, nb, cudaMemcpyDeviceToDevice, ctx->stream);
+  cudaMemcpyAsync(g2, (char*)ws->grad + nb, nb, cudaMemcpyDeviceToDevice, ctx->stream);
+  cudaMemcpyAsync(g3, (char*)ws->grad + 2 * nb, nb, cudaMemcpyDeviceToDevice, ctx->stream);
+  ctx->launches += 1;
+  return 0;
+}
+
+int wt_divergence3d(wt_ctx* ctx, wt_ws* ws, const void* F1, const void* F2, const void* F3, void* out) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!F1 || !F2 || !F3 || !out) return fail(ctx, WT_EINVAL, "wt_divergence3d: NULL argument");
+  const wt::DevMesh& m = ws->mesh->m;
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  cudaMemcpyAsync(ws->F, F1, nb, cudaMemcpyDeviceToDevice, ctx->stream);
+  cudaMemcpyAsync((char*)ws->F + nb, F2, nb, cudaMemcpyDeviceToDevice, ctx->stream);
+  cudaMemcpyAsync((char*)ws->F + 2 * nb, F3, nb, cudaMemcpyDeviceToDevice, ctx->stream);
+  ctx->launches += 1;
+  return lrc(ctx, wt::launch_div3d(m, ws->F, out, ctx->stream), "divergence3d");
+}
+
+int wt_rhs_sipg(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, void* utt, const double bdry_values[6],
+                double tau, double sommerfeld_R) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!u || !ut || !utt || !bdry_values) return fail(ctx, WT_EINVAL, "wt_rhs_sipg: NULL argument");
+  const wt::DevMesh& m = ws->mesh->m;
+  if (!m.affine) return fail(ctx, WT_ENOTSUP, "wt_rhs_sipg: this build supports axis-aligned affine meshes only");
+  WT_TRY(ensure(ws, &ws->trace, (size_t)6 * m.N * m.N * m.Ne * rsize(m.precision)));
+  const double inv_R = (std::isfinite(sommerfeld_R) && sommerfeld_R > 0) ? 1.0 / sommerfeld_R : 0.0;
+  ctx->launches += 2;
+  return lrc(ctx, wt::launch_sipg(m, u, ut, utt, ws->trace, bdry_values, tau, inv_R, ctx->stream), "rhs_sipg");
+}
+
+int wt_rhs_strong(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, void* utt, double tau,
+                  double sommerfeld_R) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!u || !ut || !utt) return fail(ctx, WT_EINVAL, "wt_rhs_strong: NULL argument");
+  wt::DevMesh& m = ws->mesh->m;
+  if (!m.dinvjac) {
+    WT_TRY(dalloc(ctx, &m.dinvjac, 27 * (size_t)m.nn * sizeof(double), &ws->mesh->owned));
+    WT_TRY(lrc(ctx, wt::launch_dinvjac(m, ctx->stream), "make_metric_derivs"));
+    ctx->launches += 1;
+  }
+  const double inv_R = (std::isfinite(sommerfeld_R) && sommerfeld_R > 0) ? 1.0 / sommerfeld_R : 0.0;
+  ctx->launches += 1;
+  return lrc(ctx, wt::launch_strong(m, u, ut, utt, tau, inv_R, ctx->stream), "rhs_strong");
+}
+
+int wt_lap_strong_cons(wt_ctx* ctx, wt_ws* ws, const void* u, void* Lu, double h, double tau) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!u || !Lu) return fail(ctx, WT_EINVAL, "wt_lap_strong_cons: NULL argument");
+  if (!(h > 0)) return fail(ctx, WT_EINVAL, "wt_lap_strong_cons: h must be positive");
+  if (!ws->mesh->m.affine) return fail(ctx, WT_EINVAL, "wt_lap_strong_cons: uniform Cartesian meshes only");
+  ctx->launches += 1;
+  return lrc(ctx, wt::launch_lap_strong_cons(ws->mesh->m, u, Lu, h, tau, ctx->stream), "lap_strong_cons");
+}
+
+// ---- reductions ---------------------------------------------------------------------------
+int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, int use_metric,
+              double* E) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!coef || !Phi || !Pi || !E) return fail(ctx, WT_EINVAL, "wt_energy: NULL argument");
+  const wt::DevMesh& m = ws->mesh->m;
+  WT_TRY(ensure(ws, &ws->grad, 3 * (size_t)m.nn * rsize(m.precision)));
+  wt::DevCoef nocoef;
+  wt::ConsBC bc;
+  wt::RKStage rk;
+  WT_TRY(lrc(ctx, wt::launch_cons_k1(m, nocoef, Phi, nullptr, nullptr, nullptr, nullptr, ws->grad, use_metric, bc,
+                                     rk, ctx->stream), "energy gradient"));
+  WT_TRY(lrc(ctx, wt::launch_energy(m, coef->c, Pi, ws->grad, use_metric, ctx->d_partial, ctx->nblocks, ctx->stream),
+             "energy"));
+  ctx->launches += 2;
+  return reduce_to_host(ctx, E);
+}
+
+int wt_energy_sipg(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, double tau, double* E) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!u || !ut || !E) return fail(ctx, WT_EINVAL, "wt_energy_sipg: NULL argument");
+  const wt::DevMesh& m = ws->mesh->m;
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  if (!ws->zero) {
+    WT_TRY(ensure(ws, &ws->zero, nb));
+    cudaMemsetAsync(ws->zero, 0, nb, ctx->stream);
+  }
+  WT_TRY(ensure(ws, &ws->Lu, nb));
+  const double bz[6] = {0, 0, 0, 0, 0, 0};
+  WT_TRY(wt_rhs_sipg(ctx, ws, u, ws->zero, ws->Lu, bz, tau, 0.0));
+  double K = 0, V = 0;
+  WT_TRY(lrc(ctx, wt::launch_dot_weighted(m, ut, ut, nullptr, nullptr, 0, 0, ctx->d_partial, ctx->nblocks,
+                                          ctx->stream), "energy_sipg"));
+  WT_TRY(reduce_to_host(ctx, &K));
+  WT_TRY(lrc(ctx, wt::launch_dot_weighted(m, u, ws->Lu, nullptr, nullptr, 0, 0, ctx->d_partial, ctx->nblocks,
+                                          ctx->stream), "energy_sipg"));
+  WT_TRY(reduce_to_host(ctx, &V));
+  ctx->launches += 2;
+  *E = K / 2 - V / 2;
+  return 0;
+}
+
+int wt_l2_diff(wt_ctx* ctx, wt_ws* ws, const void* a, const void* b, int use_metric, double* out) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!a || !out) return fail(ctx, WT_EINVAL, "wt_l2_diff: NULL argument");
+  double s = 0;
+  WT_TRY(lrc(ctx, wt::launch_dot_weighted(ws->mesh->m, a, b, nullptr, nullptr, use_metric ? 1 : 0, 1, ctx->d_partial,
+                                          ctx->nblocks, ctx->stream), "l2"));
+  ctx->launches += 1;
+  WT_TRY(reduce_to_host(ctx, &s));
+  *out = std::sqrt(s);
+  return 0;
+}
+
+// ---- time stepping ------------------------------------------------------------------------
+static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
+                            double eps_ko, const wt::ConsBC& b, int use_metric) {
+  const wt::DevMesh& m = ws->mesh->m;
+  cudaStream_t s = ctx->stream;
+  void* SP[2] = {ws->S0, ws->S1};
+  for (int st = 0; st < 4; ++st) {
+    const void* inP = st == 0 ? Phi : SP[(st - 1) % 2];
+    const void* inQ = st == 0 ? Pi : ws->SQ;
+    wt::RKStage rkP, rkQ;
+    rkP.stage = rkQ.stage = st;
+    rkP.dt = rkQ.dt = dt;
+    rkP.y = Phi; rkP.acc = ws->accP; rkP.out = SP[st % 2];
+    rkQ.y = Pi; rkQ.acc = ws->accQ; rkQ.out = ws->SQ;
+    rkP.nonfinite = rkQ.nonfinite = st == 3 ? ctx->d_flag : nullptr;
+    if (eps_ko == 0.0) {
+      rkP.on = rkQ.on = 1;
+      WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, inP, inQ, ws->F, nullptr, ws->bbuf, nullptr, use_metric, b, rkP,
+                                         s), "rk4 K1"));
+      WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, nullptr, ws->bbuf, use_metric, b, rkQ, rkQ.nonfinite, s),
+                 "rk4 K2"));
+      ctx->launches += 2;
+    } else {
+      WT_TRY(rhs_curved_impl(ctx, ws, coef, inP, inQ, ws->kP, ws->kQ, eps_ko, b, use_metric));
+      WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, st, dt, Phi, ws->accP, SP[st % 2], ws->kP, s), "rk4"));
+      WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, st, dt, Pi, ws->accQ, ws->SQ, ws->kQ, s), "rk4"));
+      ctx->launches += 2;
+    }
+  }
+  return 0;
+}
+
+int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
+                       double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!coef || !Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_step_rk4_curved: NULL argument");
+  if (nsteps < 0) return fail(ctx, WT_EINVAL, "nsteps must be >= 0");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(ctx, WT_EINVAL, "dt must be positive and finite");
+  wt::ConsBC b;
+  WT_TRY(make_bc(ctx, bc, use_metric, b));
+  WT_TRY(ws_step_buffers(ws));
+  if (eps_ko != 0.0) WT_TRY(ws_k_buffers(ws));
+  if (nsteps <= 2) {
+    for (int i = 0; i < nsteps; ++i) WT_TRY(step_curved_once(ctx, ws, coef, Phi, Pi, dt, eps_ko, b, use_metric));
+    return 0;
+  }
+  // capture one step as a CUDA graph and replay it
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long before = ctx->launches;
+  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
+  int rc = step_curved_once(ctx, ws, coef, Phi, Pi, dt, eps_ko, b, use_metric);
+  e = cudaStreamEndCapture(ctx->stream, &graph);
+  if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_fail(ctx, e, "graph instantiate"); }
+  const long long per = ctx->launches - before;
+  ctx->launches = before;
+  for (int i = 0; i < nsteps && e == cudaSuccess; ++i) e = cudaGraphLaunch(exec, ctx->stream);
+  ctx->launches += per * nsteps;
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "graph launch");
+}
+
+static int step_sipg_once(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, const double bv[6], double tau,
+                          double R, double eps_ko) {
+  const wt::DevMesh& m = ws->mesh->m;
+  cudaStream_t s = ctx->stream;
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  for (int st = 0; st < 4; ++st) {
+    const void* inU = st == 0 ? u : ws->S0;
+    const void* inV = st == 0 ? ut : ws->SQ;
+    WT_TRY(wt_rhs_sipg(ctx, ws, inU, inV, ws->kQ, bv, tau, R));
+    cudaMemcpyAsync(ws->kP, inV, nb, cudaMemcpyDeviceToDevice, s);
+    if (eps_ko != 0.0) {
+      const double koT = eps_ko * ws->inv_mu5;
+      WT_TRY(lrc(ctx, wt::launch_ko_add(m, ws->kP, inU, koT, s), "Kreiss-Oliger"));
+      WT_TRY(lrc(ctx, wt::launch_ko_add(m, ws->kQ, inV, koT, s), "Kreiss-Oliger"));
+      ctx->launches += 6;
+    }
+    WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, st, dt, u, ws->accP, ws->S0, ws->kP, s), "rk4"));
+    WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, st, dt, ut, ws->accQ, ws->SQ, ws->kQ, s), "rk4"));
+    ctx->launches += 2;
+  }
+  return 0;
+}
+
+int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int nsteps, const double bdry_values[6],
+                     double tau, double sommerfeld_R, double eps_ko) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!u || !ut || !bdry_values) return fail(ctx, WT_EINVAL, "wt_step_rk4_sipg: NULL argument");
+  if (nsteps < 0 || !(dt > 0)) return fail(ctx, WT_EINVAL, "bad nsteps/dt");
+  if (!ws->mesh->m.affine) return fail(ctx, WT_ENOTSUP, "SIPG stepping supports affine meshes only");
+  WT_TRY(ws_step_buffers(ws));
+  WT_TRY(ws_k_buffers(ws));
+  const wt::DevMesh& m = ws->mesh->m;
+  WT_TRY(ensure(ws, &ws->trace, (size_t)6 * m.N * m.N * m.Ne * rsize(m.precision)));
+  if (nsteps <= 2) {
+    for (int i = 0; i < nsteps; ++i) WT_TRY(step_sipg_once(ctx, ws, u, ut, dt, bdry_values, tau, sommerfeld_R, eps_ko));
+    return 0;
+  }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long before = ctx->launches;
+  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
+  int rc = step_sipg_once(ctx, ws, u, ut, dt, bdry_values, tau, sommerfeld_R, eps_ko);
+  e = cudaStreamEndCapture(ctx->stream, &graph);
+  if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_fail(ctx, e, "graph instantiate"); }
+  const long long per = ctx->launches - before;
+  ctx->launches = before;
+  for (int i = 0; i < nsteps && e == cudaSuccess; ++i) e = cudaGraphLaunch(exec, ctx->stream);
+  ctx->launches += per * nsteps;
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "graph launch");
+}
+
+int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* Phi_host, double* Pi_host, double dt,
+                          int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc, int use_metric,
+                          double* energy) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!coef || !Phi_host || !Pi_host) return fail(ctx, WT_EINVAL, "wt_evolve_curved_host: NULL argument");
+  if (ws->mesh->m.precision != WT_F64)
+    return fail(ctx, WT_ENOTSUP, "wt_evolve_curved_host takes FP64 host buffers; use an FP64 mesh");
+  if (steps_per_sample < 1 || nsamples < 1) return fail(ctx, WT_EINVAL, "steps_per_sample, nsamples must be >= 1");
+  const wt::DevMesh& m = ws->mesh->m;
+  const size_t nb = (size_t)m.nn * sizeof(double);
+  void *dP = nullptr, *dQ = nullptr;
+  WT_TRY(dalloc(ctx, &dP, nb, nullptr));
+  if (dalloc(ctx, &dQ, nb, nullptr)) { cudaFree(dP); return WT_ENOMEM; }
+  int rc = 0;
+  cudaMemcpyAsync(dP, Phi_host, nb, cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(dQ, Pi_host, nb, cudaMemcpyHostToDevice, ctx->stream);
+  for (int sidx = 0; sidx < nsamples && !rc; ++sidx) {
+    rc = wt_step_rk4_curved(ctx, ws, coef, dP, dQ, dt, steps_per_sample, eps_ko, bc, use_metric);
+    if (rc) break;
+    cudaMemcpyAsync(Phi_host, dP, nb, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(Pi_host, dQ, nb, cudaMemcpyDeviceToHost, ctx->stream);
+    if (energy) rc = wt_energy(ctx, ws, coef, dP, dQ, use_metric, &energy[sidx]);
+    int bad = 0;
+    if (!rc) rc = wt_ctx_nonfinite(ctx, &bad);
+    if (!rc && bad) rc = fail(ctx, WT_ENONFINITE, "state became non-finite during evolution");
+  }
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(dP);
+  cudaFree(dQ);
+  return rc;
+}
+
+}  // extern "C"

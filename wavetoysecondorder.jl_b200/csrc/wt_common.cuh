@@ -1,0 +1,185 @@
+// wt_common.cuh -- internal declarations shared by the CUDA translation units of
+// libwavetoy_b200.so.  Not part of the public ABI (include/wavetoy_b200.h is).
+//
+// Data layout in HBM (one mesh, N GLL nodes per axis, Ne elements, nn = N^3 Ne):
+//   * every scalar field is (N,N,N,Ne) element-major, i fastest: one element is a
+//     contiguous block of N^3 values (4 KB for N=8 in FP64), so a CTA that owns an
+//     element reads it with fully coalesced 128-bit loads;
+//   * multi-component fields are structure-of-arrays: component c of field X
+//     lives at X + c*nn (the reference's separate Julia arrays);
+//   * connectivity is int32 [f + 6 e], 0-based, -1 = no neighbour;
+//   * streamed per-node coefficients are stored in the state precision `real`
+//     (double for the plain form, float for the FP32 form); geometry is computed
+//     and kept in FP64 and converted once.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#define WT_MAXN 8
+
+namespace wt {
+
+// ---- host-side GLL operators (product code, independent of the oracle) -----
+struct HostOps {
+  int N = 0;
+  std::vector<double> x, H, G;  // x, H on [0,1]; G[i*N+p]
+};
+HostOps gll_operators(int N);
+
+// ---- device-side mesh --------------------------------------------------------
+struct DevMesh {
+  int N = 0;
+  long long Ne = 0, nn = 0;
+  int precision = 0;   // 0 = double, 1 = float
+  int affine = 1;      // 1 if every Jacobian is diagonal and constant per element
+  int M[3] = {0, 0, 0};
+  // connectivity
+  int32_t* nbr = nullptr;   // [f + 6e]
+  int32_t* nbrf = nullptr;
+  int32_t* bdry = nullptr;
+  int32_t* handed = nullptr;  // [e]
+  std::vector<int32_t> h_nbr, h_nbrf, h_bdry;
+  // operators on device: G (N*N), GT (transposed), H (N), x (N) -- double
+  double* G = nullptr;
+  double* H = nullptr;
+  double* x = nullptr;
+  HostOps ops;
+  // FP64 geometry
+  double* coords = nullptr;  // [a + 3n]
+  double* jac = nullptr;     // [a + 3b + 9n]
+  double* invjac = nullptr;  // [al + 3be + 9n]
+  double* detjac = nullptr;
+  double* Hphys = nullptr;
+  double* Ja = nullptr;      // 9 fields, field-major
+  double* invdetJ = nullptr;
+  double* Hd = nullptr;
+  double* dinvjac = nullptr; // lazily: [a + 3c + 9d + 27n]
+  // streamed copies in the state precision
+  void* Ja_r = nullptr;      // 9 fields
+  void* invdetJ_r = nullptr;
+  void* sdiag = nullptr;     // [3e + d] element-constant axis scale invjac[d,d] at node 0
+  // boundary faces: slot per (f,e) with bdry != 0, -1 otherwise
+  int32_t* bslot = nullptr;
+  int nbf = 0;
+  void* bnorm = nullptr;     // per boundary-face node: (nx, ny, nz, wt_curv, wF/Hphys) in real
+  // lines along each axis (for line-local Kreiss-Oliger): element lists
+  int line_ok[3] = {0, 0, 0};
+  int nlines[3] = {0, 0, 0};
+  int line_len[3] = {0, 0, 0};      // elements per line (all lines equal length)
+  int line_closed[3] = {0, 0, 0};   // periodic lines
+  int32_t* lines[3] = {nullptr, nullptr, nullptr};  // [line*len + pos] element ids
+};
+
+// Kernel-side view of the mesh (passed by value).
+struct MeshView {
+  int N;
+  long long Ne, nn;
+  const int32_t* nbr;
+  const int32_t* nbrf;
+  const int32_t* bdry;
+  const double* G;
+  const double* H;
+};
+
+inline MeshView view(const DevMesh& m) {
+  MeshView v;
+  v.N = m.N; v.Ne = m.Ne; v.nn = m.nn; v.nbr = m.nbr; v.nbrf = m.nbrf; v.bdry = m.bdry;
+  v.G = m.G; v.H = m.H;
+  return v;
+}
+
+// ---- device-side background coefficients --------------------------------------
+struct DevCoef {
+  long long nn = 0;
+  double* c11 = nullptr;  // 11 fields FP64 (sample_background3d! layout)
+  void* c10 = nullptr;    // 10 streamed fields in `real`: a, b1, b2, b3, K11, K12, K13, K22, K23, K33
+  int precision = 0;
+};
+
+// ---- face helpers -----------------------------------------------------------------
+__host__ __device__ inline int faxis(int f) { return f >> 1; }
+__host__ __device__ inline int frow(int f, int N) { return (f & 1) ? N - 1 : 0; }
+__host__ __device__ inline double fsign(int f) { return (f & 1) ? 1.0 : -1.0; }
+__host__ __device__ inline int face_node(int ax, int r, int p, int q, int N) {
+  // local node index of face node (p,q) of the face with axis ax at row r
+  return ax == 0 ? r + N * (p + N * q) : ax == 1 ? p + N * (r + N * q) : p + N * (q + N * r);
+}
+
+// ---- error reporting ----------------------------------------------------------------
+struct Status {
+  int code = 0;
+  std::string msg;
+};
+
+// ---- launchers implemented in the .cu files -------------------------------------------
+// geometry (wt_geom.cu)
+int launch_geom_analytic(DevMesh& m, double x0, double x1, double A, cudaStream_t s);
+int launch_geom_derived(DevMesh& m, cudaStream_t s);
+int launch_metric(DevMesh& m, cudaStream_t s);
+int launch_dinvjac(DevMesh& m, cudaStream_t s);
+int launch_boundary_normals(DevMesh& m, cudaStream_t s);
+int launch_streamed_geometry(DevMesh& m, cudaStream_t s);
+int launch_background(const DevMesh& m, DevCoef& c, int kind, const double* p, cudaStream_t s);
+int launch_coef_combine(const DevMesh& m, DevCoef& c, cudaStream_t s);
+int launch_min_spacing(const DevMesh& m, double* out, cudaStream_t s);
+
+// conservative first-order system (wt_cons.cu)
+struct ConsBC {
+  int on = 0;          // boundary pass requested
+  int curv = 0;        // curvilinear pass (single kind) vs affine per-side kinds
+  int kinds[6] = {0, 0, 0, 0, 0, 0};
+  double sigma = 1.0;
+  int exc_tag = 0;
+  const void* gPhi = nullptr;
+  const void* gPi = nullptr;
+  const void* gDx = nullptr;
+  const void* gDy = nullptr;
+  const void* gDz = nullptr;
+};
+struct RKStage {
+  int on = 0;          // fused RK4 epilogue instead of writing the RHS
+  int stage = 0;       // 0..3
+  double dt = 0.0;
+  void* y = nullptr;   // state (read; written at stage 3)
+  void* acc = nullptr; // accumulator
+  void* out = nullptr; // next stage input
+  unsigned int* nonfinite = nullptr;  // set to 1 if the stage-3 update is not finite
+};
+// K1: gradient, flux F, Phidot (+ affine/curv BC increments), optional RK epilogue for Phi.
+int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
+                   void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
+                   cudaStream_t s);
+// K2: divergence of F (+ boundary increments), optional RK epilogue for Pi.
+int launch_cons_k2(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
+                   const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s);
+int launch_apply_D(const DevMesh& m, const void* u, void* out, int d, cudaStream_t s);
+int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s);
+int launch_div3d(const DevMesh& m, const void* F, void* out, cudaStream_t s);
+
+// second-order forms (wt_second.cu)
+int launch_sipg(const DevMesh& m, const void* u, const void* ut, void* utt, void* trace, const double bvals[6],
+                double tau, double inv_R, cudaStream_t s);
+int launch_strong(const DevMesh& m, const void* u, const void* ut, void* utt, double tau, double inv_R,
+                  cudaStream_t s);
+int launch_lap_strong_cons(const DevMesh& m, const void* u, void* Lu, double h, double tau, cudaStream_t s);
+
+// reductions and vector updates (wt_reduce.cu)
+int launch_energy(const DevMesh& m, const DevCoef& c, const void* Pi, const void* grad, int use_metric,
+                  double* partial, int nblocks, cudaStream_t s);
+int launch_dot_weighted(const DevMesh& m, const void* a, const void* b, const void* c, const void* d,
+                        int weight_kind, int mode, double* partial, int nblocks, cudaStream_t s);
+int launch_sumsq(long long n, int precision, const void* a, double* partial, int nblocks, cudaStream_t s);
+int launch_scale(long long n, int precision, void* a, double s, cudaStream_t st);
+int launch_fill(long long n, int precision, void* a, double v, cudaStream_t st);
+int launch_copy(long long n, int precision, void* dst, const void* src, cudaStream_t st);
+int launch_rk_update(long long n, int precision, int stage, double dt, void* y, void* acc, void* out,
+                     const void* k, cudaStream_t st);
+int launch_axpy(long long n, int precision, void* y, double a, const void* x, cudaStream_t st);
+int launch_alt_sign(const DevMesh& m, void* v, cudaStream_t st);
+int launch_finite_check(long long n, int precision, const void* a, unsigned int* flag, cudaStream_t st);
+int reduce_blocks();
+
+}  // namespace wt

@@ -1,0 +1,663 @@
+// wt_cons.cu -- the hot path: the conservative first-order (Phi, Pi) ADM wave
+// right-hand side of wave3d_curved_rhs! (src/wave3d_curved.jl:205-258) with
+// its boundary passes (src/boundaries3d.jl:58-232), Kreiss-Oliger
+// dissipation (src/wave3d_curved.jl:182-192) and the RK4 stage update.
+//
+// One RHS evaluation is two element-parallel kernels (the two-pass structure
+// HexSBPSAT uses, GOALS.md:138-151, because the divergence SAT needs the
+// neighbour's flux, which needs the neighbour's gradient):
+//   K1  per element: Phi -> smem, neighbour Phi face traces -> smem; split-form
+//       (or affine per-axis) gradient with centred-flux SAT; flux
+//       F^i = beta^i Pi + K^{ij} d_j Phi; Phidot = beta.grad + a Pi; boundary
+//       increments; writes F (3 fields) and either Phidot or the fused RK4
+//       stage update of Phi.
+//   K2  per element: F -> smem, neighbour F face traces -> smem; split-form
+//       divergence with centred-flux SAT; adds the boundary increments; writes
+//       Pidot or the fused RK4 stage update of Pi.
+// One CTA owns EPB elements with one thread per node; every element block is a
+// contiguous N^3 run, so all global loads are fully coalesced; the reference
+// derivative matrix is held transposed in smem so the N-term contractions read
+// conflict-free.  Streamed coefficients: a, beta (3), K (6) and, curvilinear,
+// Ja (9) and 1/J.
+#include "wt_common.cuh"
+
+namespace wt {
+
+template <int N>
+struct Ep {
+  static constexpr int N3 = N * N * N;
+  static constexpr int N2 = N * N;
+  static constexpr int EPB = N3 >= 100 ? 1 : (128 / N3);
+  static constexpr int T = N3 * EPB;
+};
+
+template <typename real>
+struct K1P {
+  long long Ne, nn;
+  const real* Phi;
+  const real* Pi;
+  const real* c10;  // a, b1, b2, b3, K11, K12, K13, K22, K23, K33 (nullptr: gradient only)
+  const real* Ja;
+  const real* invdetJ;
+  const real* sdiag;
+  const int32_t* nbr;
+  const int32_t* nbrf;
+  const int32_t* bdry;
+  const int32_t* bslot;
+  const double* G;
+  const double* H;
+  real* F;
+  real* Phidot;
+  real* bbuf;
+  real* grad_out;
+  int bc_on, bc_curv, exc_tag, nbf;
+  int kinds[6];
+  real sigma;
+  const real* bnorm;
+  const real* gPhi;
+  const real* gPi;
+  const real* gDx;
+  const real* gDy;
+  const real* gDz;
+  int epi, stage;
+  double dt;
+  real* y;
+  real* acc;
+  real* out;
+  unsigned int* nonfinite;
+};
+
+template <typename real>
+__device__ __forceinline__ void rk_epilogue(int stage, double dt, real k, real yin, real* y, real* acc, real* out,
+                                            long long n, unsigned int* nonfinite) {
+  if (stage == 0) {
+    out[n] = yin + (real)(0.5 * dt) * k;
+    acc[n] = yin + (real)(dt / 6.0) * k;
+  } else if (stage == 1) {
+    out[n] = y[n] + (real)(0.5 * dt) * k;
+    acc[n] = acc[n] + (real)(dt / 3.0) * k;
+  } else if (stage == 2) {
+    out[n] = y[n] + (real)dt * k;
+    acc[n] = acc[n] + (real)(dt / 3.0) * k;
+  } else {
+    real v = acc[n] + (real)(dt / 6.0) * k;
+    y[n] = v;
+    if (nonfinite && !isfinite((double)v)) atomicOr(nonfinite, 1u);
+  }
+}
+
+// contraction along axis d of a smem field f (N^3) with transposed G (GT[p*N+i] = G[i][p])
+template <int N, typename real>
+__device__ __forceinline__ real contract(const real* __restrict__ f, const real* __restrict__ GT, int i, int j, int k,
+                                         int d) {
+  real s = 0;
+  if (d == 0) {
+#pragma unroll
+    for (int p = 0; p < N; ++p) s += GT[p * N + i] * f[p + N * (j + N * k)];
+  } else if (d == 1) {
+#pragma unroll
+    for (int p = 0; p < N; ++p) s += GT[p * N + j] * f[i + N * (p + N * k)];
+  } else {
+#pragma unroll
+    for (int p = 0; p < N; ++p) s += GT[p * N + k] * f[i + N * (j + N * p)];
+  }
+  return s;
+}
+
+template <int N, typename real, bool CURV>
+__global__ void __launch_bounds__(Ep<N>::T) k_cons_k1(const K1P<real> P) {
+  constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = Ep<N>::EPB;
+  __shared__ real GT[N2];
+  __shared__ real su[EPB][N3];
+  __shared__ real sun[EPB][6][N2];
+  __shared__ real sw[CURV ? EPB : 1][CURV ? 9 : 1][CURV ? N3 : 1];
+  const int tid = threadIdx.x;
+  const int le = tid / N3, t = tid - le * N3;
+  const int i = t % N, j = (t / N) % N, k = t / N2;
+  const long long e = (long long)blockIdx.x * EPB + le;
+  const bool valid = e < P.Ne;
+  const long long ec = valid ? e : 0;  // clamp for address arithmetic
+  const long long n = ec * N3 + t;
+  const long long nn = P.nn;
+  if (tid < N2) GT[(tid % N) * N + tid / N] = (real)P.G[tid];
+  const real u = valid ? P.Phi[n] : (real)0;
+  su[le][t] = u;
+  // neighbour Phi face traces
+  for (int idx = t; idx < 6 * N2; idx += N3) {
+    const int f = idx / N2, pq = idx - f * N2;
+    real v = 0;
+    if (valid) {
+      const int en = P.nbr[f + 6 * ec];
+      if (en >= 0 && P.bdry[f + 6 * ec] == 0) {
+        const int fn = P.nbrf[f + 6 * ec];
+        v = P.Phi[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq % N, pq / N, N)];
+      }
+    }
+    sun[le][f][pq] = v;
+  }
+  const bool grad_only = P.c10 == nullptr;
+  real a = 0, b[3] = {0, 0, 0}, K[6] = {0, 0, 0, 0, 0, 0}, Pi = 0;
+  if (!grad_only && valid) {
+    a = P.c10[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) b[c] = P.c10[(1 + c) * nn + n];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) K[c] = P.c10[(4 + c) * nn + n];
+    Pi = P.Pi[n];
+  }
+  real m[CURV ? 9 : 1];
+  real invJ = 0, sd[3];
+  if (CURV) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) m[c] = valid ? P.Ja[c * nn + n] : (real)0;
+    invJ = valid ? P.invdetJ[n] : (real)0;
+  } else {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sd[d] = P.sdiag[3 * ec + d];
+  }
+  const real Hend = (real)P.H[0];
+  if (CURV) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) sw[le][c][t] = m[c] * u;
+  }
+  __syncthreads();
+  real du[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) du[d] = contract<N>(su[le], GT, i, j, k, d);
+  real g[3];
+  if (CURV) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      real acc = 0;
+#pragma unroll
+      for (int al = 0; al < 3; ++al)
+        acc += (real)0.5 * contract<N>(sw[le][al * 3 + c], GT, i, j, k, al) + (real)0.5 * m[al * 3 + c] * du[al];
+      g[c] = acc;
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) g[d] = sd[d] * du[d];
+  }
+  // centred-flux SAT on interior faces through this node
+  if (valid) {
+    const int idx3[3] = {i, j, k};
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const int ax = f >> 1;
+      if (idx3[ax] != frow(f, N)) continue;
+      if (P.bdry[f + 6 * ec] != 0 || P.nbr[f + 6 * ec] < 0) continue;
+      const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
+      const real jump = sun[le][f][p + N * q] - u;
+      const real nh = (f & 1) ? (real)1 : (real)-1;
+      if (CURV) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) g[c] += nh * m[ax * 3 + c] * jump / ((real)2 * Hend);
+      } else {
+        g[ax] += nh * sd[ax] / ((real)2 * Hend) * jump;
+      }
+    }
+  }
+  if (CURV) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g[c] *= invJ;
+  }
+  if (!valid) return;
+  if (P.grad_out) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) P.grad_out[c * nn + n] = g[c];
+  }
+  if (grad_only) return;
+  // flux and Phidot
+  const real F0 = b[0] * Pi + (K[0] * g[0] + K[1] * g[1] + K[2] * g[2]);
+  const real F1 = b[1] * Pi + (K[1] * g[0] + K[3] * g[1] + K[4] * g[2]);
+  const real F2 = b[2] * Pi + (K[2] * g[0] + K[4] * g[1] + K[5] * g[2]);
+  real phid = b[0] * g[0] + b[1] * g[1] + b[2] * g[2] + a * Pi;
+  // boundary increments (per boundary face of the node; Pi parts go to the face slot)
+  if (P.bc_on) {
+    const int idx3[3] = {i, j, k};
+    for (int f = 0; f < 6; ++f) {
+      const int tag = P.bdry[f + 6 * ec];
+      if (tag == 0) continue;
+      const int ax = f >> 1;
+      if (idx3[ax] != frow(f, N)) continue;
+      const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
+      const int slot = P.bslot[f + 6 * ec];
+      real dF = 0, dP = 0;
+      if (!P.bc_curv) {
+        const int kind = P.kinds[f];
+        if (kind != 3) {
+          const real nh = (f & 1) ? (real)1 : (real)-1;
+          const real Kdd = ax == 0 ? K[0] : ax == 1 ? K[3] : K[5];
+          const real a_n = sqrt(a * Kdd);
+          const real bax = b[ax];
+          const real bn = nh * bax;
+          const real wt = sd[ax] / Hend;
+          if (kind == 4) {
+            const real tau = P.sigma * (fabs(a_n - bax) + fabs(a_n + bax)) * wt;
+            const real gp = P.gPhi ? P.gPhi[n] : (real)0, gq = P.gPi ? P.gPi[n] : (real)0;
+            dF = -tau * (u - gp);
+            dP = -tau * (Pi - gq);
+          } else {
+            const real qv = nh * g[ax];
+            const real r = Pi + ((bn + a_n) / a) * qv;
+            const real gv = kind == 2 ? (real)0 : (P.gPhi ? P.gPhi[n] : (real)0);
+            dP = -P.sigma * fabs(a_n + bn) * wt * (r - gv);
+          }
+        }
+      } else if (tag != P.exc_tag) {
+        const int kind = P.kinds[0];
+        const long long nb = (long long)P.nbf * N2;
+        const long long bi = (long long)slot * N2 + p + N * q;
+        const real nx = P.bnorm[bi], ny = P.bnorm[nb + bi], nz = P.bnorm[2 * nb + bi], wt = P.bnorm[3 * nb + bi];
+        const real Kn = K[0] * nx * nx + K[3] * ny * ny + K[5] * nz * nz +
+                        (real)2 * (K[1] * nx * ny + K[2] * nx * nz + K[4] * ny * nz);
+        const real a_n = sqrt(a * Kn);
+        const real bn = b[0] * nx + b[1] * ny + b[2] * nz;
+        if (kind == 4) {
+          const real tau = P.sigma * (fabs(a_n - bn) + fabs(a_n + bn)) * wt;
+          const real gp = P.gPhi ? P.gPhi[n] : (real)0, gq = P.gPi ? P.gPi[n] : (real)0;
+          dF = -tau * (u - gp);
+          dP = -tau * (Pi - gq);
+        } else {
+          const real qv = nx * g[0] + ny * g[1] + nz * g[2];
+          const real r = Pi + ((bn + a_n) / a) * qv;
+          real gv = 0;
+          if (kind != 2) {
+            const real gq = P.gPi ? P.gPi[n] : (real)0;
+            const real gx = P.gDx ? P.gDx[n] : (real)0, gy = P.gDy ? P.gDy[n] : (real)0,
+                       gz = P.gDz ? P.gDz[n] : (real)0;
+            gv = gq + ((bn + a_n) / a) * (nx * gx + ny * gy + nz * gz);
+          }
+          dP = -P.sigma * fabs(a_n + bn) * wt * (r - gv);
+        }
+      }
+      phid += dF;
+      P.bbuf[(long long)slot * N2 + p + N * q] = dP;
+    }
+  }
+  P.F[n] = F0;
+  P.F[nn + n] = F1;
+  P.F[2 * nn + n] = F2;
+  if (P.epi)
+    rk_epilogue<real>(P.stage, P.dt, phid, u, P.y, P.acc, P.out, n, P.nonfinite);
+  else
+    P.Phidot[n] = phid;
+}
+
+template <typename real>
+struct K2P {
+  long long Ne, nn;
+  const real* F0;
+  const real* F1;
+  const real* F2;
+  const real* Ja;
+  const real* invdetJ;
+  const real* sdiag;
+  const int32_t* nbr;
+  const int32_t* nbrf;
+  const int32_t* bdry;
+  const int32_t* bslot;
+  const double* G;
+  const double* H;
+  const real* bbuf;
+  int bc_on;
+  real* Pidot;
+  int epi, stage;
+  double dt;
+  real* y;
+  real* acc;
+  real* out;
+  unsigned int* nonfinite;
+};
+
+template <int N, typename real, bool CURV>
+__global__ void __launch_bounds__(Ep<N>::T) k_cons_k2(const K2P<real> P) {
+  constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = Ep<N>::EPB;
+  __shared__ real GT[N2];
+  __shared__ real sF[EPB][3][N3];
+  __shared__ real sFn[EPB][6][CURV ? 3 : 1][N2];
+  __shared__ real sw[CURV ? EPB : 1][CURV ? 3 : 1][CURV ? N3 : 1];
+  const int tid = threadIdx.x;
+  const int le = tid / N3, t = tid - le * N3;
+  const int i = t % N, j = (t / N) % N, k = t / N2;
+  const long long e = (long long)blockIdx.x * EPB + le;
+  const bool valid = e < P.Ne;
+  const long long ec = valid ? e : 0;
+  const long long n = ec * N3 + t;
+  const long long nn = P.nn;
+  if (tid < N2) GT[(tid % N) * N + tid / N] = (real)P.G[tid];
+  const real* Fp[3] = {P.F0, P.F1, P.F2};
+  real Fv[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    Fv[c] = valid ? Fp[c][n] : (real)0;
+    sF[le][c][t] = Fv[c];
+  }
+  for (int idx = t; idx < 6 * N2; idx += N3) {
+    const int f = idx / N2, pq = idx - f * N2;
+    long long src = -1;
+    if (valid) {
+      const int en = P.nbr[f + 6 * ec];
+      if (en >= 0 && P.bdry[f + 6 * ec] == 0) {
+        const int fn = P.nbrf[f + 6 * ec];
+        src = (long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq % N, pq / N, N);
+      }
+    }
+    if (CURV) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sFn[le][f][c][pq] = src >= 0 ? Fp[c][src] : (real)0;
+    } else {
+      sFn[le][f][0][pq] = src >= 0 ? Fp[f >> 1][src] : (real)0;
+    }
+  }
+  real m[CURV ? 9 : 1];
+  real invJ = 0, sd[3];
+  if (CURV) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) m[c] = valid ? P.Ja[c * nn + n] : (real)0;
+    invJ = valid ? P.invdetJ[n] : (real)0;
+#pragma unroll
+    for (int al = 0; al < 3; ++al) sw[le][al][t] = m[al * 3] * Fv[0] + m[al * 3 + 1] * Fv[1] + m[al * 3 + 2] * Fv[2];
+  } else {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sd[d] = P.sdiag[3 * ec + d];
+  }
+  const real Hend = (real)P.H[0];
+  __syncthreads();
+  real dv = 0;
+  if (CURV) {
+#pragma unroll
+    for (int al = 0; al < 3; ++al) {
+      dv += (real)0.5 * contract<N>(sw[le][al], GT, i, j, k, al);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dv += (real)0.5 * m[al * 3 + c] * contract<N>(sF[le][c], GT, i, j, k, al);
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dv += sd[d] * contract<N>(sF[le][d], GT, i, j, k, d);
+  }
+  if (!valid) return;
+  const int idx3[3] = {i, j, k};
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const int ax = f >> 1;
+    if (idx3[ax] != frow(f, N)) continue;
+    if (P.bdry[f + 6 * ec] != 0 || P.nbr[f + 6 * ec] < 0) continue;
+    const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
+    const real nh = (f & 1) ? (real)1 : (real)-1;
+    if (CURV) {
+      real s = 0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s += m[ax * 3 + c] * (sFn[le][f][c][p + N * q] - Fv[c]);
+      dv += nh * s / ((real)2 * Hend);
+    } else {
+      dv += nh * sd[ax] / ((real)2 * Hend) * (sFn[le][f][0][p + N * q] - Fv[ax]);
+    }
+  }
+  if (CURV) dv *= invJ;
+  if (P.bc_on) {
+    for (int f = 0; f < 6; ++f) {
+      if (P.bdry[f + 6 * ec] == 0) continue;
+      const int ax = f >> 1;
+      if (idx3[ax] != frow(f, N)) continue;
+      const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
+      dv += P.bbuf[(long long)P.bslot[f + 6 * ec] * N2 + p + N * q];
+    }
+  }
+  if (P.epi) {
+    const real yin = P.stage == 0 ? P.y[n] : (real)0;
+    rk_epilogue<real>(P.stage, P.dt, dv, yin, P.y, P.acc, P.out, n, P.nonfinite);
+  } else {
+    P.Pidot[n] = dv;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// apply_D!(Du, u, d): s_{d,e} G_d u + centred-flux SAT on interior d-faces,
+// s_{d,e} = invjac[d,d] at the element's first node.
+template <int N, typename real>
+__global__ void __launch_bounds__(Ep<N>::T) k_apply_D(long long Ne, const real* __restrict__ u, real* __restrict__ out,
+                                                     int d, const real* __restrict__ sdiag,
+                                                     const int32_t* __restrict__ nbr, const int32_t* __restrict__ nbrf,
+                                                     const int32_t* __restrict__ bdry, const double* __restrict__ G,
+                                                     const double* __restrict__ H) {
+  constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = Ep<N>::EPB;
+  __shared__ real GT[N2];
+  __shared__ real su[EPB][N3];
+  const int tid = threadIdx.x;
+  const int le = tid / N3, t = tid - le * N3;
+  const int i = t % N, j = (t / N) % N, k = t / N2;
+  const long long e = (long long)blockIdx.x * EPB + le;
+  const bool valid = e < Ne;
+  const long long ec = valid ? e : 0;
+  const long long n = ec * N3 + t;
+  if (tid < N2) GT[(tid % N) * N + tid / N] = (real)G[tid];
+  const real uv = valid ? u[n] : (real)0;
+  su[le][t] = uv;
+  __syncthreads();
+  if (!valid) return;
+  const real s = sdiag[3 * ec + d];
+  real r = s * contract<N>(su[le], GT, i, j, k, d);
+  const int idx3[3] = {i, j, k};
+  for (int f = 2 * d; f < 2 * d + 2; ++f) {
+    if (idx3[d] != frow(f, N)) continue;
+    if (bdry[f + 6 * ec] != 0) continue;
+    const int en = nbr[f + 6 * ec];
+    if (en < 0) continue;
+    const int fn = nbrf[f + 6 * ec];
+    const int p = d == 0 ? j : i, q = d == 2 ? j : k;
+    const real un = u[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), p, q, N)];
+    const real nh = (f & 1) ? (real)1 : (real)-1;
+    r += nh * s / ((real)2 * (real)H[0]) * (un - uv);
+  }
+  out[n] = r;
+}
+
+// ---------------------------------------------------------------------------
+// Line-local Kreiss-Oliger: dst += koT * D_d^6 field.  D_d couples only nodes
+// on the same axis-d grid line (METHODS.md:151-155), so a CTA loads N pencils
+// of one whole element line (N * len * N values) into smem and applies D_d six
+// times there; one thread per (pencil, element segment) keeps its N values in
+// registers.  Arithmetic is that of six apply_D! calls.
+template <int N, typename real>
+__global__ void k_ko_line(int d, int len, int closed, const int32_t* __restrict__ lines, real* __restrict__ dst,
+                          const real* __restrict__ field, real koT, const real* __restrict__ sdiag,
+                          const double* __restrict__ G, const double* __restrict__ H) {
+  extern __shared__ unsigned char smraw[];
+  real* buf = reinterpret_cast<real*>(smraw);  // [N pencils][len*N]
+  __shared__ real Gs[N * N];
+  constexpr int N3 = N * N * N;
+  const int line = blockIdx.x;
+  const int g = blockIdx.y;       // pencil group (second tangential index)
+  const int tid = threadIdx.x;
+  const int pb = tid % N;         // pencil within group (fastest tangential index)
+  const int sg = tid / N;         // element segment along the line
+  for (int idx = tid; idx < N * N; idx += blockDim.x) Gs[idx] = (real)G[idx];
+  const bool act = sg < len;
+  const int e = act ? lines[(long long)line * len + sg] : 0;
+  // node index of position l along axis d for this pencil
+  auto node = [&](int l) -> long long {
+    int ii, jj, kk;
+    if (d == 0) { ii = l; jj = pb; kk = g; }
+    else if (d == 1) { ii = pb; jj = l; kk = g; }
+    else { ii = pb; jj = g; kk = l; }
+    return (long long)e * N3 + ii + N * (jj + N * kk);
+  };
+  real v[N];
+  if (act) {
+#pragma unroll
+    for (int l = 0; l < N; ++l) v[l] = field[node(l)];
+  }
+  const real s = act ? sdiag[3 * e + d] : (real)0;
+  const real Hend = (real)H[0];
+  const bool has_prev = closed || sg > 0;
+  const bool has_next = closed || sg < len - 1;
+  const int sp = sg == 0 ? len - 1 : sg - 1;
+  const int sn = sg == len - 1 ? 0 : sg + 1;
+  for (int it = 0; it < 6; ++it) {
+    if (act) {
+#pragma unroll
+      for (int l = 0; l < N; ++l) buf[pb * len * N + sg * N + l] = v[l];
+    }
+    __syncthreads();
+    if (act) {
+      real w[N];
+#pragma unroll
+      for (int l = 0; l < N; ++l) {
+        real acc = 0;
+#pragma unroll
+        for (int p = 0; p < N; ++p) acc += Gs[l * N + p] * v[p];
+        w[l] = s * acc;
+      }
+      if (has_prev) w[0] += -s / ((real)2 * Hend) * (buf[pb * len * N + sp * N + (N - 1)] - v[0]);
+      if (has_next) w[N - 1] += s / ((real)2 * Hend) * (buf[pb * len * N + sn * N + 0] - v[N - 1]);
+#pragma unroll
+      for (int l = 0; l < N; ++l) v[l] = w[l];
+    }
+    __syncthreads();
+  }
+  if (act) {
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      long long nd = node(l);
+      dst[nd] = dst[nd] + koT * v[l];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+template <int N, typename real>
+static int k1_dispatch(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
+                       void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
+                       cudaStream_t s) {
+  K1P<real> P;
+  P.Ne = m.Ne; P.nn = m.nn;
+  P.Phi = (const real*)Phi; P.Pi = (const real*)Pi;
+  P.c10 = (const real*)c.c10;
+  P.Ja = (const real*)m.Ja_r; P.invdetJ = (const real*)m.invdetJ_r; P.sdiag = (const real*)m.sdiag;
+  P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot;
+  P.G = m.G; P.H = m.H;
+  P.F = (real*)F; P.Phidot = (real*)Phidot; P.bbuf = (real*)bbuf; P.grad_out = (real*)grad_out;
+  P.bc_on = bc.on; P.bc_curv = bc.curv; P.exc_tag = bc.exc_tag; P.nbf = m.nbf;
+  for (int f = 0; f < 6; ++f) P.kinds[f] = bc.kinds[f];
+  P.sigma = (real)bc.sigma; P.bnorm = (const real*)m.bnorm;
+  P.gPhi = (const real*)bc.gPhi; P.gPi = (const real*)bc.gPi;
+  P.gDx = (const real*)bc.gDx; P.gDy = (const real*)bc.gDy; P.gDz = (const real*)bc.gDz;
+  P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
+  P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.nonfinite = rk.nonfinite;
+  const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
+  if (use_metric)
+    k_cons_k1<N, real, true><<<blocks, Ep<N>::T, 0, s>>>(P);
+  else
+    k_cons_k1<N, real, false><<<blocks, Ep<N>::T, 0, s>>>(P);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <int N, typename real>
+static int k2_dispatch(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
+                       const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s,
+                       const void* F1 = nullptr, const void* F2 = nullptr) {
+  K2P<real> P;
+  P.Ne = m.Ne; P.nn = m.nn;
+  P.F0 = (const real*)F;
+  P.F1 = F1 ? (const real*)F1 : (const real*)F + m.nn;
+  P.F2 = F2 ? (const real*)F2 : (const real*)F + 2 * m.nn;
+  P.Ja = (const real*)m.Ja_r; P.invdetJ = (const real*)m.invdetJ_r; P.sdiag = (const real*)m.sdiag;
+  P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot;
+  P.G = m.G; P.H = m.H;
+  P.bbuf = (const real*)bbuf; P.bc_on = bc.on;
+  P.Pidot = (real*)Pidot;
+  P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
+  P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.nonfinite = nonfinite;
+  const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
+  if (use_metric)
+    k_cons_k2<N, real, true><<<blocks, Ep<N>::T, 0, s>>>(P);
+  else
+    k_cons_k2<N, real, false><<<blocks, Ep<N>::T, 0, s>>>(P);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+#define WT_DISPATCH_N(N_, CALL)   \
+  switch (N_) {                   \
+    case 2: { constexpr int NN = 2; return CALL; } \
+    case 3: { constexpr int NN = 3; return CALL; } \
+    case 4: { constexpr int NN = 4; return CALL; } \
+    case 5: { constexpr int NN = 5; return CALL; } \
+    case 6: { constexpr int NN = 6; return CALL; } \
+    case 7: { constexpr int NN = 7; return CALL; } \
+    case 8: { constexpr int NN = 8; return CALL; } \
+    default: return -4;           \
+  }
+
+int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
+                   void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
+                   cudaStream_t s) {
+  if (m.precision == 0) {
+    WT_DISPATCH_N(m.N, (k1_dispatch<NN, double>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, use_metric, bc, rk, s)));
+  } else {
+    WT_DISPATCH_N(m.N, (k1_dispatch<NN, float>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, use_metric, bc, rk, s)));
+  }
+}
+
+int launch_cons_k2(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
+                   const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s) {
+  if (m.precision == 0) {
+    WT_DISPATCH_N(m.N, (k2_dispatch<NN, double>(m, F, Pidot, bbuf, use_metric, bc, rk, nonfinite, s)));
+  } else {
+    WT_DISPATCH_N(m.N, (k2_dispatch<NN, float>(m, F, Pidot, bbuf, use_metric, bc, rk, nonfinite, s)));
+  }
+}
+
+int launch_div3d(const DevMesh& m, const void* F, void* out, cudaStream_t s) {
+  // F: 3 consecutive fields
+  ConsBC bc;
+  RKStage rk;
+  if (m.precision == 0) {
+    WT_DISPATCH_N(m.N, (k2_dispatch<NN, double>(m, F, out, nullptr, 1, bc, rk, nullptr, s)));
+  } else {
+    WT_DISPATCH_N(m.N, (k2_dispatch<NN, float>(m, F, out, nullptr, 1, bc, rk, nullptr, s)));
+  }
+}
+
+template <int N, typename real>
+static int applyD_dispatch(const DevMesh& m, const void* u, void* out, int d, cudaStream_t s) {
+  const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
+  k_apply_D<N, real><<<blocks, Ep<N>::T, 0, s>>>(m.Ne, (const real*)u, (real*)out, d, (const real*)m.sdiag, m.nbr,
+                                                 m.nbrf, m.bdry, m.G, m.H);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int launch_apply_D(const DevMesh& m, const void* u, void* out, int d, cudaStream_t s) {
+  if (m.precision == 0) {
+    WT_DISPATCH_N(m.N, (applyD_dispatch<NN, double>(m, u, out, d, s)));
+  } else {
+    WT_DISPATCH_N(m.N, (applyD_dispatch<NN, float>(m, u, out, d, s)));
+  }
+}
+
+template <int N, typename real>
+static int ko_dispatch(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s) {
+  for (int d = 0; d < 3; ++d) {
+    const int len = m.line_len[d];
+    if (!m.line_ok[d] || len * N > 1024) return -4;
+    dim3 grid((unsigned)m.nlines[d], N);
+    size_t smem = (size_t)N * len * N * sizeof(real);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_ko_line<N, real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_ko_line<N, real><<<grid, len * N, smem, s>>>(d, len, m.line_closed[d], m.lines[d], (real*)dst,
+                                                   (const real*)field, (real)koT, (const real*)m.sdiag, m.G, m.H);
+    if (cudaGetLastError() != cudaSuccess) return -2;
+  }
+  return 0;
+}
+
+int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s) {
+  if (m.precision == 0) {
+    WT_DISPATCH_N(m.N, (ko_dispatch<NN, double>(m, dst, field, koT, s)));
+  } else {
+    WT_DISPATCH_N(m.N, (ko_dispatch<NN, float>(m, dst, field, koT, s)));
+  }
+}
+
+}  // namespace wt

@@ -1,0 +1,557 @@
+"""Python host mirror of WaveToySecondOrder.jl's 3D API over the C ABI.
+
+Each function below keeps the name, argument meaning and error behaviour of
+the Julia function it stands in for (cited per function), with torch CUDA
+tensors in place of CuArrays.  All numerics run in libwavetoy_b200.so; there is
+no CPU path: without the built library or without a GPU every call raises.
+
+Array conventions: a field is a flat tensor of N^3*Ne values in the reference's
+(N,N,N,Ne) column-major order (i fastest), dtype float64 (plain form) or
+float32 (FP32 form), on the context's device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libwavetoy_b200.so")
+
+WT_F64, WT_F32 = 0, 1
+BC_DIRICHLET, BC_SOMMERFELD, BC_EXCISION, BC_FULL_DIRICHLET = 1, 2, 3, 4
+FACE_SUBLUMINAL, FACE_OUTFLOW, FACE_INFLOW, FACE_SONIC = 1, 2, 3, 4
+SOMMERFELD_BDRY_TAG = 7
+EXCISION_BDRY_TAG = 8
+BG_MINKOWSKI, BG_CONSTANT_SHIFT, BG_ADM_PERTURBED, BG_RADIAL_SHIFT = 0, 1, 2, 3
+
+_ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENOTSUP", -5: "ENONFINITE", -6: "ETIMEOUT"}
+
+_BC_FROM_SYMBOL = {"dirichlet": BC_DIRICHLET, "sommerfeld": BC_SOMMERFELD, "excision": BC_EXCISION,
+                   "full_dirichlet": BC_FULL_DIRICHLET}
+
+
+class WaveToyError(RuntimeError):
+    """Raised when the library returns an error status (ErrorException in the reference)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _MeshDesc(C.Structure):
+    _fields_ = [("N", C.c_int), ("M", C.c_int * 3), ("x0", C.c_double), ("x1", C.c_double),
+                ("warp_A", C.c_double), ("periodic", C.c_int), ("outer_tag", C.c_int), ("precision", C.c_int)]
+
+
+class _BgDesc(C.Structure):
+    _fields_ = [("kind", C.c_int), ("p", C.c_double * 16)]
+
+
+class _BcDesc(C.Structure):
+    _fields_ = [("kinds", C.c_int * 6), ("sigma", C.c_double), ("excision_tag", C.c_int),
+                ("gPhi", C.c_void_p), ("gPi", C.c_void_p), ("gDx", C.c_void_p), ("gDy", C.c_void_p),
+                ("gDz", C.c_void_p)]
+
+
+_lib = None
+
+
+def library():
+    """Load libwavetoy_b200.so (fails loudly when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with "
+                          "`python wavetoysecondorder.jl_b200/build.py` (nvcc, sm_100a)")
+    L = C.CDLL(LIB_PATH)
+    vp, pvp, i, d, ll = C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_double, C.c_longlong
+    sig = {
+        "wt_ctx_create": [i, pvp], "wt_ctx_destroy": [vp], "wt_ctx_synchronize": [vp],
+        "wt_ctx_get_stream": [vp, pvp], "wt_ctx_set_stream": [vp, vp],
+        "wt_ctx_launch_count": [vp, C.POINTER(ll)], "wt_ctx_nonfinite": [vp, C.POINTER(i)],
+        "wt_mesh_create": [vp, C.POINTER(_MeshDesc), pvp],
+        "wt_mesh_create_arrays": [vp, i, ll, vp, vp, vp, vp, vp, vp, i, pvp],
+        "wt_mesh_destroy": [vp], "wt_mesh_info": [vp, C.POINTER(i), C.POINTER(ll), C.POINTER(i)],
+        "wt_mesh_get": [vp, C.c_char_p, vp], "wt_mesh_set_bdry": [vp, vp],
+        "wt_mesh_min_spacing": [vp, C.POINTER(d)],
+        "wt_background_set": [vp, vp, C.POINTER(_BgDesc), pvp], "wt_background_set_arrays": [vp, vp, vp, pvp],
+        "wt_coef_get": [vp, vp], "wt_coef_destroy": [vp],
+        "wt_workspace_create": [vp, vp, pvp], "wt_workspace_destroy": [vp], "wt_workspace_mu": [vp, C.POINTER(d)],
+        "wt_rhs_curved": [vp, vp, vp, vp, vp, vp, vp, d, C.POINTER(_BcDesc), i],
+        "wt_apply_D": [vp, vp, vp, vp, i], "wt_ko_add": [vp, vp, vp, vp, d],
+        "wt_gradient3d": [vp, vp, vp, vp, vp, vp], "wt_divergence3d": [vp, vp, vp, vp, vp, vp],
+        "wt_rhs_sipg": [vp, vp, vp, vp, vp, C.POINTER(C.c_double * 6), d, d],
+        "wt_rhs_strong": [vp, vp, vp, vp, vp, d, d], "wt_lap_strong_cons": [vp, vp, vp, vp, d, d],
+        "wt_energy": [vp, vp, vp, vp, vp, i, C.POINTER(d)], "wt_energy_sipg": [vp, vp, vp, vp, d, C.POINTER(d)],
+        "wt_l2_diff": [vp, vp, vp, vp, i, C.POINTER(d)],
+        "wt_step_rk4_curved": [vp, vp, vp, vp, vp, d, i, d, C.POINTER(_BcDesc), i],
+        "wt_step_rk4_sipg": [vp, vp, vp, vp, d, i, C.POINTER(C.c_double * 6), d, d, d],
+        "wt_evolve_curved_host": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i, vp],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.wt_last_error.argtypes = [vp]
+    L.wt_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+class Context:
+    """One CUDA stream (the KernelAbstractions backend queue of the reference)."""
+
+    def __init__(self, device: int = 0, use_torch_stream: bool = True):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise RuntimeError("wavetoy_b200 needs a CUDA device; there is no CPU fallback")
+        self.device = device
+        self.h = C.c_void_p()
+        rc = library().wt_ctx_create(device, C.byref(self.h))
+        if rc != 0:
+            raise WaveToyError(rc, f"wt_ctx_create(device={device}) failed")
+        if use_torch_stream:
+            with torch.cuda.device(device):
+                s = torch.cuda.current_stream(device).cuda_stream
+            library().wt_ctx_set_stream(self.h, C.c_void_p(s))
+
+    def check(self, rc: int, what: str = ""):
+        if rc != 0:
+            msg = library().wt_last_error(self.h)
+            raise WaveToyError(rc, (msg.decode() if msg else "") + (f" [{what}]" if what else ""))
+
+    def synchronize(self):
+        self.check(library().wt_ctx_synchronize(self.h))
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        self.check(library().wt_ctx_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def nonfinite(self) -> bool:
+        f = C.c_int()
+        self.check(library().wt_ctx_nonfinite(self.h, C.byref(f)))
+        return bool(f.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().wt_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mesh:
+    """Mesh + MeshGeometry (+ metric terms) on the device.
+
+    Stands in for HexMeshes.make_uniform_hex / make_warped_uniform_hex followed
+    by HexSBPSAT.make_element, make_operators, make_geometry, to_device and
+    make_metric_terms3d (src/evolve.jl:1174-1196)."""
+
+    def __init__(self, ctx: Context, h, N: int, Ne: int, precision: int):
+        self.ctx, self.h, self.N, self.Ne, self.precision = ctx, h, N, Ne, precision
+        self.nn = N ** 3 * Ne
+        self.dtype = _torch().float64 if precision == WT_F64 else _torch().float32
+
+    @classmethod
+    def uniform_hex(cls, ctx: Context, N: int, M, x0: float = 0.0, x1: float = 1.0, *, periodic: bool = False,
+                    outer_tag: int = 0, warp_A: float = 0.0, precision: int = WT_F64) -> "Mesh":
+        if isinstance(M, int):
+            M = (M, M, M)
+        d = _MeshDesc()
+        d.N = N
+        for a in range(3):
+            d.M[a] = int(M[a])
+        d.x0, d.x1, d.warp_A = float(x0), float(x1), float(warp_A)
+        d.periodic, d.outer_tag, d.precision = int(periodic), int(outer_tag), int(precision)
+        h = C.c_void_p()
+        ctx.check(library().wt_mesh_create(ctx.h, C.byref(d), C.byref(h)), "wt_mesh_create")
+        m = cls(ctx, h, N, M[0] * M[1] * M[2], precision)
+        m.M, m.x0, m.x1, m.warp_A, m.periodic = tuple(M), x0, x1, warp_A, periodic
+        return m
+
+    @classmethod
+    def warped_uniform_hex(cls, ctx: Context, N: int, M, x0: float = 0.0, x1: float = 1.0, A: float = 0.05, *,
+                           periodic: bool = False, outer_tag: int = 0, precision: int = WT_F64) -> "Mesh":
+        return cls.uniform_hex(ctx, N, M, x0, x1, periodic=periodic, outer_tag=outer_tag, warp_A=A,
+                               precision=precision)
+
+    @classmethod
+    def from_arrays(cls, ctx: Context, N: int, coords, jac, neighbour, neighbour_face, orientation, bdry,
+                    precision: int = WT_F64) -> "Mesh":
+        """MeshGeometry arrays (host numpy, Julia layout, 1-based connectivity) -> device mesh."""
+        import numpy as np
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        jac = np.ascontiguousarray(jac, dtype=np.float64)
+        nb = np.ascontiguousarray(neighbour, dtype=np.int32)
+        nf = np.ascontiguousarray(neighbour_face, dtype=np.int32)
+        ori = np.ascontiguousarray(orientation, dtype=np.int8)
+        bd = np.ascontiguousarray(bdry, dtype=np.int8)
+        Ne = nb.size // 6
+        h = C.c_void_p()
+        ctx.check(library().wt_mesh_create_arrays(ctx.h, N, Ne, coords.ctypes.data, jac.ctypes.data,
+                                                  nb.ctypes.data, nf.ctypes.data, ori.ctypes.data, bd.ctypes.data,
+                                                  precision, C.byref(h)), "wt_mesh_create_arrays")
+        return cls(ctx, h, N, Ne, precision)
+
+    def get(self, name: str):
+        import numpy as np
+        n = self.nn
+        sizes = {"coords": 3 * n, "jac": 9 * n, "invjac": 9 * n, "detjac": n, "Hphys": n, "Hd": n, "invdetJ": n,
+                 "Ja": 9 * n, "x": self.N, "H": self.N, "G": self.N * self.N}
+        isizes = {"bdry": 6 * self.Ne, "neighbour": 6 * self.Ne, "handedness": self.Ne}
+        out = np.zeros(sizes[name]) if name in sizes else np.zeros(isizes[name], dtype=np.int32)
+        self.ctx.check(library().wt_mesh_get(self.h, name.encode(), out.ctypes.data), f"wt_mesh_get({name})")
+        return out
+
+    def set_bdry(self, bdry):
+        import numpy as np
+        b = np.ascontiguousarray(bdry, dtype=np.int32)
+        self.ctx.check(library().wt_mesh_set_bdry(self.h, b.ctypes.data), "wt_mesh_set_bdry")
+
+    def min_spacing(self) -> float:
+        """_min_node_spacing_3d (src/evolve.jl:60-69)."""
+        h = C.c_double()
+        self.ctx.check(library().wt_mesh_min_spacing(self.h, C.byref(h)), "min_spacing")
+        return h.value
+
+    def empty(self, *shape):
+        torch = _torch()
+        return torch.empty(*(shape or (self.nn,)), dtype=self.dtype, device=f"cuda:{self.ctx.device}")
+
+    def zeros(self):
+        torch = _torch()
+        return torch.zeros(self.nn, dtype=self.dtype, device=f"cuda:{self.ctx.device}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().wt_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Coef:
+    """The coefficient bundle of make_coef3d / sample_background3d! (src/wave3d_curved.jl:106-124)."""
+
+    def __init__(self, mesh: Mesh, h):
+        self.mesh, self.h = mesh, h
+
+    def get(self):
+        """11 fields (alpha, sqrtg, b1, b2, b3, gu11, gu12, gu13, gu22, gu23, gu33), FP64 host."""
+        import numpy as np
+        out = np.zeros(11 * self.mesh.nn)
+        self.mesh.ctx.check(library().wt_coef_get(self.h, out.ctypes.data), "wt_coef_get")
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().wt_coef_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def sample_background3d(mesh: Mesh, kind: int = BG_MINKOWSKI, params: Optional[Sequence[float]] = None) -> Coef:
+    """make_coef3d + sample_background3d! for an analytic background (src/wave3d_curved.jl:106-124)."""
+    d = _BgDesc()
+    d.kind = int(kind)
+    for k, v in enumerate(params or ()):
+        d.p[k] = float(v)
+    h = C.c_void_p()
+    mesh.ctx.check(library().wt_background_set(mesh.ctx.h, mesh.h, C.byref(d), C.byref(h)), "wt_background_set")
+    return Coef(mesh, h)
+
+
+def background_from_arrays(mesh: Mesh, coef11) -> Coef:
+    """Host-sampled 11-field bundle (the layout sample_background3d! fills)."""
+    import numpy as np
+    c = np.ascontiguousarray(coef11, dtype=np.float64)
+    if c.size != 11 * mesh.nn:
+        raise ValueError("coef11 must hold 11 fields of N^3*Ne values")
+    h = C.c_void_p()
+    mesh.ctx.check(library().wt_background_set_arrays(mesh.ctx.h, mesh.h, c.ctypes.data, C.byref(h)),
+                   "wt_background_set_arrays")
+    return Coef(mesh, h)
+
+
+class Workspace:
+    """Wave3DWorkspace: scratch + mu (src/wave3d_curved.jl:137-178)."""
+
+    def __init__(self, mesh: Mesh):
+        self.mesh, self.ctx = mesh, mesh.ctx
+        self.h = C.c_void_p()
+        self.ctx.check(library().wt_workspace_create(self.ctx.h, mesh.h, C.byref(self.h)), "wt_workspace_create")
+        mu = C.c_double()
+        library().wt_workspace_mu(self.h, C.byref(mu))
+        self.mu = mu.value
+        self.inv_mu5 = (1.0 / self.mu) ** 5 if self.mu > 0 else 0.0
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().wt_workspace_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_wave3d_workspace(mesh: Mesh) -> Workspace:
+    """make_wave3d_workspace(geom, ops) (src/wave3d_curved.jl:158-178)."""
+    return Workspace(mesh)
+
+
+@dataclass
+class BC3D:
+    """make_bc3d bundle (src/boundaries3d.jl:45-52)."""
+    kinds: tuple
+    sigma: float = 1.0
+    gPhi: object = None
+    gPi: object = None
+    gDx: object = None
+    gDy: object = None
+    gDz: object = None
+    excision_tag: int = 0
+    _c: object = field(default=None, repr=False)
+
+    def cstruct(self) -> _BcDesc:
+        b = _BcDesc()
+        for f in range(6):
+            b.kinds[f] = int(self.kinds[f])
+        b.sigma = float(self.sigma)
+        b.excision_tag = int(self.excision_tag)
+        for nm in ("gPhi", "gPi", "gDx", "gDy", "gDz"):
+            t = getattr(self, nm)
+            setattr(b, nm, t.data_ptr() if t is not None else None)
+        return b
+
+
+def bc1d_kind(s) -> int:
+    """bc1d_kind (src/boundaries1d.jl:73-77): Symbol -> BC_* code, ArgumentError otherwise."""
+    if isinstance(s, int):
+        return s
+    key = str(s).lstrip(":")
+    if key not in _BC_FROM_SYMBOL:
+        raise ValueError(f"unknown 1D boundary condition {s} (expected :dirichlet, :sommerfeld, :excision, "
+                         f":full_dirichlet)")
+    return _BC_FROM_SYMBOL[key]
+
+
+def make_bc3d(kinds, sigma: float = 1.0, gPhi=None, gPi=None, gDx=None, gDy=None, gDz=None,
+              excision_tag: int = 0) -> BC3D:
+    """make_bc3d(kinds; σ, gΦ, gΠ, gDx, gDy, gDz, excision_tag) (src/boundaries3d.jl:45-52)."""
+    if len(kinds) != 6:
+        raise ValueError("kinds must give one condition per face (-x,+x,-y,+y,-z,+z)")
+    return BC3D(tuple(bc1d_kind(k) for k in kinds), sigma, gPhi, gPi, gDx, gDy, gDz, excision_tag)
+
+
+def classify_face1d(a: float, beta: float, nhat: int, sonic_tol: Optional[float] = None) -> int:
+    """classify_face1d (src/boundaries1d.jl:98-109)."""
+    if sonic_tol is None:
+        sonic_tol = 2.0 ** -13  # eps(Float64)^(1/4)
+    s_R = a - beta
+    s_L = -a - beta
+    tol = sonic_tol * a
+    if abs(s_R) <= tol or abs(s_L) <= tol:
+        return FACE_SONIC
+    out_R = s_R * nhat > 0
+    out_L = s_L * nhat > 0
+    if out_R and out_L:
+        return FACE_OUTFLOW
+    if not out_R and not out_L:
+        return FACE_INFLOW
+    return FACE_SUBLUMINAL
+
+
+def classify_face3d(alpha, b1, b2, b3, gu11, gu22, gu33, naxis: int, nsign: int, sonic_tol=None) -> int:
+    """classify_face3d (src/boundaries3d.jl:25-32); naxis is 1-based like the reference."""
+    gunn = gu11 if naxis == 1 else gu22 if naxis == 2 else gu33
+    bax = b1 if naxis == 1 else b2 if naxis == 2 else b3
+    return classify_face1d(alpha * math.sqrt(gunn), bax, nsign, sonic_tol)
+
+
+def validate_bc1d(cls: int, kind: int, face: str):
+    """validate_bc1d (src/boundaries1d.jl:120-138): ArgumentError -> ValueError."""
+    names = {FACE_SUBLUMINAL: "subluminal", FACE_OUTFLOW: "superluminal outflow",
+             FACE_INFLOW: "superluminal inflow", FACE_SONIC: "sonic"}
+    if cls == FACE_SONIC:
+        raise ValueError(f"{face} boundary face is at a sonic point (|β| ≈ α/√γ): a characteristic speed "
+                         "vanishes there and no boundary condition is well-posed")
+    ok = ((cls == FACE_SUBLUMINAL and kind in (BC_DIRICHLET, BC_SOMMERFELD)) or
+          (cls == FACE_OUTFLOW and kind == BC_EXCISION) or (cls == FACE_INFLOW and kind == BC_FULL_DIRICHLET))
+    if not ok:
+        raise ValueError(f"{face} boundary face is {names[cls]}; the boundary condition is not admissible")
+
+
+def _bcptr(bc: Optional[BC3D]):
+    if bc is None:
+        return None, None
+    s = bc.cstruct()
+    return C.byref(s), s
+
+
+def wave3d_curved_rhs(Phidot, Pidot, Phi, Pi, coef: Coef, ws: Workspace, eps_KO: float = 0.1,
+                      bc3d: Optional[BC3D] = None, metric: bool = False):
+    """wave3d_curved_rhs!(Φ̇, Π̇, Φ, Π, coef; geom, ops, ws, ε_KO, bc3d, metric) (src/wave3d_curved.jl:205-258).
+
+    metric=True selects the curvilinear split-form path (the reference passes
+    the metric-term bundle); False the affine per-axis path."""
+    p, keep = _bcptr(bc3d)
+    ws.ctx.check(library().wt_rhs_curved(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), _ptr(Phidot), _ptr(Pidot),
+                                         float(eps_KO), p, int(metric)), "wave3d_curved_rhs!")
+    return Phidot, Pidot
+
+
+def apply_D(Du, u, d: int, ws: Workspace):
+    """HexSBPSAT.apply_D!(Du, u, d) (1-based axis d)."""
+    ws.ctx.check(library().wt_apply_D(ws.ctx.h, ws.h, _ptr(u), _ptr(Du), int(d)), "apply_D!")
+    return Du
+
+
+def ko_add(dst, field_, eps_KO: float, ws: Workspace):
+    """dst += ε μ⁻⁵ Σ_d D_d⁶ field (three _ko_axis3! calls, src/wave3d_curved.jl:182-192)."""
+    ws.ctx.check(library().wt_ko_add(ws.ctx.h, ws.h, _ptr(dst), _ptr(field_), float(eps_KO)), "ko")
+    return dst
+
+
+def apply_gradient3d(g1, g2, g3, u, ws: Workspace):
+    """apply_gradient3d!(DΦ1, DΦ2, DΦ3, Φ; geom, ops, metric) (src/wave3d_curved.jl:223)."""
+    ws.ctx.check(library().wt_gradient3d(ws.ctx.h, ws.h, _ptr(u), _ptr(g1), _ptr(g2), _ptr(g3)), "gradient3d")
+    return g1, g2, g3
+
+
+def apply_divergence3d(out, F1, F2, F3, ws: Workspace):
+    """apply_divergence3d!(Π̇, F1, F2, F3; geom, ops, metric) (src/wave3d_curved.jl:237)."""
+    ws.ctx.check(library().wt_divergence3d(ws.ctx.h, ws.h, _ptr(F1), _ptr(F2), _ptr(F3), _ptr(out)),
+                 "divergence3d")
+    return out
+
+
+def wave3d_energy(Phi, Pi, coef: Coef, ws: Workspace, metric: bool = False) -> float:
+    """wave3d_energy(Φ, Π, coef; geom, ops, ws, metric) (src/wave3d_curved.jl:268-287)."""
+    E = C.c_double()
+    ws.ctx.check(library().wt_energy(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), int(metric), C.byref(E)),
+                 "wave3d_energy")
+    return E.value
+
+
+def _bv(bdry_values):
+    arr = (C.c_double * 6)()
+    for f in range(6):
+        arr[f] = float(bdry_values[f])
+    return arr
+
+
+def rhs_wave3d(utt, u, ut, bdry_values, ws: Workspace, tau: float, sommerfeld_R: float = math.inf):
+    """rhs_wave3d!(ü, u, u̇, bdry_values; geom, ops, work, τ, sommerfeld_R) (src/wave.jl:583-611)."""
+    ws.ctx.check(library().wt_rhs_sipg(ws.ctx.h, ws.h, _ptr(u), _ptr(ut), _ptr(utt), C.byref(_bv(bdry_values)),
+                                       float(tau), float(sommerfeld_R)), "rhs_wave3d!")
+    return utt
+
+
+def wave_strong_rhs_mesh(utt, u, ut, ws: Workspace, tau: Optional[float] = None, sommerfeld_R: float = math.inf):
+    """wave_strong_rhs_mesh!(ü, u, u̇, mesh, geom, ops; τ = (N-1)², sommerfeld_R) (src/wave_strong_rhs.jl:296-360)."""
+    if tau is None:
+        tau = float((ws.mesh.N - 1) ** 2)
+    ws.ctx.check(library().wt_rhs_strong(ws.ctx.h, ws.h, _ptr(u), _ptr(ut), _ptr(utt), float(tau),
+                                         float(sommerfeld_R)), "wave_strong_rhs_mesh!")
+    return utt
+
+
+def wave_lap_strong_conservative_mesh(Lu, u, h: float, ws: Workspace, tau: Optional[float] = None):
+    """wave_lap_strong_conservative_mesh!(Lu, u, mesh, ops, h; τ = (N-1)²) (src/wave_lap_strong.jl:280-308)."""
+    if tau is None:
+        tau = float((ws.mesh.N - 1) ** 2)
+    ws.ctx.check(library().wt_lap_strong_cons(ws.ctx.h, ws.h, _ptr(u), _ptr(Lu), float(h), float(tau)),
+                 "wave_lap_strong_conservative_mesh!")
+    return Lu
+
+
+def energy_sipg(u, ut, ws: Workspace, tau: float) -> float:
+    """½⟨u̇,u̇⟩_H − ½⟨u, L u⟩_H (test/kernels3d_tests.jl:39-47)."""
+    E = C.c_double()
+    ws.ctx.check(library().wt_energy_sipg(ws.ctx.h, ws.h, _ptr(u), _ptr(ut), float(tau), C.byref(E)), "energy")
+    return E.value
+
+
+def l2_diff(a, b, ws: Workspace, metric: bool = False) -> float:
+    """sqrt(Σ (a−b)² H) (src/evolve.jl:1353-1354)."""
+    out = C.c_double()
+    ws.ctx.check(library().wt_l2_diff(ws.ctx.h, ws.h, _ptr(a), _ptr(b), int(metric), C.byref(out)), "l2")
+    return out.value
+
+
+def step_rk4_curved(Phi, Pi, coef: Coef, ws: Workspace, dt: float, nsteps: int, eps_KO: float = 0.0,
+                    bc3d: Optional[BC3D] = None, metric: bool = False):
+    """nsteps fixed-dt RK4 steps (OrdinaryDiffEq RK4(), adaptive=false; test/wave3d_tests.jl:32-44)."""
+    p, keep = _bcptr(bc3d)
+    ws.ctx.check(library().wt_step_rk4_curved(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt), int(nsteps),
+                                              float(eps_KO), p, int(metric)), "step_rk4_curved")
+    return Phi, Pi
+
+
+def step_rk4_sipg(u, ut, ws: Workspace, dt: float, nsteps: int, bdry_values=(0,) * 6, tau: float = 20.0,
+                  sommerfeld_R: float = math.inf, eps_KO: float = 0.0):
+    """RK4 of the SIPG system (u, u̇) with optional KO on both."""
+    ws.ctx.check(library().wt_step_rk4_sipg(ws.ctx.h, ws.h, _ptr(u), _ptr(ut), float(dt), int(nsteps),
+                                            C.byref(_bv(bdry_values)), float(tau), float(sommerfeld_R),
+                                            float(eps_KO)), "step_rk4_sipg")
+    return u, ut
+
+
+def evolve_curved_host(Phi_host, Pi_host, coef: Coef, ws: Workspace, dt: float, steps_per_sample: int,
+                       nsamples: int, eps_KO: float = 0.0, bc3d: Optional[BC3D] = None, metric: bool = False,
+                       energy=None):
+    """Host-buffer evolve in the shape of evolve3d(formulation = :conservative) (src/evolve.jl:1149-1366).
+
+    Phi_host / Pi_host: float64 numpy arrays (pinned torch CPU tensors also
+    work); they receive the final state.  energy: float64 array of length
+    nsamples or None."""
+    import numpy as np
+
+    def addr(a):
+        if a is None:
+            return None
+        if hasattr(a, "data_ptr"):
+            return C.c_void_p(a.data_ptr())
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+        return C.c_void_p(a.ctypes.data)
+
+    p, keep = _bcptr(bc3d)
+    ws.ctx.check(library().wt_evolve_curved_host(ws.ctx.h, ws.h, coef.h, addr(Phi_host), addr(Pi_host), float(dt),
+                                                 int(steps_per_sample), int(nsamples), float(eps_KO), p, int(metric),
+                                                 addr(energy)), "evolve_curved_host")
