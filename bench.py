@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark: DOF-updates/s of the RK4-stepped 3D SBP-SAT ADM wave solve on B200.
+
+Workload (default): warped cube (A = 0.05) with 64^3 elements and n = 8 GLL nodes
+per axis (134,217,728 nodes), perturbed ADM background, eight seeded Gaussian
+pulses, Sommerfeld outer faces, curvilinear split-form RHS, classic RK4 at CFL
+0.2, FP64 (the plain drop-in form).  One step = one RK4 step over the whole
+mesh; a DOF-update = one of (Phi, Pi) at one node advanced one step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--elements M] [--n 8] [--precision f64|f32]
+
+--impl reference times the CPU restatement of the path (the reference is Julia
+and cannot run here) on the host cores, one bounded sample per step.  For N > 1
+every rank runs its own independent solve (weak scaling, no collective on the
+data path); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "wavetoysecondorder.jl_b200")
+
+
+def package():
+    name = "wavetoy_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(key: str):
+    """DRAM bytes per node per launch of a kernel from the committed ncu summary
+    (profiles/*.md lines 'traffic_bytes_per_node <key> = <value>'), or None."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for fn in sorted(os.listdir(d)):
+        if not fn.endswith(".md"):
+            continue
+        for line in open(os.path.join(d, fn)):
+            line = line.strip().strip("`")
+            if line.startswith("traffic_bytes_per_node") and key in line and "=" in line:
+                try:
+                    return float(line.split("=")[1].split()[0])
+                except ValueError:
+                    pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit())
+        mx = max((float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[4 + k].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def workload_desc(args, nn):
+    return {"workload": f"warped-cube ADM solve, {args.elements}^3 elements, n={args.n} "
+                        f"({nn:,} nodes), Sommerfeld faces, curvilinear split form, RK4 CFL 0.2, "
+                        f"{args.precision.upper()}",
+            "elements_per_axis": args.elements, "n": args.n, "nodes": nn, "precision": args.precision,
+            "warp_A": 0.05, "eps_KO": 0.0, "seed": args.seed,
+            "l2": "inputs larger than L2 (each field %.2f GB > 126 MB)" % (nn * (8 if args.precision == "f64" else 4) / 1e9)}
+
+
+def cpu_sample(wt, O, args, seconds: float = 12.0, max_steps: int = 40):
+    """Time the CPU oracle on a bounded sample of the workload: the 16^3-element
+    cube of the same family (same n, background, pulses), RK4 steps until
+    `seconds` elapse.  Returns (DOF-updates/s, cores, description)."""
+    import numpy as np
+    M = min(16, args.elements)
+    m = O.OracleMesh(args.n, M, A=0.05, outer_tag=7)
+    p = wt.workloads.adm_params(args.seed)
+    coef = m.background(2, p)
+    x, y, z = m.coords()
+    c, a, w = wt.workloads.pulses(args.seed, 8, amp=(0.5, 1.0), width=(0.05, 0.15), centre=(0.25, 0.75))
+    Phi = wt.workloads.gaussian_field(x, y, z, c, a, w)
+    Pi = np.zeros_like(Phi)
+    dt = 0.2 * m.min_spacing() / wt.workloads.max_speed(p)
+    bc = O.make_bc([O.BC_SOMMERFELD] * 6)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        Phi, Pi = m.evolve_curved(coef, Phi, Pi, dt, 1, bc=bc, use_metric=True)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= max_steps:
+            break
+    return 2.0 * m.nn * steps / el, O.num_threads(), f"{M}^3 elements x {args.n}^3 nodes ({m.nn:,} nodes), " \
+                                                     f"{steps} RK4 steps in {el:.1f} s"
+
+
+def run_reference(args):
+    """CPU arm: the oracle restatement (the Julia reference cannot run here)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wt = package()
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    O.build()
+    import numpy as np
+    M = min(16, args.elements)
+    m = O.OracleMesh(args.n, M, A=0.05, outer_tag=7)
+    p = wt.workloads.adm_params(args.seed)
+    coef = m.background(2, p)
+    x, y, z = m.coords()
+    c, a, w = wt.workloads.pulses(args.seed, 8, amp=(0.5, 1.0), width=(0.05, 0.15), centre=(0.25, 0.75))
+    Phi = wt.workloads.gaussian_field(x, y, z, c, a, w)
+    Pi = np.zeros_like(Phi)
+    dt = 0.2 * m.min_spacing() / wt.workloads.max_speed(p)
+    bc = O.make_bc([O.BC_SOMMERFELD] * 6)
+    for _ in range(args.warmup):
+        Phi, Pi = m.evolve_curved(coef, Phi, Pi, dt, 1, bc=bc, use_metric=True)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        Phi, Pi = m.evolve_curved(coef, Phi, Pi, dt, 1, bc=bc, use_metric=True)
+    el = time.perf_counter() - t0
+    value = 2.0 * m.nn * args.steps / el
+    nn_full = args.n ** 3 * args.elements ** 3
+    sample = f"each step: one RK4 step of the {M}^3-element x {args.n}^3-node sample ({m.nn:,} nodes) " \
+             f"of the workload"
+    line = {"impl": "reference", "metric": "DOF-updates/s", "value": value, "unit": "DOF-updates/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ADM background, 8 Gaussian pulses)",
+            "config": workload_desc(args, nn_full),
+            "cpu_baseline": {"value": value, "unit": "DOF-updates/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference is Julia with unvendored dependencies (no toolchain here); its CPU path is "
+                    "timed through the C++ Float64 restatement of the same arithmetic, all host threads"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    wt = package()
+    ctx = wt.Context(local)
+    prec = wt.WT_F64 if args.precision == "f64" else wt.WT_F32
+    M, N = args.elements, args.n
+    mesh = wt.Mesh.warped_uniform_hex(ctx, N, M, 0.0, 1.0, 0.05, outer_tag=wt.SOMMERFELD_BDRY_TAG, precision=prec)
+    seed = args.seed + 7919 * rank
+    p = wt.workloads.adm_params(seed)
+    coef = wt.sample_background3d(mesh, wt.BG_ADM_PERTURBED, p)
+    ws = wt.make_wave3d_workspace(mesh)
+    nn = mesh.nn
+    Phi = mesh.zeros()
+    Pi = mesh.zeros()
+    c, a, w = wt.workloads.pulses(seed, 8, amp=(0.5, 1.0), width=(0.05, 0.15), centre=(0.25, 0.75))
+    wt.initial_data(mesh, wt.IC_GAUSSIANS, wt.gaussian_params(c, a, w), Phi)
+    dt = 0.2 * mesh.min_spacing() / wt.workloads.max_speed(p)
+    bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+
+    def step():
+        wt.step_rk4_curved(Phi, Pi, coef, ws, dt, 1, eps_KO=0.0, bc3d=bc, metric=True)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    n0 = ctx.launch_count()
+    ctx.profile(True)
+    stream = torch.cuda.current_stream()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ctx.profile(False)
+    (k1_ms, k1_n), (k2_ms, k2_n) = ctx.profile_read()
+    launches = ctx.launch_count() - n0
+    clocks = sampler.stop()
+    t_ms = ev0.elapsed_time(ev1)
+    t_tensor = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.barrier()
+        dist.all_reduce(t_tensor, op=dist.ReduceOp.MAX)
+    t_max = float(t_tensor.item()) / 1000.0
+    finite = not ctx.nonfinite()
+    value = 2.0 * nn * args.steps * world / t_max
+
+    # end to end through the host-buffer API: pinned host state in, one RK4 step
+    # per sample, state + energy back to the host after every step
+    Ph = torch.empty(nn, dtype=torch.float64, pin_memory=True)
+    Qh = torch.empty(nn, dtype=torch.float64, pin_memory=True)
+    e2e = None
+    if prec == wt.WT_F64:
+        Ph.copy_(Phi.cpu())
+        Qh.copy_(Pi.cpu())
+        E = np.zeros(args.steps)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        wt.evolve_curved_host(Ph, Qh, coef, ws, dt, 1, args.steps, bc3d=bc, metric=True, energy=E)
+        te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        te = float(te.item())
+        e2e = {"value": 2.0 * nn * args.steps * world / te, "unit": "DOF-updates/s",
+               "h2d_bytes_per_step": int(2 * nn * 8 / args.steps), "d2h_bytes_per_step": int(2 * nn * 8 + 8),
+               "api": "wt_evolve_curved_host (evolve3d shape: state and energy copied to host every step)"}
+
+    # roofline of the dominant kernel (K1: gradient + flux + Phi stage update)
+    hbm, src = peaks()
+    wbytes = 8 if prec == wt.WT_F64 else 4
+    k1_words = 1 + 1 + 20 + 3 + 3   # Phi, Pi, 20 coefficient words, F (3), Phi RK stage words (stage mean)
+    k1_avg_s = (k1_ms / max(k1_n, 1)) / 1000.0
+    k1_achieved = k1_words * wbytes * nn / k1_avg_s / 1e9 if k1_n else None
+    traffic_pn = profiled_traffic(f"k1_curv_{args.precision}")
+    k2_avg_s = (k2_ms / max(k2_n, 1)) / 1000.0
+    k2_words = 3 + 10 + 3
+    step_bytes = wbytes * (34 + 4 * 20) * nn
+    line = {
+        "metric": "DOF-updates/s", "value": value, "unit": "DOF-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
+        "data": "synthetic (seeded ADM background, 8 seeded Gaussian pulses; no dataset)",
+        "config": workload_desc(args, nn),
+        "roofline": {"bound": "hbm", "kernel": "k_cons_k1 (split-form gradient + flux + Phi RK4 stage)",
+                     "achieved": k1_achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (k1_achieved / hbm) if k1_achieved else None,
+                     "traffic": (traffic_pn * nn) if traffic_pn else None,
+                     "algorithmic_bytes_per_launch": k1_words * wbytes * nn,
+                     "avg_launch_ms": 1000.0 * k1_avg_s, "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)"},
+        "kernels": {"k_cons_k1": {"launches": k1_n, "ms": k1_ms},
+                    "k_cons_k2": {"launches": k2_n, "ms": k2_ms,
+                                  "achieved_GBps": k2_words * wbytes * nn / k2_avg_s / 1e9 if k2_n else None}},
+        "step_roofline": {"algorithmic_bytes_per_step": step_bytes,
+                          "achieved_GBps": step_bytes / (t_max / args.steps) / 1e9,
+                          "frac": step_bytes / (t_max / args.steps) / 1e9 / hbm,
+                          "definition": "w (34 + 4 C) bytes per node per RK4 step, C = 20 streamed coefficient words"},
+        "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "finite": finite,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, ROOT)
+        from oracle import oracle as O
+        O.build()
+        v, cores, sample = cpu_sample(wt, O, args)
+        line["cpu_baseline"] = {"value": v, "unit": "DOF-updates/s", "cores": cores, "kind": "port",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--elements", type=int, default=64, help="elements per axis")
+    ap.add_argument("--n", type=int, default=8, help="GLL nodes per axis")
+    ap.add_argument("--precision", choices=["f64", "f32"], default="f64")
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

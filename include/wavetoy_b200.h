@@ -68,6 +68,12 @@ int wt_ctx_launch_count(const wt_ctx* ctx, long long* count);
  * state stops being finite (the reference asserts all(isfinite, ...) per
  * sample, src/evolve.jl:1344); synchronous. */
 int wt_ctx_nonfinite(wt_ctx* ctx, int* flag);
+/* Per-kernel timing for measurement: while enabled, the fused RK4 step records
+ * CUDA events around each launch of its two kernels (gradient/flux and
+ * divergence) on the launching stream; wt_ctx_profile_read synchronises and
+ * returns the summed milliseconds and launch counts {K1, K2}, then clears. */
+int wt_ctx_profile(wt_ctx* ctx, int enable);
+int wt_ctx_profile_read(wt_ctx* ctx, double ms[2], long long count[2]);
 
 /* ---- mesh + geometry ------------------------------------------------------ */
 /* Analytic hex builder.  Replaces HexMeshes.make_uniform_hex(T, Mx, My, Mz,
@@ -128,6 +134,18 @@ int wt_background_set(wt_ctx* ctx, wt_mesh* mesh, const wt_background_desc* desc
 int wt_background_set_arrays(wt_ctx* ctx, wt_mesh* mesh, const double* coef11, wt_coef** out);
 int wt_coef_get(const wt_coef* coef, double* coef11_host);
 int wt_coef_destroy(wt_coef* coef);
+
+/* ---- initial data --------------------------------------------------------------*/
+enum { WT_IC_EIGENMODE_CARTESIAN = 0, WT_IC_GAUSSIANS = 1, WT_IC_OUTGOING_PULSE = 2, WT_IC_PLANE_WAVE = 3,
+       WT_IC_EIGENMODE_RADIAL = 4 };
+/* Fill u (and ut, may be NULL) on the device at time t:
+ *   EIGENMODE_CARTESIAN eigenmode_cartesian! (src/wave.jl:163-185): p = A, kx, ky, kz, omega, x0, x1
+ *   GAUSSIANS  the :gaussian IC (src/evolve.jl:1260-1263), summed: p = count, then (cx, cy, cz, A, w) each
+ *   OUTGOING_PULSE outgoing_pulse! (src/wave.jl:292-323): p = A, s0, sigma, cx, cy, cz
+ *   PLANE_WAVE Phi_e / Pi_e of _background3d :minkowski/:constant_shift (src/evolve.jl:1115-1118): p = k, omega, s
+ *   EIGENMODE_RADIAL eigenmode_radial! (src/wave.jl:207-226): p = A, R, n, cx, cy, cz */
+int wt_initial_data(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, int nparams, double t, void* u,
+                    void* ut);
 
 /* ---- workspace ---------------------------------------------------------------*/
 /* Replaces make_wave3d_workspace (src/wave3d_curved.jl:158-178): device

@@ -45,6 +45,4 @@ def ctx(wt):
     import torch
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    c = wt.Context(0)
-    yield c
-    c.close()
+    return wt.Context(0)

@@ -258,11 +258,19 @@ def test_sipg_standing_wave_100_steps(wt, ctx, O, tau):
     x, y, z = o.coords()
     u0 = wt.workloads.standing_wave(x, y, z)
     dt = 0.25 * o.min_spacing()
+    # tau = 20 is below the coercivity threshold at n = 6: an exponentially growing
+    # mode amplifies round-off differences, so parity is checked over 20 steps there
+    # and the growth itself (energy ratio) is compared at 100 steps.
+    nst = 100 if tau > 30 else 20
     ug, vg = dev(torch.float64, u0), g.zeros()
-    wt.step_rk4_sipg(ug, vg, ws, dt, 100, tau=tau, eps_KO=0.1)
-    uo, vo = o.evolve_sipg(u0, np.zeros_like(u0), dt, 100, tau=tau, eps_ko=0.1)
-    tol = TOL64 if tau > 30 else 1e-10
-    assert rel(host(ug), uo) < tol and rel(host(vg), vo) < tol
+    wt.step_rk4_sipg(ug, vg, ws, dt, nst, tau=tau, eps_KO=0.1)
+    uo, vo = o.evolve_sipg(u0, np.zeros_like(u0), dt, nst, tau=tau, eps_ko=0.1)
+    assert rel(host(ug), uo) < TOL64 and rel(host(vg), vo) < TOL64
+    if tau < 30:
+        wt.step_rk4_sipg(ug, vg, ws, dt, 80, tau=tau, eps_KO=0.1)
+        uo, vo, E = o.evolve_sipg(uo, vo, dt, 80, tau=tau, eps_ko=0.1, record_energy=True)
+        Eg = wt.energy_sipg(ug, vg, ws, tau)
+        assert abs(Eg / E[-1] - 1) < 1e-2 and E[-1] > 1e3 * E[0]
 
 
 def test_evolve_host_matches_device_stepping(wt, ctx, O):

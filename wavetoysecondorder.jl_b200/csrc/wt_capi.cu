@@ -24,7 +24,18 @@ struct wt_ctx {
   unsigned int* d_flag = nullptr;
   double* d_partial = nullptr;
   int nblocks = 0;
+  // per-kernel timing (CUDA events around K1/K2 launches on the launching stream)
+  int prof_on = 0;
+  std::vector<cudaEvent_t> prof_ev[2];  // [kernel] start/stop pairs
 };
+
+static void prof_mark(wt_ctx* ctx, int which) {
+  if (!ctx->prof_on) return;
+  cudaEvent_t ev;
+  if (cudaEventCreate(&ev) != cudaSuccess) return;
+  cudaEventRecord(ev, ctx->stream);
+  ctx->prof_ev[which].push_back(ev);
+}
 
 struct wt_mesh {
   wt_ctx* ctx = nullptr;
@@ -373,6 +384,30 @@ int wt_ctx_launch_count(const wt_ctx* ctx, long long* count) {
   return 0;
 }
 
+int wt_ctx_profile(wt_ctx* ctx, int enable) {
+  if (!ctx) return WT_EINVAL;
+  ctx->prof_on = enable ? 1 : 0;
+  return 0;
+}
+
+int wt_ctx_profile_read(wt_ctx* ctx, double ms[2], long long count[2]) {
+  if (!ctx || !ms || !count) return WT_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "profile");
+  for (int k = 0; k < 2; ++k) {
+    ms[k] = 0.0;
+    count[k] = 0;
+    auto& v = ctx->prof_ev[k];
+    for (size_t i = 0; i + 1 < v.size(); i += 2) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, v[i], v[i + 1]) == cudaSuccess) { ms[k] += t; ++count[k]; }
+    }
+    for (auto ev : v) cudaEventDestroy(ev);
+    v.clear();
+  }
+  return 0;
+}
+
 int wt_ctx_nonfinite(wt_ctx* ctx, int* flag) {
   if (!ctx || !flag) return WT_EINVAL;
   unsigned int h = 0;
@@ -609,6 +644,26 @@ int wt_coef_destroy(wt_coef* c) {
   return 0;
 }
 
+// ---- initial data ---------------------------------------------------------------
+int wt_initial_data(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, int nparams, double t, void* u,
+                    void* ut) {
+  if (!ctx) return WT_EINVAL;
+  if (!mesh || !u || (nparams > 0 && !params)) return fail(ctx, WT_EINVAL, "wt_initial_data: NULL argument");
+  if (kind < 0 || kind > 4) return fail(ctx, WT_EINVAL, "wt_initial_data: unknown kind");
+  if (nparams < 0 || nparams > 4096) return fail(ctx, WT_EINVAL, "wt_initial_data: bad parameter count");
+  if (kind == WT_IC_GAUSSIANS && (nparams < 1 || 1 + 5 * (int)params[0] > nparams))
+    return fail(ctx, WT_EINVAL, "wt_initial_data: Gaussian count does not match the parameters");
+  double* dp = nullptr;
+  WT_TRY(dalloc(ctx, &dp, (nparams > 0 ? nparams : 1) * sizeof(double), nullptr));
+  if (nparams > 0) cudaMemcpyAsync(dp, params, nparams * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  int rc = lrc(ctx, wt::launch_initial(mesh->m, kind, dp, nparams, t, u, ut, ctx->stream), "initial data");
+  ctx->launches += 1;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(dp);
+  if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "initial data");
+  return rc;
+}
+
 // ---- workspace ---------------------------------------------------------------------
 int wt_workspace_create(wt_ctx* ctx, wt_mesh* mesh, wt_ws** out) {
   if (!ctx) return WT_EINVAL;
@@ -823,10 +878,14 @@ static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* P
     rkP.nonfinite = rkQ.nonfinite = st == 3 ? ctx->d_flag : nullptr;
     if (eps_ko == 0.0) {
       rkP.on = rkQ.on = 1;
+      prof_mark(ctx, 0);
       WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, inP, inQ, ws->F, nullptr, ws->bbuf, nullptr, use_metric, b, rkP,
                                          s), "rk4 K1"));
+      prof_mark(ctx, 0);
+      prof_mark(ctx, 1);
       WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, nullptr, ws->bbuf, use_metric, b, rkQ, rkQ.nonfinite, s),
                  "rk4 K2"));
+      prof_mark(ctx, 1);
       ctx->launches += 2;
     } else {
       WT_TRY(rhs_curved_impl(ctx, ws, coef, inP, inQ, ws->kP, ws->kQ, eps_ko, b, use_metric));

@@ -125,6 +125,8 @@ int launch_streamed_geometry(DevMesh& m, cudaStream_t s);
 int launch_background(const DevMesh& m, DevCoef& c, int kind, const double* p, cudaStream_t s);
 int launch_coef_combine(const DevMesh& m, DevCoef& c, cudaStream_t s);
 int launch_min_spacing(const DevMesh& m, double* out, cudaStream_t s);
+int launch_initial(const DevMesh& m, int kind, const double* dparams, int np, double t, void* u, void* ut,
+                   cudaStream_t s);
 
 // conservative first-order system (wt_cons.cu)
 struct ConsBC {

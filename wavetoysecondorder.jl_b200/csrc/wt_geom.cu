@@ -419,3 +419,75 @@ int launch_min_spacing(const DevMesh& m, double* out, cudaStream_t s) {
 }
 
 }  // namespace wt
+
+namespace wt {
+
+// ---------------------------------------------------------------------------
+// Initial data on the device (src/wave.jl:100-323, src/evolve.jl:1115-1118,
+// 1257-1263).  kind: 0 eigenmode_cartesian! (A, kx, ky, kz, omega, x0, x1),
+// 1 sum of Gaussians (count; then cx, cy, cz, A, w per pulse),
+// 2 outgoing_pulse! (A, s0, sigma, cx, cy, cz), 3 plane wave of the
+// constant-shift background (k, omega, s = bx+by+bz): Phi = sin(k(x+y+z) - omega t),
+// Pi = (-omega - k s) cos(...), 4 eigenmode_radial! (A, R, n, cx, cy, cz).
+__device__ inline double sinhc_dev(double x) {
+  const double x2 = x * x;
+  if (x2 < 1.0 / 1000.0) return 1.0 + x2 * (1.0 / 6.0 + x2 * (1.0 / 120.0 + x2 * (1.0 / 5040.0)));
+  return sinh(x) / x;
+}
+
+template <typename real>
+__global__ void k_initial(long long nn, int kind, const double* __restrict__ coords, const double* __restrict__ p,
+                          int np, double t, real* __restrict__ u, real* __restrict__ ut) {
+  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  const double x = coords[3 * n], y = coords[3 * n + 1], z = coords[3 * n + 2];
+  double uv = 0.0, vv = 0.0;
+  if (kind == 0) {
+    const double A = p[0], kx = p[1], ky = p[2], kz = p[3], om = p[4], x0 = p[5], L = p[6] - p[5];
+    const double s = sin(kx * (x - x0) / L) * sin(ky * (y - x0) / L) * sin(kz * (z - x0) / L);
+    uv = A * s * cos(om * t);
+    vv = -A * om * s * sin(om * t);
+  } else if (kind == 1) {
+    const int cnt = (int)p[0];
+    for (int q = 0; q < cnt && 1 + 5 * q + 4 < np; ++q) {
+      const double* g = p + 1 + 5 * q;
+      const double d2 = (x - g[0]) * (x - g[0]) + (y - g[1]) * (y - g[1]) + (z - g[2]) * (z - g[2]);
+      uv += g[3] * exp(-d2 / (2.0 * g[4] * g[4]));
+    }
+  } else if (kind == 2) {
+    const double A = p[0], s0 = p[1], sg = p[2];
+    const double isg2 = 1.0 / (sg * sg);
+    const double be = t + s0, be2 = be * be;
+    const double r2 = (x - p[3]) * (x - p[3]) + (y - p[4]) * (y - p[4]) + (z - p[5]) * (z - p[5]);
+    const double r = sqrt(r2);
+    const double ex = exp(-0.5 * (be2 + r2) * isg2);
+    uv = 2.0 * A * be * isg2 * sinhc_dev(be * r * isg2) * ex;
+    vv = -2.0 * A * isg2 * ex * (be2 * isg2 * sinhc_dev(be * r * isg2) - cosh(be * r * isg2));
+  } else if (kind == 3) {
+    const double k = p[0], om = p[1], s = p[2];
+    uv = sin(k * (x + y + z) - om * t);
+    vv = (-om - k * s) * cos(k * (x + y + z) - om * t);
+  } else if (kind == 4) {
+    const double A = p[0], R = p[1], nr = p[2];
+    const double om = nr * M_PI / R;
+    const double r = sqrt((x - p[3]) * (x - p[3]) + (y - p[4]) * (y - p[4]) + (z - p[5]) * (z - p[5]));
+    const double arg = nr * r / R;
+    const double sc = arg == 0.0 ? 1.0 : sin(M_PI * arg) / (M_PI * arg);
+    uv = A * sc * cos(om * t);
+    vv = -A * om * sc * sin(om * t);
+  }
+  u[n] = (real)uv;
+  if (ut) ut[n] = (real)vv;
+}
+
+int launch_initial(const DevMesh& m, int kind, const double* dparams, int np, double t, void* u, void* ut,
+                   cudaStream_t s) {
+  const unsigned b = (unsigned)((m.nn + 255) / 256);
+  if (m.precision == 0)
+    k_initial<double><<<b, 256, 0, s>>>(m.nn, kind, m.coords, dparams, np, t, (double*)u, (double*)ut);
+  else
+    k_initial<float><<<b, 256, 0, s>>>(m.nn, kind, m.coords, dparams, np, t, (float*)u, (float*)ut);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace wt

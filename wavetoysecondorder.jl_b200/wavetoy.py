@@ -26,6 +26,7 @@ FACE_SUBLUMINAL, FACE_OUTFLOW, FACE_INFLOW, FACE_SONIC = 1, 2, 3, 4
 SOMMERFELD_BDRY_TAG = 7
 EXCISION_BDRY_TAG = 8
 BG_MINKOWSKI, BG_CONSTANT_SHIFT, BG_ADM_PERTURBED, BG_RADIAL_SHIFT = 0, 1, 2, 3
+IC_EIGENMODE_CARTESIAN, IC_GAUSSIANS, IC_OUTGOING_PULSE, IC_PLANE_WAVE, IC_EIGENMODE_RADIAL = 0, 1, 2, 3, 4
 
 _ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENOTSUP", -5: "ENONFINITE", -6: "ETIMEOUT"}
 
@@ -91,6 +92,8 @@ def library():
         "wt_step_rk4_curved": [vp, vp, vp, vp, vp, d, i, d, C.POINTER(_BcDesc), i],
         "wt_step_rk4_sipg": [vp, vp, vp, vp, d, i, C.POINTER(C.c_double * 6), d, d, d],
         "wt_evolve_curved_host": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i, vp],
+        "wt_initial_data": [vp, vp, i, vp, i, d, vp, vp],
+        "wt_ctx_profile": [vp, i], "wt_ctx_profile_read": [vp, C.POINTER(d * 2), C.POINTER(ll * 2)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -129,10 +132,15 @@ class Context:
         rc = library().wt_ctx_create(device, C.byref(self.h))
         if rc != 0:
             raise WaveToyError(rc, f"wt_ctx_create(device={device}) failed")
+        self._children = []  # weak references to meshes / coefficients / workspaces
         if use_torch_stream:
             with torch.cuda.device(device):
                 s = torch.cuda.current_stream(device).cuda_stream
             library().wt_ctx_set_stream(self.h, C.c_void_p(s))
+
+    def _adopt(self, obj):
+        import weakref
+        self._children.append(weakref.ref(obj))
 
     def check(self, rc: int, what: str = ""):
         if rc != 0:
@@ -147,13 +155,30 @@ class Context:
         self.check(library().wt_ctx_launch_count(self.h, C.byref(n)))
         return n.value
 
+    def profile(self, enable: bool = True):
+        self.check(library().wt_ctx_profile(self.h, int(enable)))
+
+    def profile_read(self):
+        """((K1 ms, K1 launches), (K2 ms, K2 launches)) since the last read."""
+        ms = (C.c_double * 2)()
+        cnt = (C.c_longlong * 2)()
+        self.check(library().wt_ctx_profile_read(self.h, C.byref(ms), C.byref(cnt)))
+        return (ms[0], cnt[0]), (ms[1], cnt[1])
+
     def nonfinite(self) -> bool:
         f = C.c_int()
         self.check(library().wt_ctx_nonfinite(self.h, C.byref(f)))
         return bool(f.value)
 
     def close(self):
+        """Destroy the context after every object made on it (children first:
+        workspaces and coefficients, then meshes)."""
         if getattr(self, "h", None):
+            alive = [r() for r in getattr(self, "_children", [])]
+            for kind in (Workspace, Coef, Mesh):
+                for o in alive:
+                    if isinstance(o, kind):
+                        o.close()
             library().wt_ctx_destroy(self.h)
             self.h = None
 
@@ -164,7 +189,13 @@ class Context:
             pass
 
 
-class Mesh:
+class _Child:
+    def _ctx_alive(self) -> bool:
+        c = self.ctx if hasattr(self, "ctx") else self.mesh.ctx
+        return getattr(c, "h", None) is not None
+
+
+class Mesh(_Child):
     """Mesh + MeshGeometry (+ metric terms) on the device.
 
     Stands in for HexMeshes.make_uniform_hex / make_warped_uniform_hex followed
@@ -174,6 +205,7 @@ class Mesh:
     def __init__(self, ctx: Context, h, N: int, Ne: int, precision: int):
         self.ctx, self.h, self.N, self.Ne, self.precision = ctx, h, N, Ne, precision
         self.nn = N ** 3 * Ne
+        ctx._adopt(self)
         self.dtype = _torch().float64 if precision == WT_F64 else _torch().float32
 
     @classmethod
@@ -247,7 +279,7 @@ class Mesh:
         return torch.zeros(self.nn, dtype=self.dtype, device=f"cuda:{self.ctx.device}")
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and self._ctx_alive():
             library().wt_mesh_destroy(self.h)
             self.h = None
 
@@ -258,11 +290,12 @@ class Mesh:
             pass
 
 
-class Coef:
+class Coef(_Child):
     """The coefficient bundle of make_coef3d / sample_background3d! (src/wave3d_curved.jl:106-124)."""
 
     def __init__(self, mesh: Mesh, h):
         self.mesh, self.h = mesh, h
+        mesh.ctx._adopt(self)
 
     def get(self):
         """11 fields (alpha, sqrtg, b1, b2, b3, gu11, gu12, gu13, gu22, gu23, gu33), FP64 host."""
@@ -272,7 +305,7 @@ class Coef:
         return out
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and self._ctx_alive():
             library().wt_coef_destroy(self.h)
             self.h = None
 
@@ -306,20 +339,21 @@ def background_from_arrays(mesh: Mesh, coef11) -> Coef:
     return Coef(mesh, h)
 
 
-class Workspace:
+class Workspace(_Child):
     """Wave3DWorkspace: scratch + mu (src/wave3d_curved.jl:137-178)."""
 
     def __init__(self, mesh: Mesh):
         self.mesh, self.ctx = mesh, mesh.ctx
         self.h = C.c_void_p()
         self.ctx.check(library().wt_workspace_create(self.ctx.h, mesh.h, C.byref(self.h)), "wt_workspace_create")
+        self.ctx._adopt(self)
         mu = C.c_double()
         library().wt_workspace_mu(self.h, C.byref(mu))
         self.mu = mu.value
         self.inv_mu5 = (1.0 / self.mu) ** 5 if self.mu > 0 else 0.0
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and self._ctx_alive():
             library().wt_workspace_destroy(self.h)
             self.h = None
 
@@ -555,3 +589,21 @@ def evolve_curved_host(Phi_host, Pi_host, coef: Coef, ws: Workspace, dt: float, 
     ws.ctx.check(library().wt_evolve_curved_host(ws.ctx.h, ws.h, coef.h, addr(Phi_host), addr(Pi_host), float(dt),
                                                  int(steps_per_sample), int(nsamples), float(eps_KO), p, int(metric),
                                                  addr(energy)), "evolve_curved_host")
+
+
+def initial_data(mesh: Mesh, kind: int, params: Sequence[float], u, ut=None, t: float = 0.0):
+    """Initial data / analytic references on the device: eigenmode_cartesian!,
+    the :gaussian IC (summed pulses), outgoing_pulse!, the constant-shift plane
+    wave and eigenmode_radial! (src/wave.jl:100-323, src/evolve.jl:1115-1118, 1257-1263)."""
+    import numpy as np
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    mesh.ctx.check(library().wt_initial_data(mesh.ctx.h, mesh.h, int(kind), p.ctypes.data if p.size else None,
+                                             int(p.size), float(t), _ptr(u), _ptr(ut)), "initial_data")
+    return u, ut
+
+
+def gaussian_params(centres, amps, widths):
+    out = [float(len(amps))]
+    for c, a, w in zip(centres, amps, widths):
+        out += [float(c[0]), float(c[1]), float(c[2]), float(a), float(w)]
+    return out
