@@ -323,3 +323,41 @@ def test_errors_are_reported(wt, ctx):
         wt.apply_D(a, a.clone(), 4, ws)
     with pytest.raises(wt.WaveToyError):
         wt.step_rk4_curved(a, a.clone(), cg, ws, -1.0, 3)
+
+
+@pytest.mark.parametrize("kinds,exc", [([2] * 6, 0), ([1] * 6, 8), ([4] * 6, 0)])
+def test_n8_pipelined_path_many_elements(wt, ctx, O, kinds, exc):
+    """n = 8 FP64 curvilinear RHS and RK4 on 384 elements (more than one per SM, so the
+    persistent TMA pipeline cycles both stages) with Dirichlet data, excision tags and
+    full-Dirichlet data; checked against the oracle."""
+    import torch
+    g, o = pair(wt, ctx, O, 8, (8, 8, 6), A=0.05, outer_tag=7)
+    if exc:
+        bd = o.get("bdry").copy()
+        bd[4::6][bd[4::6] != 0] = exc   # -z faces excised
+        o.set_bdry(bd)
+        g.set_bdry(bd)
+    p = wt.workloads.adm_params(9)
+    cg, co = wt.sample_background3d(g, 2, p), o.background(2, p)
+    ws = wt.make_wave3d_workspace(g)
+    rng = np.random.default_rng(41)
+    Phi, Pi = rng.standard_normal(o.nn), rng.standard_normal(o.nn)
+    data = [rng.standard_normal(o.nn) for _ in range(5)]
+    bcg = wt.make_bc3d(kinds, gPhi=dev(torch.float64, data[0]), gPi=dev(torch.float64, data[1]),
+                       gDx=dev(torch.float64, data[2]), gDy=dev(torch.float64, data[3]),
+                       gDz=dev(torch.float64, data[4]), excision_tag=exc)
+    bco = O.make_bc(kinds, gPhi=data[0], gPi=data[1], gDx=data[2], gDy=data[3], gDz=data[4], excision_tag=exc)
+    Pd, Qd = g.zeros(), g.zeros()
+    wt.wave3d_curved_rhs(Pd, Qd, dev(torch.float64, Phi), dev(torch.float64, Pi), cg, ws, eps_KO=0.0, bc3d=bcg,
+                         metric=True)
+    Po, Qo = o.rhs_curved(co, Phi, Pi, eps_ko=0.0, bc=bco, use_metric=True)
+    assert rel(host(Pd), Po) < TOL64 and rel(host(Qd), Qo) < TOL64
+    x, y, z = o.coords()
+    Phi = wt.workloads.gaussian_field(x, y, z, *wt.workloads.pulses(9, 2))
+    Pi = 0.1 * Phi
+    dt = 0.2 * o.min_spacing() / wt.workloads.max_speed(p)
+    Pg, Qg = dev(torch.float64, Phi), dev(torch.float64, Pi)
+    wt.step_rk4_curved(Pg, Qg, cg, ws, dt, 6, bc3d=bcg, metric=True)
+    Po, Qo = o.evolve_curved(co, Phi, Pi, dt, 6, bc=bco, use_metric=True)
+    assert rel(host(Pg), Po) < TOL64 and rel(host(Qg), Qo) < TOL64
+    assert not ctx.nonfinite()

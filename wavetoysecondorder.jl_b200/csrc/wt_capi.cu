@@ -27,10 +27,13 @@ struct wt_ctx {
   // per-kernel timing (CUDA events around K1/K2 launches on the launching stream)
   int prof_on = 0;
   std::vector<cudaEvent_t> prof_ev[2];  // [kernel] start/stop pairs
+  cudaEvent_t ord_a = nullptr, ord_b = nullptr;  // order the graph stream with the caller's stream
 };
 
 static void prof_mark(wt_ctx* ctx, int which) {
   if (!ctx->prof_on) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
   cudaEvent_t ev;
   if (cudaEventCreate(&ev) != cudaSuccess) return;
   cudaEventRecord(ev, ctx->stream);
@@ -342,6 +345,8 @@ int wt_ctx_create(int device, wt_ctx** out) {
     return WT_ENOMEM;
   }
   cudaMemset(c->d_flag, 0, sizeof(unsigned int));
+  cudaEventCreateWithFlags(&c->ord_a, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&c->ord_b, cudaEventDisableTiming);
   *out = c;
   return 0;
 }
@@ -352,6 +357,8 @@ int wt_ctx_destroy(wt_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   cudaFree(ctx->d_flag);
   cudaFree(ctx->d_partial);
+  cudaEventDestroy(ctx->ord_a);
+  cudaEventDestroy(ctx->ord_b);
   cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return 0;
@@ -415,7 +422,8 @@ int wt_ctx_nonfinite(wt_ctx* ctx, int* flag) {
   cudaMemsetAsync(ctx->d_flag, 0, sizeof(unsigned int), ctx->stream);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "nonfinite flag");
-  *flag = h ? 1 : 0;
+  *flag = (h & 1u) ? 1 : 0;
+  if (h & 2u) return fail(ctx, WT_ETIMEOUT, "a bounded wait for staged data gave up in a pipelined kernel");
   return 0;
 }
 
@@ -432,6 +440,7 @@ int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* d, wt_mesh** out) {
   auto* mh = new wt_mesh();
   mh->ctx = ctx;
   wt::DevMesh& m = mh->m;
+  m.errflag = ctx->d_flag;
   m.N = d->N;
   for (int a = 0; a < 3; ++a) m.M[a] = d->M[a];
   m.Ne = (long long)d->M[0] * d->M[1] * d->M[2];
@@ -487,6 +496,7 @@ int wt_mesh_create_arrays(wt_ctx* ctx, int N, long long Ne, const double* coords
   auto* mh = new wt_mesh();
   mh->ctx = ctx;
   wt::DevMesh& m = mh->m;
+  m.errflag = ctx->d_flag;
   m.N = N; m.Ne = Ne; m.nn = Ne * N * N * N; m.precision = precision; m.affine = 0;
   m.h_nbr.resize(6 * Ne); m.h_nbrf.resize(6 * Ne); m.h_bdry.resize(6 * Ne);
   for (long long i = 0; i < 6 * Ne; ++i) {
@@ -897,6 +907,42 @@ static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* P
   return 0;
 }
 
+}  // extern "C"
+
+// Capture one step (any stream may be the caller's, including the legacy
+// default stream, which cannot be captured): capture and replay on the
+// context's own stream, ordered after / before the caller's stream by events.
+template <typename F>
+static int replay_graph(wt_ctx* ctx, int nsteps, F&& one_step) {
+  cudaStream_t user = ctx->stream, own = ctx->own_stream;
+  cudaEventRecord(ctx->ord_a, user);
+  cudaStreamWaitEvent(own, ctx->ord_a, 0);
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const long long before = ctx->launches;
+  ctx->stream = own;
+  cudaError_t e = cudaStreamBeginCapture(own, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) { ctx->stream = user; return cuda_fail(ctx, e, "graph capture"); }
+  int rc = one_step();
+  e = cudaStreamEndCapture(own, &graph);
+  ctx->stream = user;
+  if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_fail(ctx, e, "graph instantiate"); }
+  const long long per = ctx->launches - before;
+  ctx->launches = before;
+  for (int i = 0; i < nsteps && e == cudaSuccess; ++i) e = cudaGraphLaunch(exec, own);
+  ctx->launches += per * nsteps;
+  cudaEventRecord(ctx->ord_b, own);
+  cudaStreamWaitEvent(user, ctx->ord_b, 0);
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "graph launch");
+}
+
+extern "C" {
+
 int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
                        double eps_ko, const wt_bc_desc* bc, int use_metric) {
   WT_TRY(check_ws(ctx, ws));
@@ -912,24 +958,7 @@ int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, v
     return 0;
   }
   // capture one step as a CUDA graph and replay it
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  long long before = ctx->launches;
-  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
-  int rc = step_curved_once(ctx, ws, coef, Phi, Pi, dt, eps_ko, b, use_metric);
-  e = cudaStreamEndCapture(ctx->stream, &graph);
-  if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
-  e = cudaGraphInstantiate(&exec, graph, 0);
-  if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_fail(ctx, e, "graph instantiate"); }
-  const long long per = ctx->launches - before;
-  ctx->launches = before;
-  for (int i = 0; i < nsteps && e == cudaSuccess; ++i) e = cudaGraphLaunch(exec, ctx->stream);
-  ctx->launches += per * nsteps;
-  cudaGraphExecDestroy(exec);
-  cudaGraphDestroy(graph);
-  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "graph launch");
+  return replay_graph(ctx, nsteps, [&]() { return step_curved_once(ctx, ws, coef, Phi, Pi, dt, eps_ko, b, use_metric); });
 }
 
 static int step_sipg_once(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, const double bv[6], double tau,
@@ -969,24 +998,8 @@ int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int n
     for (int i = 0; i < nsteps; ++i) WT_TRY(step_sipg_once(ctx, ws, u, ut, dt, bdry_values, tau, sommerfeld_R, eps_ko));
     return 0;
   }
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  long long before = ctx->launches;
-  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
-  int rc = step_sipg_once(ctx, ws, u, ut, dt, bdry_values, tau, sommerfeld_R, eps_ko);
-  e = cudaStreamEndCapture(ctx->stream, &graph);
-  if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
-  e = cudaGraphInstantiate(&exec, graph, 0);
-  if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_fail(ctx, e, "graph instantiate"); }
-  const long long per = ctx->launches - before;
-  ctx->launches = before;
-  for (int i = 0; i < nsteps && e == cudaSuccess; ++i) e = cudaGraphLaunch(exec, ctx->stream);
-  ctx->launches += per * nsteps;
-  cudaGraphExecDestroy(exec);
-  cudaGraphDestroy(graph);
-  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "graph launch");
+  return replay_graph(ctx, nsteps,
+                      [&]() { return step_sipg_once(ctx, ws, u, ut, dt, bdry_values, tau, sommerfeld_R, eps_ko); });
 }
 
 int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* Phi_host, double* Pi_host, double dt,

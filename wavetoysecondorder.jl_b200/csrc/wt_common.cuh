@@ -71,6 +71,9 @@ struct DevMesh {
   int line_len[3] = {0, 0, 0};      // elements per line (all lines equal length)
   int line_closed[3] = {0, 0, 0};   // periodic lines
   int32_t* lines[3] = {nullptr, nullptr, nullptr};  // [line*len + pos] element ids
+  // device status word of the owning context: bit 0 non-finite state, bit 1 a
+  // bounded wait in a pipelined kernel gave up
+  unsigned int* errflag = nullptr;
 };
 
 // Kernel-side view of the mesh (passed by value).
@@ -158,6 +161,11 @@ int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const vo
 int launch_cons_k2(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
                    const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s);
 int launch_apply_D(const DevMesh& m, const void* u, void* out, int d, cudaStream_t s);
+// n = 8 FP64 curvilinear path: persistent, TMA-pipelined, FP64 tensor cores (wt_cons_n8.cu)
+int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
+                      void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s);
+int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
+                      const RKStage& rk, unsigned* flag, cudaStream_t s);
 int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s);
 int launch_div3d(const DevMesh& m, const void* F, void* out, cudaStream_t s);
 

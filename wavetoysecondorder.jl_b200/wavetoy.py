@@ -136,7 +136,10 @@ class Context:
         if use_torch_stream:
             with torch.cuda.device(device):
                 s = torch.cuda.current_stream(device).cuda_stream
-            library().wt_ctx_set_stream(self.h, C.c_void_p(s))
+            # torch's default stream is the legacy default stream (handle 0); name it
+            # explicitly as cudaStreamLegacy (0x1) so launches are ordered with torch's
+            # work and torch.cuda.Event timings bracket them
+            library().wt_ctx_set_stream(self.h, C.c_void_p(s if s else 1))
 
     def _adopt(self, obj):
         import weakref
