@@ -12,6 +12,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-12
+TOL_TC = 5e-12  # one RHS evaluation through the n = 8 FP64 tensor-core path (round-off bound)
 TOL32 = 1e-5
 
 
@@ -140,8 +141,9 @@ def test_rhs_curved(wt, ctx, O, case):
     wt.wave3d_curved_rhs(Pd, Qd, dev(torch.float64, Phi), dev(torch.float64, Pi), cg, ws, eps_KO=eps, bc3d=bcg,
                          metric=um)
     Po, Qo = o.rhs_curved(co, Phi, Pi, eps_ko=eps, bc=bco, use_metric=um)
-    assert rel(host(Pd), Po) < TOL64
-    assert rel(host(Qd), Qo) < TOL64
+    tol = TOL_TC if (N == 8 and um) else TOL64
+    assert rel(host(Pd), Po) < tol
+    assert rel(host(Qd), Qo) < tol
 
 
 def test_rhs_curved_excision_tag(wt, ctx, O):
@@ -348,11 +350,20 @@ def test_n8_pipelined_path_many_elements(wt, ctx, O, kinds, exc):
                        gDz=dev(torch.float64, data[4]), excision_tag=exc)
     bco = O.make_bc(kinds, gPhi=data[0], gPi=data[1], gDx=data[2], gDy=data[3], gDz=data[4], excision_tag=exc)
     Pd, Qd = g.zeros(), g.zeros()
+    # single RHS evaluations on the n = 8 tensor-core path: the m8n8k4 contractions
+    # sum in another order than the oracle, which leaves round-off differences of
+    # ~1-3e-12 relative; the RK-evolved state below is held to 1e-12
     wt.wave3d_curved_rhs(Pd, Qd, dev(torch.float64, Phi), dev(torch.float64, Pi), cg, ws, eps_KO=0.0, bc3d=bcg,
                          metric=True)
     Po, Qo = o.rhs_curved(co, Phi, Pi, eps_ko=0.0, bc=bco, use_metric=True)
-    assert rel(host(Pd), Po) < TOL64 and rel(host(Qd), Qo) < TOL64
+    assert rel(host(Pd), Po) < TOL_TC and rel(host(Qd), Qo) < TOL_TC
     x, y, z = o.coords()
+    Phi = wt.workloads.gaussian_field(x, y, z, *wt.workloads.pulses(9, 2))
+    Pi = 0.1 * Phi
+    wt.wave3d_curved_rhs(Pd, Qd, dev(torch.float64, Phi), dev(torch.float64, Pi), cg, ws, eps_KO=0.0, bc3d=bcg,
+                         metric=True)
+    Po, Qo = o.rhs_curved(co, Phi, Pi, eps_ko=0.0, bc=bco, use_metric=True)
+    assert rel(host(Pd), Po) < TOL_TC and rel(host(Qd), Qo) < TOL_TC
     Phi = wt.workloads.gaussian_field(x, y, z, *wt.workloads.pulses(9, 2))
     Pi = 0.1 * Phi
     dt = 0.2 * o.min_spacing() / wt.workloads.max_speed(p)

@@ -4,43 +4,46 @@
 // Same arithmetic as k_cons_k1 / k_cons_k2 in wt_cons.cu (the split-form
 // gradient / flux / Phidot and the split-form divergence of
 // wave3d_curved_rhs!, src/wave3d_curved.jl:205-258, with the curvilinear
-// Sommerfeld/Dirichlet pass of src/boundaries3d.jl:131-232 and the fused RK4
-// stage update), organised for B200:
-//   * one CTA of 8 warps per SM loops over elements (persistent grid);
-//   * every per-node field of the next element (a contiguous 4 KB block per
-//     field) is staged into shared memory by one elected thread with 1D bulk
-//     copies (cp.async.bulk ... mbarrier::complete_tx) while the current
-//     element computes -- a two-stage pipeline on two mbarriers, with bounded
-//     waits that raise an error flag instead of spinning forever;
+// boundary pass of src/boundaries3d.jl:131-232 and the fused RK4 stage
+// update), organised for B200:
+//   * one CTA of 16 warps per SM loops over elements (persistent grid);
+//   * the fields the derivative contractions read at other nodes of an
+//     element (Phi and the nine metric terms in K1; the three flux components
+//     and the metric terms in K2) are staged into shared memory with 1D bulk
+//     copies (cp.async.bulk ... mbarrier::complete_tx), one copy per k-plane
+//     into a plane-padded layout (stride 68 doubles) that makes the tensor-core
+//     operand loads bank-conflict-free, double-buffered on two mbarriers with
+//     bounded waits that raise an error flag instead of spinning forever;
+//   * the fields used only at their own node (background coefficients, Pi,
+//     1/J, the RK4 state) are prefetched into registers one element ahead;
 //   * the 8x8 reference-derivative contractions run on the FP64 tensor cores
-//     (mma.sync.m8n8k4.f64): for axis al the element's 64 pencils are the N
-//     dimension, G the A operand (held in registers for the whole kernel),
-//     the staged field -- or the split-form product Ja*u / Ja.F formed while
-//     loading the B fragment -- the B operand; warp w owns pencils 8w..8w+7;
-//   * the three axes accumulate into a per-node smem array, then a node phase
-//     (2 nodes per thread) adds the SATs, flux, boundary terms and the RK4
-//     stage update and writes coalesced results.
-// Neighbour face traces of the next element are prefetched into registers
-// during the current element and parked in smem at the end of the iteration.
+//     (mma.sync.m8n8k4.f64): for axis al an element's 64 pencils are the N
+//     dimension, G the A operand (in registers), the staged field -- or the
+//     split-form product Ja*u / Ja.F formed while loading -- the B operand.
+//     Warp w owns pencil tile w&7; warps w and w+8 split the fields of a tile.
+//     The centred-flux SATs are added in the same pass: an output row l = 0
+//     or 7 of the MMA is the node row on face 2al or 2al+1;
+//   * a node phase (one node per thread) forms flux, Phidot / divergence,
+//     boundary terms (boundary elements only) and the RK4 stage update and
+//     writes coalesced results.
 #include "wt_common.cuh"
 
 namespace wt {
 
 namespace n8 {
 
-constexpr int N = 8, N2 = 64, N3 = 512, THREADS = 256;
-constexpr unsigned FIELD_BYTES = N3 * sizeof(double);  // 4096
+constexpr int N = 8, N2 = 64, N3 = 512, THREADS = 512;
+constexpr int PS = 68;             // padded k-plane stride (doubles)
+constexpr int FS = 8 * PS;         // padded field size (544 doubles = 4352 B)
+constexpr unsigned PLANE_BYTES = N2 * sizeof(double);  // 512
 constexpr long long WAIT_LIMIT = 1LL << 24;
 
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   unsigned ok;
@@ -54,10 +57,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
 }
 __device__ __forceinline__ void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -69,12 +72,26 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-// node index of position p along axis al of pencil q (q = j+8k | i+8k | i+8j)
-__device__ __forceinline__ int pnode(int al, int p, int q) {
-  return al == 0 ? p + 8 * q : al == 1 ? (q & 7) + 8 * p + 64 * (q >> 3) : q + 64 * p;
+__device__ __forceinline__ int pad(int i, int j, int k) { return i + 8 * j + PS * k; }
+
+// Per-lane operand / output node offsets (padded) for axis al, tile w:
+//   B operand: position p = 4 kc + tig along al, pencil slot g;
+//   outputs:   row l = g along al, pencil slot 2 tig + b.
+// Pencil orders: al=0 (j = w, k = slot); al=1 (i = slot, k = w); al=2 (i = slot, j = w).
+__device__ __forceinline__ int bnode(int al, int w, int kc, int g, int tig) {
+  const int p = 4 * kc + tig;
+  return al == 0 ? pad(p, w, g) : al == 1 ? pad(g, p, w) : pad(g, w, p);
+}
+__device__ __forceinline__ int onode(int al, int w, int b, int g, int tig) {
+  const int sl = 2 * tig + b;
+  return al == 0 ? pad(g, w, sl) : al == 1 ? pad(sl, g, w) : pad(sl, w, g);
+}
+// face-trace index (p + 8 q) of an output node on the al-face
+__device__ __forceinline__ int opq(int al, int w, int b, int tig) {
+  const int sl = 2 * tig + b;
+  return al == 0 ? w + 8 * sl : al == 1 ? sl + 8 * w : sl + 8 * w;
 }
 
-// bounded wait on an mbarrier phase; returns false (and sets *err) on timeout
 __device__ __forceinline__ bool wait_phase(uint64_t* bar, unsigned parity, unsigned* err) {
   for (long long it = 0; it < WAIT_LIMIT; ++it)
     if (mbar_try_wait(bar, parity)) return true;
@@ -85,8 +102,6 @@ __device__ __forceinline__ bool wait_phase(uint64_t* bar, unsigned parity, unsig
 }  // namespace n8
 
 // ---------------------------------------------------------------------------
-// K1: staged fields per element: 0 Phi, 1 Pi, 2..11 c10, 12..20 Ja, 21 invJ,
-// 22 y (stages 1, 2), 23 acc (stages 1..3).
 struct K1N8 {
   long long Ne, nn;
   const double* Phi;
@@ -119,26 +134,31 @@ struct K1N8 {
   unsigned* flag;
 };
 
-constexpr int K1_FIELDS = 24;
-constexpr size_t K1_STAGE = (size_t)K1_FIELDS * n8::N3;  // doubles
-constexpr size_t K1_SMEM = (2 * K1_STAGE + 3 * n8::N3 + 2 * 6 * n8::N2 + n8::N2) * sizeof(double) + 64;
+// K1 staged fields: 0 Phi, 1..9 Ja.  Register prefetch: c10 (10), Pi, invJ, y, acc.
+constexpr int K1_NF = 10;
+constexpr size_t K1_STAGE = (size_t)K1_NF * n8::FS;
+constexpr size_t K1_SMEM = (2 * K1_STAGE + 3 * n8::FS + 2 * 6 * n8::N2 + n8::N2) * sizeof(double) + 64;
 
 __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   using namespace n8;
   extern __shared__ __align__(128) unsigned char smraw[];
-  double* stg = reinterpret_cast<double*>(smraw);       // 2 stages
-  double* sg = stg + 2 * K1_STAGE;                      // 3 x 512 gradient accumulators
-  double* sface = sg + 3 * N3;                          // 2 x 6 x 64
+  double* stg = reinterpret_cast<double*>(smraw);       // 2 stages x 10 padded fields
+  double* sg = stg + 2 * K1_STAGE;                      // 3 padded gradient accumulators
+  double* sface = sg + 3 * FS;                          // 2 x 6 x 64
   double* sG = sface + 2 * 6 * N2;                      // 64
   uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);  // 2
   __shared__ int abort_flag;
+  __shared__ int emeta[2][2];  // [stage]: interior-face mask, boundary flag
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int gq = lane >> 2, tig = lane & 3;
+  const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
   const long long nn = P.nn;
-  const double Hend = P.H[0];
+  const double inv2H = 1.0 / (2.0 * P.H[0]);
   const bool need_y = P.epi && (P.stage == 1 || P.stage == 2);
   const bool need_acc = P.epi && P.stage >= 1;
-  const unsigned tx_bytes = (22u + (need_y ? 1u : 0u) + (need_acc ? 1u : 0u)) * FIELD_BYTES;
+  const unsigned tx_bytes = K1_NF * 8u * PLANE_BYTES;
+  // node-phase coordinates of this thread
+  const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
+  const int tpad = pad(ti, tj, tk);
 
   if (tid < N2) sG[tid] = P.G[tid];
   if (tid == 0) {
@@ -149,151 +169,172 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   }
   __syncthreads();
 
+  // warp 0 stages element e into stage s: 80 plane copies, 2-3 per lane
   auto issue = [&](long long e, int s) {
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&bar[s], tx_bytes);
+    }
+    __syncwarp();
     double* d = stg + s * K1_STAGE;
     const long long o = e * N3;
-    fence_proxy_async();
-    mbar_expect_tx(&bar[s], tx_bytes);
-    bulk_g2s(d + 0 * N3, P.Phi + o, FIELD_BYTES, &bar[s]);
-    bulk_g2s(d + 1 * N3, P.Pi + o, FIELD_BYTES, &bar[s]);
-    for (int c = 0; c < 10; ++c) bulk_g2s(d + (2 + c) * N3, P.c10 + c * nn + o, FIELD_BYTES, &bar[s]);
-    for (int c = 0; c < 9; ++c) bulk_g2s(d + (12 + c) * N3, P.Ja + c * nn + o, FIELD_BYTES, &bar[s]);
-    bulk_g2s(d + 21 * N3, P.invdetJ + o, FIELD_BYTES, &bar[s]);
-    if (need_y) bulk_g2s(d + 22 * N3, P.y + o, FIELD_BYTES, &bar[s]);
-    if (need_acc) bulk_g2s(d + 23 * N3, P.acc + o, FIELD_BYTES, &bar[s]);
+    for (int c = lane; c < K1_NF * 8; c += 32) {
+      const int f = c >> 3, k = c & 7;
+      const double* src = (f == 0 ? P.Phi + o : P.Ja + (long long)(f - 1) * nn + o) + k * N2;
+      bulk_g2s(d + f * FS + k * PS, src, PLANE_BYTES, &bar[s]);
+    }
   };
-  // neighbour Phi face traces of element e: 384 values, <= 2 per thread
-  auto face_load = [&](long long e, double fr[2]) {
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const int idx = tid + r * THREADS;
-      double v = 0.0;
-      if (e >= 0 && idx < 6 * N2) {
-        const int f = idx >> 6, pq = idx & 63;
-        const int en = P.nbr[f + 6 * e];
-        if (en >= 0 && P.bdry[f + 6 * e] == 0) {
-          const int fn = P.nbrf[f + 6 * e];
-          v = P.Phi[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N)];
-        }
+  // per-element metadata: interior-face mask (SAT faces) and boundary flag
+  auto meta = [&](long long e, int s) {
+    if (tid == 0) {
+      int mask = 0, bnd = 0;
+      for (int f = 0; f < 6; ++f) {
+        const int b = P.bdry[f + 6 * e];
+        if (b == 0 && P.nbr[f + 6 * e] >= 0) mask |= 1 << f;
+        if (b != 0) bnd = 1;
       }
-      fr[r] = v;
+      emeta[s][0] = mask;
+      emeta[s][1] = bnd;
     }
   };
-  auto face_store = [&](int s, const double fr[2]) {
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const int idx = tid + r * THREADS;
-      if (idx < 6 * N2) sface[s * 6 * N2 + idx] = fr[r];
+  // neighbour Phi face traces (384 values; threads 0..383)
+  auto face_load = [&](long long e) -> double {
+    double v = 0.0;
+    if (e >= 0 && tid < 6 * N2) {
+      const int f = tid >> 6, pq = tid & 63;
+      const int en = P.nbr[f + 6 * e];
+      if (en >= 0 && P.bdry[f + 6 * e] == 0) {
+        const int fn = P.nbrf[f + 6 * e];
+        v = P.Phi[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N)];
+      }
     }
+    return v;
+  };
+  // pointwise fields of this thread's node
+  struct PW {
+    double c[10], Pi, invJ, y, acc;
+  };
+  auto pw_load = [&](long long e, PW& w) {
+    if (e < 0) return;
+    const long long n = e * N3 + tid;
+#pragma unroll
+    for (int c = 0; c < 10; ++c) w.c[c] = P.c10[c * nn + n];
+    w.Pi = P.Pi[n];
+    w.invJ = P.invdetJ[n];
+    w.y = need_y ? P.y[n] : 0.0;
+    w.acc = need_acc ? P.acc[n] : 0.0;
   };
 
   long long e = blockIdx.x;
+  PW cur;
   if (e < P.Ne) {
-    if (tid == 0) issue(e, 0);
-    double fr[2];
-    face_load(e, fr);
-    face_store(0, fr);
+    if (warp == 0) issue(e, 0);
+    meta(e, 0);
+    const double fv = face_load(e);
+    if (tid < 6 * N2) sface[tid] = fv;
+    pw_load(e, cur);
   }
   __syncthreads();
-  // A fragments of G: row g, columns 4 kc + tig
   const double aG0 = sG[gq * 8 + tig], aG1 = sG[gq * 8 + 4 + tig];
 
   for (int it = 0; e < P.Ne; ++it, e += gridDim.x) {
     const int s = it & 1;
     const unsigned parity = (it >> 1) & 1;
     const long long en = e + gridDim.x;
-    if (tid == 0 && en < P.Ne) issue(en, s ^ 1);
-    double fr[2];
-    face_load(en < P.Ne ? en : -1, fr);
+    const bool has_next = en < P.Ne;
+    if (warp == 0 && has_next) issue(en, s ^ 1);
+    if (has_next) meta(en, s ^ 1);
+    const double fnext = face_load(has_next ? en : -1);
+    PW nxt;
+    pw_load(has_next ? en : -1, nxt);
     if (!wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
     __syncthreads();
     if (abort_flag) {
-      if (tid == 0 && en < P.Ne) wait_phase(&bar[s ^ 1], ((it + 1) >> 1) & 1, nullptr);
+      if (warp == 0 && lane == 0 && has_next) wait_phase(&bar[s ^ 1], ((it + 1) >> 1) & 1, nullptr);
       return;
     }
     const double* d = stg + s * K1_STAGE;
     const double* sPhi = d;
-    const double* sJa = d + 12 * N3;
-    // ---- tensor-core contractions, one axis per phase ----
+    const double* sJa = d + FS;  // 9 fields, index (al*3 + c)
+    const double* sfc = sface + s * 6 * N2;
+    const int mask = emeta[s][0];
+    const int bnd = emeta[s][1];
+    // ---- tensor-core contractions + SAT, one axis per phase ----
 #pragma unroll 1
     for (int al = 0; al < 3; ++al) {
-      double c[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-      const double* m0 = sJa + (al * 3 + 0) * N3;
-      const double* m1 = sJa + (al * 3 + 1) * N3;
-      const double* m2 = sJa + (al * 3 + 2) * N3;
+      // half 0: component 0; half 1: components 1 and 2
+      const int c0 = half == 0 ? 0 : 1;
+      const int ncomp = half == 0 ? 1 : 2;
+      const double* mA = sJa + (al * 3 + c0) * FS;
+      const double* mB = sJa + (al * 3 + 2) * FS;
+      double cu[2] = {0, 0}, ca[2] = {0, 0}, cb[2] = {0, 0};
 #pragma unroll
       for (int kc = 0; kc < 2; ++kc) {
-        const int nd = pnode(al, 4 * kc + tig, 8 * warp + gq);
+        const int nd = bnode(al, wt8, kc, gq, tig);
         const double u = sPhi[nd];
         const double a = kc ? aG1 : aG0;
-        dmma(c[0][0], c[0][1], a, u);
-        dmma(c[1][0], c[1][1], a, m0[nd] * u);
-        dmma(c[2][0], c[2][1], a, m1[nd] * u);
-        dmma(c[3][0], c[3][1], a, m2[nd] * u);
+        dmma(cu[0], cu[1], a, u);
+        dmma(ca[0], ca[1], a, mA[nd] * u);
+        if (ncomp == 2) dmma(cb[0], cb[1], a, mB[nd] * u);
       }
+      const int face = gq == 0 ? 2 * al : (gq == 7 ? 2 * al + 1 : -1);
+      const bool sat = face >= 0 && ((mask >> face) & 1);
+      const double nh = (face & 1) ? 1.0 : -1.0;
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
-        const int no = pnode(al, gq, 8 * warp + 2 * tig + b);
-        const double du = c[0][b];
-        const double r0 = 0.5 * c[1][b] + 0.5 * m0[no] * du;
-        const double r1 = 0.5 * c[2][b] + 0.5 * m1[no] * du;
-        const double r2 = 0.5 * c[3][b] + 0.5 * m2[no] * du;
+        const int no = onode(al, wt8, b, gq, tig);
+        const double mo_a = mA[no];
+        double ra = 0.5 * ca[b] + 0.5 * mo_a * cu[b];
+        double rb = 0.0, mo_b = 0.0;
+        if (ncomp == 2) {
+          mo_b = mB[no];
+          rb = 0.5 * cb[b] + 0.5 * mo_b * cu[b];
+        }
+        if (sat) {
+          const double jump = sfc[face * N2 + opq(al, wt8, b, tig)] - sPhi[no];
+          ra += nh * mo_a * jump * inv2H;
+          if (ncomp == 2) rb += nh * mo_b * jump * inv2H;
+        }
+        double* ga = sg + c0 * FS;
         if (al == 0) {
-          sg[no] = r0; sg[N3 + no] = r1; sg[2 * N3 + no] = r2;
+          ga[no] = ra;
+          if (ncomp == 2) sg[2 * FS + no] = rb;
         } else {
-          sg[no] += r0; sg[N3 + no] += r1; sg[2 * N3 + no] += r2;
+          ga[no] += ra;
+          if (ncomp == 2) sg[2 * FS + no] += rb;
         }
       }
       __syncthreads();
     }
-    // ---- node phase ----
-    const double* sface_s = sface + s * 6 * N2;
-#pragma unroll 1
-    for (int r = 0; r < 2; ++r) {
-      const int t = tid + r * THREADS;
-      const int i = t & 7, j = (t >> 3) & 7, k = t >> 6;
-      const long long n = e * N3 + t;
-      const double u = sPhi[t];
-      double g[3] = {sg[t], sg[N3 + t], sg[2 * N3 + t]};
-      const int idx3[3] = {i, j, k};
-#pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        const int ax = f >> 1;
-        if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
-        if (P.bdry[f + 6 * e] != 0 || P.nbr[f + 6 * e] < 0) continue;
-        const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
-        const double jump = sface_s[f * N2 + p + 8 * q] - u;
-        const double nh = (f & 1) ? 1.0 : -1.0;
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) g[cc] += nh * sJa[(ax * 3 + cc) * N3 + t] * jump / (2.0 * Hend);
-      }
-      const double invJ = d[21 * N3 + t];
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) g[cc] *= invJ;
-      const double a = d[2 * N3 + t];
-      const double b0 = d[3 * N3 + t], b1 = d[4 * N3 + t], b2 = d[5 * N3 + t];
-      const double K0 = d[6 * N3 + t], K1v = d[7 * N3 + t], K2 = d[8 * N3 + t];
-      const double K3 = d[9 * N3 + t], K4 = d[10 * N3 + t], K5 = d[11 * N3 + t];
-      const double Pi = d[1 * N3 + t];
-      const double F0 = b0 * Pi + (K0 * g[0] + K1v * g[1] + K2 * g[2]);
-      const double F1 = b1 * Pi + (K1v * g[0] + K3 * g[1] + K4 * g[2]);
-      const double F2 = b2 * Pi + (K2 * g[0] + K4 * g[1] + K5 * g[2]);
-      double phid = b0 * g[0] + b1 * g[1] + b2 * g[2] + a * Pi;
-      if (P.bc_on) {
+    // ---- node phase: one node per thread ----
+    {
+      const long long n = e * N3 + tid;
+      const double u = sPhi[tpad];
+      double g0 = sg[tpad] * cur.invJ, g1 = sg[FS + tpad] * cur.invJ, g2 = sg[2 * FS + tpad] * cur.invJ;
+      const double a = cur.c[0];
+      const double b0 = cur.c[1], b1 = cur.c[2], b2 = cur.c[3];
+      const double K0 = cur.c[4], K1v = cur.c[5], K2 = cur.c[6], K3 = cur.c[7], K4 = cur.c[8], K5 = cur.c[9];
+      const double Pi = cur.Pi;
+      const double F0 = b0 * Pi + (K0 * g0 + K1v * g1 + K2 * g2);
+      const double F1 = b1 * Pi + (K1v * g0 + K3 * g1 + K4 * g2);
+      const double F2 = b2 * Pi + (K2 * g0 + K4 * g1 + K5 * g2);
+      double phid = b0 * g0 + b1 * g1 + b2 * g2 + a * Pi;
+      if (bnd && P.bc_on) {
+        const int idx3[3] = {ti, tj, tk};
         for (int f = 0; f < 6; ++f) {
           const int tag = P.bdry[f + 6 * e];
           if (tag == 0) continue;
           const int ax = f >> 1;
           if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
-          const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
+          const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
           const int slot = P.bslot[f + 6 * e];
           double dF = 0.0, dP = 0.0;
           if (tag != P.exc_tag) {
             const long long nb = (long long)P.nbf * N2;
             const long long bi = (long long)slot * N2 + p + 8 * q;
-            const double nx = P.bnorm[bi], ny = P.bnorm[nb + bi], nz = P.bnorm[2 * nb + bi],
-                         wt = P.bnorm[3 * nb + bi];
-            const double Kn = K0 * nx * nx + K3 * ny * ny + K5 * nz * nz + 2.0 * (K1v * nx * ny + K2 * nx * nz + K4 * ny * nz);
+            const double nx = P.bnorm[bi], ny = P.bnorm[nb + bi], nz = P.bnorm[2 * nb + bi], wt = P.bnorm[3 * nb + bi];
+            const double Kn =
+                K0 * nx * nx + K3 * ny * ny + K5 * nz * nz + 2.0 * (K1v * nx * ny + K2 * nx * nz + K4 * ny * nz);
             const double a_n = sqrt(a * Kn);
             const double bn = b0 * nx + b1 * ny + b2 * nz;
             if (P.kind == 4) {
@@ -302,7 +343,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
               dF = -tau * (u - gp);
               dP = -tau * (Pi - gqv);
             } else {
-              const double qv = nx * g[0] + ny * g[1] + nz * g[2];
+              const double qv = nx * g0 + ny * g1 + nz * g2;
               const double rr = Pi + ((bn + a_n) / a) * qv;
               double gv = 0.0;
               if (P.kind != 2) {
@@ -326,13 +367,13 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
           P.out[n] = u + (0.5 * dt) * phid;
           P.acc[n] = u + (dt / 6.0) * phid;
         } else if (P.stage == 1) {
-          P.out[n] = d[22 * N3 + t] + (0.5 * dt) * phid;
-          P.acc[n] = d[23 * N3 + t] + (dt / 3.0) * phid;
+          P.out[n] = cur.y + (0.5 * dt) * phid;
+          P.acc[n] = cur.acc + (dt / 3.0) * phid;
         } else if (P.stage == 2) {
-          P.out[n] = d[22 * N3 + t] + dt * phid;
-          P.acc[n] = d[23 * N3 + t] + (dt / 3.0) * phid;
+          P.out[n] = cur.y + dt * phid;
+          P.acc[n] = cur.acc + (dt / 3.0) * phid;
         } else {
-          const double v = d[23 * N3 + t] + (dt / 6.0) * phid;
+          const double v = cur.acc + (dt / 6.0) * phid;
           P.y[n] = v;
           if (P.flag && !isfinite(v)) atomicOr(P.flag, 1u);
         }
@@ -340,14 +381,13 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
         P.Phidot[n] = phid;
       }
     }
-    face_store(s ^ 1, fr);
+    if (has_next && tid < 6 * N2) sface[(s ^ 1) * 6 * N2 + tid] = fnext;
+    cur = nxt;
     __syncthreads();
   }
 }
 
 // ---------------------------------------------------------------------------
-// K2: staged fields per element: 0..2 F, 3..11 Ja, 12 invJ, 13 y (stages 0..2),
-// 14 acc (stages 1..3).
 struct K2N8 {
   long long Ne, nn;
   const double* F0;
@@ -372,27 +412,31 @@ struct K2N8 {
   unsigned* flag;
 };
 
-constexpr int K2_FIELDS = 15;
-constexpr size_t K2_STAGE = (size_t)K2_FIELDS * n8::N3;
-constexpr size_t K2_SMEM = (2 * K2_STAGE + n8::N3 + 2 * 6 * 3 * n8::N2 + n8::N2) * sizeof(double) + 64;
+// K2 staged fields: 0..2 F, 3..11 Ja.  Register prefetch: invJ, y, acc.
+constexpr int K2_NF = 12;
+constexpr size_t K2_STAGE = (size_t)K2_NF * n8::FS;
+constexpr size_t K2_SMEM = (2 * K2_STAGE + 2 * n8::FS + 2 * 6 * 3 * n8::N2 + n8::N2) * sizeof(double) + 64;
 
 __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   using namespace n8;
   extern __shared__ __align__(128) unsigned char smraw[];
   double* stg = reinterpret_cast<double*>(smraw);
-  double* sdiv = stg + 2 * K2_STAGE;                     // 512
-  double* sface = sdiv + N3;                             // 2 x 6 x 3 x 64
+  double* sdiv = stg + 2 * K2_STAGE;                     // 2 padded partial divergences
+  double* sface = sdiv + 2 * FS;                         // 2 x 6 x 3 x 64
   double* sG = sface + 2 * 6 * 3 * N2;                   // 64
   uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);
   __shared__ int abort_flag;
+  __shared__ int emeta[2][2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int gq = lane >> 2, tig = lane & 3;
+  const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
   const long long nn = P.nn;
-  const double Hend = P.H[0];
+  const double inv2H = 1.0 / (2.0 * P.H[0]);
   const bool need_y = P.epi && P.stage <= 2;
   const bool need_acc = P.epi && P.stage >= 1;
-  const unsigned tx_bytes = (13u + (need_y ? 1u : 0u) + (need_acc ? 1u : 0u)) * FIELD_BYTES;
-  const double* Fp[3] = {P.F0, P.F1, P.F2};
+  const unsigned tx_bytes = K2_NF * 8u * PLANE_BYTES;
+  const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
+  const int tpad = pad(ti, tj, tk);
+  constexpr int NFACE = 6 * 3 * N2;  // 1152
 
   if (tid < N2) sG[tid] = P.G[tid];
   if (tid == 0) {
@@ -404,49 +448,71 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   __syncthreads();
 
   auto issue = [&](long long e, int s) {
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&bar[s], tx_bytes);
+    }
+    __syncwarp();
     double* d = stg + s * K2_STAGE;
     const long long o = e * N3;
-    fence_proxy_async();
-    mbar_expect_tx(&bar[s], tx_bytes);
-    for (int c = 0; c < 3; ++c) bulk_g2s(d + c * N3, Fp[c] + o, FIELD_BYTES, &bar[s]);
-    for (int c = 0; c < 9; ++c) bulk_g2s(d + (3 + c) * N3, P.Ja + c * nn + o, FIELD_BYTES, &bar[s]);
-    bulk_g2s(d + 12 * N3, P.invdetJ + o, FIELD_BYTES, &bar[s]);
-    if (need_y) bulk_g2s(d + 13 * N3, P.y + o, FIELD_BYTES, &bar[s]);
-    if (need_acc) bulk_g2s(d + 14 * N3, P.acc + o, FIELD_BYTES, &bar[s]);
+    for (int c = lane; c < K2_NF * 8; c += 32) {
+      const int f = c >> 3, k = c & 7;
+      const double* src = (f == 0 ? P.F0 : f == 1 ? P.F1 : f == 2 ? P.F2 : P.Ja + (long long)(f - 3) * nn) + o + k * N2;
+      bulk_g2s(d + f * FS + k * PS, src, PLANE_BYTES, &bar[s]);
+    }
   };
-  // neighbour flux face traces: 6 faces x 3 components x 64 = 1152 values
-  constexpr int NF = 6 * 3 * N2;
-  constexpr int PER = (NF + THREADS - 1) / THREADS;  // 5
-  auto face_load = [&](long long e, double fr[PER]) {
+  auto meta = [&](long long e, int s) {
+    if (tid == 0) {
+      int mask = 0, bnd = 0;
+      for (int f = 0; f < 6; ++f) {
+        const int b = P.bdry[f + 6 * e];
+        if (b == 0 && P.nbr[f + 6 * e] >= 0) mask |= 1 << f;
+        if (b != 0) bnd = 1;
+      }
+      emeta[s][0] = mask;
+      emeta[s][1] = bnd;
+    }
+  };
+  // neighbour flux face traces: [f][c][pq], 1152 values, <= 3 per thread
+  auto face_load = [&](long long e, double fv[3]) {
 #pragma unroll
-    for (int r = 0; r < PER; ++r) {
+    for (int r = 0; r < 3; ++r) {
       const int idx = tid + r * THREADS;
       double v = 0.0;
-      if (e >= 0 && idx < NF) {
+      if (e >= 0 && idx < NFACE) {
         const int f = idx / (3 * N2), rem = idx - f * 3 * N2, c = rem >> 6, pq = rem & 63;
         const int en = P.nbr[f + 6 * e];
         if (en >= 0 && P.bdry[f + 6 * e] == 0) {
           const int fn = P.nbrf[f + 6 * e];
-          v = Fp[c][(long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N)];
+          const double* Fc = c == 0 ? P.F0 : c == 1 ? P.F1 : P.F2;
+          v = Fc[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N)];
         }
       }
-      fr[r] = v;
+      fv[r] = v;
     }
   };
-  auto face_store = [&](int s, const double fr[PER]) {
-#pragma unroll
-    for (int r = 0; r < PER; ++r) {
-      const int idx = tid + r * THREADS;
-      if (idx < NF) sface[s * NF + idx] = fr[r];
-    }
+  struct PW {
+    double invJ, y, acc;
+  };
+  auto pw_load = [&](long long e, PW& w) {
+    if (e < 0) return;
+    const long long n = e * N3 + tid;
+    w.invJ = P.invdetJ[n];
+    w.y = need_y ? P.y[n] : 0.0;
+    w.acc = need_acc ? P.acc[n] : 0.0;
   };
 
   long long e = blockIdx.x;
+  PW cur;
   if (e < P.Ne) {
-    if (tid == 0) issue(e, 0);
-    double fr[PER];
-    face_load(e, fr);
-    face_store(0, fr);
+    if (warp == 0) issue(e, 0);
+    meta(e, 0);
+    double fv[3];
+    face_load(e, fv);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      if (tid + r * THREADS < NFACE) sface[tid + r * THREADS] = fv[r];
+    pw_load(e, cur);
   }
   __syncthreads();
   const double aG0 = sG[gq * 8 + tig], aG1 = sG[gq * 8 + 4 + tig];
@@ -455,89 +521,98 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     const int s = it & 1;
     const unsigned parity = (it >> 1) & 1;
     const long long en = e + gridDim.x;
-    if (tid == 0 && en < P.Ne) issue(en, s ^ 1);
-    double fr[PER];
-    face_load(en < P.Ne ? en : -1, fr);
+    const bool has_next = en < P.Ne;
+    if (warp == 0 && has_next) issue(en, s ^ 1);
+    if (has_next) meta(en, s ^ 1);
+    double fnext[3];
+    face_load(has_next ? en : -1, fnext);
+    PW nxt;
+    pw_load(has_next ? en : -1, nxt);
     if (!wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
     __syncthreads();
     if (abort_flag) {
-      if (tid == 0 && en < P.Ne) wait_phase(&bar[s ^ 1], ((it + 1) >> 1) & 1, nullptr);
+      if (warp == 0 && lane == 0 && has_next) wait_phase(&bar[s ^ 1], ((it + 1) >> 1) & 1, nullptr);
       return;
     }
     const double* d = stg + s * K2_STAGE;
-    const double* sF = d;
-    const double* sJa = d + 3 * N3;
+    const double* sF = d;           // 3 fields
+    const double* sJa = d + 3 * FS;  // 9 fields
+    const double* sfc = sface + s * NFACE;
+    const int mask = emeta[s][0];
+    const int bnd = emeta[s][1];
 #pragma unroll 1
     for (int al = 0; al < 3; ++al) {
-      double c[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-      const double* m0 = sJa + (al * 3 + 0) * N3;
-      const double* m1 = sJa + (al * 3 + 1) * N3;
-      const double* m2 = sJa + (al * 3 + 2) * N3;
+      const double* m0 = sJa + (al * 3 + 0) * FS;
+      const double* m1 = sJa + (al * 3 + 1) * FS;
+      const double* m2 = sJa + (al * 3 + 2) * FS;
+      double cx[2] = {0, 0}, cy[2] = {0, 0};
 #pragma unroll
       for (int kc = 0; kc < 2; ++kc) {
-        const int nd = pnode(al, 4 * kc + tig, 8 * warp + gq);
-        const double f0 = sF[nd], f1 = sF[N3 + nd], f2 = sF[2 * N3 + nd];
-        const double ft = m0[nd] * f0 + m1[nd] * f1 + m2[nd] * f2;
+        const int nd = bnode(al, wt8, kc, gq, tig);
         const double a = kc ? aG1 : aG0;
-        dmma(c[0][0], c[0][1], a, ft);
-        dmma(c[1][0], c[1][1], a, f0);
-        dmma(c[2][0], c[2][1], a, f1);
-        dmma(c[3][0], c[3][1], a, f2);
+        if (half == 0) {
+          // contravariant flux Ja^al . F and F_0
+          const double f0 = sF[nd];
+          const double ft = m0[nd] * f0 + m1[nd] * sF[FS + nd] + m2[nd] * sF[2 * FS + nd];
+          dmma(cx[0], cx[1], a, ft);
+          dmma(cy[0], cy[1], a, f0);
+        } else {
+          dmma(cx[0], cx[1], a, sF[FS + nd]);
+          dmma(cy[0], cy[1], a, sF[2 * FS + nd]);
+        }
       }
+      const int face = gq == 0 ? 2 * al : (gq == 7 ? 2 * al + 1 : -1);
+      const bool sat = half == 0 && face >= 0 && ((mask >> face) & 1);
+      const double nh = (face & 1) ? 1.0 : -1.0;
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
-        const int no = pnode(al, gq, 8 * warp + 2 * tig + b);
-        const double r = 0.5 * c[0][b] + (0.5 * m0[no] * c[1][b] + 0.5 * m1[no] * c[2][b] + 0.5 * m2[no] * c[3][b]);
-        if (al == 0) sdiv[no] = r;
-        else sdiv[no] += r;
+        const int no = onode(al, wt8, b, gq, tig);
+        double r;
+        if (half == 0) {
+          const double mo0 = m0[no];
+          r = 0.5 * cx[b] + 0.5 * mo0 * cy[b];
+          if (sat) {
+            const int pq = opq(al, wt8, b, tig);
+            const double jmp = mo0 * (sfc[(face * 3 + 0) * N2 + pq] - sF[no]) +
+                               m1[no] * (sfc[(face * 3 + 1) * N2 + pq] - sF[FS + no]) +
+                               m2[no] * (sfc[(face * 3 + 2) * N2 + pq] - sF[2 * FS + no]);
+            r += nh * jmp * inv2H;
+          }
+        } else {
+          r = 0.5 * m1[no] * cx[b] + 0.5 * m2[no] * cy[b];
+        }
+        double* acc_s = sdiv + half * FS;
+        if (al == 0) acc_s[no] = r;
+        else acc_s[no] += r;
       }
       __syncthreads();
     }
-    const double* sface_s = sface + s * NF;
-#pragma unroll 1
-    for (int r = 0; r < 2; ++r) {
-      const int t = tid + r * THREADS;
-      const int i = t & 7, j = (t >> 3) & 7, k = t >> 6;
-      const long long n = e * N3 + t;
-      double dv = sdiv[t];
-      const int idx3[3] = {i, j, k};
-#pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        const int ax = f >> 1;
-        if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
-        if (P.bdry[f + 6 * e] != 0 || P.nbr[f + 6 * e] < 0) continue;
-        const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
-        const double nh = (f & 1) ? 1.0 : -1.0;
-        double sacc = 0.0;
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc)
-          sacc += sJa[(ax * 3 + cc) * N3 + t] * (sface_s[(f * 3 + cc) * N2 + p + 8 * q] - sF[cc * N3 + t]);
-        dv += nh * sacc / (2.0 * Hend);
-      }
-      dv *= d[12 * N3 + t];
-      if (P.bc_on) {
+    {
+      const long long n = e * N3 + tid;
+      double dv = (sdiv[tpad] + sdiv[FS + tpad]) * cur.invJ;
+      if (bnd && P.bc_on) {
+        const int idx3[3] = {ti, tj, tk};
         for (int f = 0; f < 6; ++f) {
           if (P.bdry[f + 6 * e] == 0) continue;
           const int ax = f >> 1;
           if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
-          const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
+          const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
           dv += P.bbuf[(long long)P.bslot[f + 6 * e] * N2 + p + 8 * q];
         }
       }
       if (P.epi) {
         const double dt = P.dt;
         if (P.stage == 0) {
-          const double yv = d[13 * N3 + t];
-          P.out[n] = yv + (0.5 * dt) * dv;
-          P.acc[n] = yv + (dt / 6.0) * dv;
+          P.out[n] = cur.y + (0.5 * dt) * dv;
+          P.acc[n] = cur.y + (dt / 6.0) * dv;
         } else if (P.stage == 1) {
-          P.out[n] = d[13 * N3 + t] + (0.5 * dt) * dv;
-          P.acc[n] = d[14 * N3 + t] + (dt / 3.0) * dv;
+          P.out[n] = cur.y + (0.5 * dt) * dv;
+          P.acc[n] = cur.acc + (dt / 3.0) * dv;
         } else if (P.stage == 2) {
-          P.out[n] = d[13 * N3 + t] + dt * dv;
-          P.acc[n] = d[14 * N3 + t] + (dt / 3.0) * dv;
+          P.out[n] = cur.y + dt * dv;
+          P.acc[n] = cur.acc + (dt / 3.0) * dv;
         } else {
-          const double v = d[14 * N3 + t] + (dt / 6.0) * dv;
+          const double v = cur.acc + (dt / 6.0) * dv;
           P.y[n] = v;
           if (P.flag && !isfinite(v)) atomicOr(P.flag, 1u);
         }
@@ -545,7 +620,12 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
         P.Pidot[n] = dv;
       }
     }
-    face_store(s ^ 1, fr);
+    if (has_next) {
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        if (tid + r * THREADS < NFACE) sface[(s ^ 1) * NFACE + tid + r * THREADS] = fnext[r];
+    }
+    cur = nxt;
     __syncthreads();
   }
 }
