@@ -8,6 +8,7 @@
 #include "wt_common.cuh"
 #include "../../include/wavetoy_b200.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -216,6 +217,10 @@ int derive_geometry(wt_mesh* mh) {
   cudaStream_t s = mh->ctx->stream;
   WT_TRY(lrc(mh->ctx, wt::launch_geom_derived(m, s), "geometry"));
   WT_TRY(lrc(mh->ctx, wt::launch_metric(m, s), "metric terms"));
+  if (m.N == 8 && m.precision == 0) {  // padded element blocks for the pipelined n = 8 kernels
+    WT_TRY(dalloc(mh->ctx, &m.Ja_n8, 9 * (size_t)wt::n8_padded_field_size(m.Ne) * sizeof(double), &mh->owned));
+    WT_TRY(lrc(mh->ctx, wt::launch_pad_metric_n8(m, s), "padded metric terms"));
+  }
   if (m.precision == 0) {
     // Ja_r aliases Ja; still need sdiag
   }
@@ -240,7 +245,8 @@ int ensure(wt_ws* ws, void** p, size_t bytes) {
 int ws_buffers(wt_ws* ws) {
   const wt::DevMesh& m = ws->mesh->m;
   const size_t rs = rsize(m.precision);
-  const size_t nb = (size_t)m.nn * rs;
+  size_t nb = (size_t)m.nn * rs;
+  if (m.N == 8) nb = std::max(nb, (size_t)wt::n8_padded_field_size(m.Ne) * rs);  // padded flux layout
   WT_TRY(ensure(ws, &ws->F, 3 * nb));
   WT_TRY(ensure(ws, &ws->bbuf, (size_t)(m.nbf > 0 ? m.nbf : 1) * m.N * m.N * rs));
   return 0;
@@ -307,9 +313,11 @@ int rhs_curved_impl(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi
                     void* Pid, double eps_ko, const wt::ConsBC& bc, int use_metric) {
   const wt::DevMesh& m = ws->mesh->m;
   wt::RKStage rk;
+  const bool n8 = wt::cons_n8_path(m, coef->c, use_metric, bc, rk, rk, {Phi, Pi, ws->F, Phid, Pid});
   WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, Phi, Pi, ws->F, Phid, ws->bbuf, nullptr, use_metric, bc, rk,
-                                     ctx->stream), "rhs K1"));
-  WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, Pid, ws->bbuf, use_metric, bc, rk, nullptr, ctx->stream), "rhs K2"));
+                                     ctx->stream, n8), "rhs K1"));
+  WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, Pid, ws->bbuf, use_metric, bc, rk, nullptr, ctx->stream, n8),
+             "rhs K2"));
   ctx->launches += 2;
   if (eps_ko != 0.0) {
     const double koT = eps_ko * ws->inv_mu5;
@@ -888,12 +896,13 @@ static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* P
     rkP.nonfinite = rkQ.nonfinite = st == 3 ? ctx->d_flag : nullptr;
     if (eps_ko == 0.0) {
       rkP.on = rkQ.on = 1;
+      const bool n8 = wt::cons_n8_path(m, coef->c, use_metric, b, rkP, rkQ, {inP, inQ, ws->F});
       prof_mark(ctx, 0);
       WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, inP, inQ, ws->F, nullptr, ws->bbuf, nullptr, use_metric, b, rkP,
-                                         s), "rk4 K1"));
+                                         s, n8), "rk4 K1"));
       prof_mark(ctx, 0);
       prof_mark(ctx, 1);
-      WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, nullptr, ws->bbuf, use_metric, b, rkQ, rkQ.nonfinite, s),
+      WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, nullptr, ws->bbuf, use_metric, b, rkQ, rkQ.nonfinite, s, n8),
                  "rk4 K2"));
       prof_mark(ctx, 1);
       ctx->launches += 2;

@@ -17,6 +17,7 @@
 #include <cstdint>
 #include <string>
 #include <vector>
+#include <initializer_list>
 
 #define WT_MAXN 8
 
@@ -61,6 +62,7 @@ struct DevMesh {
   void* Ja_r = nullptr;      // 9 fields
   void* invdetJ_r = nullptr;
   void* sdiag = nullptr;     // [3e + d] element-constant axis scale invjac[d,d] at node 0
+  double* Ja_n8 = nullptr;   // n = 8 FP64: metric terms in padded element blocks (544 per element)
   // boundary faces: slot per (f,e) with bdry != 0, -1 otherwise
   int32_t* bslot = nullptr;
   int nbf = 0;
@@ -156,16 +158,22 @@ struct RKStage {
 // K1: gradient, flux F, Phidot (+ affine/curv BC increments), optional RK epilogue for Phi.
 int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
                    void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
-                   cudaStream_t s);
+                   cudaStream_t s, bool n8 = false);
 // K2: divergence of F (+ boundary increments), optional RK epilogue for Pi.
 int launch_cons_k2(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
-                   const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s);
+                   const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s, bool n8 = false);
 int launch_apply_D(const DevMesh& m, const void* u, void* out, int d, cudaStream_t s);
 // n = 8 FP64 curvilinear path: persistent, TMA-pipelined, FP64 tensor cores (wt_cons_n8.cu)
 int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
                       void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s);
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
                       const RKStage& rk, unsigned* flag, cudaStream_t s);
+int launch_pad_metric_n8(DevMesh& m, cudaStream_t s);
+long long n8_padded_field_size(long long Ne);
+// True when an RHS evaluation takes the n = 8 pipelined path (both kernels take
+// the same path: K1 then writes F in the padded layout K2 reads).
+bool cons_n8_path(const DevMesh& m, const DevCoef& c, int use_metric, const ConsBC& bc, const RKStage& rkP,
+                  const RKStage& rkQ, std::initializer_list<const void*> ptrs);
 int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s);
 int launch_div3d(const DevMesh& m, const void* F, void* out, cudaStream_t s);
 

@@ -596,22 +596,22 @@ static inline bool a16(const void* p) { return p == nullptr || ((uintptr_t)p & 1
 
 // The pipelined n = 8 kernels stage element blocks with bulk copies, which
 // need 16-byte aligned global addresses; anything else takes the generic path.
-static bool n8_path(const DevMesh& m, const DevCoef* c, int use_metric, const ConsBC& bc, const RKStage& rk,
-                    std::initializer_list<const void*> ptrs) {
-  if (m.N != 8 || m.precision != 0 || !use_metric) return false;
-  if (c && c->c10 == nullptr) return false;
+bool cons_n8_path(const DevMesh& m, const DevCoef& c, int use_metric, const ConsBC& bc, const RKStage& rkP,
+                  const RKStage& rkQ, std::initializer_list<const void*> ptrs) {
+  if (m.N != 8 || m.precision != 0 || !use_metric || m.Ja_n8 == nullptr) return false;
+  if (c.c10 == nullptr) return false;
   if (bc.on && !bc.curv) return false;
-  if (!a16(rk.y) || !a16(rk.acc) || !a16(rk.out)) return false;
+  for (const RKStage* rk : {&rkP, &rkQ})
+    if (!a16(rk->y) || !a16(rk->acc) || !a16(rk->out)) return false;
   for (const void* p : ptrs)
     if (!a16(p)) return false;
-  return a16(m.Ja_r) && a16(m.invdetJ_r);
+  return a16(c.c10) && a16(m.invdetJ_r);
 }
 
 int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
                    void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
-                   cudaStream_t s) {
-  if (grad_out == nullptr && n8_path(m, &c, use_metric, bc, rk, {Phi, Pi, c.c10, F, Phidot}))
-    return launch_cons_k1_n8(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, m.errflag, s);
+                   cudaStream_t s, bool n8) {
+  if (n8 && grad_out == nullptr) return launch_cons_k1_n8(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, m.errflag, s);
   if (m.precision == 0) {
     WT_DISPATCH_N(m.N, (k1_dispatch<NN, double>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, use_metric, bc, rk, s)));
   } else {
@@ -620,9 +620,8 @@ int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const vo
 }
 
 int launch_cons_k2(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
-                   const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s) {
-  if (n8_path(m, nullptr, use_metric, bc, rk, {F, Pidot}))
-    return launch_cons_k2_n8(m, F, Pidot, bbuf, bc, rk, m.errflag, s);
+                   const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s, bool n8) {
+  if (n8) return launch_cons_k2_n8(m, F, Pidot, bbuf, bc, rk, m.errflag, s);
   if (m.precision == 0) {
     WT_DISPATCH_N(m.N, (k2_dispatch<NN, double>(m, F, Pidot, bbuf, use_metric, bc, rk, nonfinite, s)));
   } else {

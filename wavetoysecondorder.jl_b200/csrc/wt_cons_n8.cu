@@ -73,6 +73,8 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 }
 
 __device__ __forceinline__ int pad(int i, int j, int k) { return i + 8 * j + PS * k; }
+// padded index -> unpadded node index (i + 8 j + 64 k)
+__device__ __forceinline__ int unpad(int d) { return d - (PS - 64) * (d / PS); }
 
 // Per-lane operand / output node offsets (padded) for axis al, tile w:
 //   B operand: position p = 4 kc + tig along al, pencil slot g;
@@ -134,9 +136,11 @@ struct K1N8 {
   unsigned* flag;
 };
 
-// K1 staged fields: 0 Phi, 1..9 Ja.  Register prefetch: c10 (10), Pi, invJ, y, acc.
+// K1 staged fields: Phi (unpadded, 512) and Ja (9 padded fields, one 4352-byte
+// block each from the padded global copy).  Register prefetch: c10 (10), Pi,
+// invJ, y, acc.
 constexpr int K1_NF = 10;
-constexpr size_t K1_STAGE = (size_t)K1_NF * n8::FS;
+constexpr size_t K1_STAGE = (size_t)n8::N3 + 9 * (size_t)n8::FS;
 constexpr size_t K1_SMEM = (2 * K1_STAGE + 3 * n8::FS + 2 * 6 * n8::N2 + n8::N2) * sizeof(double) + 64;
 
 __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
@@ -155,7 +159,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   const double inv2H = 1.0 / (2.0 * P.H[0]);
   const bool need_y = P.epi && (P.stage == 1 || P.stage == 2);
   const bool need_acc = P.epi && P.stage >= 1;
-  const unsigned tx_bytes = K1_NF * 8u * PLANE_BYTES;
+  const unsigned tx_bytes = N3 * 8u + 9u * FS * 8u;
   // node-phase coordinates of this thread
   const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
   const int tpad = pad(ti, tj, tk);
@@ -169,7 +173,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   }
   __syncthreads();
 
-  // warp 0 stages element e into stage s: 80 plane copies, 2-3 per lane
+  // warp 0 stages element e into stage s: 10 whole-block copies
   auto issue = [&](long long e, int s) {
     if (lane == 0) {
       fence_proxy_async();
@@ -177,12 +181,9 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     }
     __syncwarp();
     double* d = stg + s * K1_STAGE;
-    const long long o = e * N3;
-    for (int c = lane; c < K1_NF * 8; c += 32) {
-      const int f = c >> 3, k = c & 7;
-      const double* src = (f == 0 ? P.Phi + o : P.Ja + (long long)(f - 1) * nn + o) + k * N2;
-      bulk_g2s(d + f * FS + k * PS, src, PLANE_BYTES, &bar[s]);
-    }
+    if (lane == 0) bulk_g2s(d, P.Phi + e * N3, N3 * 8u, &bar[s]);
+    else if (lane <= 9)
+      bulk_g2s(d + N3 + (lane - 1) * FS, P.Ja + ((long long)(lane - 1) * P.Ne + e) * FS, FS * 8u, &bar[s]);
   };
   // per-element metadata: interior-face mask (SAT faces) and boundary flag
   auto meta = [&](long long e, int s) {
@@ -254,12 +255,12 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
       return;
     }
     const double* d = stg + s * K1_STAGE;
-    const double* sPhi = d;
-    const double* sJa = d + FS;  // 9 fields, index (al*3 + c)
+    const double* sPhi = d;      // unpadded
+    const double* sJa = d + N3;  // 9 padded fields, index (al*3 + c)
     const double* sfc = sface + s * 6 * N2;
     const int mask = emeta[s][0];
     const int bnd = emeta[s][1];
-    // ---- tensor-core contractions + SAT, one axis per phase ----
+    // ---- tensor-core contractions, one axis per phase ----
 #pragma unroll 1
     for (int al = 0; al < 3; ++al) {
       // half 0: component 0; half 1: components 1 and 2
@@ -271,30 +272,19 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
 #pragma unroll
       for (int kc = 0; kc < 2; ++kc) {
         const int nd = bnode(al, wt8, kc, gq, tig);
-        const double u = sPhi[nd];
+        const double u = sPhi[unpad(nd)];
         const double a = kc ? aG1 : aG0;
         dmma(cu[0], cu[1], a, u);
         dmma(ca[0], ca[1], a, mA[nd] * u);
         if (ncomp == 2) dmma(cb[0], cb[1], a, mB[nd] * u);
       }
-      const int face = gq == 0 ? 2 * al : (gq == 7 ? 2 * al + 1 : -1);
-      const bool sat = face >= 0 && ((mask >> face) & 1);
-      const double nh = (face & 1) ? 1.0 : -1.0;
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         const int no = onode(al, wt8, b, gq, tig);
         const double mo_a = mA[no];
         double ra = 0.5 * ca[b] + 0.5 * mo_a * cu[b];
-        double rb = 0.0, mo_b = 0.0;
-        if (ncomp == 2) {
-          mo_b = mB[no];
-          rb = 0.5 * cb[b] + 0.5 * mo_b * cu[b];
-        }
-        if (sat) {
-          const double jump = sfc[face * N2 + opq(al, wt8, b, tig)] - sPhi[no];
-          ra += nh * mo_a * jump * inv2H;
-          if (ncomp == 2) rb += nh * mo_b * jump * inv2H;
-        }
+        double rb = 0.0;
+        if (ncomp == 2) rb = 0.5 * cb[b] + 0.5 * mB[no] * cu[b];
         double* ga = sg + c0 * FS;
         if (al == 0) {
           ga[no] = ra;
@@ -309,8 +299,23 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     // ---- node phase: one node per thread ----
     {
       const long long n = e * N3 + tid;
-      const double u = sPhi[tpad];
-      double g0 = sg[tpad] * cur.invJ, g1 = sg[FS + tpad] * cur.invJ, g2 = sg[2 * FS + tpad] * cur.invJ;
+      const double u = sPhi[tid];
+      double g0 = sg[tpad], g1 = sg[FS + tpad], g2 = sg[2 * FS + tpad];
+      if (mask) {  // centred-flux SAT on interior faces through this node (after the volume terms)
+        const int idx3[3] = {ti, tj, tk};
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+          const int ax = f >> 1;
+          if (!((mask >> f) & 1) || idx3[ax] != ((f & 1) ? 7 : 0)) continue;
+          const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
+          const double jump = sfc[f * N2 + p + 8 * q] - u;
+          const double nh = (f & 1) ? 1.0 : -1.0;
+          g0 += nh * sJa[(ax * 3 + 0) * FS + tpad] * jump * inv2H;
+          g1 += nh * sJa[(ax * 3 + 1) * FS + tpad] * jump * inv2H;
+          g2 += nh * sJa[(ax * 3 + 2) * FS + tpad] * jump * inv2H;
+        }
+      }
+      g0 *= cur.invJ; g1 *= cur.invJ; g2 *= cur.invJ;
       const double a = cur.c[0];
       const double b0 = cur.c[1], b1 = cur.c[2], b2 = cur.c[3];
       const double K0 = cur.c[4], K1v = cur.c[5], K2 = cur.c[6], K3 = cur.c[7], K4 = cur.c[8], K5 = cur.c[9];
@@ -358,9 +363,12 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
           P.bbuf[(long long)slot * N2 + p + 8 * q] = dP;
         }
       }
-      P.F[n] = F0;
-      P.F[nn + n] = F1;
-      P.F[2 * nn + n] = F2;
+      {  // flux in the padded element-block layout read by K2
+        const long long fo = e * FS + tpad, fstr = P.Ne * FS;
+        P.F[fo] = F0;
+        P.F[fstr + fo] = F1;
+        P.F[2 * fstr + fo] = F2;
+      }
       if (P.epi) {
         const double dt = P.dt;
         if (P.stage == 0) {
@@ -433,7 +441,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   const double inv2H = 1.0 / (2.0 * P.H[0]);
   const bool need_y = P.epi && P.stage <= 2;
   const bool need_acc = P.epi && P.stage >= 1;
-  const unsigned tx_bytes = K2_NF * 8u * PLANE_BYTES;
+  const unsigned tx_bytes = K2_NF * FS * 8u;
   const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
   const int tpad = pad(ti, tj, tk);
   constexpr int NFACE = 6 * 3 * N2;  // 1152
@@ -454,11 +462,10 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     }
     __syncwarp();
     double* d = stg + s * K2_STAGE;
-    const long long o = e * N3;
-    for (int c = lane; c < K2_NF * 8; c += 32) {
-      const int f = c >> 3, k = c & 7;
-      const double* src = (f == 0 ? P.F0 : f == 1 ? P.F1 : f == 2 ? P.F2 : P.Ja + (long long)(f - 3) * nn) + o + k * N2;
-      bulk_g2s(d + f * FS + k * PS, src, PLANE_BYTES, &bar[s]);
+    if (lane < K2_NF) {
+      const double* src = lane < 3 ? (lane == 0 ? P.F0 : lane == 1 ? P.F1 : P.F2) + e * FS
+                                   : P.Ja + ((long long)(lane - 3) * P.Ne + e) * FS;
+      bulk_g2s(d + lane * FS, src, FS * 8u, &bar[s]);
     }
   };
   auto meta = [&](long long e, int s) {
@@ -485,7 +492,8 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
         if (en >= 0 && P.bdry[f + 6 * e] == 0) {
           const int fn = P.nbrf[f + 6 * e];
           const double* Fc = c == 0 ? P.F0 : c == 1 ? P.F1 : P.F2;
-          v = Fc[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N)];
+          const int fnode = face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N);
+          v = Fc[(long long)en * FS + pad(fnode & 7, (fnode >> 3) & 7, fnode >> 6)];
         }
       }
       fv[r] = v;
@@ -561,23 +569,12 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
           dmma(cy[0], cy[1], a, sF[2 * FS + nd]);
         }
       }
-      const int face = gq == 0 ? 2 * al : (gq == 7 ? 2 * al + 1 : -1);
-      const bool sat = half == 0 && face >= 0 && ((mask >> face) & 1);
-      const double nh = (face & 1) ? 1.0 : -1.0;
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         const int no = onode(al, wt8, b, gq, tig);
         double r;
         if (half == 0) {
-          const double mo0 = m0[no];
-          r = 0.5 * cx[b] + 0.5 * mo0 * cy[b];
-          if (sat) {
-            const int pq = opq(al, wt8, b, tig);
-            const double jmp = mo0 * (sfc[(face * 3 + 0) * N2 + pq] - sF[no]) +
-                               m1[no] * (sfc[(face * 3 + 1) * N2 + pq] - sF[FS + no]) +
-                               m2[no] * (sfc[(face * 3 + 2) * N2 + pq] - sF[2 * FS + no]);
-            r += nh * jmp * inv2H;
-          }
+          r = 0.5 * cx[b] + 0.5 * m0[no] * cy[b];
         } else {
           r = 0.5 * m1[no] * cx[b] + 0.5 * m2[no] * cy[b];
         }
@@ -589,7 +586,23 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     }
     {
       const long long n = e * N3 + tid;
-      double dv = (sdiv[tpad] + sdiv[FS + tpad]) * cur.invJ;
+      double dv = sdiv[tpad] + sdiv[FS + tpad];
+      if (mask) {  // centred-flux SAT on interior faces through this node (after the volume terms)
+        const int idx3[3] = {ti, tj, tk};
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+          const int ax = f >> 1;
+          if (!((mask >> f) & 1) || idx3[ax] != ((f & 1) ? 7 : 0)) continue;
+          const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
+          const double nh = (f & 1) ? 1.0 : -1.0;
+          double sacc = 0.0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            sacc += sJa[(ax * 3 + c) * FS + tpad] * (sfc[(f * 3 + c) * N2 + p + 8 * q] - sF[c * FS + tpad]);
+          dv += nh * sacc * inv2H;
+        }
+      }
+      dv *= cur.invJ;
       if (bnd && P.bc_on) {
         const int idx3[3] = {ti, tj, tk};
         for (int f = 0; f < 6; ++f) {
@@ -630,6 +643,25 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   }
 }
 
+// padded element-block copy of the nine metric-term fields for the n = 8 path
+__global__ void k_pad_fields(long long Ne, int nf, const double* __restrict__ src, double* __restrict__ dst) {
+  const long long total = (long long)nf * Ne * n8::N3;
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
+    const long long f = x / (Ne * n8::N3);
+    const long long r = x - f * Ne * n8::N3;
+    const long long e = r / n8::N3;
+    const int t = (int)(r - e * n8::N3);
+    dst[(f * Ne + e) * n8::FS + n8::pad(t & 7, (t >> 3) & 7, t >> 6)] = src[x];
+  }
+}
+
+int launch_pad_metric_n8(DevMesh& m, cudaStream_t s) {
+  k_pad_fields<<<4096, 256, 0, s>>>(m.Ne, 9, m.Ja, m.Ja_n8);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+long long n8_padded_field_size(long long Ne) { return Ne * n8::FS; }
+
 static int sm_count() {
   static int n = 0;
   if (!n) {
@@ -646,7 +678,7 @@ int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const
   K1N8 P;
   P.Ne = m.Ne; P.nn = m.nn;
   P.Phi = (const double*)Phi; P.Pi = (const double*)Pi; P.c10 = (const double*)c.c10;
-  P.Ja = (const double*)m.Ja_r; P.invdetJ = (const double*)m.invdetJ_r;
+  P.Ja = (const double*)m.Ja_n8; P.invdetJ = (const double*)m.invdetJ_r;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
   P.F = (double*)F; P.Phidot = (double*)Phidot; P.bbuf = (double*)bbuf;
   P.bc_on = bc.on; P.exc_tag = bc.exc_tag; P.nbf = m.nbf; P.kind = bc.kinds[0]; P.sigma = bc.sigma;
@@ -669,8 +701,8 @@ int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* 
                       const RKStage& rk, unsigned* flag, cudaStream_t s) {
   K2N8 P;
   P.Ne = m.Ne; P.nn = m.nn;
-  P.F0 = (const double*)F; P.F1 = (const double*)F + m.nn; P.F2 = (const double*)F + 2 * m.nn;
-  P.Ja = (const double*)m.Ja_r; P.invdetJ = (const double*)m.invdetJ_r;
+  P.F0 = (const double*)F; P.F1 = (const double*)F + m.Ne * n8::FS; P.F2 = (const double*)F + 2 * m.Ne * n8::FS;
+  P.Ja = (const double*)m.Ja_n8; P.invdetJ = (const double*)m.invdetJ_r;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
   P.bbuf = (const double*)bbuf; P.bc_on = bc.on;
   P.Pidot = (double*)Pidot;
