@@ -75,6 +75,13 @@ int wt_ctx_nonfinite(wt_ctx* ctx, int* flag);
 int wt_ctx_profile(wt_ctx* ctx, int enable);
 int wt_ctx_profile_read(wt_ctx* ctx, double ms[2], long long count[2]);
 
+/* ---- reference element ----------------------------------------------------- */
+/* HexSBPSAT.make_element(T, N) + make_operators(elem) (src/evolve.jl:1189):
+ * GLL nodes x and SBP norm H (diagonal) on [0,1] and the differentiation
+ * matrix G[i*N + p], with H G + (H G)^T = diag(-1,0,...,0,1) (README.md:14-19).
+ * Host only; needs no device.  N in 2..8. */
+int wt_gll_operators(int N, double* x, double* H, double* G);
+
 /* ---- mesh + geometry ------------------------------------------------------ */
 /* Analytic hex builder.  Replaces HexMeshes.make_uniform_hex(T, Mx, My, Mz,
  * x0, x1; periodic) / make_warped_uniform_hex(T, Mx, My, Mz, x0, x1, A;

@@ -52,67 +52,69 @@ struct Ops {
   std::vector<double> x, H, G;  // G[i*N + p] = d/dx of Lagrange basis p at node i
 };
 
-void legendre_q(int p, double x, double& q, double& dq, double& Lp) {
+void legendre_q(int p, long double x, long double& q, long double& dq, long double& Lp) {
   // q(x) = L_{p+1}(x) - L_{p-1}(x), derivative dq, and L_p(x).
-  double L[64], dL[64];
-  L[0] = 1.0; dL[0] = 0.0;
-  L[1] = x; dL[1] = 1.0;
+  long double L[64], dL[64];
+  L[0] = 1.0L; dL[0] = 0.0L;
+  L[1] = x; dL[1] = 1.0L;
   for (int k = 2; k <= p + 1; ++k) {
-    L[k] = ((2.0 * k - 1.0) * x * L[k - 1] - (k - 1.0) * L[k - 2]) / k;
-    dL[k] = dL[k - 2] + (2.0 * k - 1.0) * L[k - 1];
+    L[k] = ((2.0L * k - 1.0L) * x * L[k - 1] - (k - 1.0L) * L[k - 2]) / k;
+    dL[k] = dL[k - 2] + (2.0L * k - 1.0L) * L[k - 1];
   }
   q = L[p + 1] - L[p - 1];
   dq = dL[p + 1] - dL[p - 1];
   Lp = L[p];
 }
 
+// Computed in extended precision (x87 long double) and rounded once to
+// double, so the operators are correctly rounded (to within the extended
+// format's own round-off) independently of the algorithm.
 Ops make_ops(int N) {
   Ops o; o.N = N;
   int p = N - 1;
-  std::vector<double> xs(N), ws(N);
-  xs[0] = -1.0; xs[p] = 1.0;
-  double Lp;
-  {
-    double q, dq; legendre_q(p, -1.0, q, dq, Lp);
-    ws[0] = ws[p] = 2.0 / (p * (p + 1.0));
-  }
+  std::vector<long double> xs(N), ws(N);
+  xs[0] = -1.0L; xs[p] = 1.0L;
+  long double Lp;
+  ws[0] = ws[p] = 2.0L / (p * (p + 1.0L));
   for (int j = 1; j < N / 2; ++j) {
     // initial guess: Chebyshev-Gauss-Lobatto node
-    double x = -std::cos(M_PI * j / p);
+    long double x = -cosl(3.14159265358979323846264338327950288L * j / p);
     for (int it = 0; it < 100; ++it) {
-      double q, dq;
+      long double q, dq;
       legendre_q(p, x, q, dq, Lp);
-      double dx = -q / dq;
+      long double dx = -q / dq;
       x += dx;
-      if (std::fabs(dx) <= 1e-16 * std::max(1.0, std::fabs(x))) break;
+      if (fabsl(dx) <= 1e-19L * (1.0L + fabsl(x))) break;
     }
-    double q, dq; legendre_q(p, x, q, dq, Lp);
+    long double q, dq; legendre_q(p, x, q, dq, Lp);
     xs[j] = x; xs[p - j] = -x;
-    ws[j] = ws[p - j] = 2.0 / (p * (p + 1.0) * Lp * Lp);
+    ws[j] = ws[p - j] = 2.0L / (p * (p + 1.0L) * Lp * Lp);
   }
   if (N % 2 == 1) {  // centre node
-    int c = N / 2; double q, dq; legendre_q(p, 0.0, q, dq, Lp);
-    xs[c] = 0.0; ws[c] = 2.0 / (p * (p + 1.0) * Lp * Lp);
+    int c = N / 2; long double q, dq; legendre_q(p, 0.0L, q, dq, Lp);
+    xs[c] = 0.0L; ws[c] = 2.0L / (p * (p + 1.0L) * Lp * Lp);
   }
   // barycentric weights
-  std::vector<double> lam(N, 1.0);
+  std::vector<long double> lam(N, 1.0L);
   for (int j = 0; j < N; ++j)
     for (int k = 0; k < N; ++k)
       if (k != j) lam[j] /= (xs[j] - xs[k]);
-  std::vector<double> D(N * N, 0.0);
+  std::vector<long double> D(N * N, 0.0L);
   for (int i = 0; i < N; ++i) {
-    double s = 0.0;
+    long double sacc = 0.0L;
     for (int j = 0; j < N; ++j) {
       if (j == i) continue;
       D[i * N + j] = (lam[j] / lam[i]) / (xs[i] - xs[j]);
-      s += D[i * N + j];
+      sacc += D[i * N + j];
     }
-    D[i * N + i] = -s;
+    (void)sacc;
+    // exact GLL diagonal: 0 inside, -p(p+1)/4 and +p(p+1)/4 at the ends
+    D[i * N + i] = i == 0 ? -p * (p + 1.0L) / 4.0L : (i == p ? p * (p + 1.0L) / 4.0L : 0.0L);
   }
   o.x.resize(N); o.H.resize(N); o.G.resize(N * N);
-  for (int i = 0; i < N; ++i) { o.x[i] = 0.5 * (xs[i] + 1.0); o.H[i] = 0.5 * ws[i]; }
+  for (int i = 0; i < N; ++i) { o.x[i] = (double)(0.5L * (xs[i] + 1.0L)); o.H[i] = (double)(0.5L * ws[i]); }
   o.x[0] = 0.0; o.x[p] = 1.0;
-  for (int i = 0; i < N * N; ++i) o.G[i] = 2.0 * D[i];
+  for (int i = 0; i < N * N; ++i) o.G[i] = (double)(2.0L * D[i]);
   return o;
 }
 

@@ -32,3 +32,13 @@ def test_python_mirror_binds_every_symbol(wt):
     lib = wt.library()
     for n in declared_symbols():
         assert getattr(lib, n) is not None
+
+
+def test_library_operators_equal_oracle_bitwise(wt, O):
+    """The shipped GLL operators and the oracle's are computed independently in
+    extended precision and rounded once, so they agree bit for bit."""
+    import numpy as np
+    for N in range(2, 9):
+        x, H, G = wt.gll_operators(N)
+        xo, Ho, Go = O.gll_ops(N)
+        assert np.array_equal(x, xo) and np.array_equal(H, Ho) and np.array_equal(G, Go), N

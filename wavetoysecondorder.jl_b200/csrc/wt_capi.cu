@@ -435,6 +435,16 @@ int wt_ctx_nonfinite(wt_ctx* ctx, int* flag) {
   return 0;
 }
 
+// ---- reference element ------------------------------------------------------------
+int wt_gll_operators(int N, double* x, double* H, double* G) {
+  if (N < 2 || N > WT_MAXN || !x || !H || !G) return WT_EINVAL;
+  wt::HostOps o = wt::gll_operators(N);
+  std::memcpy(x, o.x.data(), N * sizeof(double));
+  std::memcpy(H, o.H.data(), N * sizeof(double));
+  std::memcpy(G, o.G.data(), N * N * sizeof(double));
+  return 0;
+}
+
 // ---- mesh -------------------------------------------------------------------
 int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* d, wt_mesh** out) {
   if (!ctx) return WT_EINVAL;

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
   const long long nn = P.nn;
-  const double inv2H = 1.0 / (2.0 * P.H[0]);
+  const double twoH = 2.0 * P.H[0];
   const bool need_y = P.epi && (P.stage == 1 || P.stage == 2);
   const bool need_acc = P.epi && P.stage >= 1;
   const unsigned tx_bytes = N3 * 8u + 9u * FS * 8u;
@@ -310,9 +310,9 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
           const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
           const double jump = sfc[f * N2 + p + 8 * q] - u;
           const double nh = (f & 1) ? 1.0 : -1.0;
-          g0 += nh * sJa[(ax * 3 + 0) * FS + tpad] * jump * inv2H;
-          g1 += nh * sJa[(ax * 3 + 1) * FS + tpad] * jump * inv2H;
-          g2 += nh * sJa[(ax * 3 + 2) * FS + tpad] * jump * inv2H;
+          g0 += nh * sJa[(ax * 3 + 0) * FS + tpad] * jump / twoH;
+          g1 += nh * sJa[(ax * 3 + 1) * FS + tpad] * jump / twoH;
+          g2 += nh * sJa[(ax * 3 + 2) * FS + tpad] * jump / twoH;
         }
       }
       g0 *= cur.invJ; g1 *= cur.invJ; g2 *= cur.invJ;
@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
   const long long nn = P.nn;
-  const double inv2H = 1.0 / (2.0 * P.H[0]);
+  const double twoH = 2.0 * P.H[0];
   const bool need_y = P.epi && P.stage <= 2;
   const bool need_acc = P.epi && P.stage >= 1;
   const unsigned tx_bytes = K2_NF * FS * 8u;
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
 #pragma unroll
           for (int c = 0; c < 3; ++c)
             sacc += sJa[(ax * 3 + c) * FS + tpad] * (sfc[(f * 3 + c) * N2 + p + 8 * q] - sF[c * FS + tpad]);
-          dv += nh * sacc * inv2H;
+          dv += nh * sacc / twoH;
         }
       }
       dv *= cur.invJ;

@@ -21,58 +21,63 @@ namespace wt {
 // recurrence for P_p, P'_p, P''_p; weights 2/(p(p+1) P_p^2); the
 // differentiation matrix is the closed form D_ij = P_p(x_i)/(P_p(x_j)(x_i-x_j))
 // with D_ii = -sum_{j!=i} D_ij (Canuto et al., "Spectral Methods", 2.3.2).
-static void legendre3(int p, double x, double& P, double& dP, double& d2P) {
-  double p0 = 1.0, p1 = x;
+static void legendre3(int p, long double x, long double& P, long double& dP, long double& d2P) {
+  long double p0 = 1.0L, p1 = x;
   if (p == 0) { P = 1; dP = 0; d2P = 0; return; }
   for (int k = 2; k <= p; ++k) {
-    double pk = ((2 * k - 1) * x * p1 - (k - 1) * p0) / k;
+    long double pk = ((2 * k - 1) * x * p1 - (k - 1) * p0) / k;
     p0 = p1; p1 = pk;
   }
   P = p1;
   // (1-x^2) P' = p (P_{p-1} - x P_p)
-  dP = p * (p0 - x * p1) / (1.0 - x * x);
+  dP = p * (p0 - x * p1) / (1.0L - x * x);
   // Legendre ODE: (1-x^2) P'' - 2x P' + p(p+1) P = 0
-  d2P = (2.0 * x * dP - p * (p + 1.0) * P) / (1.0 - x * x);
+  d2P = (2.0L * x * dP - p * (p + 1.0L) * P) / (1.0L - x * x);
 }
 
+// Evaluated in extended precision (long double) and rounded once to double,
+// so the operators are correctly rounded independently of the algorithm.
 HostOps gll_operators(int N) {
   HostOps o; o.N = N;
   const int p = N - 1;
-  std::vector<double> xs(N), ws(N), Pv(N);
-  xs[0] = -1.0; xs[p] = 1.0;
+  std::vector<long double> xs(N), ws(N), Pv(N);
+  xs[0] = -1.0L; xs[p] = 1.0L;
   for (int j = 1; j < p; ++j) {
     if (2 * j > p) break;
-    double x = -std::cos(M_PI * j / p);  // Chebyshev-Gauss-Lobatto start
-    if (2 * j == p) x = 0.0;
-    for (int it = 0; it < 60 && 2 * j != p; ++it) {
-      double P, dP, d2P;
+    long double x = -cosl(3.14159265358979323846264338327950288L * j / p);  // Chebyshev-Gauss-Lobatto start
+    if (2 * j == p) x = 0.0L;
+    for (int it = 0; it < 80 && 2 * j != p; ++it) {
+      long double P, dP, d2P;
       legendre3(p, x, P, dP, d2P);
-      double dx = dP / d2P;
+      long double dx = dP / d2P;
       x -= dx;
-      if (std::fabs(dx) < 1e-17) break;
+      if (fabsl(dx) < 1e-20L) break;
     }
     xs[j] = x; xs[p - j] = -x;
   }
   for (int j = 0; j < N; ++j) {
-    double P;
-    if (j == 0) P = (p % 2 == 0) ? 1.0 : -1.0;
-    else if (j == p) P = 1.0;
-    else { double dP, d2P; legendre3(p, xs[j], P, dP, d2P); }
+    long double P;
+    if (j == 0) P = (p % 2 == 0) ? 1.0L : -1.0L;
+    else if (j == p) P = 1.0L;
+    else { long double dP, d2P; legendre3(p, xs[j], P, dP, d2P); }
     Pv[j] = P;
-    ws[j] = 2.0 / (p * (p + 1.0) * P * P);
+    ws[j] = 2.0L / (p * (p + 1.0L) * P * P);
   }
   o.x.resize(N); o.H.resize(N); o.G.assign(N * N, 0.0);
   for (int i = 0; i < N; ++i) {
-    double s = 0.0;
+    long double sacc = 0.0L;
+    std::vector<long double> row(N, 0.0L);
     for (int j = 0; j < N; ++j) {
       if (i == j) continue;
-      double d = Pv[i] / (Pv[j] * (xs[i] - xs[j]));
-      o.G[i * N + j] = 2.0 * d;
-      s += d;
+      row[j] = Pv[i] / (Pv[j] * (xs[i] - xs[j]));
+      sacc += row[j];
     }
-    o.G[i * N + i] = -2.0 * s;
-    o.x[i] = 0.5 * (1.0 + xs[i]);
-    o.H[i] = 0.5 * ws[i];
+    (void)sacc;
+    // exact GLL diagonal: 0 inside, -p(p+1)/4 and +p(p+1)/4 at the ends
+    row[i] = i == 0 ? -p * (p + 1.0L) / 4.0L : (i == p ? p * (p + 1.0L) / 4.0L : 0.0L);
+    for (int j = 0; j < N; ++j) o.G[i * N + j] = (double)(2.0L * row[j]);
+    o.x[i] = (double)(0.5L * (1.0L + xs[i]));
+    o.H[i] = (double)(0.5L * ws[i]);
   }
   o.x[0] = 0.0; o.x[p] = 1.0;
   return o;

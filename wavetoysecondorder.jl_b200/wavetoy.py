@@ -93,6 +93,7 @@ def library():
         "wt_step_rk4_sipg": [vp, vp, vp, vp, d, i, C.POINTER(C.c_double * 6), d, d, d],
         "wt_evolve_curved_host": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i, vp],
         "wt_initial_data": [vp, vp, i, vp, i, d, vp, vp],
+        "wt_gll_operators": [i, vp, vp, vp],
         "wt_ctx_profile": [vp, i], "wt_ctx_profile_read": [vp, C.POINTER(d * 2), C.POINTER(ll * 2)],
     }
     for name, args in sig.items():
@@ -610,3 +611,13 @@ def gaussian_params(centres, amps, widths):
     for c, a, w in zip(centres, amps, widths):
         out += [float(c[0]), float(c[1]), float(c[2]), float(a), float(w)]
     return out
+
+
+def gll_operators(N: int):
+    """make_element + make_operators: GLL nodes x, SBP norm H and G (N x N) on [0,1]."""
+    import numpy as np
+    x = np.zeros(N); H = np.zeros(N); G = np.zeros(N * N)
+    rc = library().wt_gll_operators(int(N), x.ctypes.data, H.ctypes.data, G.ctypes.data)
+    if rc != 0:
+        raise WaveToyError(rc, f"wt_gll_operators(N={N})")
+    return x, H, G.reshape(N, N)
