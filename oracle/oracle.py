@@ -55,6 +55,8 @@ def lib():
         L.or_get.restype = i
         L.or_get.argtypes = [vp, C.c_char_p, vp]
         L.or_set_bdry.argtypes = [vp, vp]
+        L.or_set.restype = i
+        L.or_set.argtypes = [vp, C.c_char_p, vp]
         L.or_sample_background.argtypes = [vp, i, vp, vp]
         L.or_mu.restype = d
         L.or_mu.argtypes = [vp]
@@ -142,6 +144,10 @@ class OracleMesh:
         rc = lib().or_get(self.h, name.encode(), _p(out))
         assert rc == 0, name
         return out
+
+    def set_geometry(self, name, arr):
+        arr = np.ascontiguousarray(arr, dtype=np.float64)
+        assert lib().or_set(self.h, name.encode(), _p(arr)) == 0, name
 
     def set_bdry(self, bdry):
         bdry = np.ascontiguousarray(bdry, dtype=np.int32)

@@ -257,31 +257,45 @@ void build_mesh(Mesh& m, int N, int Mx, int My, int Mz, double x0, double x1, do
 // round-off because tensor-product derivatives commute.  Hd = H_ref*detJ is
 // the energy mass of the split-form operators, invdetJ = 1/detJ.
 void build_metric(Mesh& m) {
+  // Evaluated in extended precision (long double) and rounded once: the curl
+  // form cancels strongly (terms ~ h sum|G| for a result ~ h^2), and a plain
+  // double evaluation carries ~5e-12 relative error.
   const int N = m.N; const long Ne = m.Ne, nn = m.nn(); const long ne3 = (long)N * N * N;
   m.Ja.assign(9 * nn, 0); m.invdetJ.assign(nn, 0); m.Hd.assign(nn, 0);
+  std::vector<long double> GL(m.ops.G.begin(), m.ops.G.end());
+  auto derL = [&](const long double* f, long double* o, int d) {
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          int id = d == 0 ? i : d == 1 ? j : k;
+          long double acc = 0.0L;
+          for (int p = 0; p < N; ++p) {
+            long src = d == 0 ? nid(N, p, j, k, 0) : d == 1 ? nid(N, i, p, k, 0) : nid(N, i, j, p, 0);
+            acc += GL[id * N + p] * f[src];
+          }
+          o[nid(N, i, j, k, 0)] = acc;
+        }
+  };
 #pragma omp parallel
   {
-    std::vector<double> X(3 * ne3), dX(9 * ne3), C(3 * ne3);
-    // scratch arrays are element-local; use a Mesh view with e=0 indexing
-    Mesh loc; loc.N = N; loc.ops = m.ops; loc.Ne = 1;
+    std::vector<long double> X(3 * ne3), dX(9 * ne3), C(3 * ne3), t1(ne3), t2(ne3);
 #pragma omp for schedule(static)
     for (long e = 0; e < Ne; ++e) {
       for (long t = 0; t < ne3; ++t)
         for (int a = 0; a < 3; ++a) X[a * ne3 + t] = m.coords[a + 3 * (t + ne3 * e)];
       for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) ref_deriv(loc, &X[a * ne3], &dX[(a * 3 + b) * ne3], b, 0);
+        for (int b = 0; b < 3; ++b) derL(&X[a * ne3], &dX[(a * 3 + b) * ne3], b);
       for (int n = 0; n < 3; ++n) {
         int l = (n + 1) % 3, mm = (n + 2) % 3;
         for (int b = 0; b < 3; ++b)
           for (long t = 0; t < ne3; ++t)
-            C[b * ne3 + t] = 0.5 * (X[l * ne3 + t] * dX[(mm * 3 + b) * ne3 + t] - X[mm * ne3 + t] * dX[(l * 3 + b) * ne3 + t]);
+            C[b * ne3 + t] = 0.5L * (X[l * ne3 + t] * dX[(mm * 3 + b) * ne3 + t] - X[mm * ne3 + t] * dX[(l * 3 + b) * ne3 + t]);
         // (curl C)_al = Dhat_{al+1} C_{al+2} - Dhat_{al+2} C_{al+1}
         for (int al = 0; al < 3; ++al) {
           int b1 = (al + 1) % 3, b2 = (al + 2) % 3;
-          std::vector<double> t1(ne3), t2(ne3);
-          ref_deriv(loc, &C[b2 * ne3], t1.data(), b1, 0);
-          ref_deriv(loc, &C[b1 * ne3], t2.data(), b2, 0);
-          for (long t = 0; t < ne3; ++t) m.Ja[(al * 3 + n) * nn + t + ne3 * e] = t1[t] - t2[t];
+          derL(&C[b2 * ne3], t1.data(), b1);
+          derL(&C[b1 * ne3], t2.data(), b2);
+          for (long t = 0; t < ne3; ++t) m.Ja[(al * 3 + n) * nn + t + ne3 * e] = (double)(t1[t] - t2[t]);
         }
       }
       for (int k = 0; k < N; ++k)
@@ -586,6 +600,23 @@ int or_get(void* h, const char* name, void* out) {
   if (s == "orient") return cpi(m.orient);
   if (s == "bdry") return cpi(m.bdry);
   if (s == "handed") return cpi(m.handed);
+  return -1;
+}
+
+// overwrite a geometry array (tests use it to run the oracle on the device's
+// geometry, separating input round-off from arithmetic differences)
+int or_set(void* h, const char* name, const double* in) {
+  Mesh& m = *static_cast<Mesh*>(h);
+  auto cp = [&](std::vector<double>& v) { std::memcpy(v.data(), in, v.size() * sizeof(double)); return 0; };
+  std::string s(name);
+  if (s == "coords") return cp(m.coords);
+  if (s == "jac") return cp(m.jac);
+  if (s == "invjac") return cp(m.invjac);
+  if (s == "detjac") return cp(m.detjac);
+  if (s == "Hphys") return cp(m.Hphys);
+  if (s == "Ja") return cp(m.Ja);
+  if (s == "invdetJ") return cp(m.invdetJ);
+  if (s == "Hd") return cp(m.Hd);
   return -1;
 }
 

@@ -350,9 +350,10 @@ def test_n8_pipelined_path_many_elements(wt, ctx, O, kinds, exc):
                        gDz=dev(torch.float64, data[4]), excision_tag=exc)
     bco = O.make_bc(kinds, gPhi=data[0], gPi=data[1], gDx=data[2], gDy=data[3], gDz=data[4], excision_tag=exc)
     Pd, Qd = g.zeros(), g.zeros()
-    # single RHS evaluations on the n = 8 tensor-core path: the m8n8k4 contractions
-    # sum in another order than the oracle, which leaves round-off differences of
-    # ~1-3e-12 relative; the RK-evolved state below is held to 1e-12
+    # white-noise input through the n = 8 tensor-core path: the m8n8k4 contractions
+    # sum in another order than the oracle and n = 8 derivatives of noise cancel
+    # strongly, so this check uses the round-off bound TOL_TC; the smooth field and
+    # the RK-evolved state below are held to 1e-12
     wt.wave3d_curved_rhs(Pd, Qd, dev(torch.float64, Phi), dev(torch.float64, Pi), cg, ws, eps_KO=0.0, bc3d=bcg,
                          metric=True)
     Po, Qo = o.rhs_curved(co, Phi, Pi, eps_ko=0.0, bc=bco, use_metric=True)
@@ -363,7 +364,7 @@ def test_n8_pipelined_path_many_elements(wt, ctx, O, kinds, exc):
     wt.wave3d_curved_rhs(Pd, Qd, dev(torch.float64, Phi), dev(torch.float64, Pi), cg, ws, eps_KO=0.0, bc3d=bcg,
                          metric=True)
     Po, Qo = o.rhs_curved(co, Phi, Pi, eps_ko=0.0, bc=bco, use_metric=True)
-    assert rel(host(Pd), Po) < TOL_TC and rel(host(Qd), Qo) < TOL_TC
+    assert rel(host(Pd), Po) < TOL64 and rel(host(Qd), Qo) < TOL64
     Phi = wt.workloads.gaussian_field(x, y, z, *wt.workloads.pulses(9, 2))
     Pi = 0.1 * Phi
     dt = 0.2 * o.min_spacing() / wt.workloads.max_speed(p)

@@ -156,17 +156,54 @@ __device__ inline double sm_deriv(const double* __restrict__ f, const double* __
   return s;
 }
 
-// Curl-form metric terms, one element per CTA, N^3 threads.
-// smem: X[3], dX[9], C[3], G  -> (15 N^3 + N^2) doubles.
+// Double-double arithmetic (Dekker 1971; Shewchuk 1997): error-free products
+// via FMA and two-sums, so the strongly cancelling curl form is evaluated to
+// ~2^-104 and rounded once to double.
+struct dd { double hi, lo; };
+__device__ __forceinline__ dd two_sum(double a, double b) {
+  double s = a + b, bb = s - a;
+  return {s, (a - (s - bb)) + (b - bb)};
+}
+__device__ __forceinline__ dd dd_add(dd a, dd b) {
+  dd s = two_sum(a.hi, b.hi);
+  double lo = s.lo + a.lo + b.lo;
+  double hi = s.hi + lo;
+  return {hi, lo - (hi - s.hi)};
+}
+__device__ __forceinline__ dd dd_mul_d(dd a, double b) {  // (hi + lo) * b
+  double p = a.hi * b, e = fma(a.hi, b, -p);
+  e = fma(a.lo, b, e);
+  double hi = p + e;
+  return {hi, e - (hi - p)};
+}
+__device__ __forceinline__ dd dd_neg(dd a) { return {-a.hi, -a.lo}; }
+__device__ __forceinline__ double dd_round(dd a) { return a.hi + a.lo; }
+
+// reference derivative along axis d of a double-double smem field (hi/lo arrays)
+__device__ inline dd dd_deriv(const double* __restrict__ fh, const double* __restrict__ fl,
+                              const double* __restrict__ G, int N, int i, int j, int k, int d) {
+  dd s = {0.0, 0.0};
+  const int id = d == 0 ? i : d == 1 ? j : k;
+  for (int p = 0; p < N; ++p) {
+    const int src = d == 0 ? p + N * (j + N * k) : d == 1 ? i + N * (p + N * k) : i + N * (j + N * p);
+    s = dd_add(s, dd_mul_d({fh[src], fl ? fl[src] : 0.0}, G[id * N + p]));
+  }
+  return s;
+}
+
+// Curl-form metric terms, one element per CTA, N^3 threads, in double-double.
+// smem: X[3], dX[9] (hi, lo), C[3] (hi, lo), G -> (3 + 18 + 6) N^3 + N^2 doubles.
 __global__ void k_metric(int N, long long Ne, const double* __restrict__ Gg, const double* __restrict__ Hq,
                          const double* __restrict__ coords, const double* __restrict__ detjac,
                          double* __restrict__ Ja, double* __restrict__ invdetJ, double* __restrict__ Hd) {
   extern __shared__ double sm[];
   const int N3 = N * N * N;
-  double* X = sm;
-  double* dX = X + 3 * N3;
-  double* C = dX + 9 * N3;
-  double* G = C + 3 * N3;
+  double* X = sm;                 // 3 N3
+  double* dXh = X + 3 * N3;       // 9 N3
+  double* dXl = dXh + 9 * N3;     // 9 N3
+  double* Ch = dXl + 9 * N3;      // 3 N3
+  double* Cl = Ch + 3 * N3;       // 3 N3
+  double* G = Cl + 3 * N3;
   const long long e = blockIdx.x;
   const long long nn = Ne * N3;
   const int t = threadIdx.x;
@@ -176,17 +213,27 @@ __global__ void k_metric(int N, long long Ne, const double* __restrict__ Gg, con
   for (int a = 0; a < 3; ++a) X[a * N3 + t] = coords[a + 3 * n];
   __syncthreads();
   for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b) dX[(a * 3 + b) * N3 + t] = sm_deriv(X + a * N3, G, N, i, j, k, b);
+    for (int b = 0; b < 3; ++b) {
+      dd v = dd_deriv(X + a * N3, nullptr, G, N, i, j, k, b);
+      dXh[(a * 3 + b) * N3 + t] = v.hi;
+      dXl[(a * 3 + b) * N3 + t] = v.lo;
+    }
   __syncthreads();
   for (int c = 0; c < 3; ++c) {
     const int l = (c + 1) % 3, m = (c + 2) % 3;
-    for (int b = 0; b < 3; ++b)
-      C[b * N3 + t] = 0.5 * (X[l * N3 + t] * dX[(m * 3 + b) * N3 + t] - X[m * N3 + t] * dX[(l * 3 + b) * N3 + t]);
+    for (int b = 0; b < 3; ++b) {
+      dd p1 = dd_mul_d({dXh[(m * 3 + b) * N3 + t], dXl[(m * 3 + b) * N3 + t]}, X[l * N3 + t]);
+      dd p2 = dd_mul_d({dXh[(l * 3 + b) * N3 + t], dXl[(l * 3 + b) * N3 + t]}, X[m * N3 + t]);
+      dd v = dd_add(p1, dd_neg(p2));
+      Ch[b * N3 + t] = 0.5 * v.hi;
+      Cl[b * N3 + t] = 0.5 * v.lo;
+    }
     __syncthreads();
     for (int al = 0; al < 3; ++al) {
       const int b1 = (al + 1) % 3, b2 = (al + 2) % 3;
-      double v = sm_deriv(C + b2 * N3, G, N, i, j, k, b1) - sm_deriv(C + b1 * N3, G, N, i, j, k, b2);
-      Ja[(al * 3 + c) * nn + n] = v;
+      dd v = dd_add(dd_deriv(Ch + b2 * N3, Cl + b2 * N3, G, N, i, j, k, b1),
+                    dd_neg(dd_deriv(Ch + b1 * N3, Cl + b1 * N3, G, N, i, j, k, b2)));
+      Ja[(al * 3 + c) * nn + n] = dd_round(v);
     }
     __syncthreads();
   }
@@ -359,7 +406,7 @@ int launch_geom_derived(DevMesh& m, cudaStream_t s) {
 
 int launch_metric(DevMesh& m, cudaStream_t s) {
   const int N3 = m.N * m.N * m.N;
-  size_t smem = (15 * (size_t)N3 + m.N * m.N) * sizeof(double);
+  size_t smem = (27 * (size_t)N3 + m.N * m.N) * sizeof(double);
   cudaFuncSetAttribute(k_metric, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_metric<<<(unsigned)m.Ne, N3, smem, s>>>(m.N, m.Ne, m.G, m.H, m.coords, m.detjac, m.Ja, m.invdetJ, m.Hd);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
