@@ -181,6 +181,23 @@ typedef struct {
  * 1 the curvilinear split-form path.  bc may be NULL (periodic). */
 int wt_rhs_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi,
                   void* Phidot, void* Pidot, double eps_ko, const wt_bc_desc* bc, int use_metric);
+/* No counterpart in the reference.  The RHS of wt_rhs_curved, evaluated
+ * without a workspace and without allocating: for callers that may not
+ * allocate device memory while they evaluate the RHS (a host runtime that owns
+ * the process's device memory pool, a memory budget fixed before the time
+ * loop, or a loop that must not pay for the device-wide synchronisation of
+ * cudaMalloc/cudaFree).  Its scratch is one fixed device array of the library
+ * (8.4 MiB, held on every GPU that loads the library until exit), so the mesh
+ * may have at most WT_NOALLOC_MAX_NODES nodes and WT_NOALLOC_MAX_BOUNDARY_NODES
+ * boundary-face nodes; larger meshes are rejected with WT_EINVAL.  mu is the
+ * workspace's KO normalisation (wt_workspace_mu), used only when eps_ko != 0.
+ * The first call on a device looks up the array's device address (set-up);
+ * make that first call before any stream capture.  All calls share the array:
+ * calls whose kernels overlap on the GPU race and give wrong results. */
+#define WT_NOALLOC_MAX_NODES 262144
+#define WT_NOALLOC_MAX_BOUNDARY_NODES 262144
+int wt_rhs_curved_noalloc(wt_ctx* ctx, const wt_coef* coef, const void* Phi, const void* Pi, void* Phidot,
+                          void* Pidot, double eps_ko, double mu, const wt_bc_desc* bc, int use_metric);
 /* HexSBPSAT.apply_D!(Du, u, d) (called at src/wave3d_curved.jl:169-170, 184-189, 219-221), d = 1..3. */
 int wt_apply_D(wt_ctx* ctx, wt_ws* ws, const void* u, void* Du, int d);
 /* dst += eps * mu^-5 * sum_d D_d^6 field: the three _ko_axis3! calls of one

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1051,6 +1052,112 @@ int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* P
   cudaFree(dP);
   cudaFree(dQ);
   return rc;
+}
+
+}  // extern "C"
+
+// ---- allocation-free RHS -------------------------------------------------------------
+// Some callers cannot allocate device memory at the moment they evaluate the
+// RHS: a host runtime that owns the device memory pool of the process (and
+// frees nothing it did not hand out), code that runs inside a memory budget
+// fixed before the time loop starts, or a loop that cannot afford the
+// device-wide synchronisation cudaMalloc and cudaFree may cause.  For them
+// wt_rhs_curved_noalloc evaluates the same conservative RHS as wt_rhs_curved
+// without a workspace: the two scratch buffers the RHS needs (the flux F
+// between the gradient and the divergence pass, and the boundary-face
+// increments) live in one fixed array of device memory that the library
+// declares at file scope.  Every GPU that loads the library holds the array
+// (8.4 MiB) until the process exits.
+//
+// The array's name is only a host-side stand-in for the symbol; its device
+// address is looked up once per device, with that device current, by
+// cudaGetSymbolAddress on the first call on that device, and that address is
+// what the kernels receive.
+//
+// Every call uses the same array and it keeps the contents of the last call.
+// Nothing in it has to start at zero: the gradient pass writes every flux
+// entry and every boundary-face entry that the divergence pass of the same
+// call reads.  Calls whose kernels overlap on the GPU (different streams, or
+// different contexts on one device, without ordering between them) race on the
+// array and produce wrong results.
+namespace {
+
+constexpr long long kNoallocMaxNodes = WT_NOALLOC_MAX_NODES;
+// flux: three components of max(nodes, padded n=8 element blocks) doubles
+constexpr long long kNoallocFluxDoubles = (kNoallocMaxNodes / 512) * 544;
+constexpr long long kNoallocBdryDoubles = WT_NOALLOC_MAX_BOUNDARY_NODES;
+constexpr long long kNoallocDoubles = 3 * kNoallocFluxDoubles + kNoallocBdryDoubles;
+
+static __device__ __align__(256) double wt_noalloc_scratch[kNoallocDoubles];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of the scratch array on ctx's device (set-up on first use).
+int noalloc_scratch(wt_ctx* ctx, double** out) {
+  if (ctx->device < 0 || ctx->device >= kNoallocMaxDevices)
+    return fail(ctx, WT_ENOTSUP, "wt_rhs_curved_noalloc: device ordinal beyond the supported range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[ctx->device]) {
+    int prev = 0;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "wt_rhs_curved_noalloc set-up (cudaGetDevice)");
+    e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "wt_rhs_curved_noalloc set-up (cudaSetDevice)");
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, wt_noalloc_scratch);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return cuda_fail(ctx, e, "wt_rhs_curved_noalloc set-up (cudaGetSymbolAddress)");
+    }
+    g_noalloc_ptr[ctx->device] = (double*)p;
+  }
+  *out = g_noalloc_ptr[ctx->device];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wt_rhs_curved_noalloc(wt_ctx* ctx, const wt_coef* coef, const void* Phi, const void* Pi, void* Phidot,
+                          void* Pidot, double eps_ko, double mu, const wt_bc_desc* bc, int use_metric) {
+  if (!ctx) return WT_EINVAL;
+  if (!coef || !Phi || !Pi || !Phidot || !Pidot) return fail(ctx, WT_EINVAL, "wt_rhs_curved_noalloc: NULL argument");
+  if (coef->ctx != ctx) return fail(ctx, WT_EINVAL, "coefficients belong to another context");
+  const wt::DevMesh& m = coef->mesh->m;
+  if ((long long)m.nn > kNoallocMaxNodes)
+    return fail(ctx, WT_EINVAL, "wt_rhs_curved_noalloc: mesh has " + std::to_string((long long)m.nn) +
+                                    " nodes; the fixed scratch array holds at most " +
+                                    std::to_string(kNoallocMaxNodes) + " (use wt_rhs_curved)");
+  const long long bnodes = (long long)m.nbf * m.N * m.N;
+  if (bnodes > kNoallocBdryDoubles)
+    return fail(ctx, WT_EINVAL, "wt_rhs_curved_noalloc: mesh has " + std::to_string(bnodes) +
+                                    " boundary-face nodes; the fixed scratch array holds at most " +
+                                    std::to_string(kNoallocBdryDoubles) + " (use wt_rhs_curved)");
+  if (eps_ko != 0.0 && !(mu > 0.0))
+    return fail(ctx, WT_EINVAL, "wt_rhs_curved_noalloc: mu must be positive when eps_ko != 0");
+  wt::ConsBC b;
+  WT_TRY(make_bc(ctx, bc, use_metric, b));
+  double* scratch = nullptr;
+  WT_TRY(noalloc_scratch(ctx, &scratch));
+  void* F = scratch;
+  void* bbuf = scratch + 3 * kNoallocFluxDoubles;
+  wt::RKStage rk;
+  const bool n8 = wt::cons_n8_path(m, coef->c, use_metric, b, rk, rk, {Phi, Pi, F, Phidot, Pidot});
+  WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, Phi, Pi, F, Phidot, bbuf, nullptr, use_metric, b, rk, ctx->stream,
+                                     n8), "rhs K1"));
+  WT_TRY(lrc(ctx, wt::launch_cons_k2(m, F, Pidot, bbuf, use_metric, b, rk, nullptr, ctx->stream, n8), "rhs K2"));
+  ctx->launches += 2;
+  if (eps_ko != 0.0) {
+    const double koT = eps_ko * std::pow(1.0 / mu, 5);
+    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Phidot, Phi, koT, ctx->stream), "Kreiss-Oliger"));
+    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Pidot, Pi, koT, ctx->stream), "Kreiss-Oliger"));
+    ctx->launches += 6;
+  }
+  return 0;
 }
 
 }  // extern "C"

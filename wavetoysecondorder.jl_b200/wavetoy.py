@@ -83,6 +83,7 @@ def library():
         "wt_coef_get": [vp, vp], "wt_coef_destroy": [vp],
         "wt_workspace_create": [vp, vp, pvp], "wt_workspace_destroy": [vp], "wt_workspace_mu": [vp, C.POINTER(d)],
         "wt_rhs_curved": [vp, vp, vp, vp, vp, vp, vp, d, C.POINTER(_BcDesc), i],
+        "wt_rhs_curved_noalloc": [vp, vp, vp, vp, vp, vp, d, d, C.POINTER(_BcDesc), i],
         "wt_apply_D": [vp, vp, vp, vp, i], "wt_ko_add": [vp, vp, vp, vp, d],
         "wt_gradient3d": [vp, vp, vp, vp, vp, vp], "wt_divergence3d": [vp, vp, vp, vp, vp, vp],
         "wt_rhs_sipg": [vp, vp, vp, vp, vp, C.POINTER(C.c_double * 6), d, d],
@@ -471,6 +472,29 @@ def wave3d_curved_rhs(Phidot, Pidot, Phi, Pi, coef: Coef, ws: Workspace, eps_KO:
     p, keep = _bcptr(bc3d)
     ws.ctx.check(library().wt_rhs_curved(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), _ptr(Phidot), _ptr(Pidot),
                                          float(eps_KO), p, int(metric)), "wave3d_curved_rhs!")
+    return Phidot, Pidot
+
+
+NOALLOC_MAX_NODES = 262144
+NOALLOC_MAX_BOUNDARY_NODES = 262144
+
+
+def wave3d_curved_rhs_noalloc(Phidot, Pidot, Phi, Pi, coef: Coef, eps_KO: float = 0.0, mu: float = 0.0,
+                              bc3d: Optional[BC3D] = None, metric: bool = False):
+    """The RHS of wave3d_curved_rhs, with no workspace and no device allocation.
+
+    For callers that may not allocate device memory while they evaluate the
+    RHS (an embedding runtime that owns the device memory pool, a memory budget
+    fixed before the time loop).  The scratch is a fixed device array of the
+    library shared by all calls: meshes above NOALLOC_MAX_NODES nodes or
+    NOALLOC_MAX_BOUNDARY_NODES boundary-face nodes raise WaveToyError (code
+    WT_EINVAL), and calls
+    that overlap on the GPU race.  mu (Workspace.mu) is needed only when
+    eps_KO != 0.  No counterpart in the reference."""
+    p, keep = _bcptr(bc3d)
+    ctx = coef.mesh.ctx
+    ctx.check(library().wt_rhs_curved_noalloc(ctx.h, coef.h, _ptr(Phi), _ptr(Pi), _ptr(Phidot), _ptr(Pidot),
+                                              float(eps_KO), float(mu), p, int(metric)), "wave3d_curved_rhs_noalloc")
     return Phidot, Pidot
 
 
