@@ -132,6 +132,24 @@ int finish_topology(wt_mesh* mh) {
   cudaMemcpyAsync(m.nbrf, m.h_nbrf.data(), 6 * Ne * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream);
   cudaMemcpyAsync(m.bdry, m.h_bdry.data(), 6 * Ne * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream);
   cudaMemcpyAsync(m.bslot, slot.data(), 6 * Ne * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream);
+  {
+    std::vector<int32_t> emask(Ne, 0), fsrc(6 * Ne, -1);
+    for (long long e = 0; e < Ne; ++e)
+      for (int f = 0; f < 6; ++f) {
+        const long long i = f + 6 * e;
+        if (m.h_bdry[i] != 0) emask[e] |= 64;
+        else if (m.h_nbr[i] >= 0) {
+          emask[e] |= 1 << f;
+          fsrc[i] = 8 * m.h_nbr[i] + m.h_nbrf[i];
+        }
+      }
+    WT_TRY(dalloc(ctx, &m.emask, Ne * sizeof(int32_t), &mh->owned));
+    WT_TRY(dalloc(ctx, &m.fsrc, 6 * Ne * sizeof(int32_t), &mh->owned));
+    cudaMemcpyAsync(m.emask, emask.data(), Ne * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(m.fsrc, fsrc.data(), 6 * Ne * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream);
+    cudaError_t ce = cudaStreamSynchronize(ctx->stream);  // host vectors go out of scope
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "topology upload");
+  }
   // lines along each axis: follow face 2d+1 neighbours whose matching face is 2d
   for (int d = 0; d < 3; ++d) {
     std::vector<char> seen(Ne, 0);

@@ -63,6 +63,11 @@ struct DevMesh {
   void* invdetJ_r = nullptr;
   void* sdiag = nullptr;     // [3e + d] element-constant axis scale invjac[d,d] at node 0
   double* Ja_n8 = nullptr;   // n = 8 FP64: metric terms in padded element blocks (544 per element)
+  // per element: bits 0-5 faces that get the centred-flux SAT (interior face with a
+  // neighbour), bit 6 element has an outer face
+  int32_t* emask = nullptr;
+  // per (f,e): 8 * neighbour element + neighbour face for SAT faces, -1 otherwise
+  int32_t* fsrc = nullptr;
   // boundary faces: slot per (f,e) with bdry != 0, -1 otherwise
   int32_t* bslot = nullptr;
   int nbf = 0;

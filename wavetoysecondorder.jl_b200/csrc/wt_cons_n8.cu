@@ -115,6 +115,8 @@ struct K1N8 {
   const int32_t* nbrf;
   const int32_t* bdry;
   const int32_t* bslot;
+  const int32_t* emask;
+  const int32_t* fsrc;
   const double* G;
   const double* H;
   double* F;
@@ -152,11 +154,10 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   double* sG = sface + 2 * 6 * N2;                      // 64
   uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);  // 2
   __shared__ int abort_flag;
-  __shared__ int emeta[2][2];  // [stage]: interior-face mask, boundary flag
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
   const long long nn = P.nn;
-  const double twoH = 2.0 * P.H[0];
+  const double inv2H = 1.0 / (2.0 * P.H[0]);
   const bool need_y = P.epi && (P.stage == 1 || P.stage == 2);
   const bool need_acc = P.epi && P.stage >= 1;
   const unsigned tx_bytes = N3 * 8u + 9u * FS * 8u;
@@ -185,31 +186,15 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     else if (lane <= 9)
       bulk_g2s(d + N3 + (lane - 1) * FS, P.Ja + ((long long)(lane - 1) * P.Ne + e) * FS, FS * 8u, &bar[s]);
   };
-  // per-element metadata: interior-face mask (SAT faces) and boundary flag
-  auto meta = [&](long long e, int s) {
-    if (tid == 0) {
-      int mask = 0, bnd = 0;
-      for (int f = 0; f < 6; ++f) {
-        const int b = P.bdry[f + 6 * e];
-        if (b == 0 && P.nbr[f + 6 * e] >= 0) mask |= 1 << f;
-        if (b != 0) bnd = 1;
-      }
-      emeta[s][0] = mask;
-      emeta[s][1] = bnd;
-    }
-  };
-  // neighbour Phi face traces (384 values; threads 0..383)
-  auto face_load = [&](long long e) -> double {
-    double v = 0.0;
-    if (e >= 0 && tid < 6 * N2) {
-      const int f = tid >> 6, pq = tid & 63;
-      const int en = P.nbr[f + 6 * e];
-      if (en >= 0 && P.bdry[f + 6 * e] == 0) {
-        const int fn = P.nbrf[f + 6 * e];
-        v = P.Phi[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N)];
-      }
-    }
-    return v;
+  // neighbour Phi face traces (384 values; threads 0..383).  The face source
+  // (8 * neighbour + neighbour face) of an element is loaded one iteration
+  // before the trace itself, so no load waits on another inside the loop.
+  const int my_f = tid >> 6, my_pq = tid & 63;
+  auto src_load = [&](long long e) -> int { return (e >= 0 && tid < 6 * N2) ? P.fsrc[my_f + 6 * e] : -1; };
+  auto face_load = [&](int src) -> double {
+    if (src < 0) return 0.0;
+    const int fn = src & 7;
+    return P.Phi[(long long)(src >> 3) * N3 + face_node(faxis(fn), frow(fn, N), my_pq & 7, my_pq >> 3, N)];
   };
   // pointwise fields of this thread's node
   struct PW {
@@ -228,12 +213,14 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
 
   long long e = blockIdx.x;
   PW cur;
+  int emcur = 0, src1 = -1;
   if (e < P.Ne) {
     if (warp == 0) issue(e, 0);
-    meta(e, 0);
-    const double fv = face_load(e);
+    emcur = P.emask[e];
+    const double fv = face_load(src_load(e));
     if (tid < 6 * N2) sface[tid] = fv;
     pw_load(e, cur);
+    src1 = src_load(e + gridDim.x < P.Ne ? e + gridDim.x : -1);
   }
   __syncthreads();
   const double aG0 = sG[gq * 8 + tig], aG1 = sG[gq * 8 + 4 + tig];
@@ -241,11 +228,12 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   for (int it = 0; e < P.Ne; ++it, e += gridDim.x) {
     const int s = it & 1;
     const unsigned parity = (it >> 1) & 1;
-    const long long en = e + gridDim.x;
+    const long long en = e + gridDim.x, enn = en + gridDim.x;
     const bool has_next = en < P.Ne;
     if (warp == 0 && has_next) issue(en, s ^ 1);
-    if (has_next) meta(en, s ^ 1);
-    const double fnext = face_load(has_next ? en : -1);
+    const int emnext = has_next ? P.emask[en] : 0;
+    const int src2 = src_load(enn < P.Ne ? enn : -1);
+    const double fnext = face_load(has_next ? src1 : -1);
     PW nxt;
     pw_load(has_next ? en : -1, nxt);
     if (!wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
@@ -258,8 +246,8 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     const double* sPhi = d;      // unpadded
     const double* sJa = d + N3;  // 9 padded fields, index (al*3 + c)
     const double* sfc = sface + s * 6 * N2;
-    const int mask = emeta[s][0];
-    const int bnd = emeta[s][1];
+    const int mask = emcur & 63;
+    const int bnd = emcur >> 6;
     // ---- tensor-core contractions, one axis per phase ----
 #pragma unroll 1
     for (int al = 0; al < 3; ++al) {
@@ -308,11 +296,10 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
           const int ax = f >> 1;
           if (!((mask >> f) & 1) || idx3[ax] != ((f & 1) ? 7 : 0)) continue;
           const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
-          const double jump = sfc[f * N2 + p + 8 * q] - u;
-          const double nh = (f & 1) ? 1.0 : -1.0;
-          g0 += nh * sJa[(ax * 3 + 0) * FS + tpad] * jump / twoH;
-          g1 += nh * sJa[(ax * 3 + 1) * FS + tpad] * jump / twoH;
-          g2 += nh * sJa[(ax * 3 + 2) * FS + tpad] * jump / twoH;
+          const double jump = ((f & 1) ? inv2H : -inv2H) * (sfc[f * N2 + p + 8 * q] - u);
+          g0 += sJa[(ax * 3 + 0) * FS + tpad] * jump;
+          g1 += sJa[(ax * 3 + 1) * FS + tpad] * jump;
+          g2 += sJa[(ax * 3 + 2) * FS + tpad] * jump;
         }
       }
       g0 *= cur.invJ; g1 *= cur.invJ; g2 *= cur.invJ;
@@ -391,6 +378,8 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     }
     if (has_next && tid < 6 * N2) sface[(s ^ 1) * 6 * N2 + tid] = fnext;
     cur = nxt;
+    emcur = emnext;
+    src1 = src2;
     __syncthreads();
   }
 }
@@ -407,6 +396,8 @@ struct K2N8 {
   const int32_t* nbrf;
   const int32_t* bdry;
   const int32_t* bslot;
+  const int32_t* emask;
+  const int32_t* fsrc;
   const double* G;
   const double* H;
   const double* bbuf;
@@ -434,11 +425,10 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   double* sG = sface + 2 * 6 * 3 * N2;                   // 64
   uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);
   __shared__ int abort_flag;
-  __shared__ int emeta[2][2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
   const long long nn = P.nn;
-  const double twoH = 2.0 * P.H[0];
+  const double inv2H = 1.0 / (2.0 * P.H[0]);
   const bool need_y = P.epi && P.stage <= 2;
   const bool need_acc = P.epi && P.stage >= 1;
   const unsigned tx_bytes = K2_NF * FS * 8u;
@@ -468,33 +458,26 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
       bulk_g2s(d + lane * FS, src, FS * 8u, &bar[s]);
     }
   };
-  auto meta = [&](long long e, int s) {
-    if (tid == 0) {
-      int mask = 0, bnd = 0;
-      for (int f = 0; f < 6; ++f) {
-        const int b = P.bdry[f + 6 * e];
-        if (b == 0 && P.nbr[f + 6 * e] >= 0) mask |= 1 << f;
-        if (b != 0) bnd = 1;
-      }
-      emeta[s][0] = mask;
-      emeta[s][1] = bnd;
+  // neighbour flux face traces: [f][c][pq], 1152 values, <= 3 per thread; the
+  // face sources are loaded one iteration ahead of the traces (see K1)
+  auto src_load = [&](long long e, int src[3]) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const int idx = tid + r * THREADS;
+      src[r] = (e >= 0 && idx < NFACE) ? P.fsrc[idx / (3 * N2) + 6 * e] : -1;
     }
   };
-  // neighbour flux face traces: [f][c][pq], 1152 values, <= 3 per thread
-  auto face_load = [&](long long e, double fv[3]) {
+  auto face_load = [&](const int src[3], double fv[3]) {
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
       const int idx = tid + r * THREADS;
       double v = 0.0;
-      if (e >= 0 && idx < NFACE) {
-        const int f = idx / (3 * N2), rem = idx - f * 3 * N2, c = rem >> 6, pq = rem & 63;
-        const int en = P.nbr[f + 6 * e];
-        if (en >= 0 && P.bdry[f + 6 * e] == 0) {
-          const int fn = P.nbrf[f + 6 * e];
-          const double* Fc = c == 0 ? P.F0 : c == 1 ? P.F1 : P.F2;
-          const int fnode = face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N);
-          v = Fc[(long long)en * FS + pad(fnode & 7, (fnode >> 3) & 7, fnode >> 6)];
-        }
+      if (src[r] >= 0) {
+        const int rem = idx % (3 * N2), c = rem >> 6, pq = rem & 63;
+        const int fn = src[r] & 7;
+        const double* Fc = c == 0 ? P.F0 : c == 1 ? P.F1 : P.F2;
+        const int fnode = face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N);
+        v = Fc[(long long)(src[r] >> 3) * FS + pad(fnode & 7, (fnode >> 3) & 7, fnode >> 6)];
       }
       fv[r] = v;
     }
@@ -512,15 +495,19 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
 
   long long e = blockIdx.x;
   PW cur;
+  int emcur = 0, src1[3] = {-1, -1, -1};
   if (e < P.Ne) {
     if (warp == 0) issue(e, 0);
-    meta(e, 0);
+    emcur = P.emask[e];
+    int src0[3];
+    src_load(e, src0);
     double fv[3];
-    face_load(e, fv);
+    face_load(src0, fv);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
       if (tid + r * THREADS < NFACE) sface[tid + r * THREADS] = fv[r];
     pw_load(e, cur);
+    src_load(e + gridDim.x < P.Ne ? e + gridDim.x : -1, src1);
   }
   __syncthreads();
   const double aG0 = sG[gq * 8 + tig], aG1 = sG[gq * 8 + 4 + tig];
@@ -528,12 +515,14 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   for (int it = 0; e < P.Ne; ++it, e += gridDim.x) {
     const int s = it & 1;
     const unsigned parity = (it >> 1) & 1;
-    const long long en = e + gridDim.x;
+    const long long en = e + gridDim.x, enn = en + gridDim.x;
     const bool has_next = en < P.Ne;
     if (warp == 0 && has_next) issue(en, s ^ 1);
-    if (has_next) meta(en, s ^ 1);
+    const int emnext = has_next ? P.emask[en] : 0;
+    int src2[3];
+    src_load(enn < P.Ne ? enn : -1, src2);
     double fnext[3];
-    face_load(has_next ? en : -1, fnext);
+    face_load(src1, fnext);
     PW nxt;
     pw_load(has_next ? en : -1, nxt);
     if (!wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
@@ -546,8 +535,8 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     const double* sF = d;           // 3 fields
     const double* sJa = d + 3 * FS;  // 9 fields
     const double* sfc = sface + s * NFACE;
-    const int mask = emeta[s][0];
-    const int bnd = emeta[s][1];
+    const int mask = emcur & 63;
+    const int bnd = emcur >> 6;
 #pragma unroll 1
     for (int al = 0; al < 3; ++al) {
       const double* m0 = sJa + (al * 3 + 0) * FS;
@@ -599,7 +588,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
 #pragma unroll
           for (int c = 0; c < 3; ++c)
             sacc += sJa[(ax * 3 + c) * FS + tpad] * (sfc[(f * 3 + c) * N2 + p + 8 * q] - sF[c * FS + tpad]);
-          dv += nh * sacc / twoH;
+          dv += nh * sacc * inv2H;
         }
       }
       dv *= cur.invJ;
@@ -639,6 +628,9 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
         if (tid + r * THREADS < NFACE) sface[(s ^ 1) * NFACE + tid + r * THREADS] = fnext[r];
     }
     cur = nxt;
+    emcur = emnext;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) src1[r] = src2[r];
     __syncthreads();
   }
 }
@@ -680,6 +672,7 @@ int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const
   P.Phi = (const double*)Phi; P.Pi = (const double*)Pi; P.c10 = (const double*)c.c10;
   P.Ja = (const double*)m.Ja_n8; P.invdetJ = (const double*)m.invdetJ_r;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
+  P.emask = m.emask; P.fsrc = m.fsrc;
   P.F = (double*)F; P.Phidot = (double*)Phidot; P.bbuf = (double*)bbuf;
   P.bc_on = bc.on; P.exc_tag = bc.exc_tag; P.nbf = m.nbf; P.kind = bc.kinds[0]; P.sigma = bc.sigma;
   P.bnorm = (const double*)m.bnorm;
@@ -704,6 +697,7 @@ int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* 
   P.F0 = (const double*)F; P.F1 = (const double*)F + m.Ne * n8::FS; P.F2 = (const double*)F + 2 * m.Ne * n8::FS;
   P.Ja = (const double*)m.Ja_n8; P.invdetJ = (const double*)m.invdetJ_r;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
+  P.emask = m.emask; P.fsrc = m.fsrc;
   P.bbuf = (const double*)bbuf; P.bc_on = bc.on;
   P.Pidot = (double*)Pidot;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;

@@ -325,7 +325,10 @@ def sample_background3d(mesh: Mesh, kind: int = BG_MINKOWSKI, params: Optional[S
     """make_coef3d + sample_background3d! for an analytic background (src/wave3d_curved.jl:106-124)."""
     d = _BgDesc()
     d.kind = int(kind)
-    for k, v in enumerate(params or ()):
+    params = () if params is None else list(params)
+    if len(params) > len(d.p):
+        raise ValueError(f"at most {len(d.p)} background parameters")
+    for k, v in enumerate(params):
         d.p[k] = float(v)
     h = C.c_void_p()
     mesh.ctx.check(library().wt_background_set(mesh.ctx.h, mesh.h, C.byref(d), C.byref(h)), "wt_background_set")
