@@ -143,14 +143,14 @@ struct K1N8 {
 // invJ, y, acc.
 constexpr int K1_NF = 10;
 constexpr size_t K1_STAGE = (size_t)n8::N3 + 9 * (size_t)n8::FS;
-constexpr size_t K1_SMEM = (2 * K1_STAGE + 3 * n8::FS + 2 * 6 * n8::N2 + n8::N2) * sizeof(double) + 64;
+constexpr size_t K1_SMEM = (2 * K1_STAGE + 9 * n8::FS + 2 * 6 * n8::N2 + n8::N2) * sizeof(double) + 64;
 
 __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   using namespace n8;
   extern __shared__ __align__(128) unsigned char smraw[];
   double* stg = reinterpret_cast<double*>(smraw);       // 2 stages x 10 padded fields
-  double* sg = stg + 2 * K1_STAGE;                      // 3 padded gradient accumulators
-  double* sface = sg + 3 * FS;                          // 2 x 6 x 64
+  double* sg = stg + 2 * K1_STAGE;                      // 9 padded partial gradients [al*3 + c]
+  double* sface = sg + 9 * FS;                          // 2 x 6 x 64
   double* sG = sface + 2 * 6 * N2;                      // 64
   uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);  // 2
   __shared__ int abort_flag;
@@ -248,47 +248,48 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     const double* sfc = sface + s * 6 * N2;
     const int mask = emcur & 63;
     const int bnd = emcur >> 6;
-    // ---- tensor-core contractions, one axis per phase ----
-#pragma unroll 1
-    for (int al = 0; al < 3; ++al) {
-      // half 0: component 0; half 1: components 1 and 2
-      const int c0 = half == 0 ? 0 : 1;
-      const int ncomp = half == 0 ? 1 : 2;
-      const double* mA = sJa + (al * 3 + c0) * FS;
-      const double* mB = sJa + (al * 3 + 2) * FS;
-      double cu[2] = {0, 0}, ca[2] = {0, 0}, cb[2] = {0, 0};
+    // ---- tensor-core contractions ----
+    // Each axis writes its own partial gradients sg[al*3 + c], so the axes need
+    // no barrier between them.  Per pencil tile, warp w (half 0) does axis 0
+    // and components 0, 1 of axis 1; warp w + 8 (half 1) component 2 of axis 1
+    // and axis 2: 7 and 6 contraction chains.
+    // comps: bit c set = produce component c of axis al.
+    auto grad_axis = [&](int al, int comps) {
+      double cu[2] = {0, 0}, cm[3][2] = {{0, 0}, {0, 0}, {0, 0}};
 #pragma unroll
       for (int kc = 0; kc < 2; ++kc) {
         const int nd = bnode(al, wt8, kc, gq, tig);
         const double u = sPhi[unpad(nd)];
         const double a = kc ? aG1 : aG0;
         dmma(cu[0], cu[1], a, u);
-        dmma(ca[0], ca[1], a, mA[nd] * u);
-        if (ncomp == 2) dmma(cb[0], cb[1], a, mB[nd] * u);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          if ((comps >> c) & 1) dmma(cm[c][0], cm[c][1], a, sJa[(al * 3 + c) * FS + nd] * u);
       }
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         const int no = onode(al, wt8, b, gq, tig);
-        const double mo_a = mA[no];
-        double ra = 0.5 * ca[b] + 0.5 * mo_a * cu[b];
-        double rb = 0.0;
-        if (ncomp == 2) rb = 0.5 * cb[b] + 0.5 * mB[no] * cu[b];
-        double* ga = sg + c0 * FS;
-        if (al == 0) {
-          ga[no] = ra;
-          if (ncomp == 2) sg[2 * FS + no] = rb;
-        } else {
-          ga[no] += ra;
-          if (ncomp == 2) sg[2 * FS + no] += rb;
-        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          if ((comps >> c) & 1)
+            sg[(al * 3 + c) * FS + no] = 0.5 * cm[c][b] + 0.5 * sJa[(al * 3 + c) * FS + no] * cu[b];
       }
-      __syncthreads();
+    };
+    if (half == 0) {
+      grad_axis(0, 7);
+      grad_axis(1, 3);
+    } else {
+      grad_axis(1, 4);
+      grad_axis(2, 7);
     }
+    __syncthreads();
     // ---- node phase: one node per thread ----
     {
       const long long n = e * N3 + tid;
       const double u = sPhi[tid];
-      double g0 = sg[tpad], g1 = sg[FS + tpad], g2 = sg[2 * FS + tpad];
+      double g0 = (sg[tpad] + sg[3 * FS + tpad]) + sg[6 * FS + tpad];
+      double g1 = (sg[FS + tpad] + sg[4 * FS + tpad]) + sg[7 * FS + tpad];
+      double g2 = (sg[2 * FS + tpad] + sg[5 * FS + tpad]) + sg[8 * FS + tpad];
       if (mask) {  // centred-flux SAT on interior faces through this node (after the volume terms)
         const int idx3[3] = {ti, tj, tk};
 #pragma unroll
@@ -414,14 +415,14 @@ struct K2N8 {
 // K2 staged fields: 0..2 F, 3..11 Ja.  Register prefetch: invJ, y, acc.
 constexpr int K2_NF = 12;
 constexpr size_t K2_STAGE = (size_t)K2_NF * n8::FS;
-constexpr size_t K2_SMEM = (2 * K2_STAGE + 2 * n8::FS + 2 * 6 * 3 * n8::N2 + n8::N2) * sizeof(double) + 64;
+constexpr size_t K2_SMEM = (2 * K2_STAGE + 6 * n8::FS + 2 * 6 * 3 * n8::N2 + n8::N2) * sizeof(double) + 64;
 
 __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   using namespace n8;
   extern __shared__ __align__(128) unsigned char smraw[];
   double* stg = reinterpret_cast<double*>(smraw);
-  double* sdiv = stg + 2 * K2_STAGE;                     // 2 padded partial divergences
-  double* sface = sdiv + 2 * FS;                         // 2 x 6 x 3 x 64
+  double* sdiv = stg + 2 * K2_STAGE;                     // 6 padded partial divergences [al*2 + half]
+  double* sface = sdiv + 6 * FS;                         // 2 x 6 x 3 x 64
   double* sG = sface + 2 * 6 * 3 * N2;                   // 64
   uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);
   __shared__ int abort_flag;
@@ -537,7 +538,8 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     const double* sfc = sface + s * NFACE;
     const int mask = emcur & 63;
     const int bnd = emcur >> 6;
-#pragma unroll 1
+    // per-axis partial divergences sg[al*2 + half]: no barrier between axes
+#pragma unroll
     for (int al = 0; al < 3; ++al) {
       const double* m0 = sJa + (al * 3 + 0) * FS;
       const double* m1 = sJa + (al * 3 + 1) * FS;
@@ -567,15 +569,14 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
         } else {
           r = 0.5 * m1[no] * cx[b] + 0.5 * m2[no] * cy[b];
         }
-        double* acc_s = sdiv + half * FS;
-        if (al == 0) acc_s[no] = r;
-        else acc_s[no] += r;
+        sdiv[(al * 2 + half) * FS + no] = r;
       }
-      __syncthreads();
     }
+    __syncthreads();
     {
       const long long n = e * N3 + tid;
-      double dv = sdiv[tpad] + sdiv[FS + tpad];
+      double dv = ((sdiv[tpad] + sdiv[2 * FS + tpad]) + sdiv[4 * FS + tpad]) +
+                  ((sdiv[FS + tpad] + sdiv[3 * FS + tpad]) + sdiv[5 * FS + tpad]);
       if (mask) {  // centred-flux SAT on interior faces through this node (after the volume terms)
         const int idx3[3] = {ti, tj, tk};
 #pragma unroll
