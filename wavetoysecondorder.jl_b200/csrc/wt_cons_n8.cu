@@ -10,22 +10,29 @@
 //   * the fields the derivative contractions read at other nodes of an
 //     element (Phi and the nine metric terms in K1; the three flux components
 //     and the metric terms in K2) are staged into shared memory with 1D bulk
-//     copies (cp.async.bulk ... mbarrier::complete_tx), one copy per k-plane
-//     into a plane-padded layout (stride 68 doubles) that makes the tensor-core
-//     operand loads bank-conflict-free, double-buffered on two mbarriers with
-//     bounded waits that raise an error flag instead of spinning forever;
+//     copies (cp.async.bulk ... mbarrier::complete_tx), one copy per field
+//     block; the metric terms and the flux live in global memory in a
+//     plane-padded element layout (k-plane stride 68 doubles) that makes the
+//     tensor-core operand loads (nearly) bank-conflict-free.  A ring of
+//     NSTAGE stages keeps NSTAGE - 1 elements in flight; every wait is
+//     bounded and raises an error flag instead of spinning forever;
 //   * the fields used only at their own node (background coefficients, Pi,
 //     1/J, the RK4 state) are prefetched into registers one element ahead;
 //   * the 8x8 reference-derivative contractions run on the FP64 tensor cores
 //     (mma.sync.m8n8k4.f64): for axis al an element's 64 pencils are the N
 //     dimension, G the A operand (in registers), the staged field -- or the
 //     split-form product Ja*u / Ja.F formed while loading -- the B operand.
-//     Warp w owns pencil tile w&7; warps w and w+8 split the fields of a tile.
-//     The centred-flux SATs are added in the same pass: an output row l = 0
-//     or 7 of the MMA is the node row on face 2al or 2al+1;
+//     Warp w owns pencil tile w&7; warps w and w+8 split the fields of a tile,
+//     and every axis writes its own partial sums, so one barrier separates
+//     the contraction pass from the node pass.  The centred-flux SATs are
+//     added in the same pass: an output row l = 0 or 7 of the MMA is the node
+//     row on face 2al or 2al+1;
 //   * a node phase (one node per thread) forms flux, Phidot / divergence,
 //     boundary terms (boundary elements only) and the RK4 stage update and
-//     writes coalesced results.
+//     writes coalesced results;
+//   * per-element tables (SAT face mask, neighbour face sources) are loaded
+//     one element before the neighbour traces they address, so no load in
+//     the loop waits on another load.
 #include "wt_common.cuh"
 
 namespace wt {
@@ -35,8 +42,10 @@ namespace n8 {
 constexpr int N = 8, N2 = 64, N3 = 512, THREADS = 512;
 constexpr int PS = 68;             // padded k-plane stride (doubles)
 constexpr int FS = 8 * PS;         // padded field size (544 doubles = 4352 B)
-constexpr unsigned PLANE_BYTES = N2 * sizeof(double);  // 512
 constexpr long long WAIT_LIMIT = 1LL << 24;
+// staged elements in flight: element e + (NSTAGE - 1) * grid is copied while e
+// is processed
+constexpr int NSTAGE = 2;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
@@ -141,18 +150,17 @@ struct K1N8 {
 // K1 staged fields: Phi (unpadded, 512) and Ja (9 padded fields, one 4352-byte
 // block each from the padded global copy).  Register prefetch: c10 (10), Pi,
 // invJ, y, acc.
-constexpr int K1_NF = 10;
 constexpr size_t K1_STAGE = (size_t)n8::N3 + 9 * (size_t)n8::FS;
-constexpr size_t K1_SMEM = (2 * K1_STAGE + 9 * n8::FS + 2 * 6 * n8::N2 + n8::N2) * sizeof(double) + 64;
+constexpr size_t K1_SMEM = (n8::NSTAGE * K1_STAGE + 9 * n8::FS + 2 * 6 * n8::N2 + n8::N2) * sizeof(double) + 64;
 
 __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   using namespace n8;
   extern __shared__ __align__(128) unsigned char smraw[];
   double* stg = reinterpret_cast<double*>(smraw);       // 2 stages x 10 padded fields
-  double* sg = stg + 2 * K1_STAGE;                      // 9 padded partial gradients [al*3 + c]
+  double* sg = stg + NSTAGE * K1_STAGE;                      // 9 padded partial gradients [al*3 + c]
   double* sface = sg + 9 * FS;                          // 2 x 6 x 64
   double* sG = sface + 2 * 6 * N2;                      // 64
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);  // 2
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);  // NSTAGE
   __shared__ int abort_flag;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
@@ -168,8 +176,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   if (tid < N2) sG[tid] = P.G[tid];
   if (tid == 0) {
     abort_flag = 0;
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int k = 0; k < NSTAGE; ++k) mbar_init(&bar[k], 1);
     fence_barrier_init();
   }
   __syncthreads();
@@ -215,7 +222,9 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   PW cur;
   int emcur = 0, src1 = -1;
   if (e < P.Ne) {
-    if (warp == 0) issue(e, 0);
+    if (warp == 0)
+      for (int k = 0; k < NSTAGE - 1; ++k)
+        if (e + k * (long long)gridDim.x < P.Ne) issue(e + k * (long long)gridDim.x, k);
     emcur = P.emask[e];
     const double fv = face_load(src_load(e));
     if (tid < 6 * N2) sface[tid] = fv;
@@ -226,26 +235,34 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
   const double aG0 = sG[gq * 8 + tig], aG1 = sG[gq * 8 + 4 + tig];
 
   for (int it = 0; e < P.Ne; ++it, e += gridDim.x) {
-    const int s = it & 1;
-    const unsigned parity = (it >> 1) & 1;
+    const int s = it % NSTAGE, fb = it & 1;
+    const unsigned parity = (it / NSTAGE) & 1;
     const long long en = e + gridDim.x, enn = en + gridDim.x;
     const bool has_next = en < P.Ne;
-    if (warp == 0 && has_next) issue(en, s ^ 1);
     const int emnext = has_next ? P.emask[en] : 0;
     const int src2 = src_load(enn < P.Ne ? enn : -1);
     const double fnext = face_load(has_next ? src1 : -1);
     PW nxt;
     pw_load(has_next ? en : -1, nxt);
     if (!wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
+    // After this barrier every thread has finished the previous element, so its
+    // stage (reused for element e + (NSTAGE - 1) grid), the partial gradients
+    // and face buffer fb^1 are free.
     __syncthreads();
-    if (abort_flag) {
-      if (warp == 0 && lane == 0 && has_next) wait_phase(&bar[s ^ 1], ((it + 1) >> 1) & 1, nullptr);
+    if (abort_flag) {  // wait (bounded) for the copies still in flight, then leave
+      if (warp == 0 && lane == 0)
+        for (int k = 1; k < NSTAGE - 1; ++k)
+          if (e + k * (long long)gridDim.x < P.Ne) wait_phase(&bar[(it + k) % NSTAGE], ((it + k) / NSTAGE) & 1, nullptr);
       return;
+    }
+    {
+      const long long ei = e + (NSTAGE - 1) * (long long)gridDim.x;
+      if (warp == 0 && ei < P.Ne) issue(ei, (it + NSTAGE - 1) % NSTAGE);
     }
     const double* d = stg + s * K1_STAGE;
     const double* sPhi = d;      // unpadded
     const double* sJa = d + N3;  // 9 padded fields, index (al*3 + c)
-    const double* sfc = sface + s * 6 * N2;
+    const double* sfc = sface + fb * 6 * N2;
     const int mask = emcur & 63;
     const int bnd = emcur >> 6;
     // ---- tensor-core contractions ----
@@ -253,7 +270,9 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     // no barrier between them.  Per pencil tile, warp w (half 0) does axis 0
     // and components 0, 1 of axis 1; warp w + 8 (half 1) component 2 of axis 1
     // and axis 2: 7 and 6 contraction chains.
-    // comps: bit c set = produce component c of axis al.
+    // comps: bit c set = produce component c of axis al.  The centred-flux SAT
+    // of an interior al-face is added to the output rows on that face (row 0:
+    // face 2 al, row 7: face 2 al + 1).
     auto grad_axis = [&](int al, int comps) {
       double cu[2] = {0, 0}, cm[3][2] = {{0, 0}, {0, 0}, {0, 0}};
 #pragma unroll
@@ -266,13 +285,21 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
         for (int c = 0; c < 3; ++c)
           if ((comps >> c) & 1) dmma(cm[c][0], cm[c][1], a, sJa[(al * 3 + c) * FS + nd] * u);
       }
+      const int sface_f = gq == 0 ? 2 * al : gq == 7 ? 2 * al + 1 : -1;
+      const bool sat = sface_f >= 0 && ((mask >> sface_f) & 1);
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         const int no = onode(al, wt8, b, gq, tig);
+        double jump = 0.0;
+        if (sat) jump = (gq ? inv2H : -inv2H) * (sfc[sface_f * N2 + opq(al, wt8, b, tig)] - sPhi[unpad(no)]);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          if ((comps >> c) & 1)
-            sg[(al * 3 + c) * FS + no] = 0.5 * cm[c][b] + 0.5 * sJa[(al * 3 + c) * FS + no] * cu[b];
+          if ((comps >> c) & 1) {
+            const double m = sJa[(al * 3 + c) * FS + no];
+            double r = 0.5 * cm[c][b] + 0.5 * m * cu[b];
+            if (sat) r += m * jump;
+            sg[(al * 3 + c) * FS + no] = r;
+          }
       }
     };
     if (half == 0) {
@@ -290,19 +317,6 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
       double g0 = (sg[tpad] + sg[3 * FS + tpad]) + sg[6 * FS + tpad];
       double g1 = (sg[FS + tpad] + sg[4 * FS + tpad]) + sg[7 * FS + tpad];
       double g2 = (sg[2 * FS + tpad] + sg[5 * FS + tpad]) + sg[8 * FS + tpad];
-      if (mask) {  // centred-flux SAT on interior faces through this node (after the volume terms)
-        const int idx3[3] = {ti, tj, tk};
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-          const int ax = f >> 1;
-          if (!((mask >> f) & 1) || idx3[ax] != ((f & 1) ? 7 : 0)) continue;
-          const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
-          const double jump = ((f & 1) ? inv2H : -inv2H) * (sfc[f * N2 + p + 8 * q] - u);
-          g0 += sJa[(ax * 3 + 0) * FS + tpad] * jump;
-          g1 += sJa[(ax * 3 + 1) * FS + tpad] * jump;
-          g2 += sJa[(ax * 3 + 2) * FS + tpad] * jump;
-        }
-      }
       g0 *= cur.invJ; g1 *= cur.invJ; g2 *= cur.invJ;
       const double a = cur.c[0];
       const double b0 = cur.c[1], b1 = cur.c[2], b2 = cur.c[3];
@@ -377,11 +391,10 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
         P.Phidot[n] = phid;
       }
     }
-    if (has_next && tid < 6 * N2) sface[(s ^ 1) * 6 * N2 + tid] = fnext;
+    if (has_next && tid < 6 * N2) sface[(fb ^ 1) * 6 * N2 + tid] = fnext;
     cur = nxt;
     emcur = emnext;
     src1 = src2;
-    __syncthreads();
   }
 }
 
@@ -415,20 +428,19 @@ struct K2N8 {
 // K2 staged fields: 0..2 F, 3..11 Ja.  Register prefetch: invJ, y, acc.
 constexpr int K2_NF = 12;
 constexpr size_t K2_STAGE = (size_t)K2_NF * n8::FS;
-constexpr size_t K2_SMEM = (2 * K2_STAGE + 6 * n8::FS + 2 * 6 * 3 * n8::N2 + n8::N2) * sizeof(double) + 64;
+constexpr size_t K2_SMEM = (n8::NSTAGE * K2_STAGE + 6 * n8::FS + 2 * 6 * 3 * n8::N2 + n8::N2) * sizeof(double) + 64;
 
 __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   using namespace n8;
   extern __shared__ __align__(128) unsigned char smraw[];
   double* stg = reinterpret_cast<double*>(smraw);
-  double* sdiv = stg + 2 * K2_STAGE;                     // 6 padded partial divergences [al*2 + half]
+  double* sdiv = stg + NSTAGE * K2_STAGE;                     // 6 padded partial divergences [al*2 + half]
   double* sface = sdiv + 6 * FS;                         // 2 x 6 x 3 x 64
   double* sG = sface + 2 * 6 * 3 * N2;                   // 64
   uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);
   __shared__ int abort_flag;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
-  const long long nn = P.nn;
   const double inv2H = 1.0 / (2.0 * P.H[0]);
   const bool need_y = P.epi && P.stage <= 2;
   const bool need_acc = P.epi && P.stage >= 1;
@@ -440,8 +452,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   if (tid < N2) sG[tid] = P.G[tid];
   if (tid == 0) {
     abort_flag = 0;
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int k = 0; k < NSTAGE; ++k) mbar_init(&bar[k], 1);
     fence_barrier_init();
   }
   __syncthreads();
@@ -498,7 +509,9 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   PW cur;
   int emcur = 0, src1[3] = {-1, -1, -1};
   if (e < P.Ne) {
-    if (warp == 0) issue(e, 0);
+    if (warp == 0)
+      for (int k = 0; k < NSTAGE - 1; ++k)
+        if (e + k * (long long)gridDim.x < P.Ne) issue(e + k * (long long)gridDim.x, k);
     emcur = P.emask[e];
     int src0[3];
     src_load(e, src0);
@@ -514,11 +527,10 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
   const double aG0 = sG[gq * 8 + tig], aG1 = sG[gq * 8 + 4 + tig];
 
   for (int it = 0; e < P.Ne; ++it, e += gridDim.x) {
-    const int s = it & 1;
-    const unsigned parity = (it >> 1) & 1;
+    const int s = it % NSTAGE, fb = it & 1;
+    const unsigned parity = (it / NSTAGE) & 1;
     const long long en = e + gridDim.x, enn = en + gridDim.x;
     const bool has_next = en < P.Ne;
-    if (warp == 0 && has_next) issue(en, s ^ 1);
     const int emnext = has_next ? P.emask[en] : 0;
     int src2[3];
     src_load(enn < P.Ne ? enn : -1, src2);
@@ -527,15 +539,21 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     PW nxt;
     pw_load(has_next ? en : -1, nxt);
     if (!wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
-    __syncthreads();
-    if (abort_flag) {
-      if (warp == 0 && lane == 0 && has_next) wait_phase(&bar[s ^ 1], ((it + 1) >> 1) & 1, nullptr);
+    __syncthreads();  // the previous element is finished: its stage and the buffers are free (see K1)
+    if (abort_flag) {  // wait (bounded) for the copies still in flight, then leave
+      if (warp == 0 && lane == 0)
+        for (int k = 1; k < NSTAGE - 1; ++k)
+          if (e + k * (long long)gridDim.x < P.Ne) wait_phase(&bar[(it + k) % NSTAGE], ((it + k) / NSTAGE) & 1, nullptr);
       return;
+    }
+    {
+      const long long ei = e + (NSTAGE - 1) * (long long)gridDim.x;
+      if (warp == 0 && ei < P.Ne) issue(ei, (it + NSTAGE - 1) % NSTAGE);
     }
     const double* d = stg + s * K2_STAGE;
     const double* sF = d;           // 3 fields
     const double* sJa = d + 3 * FS;  // 9 fields
-    const double* sfc = sface + s * NFACE;
+    const double* sfc = sface + fb * NFACE;
     const int mask = emcur & 63;
     const int bnd = emcur >> 6;
     // per-axis partial divergences sg[al*2 + half]: no barrier between axes
@@ -560,6 +578,9 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
           dmma(cy[0], cy[1], a, sF[2 * FS + nd]);
         }
       }
+      // half 1 adds the centred-flux SAT of an interior al-face on its rows
+      const int sface_f = gq == 0 ? 2 * al : gq == 7 ? 2 * al + 1 : -1;
+      const bool sat = half == 1 && sface_f >= 0 && ((mask >> sface_f) & 1);
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         const int no = onode(al, wt8, b, gq, tig);
@@ -569,6 +590,13 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
         } else {
           r = 0.5 * m1[no] * cx[b] + 0.5 * m2[no] * cy[b];
         }
+        if (sat) {
+          const int pq = opq(al, wt8, b, tig);
+          const double sacc = m0[no] * (sfc[(sface_f * 3 + 0) * N2 + pq] - sF[no]) +
+                              m1[no] * (sfc[(sface_f * 3 + 1) * N2 + pq] - sF[FS + no]) +
+                              m2[no] * (sfc[(sface_f * 3 + 2) * N2 + pq] - sF[2 * FS + no]);
+          r += (gq ? inv2H : -inv2H) * sacc;
+        }
         sdiv[(al * 2 + half) * FS + no] = r;
       }
     }
@@ -577,21 +605,6 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
       const long long n = e * N3 + tid;
       double dv = ((sdiv[tpad] + sdiv[2 * FS + tpad]) + sdiv[4 * FS + tpad]) +
                   ((sdiv[FS + tpad] + sdiv[3 * FS + tpad]) + sdiv[5 * FS + tpad]);
-      if (mask) {  // centred-flux SAT on interior faces through this node (after the volume terms)
-        const int idx3[3] = {ti, tj, tk};
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-          const int ax = f >> 1;
-          if (!((mask >> f) & 1) || idx3[ax] != ((f & 1) ? 7 : 0)) continue;
-          const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
-          const double nh = (f & 1) ? 1.0 : -1.0;
-          double sacc = 0.0;
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            sacc += sJa[(ax * 3 + c) * FS + tpad] * (sfc[(f * 3 + c) * N2 + p + 8 * q] - sF[c * FS + tpad]);
-          dv += nh * sacc * inv2H;
-        }
-      }
       dv *= cur.invJ;
       if (bnd && P.bc_on) {
         const int idx3[3] = {ti, tj, tk};
@@ -626,13 +639,12 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     if (has_next) {
 #pragma unroll
       for (int r = 0; r < 3; ++r)
-        if (tid + r * THREADS < NFACE) sface[(s ^ 1) * NFACE + tid + r * THREADS] = fnext[r];
+        if (tid + r * THREADS < NFACE) sface[(fb ^ 1) * NFACE + tid + r * THREADS] = fnext[r];
     }
     cur = nxt;
     emcur = emnext;
 #pragma unroll
     for (int r = 0; r < 3; ++r) src1[r] = src2[r];
-    __syncthreads();
   }
 }
 
