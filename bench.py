@@ -123,6 +123,7 @@ def workload_desc(args, nn):
                         f"({nn:,} nodes), Sommerfeld faces, curvilinear split form, RK4 CFL 0.2, "
                         f"{args.precision.upper()}",
             "elements_per_axis": args.elements, "n": args.n, "nodes": nn, "precision": args.precision,
+            **({"fp32_form": args.fp32_form} if args.precision == "f32" else {}),
             "warp_A": 0.05, "eps_KO": 0.0, "seed": args.seed,
             "l2": "inputs larger than L2 (each field %.2f GB > 126 MB)" % (nn * (8 if args.precision == "f64" else 4) / 1e9)}
 
@@ -215,6 +216,8 @@ def run_ours(args):
     prec = wt.WT_F64 if args.precision == "f64" else wt.WT_F32
     M, N = args.elements, args.n
     mesh = wt.Mesh.warped_uniform_hex(ctx, N, M, 0.0, 1.0, 0.05, outer_tag=wt.SOMMERFELD_BDRY_TAG, precision=prec)
+    if prec == wt.WT_F32:
+        mesh.set_fp32_form({"bf16x3": wt.FP32_BF16X3, "bf16x2": wt.FP32_BF16X2, "cuda": wt.FP32_CUDA_CORES}[args.fp32_form])
     seed = args.seed + 7919 * rank
     p = wt.workloads.adm_params(seed)
     coef = wt.sample_background3d(mesh, wt.BG_ADM_PERTURBED, p)
@@ -338,6 +341,8 @@ def main():
     ap.add_argument("--elements", type=int, default=64, help="elements per axis")
     ap.add_argument("--n", type=int, default=8, help="GLL nodes per axis")
     ap.add_argument("--precision", choices=["f64", "f32"], default="f64")
+    ap.add_argument("--fp32-form", choices=["bf16x3", "bf16x2", "cuda"], default="bf16x3",
+                    help="FP32 n=8 contractions: split BF16 tensor cores (three / two terms) or CUDA cores")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

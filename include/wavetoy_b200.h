@@ -41,6 +41,12 @@ enum {
 };
 
 enum { WT_F64 = 0, WT_F32 = 1 };
+/* How an FP32 mesh evaluates the n = 8 derivative contractions (the precision
+ * forms of the large-solve study; other n always use CUDA cores):
+ * split-precision BF16 on tensor cores with three-term operands (default,
+ * FP32 accuracy), the same with two-term hi + lo operands, or FP32 on CUDA
+ * cores. */
+enum { WT_FP32_CUDA_CORES = 0, WT_FP32_BF16X3 = 1, WT_FP32_BF16X2 = 2 };
 enum { WT_BC_DIRICHLET = 1, WT_BC_SOMMERFELD = 2, WT_BC_EXCISION = 3, WT_BC_FULL_DIRICHLET = 4 };
 enum { WT_BG_MINKOWSKI = 0, WT_BG_CONSTANT_SHIFT = 1, WT_BG_ADM_PERTURBED = 2, WT_BG_RADIAL_SHIFT = 3 };
 
@@ -119,6 +125,9 @@ int wt_mesh_info(const wt_mesh* mesh, int* N, long long* Ne, int* precision);
 int wt_mesh_get(const wt_mesh* mesh, const char* name, void* host_out);
 /* Override the outer-face tags (6,Ne) int32, e.g. to mark excision faces. */
 int wt_mesh_set_bdry(wt_mesh* mesh, const int32_t* bdry);
+/* Precision form of an FP32 mesh (WT_FP32_*; default WT_FP32_BF16X3).  No
+ * counterpart in the reference (its T = Float32 path uses one form). */
+int wt_mesh_set_fp32_form(wt_mesh* mesh, int form);
 /* _min_node_spacing_3d (src/evolve.jl:60-69); synchronous. */
 int wt_mesh_min_spacing(wt_mesh* mesh, double* h);
 

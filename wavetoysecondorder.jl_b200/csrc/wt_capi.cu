@@ -71,6 +71,11 @@ struct wt_ws {
   void* trace = nullptr;  // 6 N^2 Ne
   void* zero = nullptr;   // nn zeros
   void* Lu = nullptr;     // nn
+  // FP32 state: Kahan compensation of the RK4 step sums of Phi and Pi, kept
+  // while the caller keeps stepping the same state buffers
+  void* compP = nullptr;
+  void* compQ = nullptr;
+  const void* comp_for[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -236,14 +241,11 @@ int derive_geometry(wt_mesh* mh) {
   cudaStream_t s = mh->ctx->stream;
   WT_TRY(lrc(mh->ctx, wt::launch_geom_derived(m, s), "geometry"));
   WT_TRY(lrc(mh->ctx, wt::launch_metric(m, s), "metric terms"));
-  if (m.N == 8 && m.precision == 0) {  // padded element blocks for the pipelined n = 8 kernels
-    WT_TRY(dalloc(mh->ctx, &m.Ja_n8, 9 * (size_t)wt::n8_padded_field_size(m.Ne) * sizeof(double), &mh->owned));
+  WT_TRY(lrc(mh->ctx, wt::launch_streamed_geometry(m, s), "streamed geometry"));
+  if (m.N == 8) {  // padded element blocks (state precision) for the pipelined n = 8 kernels
+    WT_TRY(dalloc(mh->ctx, &m.Ja_n8, 9 * (size_t)wt::n8_padded_field_size(m.Ne) * rsize(m.precision), &mh->owned));
     WT_TRY(lrc(mh->ctx, wt::launch_pad_metric_n8(m, s), "padded metric terms"));
   }
-  if (m.precision == 0) {
-    // Ja_r aliases Ja; still need sdiag
-  }
-  WT_TRY(lrc(mh->ctx, wt::launch_streamed_geometry(m, s), "streamed geometry"));
   WT_TRY(lrc(mh->ctx, wt::launch_boundary_normals(m, s), "boundary normals"));
   mh->ctx->launches += 6;
   cudaError_t e = cudaStreamSynchronize(s);
@@ -280,7 +282,23 @@ int ws_step_buffers(wt_ws* ws) {
   WT_TRY(ensure(ws, &ws->SQ, nb));
   WT_TRY(ensure(ws, &ws->accP, nb));
   WT_TRY(ensure(ws, &ws->accQ, nb));
+  if (m.precision == WT_F32) {
+    WT_TRY(ensure(ws, &ws->compP, nb));
+    WT_TRY(ensure(ws, &ws->compQ, nb));
+  }
   return 0;
+}
+
+// Zero the FP32 compensation when the caller steps other state buffers than
+// last time (a new solve or new initial data in other arrays).
+void comp_track(wt_ws* ws, const void* Phi, const void* Pi) {
+  if (!ws->compP) return;
+  if (ws->comp_for[0] == Phi && ws->comp_for[1] == Pi) return;
+  const size_t nb = (size_t)ws->mesh->m.nn * sizeof(float);
+  cudaMemsetAsync(ws->compP, 0, nb, ws->ctx->stream);
+  cudaMemsetAsync(ws->compQ, 0, nb, ws->ctx->stream);
+  ws->comp_for[0] = Phi;
+  ws->comp_for[1] = Pi;
 }
 
 int ws_k_buffers(wt_ws* ws) {
@@ -616,6 +634,14 @@ int wt_mesh_set_bdry(wt_mesh* mh, const int32_t* bdry) {
   return e == cudaSuccess ? 0 : cuda_fail(mh->ctx, e, "wt_mesh_set_bdry");
 }
 
+int wt_mesh_set_fp32_form(wt_mesh* mh, int form) {
+  if (!mh) return WT_EINVAL;
+  if (form != WT_FP32_CUDA_CORES && form != WT_FP32_BF16X3 && form != WT_FP32_BF16X2)
+    return fail(mh->ctx, WT_EINVAL, "unknown FP32 form " + std::to_string(form));
+  mh->m.fp32_form = form;
+  return 0;
+}
+
 int wt_mesh_min_spacing(wt_mesh* mh, double* h) {
   if (!mh || !h) return WT_EINVAL;
   mh->ctx->launches += 1;
@@ -749,7 +775,7 @@ int wt_workspace_destroy(wt_ws* ws) {
   if (!ws) return WT_EINVAL;
   cudaStreamSynchronize(ws->ctx->stream);
   void* bufs[] = {ws->F, ws->bbuf, ws->grad, ws->kP, ws->kQ, ws->S0, ws->S1, ws->SQ, ws->accP, ws->accQ,
-                  ws->trace, ws->zero, ws->Lu};
+                  ws->trace, ws->zero, ws->Lu, ws->compP, ws->compQ};
   for (void* p : bufs)
     if (p) cudaFree(p);
   delete ws;
@@ -920,8 +946,8 @@ static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* P
     wt::RKStage rkP, rkQ;
     rkP.stage = rkQ.stage = st;
     rkP.dt = rkQ.dt = dt;
-    rkP.y = Phi; rkP.acc = ws->accP; rkP.out = SP[st % 2];
-    rkQ.y = Pi; rkQ.acc = ws->accQ; rkQ.out = ws->SQ;
+    rkP.y = Phi; rkP.acc = ws->accP; rkP.out = SP[st % 2]; rkP.comp = ws->compP;
+    rkQ.y = Pi; rkQ.acc = ws->accQ; rkQ.out = ws->SQ; rkQ.comp = ws->compQ;
     rkP.nonfinite = rkQ.nonfinite = st == 3 ? ctx->d_flag : nullptr;
     if (eps_ko == 0.0) {
       rkP.on = rkQ.on = 1;
@@ -937,8 +963,10 @@ static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* P
       ctx->launches += 2;
     } else {
       WT_TRY(rhs_curved_impl(ctx, ws, coef, inP, inQ, ws->kP, ws->kQ, eps_ko, b, use_metric));
-      WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, st, dt, Phi, ws->accP, SP[st % 2], ws->kP, s), "rk4"));
-      WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, st, dt, Pi, ws->accQ, ws->SQ, ws->kQ, s), "rk4"));
+      WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, st, dt, Phi, ws->accP, SP[st % 2], ws->kP, s,
+                                           ws->compP), "rk4"));
+      WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, st, dt, Pi, ws->accQ, ws->SQ, ws->kQ, s, ws->compQ),
+                 "rk4"));
       ctx->launches += 2;
     }
   }
@@ -991,6 +1019,7 @@ int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, v
   WT_TRY(make_bc(ctx, bc, use_metric, b));
   WT_TRY(ws_step_buffers(ws));
   if (eps_ko != 0.0) WT_TRY(ws_k_buffers(ws));
+  comp_track(ws, Phi, Pi);
   if (nsteps <= 2) {
     for (int i = 0; i < nsteps; ++i) WT_TRY(step_curved_once(ctx, ws, coef, Phi, Pi, dt, eps_ko, b, use_metric));
     return 0;

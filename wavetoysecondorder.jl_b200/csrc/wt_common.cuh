@@ -35,6 +35,7 @@ struct DevMesh {
   int N = 0;
   long long Ne = 0, nn = 0;
   int precision = 0;   // 0 = double, 1 = float
+  int fp32_form = 1;   // FP32 meshes, n = 8: WT_FP32_* of include/wavetoy_b200.h
   int affine = 1;      // 1 if every Jacobian is diagonal and constant per element
   int M[3] = {0, 0, 0};
   // connectivity
@@ -62,7 +63,7 @@ struct DevMesh {
   void* Ja_r = nullptr;      // 9 fields
   void* invdetJ_r = nullptr;
   void* sdiag = nullptr;     // [3e + d] element-constant axis scale invjac[d,d] at node 0
-  double* Ja_n8 = nullptr;   // n = 8 FP64: metric terms in padded element blocks (544 per element)
+  void* Ja_n8 = nullptr;     // n = 8: metric terms in padded element blocks (544 words per element), state precision
   // per element: bits 0-5 faces that get the centred-flux SAT (interior face with a
   // neighbour), bit 6 element has an outer face
   int32_t* emask = nullptr;
@@ -158,6 +159,9 @@ struct RKStage {
   void* y = nullptr;   // state (read; written at stage 3)
   void* acc = nullptr; // accumulator
   void* out = nullptr; // next stage input
+  // FP32 state only: per-node compensation of the stage-3 sum y + increment
+  // (Kahan); with it, acc holds the step increment alone
+  void* comp = nullptr;
   unsigned int* nonfinite = nullptr;  // set to 1 if the stage-3 update is not finite
 };
 // K1: gradient, flux F, Phidot (+ affine/curv BC increments), optional RK epilogue for Phi.
@@ -199,7 +203,7 @@ int launch_scale(long long n, int precision, void* a, double s, cudaStream_t st)
 int launch_fill(long long n, int precision, void* a, double v, cudaStream_t st);
 int launch_copy(long long n, int precision, void* dst, const void* src, cudaStream_t st);
 int launch_rk_update(long long n, int precision, int stage, double dt, void* y, void* acc, void* out,
-                     const void* k, cudaStream_t st);
+                     const void* k, cudaStream_t st, void* comp = nullptr);
 int launch_axpy(long long n, int precision, void* y, double a, const void* x, cudaStream_t st);
 int launch_alt_sign(const DevMesh& m, void* v, cudaStream_t st);
 int launch_finite_check(long long n, int precision, const void* a, unsigned int* flag, cudaStream_t st);

@@ -66,12 +66,39 @@ struct K1P {
   real* y;
   real* acc;
   real* out;
+  real* comp;
   unsigned int* nonfinite;
 };
 
+// Low-storage classic RK4 stage update.  Without compensation acc holds
+// y + partial increments.  With compensation (FP32 state) acc holds the
+// increment of the step alone and the final y + increment is a Kahan sum whose
+// running error term lives in comp, so that small increments are not lost to
+// the rounding of y over many steps.
 template <typename real>
 __device__ __forceinline__ void rk_epilogue(int stage, double dt, real k, real yin, real* y, real* acc, real* out,
-                                            long long n, unsigned int* nonfinite) {
+                                            real* comp, long long n, unsigned int* nonfinite) {
+  if (comp) {
+    if (stage == 0) {
+      out[n] = yin + (real)(0.5 * dt) * k;
+      acc[n] = (real)(dt / 6.0) * k;
+    } else if (stage == 1) {
+      out[n] = y[n] + (real)(0.5 * dt) * k;
+      acc[n] = acc[n] + (real)(dt / 3.0) * k;
+    } else if (stage == 2) {
+      out[n] = y[n] + (real)dt * k;
+      acc[n] = acc[n] + (real)(dt / 3.0) * k;
+    } else {
+      const real inc = acc[n] + (real)(dt / 6.0) * k;
+      const real yv = y[n];
+      const real t = inc - comp[n];
+      const real v = yv + t;
+      comp[n] = (v - yv) - t;
+      y[n] = v;
+      if (nonfinite && !isfinite((double)v)) atomicOr(nonfinite, 1u);
+    }
+    return;
+  }
   if (stage == 0) {
     out[n] = yin + (real)(0.5 * dt) * k;
     acc[n] = yin + (real)(dt / 6.0) * k;
@@ -281,7 +308,7 @@ __global__ void __launch_bounds__(Ep<N>::T) k_cons_k1(const K1P<real> P) {
   P.F[nn + n] = F1;
   P.F[2 * nn + n] = F2;
   if (P.epi)
-    rk_epilogue<real>(P.stage, P.dt, phid, u, P.y, P.acc, P.out, n, P.nonfinite);
+    rk_epilogue<real>(P.stage, P.dt, phid, u, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
   else
     P.Phidot[n] = phid;
 }
@@ -309,6 +336,7 @@ struct K2P {
   real* y;
   real* acc;
   real* out;
+  real* comp;
   unsigned int* nonfinite;
 };
 
@@ -408,7 +436,7 @@ __global__ void __launch_bounds__(Ep<N>::T) k_cons_k2(const K2P<real> P) {
   }
   if (P.epi) {
     const real yin = P.stage == 0 ? P.y[n] : (real)0;
-    rk_epilogue<real>(P.stage, P.dt, dv, yin, P.y, P.acc, P.out, n, P.nonfinite);
+    rk_epilogue<real>(P.stage, P.dt, dv, yin, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
   } else {
     P.Pidot[n] = dv;
   }
@@ -547,7 +575,7 @@ static int k1_dispatch(const DevMesh& m, const DevCoef& c, const void* Phi, cons
   P.gPhi = (const real*)bc.gPhi; P.gPi = (const real*)bc.gPi;
   P.gDx = (const real*)bc.gDx; P.gDy = (const real*)bc.gDy; P.gDz = (const real*)bc.gDz;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
-  P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.nonfinite = rk.nonfinite;
+  P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.nonfinite = rk.nonfinite;
   const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
   if (use_metric)
     k_cons_k1<N, real, true><<<blocks, Ep<N>::T, 0, s>>>(P);
@@ -571,7 +599,7 @@ static int k2_dispatch(const DevMesh& m, const void* F, void* Pidot, const void*
   P.bbuf = (const real*)bbuf; P.bc_on = bc.on;
   P.Pidot = (real*)Pidot;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
-  P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.nonfinite = nonfinite;
+  P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.nonfinite = nonfinite;
   const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
   if (use_metric)
     k_cons_k2<N, real, true><<<blocks, Ep<N>::T, 0, s>>>(P);
@@ -598,7 +626,8 @@ static inline bool a16(const void* p) { return p == nullptr || ((uintptr_t)p & 1
 // need 16-byte aligned global addresses; anything else takes the generic path.
 bool cons_n8_path(const DevMesh& m, const DevCoef& c, int use_metric, const ConsBC& bc, const RKStage& rkP,
                   const RKStage& rkQ, std::initializer_list<const void*> ptrs) {
-  if (m.N != 8 || m.precision != 0 || !use_metric || m.Ja_n8 == nullptr) return false;
+  if (m.N != 8 || !use_metric || m.Ja_n8 == nullptr) return false;
+  if (m.precision == 1 && m.fp32_form == 0) return false;  // FP32 on CUDA cores: the generic kernels
   if (c.c10 == nullptr) return false;
   if (bc.on && !bc.curv) return false;
   for (const RKStage* rk : {&rkP, &rkQ})

@@ -1,5 +1,5 @@
-// wt_cons_n8.cu -- the n = 8 FP64 curvilinear hot path as persistent,
-// TMA-pipelined, tensor-core kernels.
+// wt_cons_n8.cu -- the n = 8 curvilinear hot path as persistent,
+// bulk-copy-pipelined, tensor-core kernels, in two precision forms.
 //
 // Same arithmetic as k_cons_k1 / k_cons_k2 in wt_cons.cu (the split-form
 // gradient / flux / Phidot and the split-form divergence of
@@ -12,40 +12,59 @@
 //     and the metric terms in K2) are staged into shared memory with 1D bulk
 //     copies (cp.async.bulk ... mbarrier::complete_tx), one copy per field
 //     block; the metric terms and the flux live in global memory in a
-//     plane-padded element layout (k-plane stride 68 doubles) that makes the
+//     plane-padded element layout (k-plane stride 68 words) that makes the
 //     tensor-core operand loads (nearly) bank-conflict-free.  A ring of
 //     NSTAGE stages keeps NSTAGE - 1 elements in flight; every wait is
 //     bounded and raises an error flag instead of spinning forever;
 //   * the fields used only at their own node (background coefficients, Pi,
 //     1/J, the RK4 state) are prefetched into registers one element ahead;
-//   * the 8x8 reference-derivative contractions run on the FP64 tensor cores
-//     (mma.sync.m8n8k4.f64): for axis al an element's 64 pencils are the N
-//     dimension, G the A operand (in registers), the staged field -- or the
-//     split-form product Ja*u / Ja.F formed while loading -- the B operand.
-//     Warp w owns pencil tile w&7; warps w and w+8 split the fields of a tile,
-//     and every axis writes its own partial sums, so one barrier separates
-//     the contraction pass from the node pass.  The centred-flux SATs are
-//     added in the same pass: an output row l = 0 or 7 of the MMA is the node
-//     row on face 2al or 2al+1;
+//   * the 8x8 reference-derivative contractions run on tensor cores.  For
+//     axis al an element's 64 pencils form 8 tiles of 8 (the MMA N
+//     dimension); warp w owns tile w&7 and warps w and w+8 split the fields
+//     of a tile.  Every axis writes its own partial sums, so one barrier
+//     separates the contraction pass from the node pass.  The centred-flux
+//     SATs are added in the same pass: output row l = 0 or 7 of the MMA is
+//     the node row on face 2al or 2al+1.
+//       FP64 form: mma.sync.m8n8k4.f64, G the A operand in registers, the
+//       staged field -- or the split-form product Ja*u / Ja.F formed while
+//       loading -- the B operand.
+//       FP32 forms: split-precision BF16, mma.sync.m16n8k16 with FP32
+//       accumulation.  Three-term split (default): G and the operand v are
+//       split into bf16 terms hi + mid + lo (24 significant bits, as FP32);
+//       MMA 1 with A = [[G_hi, G_hi], [G_mid, G_mid]], B = [v_hi; v_mid] and
+//       MMA 2 with A = [[G_hi, G_lo], [G_mid, 0]], B = [v_lo; v_hi] sum every
+//       product down to relative size 2^-16 (rows 0-7 and 8-15 added in
+//       FP32).  Two-term split (hi + lo): one MMA with A = [[G_hi, G_hi],
+//       [G_lo, G_lo]], B = [v_hi; v_lo]; it carries ~16 significant bits and
+//       misses FP32 accuracy by a factor of ~30 on the n = 8 warped workload,
+//       so it is kept only for the precision study.  Because every row of G
+//       sums to zero, the operand is taken relative to its value at node 3 of
+//       the pencil (D(v - c) = D v), so the split error scales with the
+//       variation of the field along the pencil, not with its size;
 //   * a node phase (one node per thread) forms flux, Phidot / divergence,
 //     boundary terms (boundary elements only) and the RK4 stage update and
-//     writes coalesced results;
+//     writes coalesced results (FP32 form: Kahan-compensated final sum);
 //   * per-element tables (SAT face mask, neighbour face sources) are loaded
 //     one element before the neighbour traces they address, so no load in
 //     the loop waits on another load.
 #include "wt_common.cuh"
+#include "../../include/wavetoy_b200.h"
+
+#include <cuda_bf16.h>
+#include <type_traits>
 
 namespace wt {
 
 namespace n8 {
 
 constexpr int N = 8, N2 = 64, N3 = 512, THREADS = 512;
-constexpr int PS = 68;             // padded k-plane stride (doubles)
-constexpr int FS = 8 * PS;         // padded field size (544 doubles = 4352 B)
+constexpr int PS = 68;             // padded k-plane stride (words)
+constexpr int FS = 8 * PS;         // padded field size (544 words)
 constexpr long long WAIT_LIMIT = 1LL << 24;
 // staged elements in flight: element e + (NSTAGE - 1) * grid is copied while e
 // is processed
 constexpr int NSTAGE = 2;
+constexpr int PREF = 3;            // FP32 form: pencil node whose value is the operand offset
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
@@ -81,26 +100,52 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
+__device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
+
+// D (16x8, FP32) += A (16x16 bf16, row) * B (16x8 bf16, col); b0 holds rows
+// k = 2 tig, 2 tig + 1 and b1 rows k = 8 + 2 tig, 9 + 2 tig of column n = group.
+__device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// Split-precision contraction of the two operand values this lane holds
+// (positions 2 tig, 2 tig + 1 of pencil `group`): NT = 3 three-term split
+// (two MMAs, a1/a2 from split_G), NT = 2 hi + lo (one MMA with a1).
+template <int NT>
+__device__ __forceinline__ void mma_split(float d[4], const uint32_t a1[4], const uint32_t a2[4], float v0, float v1) {
+  const __nv_bfloat162 hi = __floats2bfloat162_rn(v0, v1);
+  const float2 hf = __bfloat1622float2(hi);
+  const float r0 = v0 - hf.x, r1 = v1 - hf.y;
+  const __nv_bfloat162 mid = __floats2bfloat162_rn(r0, r1);
+  if constexpr (NT == 2) {
+    mma_bf16(d, a1, bf2_bits(hi), bf2_bits(mid));
+  } else {
+    const float2 mf = __bfloat1622float2(mid);
+    const __nv_bfloat162 lo = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
+    mma_bf16(d, a1, bf2_bits(hi), bf2_bits(mid));
+    mma_bf16(d, a2, bf2_bits(lo), bf2_bits(hi));
+  }
+}
+
 __device__ __forceinline__ int pad(int i, int j, int k) { return i + 8 * j + PS * k; }
 // padded index -> unpadded node index (i + 8 j + 64 k)
 __device__ __forceinline__ int unpad(int d) { return d - (PS - 64) * (d / PS); }
 
-// Per-lane operand / output node offsets (padded) for axis al, tile w:
-//   B operand: position p = 4 kc + tig along al, pencil slot g;
-//   outputs:   row l = g along al, pencil slot 2 tig + b.
+// Padded node of tile w for axis al at position p along al, pencil slot g.
 // Pencil orders: al=0 (j = w, k = slot); al=1 (i = slot, k = w); al=2 (i = slot, j = w).
-__device__ __forceinline__ int bnode(int al, int w, int kc, int g, int tig) {
-  const int p = 4 * kc + tig;
+__device__ __forceinline__ int bn(int al, int w, int p, int g) {
   return al == 0 ? pad(p, w, g) : al == 1 ? pad(g, p, w) : pad(g, w, p);
 }
-__device__ __forceinline__ int onode(int al, int w, int b, int g, int tig) {
-  const int sl = 2 * tig + b;
-  return al == 0 ? pad(g, w, sl) : al == 1 ? pad(sl, g, w) : pad(sl, w, g);
-}
+// FP64 B operand: position p = 4 kc + tig along al, pencil slot g
+__device__ __forceinline__ int bnode(int al, int w, int kc, int g, int tig) { return bn(al, w, 4 * kc + tig, g); }
+// outputs (both forms): row l = g along al, pencil slot 2 tig + b
+__device__ __forceinline__ int onode(int al, int w, int b, int g, int tig) { return bn(al, w, g, 2 * tig + b); }
 // face-trace index (p + 8 q) of an output node on the al-face
 __device__ __forceinline__ int opq(int al, int w, int b, int tig) {
   const int sl = 2 * tig + b;
-  return al == 0 ? w + 8 * sl : al == 1 ? sl + 8 * w : sl + 8 * w;
+  return al == 0 ? w + 8 * sl : sl + 8 * w;
 }
 
 __device__ __forceinline__ bool wait_phase(uint64_t* bar, unsigned parity, unsigned* err) {
@@ -110,16 +155,87 @@ __device__ __forceinline__ bool wait_phase(uint64_t* bar, unsigned parity, unsig
   return false;
 }
 
+// A operand fragments of the FP32 forms (register i: rows gq / gq + 8 for
+// i = 0, 2 / 1, 3; columns k < 8 for i < 2, k >= 8 otherwise).
+//   NT = 3: a1 = [[G_hi, G_hi], [G_mid, G_mid]], a2 = [[G_hi, G_lo], [G_mid, 0]]
+//   NT = 2: a1 = [[G_hi, G_hi], [G_lo, G_lo]]   (G_lo = the second term)
+__device__ __forceinline__ void split_G(const double* G, int gq, int tig, int nt, uint32_t a1[4], uint32_t a2[4]) {
+  const double g0 = G[gq * 8 + 2 * tig], g1 = G[gq * 8 + 2 * tig + 1];
+  const __nv_bfloat162 hi = __floats2bfloat162_rn((float)g0, (float)g1);
+  const float2 hf = __bfloat1622float2(hi);
+  const double r0 = g0 - (double)hf.x, r1 = g1 - (double)hf.y;
+  const __nv_bfloat162 mid = __floats2bfloat162_rn((float)r0, (float)r1);
+  const float2 mf = __bfloat1622float2(mid);
+  const __nv_bfloat162 lo = __floats2bfloat162_rn((float)(r0 - (double)mf.x), (float)(r1 - (double)mf.y));
+  a1[0] = bf2_bits(hi);
+  a1[1] = bf2_bits(mid);
+  a1[2] = bf2_bits(hi);
+  a1[3] = bf2_bits(mid);
+  a2[0] = bf2_bits(hi);
+  a2[1] = bf2_bits(mid);
+  a2[2] = nt == 3 ? bf2_bits(lo) : 0u;
+  a2[3] = 0u;
+}
+
+// resident CTAs per SM
+template <typename real>
+struct Occ {
+  static constexpr int k1 = 1, k2 = 1;
+};
+
 }  // namespace n8
 
+// RK4 stage update shared by both kernels (see rk_epilogue in wt_cons.cu):
+// with comp (FP32 state) acc holds the step increment and the final sum is
+// Kahan-compensated; yv, accv, compv are this node's prefetched values.
+template <typename real>
+__device__ __forceinline__ void n8_rk(int stage, double dt, real k, real yin, real yv, real accv, real compv,
+                                      long long n, real* y, real* acc, real* out, real* comp, unsigned* flag) {
+  if (comp) {
+    if (stage == 0) {
+      out[n] = yin + (real)(0.5 * dt) * k;
+      acc[n] = (real)(dt / 6.0) * k;
+    } else if (stage == 1) {
+      out[n] = yv + (real)(0.5 * dt) * k;
+      acc[n] = accv + (real)(dt / 3.0) * k;
+    } else if (stage == 2) {
+      out[n] = yv + (real)dt * k;
+      acc[n] = accv + (real)(dt / 3.0) * k;
+    } else {
+      const real inc = accv + (real)(dt / 6.0) * k;
+      const real t = inc - compv;
+      const real v = yv + t;
+      comp[n] = (v - yv) - t;
+      y[n] = v;
+      if (flag && !isfinite(v)) atomicOr(flag, 1u);
+    }
+    return;
+  }
+  if (stage == 0) {
+    out[n] = yin + (real)(0.5 * dt) * k;
+    acc[n] = yin + (real)(dt / 6.0) * k;
+  } else if (stage == 1) {
+    out[n] = yv + (real)(0.5 * dt) * k;
+    acc[n] = accv + (real)(dt / 3.0) * k;
+  } else if (stage == 2) {
+    out[n] = yv + (real)dt * k;
+    acc[n] = accv + (real)(dt / 3.0) * k;
+  } else {
+    const real v = accv + (real)(dt / 6.0) * k;
+    y[n] = v;
+    if (flag && !isfinite(v)) atomicOr(flag, 1u);
+  }
+}
+
 // ---------------------------------------------------------------------------
+template <typename real>
 struct K1N8 {
   long long Ne, nn;
-  const double* Phi;
-  const double* Pi;
-  const double* c10;
-  const double* Ja;
-  const double* invdetJ;
+  const real* Phi;
+  const real* Pi;
+  const real* c10;
+  const real* Ja;
+  const real* invdetJ;
   const int32_t* nbr;
   const int32_t* nbrf;
   const int32_t* bdry;
@@ -128,47 +244,56 @@ struct K1N8 {
   const int32_t* fsrc;
   const double* G;
   const double* H;
-  double* F;
-  double* Phidot;
-  double* bbuf;
+  real* F;
+  real* Phidot;
+  real* bbuf;
   int bc_on, exc_tag, nbf, kind;
   double sigma;
-  const double* bnorm;
-  const double* gPhi;
-  const double* gPi;
-  const double* gDx;
-  const double* gDy;
-  const double* gDz;
+  const real* bnorm;
+  const real* gPhi;
+  const real* gPi;
+  const real* gDx;
+  const real* gDy;
+  const real* gDz;
   int epi, stage;
   double dt;
-  double* y;
-  double* acc;
-  double* out;
+  real* y;
+  real* acc;
+  real* out;
+  real* comp;
   unsigned* flag;
 };
 
-// K1 staged fields: Phi (unpadded, 512) and Ja (9 padded fields, one 4352-byte
-// block each from the padded global copy).  Register prefetch: c10 (10), Pi,
-// invJ, y, acc.
+// K1 staged fields: Phi (unpadded, 512) and Ja (9 padded fields, one block
+// each from the padded global copy).  Register prefetch: c10 (10), Pi, invJ,
+// y, acc, comp.
 constexpr size_t K1_STAGE = (size_t)n8::N3 + 9 * (size_t)n8::FS;
-constexpr size_t K1_SMEM = (n8::NSTAGE * K1_STAGE + 9 * n8::FS + 2 * 6 * n8::N2 + n8::N2) * sizeof(double) + 64;
+template <typename real>
+constexpr size_t k1_smem() {
+  return (n8::NSTAGE * K1_STAGE + 9 * n8::FS + 2 * 6 * n8::N2) * sizeof(real) + n8::N2 * sizeof(double) + 64;
+}
 
-__global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
+// NT: FP32 split terms (3 or 2); ignored by the FP64 form
+template <typename real, int NT>
+__global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(const K1N8<real> P) {
   using namespace n8;
+  constexpr bool F64 = std::is_same<real, double>::value;
   extern __shared__ __align__(128) unsigned char smraw[];
-  double* stg = reinterpret_cast<double*>(smraw);       // 2 stages x 10 padded fields
-  double* sg = stg + NSTAGE * K1_STAGE;                      // 9 padded partial gradients [al*3 + c]
-  double* sface = sg + 9 * FS;                          // 2 x 6 x 64
-  double* sG = sface + 2 * 6 * N2;                      // 64
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);  // NSTAGE
+  double* sG = reinterpret_cast<double*>(smraw);                // 64 (FP64 operator)
+  real* stg = reinterpret_cast<real*>(sG + N2);                 // NSTAGE stages x 10 fields
+  real* sg = stg + NSTAGE * K1_STAGE;                           // 9 padded partial gradients [al*3 + c]
+  real* sface = sg + 9 * FS;                                    // 2 x 6 x 64
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sface + 2 * 6 * N2);  // NSTAGE
   __shared__ int abort_flag;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
   const long long nn = P.nn;
-  const double inv2H = 1.0 / (2.0 * P.H[0]);
-  const bool need_y = P.epi && (P.stage == 1 || P.stage == 2);
+  const real inv2H = (real)(1.0 / (2.0 * P.H[0]));
+  const bool comp_on = !F64 && P.epi && P.comp != nullptr;  // FP32 state only
+  const bool need_y = P.epi && (P.stage == 1 || P.stage == 2 || (comp_on && P.stage == 3));
   const bool need_acc = P.epi && P.stage >= 1;
-  const unsigned tx_bytes = N3 * 8u + 9u * FS * 8u;
+  const bool need_comp = comp_on && P.stage == 3;
+  const unsigned tx_bytes = (unsigned)((N3 + 9 * FS) * sizeof(real));
   // node-phase coordinates of this thread
   const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
   const int tpad = pad(ti, tj, tk);
@@ -188,24 +313,25 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
       mbar_expect_tx(&bar[s], tx_bytes);
     }
     __syncwarp();
-    double* d = stg + s * K1_STAGE;
-    if (lane == 0) bulk_g2s(d, P.Phi + e * N3, N3 * 8u, &bar[s]);
+    real* d = stg + s * K1_STAGE;
+    if (lane == 0) bulk_g2s(d, P.Phi + e * N3, N3 * (unsigned)sizeof(real), &bar[s]);
     else if (lane <= 9)
-      bulk_g2s(d + N3 + (lane - 1) * FS, P.Ja + ((long long)(lane - 1) * P.Ne + e) * FS, FS * 8u, &bar[s]);
+      bulk_g2s(d + N3 + (lane - 1) * FS, P.Ja + ((long long)(lane - 1) * P.Ne + e) * FS, FS * (unsigned)sizeof(real),
+               &bar[s]);
   };
   // neighbour Phi face traces (384 values; threads 0..383).  The face source
   // (8 * neighbour + neighbour face) of an element is loaded one iteration
   // before the trace itself, so no load waits on another inside the loop.
   const int my_f = tid >> 6, my_pq = tid & 63;
   auto src_load = [&](long long e) -> int { return (e >= 0 && tid < 6 * N2) ? P.fsrc[my_f + 6 * e] : -1; };
-  auto face_load = [&](int src) -> double {
-    if (src < 0) return 0.0;
+  auto face_load = [&](int src) -> real {
+    if (src < 0) return (real)0;
     const int fn = src & 7;
     return P.Phi[(long long)(src >> 3) * N3 + face_node(faxis(fn), frow(fn, N), my_pq & 7, my_pq >> 3, N)];
   };
   // pointwise fields of this thread's node
   struct PW {
-    double c[10], Pi, invJ, y, acc;
+    real c[10], Pi, invJ, y, acc, comp;
   };
   auto pw_load = [&](long long e, PW& w) {
     if (e < 0) return;
@@ -214,8 +340,9 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     for (int c = 0; c < 10; ++c) w.c[c] = P.c10[c * nn + n];
     w.Pi = P.Pi[n];
     w.invJ = P.invdetJ[n];
-    w.y = need_y ? P.y[n] : 0.0;
-    w.acc = need_acc ? P.acc[n] : 0.0;
+    w.y = need_y ? P.y[n] : (real)0;
+    w.acc = need_acc ? P.acc[n] : (real)0;
+    w.comp = need_comp ? P.comp[n] : (real)0;
   };
 
   long long e = blockIdx.x;
@@ -226,13 +353,21 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
       for (int k = 0; k < NSTAGE - 1; ++k)
         if (e + k * (long long)gridDim.x < P.Ne) issue(e + k * (long long)gridDim.x, k);
     emcur = P.emask[e];
-    const double fv = face_load(src_load(e));
+    const real fv = face_load(src_load(e));
     if (tid < 6 * N2) sface[tid] = fv;
     pw_load(e, cur);
     src1 = src_load(e + gridDim.x < P.Ne ? e + gridDim.x : -1);
   }
   __syncthreads();
-  const double aG0 = sG[gq * 8 + tig], aG1 = sG[gq * 8 + 4 + tig];
+  // A operand: FP64 G entries (rows gq, columns tig and 4 + tig); FP32 split pairs
+  double aG0 = 0.0, aG1 = 0.0;
+  uint32_t aS[4] = {0, 0, 0, 0}, aS2[4] = {0, 0, 0, 0};
+  if constexpr (F64) {
+    aG0 = sG[gq * 8 + tig];
+    aG1 = sG[gq * 8 + 4 + tig];
+  } else {
+    split_G(sG, gq, tig, NT, aS, aS2);
+  }
 
   for (int it = 0; e < P.Ne; ++it, e += gridDim.x) {
     const int s = it % NSTAGE, fb = it & 1;
@@ -241,7 +376,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     const bool has_next = en < P.Ne;
     const int emnext = has_next ? P.emask[en] : 0;
     const int src2 = src_load(enn < P.Ne ? enn : -1);
-    const double fnext = face_load(has_next ? src1 : -1);
+    const real fnext = face_load(has_next ? src1 : -1);
     PW nxt;
     pw_load(has_next ? en : -1, nxt);
     if (!wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
@@ -259,10 +394,10 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
       const long long ei = e + (NSTAGE - 1) * (long long)gridDim.x;
       if (warp == 0 && ei < P.Ne) issue(ei, (it + NSTAGE - 1) % NSTAGE);
     }
-    const double* d = stg + s * K1_STAGE;
-    const double* sPhi = d;      // unpadded
-    const double* sJa = d + N3;  // 9 padded fields, index (al*3 + c)
-    const double* sfc = sface + fb * 6 * N2;
+    const real* d = stg + s * K1_STAGE;
+    const real* sPhi = d;      // unpadded
+    const real* sJa = d + N3;  // 9 padded fields, index (al*3 + c)
+    const real* sfc = sface + fb * 6 * N2;
     const int mask = emcur & 63;
     const int bnd = emcur >> 6;
     // ---- tensor-core contractions ----
@@ -274,29 +409,56 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     // of an interior al-face is added to the output rows on that face (row 0:
     // face 2 al, row 7: face 2 al + 1).
     auto grad_axis = [&](int al, int comps) {
-      double cu[2] = {0, 0}, cm[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+      real cu[2], cm[3][2];
+      if constexpr (F64) {
+        double du[2] = {0, 0}, dm[3][2] = {{0, 0}, {0, 0}, {0, 0}};
 #pragma unroll
-      for (int kc = 0; kc < 2; ++kc) {
-        const int nd = bnode(al, wt8, kc, gq, tig);
-        const double u = sPhi[unpad(nd)];
-        const double a = kc ? aG1 : aG0;
-        dmma(cu[0], cu[1], a, u);
+        for (int kc = 0; kc < 2; ++kc) {
+          const int nd = bnode(al, wt8, kc, gq, tig);
+          const double u = sPhi[unpad(nd)];
+          const double a = kc ? aG1 : aG0;
+          dmma(du[0], du[1], a, u);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            if ((comps >> c) & 1) dmma(dm[c][0], dm[c][1], a, sJa[(al * 3 + c) * FS + nd] * u);
+        }
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          cu[b] = du[b];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) cm[c][b] = dm[c][b];
+        }
+      } else {
+        const int nd0 = bn(al, wt8, 2 * tig, gq), nd1 = bn(al, wt8, 2 * tig + 1, gq), ndr = bn(al, wt8, PREF, gq);
+        const float u0 = sPhi[unpad(nd0)], u1 = sPhi[unpad(nd1)], ur = sPhi[unpad(ndr)];
+        float fu[4] = {0, 0, 0, 0}, fm[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+        mma_split<NT>(fu, aS, aS2, u0 - ur, u1 - ur);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          if ((comps >> c) & 1) dmma(cm[c][0], cm[c][1], a, sJa[(al * 3 + c) * FS + nd] * u);
+          if ((comps >> c) & 1) {
+            const real* mc = sJa + (al * 3 + c) * FS;
+            const float pr = mc[ndr] * ur;
+            mma_split<NT>(fm[c], aS, aS2, fmaf(mc[nd0], u0, -pr), fmaf(mc[nd1], u1, -pr));
+          }
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          cu[b] = fu[b] + fu[b + 2];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) cm[c][b] = fm[c][b] + fm[c][b + 2];
+        }
       }
       const int sface_f = gq == 0 ? 2 * al : gq == 7 ? 2 * al + 1 : -1;
       const bool sat = sface_f >= 0 && ((mask >> sface_f) & 1);
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         const int no = onode(al, wt8, b, gq, tig);
-        double jump = 0.0;
+        real jump = 0;
         if (sat) jump = (gq ? inv2H : -inv2H) * (sfc[sface_f * N2 + opq(al, wt8, b, tig)] - sPhi[unpad(no)]);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
           if ((comps >> c) & 1) {
-            const double m = sJa[(al * 3 + c) * FS + no];
-            double r = 0.5 * cm[c][b] + 0.5 * m * cu[b];
+            const real m = sJa[(al * 3 + c) * FS + no];
+            real r = (real)0.5 * cm[c][b] + (real)0.5 * m * cu[b];
             if (sat) r += m * jump;
             sg[(al * 3 + c) * FS + no] = r;
           }
@@ -313,19 +475,19 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
     // ---- node phase: one node per thread ----
     {
       const long long n = e * N3 + tid;
-      const double u = sPhi[tid];
-      double g0 = (sg[tpad] + sg[3 * FS + tpad]) + sg[6 * FS + tpad];
-      double g1 = (sg[FS + tpad] + sg[4 * FS + tpad]) + sg[7 * FS + tpad];
-      double g2 = (sg[2 * FS + tpad] + sg[5 * FS + tpad]) + sg[8 * FS + tpad];
+      const real u = sPhi[tid];
+      real g0 = (sg[tpad] + sg[3 * FS + tpad]) + sg[6 * FS + tpad];
+      real g1 = (sg[FS + tpad] + sg[4 * FS + tpad]) + sg[7 * FS + tpad];
+      real g2 = (sg[2 * FS + tpad] + sg[5 * FS + tpad]) + sg[8 * FS + tpad];
       g0 *= cur.invJ; g1 *= cur.invJ; g2 *= cur.invJ;
-      const double a = cur.c[0];
-      const double b0 = cur.c[1], b1 = cur.c[2], b2 = cur.c[3];
-      const double K0 = cur.c[4], K1v = cur.c[5], K2 = cur.c[6], K3 = cur.c[7], K4 = cur.c[8], K5 = cur.c[9];
-      const double Pi = cur.Pi;
-      const double F0 = b0 * Pi + (K0 * g0 + K1v * g1 + K2 * g2);
-      const double F1 = b1 * Pi + (K1v * g0 + K3 * g1 + K4 * g2);
-      const double F2 = b2 * Pi + (K2 * g0 + K4 * g1 + K5 * g2);
-      double phid = b0 * g0 + b1 * g1 + b2 * g2 + a * Pi;
+      const real a = cur.c[0];
+      const real b0 = cur.c[1], b1 = cur.c[2], b2 = cur.c[3];
+      const real K0 = cur.c[4], K1v = cur.c[5], K2 = cur.c[6], K3 = cur.c[7], K4 = cur.c[8], K5 = cur.c[9];
+      const real Pi = cur.Pi;
+      const real F0 = b0 * Pi + (K0 * g0 + K1v * g1 + K2 * g2);
+      const real F1 = b1 * Pi + (K1v * g0 + K3 * g1 + K4 * g2);
+      const real F2 = b2 * Pi + (K2 * g0 + K4 * g1 + K5 * g2);
+      real phid = b0 * g0 + b1 * g1 + b2 * g2 + a * Pi;
       if (bnd && P.bc_on) {
         const int idx3[3] = {ti, tj, tk};
         for (int f = 0; f < 6; ++f) {
@@ -335,30 +497,32 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
           if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
           const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
           const int slot = P.bslot[f + 6 * e];
-          double dF = 0.0, dP = 0.0;
+          real dF = 0, dP = 0;
           if (tag != P.exc_tag) {
             const long long nb = (long long)P.nbf * N2;
             const long long bi = (long long)slot * N2 + p + 8 * q;
-            const double nx = P.bnorm[bi], ny = P.bnorm[nb + bi], nz = P.bnorm[2 * nb + bi], wt = P.bnorm[3 * nb + bi];
-            const double Kn =
-                K0 * nx * nx + K3 * ny * ny + K5 * nz * nz + 2.0 * (K1v * nx * ny + K2 * nx * nz + K4 * ny * nz);
-            const double a_n = sqrt(a * Kn);
-            const double bn = b0 * nx + b1 * ny + b2 * nz;
+            const real nx = P.bnorm[bi], ny = P.bnorm[nb + bi], nz = P.bnorm[2 * nb + bi], wt = P.bnorm[3 * nb + bi];
+            const real Kn =
+                K0 * nx * nx + K3 * ny * ny + K5 * nz * nz + (real)2 * (K1v * nx * ny + K2 * nx * nz + K4 * ny * nz);
+            const real a_n = sqrt(a * Kn);
+            const real bn_ = b0 * nx + b1 * ny + b2 * nz;
+            const real sigma = (real)P.sigma;
             if (P.kind == 4) {
-              const double tau = P.sigma * (fabs(a_n - bn) + fabs(a_n + bn)) * wt;
-              const double gp = P.gPhi ? P.gPhi[n] : 0.0, gqv = P.gPi ? P.gPi[n] : 0.0;
+              const real tau = sigma * (fabs(a_n - bn_) + fabs(a_n + bn_)) * wt;
+              const real gp = P.gPhi ? P.gPhi[n] : (real)0, gqv = P.gPi ? P.gPi[n] : (real)0;
               dF = -tau * (u - gp);
               dP = -tau * (Pi - gqv);
             } else {
-              const double qv = nx * g0 + ny * g1 + nz * g2;
-              const double rr = Pi + ((bn + a_n) / a) * qv;
-              double gv = 0.0;
+              const real qv = nx * g0 + ny * g1 + nz * g2;
+              const real rr = Pi + ((bn_ + a_n) / a) * qv;
+              real gv = 0;
               if (P.kind != 2) {
-                const double gqv = P.gPi ? P.gPi[n] : 0.0;
-                const double gx = P.gDx ? P.gDx[n] : 0.0, gy = P.gDy ? P.gDy[n] : 0.0, gz = P.gDz ? P.gDz[n] : 0.0;
-                gv = gqv + ((bn + a_n) / a) * (nx * gx + ny * gy + nz * gz);
+                const real gqv = P.gPi ? P.gPi[n] : (real)0;
+                const real gx = P.gDx ? P.gDx[n] : (real)0, gy = P.gDy ? P.gDy[n] : (real)0,
+                           gz = P.gDz ? P.gDz[n] : (real)0;
+                gv = gqv + ((bn_ + a_n) / a) * (nx * gx + ny * gy + nz * gz);
               }
-              dP = -P.sigma * fabs(a_n + bn) * wt * (rr - gv);
+              dP = -sigma * fabs(a_n + bn_) * wt * (rr - gv);
             }
           }
           phid += dF;
@@ -371,25 +535,11 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
         P.F[fstr + fo] = F1;
         P.F[2 * fstr + fo] = F2;
       }
-      if (P.epi) {
-        const double dt = P.dt;
-        if (P.stage == 0) {
-          P.out[n] = u + (0.5 * dt) * phid;
-          P.acc[n] = u + (dt / 6.0) * phid;
-        } else if (P.stage == 1) {
-          P.out[n] = cur.y + (0.5 * dt) * phid;
-          P.acc[n] = cur.acc + (dt / 3.0) * phid;
-        } else if (P.stage == 2) {
-          P.out[n] = cur.y + dt * phid;
-          P.acc[n] = cur.acc + (dt / 3.0) * phid;
-        } else {
-          const double v = cur.acc + (dt / 6.0) * phid;
-          P.y[n] = v;
-          if (P.flag && !isfinite(v)) atomicOr(P.flag, 1u);
-        }
-      } else {
+      if (P.epi)
+        n8_rk<real>(P.stage, P.dt, phid, u, cur.y, cur.acc, cur.comp, n, P.y, P.acc, P.out, comp_on ? P.comp : nullptr,
+                    P.flag);
+      else
         P.Phidot[n] = phid;
-      }
     }
     if (has_next && tid < 6 * N2) sface[(fb ^ 1) * 6 * N2 + tid] = fnext;
     cur = nxt;
@@ -399,13 +549,14 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k1_n8(const K1N8 P) {
 }
 
 // ---------------------------------------------------------------------------
+template <typename real>
 struct K2N8 {
   long long Ne, nn;
-  const double* F0;
-  const double* F1;
-  const double* F2;
-  const double* Ja;
-  const double* invdetJ;
+  const real* F0;
+  const real* F1;
+  const real* F2;
+  const real* Ja;
+  const real* invdetJ;
   const int32_t* nbr;
   const int32_t* nbrf;
   const int32_t* bdry;
@@ -414,37 +565,45 @@ struct K2N8 {
   const int32_t* fsrc;
   const double* G;
   const double* H;
-  const double* bbuf;
+  const real* bbuf;
   int bc_on;
-  double* Pidot;
+  real* Pidot;
   int epi, stage;
   double dt;
-  double* y;
-  double* acc;
-  double* out;
+  real* y;
+  real* acc;
+  real* out;
+  real* comp;
   unsigned* flag;
 };
 
-// K2 staged fields: 0..2 F, 3..11 Ja.  Register prefetch: invJ, y, acc.
+// K2 staged fields: 0..2 F, 3..11 Ja.  Register prefetch: invJ, y, acc, comp.
 constexpr int K2_NF = 12;
 constexpr size_t K2_STAGE = (size_t)K2_NF * n8::FS;
-constexpr size_t K2_SMEM = (n8::NSTAGE * K2_STAGE + 6 * n8::FS + 2 * 6 * 3 * n8::N2 + n8::N2) * sizeof(double) + 64;
+template <typename real>
+constexpr size_t k2_smem() {
+  return (n8::NSTAGE * K2_STAGE + 6 * n8::FS + 2 * 6 * 3 * n8::N2) * sizeof(real) + n8::N2 * sizeof(double) + 64;
+}
 
-__global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
+template <typename real, int NT>
+__global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2) k_cons_k2_n8(const K2N8<real> P) {
   using namespace n8;
+  constexpr bool F64 = std::is_same<real, double>::value;
   extern __shared__ __align__(128) unsigned char smraw[];
-  double* stg = reinterpret_cast<double*>(smraw);
-  double* sdiv = stg + NSTAGE * K2_STAGE;                     // 6 padded partial divergences [al*2 + half]
-  double* sface = sdiv + 6 * FS;                         // 2 x 6 x 3 x 64
-  double* sG = sface + 2 * 6 * 3 * N2;                   // 64
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sG + N2);
+  double* sG = reinterpret_cast<double*>(smraw);                   // 64
+  real* stg = reinterpret_cast<real*>(sG + N2);
+  real* sdiv = stg + NSTAGE * K2_STAGE;                            // 6 padded partial divergences [al*2 + half]
+  real* sface = sdiv + 6 * FS;                                     // 2 x 6 x 3 x 64
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sface + 2 * 6 * 3 * N2);
   __shared__ int abort_flag;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
-  const double inv2H = 1.0 / (2.0 * P.H[0]);
-  const bool need_y = P.epi && P.stage <= 2;
+  const real inv2H = (real)(1.0 / (2.0 * P.H[0]));
+  const bool comp_on = !F64 && P.epi && P.comp != nullptr;  // FP32 state only
+  const bool need_y = P.epi && (P.stage <= 2 || (comp_on && P.stage == 3));
   const bool need_acc = P.epi && P.stage >= 1;
-  const unsigned tx_bytes = K2_NF * FS * 8u;
+  const bool need_comp = comp_on && P.stage == 3;
+  const unsigned tx_bytes = (unsigned)(K2_NF * FS * sizeof(real));
   const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
   const int tpad = pad(ti, tj, tk);
   constexpr int NFACE = 6 * 3 * N2;  // 1152
@@ -463,11 +622,11 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
       mbar_expect_tx(&bar[s], tx_bytes);
     }
     __syncwarp();
-    double* d = stg + s * K2_STAGE;
+    real* d = stg + s * K2_STAGE;
     if (lane < K2_NF) {
-      const double* src = lane < 3 ? (lane == 0 ? P.F0 : lane == 1 ? P.F1 : P.F2) + e * FS
-                                   : P.Ja + ((long long)(lane - 3) * P.Ne + e) * FS;
-      bulk_g2s(d + lane * FS, src, FS * 8u, &bar[s]);
+      const real* src = lane < 3 ? (lane == 0 ? P.F0 : lane == 1 ? P.F1 : P.F2) + e * FS
+                                 : P.Ja + ((long long)(lane - 3) * P.Ne + e) * FS;
+      bulk_g2s(d + lane * FS, src, FS * (unsigned)sizeof(real), &bar[s]);
     }
   };
   // neighbour flux face traces: [f][c][pq], 1152 values, <= 3 per thread; the
@@ -479,15 +638,15 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
       src[r] = (e >= 0 && idx < NFACE) ? P.fsrc[idx / (3 * N2) + 6 * e] : -1;
     }
   };
-  auto face_load = [&](const int src[3], double fv[3]) {
+  auto face_load = [&](const int src[3], real fv[3]) {
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
       const int idx = tid + r * THREADS;
-      double v = 0.0;
+      real v = 0;
       if (src[r] >= 0) {
         const int rem = idx % (3 * N2), c = rem >> 6, pq = rem & 63;
         const int fn = src[r] & 7;
-        const double* Fc = c == 0 ? P.F0 : c == 1 ? P.F1 : P.F2;
+        const real* Fc = c == 0 ? P.F0 : c == 1 ? P.F1 : P.F2;
         const int fnode = face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N);
         v = Fc[(long long)(src[r] >> 3) * FS + pad(fnode & 7, (fnode >> 3) & 7, fnode >> 6)];
       }
@@ -495,14 +654,15 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     }
   };
   struct PW {
-    double invJ, y, acc;
+    real invJ, y, acc, comp;
   };
   auto pw_load = [&](long long e, PW& w) {
     if (e < 0) return;
     const long long n = e * N3 + tid;
     w.invJ = P.invdetJ[n];
-    w.y = need_y ? P.y[n] : 0.0;
-    w.acc = need_acc ? P.acc[n] : 0.0;
+    w.y = need_y ? P.y[n] : (real)0;
+    w.acc = need_acc ? P.acc[n] : (real)0;
+    w.comp = need_comp ? P.comp[n] : (real)0;
   };
 
   long long e = blockIdx.x;
@@ -515,7 +675,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     emcur = P.emask[e];
     int src0[3];
     src_load(e, src0);
-    double fv[3];
+    real fv[3];
     face_load(src0, fv);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
@@ -524,7 +684,14 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     src_load(e + gridDim.x < P.Ne ? e + gridDim.x : -1, src1);
   }
   __syncthreads();
-  const double aG0 = sG[gq * 8 + tig], aG1 = sG[gq * 8 + 4 + tig];
+  double aG0 = 0.0, aG1 = 0.0;
+  uint32_t aS[4] = {0, 0, 0, 0}, aS2[4] = {0, 0, 0, 0};
+  if constexpr (F64) {
+    aG0 = sG[gq * 8 + tig];
+    aG1 = sG[gq * 8 + 4 + tig];
+  } else {
+    split_G(sG, gq, tig, NT, aS, aS2);
+  }
 
   for (int it = 0; e < P.Ne; ++it, e += gridDim.x) {
     const int s = it % NSTAGE, fb = it & 1;
@@ -534,7 +701,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     const int emnext = has_next ? P.emask[en] : 0;
     int src2[3];
     src_load(enn < P.Ne ? enn : -1, src2);
-    double fnext[3];
+    real fnext[3];
     face_load(src1, fnext);
     PW nxt;
     pw_load(has_next ? en : -1, nxt);
@@ -550,33 +717,56 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
       const long long ei = e + (NSTAGE - 1) * (long long)gridDim.x;
       if (warp == 0 && ei < P.Ne) issue(ei, (it + NSTAGE - 1) % NSTAGE);
     }
-    const double* d = stg + s * K2_STAGE;
-    const double* sF = d;           // 3 fields
-    const double* sJa = d + 3 * FS;  // 9 fields
-    const double* sfc = sface + fb * NFACE;
+    const real* d = stg + s * K2_STAGE;
+    const real* sF = d;           // 3 fields
+    const real* sJa = d + 3 * FS;  // 9 fields
+    const real* sfc = sface + fb * NFACE;
     const int mask = emcur & 63;
     const int bnd = emcur >> 6;
-    // per-axis partial divergences sg[al*2 + half]: no barrier between axes
+    // per-axis partial divergences sdiv[al*2 + half]: no barrier between axes
 #pragma unroll
     for (int al = 0; al < 3; ++al) {
-      const double* m0 = sJa + (al * 3 + 0) * FS;
-      const double* m1 = sJa + (al * 3 + 1) * FS;
-      const double* m2 = sJa + (al * 3 + 2) * FS;
-      double cx[2] = {0, 0}, cy[2] = {0, 0};
+      const real* m0 = sJa + (al * 3 + 0) * FS;
+      const real* m1 = sJa + (al * 3 + 1) * FS;
+      const real* m2 = sJa + (al * 3 + 2) * FS;
+      real cx[2], cy[2];
+      if constexpr (F64) {
+        double dx[2] = {0, 0}, dy[2] = {0, 0};
 #pragma unroll
-      for (int kc = 0; kc < 2; ++kc) {
-        const int nd = bnode(al, wt8, kc, gq, tig);
-        const double a = kc ? aG1 : aG0;
-        if (half == 0) {
-          // contravariant flux Ja^al . F and F_0
-          const double f0 = sF[nd];
-          const double ft = m0[nd] * f0 + m1[nd] * sF[FS + nd] + m2[nd] * sF[2 * FS + nd];
-          dmma(cx[0], cx[1], a, ft);
-          dmma(cy[0], cy[1], a, f0);
-        } else {
-          dmma(cx[0], cx[1], a, sF[FS + nd]);
-          dmma(cy[0], cy[1], a, sF[2 * FS + nd]);
+        for (int kc = 0; kc < 2; ++kc) {
+          const int nd = bnode(al, wt8, kc, gq, tig);
+          const double a = kc ? aG1 : aG0;
+          if (half == 0) {
+            // contravariant flux Ja^al . F and F_0
+            const double f0 = sF[nd];
+            const double ft = m0[nd] * f0 + m1[nd] * sF[FS + nd] + m2[nd] * sF[2 * FS + nd];
+            dmma(dx[0], dx[1], a, ft);
+            dmma(dy[0], dy[1], a, f0);
+          } else {
+            dmma(dx[0], dx[1], a, sF[FS + nd]);
+            dmma(dy[0], dy[1], a, sF[2 * FS + nd]);
+          }
         }
+        cx[0] = dx[0]; cx[1] = dx[1]; cy[0] = dy[0]; cy[1] = dy[1];
+      } else {
+        const int nd[3] = {bn(al, wt8, 2 * tig, gq), bn(al, wt8, 2 * tig + 1, gq), bn(al, wt8, PREF, gq)};
+        float vx[3], vy[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          if (half == 0) {
+            const float f0 = sF[nd[q]];
+            vx[q] = m0[nd[q]] * f0 + m1[nd[q]] * sF[FS + nd[q]] + m2[nd[q]] * sF[2 * FS + nd[q]];
+            vy[q] = f0;
+          } else {
+            vx[q] = sF[FS + nd[q]];
+            vy[q] = sF[2 * FS + nd[q]];
+          }
+        }
+        float fx[4] = {0, 0, 0, 0}, fy[4] = {0, 0, 0, 0};
+        mma_split<NT>(fx, aS, aS2, vx[0] - vx[2], vx[1] - vx[2]);
+        mma_split<NT>(fy, aS, aS2, vy[0] - vy[2], vy[1] - vy[2]);
+        cx[0] = fx[0] + fx[2]; cx[1] = fx[1] + fx[3];
+        cy[0] = fy[0] + fy[2]; cy[1] = fy[1] + fy[3];
       }
       // half 1 adds the centred-flux SAT of an interior al-face on its rows
       const int sface_f = gq == 0 ? 2 * al : gq == 7 ? 2 * al + 1 : -1;
@@ -584,17 +774,17 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
         const int no = onode(al, wt8, b, gq, tig);
-        double r;
+        real r;
         if (half == 0) {
-          r = 0.5 * cx[b] + 0.5 * m0[no] * cy[b];
+          r = (real)0.5 * cx[b] + (real)0.5 * m0[no] * cy[b];
         } else {
-          r = 0.5 * m1[no] * cx[b] + 0.5 * m2[no] * cy[b];
+          r = (real)0.5 * m1[no] * cx[b] + (real)0.5 * m2[no] * cy[b];
         }
         if (sat) {
           const int pq = opq(al, wt8, b, tig);
-          const double sacc = m0[no] * (sfc[(sface_f * 3 + 0) * N2 + pq] - sF[no]) +
-                              m1[no] * (sfc[(sface_f * 3 + 1) * N2 + pq] - sF[FS + no]) +
-                              m2[no] * (sfc[(sface_f * 3 + 2) * N2 + pq] - sF[2 * FS + no]);
+          const real sacc = m0[no] * (sfc[(sface_f * 3 + 0) * N2 + pq] - sF[no]) +
+                            m1[no] * (sfc[(sface_f * 3 + 1) * N2 + pq] - sF[FS + no]) +
+                            m2[no] * (sfc[(sface_f * 3 + 2) * N2 + pq] - sF[2 * FS + no]);
           r += (gq ? inv2H : -inv2H) * sacc;
         }
         sdiv[(al * 2 + half) * FS + no] = r;
@@ -603,8 +793,8 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
     __syncthreads();
     {
       const long long n = e * N3 + tid;
-      double dv = ((sdiv[tpad] + sdiv[2 * FS + tpad]) + sdiv[4 * FS + tpad]) +
-                  ((sdiv[FS + tpad] + sdiv[3 * FS + tpad]) + sdiv[5 * FS + tpad]);
+      real dv = ((sdiv[tpad] + sdiv[2 * FS + tpad]) + sdiv[4 * FS + tpad]) +
+                ((sdiv[FS + tpad] + sdiv[3 * FS + tpad]) + sdiv[5 * FS + tpad]);
       dv *= cur.invJ;
       if (bnd && P.bc_on) {
         const int idx3[3] = {ti, tj, tk};
@@ -616,25 +806,11 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
           dv += P.bbuf[(long long)P.bslot[f + 6 * e] * N2 + p + 8 * q];
         }
       }
-      if (P.epi) {
-        const double dt = P.dt;
-        if (P.stage == 0) {
-          P.out[n] = cur.y + (0.5 * dt) * dv;
-          P.acc[n] = cur.y + (dt / 6.0) * dv;
-        } else if (P.stage == 1) {
-          P.out[n] = cur.y + (0.5 * dt) * dv;
-          P.acc[n] = cur.acc + (dt / 3.0) * dv;
-        } else if (P.stage == 2) {
-          P.out[n] = cur.y + dt * dv;
-          P.acc[n] = cur.acc + (dt / 3.0) * dv;
-        } else {
-          const double v = cur.acc + (dt / 6.0) * dv;
-          P.y[n] = v;
-          if (P.flag && !isfinite(v)) atomicOr(P.flag, 1u);
-        }
-      } else {
+      if (P.epi)
+        n8_rk<real>(P.stage, P.dt, dv, cur.y, cur.y, cur.acc, cur.comp, n, P.y, P.acc, P.out,
+                    comp_on ? P.comp : nullptr, P.flag);
+      else
         P.Pidot[n] = dv;
-      }
     }
     if (has_next) {
 #pragma unroll
@@ -649,7 +825,8 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_k2_n8(const K2N8 P) {
 }
 
 // padded element-block copy of the nine metric-term fields for the n = 8 path
-__global__ void k_pad_fields(long long Ne, int nf, const double* __restrict__ src, double* __restrict__ dst) {
+template <typename real>
+__global__ void k_pad_fields(long long Ne, int nf, const real* __restrict__ src, real* __restrict__ dst) {
   const long long total = (long long)nf * Ne * n8::N3;
   for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
     const long long f = x / (Ne * n8::N3);
@@ -661,7 +838,10 @@ __global__ void k_pad_fields(long long Ne, int nf, const double* __restrict__ sr
 }
 
 int launch_pad_metric_n8(DevMesh& m, cudaStream_t s) {
-  k_pad_fields<<<4096, 256, 0, s>>>(m.Ne, 9, m.Ja, m.Ja_n8);
+  if (m.precision == 0)
+    k_pad_fields<double><<<4096, 256, 0, s>>>(m.Ne, 9, (const double*)m.Ja_r, (double*)m.Ja_n8);
+  else
+    k_pad_fields<float><<<4096, 256, 0, s>>>(m.Ne, 9, (const float*)m.Ja_r, (float*)m.Ja_n8);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -678,51 +858,73 @@ static int sm_count() {
   return n;
 }
 
-int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
-                      void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s) {
-  K1N8 P;
+template <typename real, int NT>
+static int k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
+                 void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s) {
+  K1N8<real> P;
   P.Ne = m.Ne; P.nn = m.nn;
-  P.Phi = (const double*)Phi; P.Pi = (const double*)Pi; P.c10 = (const double*)c.c10;
-  P.Ja = (const double*)m.Ja_n8; P.invdetJ = (const double*)m.invdetJ_r;
+  P.Phi = (const real*)Phi; P.Pi = (const real*)Pi; P.c10 = (const real*)c.c10;
+  P.Ja = (const real*)m.Ja_n8; P.invdetJ = (const real*)m.invdetJ_r;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
   P.emask = m.emask; P.fsrc = m.fsrc;
-  P.F = (double*)F; P.Phidot = (double*)Phidot; P.bbuf = (double*)bbuf;
+  P.F = (real*)F; P.Phidot = (real*)Phidot; P.bbuf = (real*)bbuf;
   P.bc_on = bc.on; P.exc_tag = bc.exc_tag; P.nbf = m.nbf; P.kind = bc.kinds[0]; P.sigma = bc.sigma;
-  P.bnorm = (const double*)m.bnorm;
-  P.gPhi = (const double*)bc.gPhi; P.gPi = (const double*)bc.gPi;
-  P.gDx = (const double*)bc.gDx; P.gDy = (const double*)bc.gDy; P.gDz = (const double*)bc.gDz;
+  P.bnorm = (const real*)m.bnorm;
+  P.gPhi = (const real*)bc.gPhi; P.gPi = (const real*)bc.gPi;
+  P.gDx = (const real*)bc.gDx; P.gDy = (const real*)bc.gDy; P.gDz = (const real*)bc.gDz;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
-  P.y = (double*)rk.y; P.acc = (double*)rk.acc; P.out = (double*)rk.out; P.flag = flag;
+  P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_cons_k1_n8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1_SMEM);
+    if (cudaFuncSetAttribute(k_cons_k1_n8<real, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k1_smem<real>()) !=
+        cudaSuccess)
+      return -2;
     attr = true;
   }
-  const long long grid = m.Ne < sm_count() ? m.Ne : sm_count();
-  k_cons_k1_n8<<<(unsigned)grid, n8::THREADS, K1_SMEM, s>>>(P);
+  const long long cap = (long long)sm_count() * n8::Occ<real>::k1;
+  const long long grid = m.Ne < cap ? m.Ne : cap;
+  k_cons_k1_n8<real, NT><<<(unsigned)grid, n8::THREADS, k1_smem<real>(), s>>>(P);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <typename real, int NT>
+static int k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc, const RKStage& rk,
+                 unsigned* flag, cudaStream_t s) {
+  K2N8<real> P;
+  P.Ne = m.Ne; P.nn = m.nn;
+  P.F0 = (const real*)F; P.F1 = (const real*)F + m.Ne * n8::FS; P.F2 = (const real*)F + 2 * m.Ne * n8::FS;
+  P.Ja = (const real*)m.Ja_n8; P.invdetJ = (const real*)m.invdetJ_r;
+  P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
+  P.emask = m.emask; P.fsrc = m.fsrc;
+  P.bbuf = (const real*)bbuf; P.bc_on = bc.on;
+  P.Pidot = (real*)Pidot;
+  P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
+  P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_cons_k2_n8<real, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k2_smem<real>()) !=
+        cudaSuccess)
+      return -2;
+    attr = true;
+  }
+  const long long cap = (long long)sm_count() * n8::Occ<real>::k2;
+  const long long grid = m.Ne < cap ? m.Ne : cap;
+  k_cons_k2_n8<real, NT><<<(unsigned)grid, n8::THREADS, k2_smem<real>(), s>>>(P);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
+                      void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s) {
+  if (m.precision == 0) return k1_n8<double, 0>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag, s);
+  return m.fp32_form == WT_FP32_BF16X2 ? k1_n8<float, 2>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag, s)
+                                       : k1_n8<float, 3>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag, s);
 }
 
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
                       const RKStage& rk, unsigned* flag, cudaStream_t s) {
-  K2N8 P;
-  P.Ne = m.Ne; P.nn = m.nn;
-  P.F0 = (const double*)F; P.F1 = (const double*)F + m.Ne * n8::FS; P.F2 = (const double*)F + 2 * m.Ne * n8::FS;
-  P.Ja = (const double*)m.Ja_n8; P.invdetJ = (const double*)m.invdetJ_r;
-  P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
-  P.emask = m.emask; P.fsrc = m.fsrc;
-  P.bbuf = (const double*)bbuf; P.bc_on = bc.on;
-  P.Pidot = (double*)Pidot;
-  P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
-  P.y = (double*)rk.y; P.acc = (double*)rk.acc; P.out = (double*)rk.out; P.flag = flag;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_cons_k2_n8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K2_SMEM);
-    attr = true;
-  }
-  const long long grid = m.Ne < sm_count() ? m.Ne : sm_count();
-  k_cons_k2_n8<<<(unsigned)grid, n8::THREADS, K2_SMEM, s>>>(P);
-  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+  if (m.precision == 0) return k2_n8<double, 0>(m, F, Pidot, bbuf, bc, rk, flag, s);
+  return m.fp32_form == WT_FP32_BF16X2 ? k2_n8<float, 2>(m, F, Pidot, bbuf, bc, rk, flag, s)
+                                       : k2_n8<float, 3>(m, F, Pidot, bbuf, bc, rk, flag, s);
 }
 
 }  // namespace wt

@@ -81,9 +81,29 @@ __global__ void k_axpy(long long n, real* __restrict__ y, real a, const real* __
 // low-storage classic RK4 stage update (same arithmetic as the fused epilogue)
 template <typename real>
 __global__ void k_rk_update(long long n, int stage, double dt, real* __restrict__ y, real* __restrict__ acc,
-                            real* __restrict__ out, const real* __restrict__ k) {
+                            real* __restrict__ out, const real* __restrict__ k, real* __restrict__ comp) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const real kv = k[i];
+    if (comp) {  // increment form with a Kahan-compensated final sum (see rk_epilogue)
+      if (stage == 0) {
+        out[i] = y[i] + (real)(0.5 * dt) * kv;
+        acc[i] = (real)(dt / 6.0) * kv;
+      } else if (stage == 1) {
+        out[i] = y[i] + (real)(0.5 * dt) * kv;
+        acc[i] = acc[i] + (real)(dt / 3.0) * kv;
+      } else if (stage == 2) {
+        out[i] = y[i] + (real)dt * kv;
+        acc[i] = acc[i] + (real)(dt / 3.0) * kv;
+      } else {
+        const real inc = acc[i] + (real)(dt / 6.0) * kv;
+        const real yv = y[i];
+        const real t = inc - comp[i];
+        const real v = yv + t;
+        comp[i] = (v - yv) - t;
+        y[i] = v;
+      }
+      continue;
+    }
     if (stage == 0) {
       const real yv = y[i];
       out[i] = yv + (real)(0.5 * dt) * kv;
@@ -167,13 +187,13 @@ int launch_copy(long long n, int precision, void* d, const void* s, cudaStream_t
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 int launch_rk_update(long long n, int precision, int stage, double dt, void* y, void* acc, void* out, const void* k,
-                     cudaStream_t st) {
+                     cudaStream_t st, void* comp) {
   if (precision == 0)
     k_rk_update<double><<<gblocks(n), RB, 0, st>>>(n, stage, dt, (double*)y, (double*)acc, (double*)out,
-                                                  (const double*)k);
+                                                  (const double*)k, (double*)comp);
   else
     k_rk_update<float><<<gblocks(n), RB, 0, st>>>(n, stage, dt, (float*)y, (float*)acc, (float*)out,
-                                                 (const float*)k);
+                                                 (const float*)k, (float*)comp);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 int launch_axpy(long long n, int precision, void* y, double a, const void* x, cudaStream_t st) {

@@ -27,6 +27,8 @@ SOMMERFELD_BDRY_TAG = 7
 EXCISION_BDRY_TAG = 8
 BG_MINKOWSKI, BG_CONSTANT_SHIFT, BG_ADM_PERTURBED, BG_RADIAL_SHIFT = 0, 1, 2, 3
 IC_EIGENMODE_CARTESIAN, IC_GAUSSIANS, IC_OUTGOING_PULSE, IC_PLANE_WAVE, IC_EIGENMODE_RADIAL = 0, 1, 2, 3, 4
+# precision forms of an FP32 mesh (n = 8 contractions): CUDA cores, split BF16 three-term / two-term
+FP32_CUDA_CORES, FP32_BF16X3, FP32_BF16X2 = 0, 1, 2
 
 _ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENOTSUP", -5: "ENONFINITE", -6: "ETIMEOUT"}
 
@@ -84,6 +86,7 @@ def library():
         "wt_workspace_create": [vp, vp, pvp], "wt_workspace_destroy": [vp], "wt_workspace_mu": [vp, C.POINTER(d)],
         "wt_rhs_curved": [vp, vp, vp, vp, vp, vp, vp, d, C.POINTER(_BcDesc), i],
         "wt_rhs_curved_noalloc": [vp, vp, vp, vp, vp, vp, d, d, C.POINTER(_BcDesc), i],
+        "wt_mesh_set_fp32_form": [vp, i],
         "wt_apply_D": [vp, vp, vp, vp, i], "wt_ko_add": [vp, vp, vp, vp, d],
         "wt_gradient3d": [vp, vp, vp, vp, vp, vp], "wt_divergence3d": [vp, vp, vp, vp, vp, vp],
         "wt_rhs_sipg": [vp, vp, vp, vp, vp, C.POINTER(C.c_double * 6), d, d],
@@ -268,6 +271,10 @@ class Mesh(_Child):
         import numpy as np
         b = np.ascontiguousarray(bdry, dtype=np.int32)
         self.ctx.check(library().wt_mesh_set_bdry(self.h, b.ctypes.data), "wt_mesh_set_bdry")
+
+    def set_fp32_form(self, form: int):
+        """Select how an FP32 mesh evaluates the n = 8 contractions (FP32_* constants)."""
+        self.ctx.check(library().wt_mesh_set_fp32_form(self.h, int(form)), "wt_mesh_set_fp32_form")
 
     def min_spacing(self) -> float:
         """_min_node_spacing_3d (src/evolve.jl:60-69)."""
