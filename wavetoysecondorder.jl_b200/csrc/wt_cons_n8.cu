@@ -182,6 +182,16 @@ template <typename real>
 struct Occ {
   static constexpr int k1 = 1, k2 = 1;
 };
+template <>
+struct Occ<float> {
+  static constexpr int k1 = 2, k2 = 2;
+};
+// FP32 K1 stages the ten background coefficients with the copies (instead of
+// prefetching them into registers), so that two CTAs fit on an SM
+template <typename real>
+struct StageCoef {
+  static constexpr bool value = !std::is_same<real, double>::value;
+};
 
 }  // namespace n8
 
@@ -264,13 +274,16 @@ struct K1N8 {
   unsigned* flag;
 };
 
-// K1 staged fields: Phi (unpadded, 512) and Ja (9 padded fields, one block
-// each from the padded global copy).  Register prefetch: c10 (10), Pi, invJ,
-// y, acc, comp.
-constexpr size_t K1_STAGE = (size_t)n8::N3 + 9 * (size_t)n8::FS;
+// K1 staged fields: Phi (unpadded, 512), Ja (9 padded fields, one block each
+// from the padded global copy) and, for FP32, the ten coefficient fields
+// (unpadded).  Register prefetch: Pi, invJ, y, acc, comp (+ c10 for FP64).
+template <typename real>
+__host__ __device__ constexpr size_t k1_stage() {
+  return (size_t)n8::N3 + 9 * (size_t)n8::FS + (n8::StageCoef<real>::value ? 10 * (size_t)n8::N3 : 0);
+}
 template <typename real>
 constexpr size_t k1_smem() {
-  return (n8::NSTAGE * K1_STAGE + 9 * n8::FS + 2 * 6 * n8::N2) * sizeof(real) + n8::N2 * sizeof(double) + 64;
+  return (n8::NSTAGE * k1_stage<real>() + 9 * n8::FS + 2 * 6 * n8::N2) * sizeof(real) + n8::N2 * sizeof(double) + 64;
 }
 
 // NT: FP32 split terms (3 or 2); ignored by the FP64 form
@@ -278,6 +291,8 @@ template <typename real, int NT>
 __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(const K1N8<real> P) {
   using namespace n8;
   constexpr bool F64 = std::is_same<real, double>::value;
+  constexpr bool SC = StageCoef<real>::value;
+  constexpr size_t K1_STAGE = k1_stage<real>();
   extern __shared__ __align__(128) unsigned char smraw[];
   double* sG = reinterpret_cast<double*>(smraw);                // 64 (FP64 operator)
   real* stg = reinterpret_cast<real*>(sG + N2);                 // NSTAGE stages x 10 fields
@@ -293,7 +308,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(c
   const bool need_y = P.epi && (P.stage == 1 || P.stage == 2 || (comp_on && P.stage == 3));
   const bool need_acc = P.epi && P.stage >= 1;
   const bool need_comp = comp_on && P.stage == 3;
-  const unsigned tx_bytes = (unsigned)((N3 + 9 * FS) * sizeof(real));
+  const unsigned tx_bytes = (unsigned)(K1_STAGE * sizeof(real));
   // node-phase coordinates of this thread
   const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
   const int tpad = pad(ti, tj, tk);
@@ -318,6 +333,9 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(c
     else if (lane <= 9)
       bulk_g2s(d + N3 + (lane - 1) * FS, P.Ja + ((long long)(lane - 1) * P.Ne + e) * FS, FS * (unsigned)sizeof(real),
                &bar[s]);
+    else if (SC && lane < 20)
+      bulk_g2s(d + N3 + 9 * FS + (lane - 10) * N3, P.c10 + (lane - 10) * nn + e * N3, N3 * (unsigned)sizeof(real),
+               &bar[s]);
   };
   // neighbour Phi face traces (384 values; threads 0..383).  The face source
   // (8 * neighbour + neighbour face) of an element is loaded one iteration
@@ -336,8 +354,10 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(c
   auto pw_load = [&](long long e, PW& w) {
     if (e < 0) return;
     const long long n = e * N3 + tid;
+    if constexpr (!SC) {
 #pragma unroll
-    for (int c = 0; c < 10; ++c) w.c[c] = P.c10[c * nn + n];
+      for (int c = 0; c < 10; ++c) w.c[c] = P.c10[c * nn + n];
+    }
     w.Pi = P.Pi[n];
     w.invJ = P.invdetJ[n];
     w.y = need_y ? P.y[n] : (real)0;
@@ -480,9 +500,12 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(c
       real g1 = (sg[FS + tpad] + sg[4 * FS + tpad]) + sg[7 * FS + tpad];
       real g2 = (sg[2 * FS + tpad] + sg[5 * FS + tpad]) + sg[8 * FS + tpad];
       g0 *= cur.invJ; g1 *= cur.invJ; g2 *= cur.invJ;
-      const real a = cur.c[0];
-      const real b0 = cur.c[1], b1 = cur.c[2], b2 = cur.c[3];
-      const real K0 = cur.c[4], K1v = cur.c[5], K2 = cur.c[6], K3 = cur.c[7], K4 = cur.c[8], K5 = cur.c[9];
+      real cc[10];
+#pragma unroll
+      for (int c = 0; c < 10; ++c) cc[c] = SC ? d[N3 + 9 * FS + c * N3 + tid] : cur.c[c];
+      const real a = cc[0];
+      const real b0 = cc[1], b1 = cc[2], b2 = cc[3];
+      const real K0 = cc[4], K1v = cc[5], K2 = cc[6], K3 = cc[7], K4 = cc[8], K5 = cc[9];
       const real Pi = cur.Pi;
       const real F0 = b0 * Pi + (K0 * g0 + K1v * g1 + K2 * g2);
       const real F1 = b1 * Pi + (K1v * g0 + K3 * g1 + K4 * g2);
