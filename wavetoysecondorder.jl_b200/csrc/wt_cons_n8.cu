@@ -14,7 +14,8 @@
 //     block; the metric terms and the flux live in global memory in a
 //     plane-padded element layout (k-plane stride 68 words) that makes the
 //     tensor-core operand loads (nearly) bank-conflict-free.  A ring of
-//     NSTAGE stages keeps NSTAGE - 1 elements in flight; every wait is
+//     NSTAGE stages keeps NSTAGE - 1 elements in flight; one thread polls
+//     each stage's mbarrier, the rest wait at the CTA barrier; every wait is
 //     bounded and raises an error flag instead of spinning forever;
 //   * the fields used only at their own node (background coefficients, Pi,
 //     1/J, the RK4 state) are prefetched into registers one element ahead;
@@ -399,7 +400,10 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(c
     const real fnext = face_load(has_next ? src1 : -1);
     PW nxt;
     pw_load(has_next ? en : -1, nxt);
-    if (!wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
+    // One thread polls the stage's mbarrier (its acquire makes the copied data
+    // visible; the barrier below orders every other thread after it), so the
+    // other warps do not spend issue slots spinning.
+    if (tid == 0 && !wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
     // After this barrier every thread has finished the previous element, so its
     // stage (reused for element e + (NSTAGE - 1) grid), the partial gradients
     // and face buffer fb^1 are free.
@@ -728,7 +732,10 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2) k_cons_k2_n8(c
     face_load(src1, fnext);
     PW nxt;
     pw_load(has_next ? en : -1, nxt);
-    if (!wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
+    // One thread polls the stage's mbarrier (its acquire makes the copied data
+    // visible; the barrier below orders every other thread after it), so the
+    // other warps do not spend issue slots spinning.
+    if (tid == 0 && !wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
     __syncthreads();  // the previous element is finished: its stage and the buffers are free (see K1)
     if (abort_flag) {  // wait (bounded) for the copies still in flight, then leave
       if (warp == 0 && lane == 0)
