@@ -54,6 +54,7 @@ typedef struct wt_ctx wt_ctx;
 typedef struct wt_mesh wt_mesh;
 typedef struct wt_coef wt_coef;
 typedef struct wt_ws wt_ws;
+typedef struct wt_batch wt_batch;
 
 /* ---- context ------------------------------------------------------------ */
 /* No reference counterpart (Julia picks the backend per array); owns the
@@ -125,6 +126,12 @@ int wt_mesh_info(const wt_mesh* mesh, int* N, long long* Ne, int* precision);
 int wt_mesh_get(const wt_mesh* mesh, const char* name, void* host_out);
 /* Override the outer-face tags (6,Ne) int32, e.g. to mark excision faces. */
 int wt_mesh_set_bdry(wt_mesh* mesh, const int32_t* bdry);
+/* Free the FP64 set-up geometry the RHS and RK4 path no longer read (node
+ * coordinates, Jacobian, inverse, determinant; for FP32 meshes also the FP64
+ * metric terms) to make room for more solves.  Afterwards background sampling,
+ * initial data, min spacing, the strong form and reading those arrays return
+ * WT_EINVAL.  No counterpart in the reference (Julia's GC owns its arrays). */
+int wt_mesh_release_setup_geometry(wt_mesh* mesh);
 /* Precision form of an FP32 mesh (WT_FP32_*; default WT_FP32_BF16X3).  No
  * counterpart in the reference (its T = Float32 path uses one form). */
 int wt_mesh_set_fp32_form(wt_mesh* mesh, int form);
@@ -262,6 +269,29 @@ int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int n
 int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* Phi_host, double* Pi_host,
                           double dt, int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc,
                           int use_metric, double* energy);
+
+/* ---- batches of independent solves ----------------------------------------
+ * No counterpart in the reference, which advances one solve per evolve3d
+ * call (src/evolve.jl:1149-1358); the batch advances many solves of uneven
+ * element counts and orders together.  Members are existing (workspace,
+ * coefficients, Phi, Pi) sets on curvilinear meshes, each with its own dt and
+ * boundary data; they are grouped by (n, precision, kernel path), each group
+ * is one work list of (solve, element) tiles run by one kernel launch per RK4
+ * stage, and one RK4 step of all groups is a CUDA graph, captured when the
+ * membership changes and replayed by wt_batch_step.  The first step after a
+ * change also picks the elements per CTA of the generic kernels by timing
+ * (autotuner, on by default).  Every member advances by the same number of
+ * steps per call; results equal wt_step_rk4_curved on each member alone. */
+int wt_batch_create(wt_ctx* ctx, wt_batch** out);
+int wt_batch_destroy(wt_batch* batch);
+int wt_batch_add(wt_batch* batch, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
+                 const wt_bc_desc* bc, int* slot);
+int wt_batch_remove(wt_batch* batch, int slot);
+int wt_batch_set_autotune(wt_batch* batch, int on);
+int wt_batch_step(wt_batch* batch, int nsteps);
+int wt_batch_info(wt_batch* batch, int* nsolves, long long* nodes, int* ngroups);
+int wt_batch_group_info(wt_batch* batch, int group, int* N, int* precision, int* n8_path, int* epb_variant,
+                        long long* tiles);
 
 #ifdef __cplusplus
 }

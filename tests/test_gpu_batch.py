@@ -1,0 +1,107 @@
+"""Batched solves (wt_batch_*): many solves of uneven element counts, orders and
+precisions advanced together must give what each gives when stepped alone
+with wt_step_rk4_curved (<= 1e-12 relative L2 for FP64 members, <= 1e-6 for
+FP32 members, which run the same kernels), also after members leave and join.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = a.double().cpu().numpy()
+    b = b.double().cpu().numpy()
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+class Solve:
+    """One member: mesh, ADM background, pulse data, a workspace for the batch
+    and a second workspace + state copy stepped alone."""
+
+    def __init__(self, wt, ctx, N, M, seed, precision=0, form=None, amp=0.1):
+        W = wt.workloads
+        self.mesh = wt.Mesh.uniform_hex(ctx, N, M, outer_tag=7, warp_A=0.05, precision=precision)
+        if form is not None:
+            self.mesh.set_fp32_form(form)
+        p = W.adm_params(seed, amp)
+        self.coef = wt.sample_background3d(self.mesh, wt.BG_ADM_PERTURBED, p)
+        self.ws, self.ws_alone = wt.make_wave3d_workspace(self.mesh), wt.make_wave3d_workspace(self.mesh)
+        self.Phi, self.Pi = self.mesh.zeros(), self.mesh.zeros()
+        c, a, w = W.pulses(seed, 2, amp=(0.5, 1.0), width=(0.05, 0.15))
+        wt.initial_data(self.mesh, wt.IC_GAUSSIANS, wt.gaussian_params(c, a, w), self.Phi)
+        self.Pa, self.Qa = self.Phi.clone(), self.Pi.clone()
+        self.dt = 0.2 * self.mesh.min_spacing() / W.max_speed(p)
+        self.bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+        self.tol = 1e-12 if precision == 0 else 1e-6
+
+    def step_alone(self, wt, n):
+        wt.step_rk4_curved(self.Pa, self.Qa, self.coef, self.ws_alone, self.dt, n, bc3d=self.bc, metric=True)
+
+    def check(self):
+        assert rel(self.Phi, self.Pa) <= self.tol and rel(self.Pi, self.Qa) <= self.tol
+
+
+def test_batch_matches_solves_stepped_alone(wt, ctx):
+    specs = [(4, 3, 11, 0, None), (6, 2, 12, 0, None), (8, 2, 13, 0, None), (8, (3, 2, 2), 14, 0, None),
+             (8, 2, 15, 1, wt.FP32_BF16X3), (6, 3, 16, 1, None), (8, 2, 17, 1, wt.FP32_CUDA_CORES),
+             (5, 2, 18, 0, None)]
+    solves = [Solve(wt, ctx, N, M, seed, prec, form, amp=0.15 * (k % 3) / 2) for k, (N, M, seed, prec, form)
+              in enumerate(specs)]
+    batch = wt.Batch(ctx)
+    slots = [batch.add(s.Phi, s.Pi, s.coef, s.ws, s.dt, s.bc) for s in solves]
+    # the RK4 path does not read the FP64 set-up geometry; releasing it must not matter
+    solves[4].mesh.release_setup_geometry()
+    with pytest.raises(wt.WaveToyError):
+        solves[4].mesh.min_spacing()
+    nsolves, nodes, ngroups = batch.info()
+    assert nsolves == len(solves) and nodes == sum(s.mesh.nn for s in solves)
+    groups = batch.groups()
+    assert ngroups == len(groups) >= 5
+    assert any(g[2] == 1 and g[1] == 0 for g in groups) and any(g[2] == 1 and g[1] == 1 for g in groups)
+    batch.step(7)
+    for s in solves:
+        s.step_alone(wt, 7)
+    for s in solves:
+        s.check()
+    # members leave and join; the others carry on unchanged
+    batch.remove(slots[1])
+    batch.remove(slots[4])
+    extra = Solve(wt, ctx, 4, 2, 19)
+    batch.add(extra.Phi, extra.Pi, extra.coef, extra.ws, extra.dt, extra.bc)
+    batch.step(5)
+    for k, s in enumerate(solves):
+        if k not in (1, 4):
+            s.step_alone(wt, 5)
+            s.check()
+    extra.step_alone(wt, 5)
+    extra.check()
+    E = wt.wave3d_energy(solves[4].Phi, solves[4].Pi, solves[4].coef, solves[4].ws, metric=True)
+    assert np.isfinite(E) and E > 0
+    assert not ctx.nonfinite()
+    batch.close()
+
+
+def test_batch_autotune_off_gives_same_results(wt, ctx):
+    a = Solve(wt, ctx, 4, 4, 21)
+    b = Solve(wt, ctx, 4, 4, 21)
+    b1, b2 = wt.Batch(ctx, autotune=True), wt.Batch(ctx, autotune=False)
+    b1.add(a.Phi, a.Pi, a.coef, a.ws, a.dt, a.bc)
+    b2.add(b.Phi, b.Pi, b.coef, b.ws, b.dt, b.bc)
+    b1.step(4)
+    b2.step(4)
+    assert b2.groups()[0][3] == 0
+    assert rel(a.Phi, b.Phi) <= 1e-12 and rel(a.Pi, b.Pi) <= 1e-12
+
+
+def test_batch_rejects_bad_members(wt, ctx):
+    s = Solve(wt, ctx, 4, 2, 31)
+    batch = wt.Batch(ctx)
+    with pytest.raises(wt.WaveToyError):
+        batch.add(s.Phi, s.Pi, s.coef, s.ws, -1.0, s.bc)
+    batch.add(s.Phi, s.Pi, s.coef, s.ws, s.dt, s.bc)
+    with pytest.raises(wt.WaveToyError):  # one workspace serves one member
+        batch.add(s.Pa, s.Qa, s.coef, s.ws, s.dt, s.bc)
+    with pytest.raises(wt.WaveToyError):
+        batch.remove(7)

@@ -338,6 +338,13 @@ int make_bc(wt_ctx* ctx, const wt_bc_desc* bc, int use_metric, wt::ConsBC& out) 
   return 0;
 }
 
+// Entry points that evaluate the analytic map, sample a background at the
+// nodes or use the FP64 Jacobians need the set-up geometry.
+int need_setup_geometry(const wt_mesh* mh, const char* what) {
+  if (mh->m.coords && mh->m.jac) return 0;
+  return fail(mh->ctx, WT_EINVAL, std::string(what) + ": the mesh's set-up geometry was released");
+}
+
 int check_ws(wt_ctx* ctx, wt_ws* ws) {
   if (!ctx) return WT_EINVAL;
   if (!ws) return fail(ctx, WT_EINVAL, "workspace is NULL");
@@ -616,6 +623,7 @@ int wt_mesh_get(const wt_mesh* mh, const char* name, void* host_out) {
     return 0;
   } else if (s == "handedness") { src = m.handed; bytes = m.Ne * sizeof(int32_t); }
   else return fail(ctx, WT_EINVAL, "wt_mesh_get: unknown array '" + s + "'");
+  if (!src) return fail(ctx, WT_EINVAL, "wt_mesh_get: '" + s + "' was released with the set-up geometry");
   cudaMemcpyAsync(host_out, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "wt_mesh_get");
@@ -642,8 +650,29 @@ int wt_mesh_set_fp32_form(wt_mesh* mh, int form) {
   return 0;
 }
 
+int wt_mesh_release_setup_geometry(wt_mesh* mh) {
+  if (!mh) return WT_EINVAL;
+  wt::DevMesh& m = mh->m;
+  cudaStreamSynchronize(mh->ctx->stream);
+  std::vector<void*> drop = {m.coords, m.jac, m.invjac, m.detjac};
+  if (m.precision != WT_F64) {  // FP32 meshes stream their own copies of Ja and 1/J
+    drop.push_back(m.Ja);
+    drop.push_back(m.invdetJ);
+  }
+  for (void* p : drop) {
+    if (!p) continue;
+    auto it = std::find(mh->owned.begin(), mh->owned.end(), p);
+    if (it != mh->owned.end()) mh->owned.erase(it);
+    cudaFree(p);
+  }
+  m.coords = m.jac = m.invjac = m.detjac = nullptr;
+  if (m.precision != WT_F64) m.Ja = m.invdetJ = nullptr;
+  return 0;
+}
+
 int wt_mesh_min_spacing(wt_mesh* mh, double* h) {
   if (!mh || !h) return WT_EINVAL;
+  WT_TRY(need_setup_geometry(mh, "wt_mesh_min_spacing"));
   mh->ctx->launches += 1;
   return lrc(mh->ctx, wt::launch_min_spacing(mh->m, h, mh->ctx->stream), "min spacing");
 }
@@ -670,6 +699,7 @@ int wt_background_set(wt_ctx* ctx, wt_mesh* mesh, const wt_background_desc* desc
   if (desc->kind < 0 || desc->kind > 3) return fail(ctx, WT_EINVAL, "unknown background kind");
   if (desc->kind == WT_BG_ADM_PERTURBED && !(desc->p[3] > 0))
     return fail(ctx, WT_EINVAL, "ADM background needs a positive Gaussian width p[3]");
+  WT_TRY(need_setup_geometry(mesh, "wt_background_set"));
   wt_coef* c = nullptr;
   WT_TRY(coef_alloc(ctx, mesh, &c));
   int rc = lrc(ctx, wt::launch_background(mesh->m, c->c, desc->kind, desc->p, ctx->stream), "background");
@@ -726,6 +756,7 @@ int wt_initial_data(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, 
   if (nparams < 0 || nparams > 4096) return fail(ctx, WT_EINVAL, "wt_initial_data: bad parameter count");
   if (kind == WT_IC_GAUSSIANS && (nparams < 1 || 1 + 5 * (int)params[0] > nparams))
     return fail(ctx, WT_EINVAL, "wt_initial_data: Gaussian count does not match the parameters");
+  WT_TRY(need_setup_geometry(mesh, "wt_initial_data"));
   double* dp = nullptr;
   WT_TRY(dalloc(ctx, &dp, (nparams > 0 ? nparams : 1) * sizeof(double), nullptr));
   if (nparams > 0) cudaMemcpyAsync(dp, params, nparams * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
@@ -860,6 +891,7 @@ int wt_rhs_strong(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, void* u
                   double sommerfeld_R) {
   WT_TRY(check_ws(ctx, ws));
   if (!u || !ut || !utt) return fail(ctx, WT_EINVAL, "wt_rhs_strong: NULL argument");
+  WT_TRY(need_setup_geometry(ws->mesh, "wt_rhs_strong"));
   wt::DevMesh& m = ws->mesh->m;
   if (!m.dinvjac) {
     WT_TRY(dalloc(ctx, &m.dinvjac, 27 * (size_t)m.nn * sizeof(double), &ws->mesh->owned));
@@ -1099,6 +1131,328 @@ int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* P
   cudaFree(dP);
   cudaFree(dQ);
   return rc;
+}
+
+}  // extern "C"
+
+// ---- batches of independent solves -----------------------------------------------------
+// Many solves of uneven element counts and orders advance together: solves are
+// grouped by (n, precision, kernel path); each group is one work list of
+// (solve, element) tiles over which one persistent (n = 8) or element-parallel
+// kernel launch runs per RK4 stage, every tile reading its solve's parameter
+// block (meshes, coefficients, state, scratch, dt).  One RK4 step of all
+// groups is captured once as a CUDA graph and replayed; adding or removing a
+// solve only rebuilds the work lists, parameter blocks and graph.
+struct wt_batch {
+  wt_ctx* ctx = nullptr;
+  struct Member {
+    bool active = false;
+    wt_ws* ws = nullptr;
+    const wt_coef* coef = nullptr;
+    void* Phi = nullptr;
+    void* Pi = nullptr;
+    double dt = 0.0;
+    wt::ConsBC bc;
+  };
+  std::vector<Member> members;
+  struct Group {
+    int N = 0, precision = 0, fp32_form = 0;
+    bool n8 = false;
+    std::vector<int> slots;
+    long long ntiles = 0;
+    int2* d_tiles = nullptr;
+    char* d_k1 = nullptr;
+    char* d_k2 = nullptr;
+    std::vector<char> h_k1, h_k2;  // [stage][solve] parameter blocks
+    size_t k1sz = 0, k2sz = 0;
+    int epb_variant = 0;
+  };
+  std::vector<Group> groups;
+  bool dirty = true;
+  int autotune = 1;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long launches_per_step = 0;
+};
+
+namespace {
+
+void batch_release(wt_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  for (auto& g : b->groups) {
+    cudaFree(g.d_tiles);
+    cudaFree(g.d_k1);
+    cudaFree(g.d_k2);
+  }
+  b->groups.clear();
+}
+
+// the per-solve inputs of RK4 stage st (the same buffers step_curved_once uses)
+wt::SolveStage batch_stage(wt_batch* b, const wt_batch::Member& mb, int st) {
+  wt_ws* ws = mb.ws;
+  wt::SolveStage ss;
+  ss.m = &ws->mesh->m;
+  ss.c = &mb.coef->c;
+  void* SP[2] = {ws->S0, ws->S1};
+  ss.Phi = st == 0 ? mb.Phi : SP[(st - 1) % 2];
+  ss.Pi = st == 0 ? mb.Pi : ws->SQ;
+  ss.F = ws->F;
+  ss.bbuf = ws->bbuf;
+  ss.bc = mb.bc;
+  ss.rkP.on = ss.rkQ.on = 1;
+  ss.rkP.stage = ss.rkQ.stage = st;
+  ss.rkP.dt = ss.rkQ.dt = mb.dt;
+  ss.rkP.y = mb.Phi; ss.rkP.acc = ws->accP; ss.rkP.out = SP[st % 2]; ss.rkP.comp = ws->compP;
+  ss.rkQ.y = mb.Pi; ss.rkQ.acc = ws->accQ; ss.rkQ.out = ws->SQ; ss.rkQ.comp = ws->compQ;
+  ss.rkP.nonfinite = ss.rkQ.nonfinite = st == 3 ? b->ctx->d_flag : nullptr;
+  return ss;
+}
+
+int batch_launch(wt_batch* b, wt_batch::Group& g, int which, int st, cudaStream_t s) {
+  const size_t ns = g.slots.size();
+  if (g.n8) {
+    const size_t sz = which == 1 ? g.k1sz : g.k2sz;
+    const char* h = (which == 1 ? g.h_k1.data() : g.h_k2.data()) + st * ns * sz;
+    const char* d = (which == 1 ? g.d_k1 : g.d_k2) + st * ns * sz;
+    return wt::launch_cons_n8_batch(which, g.precision, g.fp32_form, h, d, g.d_tiles, g.ntiles, s);
+  }
+  const size_t sz = which == 1 ? g.k1sz : g.k2sz;
+  const char* d = (which == 1 ? g.d_k1 : g.d_k2) + st * ns * sz;
+  return wt::launch_cons_gen_batch(which, g.N, g.precision, g.epb_variant, d, g.d_tiles, g.ntiles, s);
+}
+
+int batch_one_step(wt_batch* b, cudaStream_t s) {
+  for (int st = 0; st < 4; ++st) {
+    for (auto& g : b->groups) WT_TRY(lrc(b->ctx, batch_launch(b, g, 1, st, s), "batch K1"));
+    for (auto& g : b->groups) WT_TRY(lrc(b->ctx, batch_launch(b, g, 2, st, s), "batch K2"));
+  }
+  return 0;
+}
+
+// Time stage 0 of a generic group in both elements-per-CTA variants and keep
+// the faster (stage 0 writes only stage scratch, never the solution state).
+int batch_tune_group(wt_batch* b, wt_batch::Group& g) {
+  cudaStream_t s = b->ctx->own_stream;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int best_v = 0;
+  for (int v = 0; v < 2; ++v) {
+    g.epb_variant = v;
+    int rc = 0;
+    for (int rep = 0; rep < 2 && !rc; ++rep) {  // warm up
+      rc = batch_launch(b, g, 1, 0, s);
+      if (!rc) rc = batch_launch(b, g, 2, 0, s);
+    }
+    cudaEventRecord(e0, s);
+    for (int rep = 0; rep < 3 && !rc; ++rep) {
+      rc = batch_launch(b, g, 1, 0, s);
+      if (!rc) rc = batch_launch(b, g, 2, 0, s);
+    }
+    cudaEventRecord(e1, s);
+    if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return lrc(b->ctx, rc, "batch autotune"); }
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) { best = ms; best_v = v; }
+  }
+  g.epb_variant = best_v;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return 0;
+}
+
+int batch_rebuild(wt_batch* b) {
+  wt_ctx* ctx = b->ctx;
+  batch_release(b);
+  // group the active members
+  for (int slot = 0; slot < (int)b->members.size(); ++slot) {
+    const auto& mb = b->members[slot];
+    if (!mb.active) continue;
+    const wt::DevMesh& m = mb.ws->mesh->m;
+    const wt::SolveStage s0 = batch_stage(b, mb, 0);
+    const bool n8 = wt::cons_n8_path(m, mb.coef->c, 1, mb.bc, s0.rkP, s0.rkQ,
+                                     {mb.Phi, mb.Pi, mb.ws->F, mb.ws->S0, mb.ws->S1, mb.ws->SQ});
+    const int form = m.precision == WT_F32 ? m.fp32_form : 0;
+    wt_batch::Group* g = nullptr;
+    for (auto& x : b->groups)
+      if (x.N == m.N && x.precision == m.precision && x.n8 == n8 && (!n8 || x.fp32_form == form)) g = &x;
+    if (!g) {
+      b->groups.emplace_back();
+      g = &b->groups.back();
+      g->N = m.N; g->precision = m.precision; g->n8 = n8; g->fp32_form = form;
+    }
+    g->slots.push_back(slot);
+  }
+  for (auto& g : b->groups) {
+    const size_t ns = g.slots.size();
+    std::vector<int2> tiles;
+    for (size_t i = 0; i < ns; ++i) {
+      const long long Ne = b->members[g.slots[i]].ws->mesh->m.Ne;
+      for (long long e = 0; e < Ne; ++e) tiles.push_back(make_int2((int)i, (int)e));
+    }
+    g.ntiles = (long long)tiles.size();
+    g.k1sz = g.n8 ? wt::cons_n8_param_size(g.precision, 1) : wt::cons_gen_param_size(g.precision, 1);
+    g.k2sz = g.n8 ? wt::cons_n8_param_size(g.precision, 2) : wt::cons_gen_param_size(g.precision, 2);
+    g.h_k1.assign(4 * ns * g.k1sz, 0);
+    g.h_k2.assign(4 * ns * g.k2sz, 0);
+    for (int st = 0; st < 4; ++st)
+      for (size_t i = 0; i < ns; ++i) {
+        const wt::SolveStage ss = batch_stage(b, b->members[g.slots[i]], st);
+        void* p1 = g.h_k1.data() + (st * ns + i) * g.k1sz;
+        void* p2 = g.h_k2.data() + (st * ns + i) * g.k2sz;
+        if (g.n8) {
+          wt::cons_n8_fill_params(1, ss, ctx->d_flag, p1);
+          wt::cons_n8_fill_params(2, ss, ctx->d_flag, p2);
+        } else {
+          wt::cons_gen_fill_params(1, ss, ss.rkP.nonfinite, p1);
+          wt::cons_gen_fill_params(2, ss, ss.rkQ.nonfinite, p2);
+        }
+      }
+    WT_TRY(dalloc(ctx, &g.d_tiles, tiles.size() * sizeof(int2), nullptr));
+    WT_TRY(dalloc(ctx, &g.d_k1, g.h_k1.size(), nullptr));
+    WT_TRY(dalloc(ctx, &g.d_k2, g.h_k2.size(), nullptr));
+    cudaMemcpy(g.d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice);
+    cudaMemcpy(g.d_k1, g.h_k1.data(), g.h_k1.size(), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(g.d_k2, g.h_k2.data(), g.h_k2.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch parameter upload");
+  }
+  if (b->autotune) {
+    cudaStreamSynchronize(ctx->stream);  // the tuning launches run on the context's own stream
+    for (auto& g : b->groups)
+      if (!g.n8) WT_TRY(batch_tune_group(b, g));
+  }
+  // capture one RK4 step of every group
+  cudaStream_t own = ctx->own_stream;
+  cudaError_t e = cudaStreamBeginCapture(own, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph capture");
+  int rc = batch_one_step(b, own);
+  e = cudaStreamEndCapture(own, &b->graph);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph capture");
+  e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph instantiate");
+  b->launches_per_step = 8 * (long long)b->groups.size();
+  b->dirty = false;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wt_batch_create(wt_ctx* ctx, wt_batch** out) {
+  if (!ctx) return WT_EINVAL;
+  if (!out) return fail(ctx, WT_EINVAL, "wt_batch_create: NULL argument");
+  auto* b = new wt_batch();
+  b->ctx = ctx;
+  *out = b;
+  return 0;
+}
+
+int wt_batch_destroy(wt_batch* b) {
+  if (!b) return WT_EINVAL;
+  cudaStreamSynchronize(b->ctx->own_stream);
+  cudaStreamSynchronize(b->ctx->stream);
+  batch_release(b);
+  delete b;
+  return 0;
+}
+
+int wt_batch_add(wt_batch* b, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, const wt_bc_desc* bc,
+                 int* slot) {
+  if (!b) return WT_EINVAL;
+  wt_ctx* ctx = b->ctx;
+  WT_TRY(check_ws(ctx, ws));
+  if (!coef || !Phi || !Pi || !slot) return fail(ctx, WT_EINVAL, "wt_batch_add: NULL argument");
+  if (coef->mesh != ws->mesh) return fail(ctx, WT_EINVAL, "coefficients belong to another mesh");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(ctx, WT_EINVAL, "dt must be positive and finite");
+  wt_batch::Member mb;
+  WT_TRY(make_bc(ctx, bc, 1, mb.bc));
+  WT_TRY(ws_step_buffers(ws));
+  comp_track(ws, Phi, Pi);
+  mb.active = true;
+  mb.ws = ws;
+  mb.coef = coef;
+  mb.Phi = Phi;
+  mb.Pi = Pi;
+  mb.dt = dt;
+  for (const auto& x : b->members)
+    if (x.active && x.ws == ws) return fail(ctx, WT_EINVAL, "a workspace can serve one batch member at a time");
+  int s = -1;
+  for (int i = 0; i < (int)b->members.size(); ++i)
+    if (!b->members[i].active) { s = i; break; }
+  if (s < 0) { s = (int)b->members.size(); b->members.emplace_back(); }
+  b->members[s] = mb;
+  b->dirty = true;
+  *slot = s;
+  return 0;
+}
+
+int wt_batch_remove(wt_batch* b, int slot) {
+  if (!b) return WT_EINVAL;
+  if (slot < 0 || slot >= (int)b->members.size() || !b->members[slot].active)
+    return fail(b->ctx, WT_EINVAL, "wt_batch_remove: no such member");
+  b->members[slot].active = false;
+  b->dirty = true;
+  return 0;
+}
+
+int wt_batch_set_autotune(wt_batch* b, int on) {
+  if (!b) return WT_EINVAL;
+  b->autotune = on ? 1 : 0;
+  b->dirty = true;
+  return 0;
+}
+
+int wt_batch_step(wt_batch* b, int nsteps) {
+  if (!b) return WT_EINVAL;
+  wt_ctx* ctx = b->ctx;
+  if (nsteps < 0) return fail(ctx, WT_EINVAL, "nsteps must be >= 0");
+  if (b->dirty) WT_TRY(batch_rebuild(b));
+  if (nsteps == 0 || b->groups.empty()) return 0;
+  cudaStream_t user = ctx->stream, own = ctx->own_stream;
+  cudaEventRecord(ctx->ord_a, user);
+  cudaStreamWaitEvent(own, ctx->ord_a, 0);
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < nsteps && e == cudaSuccess; ++i) e = cudaGraphLaunch(b->exec, own);
+  cudaEventRecord(ctx->ord_b, own);
+  cudaStreamWaitEvent(user, ctx->ord_b, 0);
+  ctx->launches += b->launches_per_step * nsteps;
+  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "batch graph launch");
+}
+
+int wt_batch_info(wt_batch* b, int* nsolves, long long* nodes, int* ngroups) {
+  if (!b) return WT_EINVAL;
+  int n = 0;
+  long long nn = 0;
+  for (const auto& mb : b->members)
+    if (mb.active) { ++n; nn += mb.ws->mesh->m.nn; }
+  if (nsolves) *nsolves = n;
+  if (nodes) *nodes = nn;
+  if (ngroups) {
+    if (b->dirty) WT_TRY(batch_rebuild(b));
+    *ngroups = (int)b->groups.size();
+  }
+  return 0;
+}
+
+int wt_batch_group_info(wt_batch* b, int group, int* N, int* precision, int* n8_path, int* epb_variant,
+                        long long* tiles) {
+  if (!b) return WT_EINVAL;
+  if (b->dirty) WT_TRY(batch_rebuild(b));
+  if (group < 0 || group >= (int)b->groups.size()) return fail(b->ctx, WT_EINVAL, "no such group");
+  const auto& g = b->groups[group];
+  if (N) *N = g.N;
+  if (precision) *precision = g.precision;
+  if (n8_path) *n8_path = g.n8 ? 1 : 0;
+  if (epb_variant) *epb_variant = g.epb_variant;
+  if (tiles) *tiles = g.ntiles;
+  return 0;
 }
 
 }  // extern "C"

@@ -172,7 +172,7 @@ int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const vo
 int launch_cons_k2(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
                    const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s, bool n8 = false);
 int launch_apply_D(const DevMesh& m, const void* u, void* out, int d, cudaStream_t s);
-// n = 8 FP64 curvilinear path: persistent, TMA-pipelined, FP64 tensor cores (wt_cons_n8.cu)
+// n = 8 curvilinear path: persistent, bulk-copy-pipelined, tensor cores (wt_cons_n8.cu)
 int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
                       void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s);
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
@@ -183,6 +183,33 @@ long long n8_padded_field_size(long long Ne);
 // the same path: K1 then writes F in the padded layout K2 reads).
 bool cons_n8_path(const DevMesh& m, const DevCoef& c, int use_metric, const ConsBC& bc, const RKStage& rkP,
                   const RKStage& rkQ, std::initializer_list<const void*> ptrs);
+
+// ---- work-list batching of many solves (one launch per kernel and group) ----
+// Everything one solve contributes to one RK4 stage: its mesh, coefficients,
+// stage inputs, scratch, boundary data and the stage updates of Phi and Pi.
+struct SolveStage {
+  const DevMesh* m = nullptr;
+  const DevCoef* c = nullptr;
+  const void* Phi = nullptr;
+  const void* Pi = nullptr;
+  void* F = nullptr;
+  void* bbuf = nullptr;
+  ConsBC bc;
+  RKStage rkP, rkQ;
+};
+// n = 8 pipelined kernels: parameter block size / fill / launch over a work
+// list of (solve, element) tiles; hP0 is the host copy of the first block
+// (stage-wide values), plist the device array of all blocks.
+size_t cons_n8_param_size(int precision, int which);
+void cons_n8_fill_params(int which, const SolveStage& ss, unsigned* flag, void* dst);
+int launch_cons_n8_batch(int which, int precision, int fp32_form, const void* hP0, const void* plist, const int2* tiles,
+                         long long ntiles, cudaStream_t s);
+// generic kernels (any N, curvilinear form): epb_variant 0 = default elements
+// per CTA, 1 = twice that (when it fits 1024 threads); chosen by the autotuner
+size_t cons_gen_param_size(int precision, int which);
+void cons_gen_fill_params(int which, const SolveStage& ss, unsigned* flag, void* dst);
+int launch_cons_gen_batch(int which, int N, int precision, int epb_variant, const void* plist, const int2* tiles,
+                          long long ntiles, cudaStream_t s);
 int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s);
 int launch_div3d(const DevMesh& m, const void* F, void* out, cudaStream_t s);
 

@@ -133,9 +133,13 @@ __device__ __forceinline__ real contract(const real* __restrict__ f, const real*
   return s;
 }
 
-template <int N, typename real, bool CURV>
-__global__ void __launch_bounds__(Ep<N>::T) k_cons_k1(const K1P<real> P) {
-  constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = Ep<N>::EPB;
+// BATCH: the CTA's elements come from a work list of (solve, element) tiles
+// and each tile reads the parameter block of its solve (plist); otherwise
+// element blockIdx.x * EPB + le of the single solve P0.  EPB_: elements per CTA.
+template <int N, typename real, bool CURV, bool BATCH, int EPB_>
+__global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0, const K1P<real>* __restrict__ plist,
+                                                            const int2* __restrict__ tiles, long long ntiles) {
+  constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = EPB_;
   __shared__ real GT[N2];
   __shared__ real su[EPB][N3];
   __shared__ real sun[EPB][6][N2];
@@ -143,8 +147,20 @@ __global__ void __launch_bounds__(Ep<N>::T) k_cons_k1(const K1P<real> P) {
   const int tid = threadIdx.x;
   const int le = tid / N3, t = tid - le * N3;
   const int i = t % N, j = (t / N) % N, k = t / N2;
-  const long long e = (long long)blockIdx.x * EPB + le;
-  const bool valid = e < P.Ne;
+  long long e = (long long)blockIdx.x * EPB + le;
+  int sid = 0;
+  bool valid;
+  if constexpr (BATCH) {
+    valid = e < ntiles;
+    if (valid) {
+      const int2 tl = tiles[e];
+      sid = tl.x;
+      e = tl.y;
+    }
+  } else {
+    valid = e < P0.Ne;
+  }
+  const K1P<real>& P = BATCH ? plist[sid] : P0;
   const long long ec = valid ? e : 0;  // clamp for address arithmetic
   const long long n = ec * N3 + t;
   const long long nn = P.nn;
@@ -340,9 +356,10 @@ struct K2P {
   unsigned int* nonfinite;
 };
 
-template <int N, typename real, bool CURV>
-__global__ void __launch_bounds__(Ep<N>::T) k_cons_k2(const K2P<real> P) {
-  constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = Ep<N>::EPB;
+template <int N, typename real, bool CURV, bool BATCH, int EPB_>
+__global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0, const K2P<real>* __restrict__ plist,
+                                                            const int2* __restrict__ tiles, long long ntiles) {
+  constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = EPB_;
   __shared__ real GT[N2];
   __shared__ real sF[EPB][3][N3];
   __shared__ real sFn[EPB][6][CURV ? 3 : 1][N2];
@@ -350,8 +367,20 @@ __global__ void __launch_bounds__(Ep<N>::T) k_cons_k2(const K2P<real> P) {
   const int tid = threadIdx.x;
   const int le = tid / N3, t = tid - le * N3;
   const int i = t % N, j = (t / N) % N, k = t / N2;
-  const long long e = (long long)blockIdx.x * EPB + le;
-  const bool valid = e < P.Ne;
+  long long e = (long long)blockIdx.x * EPB + le;
+  int sid = 0;
+  bool valid;
+  if constexpr (BATCH) {
+    valid = e < ntiles;
+    if (valid) {
+      const int2 tl = tiles[e];
+      sid = tl.x;
+      e = tl.y;
+    }
+  } else {
+    valid = e < P0.Ne;
+  }
+  const K2P<real>& P = BATCH ? plist[sid] : P0;
   const long long ec = valid ? e : 0;
   const long long n = ec * N3 + t;
   const long long nn = P.nn;
@@ -557,10 +586,9 @@ __global__ void k_ko_line(int d, int len, int closed, const int32_t* __restrict_
 
 // ---------------------------------------------------------------------------
 // launchers
-template <int N, typename real>
-static int k1_dispatch(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
-                       void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
-                       cudaStream_t s) {
+template <typename real>
+static K1P<real> k1p_params(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
+                            void* bbuf, void* grad_out, const ConsBC& bc, const RKStage& rk) {
   K1P<real> P;
   P.Ne = m.Ne; P.nn = m.nn;
   P.Phi = (const real*)Phi; P.Pi = (const real*)Pi;
@@ -576,18 +604,12 @@ static int k1_dispatch(const DevMesh& m, const DevCoef& c, const void* Phi, cons
   P.gDx = (const real*)bc.gDx; P.gDy = (const real*)bc.gDy; P.gDz = (const real*)bc.gDz;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.nonfinite = rk.nonfinite;
-  const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
-  if (use_metric)
-    k_cons_k1<N, real, true><<<blocks, Ep<N>::T, 0, s>>>(P);
-  else
-    k_cons_k1<N, real, false><<<blocks, Ep<N>::T, 0, s>>>(P);
-  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+  return P;
 }
 
-template <int N, typename real>
-static int k2_dispatch(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
-                       const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s,
-                       const void* F1 = nullptr, const void* F2 = nullptr) {
+template <typename real>
+static K2P<real> k2p_params(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
+                            const RKStage& rk, unsigned int* nonfinite, const void* F1, const void* F2) {
   K2P<real> P;
   P.Ne = m.Ne; P.nn = m.nn;
   P.F0 = (const real*)F;
@@ -600,12 +622,86 @@ static int k2_dispatch(const DevMesh& m, const void* F, void* Pidot, const void*
   P.Pidot = (real*)Pidot;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.nonfinite = nonfinite;
+  return P;
+}
+
+template <int N, typename real>
+static int k1_dispatch(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
+                       void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
+                       cudaStream_t s) {
+  const K1P<real> P = k1p_params<real>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, bc, rk);
   const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
   if (use_metric)
-    k_cons_k2<N, real, true><<<blocks, Ep<N>::T, 0, s>>>(P);
+    k_cons_k1<N, real, true, false, Ep<N>::EPB><<<blocks, Ep<N>::T, 0, s>>>(P, nullptr, nullptr, 0);
   else
-    k_cons_k2<N, real, false><<<blocks, Ep<N>::T, 0, s>>>(P);
+    k_cons_k1<N, real, false, false, Ep<N>::EPB><<<blocks, Ep<N>::T, 0, s>>>(P, nullptr, nullptr, 0);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <int N, typename real>
+static int k2_dispatch(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
+                       const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s,
+                       const void* F1 = nullptr, const void* F2 = nullptr) {
+  const K2P<real> P = k2p_params<real>(m, F, Pidot, bbuf, bc, rk, nonfinite, F1, F2);
+  const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
+  if (use_metric)
+    k_cons_k2<N, real, true, false, Ep<N>::EPB><<<blocks, Ep<N>::T, 0, s>>>(P, nullptr, nullptr, 0);
+  else
+    k_cons_k2<N, real, false, false, Ep<N>::EPB><<<blocks, Ep<N>::T, 0, s>>>(P, nullptr, nullptr, 0);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// elements per CTA of the work-list (batched) generic kernels: the default or twice it
+template <int N>
+struct EpAlt {
+  // the alternative must fit 1024 threads and the 48 KB of static shared memory
+  // of the curvilinear K1 (Phi, 6 face traces, 9 products per element, FP64)
+  static constexpr bool fits = Ep<N>::N3 * 2 * Ep<N>::EPB <= 1024 &&
+                               (10 * Ep<N>::N3 + 6 * Ep<N>::N2) * 2 * Ep<N>::EPB * 8 + 8 * Ep<N>::N2 <= 48 * 1024;
+  static constexpr int V1 = fits ? 2 * Ep<N>::EPB : Ep<N>::EPB;
+};
+
+template <int N, typename real, int EPB>
+static int gen_batch(int which, const void* plist, const int2* tiles, long long ntiles, cudaStream_t s) {
+  const unsigned blocks = (unsigned)((ntiles + EPB - 1) / EPB);
+  if (blocks == 0) return 0;
+  if (which == 1)
+    k_cons_k1<N, real, true, true, EPB><<<blocks, Ep<N>::N3 * EPB, 0, s>>>(K1P<real>(), (const K1P<real>*)plist, tiles,
+                                                                          ntiles);
+  else
+    k_cons_k2<N, real, true, true, EPB><<<blocks, Ep<N>::N3 * EPB, 0, s>>>(K2P<real>(), (const K2P<real>*)plist, tiles,
+                                                                          ntiles);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <int N>
+static int gen_batch_n(int which, int precision, int variant, const void* plist, const int2* tiles, long long ntiles,
+                       cudaStream_t s) {
+  if (precision == 0)
+    return variant ? gen_batch<N, double, EpAlt<N>::V1>(which, plist, tiles, ntiles, s)
+                   : gen_batch<N, double, Ep<N>::EPB>(which, plist, tiles, ntiles, s);
+  return variant ? gen_batch<N, float, EpAlt<N>::V1>(which, plist, tiles, ntiles, s)
+                 : gen_batch<N, float, Ep<N>::EPB>(which, plist, tiles, ntiles, s);
+}
+
+size_t cons_gen_param_size(int precision, int which) {
+  if (precision == 0) return which == 1 ? sizeof(K1P<double>) : sizeof(K2P<double>);
+  return which == 1 ? sizeof(K1P<float>) : sizeof(K2P<float>);
+}
+
+void cons_gen_fill_params(int which, const SolveStage& ss, unsigned* flag, void* dst) {
+  const DevMesh& m = *ss.m;
+  if (m.precision == 0) {
+    if (which == 1)
+      *(K1P<double>*)dst = k1p_params<double>(m, *ss.c, ss.Phi, ss.Pi, ss.F, nullptr, ss.bbuf, nullptr, ss.bc, ss.rkP);
+    else
+      *(K2P<double>*)dst = k2p_params<double>(m, ss.F, nullptr, ss.bbuf, ss.bc, ss.rkQ, flag, nullptr, nullptr);
+  } else {
+    if (which == 1)
+      *(K1P<float>*)dst = k1p_params<float>(m, *ss.c, ss.Phi, ss.Pi, ss.F, nullptr, ss.bbuf, nullptr, ss.bc, ss.rkP);
+    else
+      *(K2P<float>*)dst = k2p_params<float>(m, ss.F, nullptr, ss.bbuf, ss.bc, ss.rkQ, flag, nullptr, nullptr);
+  }
 }
 
 #define WT_DISPATCH_N(N_, CALL)   \
@@ -707,6 +803,11 @@ int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cu
   } else {
     WT_DISPATCH_N(m.N, (ko_dispatch<NN, float>(m, dst, field, koT, s)));
   }
+}
+
+int launch_cons_gen_batch(int which, int N, int precision, int epb_variant, const void* plist, const int2* tiles,
+                          long long ntiles, cudaStream_t s) {
+  WT_DISPATCH_N(N, (gen_batch_n<NN>(which, precision, epb_variant, plist, tiles, ntiles, s)));
 }
 
 }  // namespace wt

@@ -287,9 +287,14 @@ constexpr size_t k1_smem() {
   return (n8::NSTAGE * k1_stage<real>() + 9 * n8::FS + 2 * 6 * n8::N2) * sizeof(real) + n8::N2 * sizeof(double) + 64;
 }
 
-// NT: FP32 split terms (3 or 2); ignored by the FP64 form
-template <typename real, int NT>
-__global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(const K1N8<real> P) {
+// NT: FP32 split terms (3 or 2); ignored by the FP64 form.  BATCH: the
+// persistent loop runs over a work list of (solve, element) tiles and every
+// tile reads the parameter block of its solve (plist); P then only supplies
+// what is common to the launch (stage, operator, status word).
+template <typename real, int NT, bool BATCH>
+__global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
+    k_cons_k1_n8(const K1N8<real> P, const K1N8<real>* __restrict__ plist, const int2* __restrict__ tiles,
+                 long long ntiles) {
   using namespace n8;
   constexpr bool F64 = std::is_same<real, double>::value;
   constexpr bool SC = StageCoef<real>::value;
@@ -303,7 +308,6 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(c
   __shared__ int abort_flag;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
-  const long long nn = P.nn;
   const real inv2H = (real)(1.0 / (2.0 * P.H[0]));
   const bool comp_on = !F64 && P.epi && P.comp != nullptr;  // FP32 state only
   const bool need_y = P.epi && (P.stage == 1 || P.stage == 2 || (comp_on && P.stage == 3));
@@ -313,6 +317,18 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(c
   // node-phase coordinates of this thread
   const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
   const int tpad = pad(ti, tj, tk);
+  const long long T = BATCH ? ntiles : P.Ne;
+  const long long GS = gridDim.x;
+  // tile t = (solve, element); (-1, -1) past the end
+  auto tile_at = [&](long long t) -> int2 {
+    if (t >= T) return make_int2(-1, -1);
+    if constexpr (BATCH) return tiles[t];
+    else return make_int2(0, (int)t);
+  };
+  auto prm = [&](int sidx) -> const K1N8<real>& {
+    if constexpr (BATCH) return plist[sidx];
+    else return P;
+  };
 
   if (tid < N2) sG[tid] = P.G[tid];
   if (tid == 0) {
@@ -322,62 +338,69 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(c
   }
   __syncthreads();
 
-  // warp 0 stages element e into stage s: 10 whole-block copies
-  auto issue = [&](long long e, int s) {
+  // warp 0 stages tile tl into stage s: whole-block copies
+  auto issue = [&](int2 tl, int s) {
+    const K1N8<real>& Q = prm(tl.x);
+    const long long e = tl.y;
     if (lane == 0) {
       fence_proxy_async();
       mbar_expect_tx(&bar[s], tx_bytes);
     }
     __syncwarp();
     real* d = stg + s * K1_STAGE;
-    if (lane == 0) bulk_g2s(d, P.Phi + e * N3, N3 * (unsigned)sizeof(real), &bar[s]);
+    if (lane == 0) bulk_g2s(d, Q.Phi + e * N3, N3 * (unsigned)sizeof(real), &bar[s]);
     else if (lane <= 9)
-      bulk_g2s(d + N3 + (lane - 1) * FS, P.Ja + ((long long)(lane - 1) * P.Ne + e) * FS, FS * (unsigned)sizeof(real),
+      bulk_g2s(d + N3 + (lane - 1) * FS, Q.Ja + ((long long)(lane - 1) * Q.Ne + e) * FS, FS * (unsigned)sizeof(real),
                &bar[s]);
     else if (SC && lane < 20)
-      bulk_g2s(d + N3 + 9 * FS + (lane - 10) * N3, P.c10 + (lane - 10) * nn + e * N3, N3 * (unsigned)sizeof(real),
+      bulk_g2s(d + N3 + 9 * FS + (lane - 10) * N3, Q.c10 + (lane - 10) * Q.nn + e * N3, N3 * (unsigned)sizeof(real),
                &bar[s]);
   };
   // neighbour Phi face traces (384 values; threads 0..383).  The face source
-  // (8 * neighbour + neighbour face) of an element is loaded one iteration
-  // before the trace itself, so no load waits on another inside the loop.
+  // (8 * neighbour + neighbour face) of a tile is loaded one iteration before
+  // the trace itself, and the tile two iterations before, so no load waits on
+  // another inside the loop.
   const int my_f = tid >> 6, my_pq = tid & 63;
-  auto src_load = [&](long long e) -> int { return (e >= 0 && tid < 6 * N2) ? P.fsrc[my_f + 6 * e] : -1; };
-  auto face_load = [&](int src) -> real {
+  auto src_load = [&](int2 tl) -> int { return (tl.x >= 0 && tid < 6 * N2) ? prm(tl.x).fsrc[my_f + 6 * tl.y] : -1; };
+  auto face_load = [&](int src, int sidx) -> real {
     if (src < 0) return (real)0;
     const int fn = src & 7;
-    return P.Phi[(long long)(src >> 3) * N3 + face_node(faxis(fn), frow(fn, N), my_pq & 7, my_pq >> 3, N)];
+    return prm(sidx).Phi[(long long)(src >> 3) * N3 + face_node(faxis(fn), frow(fn, N), my_pq & 7, my_pq >> 3, N)];
   };
+  auto emask_at = [&](int2 tl) -> int { return tl.x >= 0 ? prm(tl.x).emask[tl.y] : 0; };
   // pointwise fields of this thread's node
   struct PW {
     real c[10], Pi, invJ, y, acc, comp;
   };
-  auto pw_load = [&](long long e, PW& w) {
-    if (e < 0) return;
-    const long long n = e * N3 + tid;
+  auto pw_load = [&](int2 tl, PW& w) {
+    if (tl.x < 0) return;
+    const K1N8<real>& Q = prm(tl.x);
+    const long long n = (long long)tl.y * N3 + tid;
     if constexpr (!SC) {
 #pragma unroll
-      for (int c = 0; c < 10; ++c) w.c[c] = P.c10[c * nn + n];
+      for (int c = 0; c < 10; ++c) w.c[c] = Q.c10[c * Q.nn + n];
     }
-    w.Pi = P.Pi[n];
-    w.invJ = P.invdetJ[n];
-    w.y = need_y ? P.y[n] : (real)0;
-    w.acc = need_acc ? P.acc[n] : (real)0;
-    w.comp = need_comp ? P.comp[n] : (real)0;
+    w.Pi = Q.Pi[n];
+    w.invJ = Q.invdetJ[n];
+    w.y = need_y ? Q.y[n] : (real)0;
+    w.acc = need_acc ? Q.acc[n] : (real)0;
+    w.comp = need_comp ? Q.comp[n] : (real)0;
   };
 
-  long long e = blockIdx.x;
+  int2 t0 = tile_at(blockIdx.x), t1 = tile_at(blockIdx.x + GS), t2 = tile_at(blockIdx.x + 2 * GS);
   PW cur;
   int emcur = 0, src1 = -1;
-  if (e < P.Ne) {
+  if (t0.x >= 0) {
     if (warp == 0)
-      for (int k = 0; k < NSTAGE - 1; ++k)
-        if (e + k * (long long)gridDim.x < P.Ne) issue(e + k * (long long)gridDim.x, k);
-    emcur = P.emask[e];
-    const real fv = face_load(src_load(e));
+      for (int k = 0; k < NSTAGE - 1; ++k) {
+        const int2 tk_ = tile_at(blockIdx.x + k * GS);
+        if (tk_.x >= 0) issue(tk_, k);
+      }
+    emcur = emask_at(t0);
+    const real fv = face_load(src_load(t0), t0.x);
     if (tid < 6 * N2) sface[tid] = fv;
-    pw_load(e, cur);
-    src1 = src_load(e + gridDim.x < P.Ne ? e + gridDim.x : -1);
+    pw_load(t0, cur);
+    src1 = src_load(t1);
   }
   __syncthreads();
   // A operand: FP64 G entries (rows gq, columns tig and 4 + tig); FP32 split pairs
@@ -390,34 +413,37 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(c
     split_G(sG, gq, tig, NT, aS, aS2);
   }
 
-  for (int it = 0; e < P.Ne; ++it, e += gridDim.x) {
+  int it = 0;
+  for (long long t = blockIdx.x; t < T; t += GS, ++it) {
     const int s = it % NSTAGE, fb = it & 1;
     const unsigned parity = (it / NSTAGE) & 1;
-    const long long en = e + gridDim.x, enn = en + gridDim.x;
-    const bool has_next = en < P.Ne;
-    const int emnext = has_next ? P.emask[en] : 0;
-    const int src2 = src_load(enn < P.Ne ? enn : -1);
-    const real fnext = face_load(has_next ? src1 : -1);
+    const int2 t3 = tile_at(t + 3 * GS);
+    const bool has_next = t1.x >= 0;
+    const int emnext = emask_at(t1);
+    const int src2 = src_load(t2);
+    const real fnext = face_load(has_next ? src1 : -1, t1.x);
     PW nxt;
-    pw_load(has_next ? en : -1, nxt);
+    pw_load(t1, nxt);
     // One thread polls the stage's mbarrier (its acquire makes the copied data
     // visible; the barrier below orders every other thread after it), so the
     // other warps do not spend issue slots spinning.
     if (tid == 0 && !wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
     // After this barrier every thread has finished the previous element, so its
-    // stage (reused for element e + (NSTAGE - 1) grid), the partial gradients
-    // and face buffer fb^1 are free.
+    // stage (reused for tile t + (NSTAGE - 1) grid), the partial gradients and
+    // face buffer fb^1 are free.
     __syncthreads();
     if (abort_flag) {  // wait (bounded) for the copies still in flight, then leave
       if (warp == 0 && lane == 0)
         for (int k = 1; k < NSTAGE - 1; ++k)
-          if (e + k * (long long)gridDim.x < P.Ne) wait_phase(&bar[(it + k) % NSTAGE], ((it + k) / NSTAGE) & 1, nullptr);
+          if (tile_at(t + k * GS).x >= 0) wait_phase(&bar[(it + k) % NSTAGE], ((it + k) / NSTAGE) & 1, nullptr);
       return;
     }
     {
-      const long long ei = e + (NSTAGE - 1) * (long long)gridDim.x;
-      if (warp == 0 && ei < P.Ne) issue(ei, (it + NSTAGE - 1) % NSTAGE);
+      const int2 ti_ = NSTAGE == 2 ? t1 : tile_at(t + (NSTAGE - 1) * GS);
+      if (warp == 0 && ti_.x >= 0) issue(ti_, (it + NSTAGE - 1) % NSTAGE);
     }
+    const K1N8<real>& Q = prm(t0.x);
+    const long long e = t0.y;
     const real* d = stg + s * K1_STAGE;
     const real* sPhi = d;      // unpadded
     const real* sJa = d + N3;  // 9 padded fields, index (al*3 + c)
@@ -515,63 +541,66 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1) k_cons_k1_n8(c
       const real F1 = b1 * Pi + (K1v * g0 + K3 * g1 + K4 * g2);
       const real F2 = b2 * Pi + (K2 * g0 + K4 * g1 + K5 * g2);
       real phid = b0 * g0 + b1 * g1 + b2 * g2 + a * Pi;
-      if (bnd && P.bc_on) {
+      if (bnd && Q.bc_on) {
         const int idx3[3] = {ti, tj, tk};
         for (int f = 0; f < 6; ++f) {
-          const int tag = P.bdry[f + 6 * e];
+          const int tag = Q.bdry[f + 6 * e];
           if (tag == 0) continue;
           const int ax = f >> 1;
           if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
           const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
-          const int slot = P.bslot[f + 6 * e];
+          const int slot = Q.bslot[f + 6 * e];
           real dF = 0, dP = 0;
-          if (tag != P.exc_tag) {
-            const long long nb = (long long)P.nbf * N2;
+          if (tag != Q.exc_tag) {
+            const long long nb = (long long)Q.nbf * N2;
             const long long bi = (long long)slot * N2 + p + 8 * q;
-            const real nx = P.bnorm[bi], ny = P.bnorm[nb + bi], nz = P.bnorm[2 * nb + bi], wt = P.bnorm[3 * nb + bi];
+            const real nx = Q.bnorm[bi], ny = Q.bnorm[nb + bi], nz = Q.bnorm[2 * nb + bi], wt = Q.bnorm[3 * nb + bi];
             const real Kn =
                 K0 * nx * nx + K3 * ny * ny + K5 * nz * nz + (real)2 * (K1v * nx * ny + K2 * nx * nz + K4 * ny * nz);
             const real a_n = sqrt(a * Kn);
             const real bn_ = b0 * nx + b1 * ny + b2 * nz;
-            const real sigma = (real)P.sigma;
-            if (P.kind == 4) {
+            const real sigma = (real)Q.sigma;
+            if (Q.kind == 4) {
               const real tau = sigma * (fabs(a_n - bn_) + fabs(a_n + bn_)) * wt;
-              const real gp = P.gPhi ? P.gPhi[n] : (real)0, gqv = P.gPi ? P.gPi[n] : (real)0;
+              const real gp = Q.gPhi ? Q.gPhi[n] : (real)0, gqv = Q.gPi ? Q.gPi[n] : (real)0;
               dF = -tau * (u - gp);
               dP = -tau * (Pi - gqv);
             } else {
               const real qv = nx * g0 + ny * g1 + nz * g2;
               const real rr = Pi + ((bn_ + a_n) / a) * qv;
               real gv = 0;
-              if (P.kind != 2) {
-                const real gqv = P.gPi ? P.gPi[n] : (real)0;
-                const real gx = P.gDx ? P.gDx[n] : (real)0, gy = P.gDy ? P.gDy[n] : (real)0,
-                           gz = P.gDz ? P.gDz[n] : (real)0;
+              if (Q.kind != 2) {
+                const real gqv = Q.gPi ? Q.gPi[n] : (real)0;
+                const real gx = Q.gDx ? Q.gDx[n] : (real)0, gy = Q.gDy ? Q.gDy[n] : (real)0,
+                           gz = Q.gDz ? Q.gDz[n] : (real)0;
                 gv = gqv + ((bn_ + a_n) / a) * (nx * gx + ny * gy + nz * gz);
               }
               dP = -sigma * fabs(a_n + bn_) * wt * (rr - gv);
             }
           }
           phid += dF;
-          P.bbuf[(long long)slot * N2 + p + 8 * q] = dP;
+          Q.bbuf[(long long)slot * N2 + p + 8 * q] = dP;
         }
       }
       {  // flux in the padded element-block layout read by K2
-        const long long fo = e * FS + tpad, fstr = P.Ne * FS;
-        P.F[fo] = F0;
-        P.F[fstr + fo] = F1;
-        P.F[2 * fstr + fo] = F2;
+        const long long fo = e * FS + tpad, fstr = Q.Ne * FS;
+        Q.F[fo] = F0;
+        Q.F[fstr + fo] = F1;
+        Q.F[2 * fstr + fo] = F2;
       }
       if (P.epi)
-        n8_rk<real>(P.stage, P.dt, phid, u, cur.y, cur.acc, cur.comp, n, P.y, P.acc, P.out, comp_on ? P.comp : nullptr,
+        n8_rk<real>(P.stage, Q.dt, phid, u, cur.y, cur.acc, cur.comp, n, Q.y, Q.acc, Q.out, comp_on ? Q.comp : nullptr,
                     P.flag);
       else
-        P.Phidot[n] = phid;
+        Q.Phidot[n] = phid;
     }
     if (has_next && tid < 6 * N2) sface[(fb ^ 1) * 6 * N2 + tid] = fnext;
     cur = nxt;
     emcur = emnext;
     src1 = src2;
+    t0 = t1;
+    t1 = t2;
+    t2 = t3;
   }
 }
 
@@ -612,8 +641,10 @@ constexpr size_t k2_smem() {
   return (n8::NSTAGE * K2_STAGE + 6 * n8::FS + 2 * 6 * 3 * n8::N2) * sizeof(real) + n8::N2 * sizeof(double) + 64;
 }
 
-template <typename real, int NT>
-__global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2) k_cons_k2_n8(const K2N8<real> P) {
+template <typename real, int NT, bool BATCH>
+__global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
+    k_cons_k2_n8(const K2N8<real> P, const K2N8<real>* __restrict__ plist, const int2* __restrict__ tiles,
+                 long long ntiles) {
   using namespace n8;
   constexpr bool F64 = std::is_same<real, double>::value;
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -634,6 +665,17 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2) k_cons_k2_n8(c
   const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
   const int tpad = pad(ti, tj, tk);
   constexpr int NFACE = 6 * 3 * N2;  // 1152
+  const long long T = BATCH ? ntiles : P.Ne;
+  const long long GS = gridDim.x;
+  auto tile_at = [&](long long t) -> int2 {
+    if (t >= T) return make_int2(-1, -1);
+    if constexpr (BATCH) return tiles[t];
+    else return make_int2(0, (int)t);
+  };
+  auto prm = [&](int sidx) -> const K2N8<real>& {
+    if constexpr (BATCH) return plist[sidx];
+    else return P;
+  };
 
   if (tid < N2) sG[tid] = P.G[tid];
   if (tid == 0) {
@@ -643,7 +685,9 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2) k_cons_k2_n8(c
   }
   __syncthreads();
 
-  auto issue = [&](long long e, int s) {
+  auto issue = [&](int2 tl, int s) {
+    const K2N8<real>& Q = prm(tl.x);
+    const long long e = tl.y;
     if (lane == 0) {
       fence_proxy_async();
       mbar_expect_tx(&bar[s], tx_bytes);
@@ -651,64 +695,69 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2) k_cons_k2_n8(c
     __syncwarp();
     real* d = stg + s * K2_STAGE;
     if (lane < K2_NF) {
-      const real* src = lane < 3 ? (lane == 0 ? P.F0 : lane == 1 ? P.F1 : P.F2) + e * FS
-                                 : P.Ja + ((long long)(lane - 3) * P.Ne + e) * FS;
+      const real* src = lane < 3 ? (lane == 0 ? Q.F0 : lane == 1 ? Q.F1 : Q.F2) + e * FS
+                                 : Q.Ja + ((long long)(lane - 3) * Q.Ne + e) * FS;
       bulk_g2s(d + lane * FS, src, FS * (unsigned)sizeof(real), &bar[s]);
     }
   };
   // neighbour flux face traces: [f][c][pq], 1152 values, <= 3 per thread; the
   // face sources are loaded one iteration ahead of the traces (see K1)
-  auto src_load = [&](long long e, int src[3]) {
+  auto src_load = [&](int2 tl, int src[3]) {
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
       const int idx = tid + r * THREADS;
-      src[r] = (e >= 0 && idx < NFACE) ? P.fsrc[idx / (3 * N2) + 6 * e] : -1;
+      src[r] = (tl.x >= 0 && idx < NFACE) ? prm(tl.x).fsrc[idx / (3 * N2) + 6 * tl.y] : -1;
     }
   };
-  auto face_load = [&](const int src[3], real fv[3]) {
+  auto face_load = [&](const int src[3], int sidx, real fv[3]) {
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
       const int idx = tid + r * THREADS;
       real v = 0;
       if (src[r] >= 0) {
+        const K2N8<real>& Q = prm(sidx);
         const int rem = idx % (3 * N2), c = rem >> 6, pq = rem & 63;
         const int fn = src[r] & 7;
-        const real* Fc = c == 0 ? P.F0 : c == 1 ? P.F1 : P.F2;
+        const real* Fc = c == 0 ? Q.F0 : c == 1 ? Q.F1 : Q.F2;
         const int fnode = face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N);
         v = Fc[(long long)(src[r] >> 3) * FS + pad(fnode & 7, (fnode >> 3) & 7, fnode >> 6)];
       }
       fv[r] = v;
     }
   };
+  auto emask_at = [&](int2 tl) -> int { return tl.x >= 0 ? prm(tl.x).emask[tl.y] : 0; };
   struct PW {
     real invJ, y, acc, comp;
   };
-  auto pw_load = [&](long long e, PW& w) {
-    if (e < 0) return;
-    const long long n = e * N3 + tid;
-    w.invJ = P.invdetJ[n];
-    w.y = need_y ? P.y[n] : (real)0;
-    w.acc = need_acc ? P.acc[n] : (real)0;
-    w.comp = need_comp ? P.comp[n] : (real)0;
+  auto pw_load = [&](int2 tl, PW& w) {
+    if (tl.x < 0) return;
+    const K2N8<real>& Q = prm(tl.x);
+    const long long n = (long long)tl.y * N3 + tid;
+    w.invJ = Q.invdetJ[n];
+    w.y = need_y ? Q.y[n] : (real)0;
+    w.acc = need_acc ? Q.acc[n] : (real)0;
+    w.comp = need_comp ? Q.comp[n] : (real)0;
   };
 
-  long long e = blockIdx.x;
+  int2 t0 = tile_at(blockIdx.x), t1 = tile_at(blockIdx.x + GS), t2 = tile_at(blockIdx.x + 2 * GS);
   PW cur;
   int emcur = 0, src1[3] = {-1, -1, -1};
-  if (e < P.Ne) {
+  if (t0.x >= 0) {
     if (warp == 0)
-      for (int k = 0; k < NSTAGE - 1; ++k)
-        if (e + k * (long long)gridDim.x < P.Ne) issue(e + k * (long long)gridDim.x, k);
-    emcur = P.emask[e];
+      for (int k = 0; k < NSTAGE - 1; ++k) {
+        const int2 tk_ = tile_at(blockIdx.x + k * GS);
+        if (tk_.x >= 0) issue(tk_, k);
+      }
+    emcur = emask_at(t0);
     int src0[3];
-    src_load(e, src0);
+    src_load(t0, src0);
     real fv[3];
-    face_load(src0, fv);
+    face_load(src0, t0.x, fv);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
       if (tid + r * THREADS < NFACE) sface[tid + r * THREADS] = fv[r];
-    pw_load(e, cur);
-    src_load(e + gridDim.x < P.Ne ? e + gridDim.x : -1, src1);
+    pw_load(t0, cur);
+    src_load(t1, src1);
   }
   __syncthreads();
   double aG0 = 0.0, aG1 = 0.0;
@@ -720,18 +769,19 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2) k_cons_k2_n8(c
     split_G(sG, gq, tig, NT, aS, aS2);
   }
 
-  for (int it = 0; e < P.Ne; ++it, e += gridDim.x) {
+  int it = 0;
+  for (long long t = blockIdx.x; t < T; t += GS, ++it) {
     const int s = it % NSTAGE, fb = it & 1;
     const unsigned parity = (it / NSTAGE) & 1;
-    const long long en = e + gridDim.x, enn = en + gridDim.x;
-    const bool has_next = en < P.Ne;
-    const int emnext = has_next ? P.emask[en] : 0;
+    const int2 t3 = tile_at(t + 3 * GS);
+    const bool has_next = t1.x >= 0;
+    const int emnext = emask_at(t1);
     int src2[3];
-    src_load(enn < P.Ne ? enn : -1, src2);
+    src_load(t2, src2);
     real fnext[3];
-    face_load(src1, fnext);
+    face_load(src1, t1.x, fnext);
     PW nxt;
-    pw_load(has_next ? en : -1, nxt);
+    pw_load(t1, nxt);
     // One thread polls the stage's mbarrier (its acquire makes the copied data
     // visible; the barrier below orders every other thread after it), so the
     // other warps do not spend issue slots spinning.
@@ -740,13 +790,15 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2) k_cons_k2_n8(c
     if (abort_flag) {  // wait (bounded) for the copies still in flight, then leave
       if (warp == 0 && lane == 0)
         for (int k = 1; k < NSTAGE - 1; ++k)
-          if (e + k * (long long)gridDim.x < P.Ne) wait_phase(&bar[(it + k) % NSTAGE], ((it + k) / NSTAGE) & 1, nullptr);
+          if (tile_at(t + k * GS).x >= 0) wait_phase(&bar[(it + k) % NSTAGE], ((it + k) / NSTAGE) & 1, nullptr);
       return;
     }
     {
-      const long long ei = e + (NSTAGE - 1) * (long long)gridDim.x;
-      if (warp == 0 && ei < P.Ne) issue(ei, (it + NSTAGE - 1) % NSTAGE);
+      const int2 ti_ = NSTAGE == 2 ? t1 : tile_at(t + (NSTAGE - 1) * GS);
+      if (warp == 0 && ti_.x >= 0) issue(ti_, (it + NSTAGE - 1) % NSTAGE);
     }
+    const K2N8<real>& Q = prm(t0.x);
+    const long long e = t0.y;
     const real* d = stg + s * K2_STAGE;
     const real* sF = d;           // 3 fields
     const real* sJa = d + 3 * FS;  // 9 fields
@@ -826,21 +878,21 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2) k_cons_k2_n8(c
       real dv = ((sdiv[tpad] + sdiv[2 * FS + tpad]) + sdiv[4 * FS + tpad]) +
                 ((sdiv[FS + tpad] + sdiv[3 * FS + tpad]) + sdiv[5 * FS + tpad]);
       dv *= cur.invJ;
-      if (bnd && P.bc_on) {
+      if (bnd && Q.bc_on) {
         const int idx3[3] = {ti, tj, tk};
         for (int f = 0; f < 6; ++f) {
-          if (P.bdry[f + 6 * e] == 0) continue;
+          if (Q.bdry[f + 6 * e] == 0) continue;
           const int ax = f >> 1;
           if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
           const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
-          dv += P.bbuf[(long long)P.bslot[f + 6 * e] * N2 + p + 8 * q];
+          dv += Q.bbuf[(long long)Q.bslot[f + 6 * e] * N2 + p + 8 * q];
         }
       }
       if (P.epi)
-        n8_rk<real>(P.stage, P.dt, dv, cur.y, cur.y, cur.acc, cur.comp, n, P.y, P.acc, P.out,
-                    comp_on ? P.comp : nullptr, P.flag);
+        n8_rk<real>(P.stage, Q.dt, dv, cur.y, cur.y, cur.acc, cur.comp, n, Q.y, Q.acc, Q.out,
+                    comp_on ? Q.comp : nullptr, P.flag);
       else
-        P.Pidot[n] = dv;
+        Q.Pidot[n] = dv;
     }
     if (has_next) {
 #pragma unroll
@@ -851,6 +903,9 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2) k_cons_k2_n8(c
     emcur = emnext;
 #pragma unroll
     for (int r = 0; r < 3; ++r) src1[r] = src2[r];
+    t0 = t1;
+    t1 = t2;
+    t2 = t3;
   }
 }
 
@@ -888,9 +943,9 @@ static int sm_count() {
   return n;
 }
 
-template <typename real, int NT>
-static int k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
-                 void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s) {
+template <typename real>
+static K1N8<real> k1n8_params(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F,
+                              void* Phidot, void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag) {
   K1N8<real> P;
   P.Ne = m.Ne; P.nn = m.nn;
   P.Phi = (const real*)Phi; P.Pi = (const real*)Pi; P.c10 = (const real*)c.c10;
@@ -904,22 +959,12 @@ static int k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void
   P.gDx = (const real*)bc.gDx; P.gDy = (const real*)bc.gDy; P.gDz = (const real*)bc.gDz;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_cons_k1_n8<real, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k1_smem<real>()) !=
-        cudaSuccess)
-      return -2;
-    attr = true;
-  }
-  const long long cap = (long long)sm_count() * n8::Occ<real>::k1;
-  const long long grid = m.Ne < cap ? m.Ne : cap;
-  k_cons_k1_n8<real, NT><<<(unsigned)grid, n8::THREADS, k1_smem<real>(), s>>>(P);
-  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+  return P;
 }
 
-template <typename real, int NT>
-static int k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc, const RKStage& rk,
-                 unsigned* flag, cudaStream_t s) {
+template <typename real>
+static K2N8<real> k2n8_params(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
+                              const RKStage& rk, unsigned* flag) {
   K2N8<real> P;
   P.Ne = m.Ne; P.nn = m.nn;
   P.F0 = (const real*)F; P.F1 = (const real*)F + m.Ne * n8::FS; P.F2 = (const real*)F + 2 * m.Ne * n8::FS;
@@ -930,31 +975,94 @@ static int k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf,
   P.Pidot = (real*)Pidot;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_cons_k2_n8<real, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k2_smem<real>()) !=
-        cudaSuccess)
-      return -2;
-    attr = true;
+  return P;
+}
+
+// Launch K1 (which = 1) or K2 (which = 2) of one instantiation: a single solve
+// (plist == nullptr, ntiles = P.Ne) or a work list over the solves of plist.
+template <typename real, int NT, bool BATCH>
+static int n8_launch(int which, const void* hP, const void* plist, const int2* tiles, long long ntiles, cudaStream_t s) {
+  static bool attr1 = false, attr2 = false;
+  if (which == 1) {
+    if (!attr1) {
+      if (cudaFuncSetAttribute(k_cons_k1_n8<real, NT, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)k1_smem<real>()) != cudaSuccess)
+        return -2;
+      attr1 = true;
+    }
+    const long long cap = (long long)sm_count() * n8::Occ<real>::k1;
+    const long long grid = ntiles < cap ? ntiles : cap;
+    if (grid <= 0) return 0;
+    k_cons_k1_n8<real, NT, BATCH><<<(unsigned)grid, n8::THREADS, k1_smem<real>(), s>>>(
+        *(const K1N8<real>*)hP, (const K1N8<real>*)plist, tiles, ntiles);
+  } else {
+    if (!attr2) {
+      if (cudaFuncSetAttribute(k_cons_k2_n8<real, NT, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)k2_smem<real>()) != cudaSuccess)
+        return -2;
+      attr2 = true;
+    }
+    const long long cap = (long long)sm_count() * n8::Occ<real>::k2;
+    const long long grid = ntiles < cap ? ntiles : cap;
+    if (grid <= 0) return 0;
+    k_cons_k2_n8<real, NT, BATCH><<<(unsigned)grid, n8::THREADS, k2_smem<real>(), s>>>(
+        *(const K2N8<real>*)hP, (const K2N8<real>*)plist, tiles, ntiles);
   }
-  const long long cap = (long long)sm_count() * n8::Occ<real>::k2;
-  const long long grid = m.Ne < cap ? m.Ne : cap;
-  k_cons_k2_n8<real, NT><<<(unsigned)grid, n8::THREADS, k2_smem<real>(), s>>>(P);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <bool BATCH>
+static int n8_dispatch(int which, int precision, int fp32_form, const void* hP, const void* plist, const int2* tiles,
+                       long long ntiles, cudaStream_t s) {
+  if (precision == 0) return n8_launch<double, 0, BATCH>(which, hP, plist, tiles, ntiles, s);
+  if (fp32_form == WT_FP32_BF16X2) return n8_launch<float, 2, BATCH>(which, hP, plist, tiles, ntiles, s);
+  return n8_launch<float, 3, BATCH>(which, hP, plist, tiles, ntiles, s);
 }
 
 int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
                       void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s) {
-  if (m.precision == 0) return k1_n8<double, 0>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag, s);
-  return m.fp32_form == WT_FP32_BF16X2 ? k1_n8<float, 2>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag, s)
-                                       : k1_n8<float, 3>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag, s);
+  if (m.precision == 0) {
+    const K1N8<double> P = k1n8_params<double>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag);
+    return n8_dispatch<false>(1, 0, m.fp32_form, &P, nullptr, nullptr, m.Ne, s);
+  }
+  const K1N8<float> P = k1n8_params<float>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag);
+  return n8_dispatch<false>(1, 1, m.fp32_form, &P, nullptr, nullptr, m.Ne, s);
 }
 
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
                       const RKStage& rk, unsigned* flag, cudaStream_t s) {
-  if (m.precision == 0) return k2_n8<double, 0>(m, F, Pidot, bbuf, bc, rk, flag, s);
-  return m.fp32_form == WT_FP32_BF16X2 ? k2_n8<float, 2>(m, F, Pidot, bbuf, bc, rk, flag, s)
-                                       : k2_n8<float, 3>(m, F, Pidot, bbuf, bc, rk, flag, s);
+  if (m.precision == 0) {
+    const K2N8<double> P = k2n8_params<double>(m, F, Pidot, bbuf, bc, rk, flag);
+    return n8_dispatch<false>(2, 0, m.fp32_form, &P, nullptr, nullptr, m.Ne, s);
+  }
+  const K2N8<float> P = k2n8_params<float>(m, F, Pidot, bbuf, bc, rk, flag);
+  return n8_dispatch<false>(2, 1, m.fp32_form, &P, nullptr, nullptr, m.Ne, s);
+}
+
+// ---- work-list batching -------------------------------------------------------------
+size_t cons_n8_param_size(int precision, int which) {
+  if (precision == 0) return which == 1 ? sizeof(K1N8<double>) : sizeof(K2N8<double>);
+  return which == 1 ? sizeof(K1N8<float>) : sizeof(K2N8<float>);
+}
+
+void cons_n8_fill_params(int which, const SolveStage& ss, unsigned* flag, void* dst) {
+  const DevMesh& m = *ss.m;
+  if (m.precision == 0) {
+    if (which == 1)
+      *(K1N8<double>*)dst = k1n8_params<double>(m, *ss.c, ss.Phi, ss.Pi, ss.F, nullptr, ss.bbuf, ss.bc, ss.rkP, flag);
+    else
+      *(K2N8<double>*)dst = k2n8_params<double>(m, ss.F, nullptr, ss.bbuf, ss.bc, ss.rkQ, flag);
+  } else {
+    if (which == 1)
+      *(K1N8<float>*)dst = k1n8_params<float>(m, *ss.c, ss.Phi, ss.Pi, ss.F, nullptr, ss.bbuf, ss.bc, ss.rkP, flag);
+    else
+      *(K2N8<float>*)dst = k2n8_params<float>(m, ss.F, nullptr, ss.bbuf, ss.bc, ss.rkQ, flag);
+  }
+}
+
+int launch_cons_n8_batch(int which, int precision, int fp32_form, const void* hP0, const void* plist, const int2* tiles,
+                         long long ntiles, cudaStream_t s) {
+  return n8_dispatch<true>(which, precision, fp32_form, hP0, plist, tiles, ntiles, s);
 }
 
 }  // namespace wt

@@ -87,6 +87,12 @@ def library():
         "wt_rhs_curved": [vp, vp, vp, vp, vp, vp, vp, d, C.POINTER(_BcDesc), i],
         "wt_rhs_curved_noalloc": [vp, vp, vp, vp, vp, vp, d, d, C.POINTER(_BcDesc), i],
         "wt_mesh_set_fp32_form": [vp, i],
+        "wt_mesh_release_setup_geometry": [vp],
+        "wt_batch_create": [vp, C.POINTER(vp)], "wt_batch_destroy": [vp],
+        "wt_batch_add": [vp, vp, vp, vp, vp, d, C.POINTER(_BcDesc), C.POINTER(i)],
+        "wt_batch_remove": [vp, i], "wt_batch_set_autotune": [vp, i], "wt_batch_step": [vp, i],
+        "wt_batch_info": [vp, C.POINTER(i), C.POINTER(ll), C.POINTER(i)],
+        "wt_batch_group_info": [vp, i, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(ll)],
         "wt_apply_D": [vp, vp, vp, vp, i], "wt_ko_add": [vp, vp, vp, vp, d],
         "wt_gradient3d": [vp, vp, vp, vp, vp, vp], "wt_divergence3d": [vp, vp, vp, vp, vp, vp],
         "wt_rhs_sipg": [vp, vp, vp, vp, vp, C.POINTER(C.c_double * 6), d, d],
@@ -183,7 +189,7 @@ class Context:
         workspaces and coefficients, then meshes)."""
         if getattr(self, "h", None):
             alive = [r() for r in getattr(self, "_children", [])]
-            for kind in (Workspace, Coef, Mesh):
+            for kind in (Batch, Workspace, Coef, Mesh):
                 for o in alive:
                     if isinstance(o, kind):
                         o.close()
@@ -271,6 +277,10 @@ class Mesh(_Child):
         import numpy as np
         b = np.ascontiguousarray(bdry, dtype=np.int32)
         self.ctx.check(library().wt_mesh_set_bdry(self.h, b.ctypes.data), "wt_mesh_set_bdry")
+
+    def release_setup_geometry(self):
+        """Free the FP64 set-up geometry the RK4 path does not read (see wt_mesh_release_setup_geometry)."""
+        self.ctx.check(library().wt_mesh_release_setup_geometry(self.h), "wt_mesh_release_setup_geometry")
 
     def set_fp32_form(self, form: int):
         """Select how an FP32 mesh evaluates the n = 8 contractions (FP32_* constants)."""
@@ -370,6 +380,66 @@ class Workspace(_Child):
     def close(self):
         if getattr(self, "h", None) and self._ctx_alive():
             library().wt_workspace_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch(_Child):
+    """Many independent solves advanced together (wt_batch_*; no counterpart in the
+    reference, which runs one solve per evolve3d call).
+
+    Members are (workspace, coefficients, Phi, Pi, dt, bc) sets on curvilinear
+    meshes of any order and size.  Solves of one (n, precision, path) group run
+    as one work list of (solve, element) tiles per kernel launch, one RK4 step
+    of all groups is a CUDA graph, and the elements per CTA of the generic
+    kernels are picked by timing when the membership changes."""
+
+    def __init__(self, ctx: Context, autotune: bool = True):
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        ctx.check(library().wt_batch_create(ctx.h, C.byref(self.h)), "wt_batch_create")
+        ctx._adopt(self)
+        self._keep = {}
+        if not autotune:
+            ctx.check(library().wt_batch_set_autotune(self.h, 0), "wt_batch_set_autotune")
+
+    def add(self, Phi, Pi, coef: "Coef", ws: "Workspace", dt: float, bc3d: Optional["BC3D"] = None) -> int:
+        p, keep = _bcptr(bc3d)
+        slot = C.c_int()
+        self.ctx.check(library().wt_batch_add(self.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt), p,
+                                              C.byref(slot)), "wt_batch_add")
+        self._keep[slot.value] = (Phi, Pi, coef, ws, keep, p)
+        return slot.value
+
+    def remove(self, slot: int):
+        self.ctx.check(library().wt_batch_remove(self.h, int(slot)), "wt_batch_remove")
+        self._keep.pop(slot, None)
+
+    def step(self, nsteps: int = 1):
+        self.ctx.check(library().wt_batch_step(self.h, int(nsteps)), "wt_batch_step")
+
+    def info(self):
+        ns, nn, ng = C.c_int(), C.c_longlong(), C.c_int()
+        self.ctx.check(library().wt_batch_info(self.h, C.byref(ns), C.byref(nn), C.byref(ng)), "wt_batch_info")
+        return ns.value, nn.value, ng.value
+
+    def groups(self):
+        """[(N, precision, n8_path, epb_variant, tiles)] per group."""
+        out = []
+        for g in range(self.info()[2]):
+            v = [C.c_int() for _ in range(4)] + [C.c_longlong()]
+            self.ctx.check(library().wt_batch_group_info(self.h, g, *[C.byref(x) for x in v]), "wt_batch_group_info")
+            out.append(tuple(x.value for x in v))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None) and self._ctx_alive():
+            library().wt_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):
