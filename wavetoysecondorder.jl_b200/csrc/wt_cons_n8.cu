@@ -187,11 +187,12 @@ template <>
 struct Occ<float> {
   static constexpr int k1 = 2, k2 = 2;
 };
-// FP32 K1 stages the ten background coefficients with the copies (instead of
-// prefetching them into registers), so that two CTAs fit on an SM
+// K1 stages the ten background coefficients with the copies instead of
+// prefetching them into registers (FP32: two CTAs then fit on an SM; FP64:
+// the registers go to the contraction pass)
 template <typename real>
 struct StageCoef {
-  static constexpr bool value = !std::is_same<real, double>::value;
+  static constexpr bool value = true;
 };
 
 }  // namespace n8
@@ -417,7 +418,16 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
   for (long long t = blockIdx.x; t < T; t += GS, ++it) {
     const int s = it % NSTAGE, fb = it & 1;
     const unsigned parity = (it / NSTAGE) & 1;
-    const int2 t3 = tile_at(t + 3 * GS);
+    // tiles t, t + grid, t + 2 grid: carried in registers for a work list (loaded
+    // ahead), recomputed from t for a single solve
+    int2 t3 = make_int2(-1, -1);
+    if constexpr (BATCH) {
+      t3 = tile_at(t + 3 * GS);
+    } else {
+      t0 = tile_at(t);
+      t1 = tile_at(t + GS);
+      t2 = tile_at(t + 2 * GS);
+    }
     const bool has_next = t1.x >= 0;
     const int emnext = emask_at(t1);
     const int src2 = src_load(t2);
@@ -598,9 +608,11 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
     cur = nxt;
     emcur = emnext;
     src1 = src2;
-    t0 = t1;
-    t1 = t2;
-    t2 = t3;
+    if constexpr (BATCH) {
+      t0 = t1;
+      t1 = t2;
+      t2 = t3;
+    }
   }
 }
 
@@ -773,7 +785,16 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
   for (long long t = blockIdx.x; t < T; t += GS, ++it) {
     const int s = it % NSTAGE, fb = it & 1;
     const unsigned parity = (it / NSTAGE) & 1;
-    const int2 t3 = tile_at(t + 3 * GS);
+    // tiles t, t + grid, t + 2 grid: carried in registers for a work list (loaded
+    // ahead), recomputed from t for a single solve
+    int2 t3 = make_int2(-1, -1);
+    if constexpr (BATCH) {
+      t3 = tile_at(t + 3 * GS);
+    } else {
+      t0 = tile_at(t);
+      t1 = tile_at(t + GS);
+      t2 = tile_at(t + 2 * GS);
+    }
     const bool has_next = t1.x >= 0;
     const int emnext = emask_at(t1);
     int src2[3];
@@ -903,9 +924,11 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
     emcur = emnext;
 #pragma unroll
     for (int r = 0; r < 3; ++r) src1[r] = src2[r];
-    t0 = t1;
-    t1 = t2;
-    t2 = t3;
+    if constexpr (BATCH) {
+      t0 = t1;
+      t1 = t2;
+      t2 = t3;
+    }
   }
 }
 
