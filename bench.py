@@ -267,9 +267,34 @@ def run_ours(args):
 
     # end to end through the host-buffer API: pinned host state in, one RK4 step
     # per sample, state + energy back to the host after every step
+    e2e = None
+    if prec == wt.WT_F32:
+        # FP32 state: the same shape through the public API with torch copies
+        Ph = torch.empty(nn, dtype=torch.float32, pin_memory=True)
+        Qh = torch.empty(nn, dtype=torch.float32, pin_memory=True)
+        Ph.copy_(Phi.cpu())
+        Qh.copy_(Pi.cpu())
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        Phi.copy_(Ph, non_blocking=True)
+        Pi.copy_(Qh, non_blocking=True)
+        for _ in range(args.steps):
+            wt.step_rk4_curved(Phi, Pi, coef, ws, dt, 1, eps_KO=0.0, bc3d=bc, metric=True)
+            Ph.copy_(Phi, non_blocking=True)
+            Qh.copy_(Pi, non_blocking=True)
+            wt.wave3d_energy(Phi, Pi, coef, ws, metric=True)
+        torch.cuda.synchronize()
+        te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        te = float(te.item())
+        e2e = {"value": 2.0 * nn * args.steps * world / te, "unit": "DOF-updates/s",
+               "h2d_bytes_per_step": int(2 * nn * 4 / args.steps), "d2h_bytes_per_step": int(2 * nn * 4 + 8),
+               "api": "step_rk4_curved + wave3d_energy, state copied to pinned host buffers every step"}
     Ph = torch.empty(nn, dtype=torch.float64, pin_memory=True)
     Qh = torch.empty(nn, dtype=torch.float64, pin_memory=True)
-    e2e = None
     if prec == wt.WT_F64:
         Ph.copy_(Phi.cpu())
         Qh.copy_(Pi.cpu())
@@ -332,6 +357,142 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batch(args):
+    """Batched uneven solves: args.solves warped-cube solves (e ~ U{4..24}, n ~ {4,6,8},
+    flat or perturbed ADM), FP32 split-precision form, advanced together by the
+    batch (work-list kernels, CUDA graph per RK4 step, autotuned CTA shapes) for
+    args.batch_steps steps; beside it the per-solve loop of the plain FP64 and
+    FP32 forms timed on a sample of the same solves."""
+    import numpy as np
+    import torch
+    wt = package()
+    S = wt.serve
+    ctx = wt.Context(0)
+    specs = wt.workloads.batch_specs(args.seed, args.solves)
+    reqs = [S.Request(rid=k, arrival=0.0, elements=d["elements"], n=d["n"], steps=args.batch_steps, seed=d["seed"],
+                      scale=d["scale"], pulses=2) for k, d in enumerate(specs)]
+    t_setup = time.perf_counter()
+    solves = [S.build_solve(ctx, q, wt.WT_F32) for q in reqs]
+    t_setup = time.perf_counter() - t_setup
+    batch = wt.Batch(ctx)
+    bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+    for (mesh, coef, ws, Phi, Pi, dt) in solves:
+        batch.add(Phi, Pi, coef, ws, dt, bc)
+    nodes = sum(m.nn for (m, *_r) in solves)
+    batch.step(args.warmup)  # builds the work lists, tunes, captures the graph
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    n0 = ctx.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    batch.step(args.batch_steps)
+    ev1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    t = ev0.elapsed_time(ev1) / 1000.0
+    launches = ctx.launch_count() - n0
+    groups = batch.groups()
+    finite = not ctx.nonfinite()
+    value = 2.0 * nodes * args.batch_steps / t
+    # per-solve loops of the plain forms on a sample: the smallest and largest solves
+    order = sorted(range(len(reqs)), key=lambda k: reqs[k].nodes)
+    sample = order[:8] + order[-4:]
+    batch.close()
+    for objs in solves:
+        for o in (objs[2], objs[1], objs[0]):
+            o.close()
+    del solves
+    torch.cuda.empty_cache()
+    loops = {}
+    err = 0.0
+    for prec, name in ((wt.WT_F64, "plain_fp64_per_solve_loop"), (wt.WT_F32, "plain_fp32_per_solve_loop")):
+        dof, secs = 0.0, 0.0
+        for k in sample:
+            q = reqs[k]
+            mesh, coef, ws, Phi, Pi, dt = S.build_solve(ctx, q, prec, wt.FP32_CUDA_CORES, release=False)
+            nst = 20
+            wt.step_rk4_curved(Phi, Pi, coef, ws, dt, 3, bc3d=bc, metric=True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(nst):
+                wt.step_rk4_curved(Phi, Pi, coef, ws, dt, 1, bc3d=bc, metric=True)
+            torch.cuda.synchronize()
+            secs += time.perf_counter() - t0
+            dof += 2.0 * mesh.nn * nst
+            for o in (ws, coef, mesh):
+                o.close()
+        loops[name] = {"value": dof / secs, "unit": "DOF-updates/s",
+                       "sample": f"{len(sample)} of the solves (8 smallest, 4 largest), 20 steps each, one "
+                                 "step_rk4_curved call per step"}
+    # split-precision accuracy on two small solves: batched FP32 vs the FP64 form after all steps
+    for k in order[:2]:
+        q = reqs[k]
+        runs = []
+        for prec in (wt.WT_F32, wt.WT_F64):
+            mesh, coef, ws, Phi, Pi, dt = S.build_solve(ctx, q, prec, release=False)
+            b = wt.Batch(ctx)
+            b.add(Phi, Pi, coef, ws, dt, bc)
+            b.step(args.batch_steps)
+            runs.append(torch.cat([Phi, Pi]).double().cpu().numpy())
+            b.close()
+        err = max(err, float(np.linalg.norm(runs[0] - runs[1]) / np.linalg.norm(runs[1])))
+    line = {"metric": "DOF-updates/s", "value": value, "unit": "DOF-updates/s", "n_gpus": 1,
+            "steps": args.batch_steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * t / args.batch_steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (split-BF16 tensor-core contractions for n=8)",
+            "data": "synthetic (seeded solves; no dataset)",
+            "config": {"workload": f"{len(reqs)} batched warped-cube solves, e~U{{4..24}}, n~{{4,6,8}}, flat or "
+                                   f"ADM U(0,0.15), {nodes:,} nodes in total",
+                       "solves": len(reqs), "nodes": nodes, "setup_s": t_setup,
+                       "groups": [{"n": g[0], "n8_path": g[2], "epb_variant": g[3], "tiles": g[4]} for g in groups]},
+            "gpu_launches": launches, "clocks": clocks, "finite": finite,
+            "rel_l2_vs_fp64_after_all_steps": err, **loops}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """Served solves: args.requests Poisson arrivals (e log-uniform in [4,32],
+    n ~ {6,8}, 200..2000 steps) served by the continuous-batching server in the
+    FP32 split-precision form under a 150 GB budget, beside the plain FP64
+    per-request form (one solve at a time); every FP32 result is compared with
+    its FP64 result."""
+    import numpy as np
+    import torch
+    wt = package()
+    S = wt.serve
+    ctx = wt.Context(0)
+    reqs = [S.Request.from_dict(d) for d in wt.workloads.serve_requests(args.seed, args.requests, args.rate)]
+    out = {}
+    finals = {}
+    for name, prec, max_active in (("served_fp32_split_bf16", wt.WT_F32, None), ("plain_fp64_per_request",
+                                                                              wt.WT_F64, 1)):
+        server = S.Server(ctx, precision=prec, hbm_budget=150e9, tick=50, max_active=max_active, keep_results=True)
+        t0 = time.perf_counter()
+        res = server.run(reqs)
+        makespan = time.perf_counter() - t0
+        out[name] = S.summary(res, makespan)
+        finals[name] = {r.rid: torch.cat([r.Phi, r.Pi]).double().cpu().numpy() for r in res}
+        del res
+        torch.cuda.empty_cache()
+    errs = [float(np.linalg.norm(finals["served_fp32_split_bf16"][k] - finals["plain_fp64_per_request"][k]) /
+                  np.linalg.norm(finals["plain_fp64_per_request"][k])) for k in finals["plain_fp64_per_request"]]
+    main_ = out["served_fp32_split_bf16"]
+    line = {"metric": "served solves/s", "value": main_["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+            "steps": None, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (split-BF16 tensor-core contractions for n=8)",
+            "data": "synthetic (seeded Poisson request stream; no dataset)",
+            "config": {"workload": f"{len(reqs)} served warped-cube solves, Poisson rate {args.rate}/s, "
+                                   "e log-U[4,32], n~{6,8}, 200..2000 steps, 150 GB budget",
+                       "requests": len(reqs), "rate_per_s": args.rate},
+            "p50_latency_s": main_["p50_latency_s"], "p99_latency_s": main_["p99_latency_s"],
+            "dof_updates_per_s": main_["dof_updates_per_s"], "served": main_,
+            "plain_fp64_per_request": out["plain_fp64_per_request"],
+            "max_rel_l2_fp32_vs_fp64": max(errs), "finite": not ctx.nonfinite()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -345,11 +506,22 @@ def main():
                     help="FP32 n=8 contractions: split BF16 tensor cores (three / two terms) or CUDA cores")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["solve", "batch", "serve"], default="solve",
+                    help="solve: the large warped ADM solve (default); batch: batched uneven solves; "
+                         "serve: served Poisson request stream")
+    ap.add_argument("--solves", type=int, default=256, help="batch workload: number of solves")
+    ap.add_argument("--batch-steps", type=int, default=300, help="batch workload: RK4 steps per solve")
+    ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
+    ap.add_argument("--rate", type=float, default=1.5, help="serve workload: Poisson arrival rate (1/s)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

@@ -173,7 +173,9 @@ int wt_initial_data(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, 
 /* ---- workspace ---------------------------------------------------------------*/
 /* Replaces make_wave3d_workspace (src/wave3d_curved.jl:158-178): device
  * scratch plus mu, the spectral radius of apply_D! along axis 1 from the
- * reference's 30-step power iteration (alternating-sign start). */
+ * reference's 30-step power iteration (alternating-sign start).  mu is
+ * computed on first use (wt_workspace_mu or any call with eps_ko != 0); that
+ * first use synchronises the stream, so make it before capturing a graph. */
 int wt_workspace_create(wt_ctx* ctx, wt_mesh* mesh, wt_ws** out);
 int wt_workspace_destroy(wt_ws* ws);
 int wt_workspace_mu(wt_ws* ws, double* mu);

@@ -1,0 +1,71 @@
+"""Served solves: requests that arrive while others run join the same batch;
+every served result equals the same request stepped alone (<= 1e-6 relative
+L2, FP32 state), and the split-precision results stay within 1e-5 of the
+Float64 oracle."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def requests(wt):
+    S = wt.serve
+    specs = [(0, 0.00, 3, 8, 40), (1, 0.00, 2, 6, 24), (2, 0.01, 2, 8, 60), (3, 0.02, 3, 6, 30),
+             (4, 0.05, 2, 8, 20), (5, 0.05, 2, 6, 50)]
+    return [S.Request(rid=r, arrival=t, elements=e, n=n, steps=st, seed=900 + r, scale=0.5 * (r % 3))
+            for r, t, e, n, st in specs]
+
+
+def test_served_results_equal_alone_and_oracle(wt, ctx, O):
+    import torch
+    S = wt.serve
+    reqs = requests(wt)
+    server = S.Server(ctx, precision=wt.WT_F32, hbm_budget=4e9, tick=8, keep_results=True)
+    res = server.run(reqs)
+    assert [r.rid for r in res] == [q.rid for q in reqs]
+    # the work of several requests overlapped on the device
+    assert any(a.admitted < b.finished and b.admitted < a.finished for a in res for b in res if a.rid < b.rid)
+    for q, r in zip(reqs, res):
+        mesh, coef, ws, Phi, Pi, dt = S.build_solve(ctx, q, wt.WT_F32, release=False)
+        assert dt == r.dt
+        wt.step_rk4_curved(Phi, Pi, coef, ws, dt, q.steps, bc3d=wt.make_bc3d([wt.BC_SOMMERFELD] * 6), metric=True)
+        a = torch.cat([r.Phi, r.Pi]).double().cpu().numpy()
+        b = torch.cat([Phi, Pi]).double().cpu().numpy()
+        assert rel(a, b) <= 1e-6, q.rid
+    for q, r in list(zip(reqs, res))[:2]:  # split-precision result against the Float64 oracle
+        o = O.OracleMesh(q.n, q.elements, A=0.05, outer_tag=7)
+        co = o.background(2, wt.workloads.adm_params(q.seed, q.scale))
+        x, y, z = o.coords()
+        c, amp, w = wt.workloads.pulses(q.seed, q.pulses, amp=(0.5, 1.0), width=(0.05, 0.15), centre=(0.25, 0.75))
+        P0 = wt.workloads.gaussian_field(x, y, z, c, amp, w)
+        Po, Qo = o.evolve_curved(co, P0, np.zeros_like(P0), r.dt, q.steps, bc=O.make_bc([2] * 6), use_metric=True)
+        a = np.concatenate([r.Phi.double().cpu().numpy(), r.Pi.double().cpu().numpy()])
+        assert rel(a, np.concatenate([Po, Qo])) <= 1e-5, q.rid
+
+
+def test_server_admission_respects_budget(wt, ctx):
+    S = wt.serve
+    reqs = requests(wt)
+    one = max(S.Server(ctx)._cost(q) for q in reqs)
+    server = S.Server(ctx, precision=wt.WT_F32, hbm_budget=one * 1.01, tick=16)
+    res = server.run(reqs)
+    assert len(res) == len(reqs)
+    assert server.peak_used <= server.budget
+    cost = {q.rid: server._cost(q) for q in reqs}
+    for a in res:  # requests that ran at the same time fit the budget together
+        for b in res:
+            if a.rid < b.rid and a.admitted < b.finished and b.admitted < a.finished:
+                assert cost[a.rid] + cost[b.rid] <= server.budget
+    # one slot: strictly one request at a time, all served
+    res1 = S.Server(ctx, precision=wt.WT_F32, tick=16, max_active=1).run(reqs)
+    spans = sorted((r.admitted, r.finished) for r in res1)
+    assert len(res1) == len(reqs)
+    assert all(spans[i][1] <= spans[i + 1][0] + 1e-9 for i in range(len(spans) - 1))
+    with pytest.raises(ValueError):
+        S.Server(ctx, hbm_budget=1e3).run(reqs[:1])

@@ -3,7 +3,8 @@ SBP-SAT right-hand side and RK4 time step.
 
 The numerics live in libwavetoy_b200.so (CUDA kernels behind the C ABI of
 include/wavetoy_b200.h); this package is the Python mirror of the reference's
-Julia API (wavetoy.py) plus the build step (build.py).  The directory name
+Julia API (wavetoy.py), the seeded workloads (workloads.py), the serving loop
+over batched solves (serve.py) and the build step (build.py).  The directory name
 contains a dot, so load it with importlib under the module name
 "wavetoy_b200" (see tests/conftest.py).
 """
@@ -11,3 +12,4 @@ from .wavetoy import *  # noqa: F401,F403
 from .wavetoy import library, LIB_PATH  # noqa: F401
 from . import workloads  # noqa: F401
 from . import build  # noqa: F401
+from . import serve  # noqa: F401

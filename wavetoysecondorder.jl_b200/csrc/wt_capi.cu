@@ -58,6 +58,7 @@ struct wt_ws {
   wt_ctx* ctx = nullptr;
   wt_mesh* mesh = nullptr;
   double mu = 0.0, inv_mu5 = 0.0;
+  bool mu_done = false;  // mu is computed on first use (Kreiss-Oliger or wt_workspace_mu)
   void* F = nullptr;      // 3 nn
   void* bbuf = nullptr;   // nbf N^2
   void* grad = nullptr;   // 3 nn
@@ -349,6 +350,37 @@ int check_ws(wt_ctx* ctx, wt_ws* ws) {
   if (!ctx) return WT_EINVAL;
   if (!ws) return fail(ctx, WT_EINVAL, "workspace is NULL");
   if (ws->ctx != ctx) return fail(ctx, WT_EINVAL, "workspace belongs to another context");
+  return 0;
+}
+
+// mu of make_wave3d_workspace: 30 power-iteration steps v <- D_1^2 v / ||D_1^2 v||
+// from the alternating-sign start (src/wave3d_curved.jl:163-175).  Computed on
+// first use; it synchronises the stream, so it runs outside graph capture.
+int ensure_mu(wt_ws* ws) {
+  if (ws->mu_done) return 0;
+  wt_ctx* ctx = ws->ctx;
+  const wt::DevMesh& m = ws->mesh->m;
+  WT_TRY(ws_k_buffers(ws));
+  cudaStream_t s = ctx->stream;
+  int rc = lrc(ctx, wt::launch_alt_sign(m, ws->kP, s), "mu");
+  double mu2 = 0.0;
+  for (int it = 0; it < 30 && !rc; ++it) {
+    rc = lrc(ctx, wt::launch_apply_D(m, ws->kP, ws->kQ, 0, s), "mu");
+    if (!rc) rc = lrc(ctx, wt::launch_apply_D(m, ws->kQ, ws->kP, 0, s), "mu");
+    if (!rc) rc = lrc(ctx, wt::launch_sumsq(m.nn, m.precision, ws->kP, ctx->d_partial, ctx->nblocks, s), "mu");
+    double ss = 0.0;
+    if (!rc) rc = reduce_to_host(ctx, &ss);
+    ctx->launches += 3;
+    if (rc) break;
+    mu2 = std::sqrt(ss);
+    if (!(mu2 > 0)) break;
+    rc = lrc(ctx, wt::launch_scale(m.nn, m.precision, ws->kP, mu2, s), "mu");
+    ctx->launches += 1;
+  }
+  if (rc) return rc;
+  ws->mu = std::sqrt(mu2);
+  ws->inv_mu5 = ws->mu > 0 ? std::pow(1.0 / ws->mu, 5) : 0.0;
+  ws->mu_done = true;
   return 0;
 }
 
@@ -774,30 +806,8 @@ int wt_workspace_create(wt_ctx* ctx, wt_mesh* mesh, wt_ws** out) {
   if (!mesh || !out) return fail(ctx, WT_EINVAL, "wt_workspace_create: NULL argument");
   auto* ws = new wt_ws();
   ws->ctx = ctx; ws->mesh = mesh;
-  const wt::DevMesh& m = mesh->m;
   int rc = ws_buffers(ws);
-  if (!rc) rc = ws_k_buffers(ws);
   if (rc) { wt_workspace_destroy(ws); return rc; }
-  // mu: 30 power-iteration steps v <- D_1^2 v / ||D_1^2 v|| (src/wave3d_curved.jl:163-175)
-  cudaStream_t s = ctx->stream;
-  rc = lrc(ctx, wt::launch_alt_sign(m, ws->kP, s), "mu");
-  double mu2 = 0.0;
-  for (int it = 0; it < 30 && !rc; ++it) {
-    rc = lrc(ctx, wt::launch_apply_D(m, ws->kP, ws->kQ, 0, s), "mu");
-    if (!rc) rc = lrc(ctx, wt::launch_apply_D(m, ws->kQ, ws->kP, 0, s), "mu");
-    if (!rc) rc = lrc(ctx, wt::launch_sumsq(m.nn, m.precision, ws->kP, ctx->d_partial, ctx->nblocks, s), "mu");
-    double ss = 0.0;
-    if (!rc) rc = reduce_to_host(ctx, &ss);
-    ctx->launches += 3;
-    if (rc) break;
-    mu2 = std::sqrt(ss);
-    if (!(mu2 > 0)) break;
-    rc = lrc(ctx, wt::launch_scale(m.nn, m.precision, ws->kP, mu2, s), "mu");
-    ctx->launches += 1;
-  }
-  if (rc) { wt_workspace_destroy(ws); return rc; }
-  ws->mu = std::sqrt(mu2);
-  ws->inv_mu5 = ws->mu > 0 ? std::pow(1.0 / ws->mu, 5) : 0.0;
   *out = ws;
   return 0;
 }
@@ -815,6 +825,7 @@ int wt_workspace_destroy(wt_ws* ws) {
 
 int wt_workspace_mu(wt_ws* ws, double* mu) {
   if (!ws || !mu) return WT_EINVAL;
+  WT_TRY(ensure_mu(ws));
   *mu = ws->mu;
   return 0;
 }
@@ -827,6 +838,7 @@ int wt_rhs_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, 
   if (coef->mesh != ws->mesh) return fail(ctx, WT_EINVAL, "coefficients belong to another mesh");
   wt::ConsBC b;
   WT_TRY(make_bc(ctx, bc, use_metric, b));
+  if (eps_ko != 0.0) WT_TRY(ensure_mu(ws));
   return rhs_curved_impl(ctx, ws, coef, Phi, Pi, Phidot, Pidot, eps_ko, b, use_metric);
 }
 
@@ -841,6 +853,7 @@ int wt_apply_D(wt_ctx* ctx, wt_ws* ws, const void* u, void* Du, int d) {
 int wt_ko_add(wt_ctx* ctx, wt_ws* ws, void* dst, const void* field, double eps_ko) {
   WT_TRY(check_ws(ctx, ws));
   if (!dst || !field) return fail(ctx, WT_EINVAL, "wt_ko_add: NULL argument");
+  WT_TRY(ensure_mu(ws));
   ctx->launches += 3;
   return lrc(ctx, wt::launch_ko_add(ws->mesh->m, dst, field, eps_ko * ws->inv_mu5, ctx->stream), "Kreiss-Oliger");
 }
@@ -1050,7 +1063,7 @@ int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, v
   wt::ConsBC b;
   WT_TRY(make_bc(ctx, bc, use_metric, b));
   WT_TRY(ws_step_buffers(ws));
-  if (eps_ko != 0.0) WT_TRY(ws_k_buffers(ws));
+  if (eps_ko != 0.0) WT_TRY(ensure_mu(ws));
   comp_track(ws, Phi, Pi);
   if (nsteps <= 2) {
     for (int i = 0; i < nsteps; ++i) WT_TRY(step_curved_once(ctx, ws, coef, Phi, Pi, dt, eps_ko, b, use_metric));
@@ -1091,6 +1104,7 @@ int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int n
   if (!ws->mesh->m.affine) return fail(ctx, WT_ENOTSUP, "SIPG stepping supports affine meshes only");
   WT_TRY(ws_step_buffers(ws));
   WT_TRY(ws_k_buffers(ws));
+  if (eps_ko != 0.0) WT_TRY(ensure_mu(ws));
   const wt::DevMesh& m = ws->mesh->m;
   WT_TRY(ensure(ws, &ws->trace, (size_t)6 * m.N * m.N * m.Ne * rsize(m.precision)));
   if (nsteps <= 2) {

@@ -372,10 +372,20 @@ class Workspace(_Child):
         self.h = C.c_void_p()
         self.ctx.check(library().wt_workspace_create(self.ctx.h, mesh.h, C.byref(self.h)), "wt_workspace_create")
         self.ctx._adopt(self)
-        mu = C.c_double()
-        library().wt_workspace_mu(self.h, C.byref(mu))
-        self.mu = mu.value
-        self.inv_mu5 = (1.0 / self.mu) ** 5 if self.mu > 0 else 0.0
+        self._mu = None
+
+    @property
+    def mu(self) -> float:
+        """Spectral-radius estimate of D_1^2 (30 power-iteration steps), computed on first use."""
+        if self._mu is None:
+            mu = C.c_double()
+            self.ctx.check(library().wt_workspace_mu(self.h, C.byref(mu)), "wt_workspace_mu")
+            self._mu = mu.value
+        return self._mu
+
+    @property
+    def inv_mu5(self) -> float:
+        return (1.0 / self.mu) ** 5 if self.mu > 0 else 0.0
 
     def close(self):
         if getattr(self, "h", None) and self._ctx_alive():

@@ -10,7 +10,12 @@ Workloads (sizes as named in the benchmark configuration):
   * warped ADM pulse: warped cube (A = 0.05), 16^3 elements, n = 8, perturbed
     ADM background, one Gaussian pulse, Sommerfeld outer faces, RK4 CFL 0.2;
   * large warped ADM: as above at 64^3 elements (134,217,728 nodes) with eight
-    Gaussian pulses (amplitude U(0.5,1), width U(0.05,0.15)).
+    Gaussian pulses (amplitude U(0.5,1), width U(0.05,0.15));
+  * batched solves (batch_specs): cubic warped meshes with e ~ U{4..24}
+    elements per axis and n ~ {4, 6, 8}, flat or perturbed ADM backgrounds
+    with metric-perturbation amplitude U(0, 0.15), seeded pulses;
+  * served solves (serve_requests): Poisson arrivals, e log-uniform in
+    [4, 32], n ~ {6, 8}, 200..2000 RK4 steps.
 """
 from __future__ import annotations
 
@@ -104,3 +109,38 @@ def gaussian_field_torch(coords, centres, amps, widths):
 def standing_wave(x, y, z):
     """u = sin(pi x) sin(pi y) sin(pi z) (eigenmode_cartesian!, src/wave.jl:163-185, k = pi)."""
     return np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z)
+
+
+def batch_specs(seed: int, count: int = 256, e_range=(4, 24), orders=(4, 6, 8)):
+    """The batched-solve workload: count dicts with elements per axis e ~ U{e_range},
+    order n ~ U(orders), background 'flat' or 'adm' (even odds) and, for 'adm',
+    the metric-perturbation amplitude U(0, 0.15) (adm_params scale = amp / 0.1),
+    and a pulse seed."""
+    r = SplitMix64(seed ^ 0xB47C4)
+    out = []
+    for k in range(count):
+        e = e_range[0] + min(int(r.uniform() * (e_range[1] - e_range[0] + 1)), e_range[1] - e_range[0])
+        n = orders[min(int(r.uniform() * len(orders)), len(orders) - 1)]
+        adm = r.uniform() < 0.5
+        amp = r.uniform(0.0, 0.15) if adm else 0.0
+        out.append({"elements": e, "n": n, "scale": amp / 0.1, "seed": seed * 1000 + k})
+    return out
+
+
+def serve_requests(seed: int, count: int, rate: float, e_range=(4, 32), orders=(6, 8), steps=(200, 2000)):
+    """Served-solve requests: Poisson arrivals at `rate` per second (exponential
+    gaps), e log-uniform in e_range, n ~ U(orders), ADM scale U(0, 1.5), the
+    final time as a step count U{steps} at CFL 0.2 (the U(0.5, 2) light-crossing
+    span mapped onto the step range), and seeds for background and pulses."""
+    r = SplitMix64(seed ^ 0x5E7E)
+    t = 0.0
+    out = []
+    lo, hi = math.log(e_range[0]), math.log(e_range[1])
+    for k in range(count):
+        t += -math.log(1.0 - r.uniform()) / rate
+        e = int(round(math.exp(lo + (hi - lo) * r.uniform())))
+        n = orders[min(int(r.uniform() * len(orders)), len(orders) - 1)]
+        st = steps[0] + min(int(r.uniform() * (steps[1] - steps[0] + 1)), steps[1] - steps[0])
+        out.append({"rid": k, "arrival": t, "elements": e, "n": n, "scale": r.uniform(0.0, 1.5), "steps": st,
+                    "seed": seed * 100000 + k})
+    return out
