@@ -46,6 +46,8 @@ struct K1P {
   const int32_t* nbrf;
   const int32_t* bdry;
   const int32_t* bslot;
+  const int32_t* emask;  // per element: SAT face mask (bits 0-5), outer face (bit 6)
+  const int32_t* fsrc;   // per (f,e): 8 * neighbour + neighbour face, -1 without SAT
   const double* G;
   const double* H;
   real* F;
@@ -167,16 +169,15 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
   if (tid < N2) GT[(tid % N) * N + tid / N] = (real)P.G[tid];
   const real u = valid ? P.Phi[n] : (real)0;
   su[le][t] = u;
+  // element tables: SAT mask / outer-face flag, and the neighbour face sources
+  const int emask = valid ? P.emask[ec] : 0;
   // neighbour Phi face traces
   for (int idx = t; idx < 6 * N2; idx += N3) {
     const int f = idx / N2, pq = idx - f * N2;
     real v = 0;
-    if (valid) {
-      const int en = P.nbr[f + 6 * ec];
-      if (en >= 0 && P.bdry[f + 6 * ec] == 0) {
-        const int fn = P.nbrf[f + 6 * ec];
-        v = P.Phi[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq % N, pq / N, N)];
-      }
+    if ((emask >> f) & 1) {
+      const int src = P.fsrc[f + 6 * ec], fn = src & 7;
+      v = P.Phi[(long long)(src >> 3) * N3 + face_node(faxis(fn), frow(fn, N), pq % N, pq / N, N)];
     }
     sun[le][f][pq] = v;
   }
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
     for (int f = 0; f < 6; ++f) {
       const int ax = f >> 1;
       if (idx3[ax] != frow(f, N)) continue;
-      if (P.bdry[f + 6 * ec] != 0 || P.nbr[f + 6 * ec] < 0) continue;
+      if (!((emask >> f) & 1)) continue;
       const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
       const real jump = sun[le][f][p + N * q] - u;
       const real nh = (f & 1) ? (real)1 : (real)-1;
@@ -258,7 +259,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
   const real F2 = b[2] * Pi + (K[2] * g[0] + K[4] * g[1] + K[5] * g[2]);
   real phid = b[0] * g[0] + b[1] * g[1] + b[2] * g[2] + a * Pi;
   // boundary increments (per boundary face of the node; Pi parts go to the face slot)
-  if (P.bc_on) {
+  if (P.bc_on && (emask >> 6)) {
     const int idx3[3] = {i, j, k};
     for (int f = 0; f < 6; ++f) {
       const int tag = P.bdry[f + 6 * ec];
@@ -342,6 +343,8 @@ struct K2P {
   const int32_t* nbrf;
   const int32_t* bdry;
   const int32_t* bslot;
+  const int32_t* emask;
+  const int32_t* fsrc;
   const double* G;
   const double* H;
   const real* bbuf;
@@ -392,15 +395,13 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
     Fv[c] = valid ? Fp[c][n] : (real)0;
     sF[le][c][t] = Fv[c];
   }
+  const int emask = valid ? P.emask[ec] : 0;
   for (int idx = t; idx < 6 * N2; idx += N3) {
     const int f = idx / N2, pq = idx - f * N2;
     long long src = -1;
-    if (valid) {
-      const int en = P.nbr[f + 6 * ec];
-      if (en >= 0 && P.bdry[f + 6 * ec] == 0) {
-        const int fn = P.nbrf[f + 6 * ec];
-        src = (long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq % N, pq / N, N);
-      }
+    if ((emask >> f) & 1) {
+      const int fs = P.fsrc[f + 6 * ec], fn = fs & 7;
+      src = (long long)(fs >> 3) * N3 + face_node(faxis(fn), frow(fn, N), pq % N, pq / N, N);
     }
     if (CURV) {
 #pragma unroll
@@ -441,7 +442,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
   for (int f = 0; f < 6; ++f) {
     const int ax = f >> 1;
     if (idx3[ax] != frow(f, N)) continue;
-    if (P.bdry[f + 6 * ec] != 0 || P.nbr[f + 6 * ec] < 0) continue;
+    if (!((emask >> f) & 1)) continue;
     const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
     const real nh = (f & 1) ? (real)1 : (real)-1;
     if (CURV) {
@@ -454,7 +455,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
     }
   }
   if (CURV) dv *= invJ;
-  if (P.bc_on) {
+  if (P.bc_on && (emask >> 6)) {
     for (int f = 0; f < 6; ++f) {
       if (P.bdry[f + 6 * ec] == 0) continue;
       const int ax = f >> 1;
@@ -595,6 +596,7 @@ static K1P<real> k1p_params(const DevMesh& m, const DevCoef& c, const void* Phi,
   P.c10 = (const real*)c.c10;
   P.Ja = (const real*)m.Ja_r; P.invdetJ = (const real*)m.invdetJ_r; P.sdiag = (const real*)m.sdiag;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot;
+  P.emask = m.emask; P.fsrc = m.fsrc;
   P.G = m.G; P.H = m.H;
   P.F = (real*)F; P.Phidot = (real*)Phidot; P.bbuf = (real*)bbuf; P.grad_out = (real*)grad_out;
   P.bc_on = bc.on; P.bc_curv = bc.curv; P.exc_tag = bc.exc_tag; P.nbf = m.nbf;
@@ -617,6 +619,7 @@ static K2P<real> k2p_params(const DevMesh& m, const void* F, void* Pidot, const 
   P.F2 = F2 ? (const real*)F2 : (const real*)F + 2 * m.nn;
   P.Ja = (const real*)m.Ja_r; P.invdetJ = (const real*)m.invdetJ_r; P.sdiag = (const real*)m.sdiag;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot;
+  P.emask = m.emask; P.fsrc = m.fsrc;
   P.G = m.G; P.H = m.H;
   P.bbuf = (const real*)bbuf; P.bc_on = bc.on;
   P.Pidot = (real*)Pidot;
