@@ -646,37 +646,51 @@ struct K2N8 {
 };
 
 // K2 staged fields: 0..2 F, 3..11 Ja.  Register prefetch: invJ, y, acc, comp.
+// Two shapes (K2Shape): 512 threads (one node per thread, warps w and w + 8
+// split the fields of pencil tile w & 7, a ring of NSTAGE stages) or 256
+// threads (two nodes per thread, each warp does both halves of its tile, one
+// stage whose next copy is issued as soon as the contraction pass has read
+// it) -- the 256-thread shape fits two CTAs on an SM for FP64.
 constexpr int K2_NF = 12;
 constexpr size_t K2_STAGE = (size_t)K2_NF * n8::FS;
 template <typename real>
+struct K2Shape {
+  static constexpr int THR = std::is_same<real, double>::value ? 256 : 512;
+  static constexpr int NS = THR == 512 ? n8::NSTAGE : 1;          // stages
+  static constexpr int OCC = std::is_same<real, double>::value ? 2 : n8::Occ<real>::k2;
+};
+template <typename real>
 constexpr size_t k2_smem() {
-  return (n8::NSTAGE * K2_STAGE + 6 * n8::FS + 2 * 6 * 3 * n8::N2) * sizeof(real) + n8::N2 * sizeof(double) + 64;
+  return (K2Shape<real>::NS * K2_STAGE + 6 * n8::FS + 2 * 6 * 3 * n8::N2) * sizeof(real) + n8::N2 * sizeof(double) +
+         64;
 }
 
 template <typename real, int NT, bool BATCH>
-__global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
+__global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
     k_cons_k2_n8(const K2N8<real> P, const K2N8<real>* __restrict__ plist, const int2* __restrict__ tiles,
                  long long ntiles) {
   using namespace n8;
   constexpr bool F64 = std::is_same<real, double>::value;
+  constexpr int THR = K2Shape<real>::THR, NS = K2Shape<real>::NS;
+  constexpr int NPT = N3 / THR;                 // nodes per thread in the node pass
+  constexpr int NFACE = 6 * 3 * N2;             // 1152 neighbour face values
+  constexpr int NFR = (NFACE + THR - 1) / THR;  // face values per thread
+  constexpr int NHALF = THR == 512 ? 1 : 2;     // halves of its tile a warp does
   extern __shared__ __align__(128) unsigned char smraw[];
   double* sG = reinterpret_cast<double*>(smraw);                   // 64
   real* stg = reinterpret_cast<real*>(sG + N2);
-  real* sdiv = stg + NSTAGE * K2_STAGE;                            // 6 padded partial divergences [al*2 + half]
+  real* sdiv = stg + NS * K2_STAGE;                                // 6 padded partial divergences [al*2 + half]
   real* sface = sdiv + 6 * FS;                                     // 2 x 6 x 3 x 64
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sface + 2 * 6 * 3 * N2);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sface + 2 * NFACE);
   __shared__ int abort_flag;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
+  const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7;
   const real inv2H = (real)(1.0 / (2.0 * P.H[0]));
   const bool comp_on = !F64 && P.epi && P.comp != nullptr;  // FP32 state only
   const bool need_y = P.epi && (P.stage <= 2 || (comp_on && P.stage == 3));
   const bool need_acc = P.epi && P.stage >= 1;
   const bool need_comp = comp_on && P.stage == 3;
   const unsigned tx_bytes = (unsigned)(K2_NF * FS * sizeof(real));
-  const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
-  const int tpad = pad(ti, tj, tk);
-  constexpr int NFACE = 6 * 3 * N2;  // 1152
   const long long T = BATCH ? ntiles : P.Ne;
   const long long GS = gridDim.x;
   auto tile_at = [&](long long t) -> int2 {
@@ -692,7 +706,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
   if (tid < N2) sG[tid] = P.G[tid];
   if (tid == 0) {
     abort_flag = 0;
-    for (int k = 0; k < NSTAGE; ++k) mbar_init(&bar[k], 1);
+    for (int k = 0; k < NS; ++k) mbar_init(&bar[k], 1);
     fence_barrier_init();
   }
   __syncthreads();
@@ -712,19 +726,19 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
       bulk_g2s(d + lane * FS, src, FS * (unsigned)sizeof(real), &bar[s]);
     }
   };
-  // neighbour flux face traces: [f][c][pq], 1152 values, <= 3 per thread; the
+  // neighbour flux face traces: [f][c][pq], 1152 values, NFR per thread; the
   // face sources are loaded one iteration ahead of the traces (see K1)
-  auto src_load = [&](int2 tl, int src[3]) {
+  auto src_load = [&](int2 tl, int src[NFR]) {
 #pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      const int idx = tid + r * THREADS;
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = tid + r * THR;
       src[r] = (tl.x >= 0 && idx < NFACE) ? prm(tl.x).fsrc[idx / (3 * N2) + 6 * tl.y] : -1;
     }
   };
-  auto face_load = [&](const int src[3], int sidx, real fv[3]) {
+  auto face_load = [&](const int src[NFR], int sidx, real fv[NFR]) {
 #pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      const int idx = tid + r * THREADS;
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = tid + r * THR;
       real v = 0;
       if (src[r] >= 0) {
         const K2N8<real>& Q = prm(sidx);
@@ -741,33 +755,38 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
   struct PW {
     real invJ, y, acc, comp;
   };
-  auto pw_load = [&](int2 tl, PW& w) {
+  auto pw_load = [&](int2 tl, PW w[NPT]) {
     if (tl.x < 0) return;
     const K2N8<real>& Q = prm(tl.x);
-    const long long n = (long long)tl.y * N3 + tid;
-    w.invJ = Q.invdetJ[n];
-    w.y = need_y ? Q.y[n] : (real)0;
-    w.acc = need_acc ? Q.acc[n] : (real)0;
-    w.comp = need_comp ? Q.comp[n] : (real)0;
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) {
+      const long long n = (long long)tl.y * N3 + tid + r * THR;
+      w[r].invJ = Q.invdetJ[n];
+      w[r].y = need_y ? Q.y[n] : (real)0;
+      w[r].acc = need_acc ? Q.acc[n] : (real)0;
+      w[r].comp = need_comp ? Q.comp[n] : (real)0;
+    }
   };
 
   int2 t0 = tile_at(blockIdx.x), t1 = tile_at(blockIdx.x + GS), t2 = tile_at(blockIdx.x + 2 * GS);
-  PW cur;
-  int emcur = 0, src1[3] = {-1, -1, -1};
+  PW cur[NPT];
+  int emcur = 0, src1[NFR];
+#pragma unroll
+  for (int r = 0; r < NFR; ++r) src1[r] = -1;
   if (t0.x >= 0) {
     if (warp == 0)
-      for (int k = 0; k < NSTAGE - 1; ++k) {
+      for (int k = 0; k < (NS > 1 ? NS - 1 : 1); ++k) {
         const int2 tk_ = tile_at(blockIdx.x + k * GS);
         if (tk_.x >= 0) issue(tk_, k);
       }
     emcur = emask_at(t0);
-    int src0[3];
+    int src0[NFR];
     src_load(t0, src0);
-    real fv[3];
+    real fv[NFR];
     face_load(src0, t0.x, fv);
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
-      if (tid + r * THREADS < NFACE) sface[tid + r * THREADS] = fv[r];
+    for (int r = 0; r < NFR; ++r)
+      if (tid + r * THR < NFACE) sface[tid + r * THR] = fv[r];
     pw_load(t0, cur);
     src_load(t1, src1);
   }
@@ -783,8 +802,8 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
 
   int it = 0;
   for (long long t = blockIdx.x; t < T; t += GS, ++it) {
-    const int s = it % NSTAGE, fb = it & 1;
-    const unsigned parity = (it / NSTAGE) & 1;
+    const int s = it % NS, fb = it & 1;
+    const unsigned parity = (it / NS) & 1;
     // tiles t, t + grid, t + 2 grid: carried in registers for a work list (loaded
     // ahead), recomputed from t for a single solve
     int2 t3 = make_int2(-1, -1);
@@ -797,11 +816,11 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
     }
     const bool has_next = t1.x >= 0;
     const int emnext = emask_at(t1);
-    int src2[3];
+    int src2[NFR];
     src_load(t2, src2);
-    real fnext[3];
+    real fnext[NFR];
     face_load(src1, t1.x, fnext);
-    PW nxt;
+    PW nxt[NPT];
     pw_load(t1, nxt);
     // One thread polls the stage's mbarrier (its acquire makes the copied data
     // visible; the barrier below orders every other thread after it), so the
@@ -810,13 +829,13 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
     __syncthreads();  // the previous element is finished: its stage and the buffers are free (see K1)
     if (abort_flag) {  // wait (bounded) for the copies still in flight, then leave
       if (warp == 0 && lane == 0)
-        for (int k = 1; k < NSTAGE - 1; ++k)
-          if (tile_at(t + k * GS).x >= 0) wait_phase(&bar[(it + k) % NSTAGE], ((it + k) / NSTAGE) & 1, nullptr);
+        for (int k = 1; k < NS - 1; ++k)
+          if (tile_at(t + k * GS).x >= 0) wait_phase(&bar[(it + k) % NS], ((it + k) / NS) & 1, nullptr);
       return;
     }
-    {
-      const int2 ti_ = NSTAGE == 2 ? t1 : tile_at(t + (NSTAGE - 1) * GS);
-      if (warp == 0 && ti_.x >= 0) issue(ti_, (it + NSTAGE - 1) % NSTAGE);
+    if constexpr (NS > 1) {
+      const int2 ti_ = NS == 2 ? t1 : tile_at(t + (NS - 1) * GS);
+      if (warp == 0 && ti_.x >= 0) issue(ti_, (it + NS - 1) % NS);
     }
     const K2N8<real>& Q = prm(t0.x);
     const long long e = t0.y;
@@ -828,77 +847,89 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
     const int bnd = emcur >> 6;
     // per-axis partial divergences sdiv[al*2 + half]: no barrier between axes
 #pragma unroll
-    for (int al = 0; al < 3; ++al) {
-      const real* m0 = sJa + (al * 3 + 0) * FS;
-      const real* m1 = sJa + (al * 3 + 1) * FS;
-      const real* m2 = sJa + (al * 3 + 2) * FS;
-      real cx[2], cy[2];
-      if constexpr (F64) {
-        double dx[2] = {0, 0}, dy[2] = {0, 0};
+    for (int hh = 0; hh < NHALF; ++hh) {
+      const int half = THR == 512 ? (warp >> 3) : hh;
 #pragma unroll
-        for (int kc = 0; kc < 2; ++kc) {
-          const int nd = bnode(al, wt8, kc, gq, tig);
-          const double a = kc ? aG1 : aG0;
-          if (half == 0) {
-            // contravariant flux Ja^al . F and F_0
-            const double f0 = sF[nd];
-            const double ft = m0[nd] * f0 + m1[nd] * sF[FS + nd] + m2[nd] * sF[2 * FS + nd];
-            dmma(dx[0], dx[1], a, ft);
-            dmma(dy[0], dy[1], a, f0);
-          } else {
-            dmma(dx[0], dx[1], a, sF[FS + nd]);
-            dmma(dy[0], dy[1], a, sF[2 * FS + nd]);
+      for (int al = 0; al < 3; ++al) {
+        const real* m0 = sJa + (al * 3 + 0) * FS;
+        const real* m1 = sJa + (al * 3 + 1) * FS;
+        const real* m2 = sJa + (al * 3 + 2) * FS;
+        real cx[2], cy[2];
+        if constexpr (F64) {
+          double dx[2] = {0, 0}, dy[2] = {0, 0};
+#pragma unroll
+          for (int kc = 0; kc < 2; ++kc) {
+            const int nd = bnode(al, wt8, kc, gq, tig);
+            const double a = kc ? aG1 : aG0;
+            if (half == 0) {
+              // contravariant flux Ja^al . F and F_0
+              const double f0 = sF[nd];
+              const double ft = m0[nd] * f0 + m1[nd] * sF[FS + nd] + m2[nd] * sF[2 * FS + nd];
+              dmma(dx[0], dx[1], a, ft);
+              dmma(dy[0], dy[1], a, f0);
+            } else {
+              dmma(dx[0], dx[1], a, sF[FS + nd]);
+              dmma(dy[0], dy[1], a, sF[2 * FS + nd]);
+            }
           }
-        }
-        cx[0] = dx[0]; cx[1] = dx[1]; cy[0] = dy[0]; cy[1] = dy[1];
-      } else {
-        const int nd[3] = {bn(al, wt8, 2 * tig, gq), bn(al, wt8, 2 * tig + 1, gq), bn(al, wt8, PREF, gq)};
-        float vx[3], vy[3];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          if (half == 0) {
-            const float f0 = sF[nd[q]];
-            vx[q] = m0[nd[q]] * f0 + m1[nd[q]] * sF[FS + nd[q]] + m2[nd[q]] * sF[2 * FS + nd[q]];
-            vy[q] = f0;
-          } else {
-            vx[q] = sF[FS + nd[q]];
-            vy[q] = sF[2 * FS + nd[q]];
-          }
-        }
-        float fx[4] = {0, 0, 0, 0}, fy[4] = {0, 0, 0, 0};
-        mma_split<NT>(fx, aS, aS2, vx[0] - vx[2], vx[1] - vx[2]);
-        mma_split<NT>(fy, aS, aS2, vy[0] - vy[2], vy[1] - vy[2]);
-        cx[0] = fx[0] + fx[2]; cx[1] = fx[1] + fx[3];
-        cy[0] = fy[0] + fy[2]; cy[1] = fy[1] + fy[3];
-      }
-      // half 1 adds the centred-flux SAT of an interior al-face on its rows
-      const int sface_f = gq == 0 ? 2 * al : gq == 7 ? 2 * al + 1 : -1;
-      const bool sat = half == 1 && sface_f >= 0 && ((mask >> sface_f) & 1);
-#pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        const int no = onode(al, wt8, b, gq, tig);
-        real r;
-        if (half == 0) {
-          r = (real)0.5 * cx[b] + (real)0.5 * m0[no] * cy[b];
+          cx[0] = dx[0]; cx[1] = dx[1]; cy[0] = dy[0]; cy[1] = dy[1];
         } else {
-          r = (real)0.5 * m1[no] * cx[b] + (real)0.5 * m2[no] * cy[b];
+          const int nd[3] = {bn(al, wt8, 2 * tig, gq), bn(al, wt8, 2 * tig + 1, gq), bn(al, wt8, PREF, gq)};
+          float vx[3], vy[3];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            if (half == 0) {
+              const float f0 = sF[nd[q]];
+              vx[q] = m0[nd[q]] * f0 + m1[nd[q]] * sF[FS + nd[q]] + m2[nd[q]] * sF[2 * FS + nd[q]];
+              vy[q] = f0;
+            } else {
+              vx[q] = sF[FS + nd[q]];
+              vy[q] = sF[2 * FS + nd[q]];
+            }
+          }
+          float fx[4] = {0, 0, 0, 0}, fy[4] = {0, 0, 0, 0};
+          mma_split<NT>(fx, aS, aS2, vx[0] - vx[2], vx[1] - vx[2]);
+          mma_split<NT>(fy, aS, aS2, vy[0] - vy[2], vy[1] - vy[2]);
+          cx[0] = fx[0] + fx[2]; cx[1] = fx[1] + fx[3];
+          cy[0] = fy[0] + fy[2]; cy[1] = fy[1] + fy[3];
         }
-        if (sat) {
-          const int pq = opq(al, wt8, b, tig);
-          const real sacc = m0[no] * (sfc[(sface_f * 3 + 0) * N2 + pq] - sF[no]) +
-                            m1[no] * (sfc[(sface_f * 3 + 1) * N2 + pq] - sF[FS + no]) +
-                            m2[no] * (sfc[(sface_f * 3 + 2) * N2 + pq] - sF[2 * FS + no]);
-          r += (gq ? inv2H : -inv2H) * sacc;
+        // half 1 adds the centred-flux SAT of an interior al-face on its rows
+        const int sface_f = gq == 0 ? 2 * al : gq == 7 ? 2 * al + 1 : -1;
+        const bool sat = half == 1 && sface_f >= 0 && ((mask >> sface_f) & 1);
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          const int no = onode(al, wt8, b, gq, tig);
+          real r;
+          if (half == 0) {
+            r = (real)0.5 * cx[b] + (real)0.5 * m0[no] * cy[b];
+          } else {
+            r = (real)0.5 * m1[no] * cx[b] + (real)0.5 * m2[no] * cy[b];
+          }
+          if (sat) {
+            const int pq = opq(al, wt8, b, tig);
+            const real sacc = m0[no] * (sfc[(sface_f * 3 + 0) * N2 + pq] - sF[no]) +
+                              m1[no] * (sfc[(sface_f * 3 + 1) * N2 + pq] - sF[FS + no]) +
+                              m2[no] * (sfc[(sface_f * 3 + 2) * N2 + pq] - sF[2 * FS + no]);
+            r += (gq ? inv2H : -inv2H) * sacc;
+          }
+          sdiv[(al * 2 + half) * FS + no] = r;
         }
-        sdiv[(al * 2 + half) * FS + no] = r;
       }
     }
     __syncthreads();
-    {
-      const long long n = e * N3 + tid;
+    // one stage: the contraction pass has read it, so the next copy can start
+    if constexpr (NS == 1) {
+      if (warp == 0 && t1.x >= 0) issue(t1, 0);
+    }
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) {
+      const int node = tid + r * THR;
+      const int ti = node & 7, tj = (node >> 3) & 7, tk = node >> 6;
+      const int tpad = pad(ti, tj, tk);
+      const long long n = e * N3 + node;
       real dv = ((sdiv[tpad] + sdiv[2 * FS + tpad]) + sdiv[4 * FS + tpad]) +
                 ((sdiv[FS + tpad] + sdiv[3 * FS + tpad]) + sdiv[5 * FS + tpad]);
-      dv *= cur.invJ;
+      dv *= cur[r].invJ;
       if (bnd && Q.bc_on) {
         const int idx3[3] = {ti, tj, tk};
         for (int f = 0; f < 6; ++f) {
@@ -910,20 +941,21 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k2)
         }
       }
       if (P.epi)
-        n8_rk<real>(P.stage, Q.dt, dv, cur.y, cur.y, cur.acc, cur.comp, n, Q.y, Q.acc, Q.out,
+        n8_rk<real>(P.stage, Q.dt, dv, cur[r].y, cur[r].y, cur[r].acc, cur[r].comp, n, Q.y, Q.acc, Q.out,
                     comp_on ? Q.comp : nullptr, P.flag);
       else
         Q.Pidot[n] = dv;
     }
     if (has_next) {
 #pragma unroll
-      for (int r = 0; r < 3; ++r)
-        if (tid + r * THREADS < NFACE) sface[(fb ^ 1) * NFACE + tid + r * THREADS] = fnext[r];
+      for (int r = 0; r < NFR; ++r)
+        if (tid + r * THR < NFACE) sface[(fb ^ 1) * NFACE + tid + r * THR] = fnext[r];
     }
-    cur = nxt;
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) cur[r] = nxt[r];
     emcur = emnext;
 #pragma unroll
-    for (int r = 0; r < 3; ++r) src1[r] = src2[r];
+    for (int r = 0; r < NFR; ++r) src1[r] = src2[r];
     if constexpr (BATCH) {
       t0 = t1;
       t1 = t2;
@@ -1025,10 +1057,10 @@ static int n8_launch(int which, const void* hP, const void* plist, const int2* t
         return -2;
       attr2 = true;
     }
-    const long long cap = (long long)sm_count() * n8::Occ<real>::k2;
+    const long long cap = (long long)sm_count() * K2Shape<real>::OCC;
     const long long grid = ntiles < cap ? ntiles : cap;
     if (grid <= 0) return 0;
-    k_cons_k2_n8<real, NT, BATCH><<<(unsigned)grid, n8::THREADS, k2_smem<real>(), s>>>(
+    k_cons_k2_n8<real, NT, BATCH><<<(unsigned)grid, K2Shape<real>::THR, k2_smem<real>(), s>>>(
         *(const K2N8<real>*)hP, (const K2N8<real>*)plist, tiles, ntiles);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
