@@ -38,9 +38,9 @@
 //       FP32).  Two-term split (hi + lo): one MMA with A = [[G_hi, G_hi],
 //       [G_lo, G_lo]], B = [v_hi; v_lo]; it carries ~16 significant bits and
 //       misses FP32 accuracy by a factor of ~30 on the n = 8 warped workload,
-//       so it is kept only for the precision study.  Because every row of G
-//       sums to zero, the operand is taken relative to its value at node 3 of
-//       the pencil (D(v - c) = D v), so the split error scales with the
+//       so it is kept only for the precision study; there, because every row
+//       of G sums to zero, the operand is taken relative to its value at node
+//       3 of the pencil (D(v - c) = D v), so the split error scales with the
 //       variation of the field along the pencil, not with its size;
 //   * a node phase (one node per thread) forms flux, Phidot / divergence,
 //     boundary terms (boundary elements only) and the RK4 stage update and
@@ -65,7 +65,7 @@ constexpr long long WAIT_LIMIT = 1LL << 24;
 // staged elements in flight: element e + (NSTAGE - 1) * grid is copied while e
 // is processed
 constexpr int NSTAGE = 2;
-constexpr int PREF = 3;            // FP32 form: pencil node whose value is the operand offset
+constexpr int PREF = 3;            // two-term FP32 form: pencil node whose value is the operand offset
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
@@ -489,16 +489,25 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
           for (int c = 0; c < 3; ++c) cm[c][b] = dm[c][b];
         }
       } else {
-        const int nd0 = bn(al, wt8, 2 * tig, gq), nd1 = bn(al, wt8, 2 * tig + 1, gq), ndr = bn(al, wt8, PREF, gq);
-        const float u0 = sPhi[unpad(nd0)], u1 = sPhi[unpad(nd1)], ur = sPhi[unpad(ndr)];
+        // the three-term split carries FP32's 24 bits, so only the two-term
+        // form takes the operand relative to its pencil value at node PREF
+        constexpr bool OFS = NT == 2;
+        const int nd0 = bn(al, wt8, 2 * tig, gq), nd1 = bn(al, wt8, 2 * tig + 1, gq);
+        const float u0 = sPhi[unpad(nd0)], u1 = sPhi[unpad(nd1)];
+        const int ndr = OFS ? bn(al, wt8, PREF, gq) : 0;
+        const float ur = OFS ? sPhi[unpad(ndr)] : 0.f;
         float fu[4] = {0, 0, 0, 0}, fm[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
         mma_split<NT>(fu, aS, aS2, u0 - ur, u1 - ur);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
           if ((comps >> c) & 1) {
             const real* mc = sJa + (al * 3 + c) * FS;
-            const float pr = mc[ndr] * ur;
-            mma_split<NT>(fm[c], aS, aS2, fmaf(mc[nd0], u0, -pr), fmaf(mc[nd1], u1, -pr));
+            if constexpr (OFS) {
+              const float pr = mc[ndr] * ur;
+              mma_split<NT>(fm[c], aS, aS2, fmaf(mc[nd0], u0, -pr), fmaf(mc[nd1], u1, -pr));
+            } else {
+              mma_split<NT>(fm[c], aS, aS2, mc[nd0] * u0, mc[nd1] * u1);
+            }
           }
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
@@ -874,10 +883,12 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
           }
           cx[0] = dx[0]; cx[1] = dx[1]; cy[0] = dy[0]; cy[1] = dy[1];
         } else {
+          constexpr bool OFS = NT == 2;  // operand offset only for the two-term split (see K1)
+          constexpr int NQ = OFS ? 3 : 2;
           const int nd[3] = {bn(al, wt8, 2 * tig, gq), bn(al, wt8, 2 * tig + 1, gq), bn(al, wt8, PREF, gq)};
-          float vx[3], vy[3];
+          float vx[3] = {0, 0, 0}, vy[3] = {0, 0, 0};
 #pragma unroll
-          for (int q = 0; q < 3; ++q) {
+          for (int q = 0; q < NQ; ++q) {
             if (half == 0) {
               const float f0 = sF[nd[q]];
               vx[q] = m0[nd[q]] * f0 + m1[nd[q]] * sF[FS + nd[q]] + m2[nd[q]] * sF[2 * FS + nd[q]];
