@@ -49,6 +49,8 @@ enum { WT_F64 = 0, WT_F32 = 1 };
 enum { WT_FP32_CUDA_CORES = 0, WT_FP32_BF16X3 = 1, WT_FP32_BF16X2 = 2 };
 enum { WT_BC_DIRICHLET = 1, WT_BC_SOMMERFELD = 2, WT_BC_EXCISION = 3, WT_BC_FULL_DIRICHLET = 4 };
 enum { WT_BG_MINKOWSKI = 0, WT_BG_CONSTANT_SHIFT = 1, WT_BG_ADM_PERTURBED = 2, WT_BG_RADIAL_SHIFT = 3 };
+/* prescribed 4-metrics of the fully second-order curved path */
+enum { WT_CURVED4_MINKOWSKI = 0, WT_CURVED4_GAUGE_WAVE = 1 };
 
 typedef struct wt_ctx wt_ctx;
 typedef struct wt_mesh wt_mesh;
@@ -240,6 +242,22 @@ int wt_rhs_strong(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, void* u
 /* wave_lap_strong_conservative_mesh!(Lu, u, mesh, ops, h; tau)
  * (src/wave_lap_strong.jl:280-308): uniform Cartesian meshes. */
 int wt_lap_strong_cons(wt_ctx* ctx, wt_ws* ws, const void* u, void* Lu, double h, double tau);
+
+/* Scalar wave on a prescribed 4-metric, fully second order.
+ * wt_curved4_background replaces eval_curved_background!
+ * (src/wave_curved_rhs.jl:373-418) for the analytic metrics named by
+ * WT_CURVED4_*: fills ginv (10,N,N,N,Ne: tt,tx,ty,tz,xx,xy,xz,yy,yz,zz) and
+ * gamma (4,N,N,N,Ne: contracted Christoffels), device arrays in the mesh
+ * precision; params = (A, d) of the gauge wave H = A sin(2 pi (x - t)/d).
+ * wt_rhs_curved4 replaces wave_curved_rhs_mesh! (conservative = 0,
+ * src/wave_curved_rhs.jl:155-187) and wave_curved_rhs_conservative_mesh!
+ * (conservative = 1, tau as its keyword, the reference default (N-1)^2;
+ * src/wave_curved_rhs.jl:330-362): phiddot = d_tt phi on uniform Cartesian
+ * elements of edge h, faces without a neighbour seeing zero traces. */
+int wt_curved4_background(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, double t, void* ginv,
+                          void* gamma);
+int wt_rhs_curved4(wt_ctx* ctx, wt_ws* ws, const void* phi, const void* phidot, void* phiddot, const void* ginv,
+                   const void* gamma, double h, int conservative, double tau);
 
 /* ---- reductions (FP64 accumulation, synchronous) ----------------------------- */
 /* wave3d_energy (src/wave3d_curved.jl:268-287). */

@@ -70,6 +70,8 @@ def lib():
         L.or_rhs_sipg.argtypes = [vp, vp, vp, vp, vp, d, d]
         L.or_rhs_strong.argtypes = [vp, vp, vp, vp, d, d]
         L.or_lap_strong_cons.argtypes = [vp, vp, vp, d, d]
+        L.or_rhs_curved4.argtypes = [vp, vp, vp, vp, vp, vp, d, i, d]
+        L.or_curved4_background.argtypes = [vp, i, vp, d, vp, vp]
         L.or_evolve_curved.argtypes = [vp, vp, vp, vp, d, i, d, C.POINTER(_BC), i, vp]
         L.or_sipg_f.argtypes = [vp, vp, vp, vp, vp, vp, d, d, d]
         L.or_energy_sipg.restype = d
@@ -231,6 +233,25 @@ class OracleMesh:
             tau = float((self.N - 1) ** 2)
         out = np.zeros(self.nn)
         lib().or_lap_strong_cons(self.h, _p(np.ascontiguousarray(u)), _p(out), hel, tau)
+        return out
+
+    def curved4_background(self, kind=0, params=(0.0, 1.0), t=0.0):
+        """eval_curved_background! (src/wave_curved_rhs.jl:373-418): kind 0 Minkowski,
+        1 gauge wave (A, d).  Returns ginv (10*nn, component fastest) and gam (4*nn)."""
+        ginv = np.zeros(10 * self.nn); gam = np.zeros(4 * self.nn)
+        pp = np.asarray(list(params) + [0.0] * 2, dtype=np.float64)
+        lib().or_curved4_background(self.h, int(kind), _p(pp), float(t), _p(ginv), _p(gam))
+        return ginv, gam
+
+    def rhs_curved4(self, phi, phid, ginv, gam, hel, conservative=False, tau=None):
+        """wave_curved_rhs_mesh! / wave_curved_rhs_conservative_mesh! (src/wave_curved_rhs.jl:155-362)."""
+        if tau is None:
+            tau = float((self.N - 1) ** 2)
+        out = np.zeros(self.nn)
+        lib().or_rhs_curved4(self.h, _p(np.ascontiguousarray(phi, dtype=np.float64)),
+                             _p(np.ascontiguousarray(phid, dtype=np.float64)), _p(out),
+                             _p(np.ascontiguousarray(ginv, dtype=np.float64)),
+                             _p(np.ascontiguousarray(gam, dtype=np.float64)), float(hel), int(conservative), tau)
         return out
 
     def evolve_curved(self, coef, Phi, Pi, dt, nsteps, eps_ko=0.0, bc=None, use_metric=False,

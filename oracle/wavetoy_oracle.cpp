@@ -1079,6 +1079,119 @@ void or_lap_strong_cons(void* h, const double* u, double* Lu, double hel, double
 }
 
 // ---------------------------------------------------------------------------
+// Scalar wave on a prescribed 4-metric, fully second order (wave_curved_rhs_*,
+// src/wave_curved_rhs.jl:45-362): per element, the SBP gradients of phi and
+// phidot (centred-flux SAT on the perpendicular component of each face, or no
+// SAT in the conservative variant), the six Hessian components as a second G
+// sweep of the (SAT-corrected) gradient, the pointwise solve
+//   phidd = (Gam.dphi - 2 g^{ti} d_i phidot - g^{ij} d_ij phi) / g^{tt}
+// and, conservative variant, the Mattsson-Nordstrom SAT pair per face
+// (src/wave_curved_rhs.jl:332-345).  ginv is (10,N,N,N,Ne) (tt,tx,ty,tz,xx,xy,
+// xz,yy,yz,zz), gam is (4,N,N,N,Ne); faces without a neighbour get zero traces
+// (src/wave_curved_rhs.jl:168-184).  Uniform Cartesian elements of edge hel.
+void or_rhs_curved4(void* h, const double* phi, const double* phid, double* phidd, const double* ginv,
+                    const double* gam, double hel, int conservative, double tau) {
+  Mesh& m = *static_cast<Mesh*>(h);
+  const int N = m.N; const long Ne = m.Ne; const long ne3 = (long)N * N * N;
+  const double* H = m.ops.H.data();
+  const double inv_h = 1.0 / hel;
+#pragma omp parallel
+  {
+    Mesh loc; loc.N = N; loc.ops = m.ops; loc.Ne = 1;
+    std::vector<double> ue(ne3), ve(ne3), du(3 * ne3), dv(3 * ne3), dd(6 * ne3), out(ne3);
+    std::vector<double> uf(6 * N * N), vf(6 * N * N);
+#pragma omp for schedule(static)
+    for (long e = 0; e < Ne; ++e) {
+      std::copy(phi + ne3 * e, phi + ne3 * (e + 1), ue.begin());
+      std::copy(phid + ne3 * e, phid + ne3 * (e + 1), ve.begin());
+      for (int f = 0; f < 6; ++f) {  // neighbour face traces (zero without a neighbour)
+        long en = m.nbr[f + 6 * e]; int fn = m.nbrf[f + 6 * e], rn = frow(fn, N);
+        for (int q = 0; q < N; ++q)
+          for (int p = 0; p < N; ++p) {
+            double a_ = 0.0, b_ = 0.0;
+            if (en >= 0) {
+              int a, b, c; face_ijk(faxis(fn), rn, p, q, a, b, c);
+              a_ = phi[nid(N, a, b, c, en)]; b_ = phid[nid(N, a, b, c, en)];
+            }
+            uf[f * N * N + p + N * q] = a_; vf[f * N * N + p + N * q] = b_;
+          }
+      }
+      for (int c = 0; c < 3; ++c) {
+        ref_deriv(loc, ue.data(), &du[c * ne3], c, 0);
+        ref_deriv(loc, ve.data(), &dv[c * ne3], c, 0);
+        for (long t = 0; t < ne3; ++t) { du[c * ne3 + t] *= inv_h; dv[c * ne3 + t] *= inv_h; }
+      }
+      if (!conservative) {
+        for (int f = 0; f < 6; ++f) {
+          int al = f / 2, fr = frow(f, N);
+          double coef = fsign(f) * 0.5 * (1.0 / H[fr]) * inv_h;
+          for (int q = 0; q < N; ++q)
+            for (int p = 0; p < N; ++p) {
+              int i, j, k; face_ijk(al, fr, p, q, i, j, k);
+              long t = nid(N, i, j, k, 0);
+              du[al * ne3 + t] += coef * (uf[f * N * N + p + N * q] - ue[t]);
+              dv[al * ne3 + t] += coef * (vf[f * N * N + p + N * q] - ve[t]);
+            }
+        }
+      }
+      // Hessian: xx, xy, xz from d_x phi; yy, yz from d_y phi; zz from d_z phi
+      const int src[6] = {0, 0, 0, 1, 1, 2}, axis[6] = {0, 1, 2, 1, 2, 2};
+      for (int c = 0; c < 6; ++c) {
+        ref_deriv(loc, &du[src[c] * ne3], &dd[c * ne3], axis[c], 0);
+        for (long t = 0; t < ne3; ++t) dd[c * ne3 + t] *= inv_h;
+      }
+      for (long t = 0; t < ne3; ++t) {
+        const double* g = ginv + 10 * (t + ne3 * e);
+        const double* G4 = gam + 4 * (t + ne3 * e);
+        double gdd = G4[0] * ve[t] + G4[1] * du[t] + G4[2] * du[ne3 + t] + G4[3] * du[2 * ne3 + t];
+        double gti = g[1] * dv[t] + g[2] * dv[ne3 + t] + g[3] * dv[2 * ne3 + t];
+        double gij = g[4] * dd[t] + g[7] * dd[3 * ne3 + t] + g[9] * dd[5 * ne3 + t] + 2 * g[5] * dd[ne3 + t] +
+                     2 * g[6] * dd[2 * ne3 + t] + 2 * g[8] * dd[4 * ne3 + t];
+        out[t] = (gdd - 2 * gti - gij) / g[0];
+      }
+      if (conservative) {
+        for (int f = 0; f < 6; ++f) {
+          int al = f / 2, fr = frow(f, N);
+          double coef_neu = -fsign(f) * inv_h * (1.0 / H[fr]);
+          double coef_dir = -(tau * inv_h) * (1.0 / H[fr]);
+          for (int q = 0; q < N; ++q)
+            for (int p = 0; p < N; ++p) {
+              int i, j, k; face_ijk(al, fr, p, q, i, j, k);
+              long t = nid(N, i, j, k, 0);
+              out[t] += coef_neu * du[al * ne3 + t];
+              out[t] += coef_dir * (ue[t] - uf[f * N * N + p + N * q]);
+            }
+        }
+      }
+      std::copy(out.begin(), out.end(), phidd + ne3 * e);
+    }
+  }
+}
+
+// Prescribed 4-metrics at the mesh nodes (eval_curved_background!,
+// src/wave_curved_rhs.jl:373-418): kind 0 Minkowski; kind 1 the gauge wave of
+// the Apples-with-Apples tests (Alcubierre et al. 2004), ds^2 = (1 - H)(-dt^2 +
+// dx^2) + dy^2 + dz^2, H = A sin(2 pi (x - t)/d), p = (A, d).  Its inverse is
+// diag(-1/(1-H), 1/(1-H), 1, 1), and the contracted Christoffels
+// g^{ab} Gam^c_ab = -(1/sqrt(-g)) d_a(sqrt(-g) g^{ac}) vanish (sqrt(-g) g^{tt}
+// = -1, sqrt(-g) g^{xx} = 1 are constant: the metric is in harmonic gauge).
+void or_curved4_background(void* h, int kind, const double* p, double t, double* ginv, double* gam) {
+  Mesh& m = *static_cast<Mesh*>(h);
+  const long nn = m.nn();
+  for (long n = 0; n < nn; ++n) {
+    double* g = ginv + 10 * n;
+    for (int c = 0; c < 10; ++c) g[c] = 0.0;
+    for (int c = 0; c < 4; ++c) gam[4 * n + c] = 0.0;
+    double f = 1.0;
+    if (kind == 1) f = 1.0 - p[0] * std::sin(2.0 * M_PI * (m.coords[3 * n] - t) / p[1]);
+    g[0] = -1.0 / f;
+    g[4] = 1.0 / f;
+    g[7] = 1.0;
+    g[9] = 1.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Classic RK4 (the reference's _rk4_3d!, test/wave3d_tests.jl:32-44; also
 // OrdinaryDiffEq RK4() with a fixed step): k1..k4 and
 // u += dt/6 (k1 + 2 k2 + 2 k3 + k4).  energy (nsteps+1, may be NULL) records

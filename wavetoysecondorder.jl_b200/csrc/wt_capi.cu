@@ -926,6 +926,36 @@ int wt_lap_strong_cons(wt_ctx* ctx, wt_ws* ws, const void* u, void* Lu, double h
 }
 
 // ---- reductions ---------------------------------------------------------------------------
+int wt_curved4_background(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, double t, void* ginv,
+                          void* gamma) {
+  if (!ctx) return WT_EINVAL;
+  if (!mesh || !ginv || !gamma) return fail(ctx, WT_EINVAL, "wt_curved4_background: NULL argument");
+  if (kind != WT_CURVED4_MINKOWSKI && kind != WT_CURVED4_GAUGE_WAVE)
+    return fail(ctx, WT_EINVAL, "wt_curved4_background: unknown metric kind");
+  double p[2] = {0.0, 1.0};
+  if (kind == WT_CURVED4_GAUGE_WAVE) {
+    if (!params) return fail(ctx, WT_EINVAL, "wt_curved4_background: the gauge wave needs (A, d)");
+    p[0] = params[0];
+    p[1] = params[1];
+    if (!(p[1] != 0.0) || !(std::fabs(p[0]) < 1.0))
+      return fail(ctx, WT_EINVAL, "wt_curved4_background: gauge wave needs |A| < 1 and d != 0");
+  }
+  WT_TRY(need_setup_geometry(mesh, "wt_curved4_background"));
+  ctx->launches += 1;
+  return lrc(ctx, wt::launch_curved4_background(mesh->m, kind, p, t, ginv, gamma, ctx->stream), "curved4 background");
+}
+
+int wt_rhs_curved4(wt_ctx* ctx, wt_ws* ws, const void* phi, const void* phidot, void* phiddot, const void* ginv,
+                   const void* gamma, double h, int conservative, double tau) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!phi || !phidot || !phiddot || !ginv || !gamma) return fail(ctx, WT_EINVAL, "wt_rhs_curved4: NULL argument");
+  if (!(h > 0)) return fail(ctx, WT_EINVAL, "wt_rhs_curved4: h must be positive");
+  if (!ws->mesh->m.affine) return fail(ctx, WT_EINVAL, "wt_rhs_curved4: uniform Cartesian meshes only");
+  ctx->launches += 1;
+  return lrc(ctx, wt::launch_curved4(ws->mesh->m, phi, phidot, phiddot, ginv, gamma, h, conservative ? 1 : 0, tau,
+                                     ctx->stream), "rhs_curved4");
+}
+
 int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, int use_metric,
               double* E) {
   WT_TRY(check_ws(ctx, ws));

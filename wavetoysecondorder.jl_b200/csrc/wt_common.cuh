@@ -219,6 +219,11 @@ int launch_sipg(const DevMesh& m, const void* u, const void* ut, void* utt, void
 int launch_strong(const DevMesh& m, const void* u, const void* ut, void* utt, double tau, double inv_R,
                   cudaStream_t s);
 int launch_lap_strong_cons(const DevMesh& m, const void* u, void* Lu, double h, double tau, cudaStream_t s);
+// scalar wave on a prescribed 4-metric (wt_second.cu)
+int launch_curved4(const DevMesh& m, const void* u, const void* ud, void* udd, const void* ginv, const void* gam,
+                   double h, int conservative, double tau, cudaStream_t s);
+int launch_curved4_background(const DevMesh& m, int kind, const double* p, double t, void* ginv, void* gam,
+                              cudaStream_t s);
 
 // reductions and vector updates (wt_reduce.cu)
 int launch_energy(const DevMesh& m, const DevCoef& c, const void* Pi, const void* grad, int use_metric,

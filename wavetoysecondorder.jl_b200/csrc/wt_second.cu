@@ -11,6 +11,8 @@
 //   * wave_lap_strong_conservative_mesh! (src/wave_lap_strong.jl:183-308).
 #include "wt_common.cuh"
 
+#include <algorithm>
+
 namespace wt {
 
 template <int N>
@@ -349,6 +351,130 @@ __global__ void __launch_bounds__(Sp<N>::T) k_lap_strong_cons(long long Ne, cons
   Lu[n] = (real)s;
 }
 
+// Scalar wave on a prescribed 4-metric (wave_curved_rhs_element! /
+// wave_curved_rhs_conservative_element!, src/wave_curved_rhs.jl:45-136 and
+// 217-348) on every element of a uniform Cartesian mesh: the gradients of phi
+// and phidot (centred-flux SAT on the perpendicular component of each face
+// unless CONS), the six Hessian components as a second G sweep of the gradient
+// of phi, the pointwise solve
+//   phidd = (Gam.(phidot, dphi) - 2 g^{ti} d_i phidot - g^{ij} d_ij phi) / g^{tt}
+// and, when CONS, the Mattsson-Nordstrom SAT pair on the faces.  ginv holds
+// (tt,tx,ty,tz,xx,xy,xz,yy,yz,zz) and gam (t,x,y,z) per node, component
+// fastest; faces without a neighbour see zero traces.  FP64 arithmetic.
+template <int N, typename real, bool CONS>
+__global__ void __launch_bounds__(Sp<N>::T) k_curved4(long long Ne, const real* __restrict__ u,
+                                                     const real* __restrict__ ud, real* __restrict__ udd,
+                                                     const real* __restrict__ ginv, const real* __restrict__ gam,
+                                                     double inv_h, double tau, const int32_t* __restrict__ nbr,
+                                                     const int32_t* __restrict__ nbrf, const double* __restrict__ G,
+                                                     const double* __restrict__ H) {
+  constexpr int N3 = Sp<N>::N3, N2 = Sp<N>::N2, EPB = Sp<N>::EPB;
+  __shared__ double GT[N2];
+  __shared__ double su[EPB][N3];
+  __shared__ double sv[EPB][N3];
+  __shared__ double sdu[EPB][3][N3];
+  const int tid = threadIdx.x;
+  const int le = tid / N3, t = tid - le * N3;
+  const int i = t % N, j = (t / N) % N, k = t / N2;
+  const long long e = (long long)blockIdx.x * EPB + le;
+  const bool valid = e < Ne;
+  const long long ec = valid ? e : 0;
+  const long long n = ec * N3 + t;
+  if (tid < N2) GT[(tid % N) * N + tid / N] = G[tid];
+  const double uv = valid ? (double)u[n] : 0.0, vv = valid ? (double)ud[n] : 0.0;
+  su[le][t] = uv;
+  sv[le][t] = vv;
+  // neighbour traces of phi and phidot at this node's faces (zero without one)
+  const int idx3[3] = {i, j, k};
+  double uf[6], vf[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    uf[f] = 0.0;
+    vf[f] = 0.0;
+    const int al = f >> 1;
+    if (!valid || idx3[al] != frow(f, N)) continue;
+    const int en = nbr[f + 6 * ec];
+    if (en < 0) continue;
+    const int fn = nbrf[f + 6 * ec];
+    const int p = al == 0 ? j : i, q = al == 2 ? j : k;
+    const long long src = (long long)en * N3 + face_node(faxis(fn), frow(fn, N), p, q, N);
+    uf[f] = (double)u[src];
+    vf[f] = (double)ud[src];
+  }
+  __syncthreads();
+  double du[3], dv[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    du[c] = ctr<N>(su[le], GT, i, j, k, c) * inv_h;
+    dv[c] = ctr<N>(sv[le], GT, i, j, k, c) * inv_h;
+  }
+  if (!CONS) {
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const int al = f >> 1, fr = frow(f, N);
+      if (idx3[al] != fr) continue;
+      const double coef = ((f & 1) ? 1.0 : -1.0) * 0.5 * (1.0 / H[fr]) * inv_h;
+      du[al] += coef * (uf[f] - uv);
+      dv[al] += coef * (vf[f] - vv);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) sdu[le][c][t] = du[c];
+  __syncthreads();
+  if (!valid) return;
+  // Hessian: xx, xy, xz of d_x phi; yy, yz of d_y phi; zz of d_z phi
+  const double dxx = ctr<N>(sdu[le][0], GT, i, j, k, 0) * inv_h;
+  const double dxy = ctr<N>(sdu[le][0], GT, i, j, k, 1) * inv_h;
+  const double dxz = ctr<N>(sdu[le][0], GT, i, j, k, 2) * inv_h;
+  const double dyy = ctr<N>(sdu[le][1], GT, i, j, k, 1) * inv_h;
+  const double dyz = ctr<N>(sdu[le][1], GT, i, j, k, 2) * inv_h;
+  const double dzz = ctr<N>(sdu[le][2], GT, i, j, k, 2) * inv_h;
+  double g[10], gm[4];
+#pragma unroll
+  for (int c = 0; c < 10; ++c) g[c] = (double)ginv[10 * n + c];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) gm[c] = (double)gam[4 * n + c];
+  const double gdd = gm[0] * vv + gm[1] * du[0] + gm[2] * du[1] + gm[3] * du[2];
+  const double gti = g[1] * dv[0] + g[2] * dv[1] + g[3] * dv[2];
+  const double gij = g[4] * dxx + g[7] * dyy + g[9] * dzz + 2 * g[5] * dxy + 2 * g[6] * dxz + 2 * g[8] * dyz;
+  double s = (gdd - 2 * gti - gij) / g[0];
+  if (CONS) {
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const int al = f >> 1, fr = frow(f, N);
+      if (idx3[al] != fr) continue;
+      const double coef_neu = -((f & 1) ? 1.0 : -1.0) * inv_h * (1.0 / H[fr]);
+      const double coef_dir = -(tau * inv_h) * (1.0 / H[fr]);
+      s += coef_neu * du[al];
+      s += coef_dir * (uv - uf[f]);
+    }
+  }
+  udd[n] = (real)s;
+}
+
+// Prescribed 4-metrics at the nodes (eval_curved_background!,
+// src/wave_curved_rhs.jl:373-418): kind 0 Minkowski, kind 1 the gauge wave
+// ds^2 = (1 - H)(-dt^2 + dx^2) + dy^2 + dz^2, H = A sin(2 pi (x - t)/d)
+// (Alcubierre et al. 2004), p = (A, d).  Its inverse is diag(-1/(1-H),
+// 1/(1-H), 1, 1) and its contracted Christoffels vanish (harmonic gauge).
+template <typename real>
+__global__ void k_curved4_bg(long long nn, const double* __restrict__ coords, int kind, double A, double d, double t,
+                             real* __restrict__ ginv, real* __restrict__ gam) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
+    double f = 1.0;
+    if (kind == 1) f = 1.0 - A * sin(2.0 * M_PI * (coords[3 * n] - t) / d);
+    real* g = ginv + 10 * n;
+#pragma unroll
+    for (int c = 0; c < 10; ++c) g[c] = (real)0;
+    g[0] = (real)(-1.0 / f);
+    g[4] = (real)(1.0 / f);
+    g[7] = (real)1;
+    g[9] = (real)1;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) gam[4 * n + c] = (real)0;
+  }
+}
+
 // ---------------------------------------------------------------------------
 #define WT_DISPATCH_N2(N_, CALL)  \
   switch (N_) {                   \
@@ -421,6 +547,40 @@ int launch_lap_strong_cons(const DevMesh& m, const void* u, void* Lu, double h, 
   } else {
     WT_DISPATCH_N2(m.N, (lsc_dispatch<NN, float>(m, u, Lu, h, tau, s)));
   }
+}
+
+template <int N, typename real>
+static int c4_dispatch(const DevMesh& m, const void* u, const void* ud, void* udd, const void* ginv, const void* gam,
+                       double h, int cons, double tau, cudaStream_t s) {
+  const unsigned blocks = (unsigned)((m.Ne + Sp<N>::EPB - 1) / Sp<N>::EPB);
+  if (cons)
+    k_curved4<N, real, true><<<blocks, Sp<N>::T, 0, s>>>(m.Ne, (const real*)u, (const real*)ud, (real*)udd,
+                                                          (const real*)ginv, (const real*)gam, 1.0 / h, tau, m.nbr,
+                                                          m.nbrf, m.G, m.H);
+  else
+    k_curved4<N, real, false><<<blocks, Sp<N>::T, 0, s>>>(m.Ne, (const real*)u, (const real*)ud, (real*)udd,
+                                                           (const real*)ginv, (const real*)gam, 1.0 / h, tau, m.nbr,
+                                                           m.nbrf, m.G, m.H);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int launch_curved4(const DevMesh& m, const void* u, const void* ud, void* udd, const void* ginv, const void* gam,
+                   double h, int conservative, double tau, cudaStream_t s) {
+  if (m.precision == 0) {
+    WT_DISPATCH_N2(m.N, (c4_dispatch<NN, double>(m, u, ud, udd, ginv, gam, h, conservative, tau, s)));
+  } else {
+    WT_DISPATCH_N2(m.N, (c4_dispatch<NN, float>(m, u, ud, udd, ginv, gam, h, conservative, tau, s)));
+  }
+}
+
+int launch_curved4_background(const DevMesh& m, int kind, const double* p, double t, void* ginv, void* gam,
+                              cudaStream_t s) {
+  const unsigned blocks = (unsigned)std::min<long long>((m.nn + 255) / 256, 8192);
+  if (m.precision == 0)
+    k_curved4_bg<double><<<blocks, 256, 0, s>>>(m.nn, m.coords, kind, p[0], p[1], t, (double*)ginv, (double*)gam);
+  else
+    k_curved4_bg<float><<<blocks, 256, 0, s>>>(m.nn, m.coords, kind, p[0], p[1], t, (float*)ginv, (float*)gam);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 }  // namespace wt

@@ -29,6 +29,8 @@ BG_MINKOWSKI, BG_CONSTANT_SHIFT, BG_ADM_PERTURBED, BG_RADIAL_SHIFT = 0, 1, 2, 3
 IC_EIGENMODE_CARTESIAN, IC_GAUSSIANS, IC_OUTGOING_PULSE, IC_PLANE_WAVE, IC_EIGENMODE_RADIAL = 0, 1, 2, 3, 4
 # precision forms of an FP32 mesh (n = 8 contractions): CUDA cores, split BF16 three-term / two-term
 FP32_CUDA_CORES, FP32_BF16X3, FP32_BF16X2 = 0, 1, 2
+# prescribed 4-metrics of the fully second-order curved path
+CURVED4_MINKOWSKI, CURVED4_GAUGE_WAVE = 0, 1
 
 _ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENOTSUP", -5: "ENONFINITE", -6: "ETIMEOUT"}
 
@@ -87,6 +89,8 @@ def library():
         "wt_rhs_curved": [vp, vp, vp, vp, vp, vp, vp, d, C.POINTER(_BcDesc), i],
         "wt_rhs_curved_noalloc": [vp, vp, vp, vp, vp, vp, d, d, C.POINTER(_BcDesc), i],
         "wt_mesh_set_fp32_form": [vp, i],
+        "wt_curved4_background": [vp, vp, i, vp, d, vp, vp],
+        "wt_rhs_curved4": [vp, vp, vp, vp, vp, vp, vp, d, i, d],
         "wt_mesh_release_setup_geometry": [vp],
         "wt_batch_create": [vp, C.POINTER(vp)], "wt_batch_destroy": [vp],
         "wt_batch_add": [vp, vp, vp, vp, vp, d, C.POINTER(_BcDesc), C.POINTER(i)],
@@ -651,6 +655,27 @@ def wave_lap_strong_conservative_mesh(Lu, u, h: float, ws: Workspace, tau: Optio
     ws.ctx.check(library().wt_lap_strong_cons(ws.ctx.h, ws.h, _ptr(u), _ptr(Lu), float(h), float(tau)),
                  "wave_lap_strong_conservative_mesh!")
     return Lu
+
+
+def eval_curved_background(ginv, gam, mesh: Mesh, kind: int = CURVED4_MINKOWSKI, params=(0.0, 1.0), t: float = 0.0):
+    """eval_curved_background!(ginv_all, Γc_all, mesh, xs, metric, t, h) (src/wave_curved_rhs.jl:373-418) for
+    the analytic metrics CURVED4_MINKOWSKI and CURVED4_GAUGE_WAVE (params = (A, d)); ginv has 10 * nn and
+    gam 4 * nn entries, component fastest."""
+    p = (C.c_double * 2)(*[float(v) for v in list(params)[:2]])
+    mesh.ctx.check(library().wt_curved4_background(mesh.ctx.h, mesh.h, int(kind), p, float(t), _ptr(ginv),
+                                                   _ptr(gam)), "eval_curved_background!")
+    return ginv, gam
+
+
+def wave_curved_rhs_mesh(phidd, phi, phid, ginv, gam, ws: Workspace, h: float, conservative: bool = False,
+                         tau: Optional[float] = None):
+    """wave_curved_rhs_mesh! / wave_curved_rhs_conservative_mesh!(φ̈, φ, φ̇, mesh, ginv, Γc, ops, h; τ)
+    (src/wave_curved_rhs.jl:155-362)."""
+    if tau is None:
+        tau = float((ws.mesh.N - 1) ** 2)
+    ws.ctx.check(library().wt_rhs_curved4(ws.ctx.h, ws.h, _ptr(phi), _ptr(phid), _ptr(phidd), _ptr(ginv), _ptr(gam),
+                                          float(h), int(conservative), float(tau)), "wave_curved_rhs_mesh!")
+    return phidd
 
 
 def energy_sipg(u, ut, ws: Workspace, tau: float) -> float:
