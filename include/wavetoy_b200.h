@@ -290,6 +290,19 @@ int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* P
                           double dt, int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc,
                           int use_metric, double* energy);
 
+/* Device-side diagnostics in place of evolve3d's per-sample host copies of the
+ * whole state (src/evolve.jl:1339-1358): wt_gather_nodes copies the values of
+ * `field` at `count` node indices (e.g. the 1-D slice evolve3d records) to
+ * host_out as FP64; L2 norms and energies come from wt_l2_diff / wt_energy.
+ * Snapshots: wt_snapshot_save writes Phi and Pi with a 64-byte header (magic
+ * "WTB2SNP1", version, N, Ne, precision, field count, t) to a file;
+ * wt_snapshot_load reads one back into a mesh of the same N, Ne and precision.
+ * No counterpart in the reference for the file format (IDEAS.md:57). */
+int wt_gather_nodes(wt_ctx* ctx, wt_mesh* mesh, const void* field, const int64_t* nodes, int count,
+                    double* host_out);
+int wt_snapshot_save(wt_ctx* ctx, wt_mesh* mesh, const void* Phi, const void* Pi, double t, const char* path);
+int wt_snapshot_load(wt_ctx* ctx, wt_mesh* mesh, void* Phi, void* Pi, double* t, const char* path);
+
 /* ---- batches of independent solves ----------------------------------------
  * No counterpart in the reference, which advances one solve per evolve3d
  * call (src/evolve.jl:1149-1358); the batch advances many solves of uneven

@@ -1145,6 +1145,98 @@ int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int n
                       [&]() { return step_sipg_once(ctx, ws, u, ut, dt, bdry_values, tau, sommerfeld_R, eps_ko); });
 }
 
+// ---- device-side diagnostics and snapshots ------------------------------------------
+int wt_gather_nodes(wt_ctx* ctx, wt_mesh* mesh, const void* field, const int64_t* nodes, int count,
+                    double* host_out) {
+  if (!ctx) return WT_EINVAL;
+  if (!mesh || !field || (count > 0 && (!nodes || !host_out)) || count < 0)
+    return fail(ctx, WT_EINVAL, "wt_gather_nodes: bad argument");
+  for (int q = 0; q < count; ++q)
+    if (nodes[q] < 0 || nodes[q] >= mesh->m.nn) return fail(ctx, WT_EINVAL, "wt_gather_nodes: node out of range");
+  if (count == 0) return 0;
+  int64_t* dn = nullptr;
+  double* dv = nullptr;
+  WT_TRY(dalloc(ctx, &dn, count * sizeof(int64_t), nullptr));
+  if (dalloc(ctx, &dv, count * sizeof(double), nullptr)) { cudaFree(dn); return WT_ENOMEM; }
+  cudaMemcpyAsync(dn, nodes, count * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream);
+  int rc = lrc(ctx, wt::launch_gather(mesh->m.precision, count, field, dn, dv, ctx->stream), "gather");
+  ctx->launches += 1;
+  if (!rc) cudaMemcpyAsync(host_out, dv, count * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(dn);
+  cudaFree(dv);
+  if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "gather");
+  return rc;
+}
+
+namespace {
+// Snapshot file: a 64-byte little-endian header, then Phi and Pi as raw
+// arrays in the mesh precision, (N,N,N,Ne) node order.
+struct SnapHeader {
+  char magic[8];        // "WTB2SNP1"
+  uint32_t version;     // 1
+  uint32_t N;
+  uint64_t Ne;
+  uint32_t precision;   // WT_F64 / WT_F32
+  uint32_t nfields;     // 2: Phi, Pi
+  double t;
+  uint8_t reserved[24];
+};
+static_assert(sizeof(SnapHeader) == 64, "snapshot header is 64 bytes");
+}  // namespace
+
+int wt_snapshot_save(wt_ctx* ctx, wt_mesh* mesh, const void* Phi, const void* Pi, double t, const char* path) {
+  if (!ctx) return WT_EINVAL;
+  if (!mesh || !Phi || !Pi || !path) return fail(ctx, WT_EINVAL, "wt_snapshot_save: NULL argument");
+  const wt::DevMesh& m = mesh->m;
+  SnapHeader hd;
+  std::memset(&hd, 0, sizeof(hd));
+  std::memcpy(hd.magic, "WTB2SNP1", 8);
+  hd.version = 1; hd.N = (uint32_t)m.N; hd.Ne = (uint64_t)m.Ne; hd.precision = (uint32_t)m.precision;
+  hd.nfields = 2; hd.t = t;
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  std::vector<char> buf(nb);
+  FILE* fp = std::fopen(path, "wb");
+  if (!fp) return fail(ctx, WT_EINVAL, std::string("wt_snapshot_save: cannot open ") + path);
+  int rc = std::fwrite(&hd, sizeof(hd), 1, fp) == 1 ? 0 : WT_EINVAL;
+  for (const void* f : {Phi, Pi}) {
+    if (rc) break;
+    cudaMemcpyAsync(buf.data(), f, nb, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "wt_snapshot_save"); break; }
+    if (std::fwrite(buf.data(), 1, nb, fp) != nb) rc = fail(ctx, WT_EINVAL, "wt_snapshot_save: write failed");
+  }
+  if (std::fclose(fp) != 0 && !rc) rc = fail(ctx, WT_EINVAL, "wt_snapshot_save: close failed");
+  return rc;
+}
+
+int wt_snapshot_load(wt_ctx* ctx, wt_mesh* mesh, void* Phi, void* Pi, double* t, const char* path) {
+  if (!ctx) return WT_EINVAL;
+  if (!mesh || !Phi || !Pi || !path) return fail(ctx, WT_EINVAL, "wt_snapshot_load: NULL argument");
+  const wt::DevMesh& m = mesh->m;
+  FILE* fp = std::fopen(path, "rb");
+  if (!fp) return fail(ctx, WT_EINVAL, std::string("wt_snapshot_load: cannot open ") + path);
+  SnapHeader hd;
+  int rc = 0;
+  if (std::fread(&hd, sizeof(hd), 1, fp) != 1 || std::memcmp(hd.magic, "WTB2SNP1", 8) != 0 || hd.version != 1)
+    rc = fail(ctx, WT_EINVAL, "wt_snapshot_load: not a snapshot file");
+  else if (hd.N != (uint32_t)m.N || hd.Ne != (uint64_t)m.Ne || hd.precision != (uint32_t)m.precision ||
+           hd.nfields != 2)
+    rc = fail(ctx, WT_EINVAL, "wt_snapshot_load: snapshot does not match the mesh (N, Ne or precision)");
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  std::vector<char> buf(rc ? 0 : nb);
+  for (void* f : {Phi, Pi}) {
+    if (rc) break;
+    if (std::fread(buf.data(), 1, nb, fp) != nb) { rc = fail(ctx, WT_EINVAL, "wt_snapshot_load: file too short"); break; }
+    cudaMemcpyAsync(f, buf.data(), nb, cudaMemcpyHostToDevice, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "wt_snapshot_load");
+  }
+  std::fclose(fp);
+  if (!rc && t) *t = hd.t;
+  return rc;
+}
+
 int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* Phi_host, double* Pi_host, double dt,
                           int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc, int use_metric,
                           double* energy) {

@@ -234,6 +234,7 @@ int launch_sumsq(long long n, int precision, const void* a, double* partial, int
 int launch_scale(long long n, int precision, void* a, double s, cudaStream_t st);
 int launch_fill(long long n, int precision, void* a, double v, cudaStream_t st);
 int launch_copy(long long n, int precision, void* dst, const void* src, cudaStream_t st);
+int launch_gather(int precision, int count, const void* field, const int64_t* nodes, double* out, cudaStream_t s);
 int launch_rk_update(long long n, int precision, int stage, double dt, void* y, void* acc, void* out,
                      const void* k, cudaStream_t st, void* comp = nullptr);
 int launch_axpy(long long n, int precision, void* y, double a, const void* x, cudaStream_t st);

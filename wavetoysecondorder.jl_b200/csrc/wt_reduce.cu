@@ -212,4 +212,20 @@ int launch_finite_check(long long n, int precision, const void* a, unsigned int*
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+// out[q] = field[nodes[q]] in FP64 (device-side diagnostics: slices, probes)
+template <typename real>
+__global__ void k_gather(int count, const real* __restrict__ field, const int64_t* __restrict__ nodes,
+                         double* __restrict__ out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x)
+    out[q] = (double)field[nodes[q]];
+}
+
+int launch_gather(int precision, int count, const void* field, const int64_t* nodes, double* out, cudaStream_t s) {
+  const unsigned blocks = (unsigned)((count + 255) / 256 < 4096 ? (count + 255) / 256 : 4096);
+  if (blocks == 0) return 0;
+  if (precision == 0) k_gather<double><<<blocks, 256, 0, s>>>(count, (const double*)field, nodes, out);
+  else k_gather<float><<<blocks, 256, 0, s>>>(count, (const float*)field, nodes, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 }  // namespace wt

@@ -115,8 +115,15 @@ class Server:
     FP64 requests share the batch (they run as separate groups)."""
 
     def __init__(self, ctx, precision: int = wt.WT_F32, hbm_budget: float = 150e9, tick: int = 50,
-                 max_active: Optional[int] = None, fp32_form: int = wt.FP32_BF16X3, keep_results: bool = False):
+                 max_active: Optional[int] = None, fp32_form: int = wt.FP32_BF16X3, keep_results: bool = False,
+                 fill_nodes: Optional[int] = 8_000_000):
+        """fill_nodes: admit further requests only while the running ones hold fewer
+        nodes than this (about what keeps the GPU busy); beyond it, new requests
+        wait in arrival order, so large requests are not slowed down by sharing
+        the GPU with many others, while small ones still run together.  None:
+        admit whatever the budget allows."""
         self.ctx = ctx
+        self.fill_nodes = fill_nodes
         self.precision = precision
         self.budget = float(hbm_budget)
         self.tick = int(tick)
@@ -147,7 +154,9 @@ class Server:
                 queue.append(pending.popleft())
             # admit in arrival order while the budget (and the slot limit) allows
             while queue and used + self._cost(queue[0]) <= self.budget and \
-                    (self.max_active is None or len(active) < self.max_active):
+                    (self.max_active is None or len(active) < self.max_active) and \
+                    (self.fill_nodes is None or not active or
+                     sum(a["req"].nodes for a in active.values()) < self.fill_nodes):
                 req = queue.popleft()
                 used += self._cost(req)
                 self.peak_used = max(self.peak_used, used)

@@ -89,6 +89,9 @@ def library():
         "wt_rhs_curved": [vp, vp, vp, vp, vp, vp, vp, d, C.POINTER(_BcDesc), i],
         "wt_rhs_curved_noalloc": [vp, vp, vp, vp, vp, vp, d, d, C.POINTER(_BcDesc), i],
         "wt_mesh_set_fp32_form": [vp, i],
+        "wt_gather_nodes": [vp, vp, vp, vp, i, vp],
+        "wt_snapshot_save": [vp, vp, vp, vp, d, C.c_char_p],
+        "wt_snapshot_load": [vp, vp, vp, vp, C.POINTER(d), C.c_char_p],
         "wt_curved4_background": [vp, vp, i, vp, d, vp, vp],
         "wt_rhs_curved4": [vp, vp, vp, vp, vp, vp, vp, d, i, d],
         "wt_mesh_release_setup_geometry": [vp],
@@ -708,6 +711,69 @@ def step_rk4_sipg(u, ut, ws: Workspace, dt: float, nsteps: int, bdry_values=(0,)
                                             C.byref(_bv(bdry_values)), float(tau), float(sommerfeld_R),
                                             float(eps_KO)), "step_rk4_sipg")
     return u, ut
+
+
+def gather_nodes(field, nodes, mesh: Mesh):
+    """Values of a device field at the given node indices, as a float64 numpy array."""
+    import numpy as np
+    idx = np.ascontiguousarray(nodes, dtype=np.int64)
+    out = np.zeros(len(idx))
+    mesh.ctx.check(library().wt_gather_nodes(mesh.ctx.h, mesh.h, _ptr(field), idx.ctypes.data, len(idx),
+                                             out.ctypes.data), "wt_gather_nodes")
+    return out
+
+
+def slice_nodes(mesh: Mesh, y_target: float, z_target: float, atol: float = 1.4901161193847656e-08):
+    """The 1-D diagnostic slice of evolve3d (_build_slice_3d): nodes with y, z within atol
+    of (y_target, z_target), sorted by x.  Returns (node indices, x).  Reads the set-up
+    coordinates once."""
+    import numpy as np
+    xyz = mesh.get("coords").reshape(-1, 3)
+    sel = np.nonzero((np.abs(xyz[:, 1] - y_target) <= atol) & (np.abs(xyz[:, 2] - z_target) <= atol))[0]
+    order = np.argsort(xyz[sel, 0], kind="stable")
+    return sel[order], xyz[sel[order], 0]
+
+
+def snapshot_save(path: str, Phi, Pi, mesh: Mesh, t: float = 0.0):
+    """Write (Phi, Pi) and t to a snapshot file (64-byte header + raw fields)."""
+    mesh.ctx.check(library().wt_snapshot_save(mesh.ctx.h, mesh.h, _ptr(Phi), _ptr(Pi), float(t),
+                                              str(path).encode()), "wt_snapshot_save")
+
+
+def snapshot_load(path: str, Phi, Pi, mesh: Mesh) -> float:
+    """Read a snapshot written for a mesh of the same N, Ne and precision; returns t."""
+    t = C.c_double()
+    mesh.ctx.check(library().wt_snapshot_load(mesh.ctx.h, mesh.h, _ptr(Phi), _ptr(Pi), C.byref(t),
+                                              str(path).encode()), "wt_snapshot_load")
+    return t.value
+
+
+def evolve_curved_device(Phi, Pi, coef: Coef, ws: Workspace, dt: float, steps_per_sample: int, nsamples: int,
+                         eps_KO: float = 0.0, bc3d: Optional[BC3D] = None, metric: bool = False, slice_yz=None):
+    """evolve3d's sample loop (src/evolve.jl:1339-1358) with the state kept on the device:
+    per sample only the 1-D slice of Phi and Pi (slice_yz = (y, z), default the cube
+    centre line), ||Phi||_H (zero reference) and the energy cross to the host.  Phi, Pi
+    are device tensors advanced in place.  Returns dict(ts, xs_line, Phis, Pis, l2_err,
+    energy) with time measured from the start."""
+    import numpy as np
+    mesh = ws.mesh
+    if slice_yz is None:
+        xyz = mesh.get("coords").reshape(-1, 3)
+        slice_yz = (0.5 * (xyz[:, 1].min() + xyz[:, 1].max()), 0.5 * (xyz[:, 2].min() + xyz[:, 2].max()))
+    nodes, xs = slice_nodes(mesh, *slice_yz)
+    zero = mesh.zeros()
+    Phis, Pis = np.zeros((len(nodes), nsamples)), np.zeros((len(nodes), nsamples))
+    l2, E, ts = np.zeros(nsamples), np.zeros(nsamples), np.zeros(nsamples)
+    for n in range(nsamples):
+        step_rk4_curved(Phi, Pi, coef, ws, dt, steps_per_sample, eps_KO=eps_KO, bc3d=bc3d, metric=metric)
+        ts[n] = (n + 1) * steps_per_sample * dt
+        Phis[:, n] = gather_nodes(Phi, nodes, mesh)
+        Pis[:, n] = gather_nodes(Pi, nodes, mesh)
+        l2[n] = l2_diff(Phi, zero, ws, metric)
+        E[n] = wave3d_energy(Phi, Pi, coef, ws, metric)
+    if ws.ctx.nonfinite():
+        raise WaveToyError(-5, "state became non-finite during evolution")
+    return {"ts": ts, "xs_line": xs, "Phis": Phis, "Pis": Pis, "l2_err": l2, "energy": E}
 
 
 def evolve_curved_host(Phi_host, Pi_host, coef: Coef, ws: Workspace, dt: float, steps_per_sample: int,
