@@ -63,7 +63,7 @@ struct DevMesh {
   void* Ja_r = nullptr;      // 9 fields
   void* invdetJ_r = nullptr;
   void* sdiag = nullptr;     // [3e + d] element-constant axis scale invjac[d,d] at node 0
-  void* Ja_n8 = nullptr;     // n = 8: metric terms in padded element blocks (544 words per element), state precision
+  void* Ja_n8 = nullptr;     // n = 8: metric terms in the n8 element-block layout (FP64 512, FP32 544 words per element), state precision
   // per element: bits 0-5 faces that get the centred-flux SAT (interior face with a
   // neighbour), bit 6 element has an outer face
   int32_t* emask = nullptr;

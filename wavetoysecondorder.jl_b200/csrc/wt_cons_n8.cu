@@ -11,9 +11,10 @@
 //     element (Phi and the nine metric terms in K1; the three flux components
 //     and the metric terms in K2) are staged into shared memory with 1D bulk
 //     copies (cp.async.bulk ... mbarrier::complete_tx), one copy per field
-//     block; the metric terms and the flux live in global memory in a
-//     plane-padded element layout (k-plane stride 68 words) that makes the
-//     tensor-core operand loads (nearly) bank-conflict-free.  A ring of
+//     block; the metric terms and the flux live in global memory in an
+//     element layout that makes the shared-memory accesses bank-conflict-free
+//     (FP64: an XOR swizzle of the node index; FP32: k-planes padded to 68
+//     words; see Lay below).  A ring of
 //     NSTAGE stages keeps NSTAGE - 1 elements in flight; one thread polls
 //     each stage's mbarrier, the rest wait at the CTA barrier; every wait is
 //     bounded and raises an error flag instead of spinning forever;
@@ -131,13 +132,55 @@ __device__ __forceinline__ void mma_split(float d[4], const uint32_t a1[4], cons
 }
 
 __device__ __forceinline__ int pad(int i, int j, int k) { return i + 8 * j + PS * k; }
-// padded index -> unpadded node index (i + 8 j + 64 k)
-__device__ __forceinline__ int unpad(int d) { return d - (PS - 64) * (d / PS); }
 
-// Padded node of tile w for axis al at position p along al, pencil slot g.
+// Element-block layouts of the staged fields (the same in global memory and in
+// shared memory, since a bulk copy moves the block verbatim).  n = i + 8 j + 64 k.
+//   FP64: 512 words, the node index with bits 0, 2, 3 XOR-ed by bits 4-8
+//     (bit0 ^= b4 ^ b6, bit2 ^= b4 ^ b6 ^ b8, bit3 ^= b7).  Each half-warp of
+//     every 64-bit access the kernels make -- tensor-core operands along any
+//     axis (position 4 kc + tig, pencil slot gq), accumulator rows (position
+//     gq, slot 2 tig + b) and node order -- then touches 16 distinct 8-byte
+//     bank pairs, i.e. no bank conflicts, and no padding is needed.
+//   FP32: 544 words, k-planes padded to a stride of 68 words.
+template <typename real>
+struct Lay;
+template <>
+struct Lay<double> {
+  static constexpr int FS = 512;
+  __device__ __forceinline__ static int at(int n) {
+    const int b4 = (n >> 4) & 1, b6 = (n >> 6) & 1, b7 = (n >> 7) & 1, b8 = (n >> 8) & 1;
+    return n ^ ((b4 ^ b6) | ((b4 ^ b6 ^ b8) << 2) | (b7 << 3));
+  }
+};
+template <>
+struct Lay<float> {
+  static constexpr int FS = ::wt::n8::FS;
+  __device__ __forceinline__ static int at(int n) { return pad(n & 7, (n >> 3) & 7, n >> 6); }
+};
+// K1's Phi (the caller's unpadded element block).  FP64: every thread loads
+// its node one element ahead (coalesced) and stores it into a double buffer in
+// the Lay<double> layout (REG = true, conflict-free like the other fields;
+// copying it by rows instead needs many small bulk copies, which the copy
+// engine serialises).  FP32: one bulk copy into the stage (unpadded).
+template <typename real>
+struct PhiLay;
+template <>
+struct PhiLay<double> {
+  static constexpr bool REG = true;
+  static constexpr int SZ = 0;  // words in the stage
+  __device__ __forceinline__ static int at(int n) { return Lay<double>::at(n); }
+};
+template <>
+struct PhiLay<float> {
+  static constexpr bool REG = false;
+  static constexpr int SZ = N3;
+  __device__ __forceinline__ static int at(int n) { return n; }
+};
+
+// Node of tile w for axis al at position p along al, pencil slot g.
 // Pencil orders: al=0 (j = w, k = slot); al=1 (i = slot, k = w); al=2 (i = slot, j = w).
 __device__ __forceinline__ int bn(int al, int w, int p, int g) {
-  return al == 0 ? pad(p, w, g) : al == 1 ? pad(g, p, w) : pad(g, w, p);
+  return al == 0 ? p + 8 * w + 64 * g : al == 1 ? g + 8 * p + 64 * w : g + 8 * w + 64 * p;
 }
 // FP64 B operand: position p = 4 kc + tig along al, pencil slot g
 __device__ __forceinline__ int bnode(int al, int w, int kc, int g, int tig) { return bn(al, w, 4 * kc + tig, g); }
@@ -276,16 +319,20 @@ struct K1N8 {
   unsigned* flag;
 };
 
-// K1 staged fields: Phi (unpadded, 512), Ja (9 padded fields, one block each
-// from the padded global copy) and, for FP32, the ten coefficient fields
-// (unpadded).  Register prefetch: Pi, invJ, y, acc, comp (+ c10 for FP64).
+// K1 staged fields: Phi (PhiLay), Ja (9 fields in the Lay layout, one block
+// each from the global copy) and the ten coefficient fields (unpadded, read in
+// node order).  Register prefetch: Pi, invJ, y, acc, comp.
 template <typename real>
 __host__ __device__ constexpr size_t k1_stage() {
-  return (size_t)n8::N3 + 9 * (size_t)n8::FS + (n8::StageCoef<real>::value ? 10 * (size_t)n8::N3 : 0);
+  return (size_t)n8::PhiLay<real>::SZ + 9 * (size_t)n8::Lay<real>::FS +
+         (n8::StageCoef<real>::value ? 10 * (size_t)n8::N3 : 0);
 }
 template <typename real>
 constexpr size_t k1_smem() {
-  return (n8::NSTAGE * k1_stage<real>() + 9 * n8::FS + 2 * 6 * n8::N2) * sizeof(real) + n8::N2 * sizeof(double) + 64;
+  return (n8::NSTAGE * k1_stage<real>() + 9 * n8::Lay<real>::FS + 2 * 6 * n8::N2 +
+          (n8::PhiLay<real>::REG ? 2 * n8::N3 : 0)) *
+             sizeof(real) +
+         n8::N2 * sizeof(double) + 64;
 }
 
 // NT: FP32 split terms (3 or 2); ignored by the FP64 form.  BATCH: the
@@ -300,12 +347,15 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
   constexpr bool F64 = std::is_same<real, double>::value;
   constexpr bool SC = StageCoef<real>::value;
   constexpr size_t K1_STAGE = k1_stage<real>();
+  constexpr int FS = Lay<real>::FS, PSZ = PhiLay<real>::SZ;
   extern __shared__ __align__(128) unsigned char smraw[];
   double* sG = reinterpret_cast<double*>(smraw);                // 64 (FP64 operator)
   real* stg = reinterpret_cast<real*>(sG + N2);                 // NSTAGE stages x 10 fields
   real* sg = stg + NSTAGE * K1_STAGE;                           // 9 padded partial gradients [al*3 + c]
   real* sface = sg + 9 * FS;                                    // 2 x 6 x 64
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sface + 2 * 6 * N2);  // NSTAGE
+  real* sphi = sface + 2 * 6 * N2;                              // PhiLay::REG: 2 x 512 (Lay)
+  constexpr bool PHIR = PhiLay<real>::REG;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sphi + (PHIR ? 2 * N3 : 0));  // NSTAGE
   __shared__ int abort_flag;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7, half = warp >> 3;
@@ -317,7 +367,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
   const unsigned tx_bytes = (unsigned)(K1_STAGE * sizeof(real));
   // node-phase coordinates of this thread
   const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
-  const int tpad = pad(ti, tj, tk);
+  const int tpad = Lay<real>::at(tid), tphi = PhiLay<real>::at(tid);
   const long long T = BATCH ? ntiles : P.Ne;
   const long long GS = gridDim.x;
   // tile t = (solve, element); (-1, -1) past the end
@@ -349,13 +399,19 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
     }
     __syncwarp();
     real* d = stg + s * K1_STAGE;
-    if (lane == 0) bulk_g2s(d, Q.Phi + e * N3, N3 * (unsigned)sizeof(real), &bar[s]);
-    else if (lane <= 9)
-      bulk_g2s(d + N3 + (lane - 1) * FS, Q.Ja + ((long long)(lane - 1) * Q.Ne + e) * FS, FS * (unsigned)sizeof(real),
-               &bar[s]);
-    else if (SC && lane < 20)
-      bulk_g2s(d + N3 + 9 * FS + (lane - 10) * N3, Q.c10 + (lane - 10) * Q.nn + e * N3, N3 * (unsigned)sizeof(real),
-               &bar[s]);
+    // copies: Phi (unless it goes through registers), 9 Ja, 10 coefficients
+    constexpr int NPHI = PHIR ? 0 : 1;
+    for (int c = lane; c < NPHI + 9 + (SC ? 10 : 0); c += 32) {
+      if (c < NPHI) {
+        bulk_g2s(d, Q.Phi + e * N3, N3 * (unsigned)sizeof(real), &bar[s]);
+      } else if (c < NPHI + 9) {
+        const int f = c - NPHI;
+        bulk_g2s(d + PSZ + f * FS, Q.Ja + ((long long)f * Q.Ne + e) * FS, FS * (unsigned)sizeof(real), &bar[s]);
+      } else {
+        const int f = c - NPHI - 9;
+        bulk_g2s(d + PSZ + 9 * FS + f * N3, Q.c10 + f * Q.nn + e * N3, N3 * (unsigned)sizeof(real), &bar[s]);
+      }
+    }
   };
   // neighbour Phi face traces (384 values; threads 0..383).  The face source
   // (8 * neighbour + neighbour face) of a tile is loaded one iteration before
@@ -371,7 +427,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
   auto emask_at = [&](int2 tl) -> int { return tl.x >= 0 ? prm(tl.x).emask[tl.y] : 0; };
   // pointwise fields of this thread's node
   struct PW {
-    real c[10], Pi, invJ, y, acc, comp;
+    real c[10], Pi, invJ, y, acc, comp, phi;
   };
   auto pw_load = [&](int2 tl, PW& w) {
     if (tl.x < 0) return;
@@ -382,6 +438,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
       for (int c = 0; c < 10; ++c) w.c[c] = Q.c10[c * Q.nn + n];
     }
     w.Pi = Q.Pi[n];
+    if constexpr (PHIR) w.phi = Q.Phi[n];
     w.invJ = Q.invdetJ[n];
     w.y = need_y ? Q.y[n] : (real)0;
     w.acc = need_acc ? Q.acc[n] : (real)0;
@@ -401,6 +458,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
     const real fv = face_load(src_load(t0), t0.x);
     if (tid < 6 * N2) sface[tid] = fv;
     pw_load(t0, cur);
+    if constexpr (PHIR) sphi[tphi] = cur.phi;
     src1 = src_load(t1);
   }
   __syncthreads();
@@ -455,8 +513,8 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
     const K1N8<real>& Q = prm(t0.x);
     const long long e = t0.y;
     const real* d = stg + s * K1_STAGE;
-    const real* sPhi = d;      // unpadded
-    const real* sJa = d + N3;  // 9 padded fields, index (al*3 + c)
+    const real* sPhi = PHIR ? sphi + fb * N3 : d;  // PhiLay
+    const real* sJa = d + PSZ;                      // 9 fields (Lay), index (al*3 + c)
     const real* sfc = sface + fb * 6 * N2;
     const int mask = emcur & 63;
     const int bnd = emcur >> 6;
@@ -474,8 +532,8 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
         double du[2] = {0, 0}, dm[3][2] = {{0, 0}, {0, 0}, {0, 0}};
 #pragma unroll
         for (int kc = 0; kc < 2; ++kc) {
-          const int nd = bnode(al, wt8, kc, gq, tig);
-          const double u = sPhi[unpad(nd)];
+          const int nn = bnode(al, wt8, kc, gq, tig), nd = Lay<real>::at(nn);
+          const double u = sPhi[PhiLay<real>::at(nn)];
           const double a = kc ? aG1 : aG0;
           dmma(du[0], du[1], a, u);
 #pragma unroll
@@ -492,10 +550,11 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
         // the three-term split carries FP32's 24 bits, so only the two-term
         // form takes the operand relative to its pencil value at node PREF
         constexpr bool OFS = NT == 2;
-        const int nd0 = bn(al, wt8, 2 * tig, gq), nd1 = bn(al, wt8, 2 * tig + 1, gq);
-        const float u0 = sPhi[unpad(nd0)], u1 = sPhi[unpad(nd1)];
-        const int ndr = OFS ? bn(al, wt8, PREF, gq) : 0;
-        const float ur = OFS ? sPhi[unpad(ndr)] : 0.f;
+        const int nn0 = bn(al, wt8, 2 * tig, gq), nn1 = bn(al, wt8, 2 * tig + 1, gq);
+        const int nd0 = Lay<real>::at(nn0), nd1 = Lay<real>::at(nn1);
+        const float u0 = sPhi[PhiLay<real>::at(nn0)], u1 = sPhi[PhiLay<real>::at(nn1)];
+        const int nnr = OFS ? bn(al, wt8, PREF, gq) : 0, ndr = Lay<real>::at(nnr);
+        const float ur = OFS ? sPhi[PhiLay<real>::at(nnr)] : 0.f;
         float fu[4] = {0, 0, 0, 0}, fm[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
         mma_split<NT>(fu, aS, aS2, u0 - ur, u1 - ur);
 #pragma unroll
@@ -520,9 +579,9 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
       const bool sat = sface_f >= 0 && ((mask >> sface_f) & 1);
 #pragma unroll
       for (int b = 0; b < 2; ++b) {
-        const int no = onode(al, wt8, b, gq, tig);
+        const int nno = onode(al, wt8, b, gq, tig), no = Lay<real>::at(nno);
         real jump = 0;
-        if (sat) jump = (gq ? inv2H : -inv2H) * (sfc[sface_f * N2 + opq(al, wt8, b, tig)] - sPhi[unpad(no)]);
+        if (sat) jump = (gq ? inv2H : -inv2H) * (sfc[sface_f * N2 + opq(al, wt8, b, tig)] - sPhi[PhiLay<real>::at(nno)]);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
           if ((comps >> c) & 1) {
@@ -544,14 +603,16 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
     // ---- node phase: one node per thread ----
     {
       const long long n = e * N3 + tid;
-      const real u = sPhi[tid];
+      real u;
+      if constexpr (PHIR) u = cur.phi;
+      else u = sPhi[tphi];
       real g0 = (sg[tpad] + sg[3 * FS + tpad]) + sg[6 * FS + tpad];
       real g1 = (sg[FS + tpad] + sg[4 * FS + tpad]) + sg[7 * FS + tpad];
       real g2 = (sg[2 * FS + tpad] + sg[5 * FS + tpad]) + sg[8 * FS + tpad];
       g0 *= cur.invJ; g1 *= cur.invJ; g2 *= cur.invJ;
       real cc[10];
 #pragma unroll
-      for (int c = 0; c < 10; ++c) cc[c] = SC ? d[N3 + 9 * FS + c * N3 + tid] : cur.c[c];
+      for (int c = 0; c < 10; ++c) cc[c] = SC ? d[PSZ + 9 * FS + c * N3 + tid] : cur.c[c];
       const real a = cc[0];
       const real b0 = cc[1], b1 = cc[2], b2 = cc[3];
       const real K0 = cc[4], K1v = cc[5], K2 = cc[6], K3 = cc[7], K4 = cc[8], K5 = cc[9];
@@ -601,7 +662,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
           Q.bbuf[(long long)slot * N2 + p + 8 * q] = dP;
         }
       }
-      {  // flux in the padded element-block layout read by K2
+      {  // flux in the element-block layout (Lay) read by K2
         const long long fo = e * FS + tpad, fstr = Q.Ne * FS;
         Q.F[fo] = F0;
         Q.F[fstr + fo] = F1;
@@ -614,6 +675,8 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
         Q.Phidot[n] = phid;
     }
     if (has_next && tid < 6 * N2) sface[(fb ^ 1) * 6 * N2 + tid] = fnext;
+    if constexpr (PHIR)
+      if (has_next) sphi[(fb ^ 1) * N3 + tphi] = nxt.phi;
     cur = nxt;
     emcur = emnext;
     src1 = src2;
@@ -659,19 +722,23 @@ struct K2N8 {
 // split the fields of pencil tile w & 7, a ring of NSTAGE stages) or 256
 // threads (two nodes per thread, each warp does both halves of its tile, one
 // stage whose next copy is issued as soon as the contraction pass has read
-// it) -- the 256-thread shape fits two CTAs on an SM for FP64.
+// it) -- the 256-thread shape fits two CTAs on an SM for FP64.  Partial
+// divergences: one field per (axis, half) in the 512-thread shape; one per axis
+// in the 256-thread shape, whose threads add the two halves in registers.
 constexpr int K2_NF = 12;
-constexpr size_t K2_STAGE = (size_t)K2_NF * n8::FS;
 template <typename real>
 struct K2Shape {
   static constexpr int THR = std::is_same<real, double>::value ? 256 : 512;
   static constexpr int NS = THR == 512 ? n8::NSTAGE : 1;          // stages
   static constexpr int OCC = std::is_same<real, double>::value ? 2 : n8::Occ<real>::k2;
+  static constexpr int NSD = THR == 512 ? 6 : 3;                  // partial-divergence fields
+  static constexpr size_t STAGE = (size_t)K2_NF * n8::Lay<real>::FS;
 };
 template <typename real>
 constexpr size_t k2_smem() {
-  return (K2Shape<real>::NS * K2_STAGE + 6 * n8::FS + 2 * 6 * 3 * n8::N2) * sizeof(real) + n8::N2 * sizeof(double) +
-         64;
+  return (K2Shape<real>::NS * K2Shape<real>::STAGE + K2Shape<real>::NSD * n8::Lay<real>::FS + 2 * 6 * 3 * n8::N2) *
+             sizeof(real) +
+         n8::N2 * sizeof(double) + 64;
 }
 
 template <typename real, int NT, bool BATCH>
@@ -685,11 +752,13 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
   constexpr int NFACE = 6 * 3 * N2;             // 1152 neighbour face values
   constexpr int NFR = (NFACE + THR - 1) / THR;  // face values per thread
   constexpr int NHALF = THR == 512 ? 1 : 2;     // halves of its tile a warp does
+  constexpr int FS = Lay<real>::FS, NSD = K2Shape<real>::NSD;
+  constexpr size_t K2_STAGE = K2Shape<real>::STAGE;
   extern __shared__ __align__(128) unsigned char smraw[];
   double* sG = reinterpret_cast<double*>(smraw);                   // 64
   real* stg = reinterpret_cast<real*>(sG + N2);
-  real* sdiv = stg + NS * K2_STAGE;                                // 6 padded partial divergences [al*2 + half]
-  real* sface = sdiv + 6 * FS;                                     // 2 x 6 x 3 x 64
+  real* sdiv = stg + NS * K2_STAGE;                                // NSD partial divergences (Lay)
+  real* sface = sdiv + NSD * FS;                                   // 2 x 6 x 3 x 64
   uint64_t* bar = reinterpret_cast<uint64_t*>(sface + 2 * NFACE);
   __shared__ int abort_flag;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -755,7 +824,7 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
         const int fn = src[r] & 7;
         const real* Fc = c == 0 ? Q.F0 : c == 1 ? Q.F1 : Q.F2;
         const int fnode = face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N);
-        v = Fc[(long long)(src[r] >> 3) * FS + pad(fnode & 7, (fnode >> 3) & 7, fnode >> 6)];
+        v = Fc[(long long)(src[r] >> 3) * FS + Lay<real>::at(fnode)];
       }
       fv[r] = v;
     }
@@ -854,21 +923,23 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
     const real* sfc = sface + fb * NFACE;
     const int mask = emcur & 63;
     const int bnd = emcur >> 6;
-    // per-axis partial divergences sdiv[al*2 + half]: no barrier between axes
+    // per-axis partial divergences (sdiv[al*2 + half], or sdiv[al] with the two
+    // halves added in registers): no barrier between axes
 #pragma unroll
-    for (int hh = 0; hh < NHALF; ++hh) {
-      const int half = THR == 512 ? (warp >> 3) : hh;
+    for (int al = 0; al < 3; ++al) {
+      const real* m0 = sJa + (al * 3 + 0) * FS;
+      const real* m1 = sJa + (al * 3 + 1) * FS;
+      const real* m2 = sJa + (al * 3 + 2) * FS;
+      real rsum[2] = {0, 0};
 #pragma unroll
-      for (int al = 0; al < 3; ++al) {
-        const real* m0 = sJa + (al * 3 + 0) * FS;
-        const real* m1 = sJa + (al * 3 + 1) * FS;
-        const real* m2 = sJa + (al * 3 + 2) * FS;
+      for (int hh = 0; hh < NHALF; ++hh) {
+        const int half = THR == 512 ? (warp >> 3) : hh;
         real cx[2], cy[2];
         if constexpr (F64) {
           double dx[2] = {0, 0}, dy[2] = {0, 0};
 #pragma unroll
           for (int kc = 0; kc < 2; ++kc) {
-            const int nd = bnode(al, wt8, kc, gq, tig);
+            const int nd = Lay<real>::at(bnode(al, wt8, kc, gq, tig));
             const double a = kc ? aG1 : aG0;
             if (half == 0) {
               // contravariant flux Ja^al . F and F_0
@@ -885,7 +956,8 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
         } else {
           constexpr bool OFS = NT == 2;  // operand offset only for the two-term split (see K1)
           constexpr int NQ = OFS ? 3 : 2;
-          const int nd[3] = {bn(al, wt8, 2 * tig, gq), bn(al, wt8, 2 * tig + 1, gq), bn(al, wt8, PREF, gq)};
+          const int nd[3] = {Lay<real>::at(bn(al, wt8, 2 * tig, gq)), Lay<real>::at(bn(al, wt8, 2 * tig + 1, gq)),
+                             Lay<real>::at(bn(al, wt8, PREF, gq))};
           float vx[3] = {0, 0, 0}, vy[3] = {0, 0, 0};
 #pragma unroll
           for (int q = 0; q < NQ; ++q) {
@@ -909,7 +981,7 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
         const bool sat = half == 1 && sface_f >= 0 && ((mask >> sface_f) & 1);
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
-          const int no = onode(al, wt8, b, gq, tig);
+          const int no = Lay<real>::at(onode(al, wt8, b, gq, tig));
           real r;
           if (half == 0) {
             r = (real)0.5 * cx[b] + (real)0.5 * m0[no] * cy[b];
@@ -923,8 +995,13 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
                               m2[no] * (sfc[(sface_f * 3 + 2) * N2 + pq] - sF[2 * FS + no]);
             r += (gq ? inv2H : -inv2H) * sacc;
           }
-          sdiv[(al * 2 + half) * FS + no] = r;
+          if constexpr (NHALF == 2) rsum[b] = hh ? rsum[b] + r : r;
+          else sdiv[(al * 2 + half) * FS + no] = r;
         }
+      }
+      if constexpr (NHALF == 2) {
+#pragma unroll
+        for (int b = 0; b < 2; ++b) sdiv[al * FS + Lay<real>::at(onode(al, wt8, b, gq, tig))] = rsum[b];
       }
     }
     __syncthreads();
@@ -936,10 +1013,14 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
     for (int r = 0; r < NPT; ++r) {
       const int node = tid + r * THR;
       const int ti = node & 7, tj = (node >> 3) & 7, tk = node >> 6;
-      const int tpad = pad(ti, tj, tk);
+      const int tpad = Lay<real>::at(node);
       const long long n = e * N3 + node;
-      real dv = ((sdiv[tpad] + sdiv[2 * FS + tpad]) + sdiv[4 * FS + tpad]) +
-                ((sdiv[FS + tpad] + sdiv[3 * FS + tpad]) + sdiv[5 * FS + tpad]);
+      real dv;
+      if constexpr (NSD == 3)
+        dv = (sdiv[tpad] + sdiv[FS + tpad]) + sdiv[2 * FS + tpad];
+      else
+        dv = ((sdiv[tpad] + sdiv[2 * FS + tpad]) + sdiv[4 * FS + tpad]) +
+             ((sdiv[FS + tpad] + sdiv[3 * FS + tpad]) + sdiv[5 * FS + tpad]);
       dv *= cur[r].invJ;
       if (bnd && Q.bc_on) {
         const int idx3[3] = {ti, tj, tk};
@@ -984,7 +1065,7 @@ __global__ void k_pad_fields(long long Ne, int nf, const real* __restrict__ src,
     const long long r = x - f * Ne * n8::N3;
     const long long e = r / n8::N3;
     const int t = (int)(r - e * n8::N3);
-    dst[(f * Ne + e) * n8::FS + n8::pad(t & 7, (t >> 3) & 7, t >> 6)] = src[x];
+    dst[(f * Ne + e) * n8::Lay<real>::FS + n8::Lay<real>::at(t)] = src[x];
   }
 }
 
@@ -996,6 +1077,8 @@ int launch_pad_metric_n8(DevMesh& m, cudaStream_t s) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+// words per field of the element-block layouts (the larger, FP32, one: an
+// allocation of this size serves both precisions)
 long long n8_padded_field_size(long long Ne) { return Ne * n8::FS; }
 
 static int sm_count() {
@@ -1033,7 +1116,8 @@ static K2N8<real> k2n8_params(const DevMesh& m, const void* F, void* Pidot, cons
                               const RKStage& rk, unsigned* flag) {
   K2N8<real> P;
   P.Ne = m.Ne; P.nn = m.nn;
-  P.F0 = (const real*)F; P.F1 = (const real*)F + m.Ne * n8::FS; P.F2 = (const real*)F + 2 * m.Ne * n8::FS;
+  const long long fs = m.Ne * n8::Lay<real>::FS;
+  P.F0 = (const real*)F; P.F1 = (const real*)F + fs; P.F2 = (const real*)F + 2 * fs;
   P.Ja = (const real*)m.Ja_n8; P.invdetJ = (const real*)m.invdetJ_r;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
   P.emask = m.emask; P.fsrc = m.fsrc;
