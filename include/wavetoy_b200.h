@@ -283,12 +283,20 @@ int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int n
                      const double bdry_values[6], double tau, double sommerfeld_R, double eps_ko);
 /* End-to-end evolve with host buffers, the shape of evolve3d(formulation =
  * :conservative) (src/evolve.jl:1149-1366): upload Phi/Pi, then nsamples times
- * run steps_per_sample RK4 steps and copy the state back into
- * Phi_hist/Pi_hist[s] (host, nsamples*nn each, may be NULL) and the energy
- * into energy[s] (may be NULL).  Phi_host/Pi_host receive the final state. */
+ * run steps_per_sample RK4 steps, copy the state back into Phi_host/Pi_host
+ * and the energy into energy[s] (may be NULL).  Phi_host/Pi_host hold the
+ * final state on return.  Each sample is copied device to device into a
+ * staging pair and from there to the host on a second stream, so the copy
+ * overlaps the next sample's steps (page-locked host buffers make it
+ * asynchronous); four state-sized device buffers are allocated per call. */
 int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* Phi_host, double* Pi_host,
                           double dt, int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc,
                           int use_metric, double* energy);
+/* The same for an FP32 mesh with FP32 host buffers (no reference counterpart:
+ * the reference's evolve3d keeps Float64 host arrays). */
+int wt_evolve_curved_host_f32(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, float* Phi_host, float* Pi_host,
+                              double dt, int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc,
+                              int use_metric, double* energy);
 
 /* Device-side diagnostics in place of evolve3d's per-sample host copies of the
  * whole state (src/evolve.jl:1339-1358): wt_gather_nodes copies the values of

@@ -294,6 +294,39 @@ def test_evolve_host_matches_device_stepping(wt, ctx, O):
     assert E[-1] <= E[0] * (1 + 1e-6)
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_evolve_host_pinned_equals_device_stepping(wt, ctx, prec):
+    """Page-locked host buffers (copies overlapped with the next sample) give the
+    state and energies of device stepping bit for bit, in both precisions; a
+    host buffer of the wrong dtype is rejected."""
+    import torch
+    g = wt.Mesh.uniform_hex(ctx, 8, 2, outer_tag=7, warp_A=0.05, precision=prec)
+    p = wt.workloads.adm_params(7)
+    c = wt.sample_background3d(g, wt.BG_ADM_PERTURBED, p)
+    dt = 0.2 * g.min_spacing() / wt.workloads.max_speed(p)
+    Phi, Pi = g.zeros(), g.zeros()
+    cc, a, w = wt.workloads.pulses(7, 2)
+    wt.initial_data(g, wt.IC_GAUSSIANS, wt.gaussian_params(cc, a, w), Phi)
+    bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+    hdt = torch.float64 if prec == 0 else torch.float32
+    Ph = torch.empty(g.nn, dtype=hdt, pin_memory=True)
+    Qh = torch.empty(g.nn, dtype=hdt, pin_memory=True)
+    Ph.copy_(Phi.cpu())
+    Qh.copy_(Pi.cpu())
+    E = np.zeros(4)
+    wt.evolve_curved_host(Ph, Qh, c, wt.make_wave3d_workspace(g), dt, 2, 4, bc3d=bc, metric=True, energy=E)
+    ws = wt.make_wave3d_workspace(g)
+    Ed = []
+    for _ in range(4):
+        wt.step_rk4_curved(Phi, Pi, c, ws, dt, 2, bc3d=bc, metric=True)
+        Ed.append(wt.wave3d_energy(Phi, Pi, c, ws, metric=True))
+    assert torch.equal(Ph, Phi.cpu()) and torch.equal(Qh, Pi.cpu())
+    assert np.array_equal(E, np.array(Ed))
+    bad = torch.empty(g.nn, dtype=torch.float32 if prec == 0 else torch.float64)
+    with pytest.raises(wt.WaveToyError):
+        wt.evolve_curved_host(bad, bad, c, ws, dt, 1, 1, bc3d=bc, metric=True)
+
+
 def test_fp32_form_rhs(wt, ctx, O):
     import torch
     g, o = pair(wt, ctx, O, 8, 2, A=0.05, outer_tag=7, precision=1)

@@ -1237,36 +1237,86 @@ int wt_snapshot_load(wt_ctx* ctx, wt_mesh* mesh, void* Phi, void* Pi, double* t,
   return rc;
 }
 
-int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* Phi_host, double* Pi_host, double dt,
-                          int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc, int use_metric,
-                          double* energy) {
+}  // extern "C"
+
+// host-buffer evolve for state words of `prec` (the mesh precision)
+static int evolve_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi_host, void* Pi_host, int prec,
+                       const char* name, double dt, int steps_per_sample, int nsamples, double eps_ko,
+                       const wt_bc_desc* bc, int use_metric, double* energy) {
   WT_TRY(check_ws(ctx, ws));
-  if (!coef || !Phi_host || !Pi_host) return fail(ctx, WT_EINVAL, "wt_evolve_curved_host: NULL argument");
-  if (ws->mesh->m.precision != WT_F64)
-    return fail(ctx, WT_ENOTSUP, "wt_evolve_curved_host takes FP64 host buffers; use an FP64 mesh");
+  if (!coef || !Phi_host || !Pi_host) return fail(ctx, WT_EINVAL, std::string(name) + ": NULL argument");
+  if (ws->mesh->m.precision != prec)
+    return fail(ctx, WT_ENOTSUP,
+                std::string(name) + (prec == WT_F64 ? " takes FP64 host buffers; use an FP64 mesh"
+                                                    : " takes FP32 host buffers; use an FP32 mesh"));
   if (steps_per_sample < 1 || nsamples < 1) return fail(ctx, WT_EINVAL, "steps_per_sample, nsamples must be >= 1");
   const wt::DevMesh& m = ws->mesh->m;
-  const size_t nb = (size_t)m.nn * sizeof(double);
-  void *dP = nullptr, *dQ = nullptr;
-  WT_TRY(dalloc(ctx, &dP, nb, nullptr));
-  if (dalloc(ctx, &dQ, nb, nullptr)) { cudaFree(dP); return WT_ENOMEM; }
+  const size_t nb = (size_t)m.nn * rsize(prec);
+  // device state (dP, dQ) and a staging copy of the last sample (sP, sQ): each
+  // sample is copied device to device on the compute stream and from the
+  // staging pair to the host on a second stream, so the device-to-host copy of
+  // sample s overlaps the steps of sample s + 1
+  void* buf[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (void*& p : buf)
+    if (dalloc(ctx, &p, nb, nullptr)) {
+      for (void* q : buf) cudaFree(q);
+      return WT_ENOMEM;
+    }
+  void *dP = buf[0], *dQ = buf[1], *sP = buf[2], *sQ = buf[3];
+  cudaStream_t cs = nullptr;
+  cudaEvent_t staged = nullptr, copied = nullptr;
   int rc = 0;
-  cudaMemcpyAsync(dP, Phi_host, nb, cudaMemcpyHostToDevice, ctx->stream);
-  cudaMemcpyAsync(dQ, Pi_host, nb, cudaMemcpyHostToDevice, ctx->stream);
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&staged, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&copied, cudaEventDisableTiming) != cudaSuccess)
+    rc = fail(ctx, WT_ECUDA, std::string(name) + ": stream or event creation failed");
+  if (!rc) {
+    cudaMemcpyAsync(dP, Phi_host, nb, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(dQ, Pi_host, nb, cudaMemcpyHostToDevice, ctx->stream);
+  }
   for (int sidx = 0; sidx < nsamples && !rc; ++sidx) {
     rc = wt_step_rk4_curved(ctx, ws, coef, dP, dQ, dt, steps_per_sample, eps_ko, bc, use_metric);
     if (rc) break;
-    cudaMemcpyAsync(Phi_host, dP, nb, cudaMemcpyDeviceToHost, ctx->stream);
-    cudaMemcpyAsync(Pi_host, dQ, nb, cudaMemcpyDeviceToHost, ctx->stream);
     if (energy) rc = wt_energy(ctx, ws, coef, dP, dQ, use_metric, &energy[sidx]);
     int bad = 0;
     if (!rc) rc = wt_ctx_nonfinite(ctx, &bad);
     if (!rc && bad) rc = fail(ctx, WT_ENONFINITE, "state became non-finite during evolution");
+    if (rc) break;
+    if (sidx > 0) cudaStreamWaitEvent(ctx->stream, copied, 0);  // the previous sample has left the staging pair
+    cudaMemcpyAsync(sP, dP, nb, cudaMemcpyDeviceToDevice, ctx->stream);
+    cudaMemcpyAsync(sQ, dQ, nb, cudaMemcpyDeviceToDevice, ctx->stream);
+    cudaEventRecord(staged, ctx->stream);
+    cudaStreamWaitEvent(cs, staged, 0);
+    cudaMemcpyAsync(Phi_host, sP, nb, cudaMemcpyDeviceToHost, cs);
+    cudaMemcpyAsync(Pi_host, sQ, nb, cudaMemcpyDeviceToHost, cs);
+    cudaEventRecord(copied, cs);
+  }
+  if (cs) {
+    cudaError_t e = cudaStreamSynchronize(cs);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, name);
   }
   cudaStreamSynchronize(ctx->stream);
-  cudaFree(dP);
-  cudaFree(dQ);
+  if (staged) cudaEventDestroy(staged);
+  if (copied) cudaEventDestroy(copied);
+  if (cs) cudaStreamDestroy(cs);
+  for (void* p : buf) cudaFree(p);
   return rc;
+}
+
+extern "C" {
+
+int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* Phi_host, double* Pi_host, double dt,
+                          int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc, int use_metric,
+                          double* energy) {
+  return evolve_host(ctx, ws, coef, Phi_host, Pi_host, WT_F64, "wt_evolve_curved_host", dt, steps_per_sample,
+                     nsamples, eps_ko, bc, use_metric, energy);
+}
+
+int wt_evolve_curved_host_f32(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, float* Phi_host, float* Pi_host, double dt,
+                              int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc, int use_metric,
+                              double* energy) {
+  return evolve_host(ctx, ws, coef, Phi_host, Pi_host, WT_F32, "wt_evolve_curved_host_f32", dt, steps_per_sample,
+                     nsamples, eps_ko, bc, use_metric, energy);
 }
 
 }  // extern "C"

@@ -109,6 +109,7 @@ def library():
         "wt_step_rk4_curved": [vp, vp, vp, vp, vp, d, i, d, C.POINTER(_BcDesc), i],
         "wt_step_rk4_sipg": [vp, vp, vp, vp, d, i, C.POINTER(C.c_double * 6), d, d, d],
         "wt_evolve_curved_host": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i, vp],
+        "wt_evolve_curved_host_f32": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i, vp],
         "wt_initial_data": [vp, vp, i, vp, i, d, vp, vp],
         "wt_gll_operators": [i, vp, vp, vp],
         "wt_ctx_profile": [vp, i], "wt_ctx_profile_read": [vp, C.POINTER(d * 2), C.POINTER(ll * 2)],
@@ -781,23 +782,31 @@ def evolve_curved_host(Phi_host, Pi_host, coef: Coef, ws: Workspace, dt: float, 
                        energy=None):
     """Host-buffer evolve in the shape of evolve3d(formulation = :conservative) (src/evolve.jl:1149-1366).
 
-    Phi_host / Pi_host: float64 numpy arrays (pinned torch CPU tensors also
-    work); they receive the final state.  energy: float64 array of length
-    nsamples or None."""
+    Phi_host / Pi_host: C-contiguous host arrays in the mesh precision (float64
+    numpy arrays or CPU torch tensors; page-locked torch tensors let the
+    per-sample copies overlap the next sample's steps); they receive the final
+    state.  energy: float64 array of length nsamples or None."""
     import numpy as np
 
-    def addr(a):
+    f32 = ws.mesh.precision == WT_F32
+
+    def addr(a, want):
         if a is None:
             return None
         if hasattr(a, "data_ptr"):
+            import torch
+            if a.device.type != "cpu" or not a.is_contiguous() or a.dtype != getattr(torch, want):
+                raise WaveToyError(-1, f"evolve_curved_host: expected a contiguous CPU {want} tensor")
             return C.c_void_p(a.data_ptr())
-        assert a.dtype == np.float64 and a.flags.c_contiguous
+        if a.dtype != np.dtype(want) or not a.flags.c_contiguous:
+            raise WaveToyError(-1, f"evolve_curved_host: expected a C-contiguous {want} array")
         return C.c_void_p(a.ctypes.data)
 
+    sw = "float32" if f32 else "float64"
+    fn = library().wt_evolve_curved_host_f32 if f32 else library().wt_evolve_curved_host
     p, keep = _bcptr(bc3d)
-    ws.ctx.check(library().wt_evolve_curved_host(ws.ctx.h, ws.h, coef.h, addr(Phi_host), addr(Pi_host), float(dt),
-                                                 int(steps_per_sample), int(nsamples), float(eps_KO), p, int(metric),
-                                                 addr(energy)), "evolve_curved_host")
+    ws.ctx.check(fn(ws.ctx.h, ws.h, coef.h, addr(Phi_host, sw), addr(Pi_host, sw), float(dt), int(steps_per_sample),
+                    int(nsamples), float(eps_KO), p, int(metric), addr(energy, "float64")), "evolve_curved_host")
 
 
 def initial_data(mesh: Mesh, kind: int, params: Sequence[float], u, ut=None, t: float = 0.0):
