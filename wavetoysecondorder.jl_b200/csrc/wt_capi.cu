@@ -678,7 +678,15 @@ int wt_mesh_set_fp32_form(wt_mesh* mh, int form) {
   if (!mh) return WT_EINVAL;
   if (form != WT_FP32_CUDA_CORES && form != WT_FP32_BF16X3 && form != WT_FP32_BF16X2)
     return fail(mh->ctx, WT_EINVAL, "unknown FP32 form " + std::to_string(form));
-  mh->m.fp32_form = form;
+  wt::DevMesh& m = mh->m;
+  m.fp32_form = form;
+  // the FP32 CUDA-core n = 8 kernels read the metric terms in their own layout
+  const int want = m.precision == WT_F32 && form == WT_FP32_CUDA_CORES ? 1 : 0;
+  if (m.N == 8 && m.Ja_n8 && m.ja_n8_layout != want) {
+    WT_TRY(lrc(mh->ctx, wt::launch_pad_metric_n8(m, mh->ctx->stream), "n = 8 metric layout"));
+    cudaError_t e = cudaStreamSynchronize(mh->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(mh->ctx, e, "wt_mesh_set_fp32_form");
+  }
   return 0;
 }
 

@@ -726,7 +726,6 @@ static inline bool a16(const void* p) { return p == nullptr || ((uintptr_t)p & 1
 bool cons_n8_path(const DevMesh& m, const DevCoef& c, int use_metric, const ConsBC& bc, const RKStage& rkP,
                   const RKStage& rkQ, std::initializer_list<const void*> ptrs) {
   if (m.N != 8 || !use_metric || m.Ja_n8 == nullptr) return false;
-  if (m.precision == 1 && m.fp32_form == 0) return false;  // FP32 on CUDA cores: the generic kernels
   if (c.c10 == nullptr) return false;
   if (bc.on && !bc.curv) return false;
   for (const RKStage* rk : {&rkP, &rkQ})

@@ -317,7 +317,60 @@ struct K1N8 {
   real* out;
   real* comp;
   unsigned* flag;
+  float Gf[64];  // the operator in FP32 (the CUDA-core form reads it from the constant bank)
 };
+
+// Boundary terms of K1 at a node on an outer face (the curvilinear boundary
+// pass of src/boundaries3d.jl:131-232): characteristic SAT into phid and the
+// Pi boundary contribution into bbuf (read by K2).  cc: the ten coefficients.
+template <typename real>
+__device__ __forceinline__ void k1_boundary(const K1N8<real>& Q, long long e, int ti, int tj, int tk, long long n,
+                                            real u, real Pi, real g0, real g1, real g2, const real cc[10],
+                                            real& phid) {
+  using n8::N2;
+  const real a = cc[0];
+  const real b0 = cc[1], b1 = cc[2], b2 = cc[3];
+  const real K0 = cc[4], K1v = cc[5], K2 = cc[6], K3 = cc[7], K4 = cc[8], K5 = cc[9];
+  const int idx3[3] = {ti, tj, tk};
+  for (int f = 0; f < 6; ++f) {
+    const int tag = Q.bdry[f + 6 * e];
+    if (tag == 0) continue;
+    const int ax = f >> 1;
+    if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
+    const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
+    const int slot = Q.bslot[f + 6 * e];
+    real dF = 0, dP = 0;
+    if (tag != Q.exc_tag) {
+      const long long nb = (long long)Q.nbf * N2;
+      const long long bi = (long long)slot * N2 + p + 8 * q;
+      const real nx = Q.bnorm[bi], ny = Q.bnorm[nb + bi], nz = Q.bnorm[2 * nb + bi], wt = Q.bnorm[3 * nb + bi];
+      const real Kn =
+          K0 * nx * nx + K3 * ny * ny + K5 * nz * nz + (real)2 * (K1v * nx * ny + K2 * nx * nz + K4 * ny * nz);
+      const real a_n = sqrt(a * Kn);
+      const real bn_ = b0 * nx + b1 * ny + b2 * nz;
+      const real sigma = (real)Q.sigma;
+      if (Q.kind == 4) {
+        const real tau = sigma * (fabs(a_n - bn_) + fabs(a_n + bn_)) * wt;
+        const real gp = Q.gPhi ? Q.gPhi[n] : (real)0, gqv = Q.gPi ? Q.gPi[n] : (real)0;
+        dF = -tau * (u - gp);
+        dP = -tau * (Pi - gqv);
+      } else {
+        const real qv = nx * g0 + ny * g1 + nz * g2;
+        const real rr = Pi + ((bn_ + a_n) / a) * qv;
+        real gv = 0;
+        if (Q.kind != 2) {
+          const real gqv = Q.gPi ? Q.gPi[n] : (real)0;
+          const real gx = Q.gDx ? Q.gDx[n] : (real)0, gy = Q.gDy ? Q.gDy[n] : (real)0,
+                     gz = Q.gDz ? Q.gDz[n] : (real)0;
+          gv = gqv + ((bn_ + a_n) / a) * (nx * gx + ny * gy + nz * gz);
+        }
+        dP = -sigma * fabs(a_n + bn_) * wt * (rr - gv);
+      }
+    }
+    phid += dF;
+    Q.bbuf[(long long)slot * N2 + p + 8 * q] = dP;
+  }
+}
 
 // K1 staged fields: Phi (PhiLay), Ja (9 fields in the Lay layout, one block
 // each from the global copy) and the ten coefficient fields (unpadded, read in
@@ -621,47 +674,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
       const real F1 = b1 * Pi + (K1v * g0 + K3 * g1 + K4 * g2);
       const real F2 = b2 * Pi + (K2 * g0 + K4 * g1 + K5 * g2);
       real phid = b0 * g0 + b1 * g1 + b2 * g2 + a * Pi;
-      if (bnd && Q.bc_on) {
-        const int idx3[3] = {ti, tj, tk};
-        for (int f = 0; f < 6; ++f) {
-          const int tag = Q.bdry[f + 6 * e];
-          if (tag == 0) continue;
-          const int ax = f >> 1;
-          if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
-          const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
-          const int slot = Q.bslot[f + 6 * e];
-          real dF = 0, dP = 0;
-          if (tag != Q.exc_tag) {
-            const long long nb = (long long)Q.nbf * N2;
-            const long long bi = (long long)slot * N2 + p + 8 * q;
-            const real nx = Q.bnorm[bi], ny = Q.bnorm[nb + bi], nz = Q.bnorm[2 * nb + bi], wt = Q.bnorm[3 * nb + bi];
-            const real Kn =
-                K0 * nx * nx + K3 * ny * ny + K5 * nz * nz + (real)2 * (K1v * nx * ny + K2 * nx * nz + K4 * ny * nz);
-            const real a_n = sqrt(a * Kn);
-            const real bn_ = b0 * nx + b1 * ny + b2 * nz;
-            const real sigma = (real)Q.sigma;
-            if (Q.kind == 4) {
-              const real tau = sigma * (fabs(a_n - bn_) + fabs(a_n + bn_)) * wt;
-              const real gp = Q.gPhi ? Q.gPhi[n] : (real)0, gqv = Q.gPi ? Q.gPi[n] : (real)0;
-              dF = -tau * (u - gp);
-              dP = -tau * (Pi - gqv);
-            } else {
-              const real qv = nx * g0 + ny * g1 + nz * g2;
-              const real rr = Pi + ((bn_ + a_n) / a) * qv;
-              real gv = 0;
-              if (Q.kind != 2) {
-                const real gqv = Q.gPi ? Q.gPi[n] : (real)0;
-                const real gx = Q.gDx ? Q.gDx[n] : (real)0, gy = Q.gDy ? Q.gDy[n] : (real)0,
-                           gz = Q.gDz ? Q.gDz[n] : (real)0;
-                gv = gqv + ((bn_ + a_n) / a) * (nx * gx + ny * gy + nz * gz);
-              }
-              dP = -sigma * fabs(a_n + bn_) * wt * (rr - gv);
-            }
-          }
-          phid += dF;
-          Q.bbuf[(long long)slot * N2 + p + 8 * q] = dP;
-        }
-      }
+      if (bnd && Q.bc_on) k1_boundary<real>(Q, e, ti, tj, tk, n, u, Pi, g0, g1, g2, cc, phid);
       {  // flux in the element-block layout (Lay) read by K2
         const long long fo = e * FS + tpad, fstr = Q.Ne * FS;
         Q.F[fo] = F0;
@@ -715,6 +728,7 @@ struct K2N8 {
   real* out;
   real* comp;
   unsigned* flag;
+  float Gf[64];
 };
 
 // K2 staged fields: 0..2 F, 3..11 Ja.  Register prefetch: invJ, y, acc, comp.
@@ -1056,8 +1070,532 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 CUDA-core form (WT_FP32_CUDA_CORES) of the two n = 8 kernels: one
+// thread per (axis, pencil) -- 3 x 64 = 192 threads -- does the 8x8
+// contractions of its pencil as FFMAs whose operator entries come from the
+// kernel's constant bank (the parameter block).  Exact FP32 arithmetic with
+// about a quarter of the instructions of the split-BF16 form.  The staging,
+// tables, face traces, prefetch and bounded waits are those of the kernels
+// above; element blocks use the LayC layout.
+namespace n8 {
+// Element-block layout of the FP32 CUDA-core form: the node index with bits
+// 0-4 XOR-ed by bits 5-7 (bit0 ^= b6, bit1 ^= b7, bit2 ^= b5, bit3 ^= b6,
+// bit4 ^= b7), so that a warp reading one node of each of 32 pencils along any
+// axis, or 32 nodes in order, touches 32 distinct banks.
+struct LayC {
+  static constexpr int FS = 512;
+  __host__ __device__ __forceinline__ static int at(int n) {
+    const int j2 = (n >> 5) & 1, k0 = (n >> 6) & 1, k1 = (n >> 7) & 1;
+    return n ^ ((k0 * 9) ^ (k1 * 18) ^ (j2 * 4));
+  }
+};
+constexpr int CTHR = 192;
+// per-thread 4-byte asynchronous copy global -> shared (zero-filled when !valid)
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// node at position pos of pencil pc along axis al; pc = a + 8 b numbers the
+// other two axes in increasing order, so it is also the pencil's face index
+__device__ __forceinline__ int pnode(int al, int pc, int pos) {
+  const int a = pc & 7, b = pc >> 3;
+  return al == 0 ? pos + 8 * a + 64 * b : al == 1 ? a + 8 * pos + 64 * b : a + 8 * b + 64 * pos;
+}
+// out[l] = sum_m G[l][m] v[m]
+__device__ __forceinline__ void contract8(const float* G, const float v[8], float out[8]) {
+#pragma unroll
+  for (int l = 0; l < 8; ++l) {
+    float acc = G[l * 8] * v[0];
+#pragma unroll
+    for (int m = 1; m < 8; ++m) acc = fmaf(G[l * 8 + m], v[m], acc);
+    out[l] = acc;
+  }
+}
+}  // namespace n8
+
+constexpr size_t K1C_STAGE = 9 * (size_t)n8::LayC::FS + 10 * (size_t)n8::N3;  // Ja (LayC), ten coefficients
+constexpr size_t K2C_STAGE = (size_t)K2_NF * n8::LayC::FS;
+constexpr int K1C_OCC = 2, K2C_OCC = 3;
+constexpr size_t k1c_smem() {
+  return (n8::NSTAGE * K1C_STAGE + 9 * n8::LayC::FS + 2 * 6 * n8::N2 + 2 * n8::N3) * sizeof(float) + 64;
+}
+constexpr size_t k2c_smem() {
+  return (n8::NSTAGE * K2C_STAGE + 3 * n8::LayC::FS + 2 * 6 * 3 * n8::N2) * sizeof(float) + 64;
+}
+
+template <bool BATCH>
+__global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
+    k_cons_k1_n8c(const __grid_constant__ K1N8<float> P, const K1N8<float>* __restrict__ plist,
+                  const int2* __restrict__ tiles, long long ntiles) {
+  using namespace n8;
+  using real = float;
+  constexpr int THR = CTHR, NS = NSTAGE, FSC = LayC::FS;
+  constexpr int NPT = (N3 + THR - 1) / THR;  // node slots per thread (3, the last one partly)
+  constexpr int NFT = 6 * N2;                // 384 neighbour Phi face values
+  constexpr int NFR = (NFT + THR - 1) / THR;  // 2 per thread
+  extern __shared__ __align__(128) unsigned char smraw[];
+  real* stg = reinterpret_cast<real*>(smraw);  // NS stages
+  real* sg = stg + NS * K1C_STAGE;             // 9 partial gradients [al*3 + c] (LayC)
+  real* sface = sg + 9 * FSC;                  // 2 x 384
+  real* sphi = sface + 2 * NFT;                // 2 x 512 (LayC)
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sphi + 2 * N3);
+  __shared__ int abort_flag;
+  __shared__ int ftab[6 * N2];  // node of face-trace point pq on face fn of an element block
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int al = tid >> 6, pc = tid & 63;  // contraction: axis (warp-uniform) and pencil
+  const real inv2H = (real)(1.0 / (2.0 * P.H[0]));
+  const bool comp_on = P.epi && P.comp != nullptr;
+  const bool need_y = P.epi && (P.stage == 1 || P.stage == 2 || (comp_on && P.stage == 3));
+  const bool need_acc = P.epi && P.stage >= 1;
+  const bool need_comp = comp_on && P.stage == 3;
+  const unsigned tx_bytes = (unsigned)(K1C_STAGE * sizeof(real));
+  const long long T = BATCH ? ntiles : P.Ne;
+  const long long GS = gridDim.x;
+  auto tile_at = [&](long long t) -> int2 {
+    if (t >= T) return make_int2(-1, -1);
+    if constexpr (BATCH) return tiles[t];
+    else return make_int2(0, (int)t);
+  };
+  auto prm = [&](int sidx) -> const K1N8<real>& {
+    if constexpr (BATCH) return plist[sidx];
+    else return P;
+  };
+  int addr[8];
+#pragma unroll
+  for (int pos = 0; pos < 8; ++pos) addr[pos] = LayC::at(pnode(al, pc, pos));
+
+  for (int i = tid; i < 6 * N2; i += THR)
+    ftab[i] = face_node(faxis(i >> 6), frow(i >> 6, N), i & 7, (i >> 3) & 7, N);
+  if (tid == 0) {
+    abort_flag = 0;
+    for (int k = 0; k < NS; ++k) mbar_init(&bar[k], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  // warp 0 stages tile tl into stage s: 9 Ja blocks, 10 coefficient blocks
+  auto issue = [&](int2 tl, int s) {
+    const K1N8<real>& Q = prm(tl.x);
+    const long long e = tl.y;
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&bar[s], tx_bytes);
+    }
+    __syncwarp();
+    real* d = stg + s * K1C_STAGE;
+    if (lane < 9)
+      bulk_g2s(d + lane * FSC, Q.Ja + ((long long)lane * Q.Ne + e) * FSC, FSC * (unsigned)sizeof(real), &bar[s]);
+    else if (lane < 19)
+      bulk_g2s(d + 9 * FSC + (lane - 9) * N3, Q.c10 + (lane - 9) * Q.nn + e * N3, N3 * (unsigned)sizeof(real),
+               &bar[s]);
+  };
+  // face-trace slot r of this thread: value tid + r * THR = (face, pq) of the 384
+  auto src_load = [&](int2 tl, int src[NFR]) {
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = tid + r * THR;
+      src[r] = (tl.x >= 0 && idx < NFT) ? prm(tl.x).fsrc[(idx >> 6) + 6 * tl.y] : -1;
+    }
+  };
+  // neighbour Phi face traces and this element's Phi of tile tl straight into
+  // shared buffer b (asynchronous copies: no registers held)
+  auto async_load = [&](int2 tl, const int src[NFR], int b) {
+    const K1N8<real>& Q = prm(tl.x);
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = tid + r * THR;
+      if (idx < NFT) {
+        const bool ok = src[r] >= 0;
+        const real* g = ok ? Q.Phi + (long long)(src[r] >> 3) * N3 + ftab[((src[r] & 7) << 6) + (idx & 63)] : Q.Phi;
+        cp_async4(sface + b * NFT + idx, g, ok);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) {
+      const int node = tid + r * THR;
+      if (node < N3) cp_async4(sphi + b * N3 + LayC::at(node), Q.Phi + (long long)tl.y * N3 + node, true);
+    }
+  };
+  auto emask_at = [&](int2 tl) -> int { return tl.x >= 0 ? prm(tl.x).emask[tl.y] : 0; };
+  struct PW {
+    real Pi, invJ, y, acc, comp;
+  };
+  auto pw_load = [&](int2 tl, PW w[NPT]) {
+    if (tl.x < 0) return;
+    const K1N8<real>& Q = prm(tl.x);
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) {
+      const int node = tid + r * THR;
+      if (node >= N3) continue;
+      const long long n = (long long)tl.y * N3 + node;
+      w[r].Pi = Q.Pi[n];
+      w[r].invJ = Q.invdetJ[n];
+      w[r].y = need_y ? Q.y[n] : (real)0;
+      w[r].acc = need_acc ? Q.acc[n] : (real)0;
+      w[r].comp = need_comp ? Q.comp[n] : (real)0;
+    }
+  };
+
+  int2 t0 = tile_at(blockIdx.x), t1 = tile_at(blockIdx.x + GS), t2 = tile_at(blockIdx.x + 2 * GS);
+  PW cur[NPT];
+  int emcur = 0, src1[NFR];
+#pragma unroll
+  for (int r = 0; r < NFR; ++r) src1[r] = -1;
+  if (t0.x >= 0) {
+    if (warp == 0) issue(t0, 0);
+    emcur = emask_at(t0);
+    int src0[NFR];
+    src_load(t0, src0);
+    async_load(t0, src0, 0);
+    pw_load(t0, cur);
+    src_load(t1, src1);
+    cp_async_wait_all();
+  }
+  __syncthreads();
+
+  int it = 0;
+  for (long long t = blockIdx.x; t < T; t += GS, ++it) {
+    const int s = it % NS, fb = it & 1;
+    const unsigned parity = (it / NS) & 1;
+    int2 t3 = make_int2(-1, -1);
+    if constexpr (BATCH) {
+      t3 = tile_at(t + 3 * GS);
+    } else {
+      t0 = tile_at(t);
+      t1 = tile_at(t + GS);
+      t2 = tile_at(t + 2 * GS);
+    }
+    const bool has_next = t1.x >= 0;
+    const int emnext = emask_at(t1);
+    int src2[NFR];
+    src_load(t2, src2);
+    PW nxt[NPT];
+    pw_load(t1, nxt);
+    if (tid == 0 && !wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
+    __syncthreads();  // the previous element is finished: stage (it+1) % NS and buffers fb^1 are free
+    if (abort_flag) {
+      return;  // NS = 2: the only copy in flight is the one waited for
+    }
+    if (warp == 0 && t1.x >= 0) issue(t1, (it + 1) % NS);
+    if (has_next) async_load(t1, src1, fb ^ 1);  // lands in the buffers the next element reads
+    const K1N8<real>& Q = prm(t0.x);
+    const long long e = t0.y;
+    const real* d = stg + s * K1C_STAGE;
+    const real* sJa = d;  // 9 fields (LayC), index al*3 + c
+    const real* sPhi = sphi + fb * N3;
+    const real* sfc = sface + fb * NFT;
+    const int mask = emcur & 63;
+    const int bnd = emcur >> 6;
+    // ---- contractions: thread (al, pc) ----
+    {
+      float u[8], cu[8], w[8], o[8];
+#pragma unroll
+      for (int pos = 0; pos < 8; ++pos) u[pos] = sPhi[addr[pos]];
+      contract8(P.Gf, u, cu);
+      // centred-flux SAT of an interior al-face: jump on the face row
+      const bool sat0 = (mask >> (2 * al)) & 1, sat1 = (mask >> (2 * al + 1)) & 1;
+      const real jmp0 = sat0 ? -inv2H * (sfc[(2 * al) * N2 + pc] - u[0]) : (real)0;
+      const real jmp1 = sat1 ? inv2H * (sfc[(2 * al + 1) * N2 + pc] - u[7]) : (real)0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const real* mc = sJa + (al * 3 + c) * FSC;
+        float m[8];
+#pragma unroll
+        for (int pos = 0; pos < 8; ++pos) {
+          m[pos] = mc[addr[pos]];
+          w[pos] = m[pos] * u[pos];
+        }
+        contract8(P.Gf, w, o);
+        real* gout = sg + (al * 3 + c) * FSC;
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+          real r = 0.5f * o[l] + 0.5f * m[l] * cu[l];
+          if (l == 0) r += m[0] * jmp0;
+          if (l == 7) r += m[7] * jmp1;
+          gout[addr[l]] = r;
+        }
+      }
+    }
+    __syncthreads();
+    // ---- node phase ----
+#pragma unroll
+    for (int rr = 0; rr < NPT; ++rr) {
+      const int node = tid + rr * THR;
+      if (node >= N3) continue;
+      const int ti = node & 7, tj = (node >> 3) & 7, tk = node >> 6;
+      const int at = LayC::at(node);
+      const long long n = e * N3 + node;
+      const real u = sPhi[at];
+      real g0 = (sg[at] + sg[3 * FSC + at]) + sg[6 * FSC + at];
+      real g1 = (sg[FSC + at] + sg[4 * FSC + at]) + sg[7 * FSC + at];
+      real g2 = (sg[2 * FSC + at] + sg[5 * FSC + at]) + sg[8 * FSC + at];
+      g0 *= cur[rr].invJ; g1 *= cur[rr].invJ; g2 *= cur[rr].invJ;
+      real cc[10];
+#pragma unroll
+      for (int c = 0; c < 10; ++c) cc[c] = d[9 * FSC + c * N3 + node];
+      const real a = cc[0];
+      const real b0 = cc[1], b1 = cc[2], b2 = cc[3];
+      const real K0 = cc[4], K1v = cc[5], K2 = cc[6], K3 = cc[7], K4 = cc[8], K5 = cc[9];
+      const real Pi = cur[rr].Pi;
+      const real F0 = b0 * Pi + (K0 * g0 + K1v * g1 + K2 * g2);
+      const real F1 = b1 * Pi + (K1v * g0 + K3 * g1 + K4 * g2);
+      const real F2 = b2 * Pi + (K2 * g0 + K4 * g1 + K5 * g2);
+      real phid = b0 * g0 + b1 * g1 + b2 * g2 + a * Pi;
+      if (bnd && Q.bc_on) k1_boundary<real>(Q, e, ti, tj, tk, n, u, Pi, g0, g1, g2, cc, phid);
+      {  // flux in the LayC element-block layout read by K2
+        const long long fo = e * FSC + at, fstr = Q.Ne * FSC;
+        Q.F[fo] = F0;
+        Q.F[fstr + fo] = F1;
+        Q.F[2 * fstr + fo] = F2;
+      }
+      if (P.epi)
+        n8_rk<real>(P.stage, Q.dt, phid, u, cur[rr].y, cur[rr].acc, cur[rr].comp, n, Q.y, Q.acc, Q.out,
+                    comp_on ? Q.comp : nullptr, P.flag);
+      else
+        Q.Phidot[n] = phid;
+    }
+    cp_async_wait_all();  // this thread's copies into buffers fb^1 (the barrier above the next element publishes them)
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) cur[r] = nxt[r];
+    emcur = emnext;
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) src1[r] = src2[r];
+    if constexpr (BATCH) {
+      t0 = t1;
+      t1 = t2;
+      t2 = t3;
+    }
+  }
+}
+
+template <bool BATCH>
+__global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
+    k_cons_k2_n8c(const __grid_constant__ K2N8<float> P, const K2N8<float>* __restrict__ plist,
+                  const int2* __restrict__ tiles, long long ntiles) {
+  using namespace n8;
+  using real = float;
+  constexpr int THR = CTHR, NS = NSTAGE, FSC = LayC::FS;
+  constexpr int NPT = (N3 + THR - 1) / THR;  // 3 node slots per thread
+  constexpr int NFACE = 6 * 3 * N2;          // 1152 neighbour flux face values
+  constexpr int NFR = NFACE / THR;           // 6 per thread
+  extern __shared__ __align__(128) unsigned char smraw[];
+  real* stg = reinterpret_cast<real*>(smraw);  // NS stages x 12 fields
+  real* sdiv = stg + NS * K2C_STAGE;           // 3 partial divergences (LayC)
+  real* sface = sdiv + 3 * FSC;                // 2 x 1152
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sface + 2 * NFACE);
+  __shared__ int abort_flag;
+  __shared__ int ftab[6 * N2];  // LayC offset of face-trace point pq on face fn of an element block
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int al = tid >> 6, pc = tid & 63;
+  const real inv2H = (real)(1.0 / (2.0 * P.H[0]));
+  const bool comp_on = P.epi && P.comp != nullptr;
+  const bool need_y = P.epi && (P.stage <= 2 || (comp_on && P.stage == 3));
+  const bool need_acc = P.epi && P.stage >= 1;
+  const bool need_comp = comp_on && P.stage == 3;
+  const unsigned tx_bytes = (unsigned)(K2C_STAGE * sizeof(real));
+  const long long T = BATCH ? ntiles : P.Ne;
+  const long long GS = gridDim.x;
+  auto tile_at = [&](long long t) -> int2 {
+    if (t >= T) return make_int2(-1, -1);
+    if constexpr (BATCH) return tiles[t];
+    else return make_int2(0, (int)t);
+  };
+  auto prm = [&](int sidx) -> const K2N8<real>& {
+    if constexpr (BATCH) return plist[sidx];
+    else return P;
+  };
+  int addr[8];
+#pragma unroll
+  for (int pos = 0; pos < 8; ++pos) addr[pos] = LayC::at(pnode(al, pc, pos));
+
+  for (int i = tid; i < 6 * N2; i += THR)
+    ftab[i] = LayC::at(face_node(faxis(i >> 6), frow(i >> 6, N), i & 7, (i >> 3) & 7, N));
+  if (tid == 0) {
+    abort_flag = 0;
+    for (int k = 0; k < NS; ++k) mbar_init(&bar[k], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  auto issue = [&](int2 tl, int s) {
+    const K2N8<real>& Q = prm(tl.x);
+    const long long e = tl.y;
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&bar[s], tx_bytes);
+    }
+    __syncwarp();
+    real* d = stg + s * K2C_STAGE;
+    if (lane < K2_NF) {
+      const real* src = lane < 3 ? (lane == 0 ? Q.F0 : lane == 1 ? Q.F1 : Q.F2) + e * FSC
+                                 : Q.Ja + ((long long)(lane - 3) * Q.Ne + e) * FSC;
+      bulk_g2s(d + lane * FSC, src, FSC * (unsigned)sizeof(real), &bar[s]);
+    }
+  };
+  // face-trace slot r of this thread is face r, flux component tid >> 6 (warp-
+  // uniform), point tid & 63: sface[(r * 3 + c) * 64 + pq] = sface[r * THR + tid]
+  auto src_load = [&](int2 tl, int src[NFR]) {
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) src[r] = tl.x >= 0 ? prm(tl.x).fsrc[r + 6 * tl.y] : -1;
+  };
+  // neighbour flux face traces of tile tl straight into shared buffer b
+  auto async_faces = [&](int2 tl, const int src[NFR], int b) {
+    const K2N8<real>& Q = prm(tl.x);
+    const int c = tid >> 6, pq = tid & 63;
+    const real* Fc = c == 0 ? Q.F0 : c == 1 ? Q.F1 : Q.F2;
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) {
+      const bool ok = src[r] >= 0;
+      const real* g = ok ? Fc + (long long)(src[r] >> 3) * FSC + ftab[((src[r] & 7) << 6) + pq] : Fc;
+      cp_async4(sface + b * NFACE + r * THR + tid, g, ok);
+    }
+  };
+  auto emask_at = [&](int2 tl) -> int { return tl.x >= 0 ? prm(tl.x).emask[tl.y] : 0; };
+  struct PW {
+    real invJ, y, acc, comp;
+  };
+  auto pw_load = [&](int2 tl, PW w[NPT]) {
+    if (tl.x < 0) return;
+    const K2N8<real>& Q = prm(tl.x);
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) {
+      const int node = tid + r * THR;
+      if (node >= N3) continue;
+      const long long n = (long long)tl.y * N3 + node;
+      w[r].invJ = Q.invdetJ[n];
+      w[r].y = need_y ? Q.y[n] : (real)0;
+      w[r].acc = need_acc ? Q.acc[n] : (real)0;
+      w[r].comp = need_comp ? Q.comp[n] : (real)0;
+    }
+  };
+
+  int2 t0 = tile_at(blockIdx.x), t1 = tile_at(blockIdx.x + GS), t2 = tile_at(blockIdx.x + 2 * GS);
+  PW cur[NPT];
+  int emcur = 0, src1[NFR];
+#pragma unroll
+  for (int r = 0; r < NFR; ++r) src1[r] = -1;
+  if (t0.x >= 0) {
+    if (warp == 0) issue(t0, 0);
+    emcur = emask_at(t0);
+    int src0[NFR];
+    src_load(t0, src0);
+    async_faces(t0, src0, 0);
+    pw_load(t0, cur);
+    src_load(t1, src1);
+    cp_async_wait_all();
+  }
+  __syncthreads();
+
+  int it = 0;
+  for (long long t = blockIdx.x; t < T; t += GS, ++it) {
+    const int s = it % NS, fb = it & 1;
+    const unsigned parity = (it / NS) & 1;
+    int2 t3 = make_int2(-1, -1);
+    if constexpr (BATCH) {
+      t3 = tile_at(t + 3 * GS);
+    } else {
+      t0 = tile_at(t);
+      t1 = tile_at(t + GS);
+      t2 = tile_at(t + 2 * GS);
+    }
+    const bool has_next = t1.x >= 0;
+    const int emnext = emask_at(t1);
+    int src2[NFR];
+    src_load(t2, src2);
+    PW nxt[NPT];
+    pw_load(t1, nxt);
+    if (tid == 0 && !wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
+    __syncthreads();
+    if (abort_flag) {
+      return;  // NS = 2: the only copy in flight is the one waited for
+    }
+    if (warp == 0 && t1.x >= 0) issue(t1, (it + 1) % NS);
+    if (has_next) async_faces(t1, src1, fb ^ 1);
+    const K2N8<real>& Q = prm(t0.x);
+    const long long e = t0.y;
+    const real* d = stg + s * K2C_STAGE;
+    const real* sF = d;
+    const real* sJa = d + 3 * FSC;
+    const real* sfc = sface + fb * NFACE;
+    const int mask = emcur & 63;
+    const int bnd = emcur >> 6;
+    // ---- contractions: thread (al, pc) ----
+    {
+      const real* m0 = sJa + (al * 3 + 0) * FSC;
+      const real* m1 = sJa + (al * 3 + 1) * FSC;
+      const real* m2 = sJa + (al * 3 + 2) * FSC;
+      // r = 0.5 D(Ja^al . F) + 0.5 sum_c Ja^al_c D(F_c), one component live at a time
+      float v[8], o[8], r[8];
+#pragma unroll
+      for (int pos = 0; pos < 8; ++pos) {
+        const int ad = addr[pos];
+        v[pos] = m0[ad] * sF[ad] + m1[ad] * sF[FSC + ad] + m2[ad] * sF[2 * FSC + ad];
+      }
+      contract8(P.Gf, v, o);
+#pragma unroll
+      for (int l = 0; l < 8; ++l) r[l] = 0.5f * o[l];
+      const bool sat0 = (mask >> (2 * al)) & 1, sat1 = (mask >> (2 * al + 1)) & 1;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const real* mc = sJa + (al * 3 + c) * FSC;
+        const real* fc = sF + c * FSC;
+        float fv[8];
+#pragma unroll
+        for (int pos = 0; pos < 8; ++pos) fv[pos] = fc[addr[pos]];
+        contract8(P.Gf, fv, o);
+#pragma unroll
+        for (int l = 0; l < 8; ++l) r[l] += 0.5f * mc[addr[l]] * o[l];
+        // centred-flux SAT of an interior al-face on the face rows
+        if (sat0) r[0] -= inv2H * mc[addr[0]] * (sfc[((2 * al) * 3 + c) * N2 + pc] - fv[0]);
+        if (sat1) r[7] += inv2H * mc[addr[7]] * (sfc[((2 * al + 1) * 3 + c) * N2 + pc] - fv[7]);
+      }
+#pragma unroll
+      for (int l = 0; l < 8; ++l) sdiv[al * FSC + addr[l]] = r[l];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int rr = 0; rr < NPT; ++rr) {
+      const int node = tid + rr * THR;
+      if (node >= N3) continue;
+      const int ti = node & 7, tj = (node >> 3) & 7, tk = node >> 6;
+      const int at = LayC::at(node);
+      const long long n = e * N3 + node;
+      real dv = (sdiv[at] + sdiv[FSC + at]) + sdiv[2 * FSC + at];
+      dv *= cur[rr].invJ;
+      if (bnd && Q.bc_on) {
+        const int idx3[3] = {ti, tj, tk};
+        for (int f = 0; f < 6; ++f) {
+          if (Q.bdry[f + 6 * e] == 0) continue;
+          const int ax = f >> 1;
+          if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
+          const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
+          dv += Q.bbuf[(long long)Q.bslot[f + 6 * e] * N2 + p + 8 * q];
+        }
+      }
+      if (P.epi)
+        n8_rk<real>(P.stage, Q.dt, dv, cur[rr].y, cur[rr].y, cur[rr].acc, cur[rr].comp, n, Q.y, Q.acc, Q.out,
+                    comp_on ? Q.comp : nullptr, P.flag);
+      else
+        Q.Pidot[n] = dv;
+    }
+    cp_async_wait_all();  // this thread's face copies into buffer fb^1
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) cur[r] = nxt[r];
+    emcur = emnext;
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) src1[r] = src2[r];
+    if constexpr (BATCH) {
+      t0 = t1;
+      t1 = t2;
+      t2 = t3;
+    }
+  }
+}
+
 // padded element-block copy of the nine metric-term fields for the n = 8 path
-template <typename real>
+template <typename real, typename L>
 __global__ void k_pad_fields(long long Ne, int nf, const real* __restrict__ src, real* __restrict__ dst) {
   const long long total = (long long)nf * Ne * n8::N3;
   for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
@@ -1065,15 +1603,24 @@ __global__ void k_pad_fields(long long Ne, int nf, const real* __restrict__ src,
     const long long r = x - f * Ne * n8::N3;
     const long long e = r / n8::N3;
     const int t = (int)(r - e * n8::N3);
-    dst[(f * Ne + e) * n8::Lay<real>::FS + n8::Lay<real>::at(t)] = src[x];
+    dst[(f * Ne + e) * L::FS + L::at(t)] = src[x];
   }
+}
+
+// element-block layout of the mesh's n = 8 kernels: 0 = Lay<real>, 1 = LayC (FP32 CUDA-core form)
+static int n8_layout(const DevMesh& m) { return m.precision == 1 && m.fp32_form == WT_FP32_CUDA_CORES ? 1 : 0; }
+static long long n8_fs(const DevMesh& m) {
+  return m.precision == 0 ? n8::Lay<double>::FS : n8_layout(m) ? n8::LayC::FS : n8::Lay<float>::FS;
 }
 
 int launch_pad_metric_n8(DevMesh& m, cudaStream_t s) {
   if (m.precision == 0)
-    k_pad_fields<double><<<4096, 256, 0, s>>>(m.Ne, 9, (const double*)m.Ja_r, (double*)m.Ja_n8);
+    k_pad_fields<double, n8::Lay<double>><<<4096, 256, 0, s>>>(m.Ne, 9, (const double*)m.Ja_r, (double*)m.Ja_n8);
+  else if (n8_layout(m))
+    k_pad_fields<float, n8::LayC><<<4096, 256, 0, s>>>(m.Ne, 9, (const float*)m.Ja_r, (float*)m.Ja_n8);
   else
-    k_pad_fields<float><<<4096, 256, 0, s>>>(m.Ne, 9, (const float*)m.Ja_r, (float*)m.Ja_n8);
+    k_pad_fields<float, n8::Lay<float>><<<4096, 256, 0, s>>>(m.Ne, 9, (const float*)m.Ja_r, (float*)m.Ja_n8);
+  m.ja_n8_layout = n8_layout(m);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -1108,6 +1655,7 @@ static K1N8<real> k1n8_params(const DevMesh& m, const DevCoef& c, const void* Ph
   P.gDx = (const real*)bc.gDx; P.gDy = (const real*)bc.gDy; P.gDz = (const real*)bc.gDz;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
+  for (int i = 0; i < 64; ++i) P.Gf[i] = (float)m.ops.G[i];
   return P;
 }
 
@@ -1116,7 +1664,7 @@ static K2N8<real> k2n8_params(const DevMesh& m, const void* F, void* Pidot, cons
                               const RKStage& rk, unsigned* flag) {
   K2N8<real> P;
   P.Ne = m.Ne; P.nn = m.nn;
-  const long long fs = m.Ne * n8::Lay<real>::FS;
+  const long long fs = m.Ne * n8_fs(m);
   P.F0 = (const real*)F; P.F1 = (const real*)F + fs; P.F2 = (const real*)F + 2 * fs;
   P.Ja = (const real*)m.Ja_n8; P.invdetJ = (const real*)m.invdetJ_r;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
@@ -1125,6 +1673,7 @@ static K2N8<real> k2n8_params(const DevMesh& m, const void* F, void* Pidot, cons
   P.Pidot = (real*)Pidot;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
+  for (int i = 0; i < 64; ++i) P.Gf[i] = (float)m.ops.G[i];
   return P;
 }
 
@@ -1162,9 +1711,41 @@ static int n8_launch(int which, const void* hP, const void* plist, const int2* t
 }
 
 template <bool BATCH>
+static int n8c_launch(int which, const void* hP, const void* plist, const int2* tiles, long long ntiles,
+                      cudaStream_t s) {
+  static bool attr1 = false, attr2 = false;
+  const int occ = which == 1 ? K1C_OCC : K2C_OCC;
+  const long long cap = (long long)sm_count() * occ;
+  const long long grid = ntiles < cap ? ntiles : cap;
+  if (which == 1) {
+    if (!attr1) {
+      if (cudaFuncSetAttribute(k_cons_k1_n8c<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k1c_smem()) !=
+          cudaSuccess)
+        return -2;
+      attr1 = true;
+    }
+    if (grid <= 0) return 0;
+    k_cons_k1_n8c<BATCH><<<(unsigned)grid, n8::CTHR, k1c_smem(), s>>>(*(const K1N8<float>*)hP,
+                                                                       (const K1N8<float>*)plist, tiles, ntiles);
+  } else {
+    if (!attr2) {
+      if (cudaFuncSetAttribute(k_cons_k2_n8c<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k2c_smem()) !=
+          cudaSuccess)
+        return -2;
+      attr2 = true;
+    }
+    if (grid <= 0) return 0;
+    k_cons_k2_n8c<BATCH><<<(unsigned)grid, n8::CTHR, k2c_smem(), s>>>(*(const K2N8<float>*)hP,
+                                                                       (const K2N8<float>*)plist, tiles, ntiles);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <bool BATCH>
 static int n8_dispatch(int which, int precision, int fp32_form, const void* hP, const void* plist, const int2* tiles,
                        long long ntiles, cudaStream_t s) {
   if (precision == 0) return n8_launch<double, 0, BATCH>(which, hP, plist, tiles, ntiles, s);
+  if (fp32_form == WT_FP32_CUDA_CORES) return n8c_launch<BATCH>(which, hP, plist, tiles, ntiles, s);
   if (fp32_form == WT_FP32_BF16X2) return n8_launch<float, 2, BATCH>(which, hP, plist, tiles, ntiles, s);
   return n8_launch<float, 3, BATCH>(which, hP, plist, tiles, ntiles, s);
 }
