@@ -317,7 +317,7 @@ struct K1N8 {
   real* out;
   real* comp;
   unsigned* flag;
-  float Gf[64];  // the operator in FP32 (the CUDA-core form reads it from the constant bank)
+  float Gh[64];  // 0.5 G in FP32 (the CUDA-core form reads it from the constant bank)
 };
 
 // Boundary terms of K1 at a node on an outer face (the curvilinear boundary
@@ -728,7 +728,7 @@ struct K2N8 {
   real* out;
   real* comp;
   unsigned* flag;
-  float Gf[64];
+  float Gh[64];
 };
 
 // K2 staged fields: 0..2 F, 3..11 Ja.  Register prefetch: invJ, y, acc, comp.
@@ -1115,14 +1115,21 @@ __device__ __forceinline__ void contract8(const float* G, const float v[8], floa
 }
 }  // namespace n8
 
-constexpr size_t K1C_STAGE = 9 * (size_t)n8::LayC::FS + 10 * (size_t)n8::N3;  // Ja (LayC), ten coefficients
+// K1c: the nine Ja blocks in one stage (read by the contraction pass) and the
+// node-pass fields in a second buffer (ten coefficients, Pi, 1/J, y, acc, comp),
+// each single-buffered and bulk-copied as soon as the pass that reads it is done,
+// so that three CTAs fit on an SM.
+constexpr size_t K1C_STAGE = 9 * (size_t)n8::LayC::FS;
+constexpr size_t K1C_B = 15 * (size_t)n8::N3;
 constexpr size_t K2C_STAGE = (size_t)K2_NF * n8::LayC::FS;
-constexpr int K1C_OCC = 2, K2C_OCC = 3;
+constexpr int K1C_OCC = 3, K2C_OCC = 3;
 constexpr size_t k1c_smem() {
-  return (n8::NSTAGE * K1C_STAGE + 9 * n8::LayC::FS + 2 * 6 * n8::N2 + 2 * n8::N3) * sizeof(float) + 64;
+  return (K1C_STAGE + K1C_B + 9 * n8::LayC::FS + 2 * 6 * n8::N2 + 2 * n8::N3) * sizeof(float) + 64;
 }
+// K2c node-pass fields (1/J and the RK state: invJ, y, acc, comp), one bulk-copied buffer
+constexpr size_t K2C_B = 4 * (size_t)n8::N3;
 constexpr size_t k2c_smem() {
-  return (n8::NSTAGE * K2C_STAGE + 3 * n8::LayC::FS + 2 * 6 * 3 * n8::N2) * sizeof(float) + 64;
+  return (n8::NSTAGE * K2C_STAGE + 3 * n8::LayC::FS + 2 * 6 * 3 * n8::N2 + K2C_B) * sizeof(float) + 64;
 }
 
 template <bool BATCH>
@@ -1131,18 +1138,19 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
                   const int2* __restrict__ tiles, long long ntiles) {
   using namespace n8;
   using real = float;
-  constexpr int THR = CTHR, NS = NSTAGE, FSC = LayC::FS;
-  constexpr int NPT = (N3 + THR - 1) / THR;  // node slots per thread (3, the last one partly)
-  constexpr int NFT = 6 * N2;                // 384 neighbour Phi face values
+  constexpr int THR = CTHR, FSC = LayC::FS;
+  constexpr int NPT = (N3 + THR - 1) / THR;   // node slots per thread (3, the last one partly)
+  constexpr int NFT = 6 * N2;                 // 384 neighbour Phi face values
   constexpr int NFR = (NFT + THR - 1) / THR;  // 2 per thread
   extern __shared__ __align__(128) unsigned char smraw[];
-  real* stg = reinterpret_cast<real*>(smraw);  // NS stages
-  real* sg = stg + NS * K1C_STAGE;             // 9 partial gradients [al*3 + c] (LayC)
+  real* sJa = reinterpret_cast<real*>(smraw);  // 9 fields (LayC), index al*3 + c
+  real* sB = sJa + K1C_STAGE;                  // node order: c10 (10), Pi, invJ, y, acc, comp
+  real* sg = sB + K1C_B;                       // 9 partial gradients [al*3 + c] (LayC)
   real* sface = sg + 9 * FSC;                  // 2 x 384
   real* sphi = sface + 2 * NFT;                // 2 x 512 (LayC)
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sphi + 2 * N3);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sphi + 2 * N3);  // [0] Ja stage, [1] sB
   __shared__ int abort_flag;
-  __shared__ int ftab[6 * N2];  // node of face-trace point pq on face fn of an element block
+  __shared__ short ftab[6 * N2];  // node of face-trace point pq on face fn of an element block
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int al = tid >> 6, pc = tid & 63;  // contraction: axis (warp-uniform) and pencil
   const real inv2H = (real)(1.0 / (2.0 * P.H[0]));
@@ -1150,7 +1158,8 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
   const bool need_y = P.epi && (P.stage == 1 || P.stage == 2 || (comp_on && P.stage == 3));
   const bool need_acc = P.epi && P.stage >= 1;
   const bool need_comp = comp_on && P.stage == 3;
-  const unsigned tx_bytes = (unsigned)(K1C_STAGE * sizeof(real));
+  const unsigned txA = (unsigned)(K1C_STAGE * sizeof(real));
+  const unsigned txB = (unsigned)((12 + need_y + need_acc + need_comp) * N3 * sizeof(real));
   const long long T = BATCH ? ntiles : P.Ne;
   const long long GS = gridDim.x;
   auto tile_at = [&](long long t) -> int2 {
@@ -1167,29 +1176,43 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
   for (int pos = 0; pos < 8; ++pos) addr[pos] = LayC::at(pnode(al, pc, pos));
 
   for (int i = tid; i < 6 * N2; i += THR)
-    ftab[i] = face_node(faxis(i >> 6), frow(i >> 6, N), i & 7, (i >> 3) & 7, N);
+    ftab[i] = (short)face_node(faxis(i >> 6), frow(i >> 6, N), i & 7, (i >> 3) & 7, N);
   if (tid == 0) {
     abort_flag = 0;
-    for (int k = 0; k < NS; ++k) mbar_init(&bar[k], 1);
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
     fence_barrier_init();
   }
   __syncthreads();
 
-  // warp 0 stages tile tl into stage s: 9 Ja blocks, 10 coefficient blocks
-  auto issue = [&](int2 tl, int s) {
+  // warp 0 copies the Ja blocks (issueA) or the node-pass fields (issueB) of tile tl
+  auto issueA = [&](int2 tl) {
     const K1N8<real>& Q = prm(tl.x);
-    const long long e = tl.y;
     if (lane == 0) {
       fence_proxy_async();
-      mbar_expect_tx(&bar[s], tx_bytes);
+      mbar_expect_tx(&bar[0], txA);
     }
     __syncwarp();
-    real* d = stg + s * K1C_STAGE;
     if (lane < 9)
-      bulk_g2s(d + lane * FSC, Q.Ja + ((long long)lane * Q.Ne + e) * FSC, FSC * (unsigned)sizeof(real), &bar[s]);
-    else if (lane < 19)
-      bulk_g2s(d + 9 * FSC + (lane - 9) * N3, Q.c10 + (lane - 9) * Q.nn + e * N3, N3 * (unsigned)sizeof(real),
-               &bar[s]);
+      bulk_g2s(sJa + lane * FSC, Q.Ja + ((long long)lane * Q.Ne + tl.y) * FSC, FSC * (unsigned)sizeof(real), &bar[0]);
+  };
+  auto issueB = [&](int2 tl) {
+    const K1N8<real>& Q = prm(tl.x);
+    const long long o = (long long)tl.y * N3;
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&bar[1], txB);
+    }
+    __syncwarp();
+    const unsigned nb = N3 * (unsigned)sizeof(real);
+    const real* src = nullptr;
+    if (lane < 10) src = Q.c10 + lane * Q.nn + o;
+    else if (lane == 10) src = Q.Pi + o;
+    else if (lane == 11) src = Q.invdetJ + o;
+    else if (lane == 12 && need_y) src = Q.y + o;
+    else if (lane == 13 && need_acc) src = Q.acc + o;
+    else if (lane == 14 && need_comp) src = Q.comp + o;
+    if (src) bulk_g2s(sB + lane * N3, src, nb, &bar[1]);
   };
   // face-trace slot r of this thread: value tid + r * THR = (face, pq) of the 384
   auto src_load = [&](int2 tl, int src[NFR]) {
@@ -1219,37 +1242,17 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
     }
   };
   auto emask_at = [&](int2 tl) -> int { return tl.x >= 0 ? prm(tl.x).emask[tl.y] : 0; };
-  struct PW {
-    real Pi, invJ, y, acc, comp;
-  };
-  auto pw_load = [&](int2 tl, PW w[NPT]) {
-    if (tl.x < 0) return;
-    const K1N8<real>& Q = prm(tl.x);
-#pragma unroll
-    for (int r = 0; r < NPT; ++r) {
-      const int node = tid + r * THR;
-      if (node >= N3) continue;
-      const long long n = (long long)tl.y * N3 + node;
-      w[r].Pi = Q.Pi[n];
-      w[r].invJ = Q.invdetJ[n];
-      w[r].y = need_y ? Q.y[n] : (real)0;
-      w[r].acc = need_acc ? Q.acc[n] : (real)0;
-      w[r].comp = need_comp ? Q.comp[n] : (real)0;
-    }
-  };
 
   int2 t0 = tile_at(blockIdx.x), t1 = tile_at(blockIdx.x + GS), t2 = tile_at(blockIdx.x + 2 * GS);
-  PW cur[NPT];
   int emcur = 0, src1[NFR];
 #pragma unroll
   for (int r = 0; r < NFR; ++r) src1[r] = -1;
   if (t0.x >= 0) {
-    if (warp == 0) issue(t0, 0);
+    if (warp == 0) issueA(t0);
     emcur = emask_at(t0);
     int src0[NFR];
     src_load(t0, src0);
     async_load(t0, src0, 0);
-    pw_load(t0, cur);
     src_load(t1, src1);
     cp_async_wait_all();
   }
@@ -1257,8 +1260,8 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
 
   int it = 0;
   for (long long t = blockIdx.x; t < T; t += GS, ++it) {
-    const int s = it % NS, fb = it & 1;
-    const unsigned parity = (it / NS) & 1;
+    const int fb = it & 1;
+    const unsigned parity = it & 1;
     int2 t3 = make_int2(-1, -1);
     if constexpr (BATCH) {
       t3 = tile_at(t + 3 * GS);
@@ -1271,29 +1274,24 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
     const int emnext = emask_at(t1);
     int src2[NFR];
     src_load(t2, src2);
-    PW nxt[NPT];
-    pw_load(t1, nxt);
-    if (tid == 0 && !wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
-    __syncthreads();  // the previous element is finished: stage (it+1) % NS and buffers fb^1 are free
-    if (abort_flag) {
-      return;  // NS = 2: the only copy in flight is the one waited for
-    }
-    if (warp == 0 && t1.x >= 0) issue(t1, (it + 1) % NS);
-    if (has_next) async_load(t1, src1, fb ^ 1);  // lands in the buffers the next element reads
+    if (tid == 0 && !wait_phase(&bar[0], parity, P.flag)) abort_flag = 1;
+    __syncthreads();  // the previous element is finished: sB and buffers fb^1 are free
+    if (abort_flag) return;  // the only copy in flight is the one waited for
+    if (warp == 0) issueB(t0);  // lands while the contraction pass runs
+    if (has_next) async_load(t1, src1, fb ^ 1);
     const K1N8<real>& Q = prm(t0.x);
     const long long e = t0.y;
-    const real* d = stg + s * K1C_STAGE;
-    const real* sJa = d;  // 9 fields (LayC), index al*3 + c
     const real* sPhi = sphi + fb * N3;
     const real* sfc = sface + fb * NFT;
     const int mask = emcur & 63;
     const int bnd = emcur >> 6;
-    // ---- contractions: thread (al, pc) ----
+    // ---- contractions: thread (al, pc); the operator in the constant bank is
+    // 0.5 G (scaling by 1/2 is exact) ----
     {
       float u[8], cu[8], w[8], o[8];
 #pragma unroll
       for (int pos = 0; pos < 8; ++pos) u[pos] = sPhi[addr[pos]];
-      contract8(P.Gf, u, cu);
+      contract8(P.Gh, u, cu);  // 0.5 D u
       // centred-flux SAT of an interior al-face: jump on the face row
       const bool sat0 = (mask >> (2 * al)) & 1, sat1 = (mask >> (2 * al + 1)) & 1;
       const real jmp0 = sat0 ? -inv2H * (sfc[(2 * al) * N2 + pc] - u[0]) : (real)0;
@@ -1307,18 +1305,21 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
           m[pos] = mc[addr[pos]];
           w[pos] = m[pos] * u[pos];
         }
-        contract8(P.Gf, w, o);
+        contract8(P.Gh, w, o);  // 0.5 D (Ja u)
         real* gout = sg + (al * 3 + c) * FSC;
 #pragma unroll
         for (int l = 0; l < 8; ++l) {
-          real r = 0.5f * o[l] + 0.5f * m[l] * cu[l];
+          real r = fmaf(m[l], cu[l], o[l]);  // 0.5 D(Ja u) + 0.5 Ja D u
           if (l == 0) r += m[0] * jmp0;
           if (l == 7) r += m[7] * jmp1;
           gout[addr[l]] = r;
         }
       }
     }
-    __syncthreads();
+    if (tid == 0 && !wait_phase(&bar[1], parity, P.flag)) abort_flag = 1;
+    __syncthreads();  // partial gradients and sB complete; the Ja stage is free
+    if (abort_flag) return;
+    if (warp == 0 && has_next) issueA(t1);  // lands while the node pass runs
     // ---- node phase ----
 #pragma unroll
     for (int rr = 0; rr < NPT; ++rr) {
@@ -1328,17 +1329,18 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
       const int at = LayC::at(node);
       const long long n = e * N3 + node;
       const real u = sPhi[at];
+      const real invJ = sB[11 * N3 + node];
       real g0 = (sg[at] + sg[3 * FSC + at]) + sg[6 * FSC + at];
       real g1 = (sg[FSC + at] + sg[4 * FSC + at]) + sg[7 * FSC + at];
       real g2 = (sg[2 * FSC + at] + sg[5 * FSC + at]) + sg[8 * FSC + at];
-      g0 *= cur[rr].invJ; g1 *= cur[rr].invJ; g2 *= cur[rr].invJ;
+      g0 *= invJ; g1 *= invJ; g2 *= invJ;
       real cc[10];
 #pragma unroll
-      for (int c = 0; c < 10; ++c) cc[c] = d[9 * FSC + c * N3 + node];
+      for (int c = 0; c < 10; ++c) cc[c] = sB[c * N3 + node];
       const real a = cc[0];
       const real b0 = cc[1], b1 = cc[2], b2 = cc[3];
       const real K0 = cc[4], K1v = cc[5], K2 = cc[6], K3 = cc[7], K4 = cc[8], K5 = cc[9];
-      const real Pi = cur[rr].Pi;
+      const real Pi = sB[10 * N3 + node];
       const real F0 = b0 * Pi + (K0 * g0 + K1v * g1 + K2 * g2);
       const real F1 = b1 * Pi + (K1v * g0 + K3 * g1 + K4 * g2);
       const real F2 = b2 * Pi + (K2 * g0 + K4 * g1 + K5 * g2);
@@ -1350,15 +1352,14 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
         Q.F[fstr + fo] = F1;
         Q.F[2 * fstr + fo] = F2;
       }
+      const real yv = need_y ? sB[12 * N3 + node] : (real)0, accv = need_acc ? sB[13 * N3 + node] : (real)0;
+      const real compv = need_comp ? sB[14 * N3 + node] : (real)0;
       if (P.epi)
-        n8_rk<real>(P.stage, Q.dt, phid, u, cur[rr].y, cur[rr].acc, cur[rr].comp, n, Q.y, Q.acc, Q.out,
-                    comp_on ? Q.comp : nullptr, P.flag);
+        n8_rk<real>(P.stage, Q.dt, phid, u, yv, accv, compv, n, Q.y, Q.acc, Q.out, comp_on ? Q.comp : nullptr, P.flag);
       else
         Q.Phidot[n] = phid;
     }
     cp_async_wait_all();  // this thread's copies into buffers fb^1 (the barrier above the next element publishes them)
-#pragma unroll
-    for (int r = 0; r < NPT; ++r) cur[r] = nxt[r];
     emcur = emnext;
 #pragma unroll
     for (int r = 0; r < NFR; ++r) src1[r] = src2[r];
@@ -1384,7 +1385,8 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
   real* stg = reinterpret_cast<real*>(smraw);  // NS stages x 12 fields
   real* sdiv = stg + NS * K2C_STAGE;           // 3 partial divergences (LayC)
   real* sface = sdiv + 3 * FSC;                // 2 x 1152
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sface + 2 * NFACE);
+  real* sB = sface + 2 * NFACE;                // node-pass fields: invJ, y, acc, comp (node order)
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sB + K2C_B);  // NS stage barriers, then the sB barrier
   __shared__ int abort_flag;
   __shared__ int ftab[6 * N2];  // LayC offset of face-trace point pq on face fn of an element block
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1395,6 +1397,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
   const bool need_acc = P.epi && P.stage >= 1;
   const bool need_comp = comp_on && P.stage == 3;
   const unsigned tx_bytes = (unsigned)(K2C_STAGE * sizeof(real));
+  const unsigned txB = (unsigned)((1 + need_y + need_acc + need_comp) * N3 * sizeof(real));
   const long long T = BATCH ? ntiles : P.Ne;
   const long long GS = gridDim.x;
   auto tile_at = [&](long long t) -> int2 {
@@ -1414,7 +1417,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
     ftab[i] = LayC::at(face_node(faxis(i >> 6), frow(i >> 6, N), i & 7, (i >> 3) & 7, N));
   if (tid == 0) {
     abort_flag = 0;
-    for (int k = 0; k < NS; ++k) mbar_init(&bar[k], 1);
+    for (int k = 0; k <= NS; ++k) mbar_init(&bar[k], 1);
     fence_barrier_init();
   }
   __syncthreads();
@@ -1453,26 +1456,23 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
     }
   };
   auto emask_at = [&](int2 tl) -> int { return tl.x >= 0 ? prm(tl.x).emask[tl.y] : 0; };
-  struct PW {
-    real invJ, y, acc, comp;
-  };
-  auto pw_load = [&](int2 tl, PW w[NPT]) {
-    if (tl.x < 0) return;
+  // warp 0 copies the node-pass fields of tile tl into sB
+  auto issueB = [&](int2 tl) {
     const K2N8<real>& Q = prm(tl.x);
-#pragma unroll
-    for (int r = 0; r < NPT; ++r) {
-      const int node = tid + r * THR;
-      if (node >= N3) continue;
-      const long long n = (long long)tl.y * N3 + node;
-      w[r].invJ = Q.invdetJ[n];
-      w[r].y = need_y ? Q.y[n] : (real)0;
-      w[r].acc = need_acc ? Q.acc[n] : (real)0;
-      w[r].comp = need_comp ? Q.comp[n] : (real)0;
+    const long long o = (long long)tl.y * N3;
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&bar[NS], txB);
     }
+    __syncwarp();
+    const unsigned nb = N3 * (unsigned)sizeof(real);
+    if (lane == 0) bulk_g2s(sB, Q.invdetJ + o, nb, &bar[NS]);
+    else if (lane == 1 && need_y) bulk_g2s(sB + N3, Q.y + o, nb, &bar[NS]);
+    else if (lane == 2 && need_acc) bulk_g2s(sB + 2 * N3, Q.acc + o, nb, &bar[NS]);
+    else if (lane == 3 && need_comp) bulk_g2s(sB + 3 * N3, Q.comp + o, nb, &bar[NS]);
   };
 
   int2 t0 = tile_at(blockIdx.x), t1 = tile_at(blockIdx.x + GS), t2 = tile_at(blockIdx.x + 2 * GS);
-  PW cur[NPT];
   int emcur = 0, src1[NFR];
 #pragma unroll
   for (int r = 0; r < NFR; ++r) src1[r] = -1;
@@ -1482,7 +1482,6 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
     int src0[NFR];
     src_load(t0, src0);
     async_faces(t0, src0, 0);
-    pw_load(t0, cur);
     src_load(t1, src1);
     cp_async_wait_all();
   }
@@ -1504,14 +1503,15 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
     const int emnext = emask_at(t1);
     int src2[NFR];
     src_load(t2, src2);
-    PW nxt[NPT];
-    pw_load(t1, nxt);
     if (tid == 0 && !wait_phase(&bar[s], parity, P.flag)) abort_flag = 1;
-    __syncthreads();
+    __syncthreads();  // the previous element is finished: stage (it+1) % NS, sB and face buffer fb^1 are free
     if (abort_flag) {
       return;  // NS = 2: the only copy in flight is the one waited for
     }
-    if (warp == 0 && t1.x >= 0) issue(t1, (it + 1) % NS);
+    if (warp == 0) {
+      if (t1.x >= 0) issue(t1, (it + 1) % NS);
+      issueB(t0);  // lands while the contraction below runs
+    }
     if (has_next) async_faces(t1, src1, fb ^ 1);
     const K2N8<real>& Q = prm(t0.x);
     const long long e = t0.y;
@@ -1527,15 +1527,14 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
       const real* m1 = sJa + (al * 3 + 1) * FSC;
       const real* m2 = sJa + (al * 3 + 2) * FSC;
       // r = 0.5 D(Ja^al . F) + 0.5 sum_c Ja^al_c D(F_c), one component live at a time
+      // (the operator in the constant bank is 0.5 G; scaling by 1/2 is exact)
       float v[8], o[8], r[8];
 #pragma unroll
       for (int pos = 0; pos < 8; ++pos) {
         const int ad = addr[pos];
         v[pos] = m0[ad] * sF[ad] + m1[ad] * sF[FSC + ad] + m2[ad] * sF[2 * FSC + ad];
       }
-      contract8(P.Gf, v, o);
-#pragma unroll
-      for (int l = 0; l < 8; ++l) r[l] = 0.5f * o[l];
+      contract8(P.Gh, v, r);  // 0.5 D (Ja^al . F)
       const bool sat0 = (mask >> (2 * al)) & 1, sat1 = (mask >> (2 * al + 1)) & 1;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -1544,9 +1543,9 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
         float fv[8];
 #pragma unroll
         for (int pos = 0; pos < 8; ++pos) fv[pos] = fc[addr[pos]];
-        contract8(P.Gf, fv, o);
+        contract8(P.Gh, fv, o);  // 0.5 D F_c
 #pragma unroll
-        for (int l = 0; l < 8; ++l) r[l] += 0.5f * mc[addr[l]] * o[l];
+        for (int l = 0; l < 8; ++l) r[l] = fmaf(mc[addr[l]], o[l], r[l]);
         // centred-flux SAT of an interior al-face on the face rows
         if (sat0) r[0] -= inv2H * mc[addr[0]] * (sfc[((2 * al) * 3 + c) * N2 + pc] - fv[0]);
         if (sat1) r[7] += inv2H * mc[addr[7]] * (sfc[((2 * al + 1) * 3 + c) * N2 + pc] - fv[7]);
@@ -1554,7 +1553,9 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
 #pragma unroll
       for (int l = 0; l < 8; ++l) sdiv[al * FSC + addr[l]] = r[l];
     }
+    if (tid == 0 && !wait_phase(&bar[NS], it & 1, P.flag)) abort_flag = 1;
     __syncthreads();
+    if (abort_flag) return;
 #pragma unroll
     for (int rr = 0; rr < NPT; ++rr) {
       const int node = tid + rr * THR;
@@ -1563,7 +1564,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
       const int at = LayC::at(node);
       const long long n = e * N3 + node;
       real dv = (sdiv[at] + sdiv[FSC + at]) + sdiv[2 * FSC + at];
-      dv *= cur[rr].invJ;
+      dv *= sB[node];
       if (bnd && Q.bc_on) {
         const int idx3[3] = {ti, tj, tk};
         for (int f = 0; f < 6; ++f) {
@@ -1574,15 +1575,14 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
           dv += Q.bbuf[(long long)Q.bslot[f + 6 * e] * N2 + p + 8 * q];
         }
       }
+      const real yv = need_y ? sB[N3 + node] : (real)0, accv = need_acc ? sB[2 * N3 + node] : (real)0;
+      const real compv = need_comp ? sB[3 * N3 + node] : (real)0;
       if (P.epi)
-        n8_rk<real>(P.stage, Q.dt, dv, cur[rr].y, cur[rr].y, cur[rr].acc, cur[rr].comp, n, Q.y, Q.acc, Q.out,
-                    comp_on ? Q.comp : nullptr, P.flag);
+        n8_rk<real>(P.stage, Q.dt, dv, yv, yv, accv, compv, n, Q.y, Q.acc, Q.out, comp_on ? Q.comp : nullptr, P.flag);
       else
         Q.Pidot[n] = dv;
     }
     cp_async_wait_all();  // this thread's face copies into buffer fb^1
-#pragma unroll
-    for (int r = 0; r < NPT; ++r) cur[r] = nxt[r];
     emcur = emnext;
 #pragma unroll
     for (int r = 0; r < NFR; ++r) src1[r] = src2[r];
@@ -1655,7 +1655,7 @@ static K1N8<real> k1n8_params(const DevMesh& m, const DevCoef& c, const void* Ph
   P.gDx = (const real*)bc.gDx; P.gDy = (const real*)bc.gDy; P.gDz = (const real*)bc.gDz;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
-  for (int i = 0; i < 64; ++i) P.Gf[i] = (float)m.ops.G[i];
+  for (int i = 0; i < 64; ++i) P.Gh[i] = (float)(0.5 * m.ops.G[i]);
   return P;
 }
 
@@ -1673,7 +1673,7 @@ static K2N8<real> k2n8_params(const DevMesh& m, const void* F, void* Pidot, cons
   P.Pidot = (real*)Pidot;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
-  for (int i = 0; i < 64; ++i) P.Gf[i] = (float)m.ops.G[i];
+  for (int i = 0; i < 64; ++i) P.Gh[i] = (float)(0.5 * m.ops.G[i]);
   return P;
 }
 
@@ -1719,8 +1719,11 @@ static int n8c_launch(int which, const void* hP, const void* plist, const int2* 
   const long long grid = ntiles < cap ? ntiles : cap;
   if (which == 1) {
     if (!attr1) {
+      // three CTAs per SM need (nearly) all of the SM's shared memory
       if (cudaFuncSetAttribute(k_cons_k1_n8c<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k1c_smem()) !=
-          cudaSuccess)
+              cudaSuccess ||
+          cudaFuncSetAttribute(k_cons_k1_n8c<BATCH>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
         return -2;
       attr1 = true;
     }
@@ -1730,7 +1733,9 @@ static int n8c_launch(int which, const void* hP, const void* plist, const int2* 
   } else {
     if (!attr2) {
       if (cudaFuncSetAttribute(k_cons_k2_n8c<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k2c_smem()) !=
-          cudaSuccess)
+              cudaSuccess ||
+          cudaFuncSetAttribute(k_cons_k2_n8c<BATCH>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
         return -2;
       attr2 = true;
     }
