@@ -353,7 +353,7 @@ def run_ours(args):
 
 def run_batch(args):
     """Batched uneven solves: args.solves warped-cube solves (e ~ U{4..24}, n ~ {4,6,8},
-    flat or perturbed ADM), FP32 split-precision form, advanced together by the
+    flat or perturbed ADM), FP32 form (CUDA-core n = 8 kernels), advanced together by the
     batch (work-list kernels, CUDA graph per RK4 step, autotuned CTA shapes) for
     args.batch_steps steps; beside it the per-solve loop of the plain FP64 and
     FP32 forms timed on a sample of the same solves."""
@@ -446,8 +446,8 @@ def run_batch(args):
 def run_serve(args):
     """Served solves: args.requests Poisson arrivals (e log-uniform in [4,32],
     n ~ {6,8}, 200..2000 steps) served by the continuous-batching server under
-    a 150 GB budget in three forms: FP32 split precision for every request,
-    the accuracy-bounded mix (split precision where the step count keeps the
+    a 150 GB budget in three forms: FP32 (CUDA-core n = 8 kernels) for every
+    request, the accuracy-bounded mix (FP32 where the step count keeps the
     FP32 error under 1e-5, FP64 otherwise), and the plain FP64 per-request form
     (one solve at a time).  Every result is compared with its FP64 result."""
     import numpy as np
@@ -498,8 +498,9 @@ def main():
     ap.add_argument("--elements", type=int, default=64, help="elements per axis")
     ap.add_argument("--n", type=int, default=8, help="GLL nodes per axis")
     ap.add_argument("--precision", choices=["f64", "f32"], default="f64")
-    ap.add_argument("--fp32-form", choices=["bf16x3", "bf16x2", "cuda"], default="bf16x3",
-                    help="FP32 n=8 contractions: split BF16 tensor cores (three / two terms) or CUDA cores")
+    ap.add_argument("--fp32-form", choices=["bf16x3", "bf16x2", "cuda"], default="cuda",
+                    help="FP32 n=8 contractions: CUDA cores (FFMA, default) or split BF16 tensor cores "
+                         "(three / two terms)")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["solve", "batch", "serve"], default="solve",

@@ -134,8 +134,12 @@ int wt_mesh_set_bdry(wt_mesh* mesh, const int32_t* bdry);
  * initial data, min spacing, the strong form and reading those arrays return
  * WT_EINVAL.  No counterpart in the reference (Julia's GC owns its arrays). */
 int wt_mesh_release_setup_geometry(wt_mesh* mesh);
-/* Precision form of an FP32 mesh (WT_FP32_*; default WT_FP32_BF16X3).  No
- * counterpart in the reference (its T = Float32 path uses one form). */
+/* Precision form of an FP32 mesh's n = 8 contractions (WT_FP32_*; default
+ * WT_FP32_CUDA_CORES: FFMA contractions, exact FP32, the fastest form; the
+ * split-BF16 tensor-core forms are kept for the precision study).  Switching
+ * between the CUDA-core and the BF16 forms re-lays the mesh's metric blocks
+ * (synchronous).  No counterpart in the reference (its T = Float32 path uses
+ * one form). */
 int wt_mesh_set_fp32_form(wt_mesh* mesh, int form);
 /* _min_node_spacing_3d (src/evolve.jl:60-69); synchronous. */
 int wt_mesh_min_spacing(wt_mesh* mesh, double* h);

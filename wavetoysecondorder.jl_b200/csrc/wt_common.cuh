@@ -35,7 +35,7 @@ struct DevMesh {
   int N = 0;
   long long Ne = 0, nn = 0;
   int precision = 0;   // 0 = double, 1 = float
-  int fp32_form = 1;   // FP32 meshes, n = 8: WT_FP32_* of include/wavetoy_b200.h
+  int fp32_form = 0;   // FP32 meshes, n = 8: WT_FP32_* of include/wavetoy_b200.h (default CUDA cores)
   int ja_n8_layout = 0;  // layout Ja_n8 holds (0: Lay<real>, 1: LayC of the FP32 CUDA-core form)
   int affine = 1;      // 1 if every Jacobian is diagonal and constant per element
   int M[3] = {0, 0, 0};

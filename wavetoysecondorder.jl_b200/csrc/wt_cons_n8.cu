@@ -1123,13 +1123,14 @@ constexpr size_t K1C_STAGE = 9 * (size_t)n8::LayC::FS;
 constexpr size_t K1C_B = 15 * (size_t)n8::N3;
 constexpr size_t K2C_STAGE = (size_t)K2_NF * n8::LayC::FS;
 constexpr int K1C_OCC = 3, K2C_OCC = 3;
+constexpr int K2C_NS = 2;  // K2c flux + Ja stages (one stage at four CTAs per SM leaves 80 registers: spills)
 constexpr size_t k1c_smem() {
   return (K1C_STAGE + K1C_B + 9 * n8::LayC::FS + 2 * 6 * n8::N2 + 2 * n8::N3) * sizeof(float) + 64;
 }
 // K2c node-pass fields (1/J and the RK state: invJ, y, acc, comp), one bulk-copied buffer
 constexpr size_t K2C_B = 4 * (size_t)n8::N3;
 constexpr size_t k2c_smem() {
-  return (n8::NSTAGE * K2C_STAGE + 3 * n8::LayC::FS + 2 * 6 * 3 * n8::N2 + K2C_B) * sizeof(float) + 64;
+  return (K2C_NS * K2C_STAGE + 3 * n8::LayC::FS + 2 * 6 * 3 * n8::N2 + K2C_B) * sizeof(float) + 64;
 }
 
 template <bool BATCH>
@@ -1377,7 +1378,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
                   const int2* __restrict__ tiles, long long ntiles) {
   using namespace n8;
   using real = float;
-  constexpr int THR = CTHR, NS = NSTAGE, FSC = LayC::FS;
+  constexpr int THR = CTHR, NS = K2C_NS, FSC = LayC::FS;
   constexpr int NPT = (N3 + THR - 1) / THR;  // 3 node slots per thread
   constexpr int NFACE = 6 * 3 * N2;          // 1152 neighbour flux face values
   constexpr int NFR = NFACE / THR;           // 6 per thread
@@ -1388,7 +1389,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
   real* sB = sface + 2 * NFACE;                // node-pass fields: invJ, y, acc, comp (node order)
   uint64_t* bar = reinterpret_cast<uint64_t*>(sB + K2C_B);  // NS stage barriers, then the sB barrier
   __shared__ int abort_flag;
-  __shared__ int ftab[6 * N2];  // LayC offset of face-trace point pq on face fn of an element block
+  __shared__ short ftab[6 * N2];  // LayC offset of face-trace point pq on face fn of an element block
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int al = tid >> 6, pc = tid & 63;
   const real inv2H = (real)(1.0 / (2.0 * P.H[0]));
@@ -1414,7 +1415,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
   for (int pos = 0; pos < 8; ++pos) addr[pos] = LayC::at(pnode(al, pc, pos));
 
   for (int i = tid; i < 6 * N2; i += THR)
-    ftab[i] = LayC::at(face_node(faxis(i >> 6), frow(i >> 6, N), i & 7, (i >> 3) & 7, N));
+    ftab[i] = (short)LayC::at(face_node(faxis(i >> 6), frow(i >> 6, N), i & 7, (i >> 3) & 7, N));
   if (tid == 0) {
     abort_flag = 0;
     for (int k = 0; k <= NS; ++k) mbar_init(&bar[k], 1);
@@ -1509,7 +1510,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
       return;  // NS = 2: the only copy in flight is the one waited for
     }
     if (warp == 0) {
-      if (t1.x >= 0) issue(t1, (it + 1) % NS);
+      if (NS > 1 && t1.x >= 0) issue(t1, (it + 1) % NS);
       issueB(t0);  // lands while the contraction below runs
     }
     if (has_next) async_faces(t1, src1, fb ^ 1);
@@ -1556,6 +1557,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
     if (tid == 0 && !wait_phase(&bar[NS], it & 1, P.flag)) abort_flag = 1;
     __syncthreads();
     if (abort_flag) return;
+    if (NS == 1 && warp == 0 && t1.x >= 0) issue(t1, 0);  // one stage: refilled once the contraction has read it
 #pragma unroll
     for (int rr = 0; rr < NPT; ++rr) {
       const int node = tid + rr * THR;

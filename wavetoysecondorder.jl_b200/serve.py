@@ -65,7 +65,7 @@ def request_dt(req: Request, mesh) -> float:
     return 0.2 * mesh.min_spacing() / W.max_speed(p, 24)
 
 
-def build_solve(ctx, req: Request, precision: int, fp32_form: int = wt.FP32_BF16X3, release: bool = True):
+def build_solve(ctx, req: Request, precision: int, fp32_form: int = wt.FP32_CUDA_CORES, release: bool = True):
     """Mesh, background, workspace, initial data and dt of one request."""
     mesh = wt.Mesh.warped_uniform_hex(ctx, req.n, req.elements, 0.0, 1.0, 0.05, outer_tag=wt.SOMMERFELD_BDRY_TAG,
                                       precision=precision)
@@ -115,7 +115,7 @@ class Server:
     FP64 requests share the batch (they run as separate groups)."""
 
     def __init__(self, ctx, precision: int = wt.WT_F32, hbm_budget: float = 150e9, tick: int = 50,
-                 max_active: Optional[int] = None, fp32_form: int = wt.FP32_BF16X3, keep_results: bool = False,
+                 max_active: Optional[int] = None, fp32_form: int = wt.FP32_CUDA_CORES, keep_results: bool = False,
                  fill_nodes: Optional[int] = 8_000_000):
         """fill_nodes: admit further requests only while the running ones hold fewer
         nodes than this (about what keeps the GPU busy); beyond it, new requests
