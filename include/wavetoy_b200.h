@@ -115,16 +115,51 @@ int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* desc, wt_mesh** out);
  * coords (3,N,N,N,Ne), jac (3,3,N,N,N,Ne) = dx_a/dxi_b, neighbour /
  * neighbour_face (6,Ne) int32 1-based, orientation / bdry (6,Ne) int8.
  * Replaces HexSBPSAT.to_device(geom, backend) (src/evolve.jl:1191).
- * Orientation must be 0 in this build (WT_ENOTSUP otherwise). */
+ * The face orientation of every interior face is inferred from the node
+ * coordinates (the D4 map under which the two faces' nodes coincide, or differ
+ * by one constant shift for periodic faces); `orientation` may be NULL and is
+ * not read.  Faces that coincide under no such map give WT_EINVAL. */
 int wt_mesh_create_arrays(wt_ctx* ctx, int N, long long Ne, const double* coords, const double* jac,
                           const int32_t* neighbour, const int32_t* neighbour_face,
                           const int8_t* orientation, const int8_t* bdry, int precision, wt_mesh** out);
+/* Multi-patch curvilinear meshes of evolve3d's mesh kinds (src/evolve.jl:1176-1184;
+ * the builders are HexMeshes' make_cubed_cube_mesh / make_inflated_cube_mesh /
+ * make_radial_shell_mesh in the reference, restated with this library's own
+ * maps): WT_MESH_CUBED_CUBE (p = {R}: [-1,1]^3 around a centre cube [-R,R]^3,
+ * 7 M^3 elements), WT_MESH_INFLATED_CUBE (p = {L, R1, R2}: centre cube
+ * [-L,L]^3, a layer to the sphere R1 and a shell to R2, 13 M^3 elements),
+ * WT_MESH_RADIAL_SHELL (p = {R1, R2}: 6 M^3 elements).  Neighbours and face
+ * orientations come from matching node coordinates; outer faces get
+ * outer_tag, the radial shell's inner sphere inner_tag (the excision tag 8 in
+ * evolve3d). */
+enum { WT_MESH_CUBED_CUBE = 1, WT_MESH_INFLATED_CUBE = 2, WT_MESH_RADIAL_SHELL = 3 };
+typedef struct {
+  int kind;       /* WT_MESH_* */
+  int N;          /* nodes per axis, 2..8 */
+  int M;          /* elements per patch and axis */
+  double p[3];    /* kind parameters (above) */
+  int outer_tag;  /* tag of the outer faces (nonzero) */
+  int inner_tag;  /* radial shell: tag of the inner faces (nonzero) */
+  int precision;  /* WT_F64 or WT_F32 */
+} wt_patch_desc;
+int wt_mesh_create_patches(wt_ctx* ctx, const wt_patch_desc* desc, wt_mesh** out);
+/* The same mesh as host arrays (host only, no device work): *Ne, and when
+ * coords != NULL also coords (3,N,N,N,Ne), jac (9 per node, may be NULL),
+ * neighbour / neighbour_face (6,Ne, 1-based, 0 = none), orientation (6,Ne, the
+ * D4 code described at wt_mesh_get) and bdry (6,Ne).  Call once with
+ * coords = NULL for *Ne.  No counterpart in the reference (HexMeshes returns
+ * the mesh object). */
+int wt_patch_mesh_arrays(const wt_patch_desc* desc, long long* Ne, double* coords, double* jac, int32_t* neighbour,
+                         int32_t* neighbour_face, int32_t* orientation, int32_t* bdry);
 int wt_mesh_destroy(wt_mesh* mesh);
 int wt_mesh_info(const wt_mesh* mesh, int* N, long long* Ne, int* precision);
 /* Copy a geometry array to host (FP64): "coords" (3*nn), "jac", "invjac"
  * (9*nn), "detjac", "Hphys", "Hd", "invdetJ" (nn), "Ja" (9*nn, field-major:
  * Ja[(al*3+i)*nn + node] = J dxi_al/dx_i), "x","H" (N), "G" (N*N, G[i*N+p]);
- * int32 arrays: "bdry", "neighbour" (6*Ne, 1-based), "handedness" (Ne). */
+ * int32 arrays: "bdry", "neighbour" (6*Ne, 1-based), "neighbour_face" (6*Ne,
+ * 1-based, 0 where there is no neighbour), "orientation" (6*Ne: the D4 code
+ * ori whose map (p,q) -> (p',q') is: swap if ori & 4, then reverse p' if
+ * ori & 1 and q' if ori & 2), "handedness" (Ne). */
 int wt_mesh_get(const wt_mesh* mesh, const char* name, void* host_out);
 /* Override the outer-face tags (6,Ne) int32, e.g. to mark excision faces. */
 int wt_mesh_set_bdry(wt_mesh* mesh, const int32_t* bdry);

@@ -48,6 +48,8 @@ def lib():
         vp, d, i = C.c_void_p, C.c_double, C.c_int
         L.or_mesh_create.restype = vp
         L.or_mesh_create.argtypes = [i, i, i, i, d, d, d, i, i]
+        L.or_mesh_create_arrays.restype = vp
+        L.or_mesh_create_arrays.argtypes = [i, C.c_long, vp, vp, vp, vp, vp, vp]
         L.or_mesh_destroy.argtypes = [vp]
         L.or_mesh_ne.restype = C.c_long
         L.or_mesh_ne.argtypes = [vp]
@@ -126,6 +128,23 @@ class OracleMesh:
         self.Ne = int(lib().or_mesh_ne(self.h))
         self.nn = N ** 3 * self.Ne
         self.x0, self.x1, self.A, self.periodic, self.outer_tag = x0, x1, A, periodic, outer_tag
+
+    @classmethod
+    def from_arrays(cls, N, coords, jac, nbr, nbrf, orient, bdry):
+        """Mesh from arrays: coords (3*nn), jac (9*nn), 0-based topology (6*Ne: neighbour
+        element or -1, neighbour face 0..5, orientation code, boundary tag)."""
+        self = cls.__new__(cls)
+        c = np.ascontiguousarray(coords, dtype=np.float64)
+        J = np.ascontiguousarray(jac, dtype=np.float64)
+        ti = [np.ascontiguousarray(a, dtype=np.int32) for a in (nbr, nbrf, orient, bdry)]
+        Ne = ti[0].size // 6
+        self.N, self.M = N, None
+        self.h = lib().or_mesh_create_arrays(N, Ne, _p(c), _p(J), *[_p(a) for a in ti])
+        self.Ne = int(lib().or_mesh_ne(self.h))
+        self.nn = N ** 3 * self.Ne
+        self.x0 = self.x1 = self.A = None
+        self.periodic, self.outer_tag = False, None
+        return self
 
     def __del__(self):
         try:

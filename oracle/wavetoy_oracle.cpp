@@ -145,6 +145,19 @@ struct Mesh {
   long nn() const { return (long)N * N * N * Ne; }
 };
 
+// Neighbour element's node (a,b,c) coinciding with node (p,q) of face f of
+// element e.  Face orientation orient[f + 6e] is the D4 map of the library's
+// convention (include/wavetoy_b200.h, "orientation"): swap p and q if bit 2,
+// then reverse the first index if bit 0 and the second if bit 1.  This is
+// the role of _neigh_pq in _extract_face_oriented! (src/wave_strong_rhs.jl:41-73).
+inline void nbr_face_ijk(const Mesh& m, long e, int f, int p, int q, int& a, int& b, int& c) {
+  const int N = m.N, fn = m.nbrf[f + 6 * e], ori = m.orient[f + 6 * e];
+  int u = (ori & 4) ? q : p, v = (ori & 4) ? p : q;
+  if (ori & 1) u = N - 1 - u;
+  if (ori & 2) v = N - 1 - v;
+  face_ijk(faxis(fn), frow(fn, N), u, v, a, b, c);
+}
+
 // Reference derivative along axis d of field u (element-local, no scaling):
 // out[node] = sum_p G[idx_d(node), p] * u[node with idx_d = p].
 void ref_deriv(const Mesh& m, const double* u, double* out, int d, long e) {
@@ -230,6 +243,50 @@ void build_mesh(Mesh& m, int N, int Mx, int My, int Mz, double x0, double x1, do
           double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
           double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
           // inverse: invjac[al][be] = cof(J)[be][al] / det
+          double inv[3][3];
+          inv[0][0] = c00 / det;
+          inv[1][0] = c01 / det;
+          inv[2][0] = c02 / det;
+          inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+          inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+          inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+          inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+          inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+          inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) m.invjac[a + 3 * b + 9 * n] = inv[a][b];
+          m.detjac[n] = det;
+          m.Hphys[n] = m.ops.H[i] * m.ops.H[j] * m.ops.H[k] * std::fabs(det);
+        }
+    m.handed[e] = m.detjac[nid(N, 0, 0, 0, e)] < 0 ? -1 : 1;
+  }
+}
+
+// Mesh from arrays (coords (3,N,N,N,Ne), jac = dx_a/dxi_b, 0-based topology with
+// face orientations): invjac, detjac, Hphys and handedness from the Jacobian as
+// in build_mesh.
+void build_mesh_arrays(Mesh& m, int N, long Ne, const double* coords, const double* jac, const int32_t* nbr,
+                       const int32_t* nbrf, const int32_t* orient, const int32_t* bdry) {
+  m.N = N; m.Ne = Ne; m.M[0] = m.M[1] = m.M[2] = 0;
+  m.ops = make_ops(N);
+  const long nn = m.nn();
+  m.nbr.assign(nbr, nbr + 6 * Ne); m.nbrf.assign(nbrf, nbrf + 6 * Ne);
+  m.orient.assign(orient, orient + 6 * Ne); m.bdry.assign(bdry, bdry + 6 * Ne);
+  m.coords.assign(coords, coords + 3 * nn); m.jac.assign(jac, jac + 9 * nn);
+  m.invjac.assign(9 * nn, 0); m.detjac.assign(nn, 0); m.Hphys.assign(nn, 0); m.handed.assign(Ne, 1);
+#pragma omp parallel for schedule(static)
+  for (long e = 0; e < Ne; ++e) {
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          long n = nid(N, i, j, k, e);
+          double J[3][3];
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) J[a][b] = m.jac[a + 3 * b + 9 * n];
+          double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+          double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+          double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+          double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
           double inv[3][3];
           inv[0][0] = c00 / det;
           inv[1][0] = c01 / det;
@@ -345,7 +402,7 @@ void apply_D(const Mesh& m, const double* u, double* out, int d) {
         for (int p = 0; p < N; ++p) {
           int i, j, k, a, b, c;
           face_ijk(d, r, p, q, i, j, k);
-          face_ijk(faxis(fn), rn, p, q, a, b, c);
+          nbr_face_ijk(m, e, f, p, q, a, b, c);
           long n = nid(N, i, j, k, e), nb = nid(N, a, b, c, en);
           out[n] += nh * sc / (2.0 * H[r]) * (u[nb] - u[n]);
         }
@@ -390,7 +447,7 @@ void grad3d(const Mesh& m, const double* u, double* g1, double* g2, double* g3) 
           for (int p = 0; p < N; ++p) {
             int i, j, k, a, b, c;
             face_ijk(al, r, p, q, i, j, k);
-            face_ijk(faxis(fn), rn, p, q, a, b, c);
+            nbr_face_ijk(m, e, f, p, q, a, b, c);
             long t = nid(N, i, j, k, 0), nb = nid(N, a, b, c, en);
             double jump = u[nb] - ue[t];
             for (int ii = 0; ii < 3; ++ii)
@@ -439,7 +496,7 @@ void div3d(const Mesh& m, const double* F1, const double* F2, const double* F3, 
           for (int p = 0; p < N; ++p) {
             int i, j, k, a, b, c;
             face_ijk(al, r, p, q, i, j, k);
-            face_ijk(faxis(fn), rn, p, q, a, b, c);
+            nbr_face_ijk(m, e, f, p, q, a, b, c);
             long t = nid(N, i, j, k, 0), nb = nid(N, a, b, c, en);
             double s = 0.0;
             for (int ii = 0; ii < 3; ++ii)
@@ -568,6 +625,13 @@ void* or_mesh_create(int N, int Mx, int My, int Mz, double x0, double x1, double
                      int periodic, int outer_tag) {
   Mesh* m = new Mesh();
   build_mesh(*m, N, Mx, My, Mz, x0, x1, A, periodic, outer_tag);
+  build_metric(*m);
+  return m;
+}
+void* or_mesh_create_arrays(int N, long Ne, const double* coords, const double* jac, const int32_t* nbr,
+                            const int32_t* nbrf, const int32_t* orient, const int32_t* bdry) {
+  Mesh* m = new Mesh();
+  build_mesh_arrays(*m, N, Ne, coords, jac, nbr, nbrf, orient, bdry);
   build_metric(*m);
   return m;
 }
@@ -871,7 +935,7 @@ void or_rhs_sipg(void* h, const double* u, const double* ut, double* utt, const 
             double s = m.invjac[d + 3 * d + 9 * n];
             double du, dGu;
             if (tag == 0) {
-              int a, b, c; face_ijk(faxis(fn), rn, p, q, a, b, c);
+              int a, b, c; nbr_face_ijk(m, e, f, p, q, a, b, c);
               long nb = nid(N, a, b, c, en);
               du = u[n] - u[nb];
               dGu = Du[d * nn + n] - Du[d * nn + nb];
@@ -962,7 +1026,7 @@ void or_rhs_strong(void* h, const double* u, const double* ut, double* utt, doub
         for (int q = 0; q < N; ++q)
           for (int p = 0; p < N; ++p) {
             double v = 0.0;
-            if (en >= 0) { int a, b, c; face_ijk(faxis(fn), rn, p, q, a, b, c); v = u[nid(N, a, b, c, en)]; }
+            if (en >= 0) { int a, b, c; nbr_face_ijk(m, e, f, p, q, a, b, c); v = u[nid(N, a, b, c, en)]; }
             uface[f * N * N + p + N * q] = v;
           }
       }
@@ -1068,7 +1132,7 @@ void or_lap_strong_cons(void* h, const double* u, double* Lu, double hel, double
             int i, j, k; face_ijk(al, fr, p, q, i, j, k);
             long t = nid(N, i, j, k, 0);
             double uf = 0.0;
-            if (en >= 0) { int a, b, c; face_ijk(faxis(fn), rn, p, q, a, b, c); uf = u[nid(N, a, b, c, en)]; }
+            if (en >= 0) { int a, b, c; nbr_face_ijk(m, e, f, p, q, a, b, c); uf = u[nid(N, a, b, c, en)]; }
             out[t] += coef_neu * du[al * ne3 + t];
             out[t] += coef_dir * (ue[t] - uf);
           }
@@ -1110,7 +1174,7 @@ void or_rhs_curved4(void* h, const double* phi, const double* phid, double* phid
           for (int p = 0; p < N; ++p) {
             double a_ = 0.0, b_ = 0.0;
             if (en >= 0) {
-              int a, b, c; face_ijk(faxis(fn), rn, p, q, a, b, c);
+              int a, b, c; nbr_face_ijk(m, e, f, p, q, a, b, c);
               a_ = phi[nid(N, a, b, c, en)]; b_ = phid[nid(N, a, b, c, en)];
             }
             uf[f * N * N + p + N * q] = a_; vf[f * N * N + p + N * q] = b_;

@@ -146,7 +146,8 @@ int finish_topology(wt_mesh* mh) {
         if (m.h_bdry[i] != 0) emask[e] |= 64;
         else if (m.h_nbr[i] >= 0) {
           emask[e] |= 1 << f;
-          fsrc[i] = 8 * m.h_nbr[i] + m.h_nbrf[i];
+          fsrc[i] = 64 * m.h_nbr[i] + m.h_nbrf[i];  // h_nbrf = fn | ori << 3
+          if (m.h_nbrf[i] >> 3) m.has_ori = 1;
         }
       }
     WT_TRY(dalloc(ctx, &m.emask, Ne * sizeof(int32_t), &mh->owned));
@@ -171,6 +172,11 @@ int finish_topology(wt_mesh* mh) {
       int en = m.h_nbr[2 * d + 6 * e];
       return en >= 0 && m.h_nbrf[2 * d + 6 * e] == 2 * d + 1 && m.h_bdry[2 * d + 6 * e] == 0;
     };
+    // a face that couples to a neighbour (apply_D!'s SAT) but does not continue
+    // a straight line: a line may not end there (multi-patch meshes)
+    auto coupled = [&](long long e, int f) -> bool { return m.h_nbr[f + 6 * e] >= 0 && m.h_bdry[f + 6 * e] == 0; };
+    for (long long e = 0; e < Ne && ok; ++e)
+      if ((coupled(e, 2 * d + 1) && fwd(e) < 0) || (coupled(e, 2 * d) && !has_back(e))) ok = false;
     for (long long e0 = 0; e0 < Ne && ok; ++e0) {
       if (seen[e0] || has_back(e0)) continue;
       std::vector<int32_t> ln;
@@ -397,8 +403,9 @@ int rhs_curved_impl(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi
   ctx->launches += 2;
   if (eps_ko != 0.0) {
     const double koT = eps_ko * ws->inv_mu5;
-    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Phid, Phi, koT, ctx->stream), "Kreiss-Oliger"));
-    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Pid, Pi, koT, ctx->stream), "Kreiss-Oliger"));
+    // the flux scratch is free once K2 has run
+    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Phid, Phi, koT, ctx->stream, ws->F), "Kreiss-Oliger"));
+    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Pid, Pi, koT, ctx->stream, ws->F), "Kreiss-Oliger"));
     ctx->launches += 6;
   }
   return 0;
@@ -572,36 +579,19 @@ int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* d, wt_mesh** out) {
   return 0;
 }
 
-int wt_mesh_create_arrays(wt_ctx* ctx, int N, long long Ne, const double* coords, const double* jac,
-                          const int32_t* neighbour, const int32_t* neighbour_face, const int8_t* orientation,
-                          const int8_t* bdry, int precision, wt_mesh** out) {
-  if (!ctx) return WT_EINVAL;
-  if (!out || !coords || !jac || !neighbour || !neighbour_face || !bdry)
-    return fail(ctx, WT_EINVAL, "wt_mesh_create_arrays: NULL argument");
-  *out = nullptr;
-  if (N < 2 || N > WT_MAXN) return fail(ctx, WT_EINVAL, "N must be in 2..8");
-  if (Ne < 1) return fail(ctx, WT_EINVAL, "Ne must be >= 1");
-  if (precision != WT_F64 && precision != WT_F32) return fail(ctx, WT_EINVAL, "bad precision");
-  if (orientation)
-    for (long long i = 0; i < 6 * Ne; ++i)
-      if (orientation[i] != 0)
-        return fail(ctx, WT_ENOTSUP, "face orientation != 0 is not supported by this build");
+}  // extern "C"
+
+// A mesh from host coordinates, Jacobian and 0-based topology (nbrf = fn | ori << 3).
+static int create_from_host(wt_ctx* ctx, int N, long long Ne, const double* coords, const double* jac,
+                            std::vector<int32_t>& nbr, std::vector<int32_t>& nbrf, std::vector<int32_t>& bdry,
+                            int precision, wt_mesh** out) {
   cudaSetDevice(ctx->device);
   auto* mh = new wt_mesh();
   mh->ctx = ctx;
   wt::DevMesh& m = mh->m;
   m.errflag = ctx->d_flag;
   m.N = N; m.Ne = Ne; m.nn = Ne * N * N * N; m.precision = precision; m.affine = 0;
-  m.h_nbr.resize(6 * Ne); m.h_nbrf.resize(6 * Ne); m.h_bdry.resize(6 * Ne);
-  for (long long i = 0; i < 6 * Ne; ++i) {
-    const int en = neighbour[i];
-    if (en < 0 || en > Ne) { delete mh; return fail(ctx, WT_EINVAL, "neighbour index out of range"); }
-    m.h_nbr[i] = en - 1;
-    const int fn = neighbour_face[i];
-    if (en > 0 && (fn < 1 || fn > 6)) { delete mh; return fail(ctx, WT_EINVAL, "neighbour_face out of range"); }
-    m.h_nbrf[i] = en > 0 ? fn - 1 : 0;
-    m.h_bdry[i] = bdry[i];
-  }
+  m.h_nbr.swap(nbr); m.h_nbrf.swap(nbrf); m.h_bdry.swap(bdry);
   int rc = finish_topology(mh);
   if (!rc) rc = alloc_geometry(mh);
   if (!rc) {
@@ -611,6 +601,114 @@ int wt_mesh_create_arrays(wt_ctx* ctx, int N, long long Ne, const double* coords
   }
   if (rc) { free_mesh(mh); delete mh; return rc; }
   *out = mh;
+  return 0;
+}
+
+extern "C" {
+
+int wt_mesh_create_arrays(wt_ctx* ctx, int N, long long Ne, const double* coords, const double* jac,
+                          const int32_t* neighbour, const int32_t* neighbour_face, const int8_t* orientation,
+                          const int8_t* bdry, int precision, wt_mesh** out) {
+  (void)orientation;  // inferred from the coordinates
+  if (!ctx) return WT_EINVAL;
+  if (!out || !coords || !jac || !neighbour || !neighbour_face || !bdry)
+    return fail(ctx, WT_EINVAL, "wt_mesh_create_arrays: NULL argument");
+  *out = nullptr;
+  if (N < 2 || N > WT_MAXN) return fail(ctx, WT_EINVAL, "N must be in 2..8");
+  if (Ne < 1) return fail(ctx, WT_EINVAL, "Ne must be >= 1");
+  if (precision != WT_F64 && precision != WT_F32) return fail(ctx, WT_EINVAL, "bad precision");
+  std::vector<int32_t> nbr(6 * Ne), nbrf(6 * Ne), bd(6 * Ne);
+  double scale = 0.0;
+  for (long long i = 0; i < 3 * Ne * N * N * N; ++i) scale = std::max(scale, std::fabs(coords[i]));
+  const double tol = 1e-9 * (scale > 0.0 ? scale : 1.0);
+  for (long long i = 0; i < 6 * Ne; ++i) {
+    const int en = neighbour[i];
+    if (en < 0 || en > Ne) return fail(ctx, WT_EINVAL, "neighbour index out of range");
+    nbr[i] = en - 1;
+    const int fn = neighbour_face[i];
+    if (en > 0 && (fn < 1 || fn > 6)) return fail(ctx, WT_EINVAL, "neighbour_face out of range");
+    bd[i] = bdry[i];
+    nbrf[i] = 0;
+    if (en > 0) {
+      const long long e = i / 6;
+      const int f = (int)(i % 6);
+      int ori = wt::infer_orientation(N, coords, e, f, en - 1, fn - 1, tol, false);
+      if (ori < 0) ori = wt::infer_orientation(N, coords, e, f, en - 1, fn - 1, tol, true);  // periodic faces
+      if (ori < 0)
+        return fail(ctx, WT_EINVAL, "face " + std::to_string(f + 1) + " of element " + std::to_string(e + 1) +
+                                        " does not coincide with its neighbour's face under any orientation");
+      nbrf[i] = (fn - 1) | (ori << 3);
+    }
+  }
+  return create_from_host(ctx, N, Ne, coords, jac, nbr, nbrf, bd, precision, out);
+}
+
+}  // extern "C"
+
+// Host arrays of a WT_MESH_* patch mesh (0-based topology, nbrf = fn | ori << 3);
+// "" or the reason it was refused.
+static std::string patch_arrays(const wt_patch_desc* d, std::vector<double>& X, std::vector<double>& J,
+                                std::vector<int32_t>& nbr, std::vector<int32_t>& nbrf, std::vector<int32_t>& bd) {
+  if (d->N < 2 || d->N > WT_MAXN) return "N must be in 2..8";
+  if (d->M < 1 || d->M > 64) return "M must be in 1..64";
+  if (d->precision != WT_F64 && d->precision != WT_F32) return "bad precision";
+  if (d->outer_tag == 0 || (d->kind == WT_MESH_RADIAL_SHELL && d->inner_tag == 0))
+    return "outer_tag (and the radial shell's inner_tag) must be nonzero";
+  const wt::HostOps ops = wt::gll_operators(d->N);
+  double scale = 1.0;
+  const int brc = wt::build_patch_mesh(d->kind, d->N, d->M, d->p, ops.x, X, scale);
+  if (brc == -2) return "unknown mesh kind " + std::to_string(d->kind);
+  if (brc) return "bad mesh parameters for kind " + std::to_string(d->kind);
+  const long long N3 = (long long)d->N * d->N * d->N, Ne = (long long)X.size() / (3 * N3);
+  if (wt::match_faces(d->N, Ne, X.data(), 1e-9 * scale, nbr, nbrf)) return "inconsistent face matching";
+  bd.assign(6 * Ne, 0);
+  for (long long i = 0; i < 6 * Ne; ++i) {
+    if (nbr[i] >= 0) continue;
+    int tag = d->outer_tag;
+    if (d->kind == WT_MESH_RADIAL_SHELL) {  // inner or outer sphere: the radius of the face's first node
+      const long long e = i / 6;
+      const int f = (int)(i % 6);
+      const double* x = &X[3 * (e * N3 + wt::face_node(wt::faxis(f), wt::frow(f, d->N), 0, 0, d->N))];
+      if (std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]) < 0.5 * (d->p[0] + d->p[1])) tag = d->inner_tag;
+    }
+    bd[i] = tag;
+  }
+  J.assign(9 * N3 * Ne, 0.0);
+  wt::coords_jacobian(d->N, Ne, X.data(), ops.G, J.data());
+  return "";
+}
+
+extern "C" {
+
+int wt_mesh_create_patches(wt_ctx* ctx, const wt_patch_desc* d, wt_mesh** out) {
+  if (!ctx) return WT_EINVAL;
+  if (!d || !out) return fail(ctx, WT_EINVAL, "wt_mesh_create_patches: NULL argument");
+  *out = nullptr;
+  std::vector<double> X, J;
+  std::vector<int32_t> nbr, nbrf, bd;
+  const std::string why = patch_arrays(d, X, J, nbr, nbrf, bd);
+  if (!why.empty()) return fail(ctx, WT_EINVAL, "wt_mesh_create_patches: " + why);
+  const long long Ne = (long long)nbr.size() / 6;
+  return create_from_host(ctx, d->N, Ne, X.data(), J.data(), nbr, nbrf, bd, d->precision, out);
+}
+
+int wt_patch_mesh_arrays(const wt_patch_desc* d, long long* Ne, double* coords, double* jac, int32_t* neighbour,
+                         int32_t* neighbour_face, int32_t* orientation, int32_t* bdry) {
+  if (!d || !Ne) return WT_EINVAL;
+  std::vector<double> X, J;
+  std::vector<int32_t> nbr, nbrf, bd;
+  if (!patch_arrays(d, X, J, nbr, nbrf, bd).empty()) return WT_EINVAL;
+  const long long ne = (long long)nbr.size() / 6;
+  *Ne = ne;
+  if (!coords) return 0;
+  std::memcpy(coords, X.data(), X.size() * sizeof(double));
+  if (jac) std::memcpy(jac, J.data(), J.size() * sizeof(double));
+  for (long long i = 0; i < 6 * ne; ++i) {
+    if (neighbour) neighbour[i] = nbr[i] + 1;
+    if (neighbour_face) neighbour_face[i] = nbr[i] < 0 ? 0 : (nbrf[i] & 7) + 1;
+    if (orientation) orientation[i] = nbr[i] < 0 ? 0 : nbrf[i] >> 3;
+    if (bdry) bdry[i] = bd[i];
+  }
   return 0;
 }
 
@@ -652,6 +750,12 @@ int wt_mesh_get(const wt_mesh* mh, const char* name, void* host_out) {
   else if (s == "neighbour") {
     int32_t* o = (int32_t*)host_out;
     for (long long i = 0; i < 6 * m.Ne; ++i) o[i] = m.h_nbr[i] + 1;
+    return 0;
+  } else if (s == "neighbour_face" || s == "orientation") {  // 1-based face; D4 code of face_perm
+    int32_t* o = (int32_t*)host_out;
+    const bool face = s == "neighbour_face";
+    for (long long i = 0; i < 6 * m.Ne; ++i)
+      o[i] = m.h_nbr[i] < 0 ? 0 : face ? (m.h_nbrf[i] & 7) + 1 : m.h_nbrf[i] >> 3;
     return 0;
   } else if (s == "handedness") { src = m.handed; bytes = m.Ne * sizeof(int32_t); }
   else return fail(ctx, WT_EINVAL, "wt_mesh_get: unknown array '" + s + "'");
@@ -862,8 +966,10 @@ int wt_ko_add(wt_ctx* ctx, wt_ws* ws, void* dst, const void* field, double eps_k
   WT_TRY(check_ws(ctx, ws));
   if (!dst || !field) return fail(ctx, WT_EINVAL, "wt_ko_add: NULL argument");
   WT_TRY(ensure_mu(ws));
+  WT_TRY(ws_buffers(ws));
   ctx->launches += 3;
-  return lrc(ctx, wt::launch_ko_add(ws->mesh->m, dst, field, eps_ko * ws->inv_mu5, ctx->stream), "Kreiss-Oliger");
+  return lrc(ctx, wt::launch_ko_add(ws->mesh->m, dst, field, eps_ko * ws->inv_mu5, ctx->stream, ws->F),
+             "Kreiss-Oliger");
 }
 
 int wt_gradient3d(wt_ctx* ctx, wt_ws* ws, const void* u, void* g1, void* g2, void* g3) {
@@ -1123,8 +1229,8 @@ static int step_sipg_once(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, 
     cudaMemcpyAsync(ws->kP, inV, nb, cudaMemcpyDeviceToDevice, s);
     if (eps_ko != 0.0) {
       const double koT = eps_ko * ws->inv_mu5;
-      WT_TRY(lrc(ctx, wt::launch_ko_add(m, ws->kP, inU, koT, s), "Kreiss-Oliger"));
-      WT_TRY(lrc(ctx, wt::launch_ko_add(m, ws->kQ, inV, koT, s), "Kreiss-Oliger"));
+      WT_TRY(lrc(ctx, wt::launch_ko_add(m, ws->kP, inU, koT, s, ws->F), "Kreiss-Oliger"));
+      WT_TRY(lrc(ctx, wt::launch_ko_add(m, ws->kQ, inV, koT, s, ws->F), "Kreiss-Oliger"));
       ctx->launches += 6;
     }
     WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, st, dt, u, ws->accP, ws->S0, ws->kP, s), "rk4"));
@@ -1142,6 +1248,7 @@ int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int n
   if (!ws->mesh->m.affine) return fail(ctx, WT_ENOTSUP, "SIPG stepping supports affine meshes only");
   WT_TRY(ws_step_buffers(ws));
   WT_TRY(ws_k_buffers(ws));
+  WT_TRY(ws_buffers(ws));  // Kreiss-Oliger scratch (allocated before any graph capture)
   if (eps_ko != 0.0) WT_TRY(ensure_mu(ws));
   const wt::DevMesh& m = ws->mesh->m;
   WT_TRY(ensure(ws, &ws->trace, (size_t)6 * m.N * m.N * m.Ne * rsize(m.precision)));
@@ -1748,8 +1855,9 @@ int wt_rhs_curved_noalloc(wt_ctx* ctx, const wt_coef* coef, const void* Phi, con
   ctx->launches += 2;
   if (eps_ko != 0.0) {
     const double koT = eps_ko * std::pow(1.0 / mu, 5);
-    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Phidot, Phi, koT, ctx->stream), "Kreiss-Oliger"));
-    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Pidot, Pi, koT, ctx->stream), "Kreiss-Oliger"));
+    // the flux scratch is free once K2 has run
+    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Phidot, Phi, koT, ctx->stream, F), "Kreiss-Oliger"));
+    WT_TRY(lrc(ctx, wt::launch_ko_add(m, Pidot, Pi, koT, ctx->stream, F), "Kreiss-Oliger"));
     ctx->launches += 6;
   }
   return 0;

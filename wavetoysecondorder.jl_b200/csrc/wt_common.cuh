@@ -68,8 +68,9 @@ struct DevMesh {
   // per element: bits 0-5 faces that get the centred-flux SAT (interior face with a
   // neighbour), bit 6 element has an outer face
   int32_t* emask = nullptr;
-  // per (f,e): 8 * neighbour element + neighbour face for SAT faces, -1 otherwise
+  // per (f,e): 64 * neighbour element + 8 * orientation + neighbour face for SAT faces, -1 otherwise
   int32_t* fsrc = nullptr;
+  int has_ori = 0;           // some face has orientation != 0 (multi-patch mesh)
   // boundary faces: slot per (f,e) with bdry != 0, -1 otherwise
   int32_t* bslot = nullptr;
   int nbf = 0;
@@ -119,6 +120,37 @@ __host__ __device__ inline int face_node(int ax, int r, int p, int q, int N) {
   // local node index of face node (p,q) of the face with axis ax at row r
   return ax == 0 ? r + N * (p + N * q) : ax == 1 ? p + N * (r + N * q) : p + N * (q + N * r);
 }
+// Face orientation: the neighbour's face node (pn, qn) that coincides with this
+// face's node (p, q), for the D4 element ori (bit 2: swap p and q; bit 0:
+// reverse the first index; bit 1: reverse the second).  ori = 0 is the
+// identity (aligned patches); the library infers ori from the node
+// coordinates when it builds the topology.  Encodings: nbrf[f + 6e] = fn |
+// ori << 3; fsrc[f + 6e] = 64 nbr + 8 ori + fn.
+__host__ __device__ inline void face_perm(int ori, int p, int q, int N, int& pn, int& qn) {
+  const int a = (ori & 4) ? q : p, b = (ori & 4) ? p : q;
+  pn = (ori & 1) ? N - 1 - a : a;
+  qn = (ori & 2) ? N - 1 - b : b;
+}
+// neighbour face node for face source fs = 64 nbr + 8 ori + fn (node within the neighbour element)
+__host__ __device__ inline int nbr_face_node(int fs, int p, int q, int N) {
+  const int fn = fs & 7;
+  int pn, qn;
+  face_perm((fs >> 3) & 7, p, q, N, pn, qn);
+  return face_node(faxis(fn), frow(fn, N), pn, qn, N);
+}
+
+// ---- meshes built from node coordinates (wt_patches.cu, host) ----------------------
+// D4 orientation under which face (e,f)'s nodes coincide with face (en,fn)'s
+// (within tol; with shift, up to one constant translation); -1 if none
+int infer_orientation(int N, const double* X, long long e, int f, long long en, int fn, double tol, bool shift);
+// neighbours (-1: none) and nbrf = fn | ori << 3 of every face, by matching coordinates; -1 on inconsistency
+int match_faces(int N, long long Ne, const double* X, double tol, std::vector<int32_t>& nbr,
+                std::vector<int32_t>& nbrf);
+// jac[a + 3 b + 9 n] = SBP derivative of the node coordinates along xi_b
+void coords_jacobian(int N, long long Ne, const double* X, const std::vector<double>& G, double* jac);
+// node coordinates of a WT_MESH_* multi-patch mesh; scale = the domain's size; -1 bad parameters, -2 bad kind
+int build_patch_mesh(int kind, int N, int M, const double p[3], const std::vector<double>& xg,
+                     std::vector<double>& X, double& scale);
 
 // ---- error reporting ----------------------------------------------------------------
 struct Status {
@@ -211,7 +243,9 @@ size_t cons_gen_param_size(int precision, int which);
 void cons_gen_fill_params(int which, const SolveStage& ss, unsigned* flag, void* dst);
 int launch_cons_gen_batch(int which, int N, int precision, int epb_variant, const void* plist, const int2* tiles,
                           long long ntiles, cudaStream_t s);
-int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s);
+// dst += koT * sum_d D_d^6 field; scratch (2 nn words, may be NULL when every
+// axis has straight element lines) serves meshes without them
+int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s, void* scratch);
 int launch_div3d(const DevMesh& m, const void* F, void* out, cudaStream_t s);
 
 // second-order forms (wt_second.cu)

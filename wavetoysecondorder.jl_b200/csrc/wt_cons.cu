@@ -176,8 +176,8 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
     const int f = idx / N2, pq = idx - f * N2;
     real v = 0;
     if ((emask >> f) & 1) {
-      const int src = P.fsrc[f + 6 * ec], fn = src & 7;
-      v = P.Phi[(long long)(src >> 3) * N3 + face_node(faxis(fn), frow(fn, N), pq % N, pq / N, N)];
+      const int src = P.fsrc[f + 6 * ec];
+      v = P.Phi[(long long)(src >> 6) * N3 + nbr_face_node(src, pq % N, pq / N, N)];
     }
     sun[le][f][pq] = v;
   }
@@ -400,8 +400,8 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
     const int f = idx / N2, pq = idx - f * N2;
     long long src = -1;
     if ((emask >> f) & 1) {
-      const int fs = P.fsrc[f + 6 * ec], fn = fs & 7;
-      src = (long long)(fs >> 3) * N3 + face_node(faxis(fn), frow(fn, N), pq % N, pq / N, N);
+      const int fs = P.fsrc[f + 6 * ec];
+      src = (long long)(fs >> 6) * N3 + nbr_face_node(fs, pq % N, pq / N, N);
     }
     if (CURV) {
 #pragma unroll
@@ -504,9 +504,8 @@ __global__ void __launch_bounds__(Ep<N>::T) k_apply_D(long long Ne, const real* 
     if (bdry[f + 6 * ec] != 0) continue;
     const int en = nbr[f + 6 * ec];
     if (en < 0) continue;
-    const int fn = nbrf[f + 6 * ec];
     const int p = d == 0 ? j : i, q = d == 2 ? j : k;
-    const real un = u[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), p, q, N)];
+    const real un = u[(long long)en * N3 + nbr_face_node(nbrf[f + 6 * ec], p, q, N)];
     const real nh = (f & 1) ? (real)1 : (real)-1;
     r += nh * s / ((real)2 * (real)H[0]) * (un - uv);
   }
@@ -783,11 +782,34 @@ int launch_apply_D(const DevMesh& m, const void* u, void* out, int d, cudaStream
   }
 }
 
+template <typename real>
+__global__ void k_axpy(long long n, real a, const real* __restrict__ x, real* __restrict__ y) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] += a * x[i];
+}
+
+// Kreiss-Oliger along axis d: on whole grid lines in shared memory where the
+// elements form straight lines along d (k_ko_line), otherwise as the
+// reference's _ko_axis3! does it (src/wave3d_curved.jl:182-192): six apply_D!
+// calls ping-ponging through scratch (2 nn words), then dst += koT * result.
+// The second form serves multi-patch meshes, whose axis-d neighbours may meet
+// at another face or orientation.
 template <int N, typename real>
-static int ko_dispatch(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s) {
+static int ko_dispatch(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s, void* scratch) {
   for (int d = 0; d < 3; ++d) {
     const int len = m.line_len[d];
-    if (!m.line_ok[d] || len * N > 1024) return -4;
+    if (!m.line_ok[d] || len * N > 1024) {
+      if (!scratch) return -4;
+      real* buf[2] = {(real*)scratch, (real*)scratch + m.nn};
+      const real* src = (const real*)field;
+      for (int r = 0; r < 6; ++r) {
+        if (applyD_dispatch<N, real>(m, src, buf[r & 1], d, s)) return -2;
+        src = buf[r & 1];
+      }
+      k_axpy<real><<<4096, 256, 0, s>>>(m.nn, (real)koT, src, (real*)dst);
+      if (cudaGetLastError() != cudaSuccess) return -2;
+      continue;
+    }
     dim3 grid((unsigned)m.nlines[d], N);
     size_t smem = (size_t)N * len * N * sizeof(real);
     if (smem > 48 * 1024)
@@ -799,11 +821,11 @@ static int ko_dispatch(const DevMesh& m, void* dst, const void* field, double ko
   return 0;
 }
 
-int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s) {
+int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cudaStream_t s, void* scratch) {
   if (m.precision == 0) {
-    WT_DISPATCH_N(m.N, (ko_dispatch<NN, double>(m, dst, field, koT, s)));
+    WT_DISPATCH_N(m.N, (ko_dispatch<NN, double>(m, dst, field, koT, s, scratch)));
   } else {
-    WT_DISPATCH_N(m.N, (ko_dispatch<NN, float>(m, dst, field, koT, s)));
+    WT_DISPATCH_N(m.N, (ko_dispatch<NN, float>(m, dst, field, koT, s, scratch)));
   }
 }
 

@@ -474,8 +474,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
   auto src_load = [&](int2 tl) -> int { return (tl.x >= 0 && tid < 6 * N2) ? prm(tl.x).fsrc[my_f + 6 * tl.y] : -1; };
   auto face_load = [&](int src, int sidx) -> real {
     if (src < 0) return (real)0;
-    const int fn = src & 7;
-    return prm(sidx).Phi[(long long)(src >> 3) * N3 + face_node(faxis(fn), frow(fn, N), my_pq & 7, my_pq >> 3, N)];
+    return prm(sidx).Phi[(long long)(src >> 6) * N3 + nbr_face_node(src, my_pq & 7, my_pq >> 3, N)];
   };
   auto emask_at = [&](int2 tl) -> int { return tl.x >= 0 ? prm(tl.x).emask[tl.y] : 0; };
   // pointwise fields of this thread's node
@@ -835,10 +834,8 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
       if (src[r] >= 0) {
         const K2N8<real>& Q = prm(sidx);
         const int rem = idx % (3 * N2), c = rem >> 6, pq = rem & 63;
-        const int fn = src[r] & 7;
         const real* Fc = c == 0 ? Q.F0 : c == 1 ? Q.F1 : Q.F2;
-        const int fnode = face_node(faxis(fn), frow(fn, N), pq & 7, pq >> 3, N);
-        v = Fc[(long long)(src[r] >> 3) * FS + Lay<real>::at(fnode)];
+        v = Fc[(long long)(src[r] >> 6) * FS + Lay<real>::at(nbr_face_node(src[r], pq & 7, pq >> 3, N))];
       }
       fv[r] = v;
     }
@@ -1097,6 +1094,13 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src, bool valid
                : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// index into a per-CTA table of the 6 x 64 face nodes for face source fs and
+// this face's point pq: the neighbour face's point after the orientation
+__device__ __forceinline__ int face_slot(int fs, int pq) {
+  int pn, qn;
+  face_perm((fs >> 3) & 7, pq & 7, pq >> 3, N, pn, qn);
+  return ((fs & 7) << 6) + pn + 8 * qn;
+}
 // node at position pos of pencil pc along axis al; pc = a + 8 b numbers the
 // other two axes in increasing order, so it is also the pencil's face index
 __device__ __forceinline__ int pnode(int al, int pc, int pos) {
@@ -1232,7 +1236,7 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
       const int idx = tid + r * THR;
       if (idx < NFT) {
         const bool ok = src[r] >= 0;
-        const real* g = ok ? Q.Phi + (long long)(src[r] >> 3) * N3 + ftab[((src[r] & 7) << 6) + (idx & 63)] : Q.Phi;
+        const real* g = ok ? Q.Phi + (long long)(src[r] >> 6) * N3 + ftab[face_slot(src[r], idx & 63)] : Q.Phi;
         cp_async4(sface + b * NFT + idx, g, ok);
       }
     }
@@ -1452,7 +1456,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
 #pragma unroll
     for (int r = 0; r < NFR; ++r) {
       const bool ok = src[r] >= 0;
-      const real* g = ok ? Fc + (long long)(src[r] >> 3) * FSC + ftab[((src[r] & 7) << 6) + pq] : Fc;
+      const real* g = ok ? Fc + (long long)(src[r] >> 6) * FSC + ftab[face_slot(src[r], pq)] : Fc;
       cp_async4(sface + b * NFACE + r * THR + tid, g, ok);
     }
   };

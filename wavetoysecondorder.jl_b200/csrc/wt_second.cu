@@ -124,8 +124,8 @@ __global__ void __launch_bounds__(Sp<N>::T) k_sipg_rhs(const SipgP<real> P) {
       const int ax = f >> 1;
       const int fl = face_node(ax, frow(f, N), pq % N, pq / N, N);
       if (tag == 0 && en >= 0) {
-        const int fn = P.nbrf[f + 6 * ec];
-        du = su[le][fl] - P.u[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq % N, pq / N, N)];
+        const int fs = P.nbrf[f + 6 * ec];  // fn | ori << 3
+        du = su[le][fl] - P.u[(long long)en * N3 + nbr_face_node(fs, pq % N, pq / N, N)];
       } else if (tag >= 1 && tag <= 6) {
         du = su[le][fl] - P.bv[tag - 1];
       }
@@ -156,8 +156,10 @@ __global__ void __launch_bounds__(Sp<N>::T) k_sipg_rhs(const SipgP<real> P) {
     if (l == r) {
       real dGu = 0;
       if (interior) {
-        const int fn = P.nbrf[f + 6 * ec];
-        dGu = D[ax] - P.trace[((long long)6 * en + fn) * N2 + p + N * q];
+        const int fs = P.nbrf[f + 6 * ec];  // fn | ori << 3
+        int pn, qn;
+        face_perm((fs >> 3) & 7, p, q, N, pn, qn);
+        dGu = D[ax] - P.trace[((long long)6 * en + (fs & 7)) * N2 + pn + N * qn];
       }
       acc += -P.tau * s * s / Hs[r] * du;
       acc += (real)-0.5 * nh * s / Hs[r] * dGu;
@@ -223,8 +225,8 @@ __global__ void __launch_bounds__(Sp<N>::T) k_strong(const StrongP<real> P) {
     if (valid) {
       const int en = P.nbr[f + 6 * ec];
       if (en >= 0) {
-        const int fn = P.nbrf[f + 6 * ec];
-        v = (double)P.u[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), pq % N, pq / N, N)];
+        const int fs = P.nbrf[f + 6 * ec];  // fn | ori << 3
+        v = (double)P.u[(long long)en * N3 + nbr_face_node(fs, pq % N, pq / N, N)];
       }
     }
     suf[le][f][pq] = v;
@@ -342,8 +344,8 @@ __global__ void __launch_bounds__(Sp<N>::T) k_lap_strong_cons(long long Ne, cons
     double uf = 0.0;
     const int en = nbr[f + 6 * ec];
     if (en >= 0) {
-      const int fn = nbrf[f + 6 * ec];
-      uf = (double)u[(long long)en * N3 + face_node(faxis(fn), frow(fn, N), p, q, N)];
+      const int fs = nbrf[f + 6 * ec];  // fn | ori << 3
+      uf = (double)u[(long long)en * N3 + nbr_face_node(fs, p, q, N)];
     }
     s += coef_neu * du[al];
     s += coef_dir * (uv - uf);
@@ -395,9 +397,9 @@ __global__ void __launch_bounds__(Sp<N>::T) k_curved4(long long Ne, const real* 
     if (!valid || idx3[al] != frow(f, N)) continue;
     const int en = nbr[f + 6 * ec];
     if (en < 0) continue;
-    const int fn = nbrf[f + 6 * ec];
+    const int fs = nbrf[f + 6 * ec];  // fn | ori << 3
     const int p = al == 0 ? j : i, q = al == 2 ? j : k;
-    const long long src = (long long)en * N3 + face_node(faxis(fn), frow(fn, N), p, q, N);
+    const long long src = (long long)en * N3 + nbr_face_node(fs, p, q, N);
     uf[f] = (double)u[src];
     vf[f] = (double)ud[src];
   }

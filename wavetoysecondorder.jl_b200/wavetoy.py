@@ -29,6 +29,8 @@ BG_MINKOWSKI, BG_CONSTANT_SHIFT, BG_ADM_PERTURBED, BG_RADIAL_SHIFT = 0, 1, 2, 3
 IC_EIGENMODE_CARTESIAN, IC_GAUSSIANS, IC_OUTGOING_PULSE, IC_PLANE_WAVE, IC_EIGENMODE_RADIAL = 0, 1, 2, 3, 4
 # precision forms of an FP32 mesh (n = 8 contractions): CUDA cores, split BF16 three-term / two-term
 FP32_CUDA_CORES, FP32_BF16X3, FP32_BF16X2 = 0, 1, 2
+# multi-patch mesh kinds (evolve3d mesh_kind :cubed_cube, :inflated_cube, :radial_shell)
+MESH_CUBED_CUBE, MESH_INFLATED_CUBE, MESH_RADIAL_SHELL = 1, 2, 3
 # prescribed 4-metrics of the fully second-order curved path
 CURVED4_MINKOWSKI, CURVED4_GAUGE_WAVE = 0, 1
 
@@ -49,6 +51,11 @@ class WaveToyError(RuntimeError):
 class _MeshDesc(C.Structure):
     _fields_ = [("N", C.c_int), ("M", C.c_int * 3), ("x0", C.c_double), ("x1", C.c_double),
                 ("warp_A", C.c_double), ("periodic", C.c_int), ("outer_tag", C.c_int), ("precision", C.c_int)]
+
+
+class _PatchDesc(C.Structure):
+    _fields_ = [("kind", C.c_int), ("N", C.c_int), ("M", C.c_int), ("p", C.c_double * 3), ("outer_tag", C.c_int),
+                ("inner_tag", C.c_int), ("precision", C.c_int)]
 
 
 class _BgDesc(C.Structure):
@@ -80,6 +87,8 @@ def library():
         "wt_ctx_launch_count": [vp, C.POINTER(ll)], "wt_ctx_nonfinite": [vp, C.POINTER(i)],
         "wt_mesh_create": [vp, C.POINTER(_MeshDesc), pvp],
         "wt_mesh_create_arrays": [vp, i, ll, vp, vp, vp, vp, vp, vp, i, pvp],
+        "wt_mesh_create_patches": [vp, C.POINTER(_PatchDesc), pvp],
+        "wt_patch_mesh_arrays": [C.POINTER(_PatchDesc), C.POINTER(ll), vp, vp, vp, vp, vp, vp],
         "wt_mesh_destroy": [vp], "wt_mesh_info": [vp, C.POINTER(i), C.POINTER(ll), C.POINTER(i)],
         "wt_mesh_get": [vp, C.c_char_p, vp], "wt_mesh_set_bdry": [vp, vp],
         "wt_mesh_min_spacing": [vp, C.POINTER(d)],
@@ -271,12 +280,32 @@ class Mesh(_Child):
                                                   precision, C.byref(h)), "wt_mesh_create_arrays")
         return cls(ctx, h, N, Ne, precision)
 
+    @classmethod
+    def patches(cls, ctx: Context, kind: int, N: int, M: int, params: Sequence[float], *, outer_tag: int = 7,
+                inner_tag: int = 8, precision: int = WT_F64) -> "Mesh":
+        """Multi-patch curvilinear mesh: make_cubed_cube_mesh(T, M, R), make_inflated_cube_mesh(T, L, R1, R2, M)
+        and make_radial_shell_mesh(T, R1, R2, M) as evolve3d builds them (src/evolve.jl:1176-1184), with this
+        library's own patch maps; params = (R,), (L, R1, R2) or (R1, R2)."""
+        d = _PatchDesc()
+        d.kind, d.N, d.M = int(kind), int(N), int(M)
+        for a, v in enumerate(list(params)[:3]):
+            d.p[a] = float(v)
+        d.outer_tag, d.inner_tag, d.precision = int(outer_tag), int(inner_tag), int(precision)
+        h = C.c_void_p()
+        ctx.check(library().wt_mesh_create_patches(ctx.h, C.byref(d), C.byref(h)), "wt_mesh_create_patches")
+        ne = C.c_longlong()
+        library().wt_mesh_info(h, None, C.byref(ne), None)
+        m = cls(ctx, h, N, int(ne.value), precision)
+        m.kind, m.M, m.params = kind, M, tuple(params)
+        return m
+
     def get(self, name: str):
         import numpy as np
         n = self.nn
         sizes = {"coords": 3 * n, "jac": 9 * n, "invjac": 9 * n, "detjac": n, "Hphys": n, "Hd": n, "invdetJ": n,
                  "Ja": 9 * n, "x": self.N, "H": self.N, "G": self.N * self.N}
-        isizes = {"bdry": 6 * self.Ne, "neighbour": 6 * self.Ne, "handedness": self.Ne}
+        isizes = {"bdry": 6 * self.Ne, "neighbour": 6 * self.Ne, "neighbour_face": 6 * self.Ne,
+                  "orientation": 6 * self.Ne, "handedness": self.Ne}
         out = np.zeros(sizes[name]) if name in sizes else np.zeros(isizes[name], dtype=np.int32)
         self.ctx.check(library().wt_mesh_get(self.h, name.encode(), out.ctypes.data), f"wt_mesh_get({name})")
         return out
@@ -807,6 +836,32 @@ def evolve_curved_host(Phi_host, Pi_host, coef: Coef, ws: Workspace, dt: float, 
     p, keep = _bcptr(bc3d)
     ws.ctx.check(fn(ws.ctx.h, ws.h, coef.h, addr(Phi_host, sw), addr(Pi_host, sw), float(dt), int(steps_per_sample),
                     int(nsamples), float(eps_KO), p, int(metric), addr(energy, "float64")), "evolve_curved_host")
+
+
+def patch_mesh_arrays(kind: int, N: int, M: int, params: Sequence[float], outer_tag: int = 7, inner_tag: int = 8):
+    """Host arrays of a multi-patch mesh (the mesh Mesh.patches builds; no GPU needed): coords
+    (3,N,N,N,Ne) and jac (9 per node) as flat float64, neighbour / neighbour_face (1-based, 0 = none),
+    orientation (D4 code) and bdry as flat int32 of 6*Ne, in the reference's column-major order."""
+    import numpy as np
+    d = _PatchDesc()
+    d.kind, d.N, d.M = int(kind), int(N), int(M)
+    for a, v in enumerate(list(params)[:3]):
+        d.p[a] = float(v)
+    d.outer_tag, d.inner_tag, d.precision = int(outer_tag), int(inner_tag), WT_F64
+    ne = C.c_longlong()
+    rc = library().wt_patch_mesh_arrays(C.byref(d), C.byref(ne), None, None, None, None, None, None)
+    if rc != 0:
+        raise WaveToyError(rc, "wt_patch_mesh_arrays: bad mesh description")
+    Ne, nn = int(ne.value), N ** 3 * int(ne.value)
+    out = {"Ne": Ne, "coords": np.zeros(3 * nn), "jac": np.zeros(9 * nn)}
+    for k in ("neighbour", "neighbour_face", "orientation", "bdry"):
+        out[k] = np.zeros(6 * Ne, dtype=np.int32)
+    rc = library().wt_patch_mesh_arrays(C.byref(d), C.byref(ne), out["coords"].ctypes.data, out["jac"].ctypes.data,
+                                        *[out[k].ctypes.data for k in ("neighbour", "neighbour_face",
+                                                                       "orientation", "bdry")])
+    if rc != 0:
+        raise WaveToyError(rc, "wt_patch_mesh_arrays failed")
+    return out
 
 
 def initial_data(mesh: Mesh, kind: int, params: Sequence[float], u, ut=None, t: float = 0.0):
