@@ -116,12 +116,20 @@ class Server:
 
     def __init__(self, ctx, precision: int = wt.WT_F32, hbm_budget: float = 150e9, tick: int = 50,
                  max_active: Optional[int] = None, fp32_form: int = wt.FP32_CUDA_CORES, keep_results: bool = False,
-                 fill_nodes: Optional[int] = 8_000_000):
+                 fill_nodes: Optional[int] = 8_000_000, order: str = "hrrn"):
         """fill_nodes: admit further requests only while the running ones hold fewer
         nodes than this (about what keeps the GPU busy); beyond it, new requests
-        wait in arrival order, so large requests are not slowed down by sharing
-        the GPU with many others, while small ones still run together.  None:
-        admit whatever the budget allows."""
+        wait, so large requests are not slowed down by sharing the GPU with many
+        others, while small ones still run together.  None: admit whatever the
+        budget allows.  order: which waiting request is admitted next --
+        "hrrn" (highest response ratio (wait + service) / service first, with the
+        service time estimated from the request's DOF-updates: short requests go
+        ahead under a backlog, and a long one's priority grows while it waits),
+        "sjf" (least work first; long requests can wait until the backlog
+        clears) or "fifo" (arrival order)."""
+        if order not in ("hrrn", "sjf", "fifo"):
+            raise ValueError("order must be 'hrrn', 'sjf' or 'fifo'")
+        self.order = order
         self.ctx = ctx
         self.fill_nodes = fill_nodes
         self.precision = precision
@@ -130,6 +138,11 @@ class Server:
         self.max_active = max_active
         self.fp32_form = fp32_form
         self.keep = keep_results
+
+    def _service_s(self, req: Request) -> float:
+        # rough service time at the measured single-GPU rates (FP64 ~3e9, FP32 ~6e9 DOF-updates/s)
+        rate = 3e9 if request_precision(self.precision, req) == wt.WT_F64 else 6e9
+        return 2.0 * req.nodes * req.steps / rate + 0.05
 
     def _cost(self, req: Request) -> float:
         # running footprint plus the FP64 set-up geometry held while it is built
@@ -152,7 +165,12 @@ class Server:
             now = time.perf_counter() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.popleft())
-            # admit in arrival order while the budget (and the slot limit) allows
+            if self.order == "sjf":
+                queue = deque(sorted(queue, key=lambda r: (r.nodes * r.steps, r.arrival)))
+            elif self.order == "hrrn":
+                queue = deque(sorted(queue, key=lambda r: (-(now - r.arrival + self._service_s(r)) / self._service_s(r),
+                                                           r.arrival)))
+            # admit in queue order while the budget (and the slot limit) allows
             while queue and used + self._cost(queue[0]) <= self.budget and \
                     (self.max_active is None or len(active) < self.max_active) and \
                     (self.fill_nodes is None or not active or
