@@ -62,9 +62,10 @@ def profiled_traffic(key: str):
             continue
         for line in open(os.path.join(d, fn)):
             line = line.strip().strip("`")
-            if line.startswith("traffic_bytes_per_node") and key in line and "=" in line:
+            parts = line.replace("=", " = ").split()
+            if len(parts) >= 4 and parts[0] == "traffic_bytes_per_node" and parts[1] == key and parts[2] == "=":
                 try:
-                    return float(line.split("=")[1].split()[0])
+                    return float(parts[3])
                 except ValueError:
                     pass
     return None
@@ -312,7 +313,8 @@ def run_ours(args):
     k1_words = 1 + 1 + 20 + 3 + 3   # Phi, Pi, 20 coefficient words, F (3), Phi RK stage words (stage mean)
     k1_avg_s = (k1_ms / max(k1_n, 1)) / 1000.0
     k1_achieved = k1_words * wbytes * nn / k1_avg_s / 1e9 if k1_n else None
-    traffic_pn = profiled_traffic(f"k1_curv_{args.precision}")
+    traffic_pn = profiled_traffic(f"k1_curv_{args.precision}" if args.precision == "f64" or args.fp32_form == "cuda"
+                                  else f"k1_curv_f32_{args.fp32_form}")
     k2_avg_s = (k2_ms / max(k2_n, 1)) / 1000.0
     k2_words = 3 + 10 + 3
     step_bytes = wbytes * (34 + 4 * 20) * nn
