@@ -42,13 +42,13 @@ enum {
 
 enum { WT_F64 = 0, WT_F32 = 1 };
 /* How an FP32 mesh evaluates the n = 8 derivative contractions (the precision
- * forms of the large-solve study; other n always use CUDA cores):
- * split-precision BF16 on tensor cores with three-term operands (default,
- * FP32 accuracy), the same with two-term hi + lo operands, or FP32 on CUDA
- * cores. */
+ * forms of the large-solve study; other n always use CUDA cores): FP32 on
+ * CUDA cores (default), split-precision BF16 on tensor cores with three-term
+ * operands (FP32 accuracy), or the same with two-term hi + lo operands. */
 enum { WT_FP32_CUDA_CORES = 0, WT_FP32_BF16X3 = 1, WT_FP32_BF16X2 = 2 };
 enum { WT_BC_DIRICHLET = 1, WT_BC_SOMMERFELD = 2, WT_BC_EXCISION = 3, WT_BC_FULL_DIRICHLET = 4 };
-enum { WT_BG_MINKOWSKI = 0, WT_BG_CONSTANT_SHIFT = 1, WT_BG_ADM_PERTURBED = 2, WT_BG_RADIAL_SHIFT = 3 };
+enum { WT_BG_MINKOWSKI = 0, WT_BG_CONSTANT_SHIFT = 1, WT_BG_ADM_PERTURBED = 2, WT_BG_RADIAL_SHIFT = 3,
+       WT_BG_GAUGE_WAVE = 4, WT_BG_SINE_SHIFT = 5 };
 /* prescribed 4-metrics of the fully second-order curved path */
 enum { WT_CURVED4_MINKOWSKI = 0, WT_CURVED4_GAUGE_WAVE = 1 };
 
@@ -186,7 +186,19 @@ int wt_mesh_min_spacing(wt_mesh* mesh, double* h);
  *   ADM_PERTURBED: alpha = 1 + p0 sin 2pi x, beta^i = p1 cos 2pi x_i,
  *     gamma_ij = d_ij + p2 exp(-|x-c|^2/p3)(d_ij + 0.5 s_ij), c = p4..p6,
  *     s = p7..p12 (s11,s12,s13,s22,s23,s33)
- *   RADIAL_SHIFT: beta_r linear from p0 at r=p2 to p1 at r=p3 (src/evolve.jl:1128-1145) */
+ *   RADIAL_SHIFT: beta_r linear from p0 at r=p2 to p1 at r=p3 (src/evolve.jl:1128-1145)
+ * Time-dependent backgrounds from a spacetime metric (MetricBackground3D,
+ * src/wave3d_curved.jl:56-71: ADM variables of the metric at (t, x, y, z)),
+ * p[0] = A, p[1] = d, p[2] = the time t0 they are first sampled at; with
+ * H = 1 - A sin(2 pi (x - t)/d) and c = cos(2 pi (x - t)/d):
+ *   GAUGE_WAVE (SpacetimeMetrics.GaugeWave): alpha = sqrt(H), beta = 0,
+ *     gamma = diag(H, 1, 1);
+ *   SINE_SHIFT (SpacetimeMetrics.SineShift): alpha = 1, beta^x = -A c/(1 + A c),
+ *     gamma = diag((1 + A c)^2, 1, 1)
+ * (the decompositions evolve1d documents, src/evolve.jl:171-195, flat in y, z).
+ * wt_step_rk4_curved re-samples them at every stage time, as evolve3d's rhs!
+ * calls sample_background3d!(coef, bg, t) (src/evolve.jl:1289), and advances
+ * the coefficients' time; wt_coef_set_time samples them at a given time. */
 typedef struct {
   int kind;
   double p[16];
@@ -197,6 +209,11 @@ int wt_background_set(wt_ctx* ctx, wt_mesh* mesh, const wt_background_desc* desc
  * fills. */
 int wt_background_set_arrays(wt_ctx* ctx, wt_mesh* mesh, const double* coef11, wt_coef** out);
 int wt_coef_get(const wt_coef* coef, double* coef11_host);
+/* Time-dependent coefficients (WT_BG_GAUGE_WAVE, WT_BG_SINE_SHIFT): sample at
+ * time t (synchronous); the time they hold.  Static coefficients: set_time
+ * returns WT_EINVAL, get_time gives 0. */
+int wt_coef_set_time(wt_ctx* ctx, wt_coef* coef, double t);
+int wt_coef_get_time(const wt_coef* coef, double* t);
 int wt_coef_destroy(wt_coef* coef);
 
 /* ---- initial data --------------------------------------------------------------*/

@@ -48,6 +48,7 @@ def lib():
         vp, d, i = C.c_void_p, C.c_double, C.c_int
         L.or_mesh_create.restype = vp
         L.or_mesh_create.argtypes = [i, i, i, i, d, d, d, i, i]
+        L.or_evolve_curved_td.argtypes = [vp, i, vp, vp, vp, d, i, d, C.POINTER(_BC), i]
         L.or_mesh_create_arrays.restype = vp
         L.or_mesh_create_arrays.argtypes = [i, C.c_long, vp, vp, vp, vp, vp, vp]
         L.or_mesh_destroy.argtypes = [vp]
@@ -280,6 +281,16 @@ class OracleMesh:
         lib().or_evolve_curved(self.h, _p(coef), _p(Phi), _p(Pi), dt, nsteps, eps_ko,
                                C.byref(bc) if bc is not None else None, int(use_metric), _p(E))
         return (Phi, Pi, E) if record_energy else (Phi, Pi)
+
+    def evolve_curved_td(self, kind, params, t0, Phi, Pi, dt, nsteps, eps_ko=0.0, bc=None, use_metric=False):
+        """RK4 with the time-dependent background kind (4 gauge wave, 5 sine shift; params (A, d))
+        re-sampled at every stage time from t0."""
+        Phi = np.array(Phi, dtype=np.float64, copy=True); Pi = np.array(Pi, dtype=np.float64, copy=True)
+        p = np.zeros(16)
+        p[0], p[1], p[2] = params[0], params[1], t0
+        lib().or_evolve_curved_td(self.h, int(kind), _p(p), _p(Phi), _p(Pi), dt, nsteps, eps_ko,
+                                  C.byref(bc) if bc is not None else None, int(use_metric))
+        return Phi, Pi
 
     def evolve_sipg(self, u, v, dt, nsteps, bdry_values=(0,) * 6, tau=20.0, R=np.inf, eps_ko=0.0,
                     record_energy=False):

@@ -522,8 +522,54 @@ void div3d(const Mesh& m, const double* F1, const double* F2, const double* F3, 
 //           c = (p4,p5,p6), s = (p7..p12) = (s11,s12,s13,s22,s23,s33)
 //   kind 3  radial shift (src/evolve.jl:1128-1145): alpha = 1, gamma = I,
 //           beta = beta_r(r) x/r with beta_r linear from p0 at r=p2 to p1 at r=p3.
+// adm_decompose of a 4-metric g (lower indices, g[mu][nu], mu = 0 time):
+// gamma_ij = g_ij, beta_i = g_0i, beta^i = gamma^ij beta_j,
+// alpha = sqrt(beta_i beta^i - g_00) (the standard 3+1 split; SpacetimeMetrics'
+// adm_decompose, called at src/wave3d_curved.jl:68, is unvendored).
+void adm_from_metric(const double g[4][4], double out[10]) {
+  const double g11 = g[1][1], g12 = g[1][2], g13 = g[1][3], g22 = g[2][2], g23 = g[2][3], g33 = g[3][3];
+  const double det = g11 * (g22 * g33 - g23 * g23) - g12 * (g12 * g33 - g23 * g13) + g13 * (g12 * g23 - g22 * g13);
+  const double u[3][3] = {{(g22 * g33 - g23 * g23) / det, (g13 * g23 - g12 * g33) / det, (g12 * g23 - g13 * g22) / det},
+                          {(g13 * g23 - g12 * g33) / det, (g11 * g33 - g13 * g13) / det, (g12 * g13 - g11 * g23) / det},
+                          {(g12 * g23 - g13 * g22) / det, (g12 * g13 - g11 * g23) / det, (g11 * g22 - g12 * g12) / det}};
+  const double bl[3] = {g[0][1], g[0][2], g[0][3]};
+  double bu[3], bb = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    bu[i] = u[i][0] * bl[0] + u[i][1] * bl[1] + u[i][2] * bl[2];
+    bb += bl[i] * bu[i];
+  }
+  out[0] = std::sqrt(bb - g[0][0]);
+  out[1] = bu[0]; out[2] = bu[1]; out[3] = bu[2];
+  out[4] = g11; out[5] = g12; out[6] = g13; out[7] = g22; out[8] = g23; out[9] = g33;
+}
+
+// The spacetime metrics of the time-dependent backgrounds at (t, x) (flat in y, z):
+//   gauge wave  ds^2 = -H dt^2 + H dx^2 + dy^2 + dz^2, H = 1 - A sin(2 pi (x - t)/d)
+//   sine shift  the metric whose 3+1 split is alpha = 1, beta^x = -A c/(1 + A c),
+//               gamma_xx = (1 + A c)^2, c = cos(2 pi (x - t)/d)  (src/evolve.jl:171-195)
+void spacetime_metric(int kind, double A, double d, double t, double x, double g[4][4]) {
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) g[a][b] = a == b ? (a == 0 ? -1.0 : 1.0) : 0.0;
+  const double ph = 2.0 * M_PI * (x - t) / d;
+  if (kind == 4) {
+    const double H = 1.0 - A * std::sin(ph);
+    g[0][0] = -H; g[1][1] = H;
+  } else if (kind == 5) {
+    const double ac = A * std::cos(ph), gxx = (1.0 + ac) * (1.0 + ac), bx = -ac / (1.0 + ac);
+    g[1][1] = gxx;
+    g[0][1] = g[1][0] = gxx * bx;            // beta_x = gamma_xx beta^x
+    g[0][0] = -1.0 + gxx * bx * bx;          // -alpha^2 + beta_i beta^i
+  }
+}
+
 void bg_point(int kind, const double* p, double x, double y, double z, double out[10]) {
   double al = 1, b1 = 0, b2 = 0, b3 = 0, g11 = 1, g12 = 0, g13 = 0, g22 = 1, g23 = 0, g33 = 1;
+  if (kind == 4 || kind == 5) {  // MetricBackground3D at time p[2]: A = p[0], d = p[1]
+    double g[4][4];
+    spacetime_metric(kind, p[0], p[1], p[2], x, g);
+    adm_from_metric(g, out);
+    return;
+  }
   if (kind == 1) { b1 = p[0]; b2 = p[1]; b3 = p[2]; }
   else if (kind == 2) {
     const double tp = 2.0 * M_PI;
@@ -1279,6 +1325,37 @@ void or_evolve_curved(void* h, const double* coef, double* Phi, double* Pi, doub
       Pi[n] += dt / 6 * (k2[n] + 2 * k4[n] + 2 * k6[n] + k8[n]);
     }
     if (energy) energy[s + 1] = or_energy(h, coef, Phi, Pi, use_metric);
+  }
+}
+
+// RK4 with a time-dependent background re-sampled at every stage time, as
+// evolve3d's rhs! closure calls sample_background3d!(coef, bg, t)
+// (src/evolve.jl:1287-1307); p[2] is the start time t0.
+void or_evolve_curved_td(void* h, int kind, const double* p0, double* Phi, double* Pi, double dt, int nsteps,
+                         double eps_ko, const or_bc* bc, int use_metric) {
+  Mesh& m = *static_cast<Mesh*>(h);
+  const long nn = m.nn();
+  std::vector<double> k1(nn), k2(nn), k3(nn), k4(nn), k5(nn), k6(nn), k7(nn), k8(nn), Ps(nn), Qs(nn), coef(11 * nn);
+  double p[16];
+  std::memcpy(p, p0, sizeof(p));
+  const double t0 = p0[2];
+  auto at = [&](double t) { p[2] = t; sample_background(m, kind, p, coef.data()); };
+  for (int s = 0; s < nsteps; ++s) {
+    const double t = t0 + s * dt;
+    at(t);
+    or_rhs_curved(h, coef.data(), Phi, Pi, k1.data(), k2.data(), eps_ko, bc, use_metric, nullptr);
+    for (long n = 0; n < nn; ++n) { Ps[n] = Phi[n] + dt / 2 * k1[n]; Qs[n] = Pi[n] + dt / 2 * k2[n]; }
+    at(t + dt / 2);
+    or_rhs_curved(h, coef.data(), Ps.data(), Qs.data(), k3.data(), k4.data(), eps_ko, bc, use_metric, nullptr);
+    for (long n = 0; n < nn; ++n) { Ps[n] = Phi[n] + dt / 2 * k3[n]; Qs[n] = Pi[n] + dt / 2 * k4[n]; }
+    or_rhs_curved(h, coef.data(), Ps.data(), Qs.data(), k5.data(), k6.data(), eps_ko, bc, use_metric, nullptr);
+    for (long n = 0; n < nn; ++n) { Ps[n] = Phi[n] + dt * k5[n]; Qs[n] = Pi[n] + dt * k6[n]; }
+    at(t + dt);
+    or_rhs_curved(h, coef.data(), Ps.data(), Qs.data(), k7.data(), k8.data(), eps_ko, bc, use_metric, nullptr);
+    for (long n = 0; n < nn; ++n) {
+      Phi[n] += dt / 6 * (k1[n] + 2 * k3[n] + 2 * k5[n] + k7[n]);
+      Pi[n] += dt / 6 * (k2[n] + 2 * k4[n] + 2 * k6[n] + k8[n]);
+    }
   }
 }
 

@@ -52,6 +52,14 @@ struct wt_coef {
   wt_ctx* ctx = nullptr;
   wt_mesh* mesh = nullptr;
   wt::DevCoef c;
+  // time-dependent (spacetime-metric) backgrounds: kind, parameters and the
+  // time the coefficients hold (on the host, and on the device for kernels
+  // captured in a CUDA graph)
+  int kind = -1;
+  double p[16] = {};
+  bool td = false;
+  mutable double t = 0.0;
+  double* d_t = nullptr;
 };
 
 struct wt_ws {
@@ -840,13 +848,25 @@ static int coef_alloc(wt_ctx* ctx, wt_mesh* mesh, wt_coef** out) {
 int wt_background_set(wt_ctx* ctx, wt_mesh* mesh, const wt_background_desc* desc, wt_coef** out) {
   if (!ctx) return WT_EINVAL;
   if (!mesh || !desc || !out) return fail(ctx, WT_EINVAL, "wt_background_set: NULL argument");
-  if (desc->kind < 0 || desc->kind > 3) return fail(ctx, WT_EINVAL, "unknown background kind");
+  if (desc->kind < 0 || desc->kind > 5) return fail(ctx, WT_EINVAL, "unknown background kind");
   if (desc->kind == WT_BG_ADM_PERTURBED && !(desc->p[3] > 0))
     return fail(ctx, WT_EINVAL, "ADM background needs a positive Gaussian width p[3]");
+  const bool td = desc->kind == WT_BG_GAUGE_WAVE || desc->kind == WT_BG_SINE_SHIFT;
+  if (td && (!(std::fabs(desc->p[0]) < 1.0) || !(desc->p[1] > 0.0) || !std::isfinite(desc->p[2])))
+    return fail(ctx, WT_EINVAL, "metric backgrounds need |A| < 1, d > 0 and a finite t0 (p[0..2])");
   WT_TRY(need_setup_geometry(mesh, "wt_background_set"));
   wt_coef* c = nullptr;
   WT_TRY(coef_alloc(ctx, mesh, &c));
-  int rc = lrc(ctx, wt::launch_background(mesh->m, c->c, desc->kind, desc->p, ctx->stream), "background");
+  c->kind = desc->kind;
+  std::memcpy(c->p, desc->p, sizeof(c->p));
+  c->td = td;
+  if (td) {
+    c->t = desc->p[2];
+    if (dalloc(ctx, (void**)&c->d_t, sizeof(double), nullptr)) { wt_coef_destroy(c); return WT_ENOMEM; }
+    cudaMemcpyAsync(c->d_t, &c->t, sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  }
+  int rc = lrc(ctx, wt::launch_background(mesh->m, c->c, desc->kind, desc->p, ctx->stream, c->d_t, 0.0),
+               "background");
   if (!rc) rc = lrc(ctx, wt::launch_coef_combine(mesh->m, c->c, ctx->stream), "background");
   ctx->launches += 2;
   if (!rc) {
@@ -887,7 +907,32 @@ int wt_coef_destroy(wt_coef* c) {
   cudaStreamSynchronize(c->ctx->stream);
   cudaFree(c->c.c11);
   cudaFree(c->c.c10);
+  if (c->d_t) cudaFree(c->d_t);
   delete c;
+  return 0;
+}
+
+int wt_coef_set_time(wt_ctx* ctx, wt_coef* c, double t) {
+  if (!ctx) return WT_EINVAL;
+  if (!c) return fail(ctx, WT_EINVAL, "wt_coef_set_time: NULL argument");
+  if (!c->td) return fail(ctx, WT_EINVAL, "wt_coef_set_time: the coefficients are not time-dependent");
+  if (!std::isfinite(t)) return fail(ctx, WT_EINVAL, "wt_coef_set_time: t must be finite");
+  WT_TRY(need_setup_geometry(c->mesh, "wt_coef_set_time"));
+  c->t = t;
+  cudaMemcpyAsync(c->d_t, &c->t, sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  int rc = lrc(ctx, wt::launch_background(c->mesh->m, c->c, c->kind, c->p, ctx->stream, c->d_t, 0.0), "background");
+  if (!rc) rc = lrc(ctx, wt::launch_coef_combine(c->mesh->m, c->c, ctx->stream), "background");
+  ctx->launches += 2;
+  if (!rc) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "wt_coef_set_time");
+  }
+  return rc;
+}
+
+int wt_coef_get_time(const wt_coef* c, double* t) {
+  if (!c || !t) return WT_EINVAL;
+  *t = c->td ? c->t : 0.0;
   return 0;
 }
 
@@ -1124,12 +1169,23 @@ int wt_l2_diff(wt_ctx* ctx, wt_ws* ws, const void* a, const void* b, int use_met
 }
 
 // ---- time stepping ------------------------------------------------------------------------
+// Time-dependent coefficients: sample at the coefficients' time + toff (stage times of RK4).
+static int coef_resample(wt_ctx* ctx, const wt_coef* coef, double toff, cudaStream_t s) {
+  wt::DevCoef c = coef->c;
+  WT_TRY(lrc(ctx, wt::launch_background(coef->mesh->m, c, coef->kind, coef->p, s, coef->d_t, toff), "background"));
+  WT_TRY(lrc(ctx, wt::launch_coef_combine(coef->mesh->m, c, s), "background"));
+  ctx->launches += 2;
+  return 0;
+}
+
 static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
                             double eps_ko, const wt::ConsBC& b, int use_metric) {
   const wt::DevMesh& m = ws->mesh->m;
   cudaStream_t s = ctx->stream;
   void* SP[2] = {ws->S0, ws->S1};
+  const double toff[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};  // RK4 stage times
   for (int st = 0; st < 4; ++st) {
+    if (coef->td) WT_TRY(coef_resample(ctx, coef, toff[st], s));
     const void* inP = st == 0 ? Phi : SP[(st - 1) % 2];
     const void* inQ = st == 0 ? Pi : ws->SQ;
     wt::RKStage rkP, rkQ;
@@ -1158,6 +1214,10 @@ static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* P
                  "rk4"));
       ctx->launches += 2;
     }
+  }
+  if (coef->td) {
+    WT_TRY(lrc(ctx, wt::launch_advance_time(coef->d_t, dt, s), "background time"));
+    ctx->launches += 1;
   }
   return 0;
 }
@@ -1208,13 +1268,18 @@ int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, v
   WT_TRY(make_bc(ctx, bc, use_metric, b));
   WT_TRY(ws_step_buffers(ws));
   if (eps_ko != 0.0) WT_TRY(ensure_mu(ws));
+  if (coef->td) WT_TRY(need_setup_geometry(coef->mesh, "wt_step_rk4_curved (time-dependent background)"));
   comp_track(ws, Phi, Pi);
+  int rc = 0;
   if (nsteps <= 2) {
-    for (int i = 0; i < nsteps; ++i) WT_TRY(step_curved_once(ctx, ws, coef, Phi, Pi, dt, eps_ko, b, use_metric));
-    return 0;
+    for (int i = 0; i < nsteps && !rc; ++i) rc = step_curved_once(ctx, ws, coef, Phi, Pi, dt, eps_ko, b, use_metric);
+  } else {
+    // capture one step as a CUDA graph and replay it
+    rc = replay_graph(ctx, nsteps,
+                      [&]() { return step_curved_once(ctx, ws, coef, Phi, Pi, dt, eps_ko, b, use_metric); });
   }
-  // capture one step as a CUDA graph and replay it
-  return replay_graph(ctx, nsteps, [&]() { return step_curved_once(ctx, ws, coef, Phi, Pi, dt, eps_ko, b, use_metric); });
+  if (!rc && coef->td) coef->t += nsteps * dt;  // the device copy was advanced step by step
+  return rc;
 }
 
 static int step_sipg_once(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, const double bv[6], double tau,
@@ -1672,6 +1737,7 @@ int wt_batch_add(wt_batch* b, wt_ws* ws, const wt_coef* coef, void* Phi, void* P
   if (!coef || !Phi || !Pi || !slot) return fail(ctx, WT_EINVAL, "wt_batch_add: NULL argument");
   if (coef->mesh != ws->mesh) return fail(ctx, WT_EINVAL, "coefficients belong to another mesh");
   if (!(dt > 0) || !std::isfinite(dt)) return fail(ctx, WT_EINVAL, "dt must be positive and finite");
+  if (coef->td) return fail(ctx, WT_ENOTSUP, "wt_batch_add: time-dependent backgrounds are not batched");
   wt_batch::Member mb;
   WT_TRY(make_bc(ctx, bc, 1, mb.bc));
   WT_TRY(ws_step_buffers(ws));

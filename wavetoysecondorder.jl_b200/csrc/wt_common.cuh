@@ -166,7 +166,10 @@ int launch_metric(DevMesh& m, cudaStream_t s);
 int launch_dinvjac(DevMesh& m, cudaStream_t s);
 int launch_boundary_normals(DevMesh& m, cudaStream_t s);
 int launch_streamed_geometry(DevMesh& m, cudaStream_t s);
-int launch_background(const DevMesh& m, DevCoef& c, int kind, const double* p, cudaStream_t s);
+// kinds 4, 5 (spacetime-metric backgrounds) are sampled at time *d_t + toff
+int launch_background(const DevMesh& m, DevCoef& c, int kind, const double* p, cudaStream_t s,
+                      const double* d_t = nullptr, double toff = 0.0);
+int launch_advance_time(double* d_t, double dt, cudaStream_t s);
 int launch_coef_combine(const DevMesh& m, DevCoef& c, cudaStream_t s);
 int launch_min_spacing(const DevMesh& m, double* out, cudaStream_t s);
 int launch_initial(const DevMesh& m, int kind, const double* dparams, int np, double t, void* u, void* ut,

@@ -316,14 +316,28 @@ __global__ void k_streamed_geom(int N, long long Ne, const double* __restrict__ 
 
 // Background sampling: alpha, sqrt(det gamma), beta, gamma^{ij} (symmetric
 // cofactor inverse) exactly as _sample_bg3d_kernel!.
+// Kinds 4 and 5 are the spacetime-metric backgrounds at time *d_t + toff (the
+// time lives on the device so that a captured RK4 step stays valid).
 __global__ void k_background(long long nn, int kind, const double* __restrict__ coords, double p0, double p1,
                              double p2, double p3, double p4, double p5, double p6, double s11, double s12,
-                             double s13, double s22, double s23, double s33, double* __restrict__ c11) {
+                             double s13, double s22, double s23, double s33, const double* __restrict__ d_t,
+                             double toff, double* __restrict__ c11) {
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n >= nn) return;
   const double x = coords[3 * n], y = coords[3 * n + 1], z = coords[3 * n + 2];
   double al = 1, b1 = 0, b2 = 0, b3 = 0, g11 = 1, g12 = 0, g13 = 0, g22 = 1, g23 = 0, g33 = 1;
-  if (kind == 1) {
+  if (kind == 4 || kind == 5) {
+    const double t = d_t[0] + toff, ph = 2.0 * M_PI * (x - t) / p1;
+    if (kind == 4) {  // gauge wave
+      const double H = 1.0 - p0 * sin(ph);
+      al = sqrt(H);
+      g11 = H;
+    } else {          // sine shift
+      const double ac = p0 * cos(ph);
+      b1 = -ac / (1.0 + ac);
+      g11 = (1.0 + ac) * (1.0 + ac);
+    }
+  } else if (kind == 1) {
     b1 = p0; b2 = p1; b3 = p2;
   } else if (kind == 2) {
     const double tp = 2.0 * M_PI;
@@ -441,9 +455,18 @@ int launch_streamed_geometry(DevMesh& m, cudaStream_t s) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-int launch_background(const DevMesh& m, DevCoef& c, int kind, const double* p, cudaStream_t s) {
+int launch_background(const DevMesh& m, DevCoef& c, int kind, const double* p, cudaStream_t s, const double* d_t,
+                      double toff) {
+  if ((kind == 4 || kind == 5) && !d_t) return -1;
   k_background<<<nblk(m.nn, 256), 256, 0, s>>>(m.nn, kind, m.coords, p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7],
-                                               p[8], p[9], p[10], p[11], p[12], c.c11);
+                                               p[8], p[9], p[10], p[11], p[12], d_t, toff, c.c11);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+__global__ void k_advance_time(double* __restrict__ d_t, double dt) { d_t[0] += dt; }
+
+int launch_advance_time(double* d_t, double dt, cudaStream_t s) {
+  k_advance_time<<<1, 1, 0, s>>>(d_t, dt);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

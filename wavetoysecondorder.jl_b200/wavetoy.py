@@ -26,6 +26,8 @@ FACE_SUBLUMINAL, FACE_OUTFLOW, FACE_INFLOW, FACE_SONIC = 1, 2, 3, 4
 SOMMERFELD_BDRY_TAG = 7
 EXCISION_BDRY_TAG = 8
 BG_MINKOWSKI, BG_CONSTANT_SHIFT, BG_ADM_PERTURBED, BG_RADIAL_SHIFT = 0, 1, 2, 3
+# time-dependent backgrounds from a spacetime metric (MetricBackground3D): params (A, d, t0)
+BG_GAUGE_WAVE, BG_SINE_SHIFT = 4, 5
 IC_EIGENMODE_CARTESIAN, IC_GAUSSIANS, IC_OUTGOING_PULSE, IC_PLANE_WAVE, IC_EIGENMODE_RADIAL = 0, 1, 2, 3, 4
 # precision forms of an FP32 mesh (n = 8 contractions): CUDA cores, split BF16 three-term / two-term
 FP32_CUDA_CORES, FP32_BF16X3, FP32_BF16X2 = 0, 1, 2
@@ -94,6 +96,7 @@ def library():
         "wt_mesh_min_spacing": [vp, C.POINTER(d)],
         "wt_background_set": [vp, vp, C.POINTER(_BgDesc), pvp], "wt_background_set_arrays": [vp, vp, vp, pvp],
         "wt_coef_get": [vp, vp], "wt_coef_destroy": [vp],
+        "wt_coef_set_time": [vp, vp, d], "wt_coef_get_time": [vp, C.POINTER(d)],
         "wt_workspace_create": [vp, vp, pvp], "wt_workspace_destroy": [vp], "wt_workspace_mu": [vp, C.POINTER(d)],
         "wt_rhs_curved": [vp, vp, vp, vp, vp, vp, vp, d, C.POINTER(_BcDesc), i],
         "wt_rhs_curved_noalloc": [vp, vp, vp, vp, vp, vp, d, d, C.POINTER(_BcDesc), i],
@@ -363,6 +366,18 @@ class Coef(_Child):
         self.mesh.ctx.check(library().wt_coef_get(self.h, out.ctypes.data), "wt_coef_get")
         return out
 
+    def set_time(self, t: float):
+        """Sample a time-dependent background (BG_GAUGE_WAVE, BG_SINE_SHIFT) at time t, as
+        sample_background3d!(coef, bg, t) does for a MetricBackground3D."""
+        self.mesh.ctx.check(library().wt_coef_set_time(self.mesh.ctx.h, self.h, float(t)), "wt_coef_set_time")
+
+    @property
+    def time(self) -> float:
+        """The time a time-dependent background holds (RK4 stepping advances it); 0 for static ones."""
+        t = C.c_double()
+        library().wt_coef_get_time(self.h, C.byref(t))
+        return float(t.value)
+
     def close(self):
         if getattr(self, "h", None) and self._ctx_alive():
             library().wt_coef_destroy(self.h)
@@ -376,7 +391,9 @@ class Coef(_Child):
 
 
 def sample_background3d(mesh: Mesh, kind: int = BG_MINKOWSKI, params: Optional[Sequence[float]] = None) -> Coef:
-    """make_coef3d + sample_background3d! for an analytic background (src/wave3d_curved.jl:106-124)."""
+    """make_coef3d + sample_background3d! for an analytic background (src/wave3d_curved.jl:106-124), or for a
+    MetricBackground3D of the gauge wave / sine shift (kinds BG_GAUGE_WAVE, BG_SINE_SHIFT, params (A, d, t0)):
+    time-dependent, re-sampled at every RK4 stage time by step_rk4_curved."""
     d = _BgDesc()
     d.kind = int(kind)
     params = () if params is None else list(params)
