@@ -333,6 +333,16 @@ int wt_l2_diff(wt_ctx* ctx, wt_ws* ws, const void* a, const void* b, int use_met
  * (checked at the end; the reference asserts isfinite per sample). */
 int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
                        double eps_ko, const wt_bc_desc* bc, int use_metric);
+/* Fixed-step explicit Runge-Kutta methods of pick_integrator_first_order
+ * (src/evolve.jl:43-48; evolve3d runs them with adaptive = false):
+ * WT_ERK_RK4 (the fused low-storage RK4 above) and WT_ERK_TSIT5 (Tsitouras
+ * 2011, fifth order).  Time-dependent backgrounds are re-sampled at every
+ * stage time.  Vern7 (N >= 7 in the reference) is not provided. */
+enum { WT_ERK_RK4 = 0, WT_ERK_TSIT5 = 1 };
+int wt_step_erk_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
+                       int method, double eps_ko, const wt_bc_desc* bc, int use_metric);
+/* The method's Butcher tableau (host only): stages, c[s], A[s*s] (row major), b[s]. */
+int wt_erk_tableau(int method, int* stages, double* c, double* A, double* b);
 /* RK4 of the SIPG system as first-order (u, ut):
  * u' = ut + eps mu^-5 sum_d D_d^6 u,  ut' = rhs_wave3d!(u, ut) + eps mu^-5 sum_d D_d^6 ut. */
 int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int nsteps,

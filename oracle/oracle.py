@@ -49,6 +49,9 @@ def lib():
         L.or_mesh_create.restype = vp
         L.or_mesh_create.argtypes = [i, i, i, i, d, d, d, i, i]
         L.or_evolve_curved_td.argtypes = [vp, i, vp, vp, vp, d, i, d, C.POINTER(_BC), i]
+        L.or_evolve_curved_erk.argtypes = [vp, vp, i, vp, vp, vp, d, i, i, d, C.POINTER(_BC), i]
+        L.or_erk_tableau.argtypes = [i, vp, vp, vp]
+        L.or_erk_tableau.restype = i
         L.or_mesh_create_arrays.restype = vp
         L.or_mesh_create_arrays.argtypes = [i, C.c_long, vp, vp, vp, vp, vp, vp]
         L.or_mesh_destroy.argtypes = [vp]
@@ -292,6 +295,20 @@ class OracleMesh:
                                   C.byref(bc) if bc is not None else None, int(use_metric))
         return Phi, Pi
 
+    def evolve_curved_erk(self, coef, Phi, Pi, dt, nsteps, method=1, eps_ko=0.0, bc=None, use_metric=False,
+                          td=None):
+        """Fixed-step explicit RK (method 1 Tsit5, 0 RK4) with the static coef, or with td =
+        (kind, (A, d), t0) a time-dependent background re-sampled at every stage time."""
+        Phi = np.array(Phi, dtype=np.float64, copy=True); Pi = np.array(Pi, dtype=np.float64, copy=True)
+        p = np.zeros(16)
+        kind = -1
+        if td is not None:
+            kind = int(td[0]); p[0], p[1], p[2] = td[1][0], td[1][1], td[2]
+        lib().or_evolve_curved_erk(self.h, _p(coef) if coef is not None else None, kind, _p(p), _p(Phi), _p(Pi),
+                                   dt, nsteps, int(method), eps_ko, C.byref(bc) if bc is not None else None,
+                                   int(use_metric))
+        return Phi, Pi
+
     def evolve_sipg(self, u, v, dt, nsteps, bdry_values=(0,) * 6, tau=20.0, R=np.inf, eps_ko=0.0,
                     record_energy=False):
         u = np.array(u, dtype=np.float64, copy=True); v = np.array(v, dtype=np.float64, copy=True)
@@ -303,6 +320,13 @@ class OracleMesh:
 
     def min_spacing(self):
         return lib().or_min_spacing(self.h)
+
+
+def erk_tableau(method):
+    """(c, A, b) of the oracle's Butcher tableau for method (1 Tsit5, 0 RK4)."""
+    c, A, b = np.zeros(7), np.zeros(49), np.zeros(7)
+    n = lib().or_erk_tableau(int(method), _p(c), _p(A), _p(b))
+    return c[:n], A[: n * n].reshape(n, n), b[:n]
 
 
 def num_threads() -> int:

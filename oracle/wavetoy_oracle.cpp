@@ -1359,6 +1359,80 @@ void or_evolve_curved_td(void* h, int kind, const double* p0, double* Phi, doubl
   }
 }
 
+// Fixed-step explicit RK with a Butcher tableau (pick_integrator_first_order,
+// src/evolve.jl:43-48, run with adaptive = false): method 1 = Tsit5 (Ch. Tsitouras,
+// Comput. Math. Appl. 62 (2011) 770-775; fifth-order weights), method 0 = classic
+// RK4.  kind >= 0: the time-dependent background of that kind (params p, start
+// time p[2]) re-sampled at every stage time; kind < 0: the static coef.
+struct OrTableau { int s; double c[7]; double a[7][7]; double b[7]; };
+OrTableau or_tableau(int method) {
+  OrTableau T{};
+  if (method == 0) {
+    T.s = 4;
+    T.c[1] = T.c[2] = 0.5; T.c[3] = 1.0;
+    T.a[1][0] = 0.5; T.a[2][1] = 0.5; T.a[3][2] = 1.0;
+    T.b[0] = T.b[3] = 1.0 / 6.0; T.b[1] = T.b[2] = 1.0 / 3.0;
+    return T;
+  }
+  T.s = 7;
+  const double c[7] = {0.0, 0.161, 0.327, 0.9, 0.9800255409045097, 1.0, 1.0};
+  const double a[7][6] = {
+      {0, 0, 0, 0, 0, 0},
+      {0.161, 0, 0, 0, 0, 0},
+      {-0.008480655492356989, 0.335480655492357, 0, 0, 0, 0},
+      {2.897153057105493, -6.359448489975075, 4.3622954328695815, 0, 0, 0},
+      {5.325864828439257, -11.748883564062828, 7.4955393428898365, -0.09249506636175525, 0, 0},
+      {5.86145544294642, -12.92096931784711, 8.159367898576159, -0.071584973281401, -0.028269050394068383, 0},
+      {0.09646076681806523, 0.01, 0.4798896504144996, 1.379008574103742, -3.290069515436081, 2.324710524099774}};
+  for (int i = 0; i < 7; ++i) {
+    T.c[i] = c[i];
+    for (int j = 0; j < 6; ++j) T.a[i][j] = a[i][j];
+  }
+  for (int j = 0; j < 6; ++j) T.b[j] = a[6][j];
+  return T;
+}
+
+int or_erk_tableau(int method, double* c, double* A, double* b) {
+  OrTableau T = or_tableau(method);
+  for (int i = 0; i < T.s; ++i) {
+    c[i] = T.c[i]; b[i] = T.b[i];
+    for (int j = 0; j < T.s; ++j) A[i * T.s + j] = T.a[i][j];
+  }
+  return T.s;
+}
+
+void or_evolve_curved_erk(void* h, const double* coef0, int kind, const double* p0, double* Phi, double* Pi, double dt,
+                          int nsteps, int method, double eps_ko, const or_bc* bc, int use_metric) {
+  Mesh& m = *static_cast<Mesh*>(h);
+  const long nn = m.nn();
+  const OrTableau T = or_tableau(method);
+  std::vector<std::vector<double>> kP(T.s, std::vector<double>(nn)), kQ(T.s, std::vector<double>(nn));
+  std::vector<double> Ps(nn), Qs(nn), coef(coef0 ? coef0 : nullptr, coef0 ? coef0 + 11 * nn : nullptr);
+  double p[16] = {};
+  if (kind >= 0) { std::memcpy(p, p0, sizeof(p)); coef.assign(11 * nn, 0.0); }
+  const double t0 = kind >= 0 ? p0[2] : 0.0;
+  for (int n = 0; n < nsteps; ++n) {
+    for (int st = 0; st < T.s; ++st) {
+      bool used = false;  // a stage that no later stage and no weight uses is skipped
+      for (int i = st + 1; i < T.s; ++i) used |= T.a[i][st] != 0.0;
+      if (!used && T.b[st] == 0.0) continue;
+      for (long q = 0; q < nn; ++q) {
+        double sp = 0.0, sq = 0.0;
+        for (int j = 0; j < st; ++j) { sp += T.a[st][j] * kP[j][q]; sq += T.a[st][j] * kQ[j][q]; }
+        Ps[q] = Phi[q] + dt * sp; Qs[q] = Pi[q] + dt * sq;
+      }
+      if (kind >= 0) { p[2] = t0 + n * dt + T.c[st] * dt; sample_background(m, kind, p, coef.data()); }
+      or_rhs_curved(h, coef.data(), Ps.data(), Qs.data(), kP[st].data(), kQ[st].data(), eps_ko, bc, use_metric,
+                    nullptr);
+    }
+    for (long q = 0; q < nn; ++q) {
+      double sp = 0.0, sq = 0.0;
+      for (int j = 0; j < T.s; ++j) { sp += T.b[j] * kP[j][q]; sq += T.b[j] * kQ[j][q]; }
+      Phi[q] += dt * sp; Pi[q] += dt * sq;
+    }
+  }
+}
+
 // RK4 on the second-order SIPG system written first order: (u, v = u_t) with
 //   u' = v + eps mu^-5 sum_d D_d^6 u,   v' = L_SAT u (+ Sommerfeld) + eps mu^-5 sum_d D_d^6 v.
 void or_sipg_f(void* h, const double* u, const double* v, double* du, double* dv, const double* bvals,

@@ -85,6 +85,7 @@ struct wt_ws {
   void* compP = nullptr;
   void* compQ = nullptr;
   const void* comp_for[2] = {nullptr, nullptr};
+  void* erk = nullptr;    // explicit RK stage slopes: 2 x 8 x nn (Phi slopes, then Pi slopes)
 };
 
 namespace {
@@ -973,7 +974,7 @@ int wt_workspace_destroy(wt_ws* ws) {
   if (!ws) return WT_EINVAL;
   cudaStreamSynchronize(ws->ctx->stream);
   void* bufs[] = {ws->F, ws->bbuf, ws->grad, ws->kP, ws->kQ, ws->S0, ws->S1, ws->SQ, ws->accP, ws->accQ,
-                  ws->trace, ws->zero, ws->Lu, ws->compP, ws->compQ};
+                  ws->trace, ws->zero, ws->Lu, ws->compP, ws->compQ, ws->erk};
   for (void* p : bufs)
     if (p) cudaFree(p);
   delete ws;
@@ -1222,6 +1223,87 @@ static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* P
   return 0;
 }
 
+// Butcher tableaus of the fixed-step explicit Runge-Kutta methods that
+// pick_integrator_first_order selects (src/evolve.jl:43-48; evolve3d calls them
+// with adaptive = false, src/evolve.jl:1311): the classic RK4 and Tsit5
+// (Ch. Tsitouras, "Runge-Kutta pairs of order 5(4) satisfying only the first
+// column simplifying assumption", Comput. Math. Appl. 62 (2011) 770-775: the
+// fifth-order solution).  Tsit5's seventh stage has weight 0 (it only serves
+// the embedded error estimate and the first-same-as-last reuse), so a fixed
+// step evaluates six stages.
+struct ErkTableau {
+  int s = 0;
+  double c[8] = {};
+  double A[8][8] = {};
+  double b[8] = {};
+};
+
+static const ErkTableau* erk_tableau(int method) {
+  static ErkTableau rk4, tsit5;
+  static bool init = false;
+  if (!init) {
+    rk4.s = 4;
+    const double c4[4] = {0.0, 0.5, 0.5, 1.0};
+    const double b4[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+    for (int i = 0; i < 4; ++i) { rk4.c[i] = c4[i]; rk4.b[i] = b4[i]; }
+    rk4.A[1][0] = 0.5; rk4.A[2][1] = 0.5; rk4.A[3][2] = 1.0;
+    tsit5.s = 7;
+    const double c7[7] = {0.0, 0.161, 0.327, 0.9, 0.9800255409045097, 1.0, 1.0};
+    for (int i = 0; i < 7; ++i) tsit5.c[i] = c7[i];
+    const double a[7][6] = {
+        {0, 0, 0, 0, 0, 0},
+        {0.161, 0, 0, 0, 0, 0},
+        {-0.008480655492356989, 0.335480655492357, 0, 0, 0, 0},
+        {2.897153057105493, -6.359448489975075, 4.3622954328695815, 0, 0, 0},
+        {5.325864828439257, -11.748883564062828, 7.4955393428898365, -0.09249506636175525, 0, 0},
+        {5.86145544294642, -12.92096931784711, 8.159367898576159, -0.071584973281401, -0.028269050394068383, 0},
+        {0.09646076681806523, 0.01, 0.4798896504144996, 1.379008574103742, -3.290069515436081, 2.324710524099774}};
+    for (int i = 0; i < 7; ++i)
+      for (int j = 0; j < 6; ++j) tsit5.A[i][j] = a[i][j];
+    for (int j = 0; j < 6; ++j) tsit5.b[j] = a[6][j];  // first same as last: b = the last row
+    tsit5.b[6] = 0.0;
+    init = true;
+  }
+  return method == WT_ERK_RK4 ? &rk4 : method == WT_ERK_TSIT5 ? &tsit5 : nullptr;
+}
+
+// One fixed step of an explicit RK method (general tableau, stage slopes kept
+// in ws->erk): stage states y + dt sum_j a_ij k_j, the RHS at the stage time
+// (time-dependent backgrounds re-sampled), then y += dt sum_j b_j k_j.
+static int step_erk_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
+                         const ErkTableau& T, double eps_ko, const wt::ConsBC& b, int use_metric) {
+  const wt::DevMesh& m = ws->mesh->m;
+  cudaStream_t s = ctx->stream;
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  char* base = static_cast<char*>(ws->erk);
+  const void* kP[8];
+  const void* kQ[8];
+  for (int j = 0; j < 8; ++j) { kP[j] = base + j * nb; kQ[j] = base + (8 + j) * nb; }
+  int last = T.s - 1;
+  while (last > 0 && T.b[last] == 0.0) --last;  // stages past the last nonzero weight do not contribute
+  for (int st = 0; st <= last; ++st) {
+    const void* inP = Phi;
+    const void* inQ = Pi;
+    if (st > 0) {
+      WT_TRY(lrc(ctx, wt::launch_erk_combine(m.nn, m.precision, dt, Phi, ws->S0, st, kP, T.A[st], s), "RK stage"));
+      WT_TRY(lrc(ctx, wt::launch_erk_combine(m.nn, m.precision, dt, Pi, ws->SQ, st, kQ, T.A[st], s), "RK stage"));
+      ctx->launches += 2;
+      inP = ws->S0;
+      inQ = ws->SQ;
+    }
+    if (coef->td) WT_TRY(coef_resample(ctx, coef, T.c[st] * dt, s));
+    WT_TRY(rhs_curved_impl(ctx, ws, coef, inP, inQ, (void*)kP[st], (void*)kQ[st], eps_ko, b, use_metric));
+  }
+  WT_TRY(lrc(ctx, wt::launch_erk_combine(m.nn, m.precision, dt, Phi, Phi, last + 1, kP, T.b, s), "RK step"));
+  WT_TRY(lrc(ctx, wt::launch_erk_combine(m.nn, m.precision, dt, Pi, Pi, last + 1, kQ, T.b, s), "RK step"));
+  ctx->launches += 2;
+  if (coef->td) {
+    WT_TRY(lrc(ctx, wt::launch_advance_time(coef->d_t, dt, s), "background time"));
+    ctx->launches += 1;
+  }
+  return 0;
+}
+
 }  // extern "C"
 
 // Capture one step (any stream may be the caller's, including the legacy
@@ -1280,6 +1362,47 @@ int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, v
   }
   if (!rc && coef->td) coef->t += nsteps * dt;  // the device copy was advanced step by step
   return rc;
+}
+
+int wt_step_erk_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
+                       int method, double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  WT_TRY(check_ws(ctx, ws));
+  const ErkTableau* T = erk_tableau(method);
+  if (!T) return fail(ctx, WT_EINVAL, "wt_step_erk_curved: unknown method " + std::to_string(method));
+  if (method == WT_ERK_RK4)  // the fused low-storage stages
+    return wt_step_rk4_curved(ctx, ws, coef, Phi, Pi, dt, nsteps, eps_ko, bc, use_metric);
+  if (!coef || !Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_step_erk_curved: NULL argument");
+  if (nsteps < 0) return fail(ctx, WT_EINVAL, "nsteps must be >= 0");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(ctx, WT_EINVAL, "dt must be positive and finite");
+  wt::ConsBC b;
+  WT_TRY(make_bc(ctx, bc, use_metric, b));
+  WT_TRY(ws_step_buffers(ws));
+  const wt::DevMesh& m = ws->mesh->m;
+  WT_TRY(ensure(ws, &ws->erk, 16 * (size_t)m.nn * rsize(m.precision)));
+  if (eps_ko != 0.0) WT_TRY(ensure_mu(ws));
+  if (coef->td) WT_TRY(need_setup_geometry(coef->mesh, "wt_step_erk_curved (time-dependent background)"));
+  int rc = 0;
+  if (nsteps <= 2) {
+    for (int i = 0; i < nsteps && !rc; ++i) rc = step_erk_once(ctx, ws, coef, Phi, Pi, dt, *T, eps_ko, b, use_metric);
+  } else {
+    rc = replay_graph(ctx, nsteps,
+                      [&]() { return step_erk_once(ctx, ws, coef, Phi, Pi, dt, *T, eps_ko, b, use_metric); });
+  }
+  if (!rc && coef->td) coef->t += nsteps * dt;
+  return rc;
+}
+
+int wt_erk_tableau(int method, int* stages, double* c, double* A, double* b) {
+  const ErkTableau* T = erk_tableau(method);
+  if (!T || !stages) return WT_EINVAL;
+  *stages = T->s;
+  for (int i = 0; i < T->s; ++i) {
+    if (c) c[i] = T->c[i];
+    if (b) b[i] = T->b[i];
+    if (A)
+      for (int j = 0; j < T->s; ++j) A[i * T->s + j] = T->A[i][j];
+  }
+  return 0;
 }
 
 static int step_sipg_once(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, const double bv[6], double tau,

@@ -170,6 +170,9 @@ int launch_streamed_geometry(DevMesh& m, cudaStream_t s);
 int launch_background(const DevMesh& m, DevCoef& c, int kind, const double* p, cudaStream_t s,
                       const double* d_t = nullptr, double toff = 0.0);
 int launch_advance_time(double* d_t, double dt, cudaStream_t s);
+// out = y + dt * sum_{j < nk} a_j k_j (nk <= 8)
+int launch_erk_combine(long long n, int precision, double dt, const void* y, void* out, int nk, const void* const* k,
+                       const double* a, cudaStream_t s);
 int launch_coef_combine(const DevMesh& m, DevCoef& c, cudaStream_t s);
 int launch_min_spacing(const DevMesh& m, double* out, cudaStream_t s);
 int launch_initial(const DevMesh& m, int kind, const double* dparams, int np, double t, void* u, void* ut,

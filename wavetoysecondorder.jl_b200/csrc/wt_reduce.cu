@@ -4,6 +4,8 @@
 // a fixed order, so results are deterministic run to run.
 #include "wt_common.cuh"
 
+#include <algorithm>
+
 namespace wt {
 
 static constexpr int RB = 256;
@@ -79,6 +81,39 @@ __global__ void k_axpy(long long n, real* __restrict__ y, real a, const real* __
     y[i] = y[i] + a * x[i];
 }
 // low-storage classic RK4 stage update (same arithmetic as the fused epilogue)
+// Explicit RK stage/step combination: out = y + dt * sum_j a_j k_j (j < nk),
+// summed in j order.
+struct ErkSum {
+  const void* k[8];
+  double a[8];
+  int nk;
+};
+template <typename real>
+__global__ void k_erk_combine(long long n, double dt, const real* __restrict__ y, real* __restrict__ out, ErkSum S) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    real acc = 0;
+    for (int j = 0; j < S.nk; ++j) acc += (real)S.a[j] * ((const real*)S.k[j])[i];
+    out[i] = y[i] + (real)dt * acc;
+  }
+}
+
+int launch_erk_combine(long long n, int precision, double dt, const void* y, void* out, int nk, const void* const* k,
+                       const double* a, cudaStream_t s) {
+  if (nk < 0 || nk > 8) return -1;
+  ErkSum S;
+  S.nk = nk;
+  for (int j = 0; j < 8; ++j) {
+    S.k[j] = j < nk ? k[j] : nullptr;
+    S.a[j] = j < nk ? a[j] : 0.0;
+  }
+  const unsigned grid = (unsigned)std::min<long long>((n + 255) / 256, 4096);
+  if (precision == 0)
+    k_erk_combine<double><<<grid, 256, 0, s>>>(n, dt, (const double*)y, (double*)out, S);
+  else
+    k_erk_combine<float><<<grid, 256, 0, s>>>(n, dt, (const float*)y, (float*)out, S);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 template <typename real>
 __global__ void k_rk_update(long long n, int stage, double dt, real* __restrict__ y, real* __restrict__ acc,
                             real* __restrict__ out, const real* __restrict__ k, real* __restrict__ comp) {

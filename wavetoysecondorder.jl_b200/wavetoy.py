@@ -28,6 +28,8 @@ EXCISION_BDRY_TAG = 8
 BG_MINKOWSKI, BG_CONSTANT_SHIFT, BG_ADM_PERTURBED, BG_RADIAL_SHIFT = 0, 1, 2, 3
 # time-dependent backgrounds from a spacetime metric (MetricBackground3D): params (A, d, t0)
 BG_GAUGE_WAVE, BG_SINE_SHIFT = 4, 5
+# fixed-step explicit Runge-Kutta methods (pick_integrator_first_order)
+ERK_RK4, ERK_TSIT5 = 0, 1
 IC_EIGENMODE_CARTESIAN, IC_GAUSSIANS, IC_OUTGOING_PULSE, IC_PLANE_WAVE, IC_EIGENMODE_RADIAL = 0, 1, 2, 3, 4
 # precision forms of an FP32 mesh (n = 8 contractions): CUDA cores, split BF16 three-term / two-term
 FP32_CUDA_CORES, FP32_BF16X3, FP32_BF16X2 = 0, 1, 2
@@ -119,6 +121,8 @@ def library():
         "wt_energy": [vp, vp, vp, vp, vp, i, C.POINTER(d)], "wt_energy_sipg": [vp, vp, vp, vp, d, C.POINTER(d)],
         "wt_l2_diff": [vp, vp, vp, vp, i, C.POINTER(d)],
         "wt_step_rk4_curved": [vp, vp, vp, vp, vp, d, i, d, C.POINTER(_BcDesc), i],
+        "wt_step_erk_curved": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i],
+        "wt_erk_tableau": [i, C.POINTER(i), vp, vp, vp],
         "wt_step_rk4_sipg": [vp, vp, vp, vp, d, i, C.POINTER(C.c_double * 6), d, d, d],
         "wt_evolve_curved_host": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i, vp],
         "wt_evolve_curved_host_f32": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i, vp],
@@ -749,6 +753,28 @@ def step_rk4_curved(Phi, Pi, coef: Coef, ws: Workspace, dt: float, nsteps: int, 
     ws.ctx.check(library().wt_step_rk4_curved(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt), int(nsteps),
                                               float(eps_KO), p, int(metric)), "step_rk4_curved")
     return Phi, Pi
+
+
+def step_erk_curved(Phi, Pi, coef: Coef, ws: Workspace, dt: float, nsteps: int, method: int = ERK_TSIT5,
+                    eps_KO: float = 0.0, bc3d: Optional[BC3D] = None, metric: bool = False):
+    """nsteps fixed-dt steps of the explicit RK method pick_integrator_first_order selects
+    (src/evolve.jl:43-48; ERK_TSIT5 for N 5-6, ERK_RK4 for N <= 4), adaptive = false."""
+    p, keep = _bcptr(bc3d)
+    ws.ctx.check(library().wt_step_erk_curved(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt), int(nsteps),
+                                              int(method), float(eps_KO), p, int(metric)), "step_erk_curved")
+    return Phi, Pi
+
+
+def erk_tableau(method: int):
+    """(c, A, b) of the library's Butcher tableau for method (host only)."""
+    import numpy as np
+    st = C.c_int()
+    if library().wt_erk_tableau(int(method), C.byref(st), None, None, None) != 0:
+        raise WaveToyError(-1, f"unknown method {method}")
+    n = st.value
+    c, A, b = np.zeros(n), np.zeros(n * n), np.zeros(n)
+    library().wt_erk_tableau(int(method), C.byref(st), c.ctypes.data, A.ctypes.data, b.ctypes.data)
+    return c, A.reshape(n, n), b
 
 
 def step_rk4_sipg(u, ut, ws: Workspace, dt: float, nsteps: int, bdry_values=(0,) * 6, tau: float = 20.0,
