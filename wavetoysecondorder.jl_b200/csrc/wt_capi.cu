@@ -1566,12 +1566,16 @@ static int evolve_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi_ho
       return WT_ENOMEM;
     }
   void *dP = buf[0], *dQ = buf[1], *sP = buf[2], *sQ = buf[3];
-  cudaStream_t cs = nullptr;
-  cudaEvent_t staged = nullptr, copied = nullptr;
+  // one copy stream per field, so that the two device-to-host copies can run on
+  // separate copy engines at the same time
+  cudaStream_t cs = nullptr, cs2 = nullptr;
+  cudaEvent_t staged = nullptr, copied = nullptr, copied2 = nullptr;
   int rc = 0;
   if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&cs2, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&staged, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&copied, cudaEventDisableTiming) != cudaSuccess)
+      cudaEventCreateWithFlags(&copied, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&copied2, cudaEventDisableTiming) != cudaSuccess)
     rc = fail(ctx, WT_ECUDA, std::string(name) + ": stream or event creation failed");
   if (!rc) {
     cudaMemcpyAsync(dP, Phi_host, nb, cudaMemcpyHostToDevice, ctx->stream);
@@ -1585,23 +1589,31 @@ static int evolve_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi_ho
     if (!rc) rc = wt_ctx_nonfinite(ctx, &bad);
     if (!rc && bad) rc = fail(ctx, WT_ENONFINITE, "state became non-finite during evolution");
     if (rc) break;
-    if (sidx > 0) cudaStreamWaitEvent(ctx->stream, copied, 0);  // the previous sample has left the staging pair
+    if (sidx > 0) {  // the previous sample has left the staging pair
+      cudaStreamWaitEvent(ctx->stream, copied, 0);
+      cudaStreamWaitEvent(ctx->stream, copied2, 0);
+    }
     cudaMemcpyAsync(sP, dP, nb, cudaMemcpyDeviceToDevice, ctx->stream);
     cudaMemcpyAsync(sQ, dQ, nb, cudaMemcpyDeviceToDevice, ctx->stream);
     cudaEventRecord(staged, ctx->stream);
     cudaStreamWaitEvent(cs, staged, 0);
+    cudaStreamWaitEvent(cs2, staged, 0);
     cudaMemcpyAsync(Phi_host, sP, nb, cudaMemcpyDeviceToHost, cs);
-    cudaMemcpyAsync(Pi_host, sQ, nb, cudaMemcpyDeviceToHost, cs);
+    cudaMemcpyAsync(Pi_host, sQ, nb, cudaMemcpyDeviceToHost, cs2);
     cudaEventRecord(copied, cs);
+    cudaEventRecord(copied2, cs2);
   }
-  if (cs) {
-    cudaError_t e = cudaStreamSynchronize(cs);
-    if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, name);
-  }
+  for (cudaStream_t c : {cs, cs2})
+    if (c) {
+      cudaError_t e = cudaStreamSynchronize(c);
+      if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, name);
+    }
   cudaStreamSynchronize(ctx->stream);
   if (staged) cudaEventDestroy(staged);
   if (copied) cudaEventDestroy(copied);
+  if (copied2) cudaEventDestroy(copied2);
   if (cs) cudaStreamDestroy(cs);
+  if (cs2) cudaStreamDestroy(cs2);
   for (void* p : buf) cudaFree(p);
   return rc;
 }
