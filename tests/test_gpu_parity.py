@@ -180,6 +180,27 @@ def test_energy(wt, ctx, O, um):
     assert abs(Eg - Eo) / abs(Eo) < 1e-12
 
 
+@pytest.mark.parametrize("prec,form", [(0, None), (1, 0), (1, 1)])
+def test_energy_n8_gradient_path(wt, ctx, O, prec, form):
+    """wave3d_energy on an n = 8 curvilinear mesh, where the split-form gradient runs
+    through the n = 8 kernels' gradient-only mode (FP64 tensor cores, FP32 CUDA cores
+    and split BF16), against the oracle."""
+    import torch
+    g, o = pair(wt, ctx, O, 8, (3, 2, 2), A=0.05, outer_tag=7, precision=prec)
+    if form is not None:
+        g.set_fp32_form(form)
+    p = wt.workloads.adm_params(12)
+    cg, co = wt.sample_background3d(g, 2, p), o.background(2, p)
+    ws = wt.make_wave3d_workspace(g)
+    x, y, z = o.coords()
+    Phi = np.sin(3 * x) * np.cos(2 * y + z)
+    Pi = 0.5 * np.cos(x - y) * np.sin(2 * z)
+    t = torch.float64 if prec == 0 else torch.float32
+    Eg = wt.wave3d_energy(dev(t, Phi), dev(t, Pi), cg, ws, metric=True)
+    Eo = o.energy(co, Phi, Pi, use_metric=True)
+    assert abs(Eg - Eo) / abs(Eo) < (1e-12 if prec == 0 else 1e-5)
+
+
 @pytest.mark.parametrize("tags,R", [(0, math.inf), (7, math.inf), (7, 1.5)])
 def test_rhs_sipg(wt, ctx, O, tags, R):
     import torch

@@ -1125,8 +1125,12 @@ int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, cons
   wt::DevCoef nocoef;
   wt::ConsBC bc;
   wt::RKStage rk;
-  WT_TRY(lrc(ctx, wt::launch_cons_k1(m, nocoef, Phi, nullptr, nullptr, nullptr, nullptr, ws->grad, use_metric, bc,
-                                     rk, ctx->stream), "energy gradient"));
+  auto a16 = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+  if (m.N == 8 && use_metric && m.Ja_n8 && a16(Phi) && a16(ws->grad) && a16(m.invdetJ_r))
+    WT_TRY(lrc(ctx, wt::launch_grad_n8(m, Phi, ws->grad, m.errflag, ctx->stream), "energy gradient"));
+  else
+    WT_TRY(lrc(ctx, wt::launch_cons_k1(m, nocoef, Phi, nullptr, nullptr, nullptr, nullptr, ws->grad, use_metric, bc,
+                                       rk, ctx->stream), "energy gradient"));
   WT_TRY(lrc(ctx, wt::launch_energy(m, coef->c, Pi, ws->grad, use_metric, ctx->d_partial, ctx->nblocks, ctx->stream),
              "energy"));
   ctx->launches += 2;

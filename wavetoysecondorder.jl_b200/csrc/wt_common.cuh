@@ -217,6 +217,8 @@ int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
                       const RKStage& rk, unsigned* flag, cudaStream_t s);
 int launch_pad_metric_n8(DevMesh& m, cudaStream_t s);
+// the split-form gradient of Phi through the n = 8 kernels (3 fields of nn words into grad)
+int launch_grad_n8(const DevMesh& m, const void* Phi, void* grad, unsigned* flag, cudaStream_t s);
 long long n8_padded_field_size(long long Ne);
 // True when an RHS evaluation takes the n = 8 pipelined path (both kernels take
 // the same path: K1 then writes F in the padded layout K2 reads).

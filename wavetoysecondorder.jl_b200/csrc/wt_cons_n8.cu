@@ -318,6 +318,7 @@ struct K1N8 {
   real* comp;
   unsigned* flag;
   float Gh[64];  // 0.5 G in FP32 (the CUDA-core form reads it from the constant bank)
+  real* gout;    // gradient-only launches (GR): the three components of the split-form gradient
 };
 
 // Boundary terms of K1 at a node on an outer face (the curvilinear boundary
@@ -392,13 +393,16 @@ constexpr size_t k1_smem() {
 // persistent loop runs over a work list of (solve, element) tiles and every
 // tile reads the parameter block of its solve (plist); P then only supplies
 // what is common to the launch (stage, operator, status word).
-template <typename real, int NT, bool BATCH>
+// GR: gradient-only instantiation (the energy's apply_gradient3d!, src/wave3d_curved.jl:275-280):
+// no coefficients, Pi or RK state are read; the node phase writes the gradient to P.gout.
+template <typename real, int NT, bool BATCH, bool GR = false>
 __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
     k_cons_k1_n8(const K1N8<real> P, const K1N8<real>* __restrict__ plist, const int2* __restrict__ tiles,
                  long long ntiles) {
   using namespace n8;
   constexpr bool F64 = std::is_same<real, double>::value;
   constexpr bool SC = StageCoef<real>::value;
+  constexpr int NCOPY_C = SC && !GR ? 10 : 0;  // coefficient blocks copied per stage
   constexpr size_t K1_STAGE = k1_stage<real>();
   constexpr int FS = Lay<real>::FS, PSZ = PhiLay<real>::SZ;
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -417,7 +421,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
   const bool need_y = P.epi && (P.stage == 1 || P.stage == 2 || (comp_on && P.stage == 3));
   const bool need_acc = P.epi && P.stage >= 1;
   const bool need_comp = comp_on && P.stage == 3;
-  const unsigned tx_bytes = (unsigned)(K1_STAGE * sizeof(real));
+  const unsigned tx_bytes = (unsigned)((K1_STAGE - (SC ? 10 - NCOPY_C : 0) * (size_t)N3) * sizeof(real));
   // node-phase coordinates of this thread
   const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
   const int tpad = Lay<real>::at(tid), tphi = PhiLay<real>::at(tid);
@@ -454,7 +458,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
     real* d = stg + s * K1_STAGE;
     // copies: Phi (unless it goes through registers), 9 Ja, 10 coefficients
     constexpr int NPHI = PHIR ? 0 : 1;
-    for (int c = lane; c < NPHI + 9 + (SC ? 10 : 0); c += 32) {
+    for (int c = lane; c < NPHI + 9 + NCOPY_C; c += 32) {
       if (c < NPHI) {
         bulk_g2s(d, Q.Phi + e * N3, N3 * (unsigned)sizeof(real), &bar[s]);
       } else if (c < NPHI + 9) {
@@ -485,13 +489,14 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
     if (tl.x < 0) return;
     const K1N8<real>& Q = prm(tl.x);
     const long long n = (long long)tl.y * N3 + tid;
+    if constexpr (PHIR) w.phi = Q.Phi[n];
+    w.invJ = Q.invdetJ[n];
+    if constexpr (GR) return;
     if constexpr (!SC) {
 #pragma unroll
       for (int c = 0; c < 10; ++c) w.c[c] = Q.c10[c * Q.nn + n];
     }
     w.Pi = Q.Pi[n];
-    if constexpr (PHIR) w.phi = Q.Phi[n];
-    w.invJ = Q.invdetJ[n];
     w.y = need_y ? Q.y[n] : (real)0;
     w.acc = need_acc ? Q.acc[n] : (real)0;
     w.comp = need_comp ? Q.comp[n] : (real)0;
@@ -662,6 +667,11 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
       real g1 = (sg[FS + tpad] + sg[4 * FS + tpad]) + sg[7 * FS + tpad];
       real g2 = (sg[2 * FS + tpad] + sg[5 * FS + tpad]) + sg[8 * FS + tpad];
       g0 *= cur.invJ; g1 *= cur.invJ; g2 *= cur.invJ;
+      if constexpr (GR) {
+        Q.gout[n] = g0;
+        Q.gout[Q.nn + n] = g1;
+        Q.gout[2 * Q.nn + n] = g2;
+      } else {
       real cc[10];
 #pragma unroll
       for (int c = 0; c < 10; ++c) cc[c] = SC ? d[PSZ + 9 * FS + c * N3 + tid] : cur.c[c];
@@ -685,6 +695,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
                     P.flag);
       else
         Q.Phidot[n] = phid;
+      }  // !GR
     }
     if (has_next && tid < 6 * N2) sface[(fb ^ 1) * 6 * N2 + tid] = fnext;
     if constexpr (PHIR)
@@ -1137,7 +1148,7 @@ constexpr size_t k2c_smem() {
   return (K2C_NS * K2C_STAGE + 3 * n8::LayC::FS + 2 * 6 * 3 * n8::N2 + K2C_B) * sizeof(float) + 64;
 }
 
-template <bool BATCH>
+template <bool BATCH, bool GR = false>  // GR: gradient only (see k_cons_k1_n8)
 __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
     k_cons_k1_n8c(const __grid_constant__ K1N8<float> P, const K1N8<float>* __restrict__ plist,
                   const int2* __restrict__ tiles, long long ntiles) {
@@ -1164,7 +1175,7 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
   const bool need_acc = P.epi && P.stage >= 1;
   const bool need_comp = comp_on && P.stage == 3;
   const unsigned txA = (unsigned)(K1C_STAGE * sizeof(real));
-  const unsigned txB = (unsigned)((12 + need_y + need_acc + need_comp) * N3 * sizeof(real));
+  const unsigned txB = (unsigned)((GR ? 1 : 12 + need_y + need_acc + need_comp) * N3 * sizeof(real));
   const long long T = BATCH ? ntiles : P.Ne;
   const long long GS = gridDim.x;
   auto tile_at = [&](long long t) -> int2 {
@@ -1211,7 +1222,9 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
     __syncwarp();
     const unsigned nb = N3 * (unsigned)sizeof(real);
     const real* src = nullptr;
-    if (lane < 10) src = Q.c10 + lane * Q.nn + o;
+    if (GR) {
+      if (lane == 11) src = Q.invdetJ + o;
+    } else if (lane < 10) src = Q.c10 + lane * Q.nn + o;
     else if (lane == 10) src = Q.Pi + o;
     else if (lane == 11) src = Q.invdetJ + o;
     else if (lane == 12 && need_y) src = Q.y + o;
@@ -1339,6 +1352,12 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
       real g1 = (sg[FSC + at] + sg[4 * FSC + at]) + sg[7 * FSC + at];
       real g2 = (sg[2 * FSC + at] + sg[5 * FSC + at]) + sg[8 * FSC + at];
       g0 *= invJ; g1 *= invJ; g2 *= invJ;
+      if constexpr (GR) {
+        Q.gout[n] = g0;
+        Q.gout[Q.nn + n] = g1;
+        Q.gout[2 * Q.nn + n] = g2;
+        continue;
+      }
       real cc[10];
 #pragma unroll
       for (int c = 0; c < 10; ++c) cc[c] = sB[c * N3 + node];
@@ -1662,6 +1681,7 @@ static K1N8<real> k1n8_params(const DevMesh& m, const DevCoef& c, const void* Ph
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
   for (int i = 0; i < 64; ++i) P.Gh[i] = (float)(0.5 * m.ops.G[i]);
+  P.gout = nullptr;
   return P;
 }
 
@@ -1779,6 +1799,53 @@ int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* 
   }
   const K2N8<float> P = k2n8_params<float>(m, F, Pidot, bbuf, bc, rk, flag);
   return n8_dispatch<false>(2, 1, m.fp32_form, &P, nullptr, nullptr, m.Ne, s);
+}
+
+// Gradient-only launch (the energy's split-form gradient, apply_gradient3d! with the
+// centred-flux SAT) through the n = 8 kernels: gout = 3 fields of nn words.
+template <typename real, int NT>
+static int launch_grad_n8_t(const K1N8<real>& P, bool cuda_core, cudaStream_t s) {
+  if constexpr (std::is_same<real, float>::value) {
+    if (cuda_core) {
+      static bool attr = false;
+      if (!attr) {
+        if (cudaFuncSetAttribute(k_cons_k1_n8c<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)k1c_smem()) != cudaSuccess ||
+            cudaFuncSetAttribute(k_cons_k1_n8c<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+          return -2;
+        attr = true;
+      }
+      const long long cap = (long long)sm_count() * K1C_OCC, grid = P.Ne < cap ? P.Ne : cap;
+      k_cons_k1_n8c<false, true><<<(unsigned)grid, n8::CTHR, k1c_smem(), s>>>(P, nullptr, nullptr, P.Ne);
+      return cudaGetLastError() == cudaSuccess ? 0 : -2;
+    }
+  }
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_cons_k1_n8<real, NT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)k1_smem<real>()) != cudaSuccess)
+      return -2;
+    attr = true;
+  }
+  const long long cap = (long long)sm_count() * n8::Occ<real>::k1, grid = P.Ne < cap ? P.Ne : cap;
+  k_cons_k1_n8<real, NT, false, true><<<(unsigned)grid, n8::THREADS, k1_smem<real>(), s>>>(P, nullptr, nullptr, P.Ne);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int launch_grad_n8(const DevMesh& m, const void* Phi, void* grad, unsigned* flag, cudaStream_t s) {
+  DevCoef none;
+  ConsBC bc;
+  RKStage rk;
+  if (m.precision == 0) {
+    K1N8<double> P = k1n8_params<double>(m, none, Phi, nullptr, nullptr, nullptr, nullptr, bc, rk, flag);
+    P.gout = (double*)grad;
+    return launch_grad_n8_t<double, 0>(P, false, s);
+  }
+  K1N8<float> P = k1n8_params<float>(m, none, Phi, nullptr, nullptr, nullptr, nullptr, bc, rk, flag);
+  P.gout = (float*)grad;
+  if (m.fp32_form == WT_FP32_BF16X2) return launch_grad_n8_t<float, 2>(P, false, s);
+  return launch_grad_n8_t<float, 3>(P, m.fp32_form == WT_FP32_CUDA_CORES, s);
 }
 
 // ---- work-list batching -------------------------------------------------------------
