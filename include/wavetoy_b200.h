@@ -77,6 +77,12 @@ int wt_ctx_launch_count(const wt_ctx* ctx, long long* count);
  * state stops being finite (the reference asserts all(isfinite, ...) per
  * sample, src/evolve.jl:1344); synchronous. */
 int wt_ctx_nonfinite(wt_ctx* ctx, int* flag);
+/* Self-test of the bounded-wait failure path (no counterpart in the reference):
+ * one thread polls an mbarrier as the pipelined kernels do, at most `polls`
+ * times (1..2^24), after arriving on it (arrive = 1: returns 0) or not
+ * (arrive = 0: the wait gives up, sets the status word and the call returns
+ * WT_ETIMEOUT); the context stays usable.  Nothing faults or waits unbounded. */
+int wt_ctx_selftest_wait(wt_ctx* ctx, int arrive, long long polls);
 /* Per-kernel timing for measurement: while enabled, the fused RK4 step records
  * CUDA events around each launch of its two kernels (gradient/flux and
  * divergence) on the launching stream; wt_ctx_profile_read synchronises and

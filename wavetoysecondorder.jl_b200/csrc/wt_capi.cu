@@ -527,6 +527,16 @@ int wt_ctx_nonfinite(wt_ctx* ctx, int* flag) {
   return 0;
 }
 
+int wt_ctx_selftest_wait(wt_ctx* ctx, int arrive, long long polls) {
+  if (!ctx) return WT_EINVAL;
+  if (polls < 1 || polls > (1LL << 24)) return fail(ctx, WT_EINVAL, "wt_ctx_selftest_wait: polls must be in 1..2^24");
+  int bad = 0;
+  WT_TRY(wt_ctx_nonfinite(ctx, &bad));  // start from a clear status word
+  WT_TRY(lrc(ctx, wt::launch_wait_selftest(polls, arrive, ctx->d_flag, ctx->stream), "wait self-test"));
+  ctx->launches += 1;
+  return wt_ctx_nonfinite(ctx, &bad);
+}
+
 // ---- reference element ------------------------------------------------------------
 int wt_gll_operators(int N, double* x, double* H, double* G) {
   if (N < 2 || N > WT_MAXN || !x || !H || !G) return WT_EINVAL;

@@ -217,6 +217,8 @@ int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
                       const RKStage& rk, unsigned* flag, cudaStream_t s);
 int launch_pad_metric_n8(DevMesh& m, cudaStream_t s);
+// bounded-wait self-test (see k_wait_selftest)
+int launch_wait_selftest(long long polls, int arrive, unsigned* flag, cudaStream_t s);
 // the split-form gradient of Phi through the n = 8 kernels (3 fields of nn words into grad)
 int launch_grad_n8(const DevMesh& m, const void* Phi, void* grad, unsigned* flag, cudaStream_t s);
 long long n8_padded_field_size(long long Ne);

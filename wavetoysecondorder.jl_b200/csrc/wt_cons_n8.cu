@@ -1848,6 +1848,27 @@ int launch_grad_n8(const DevMesh& m, const void* Phi, void* grad, unsigned* flag
   return launch_grad_n8_t<float, 3>(P, m.fp32_form == WT_FP32_CUDA_CORES, s);
 }
 
+// Self-test of the bounded-wait failure path: one thread polls an mbarrier the
+// way the pipelined kernels do -- at most `polls` times, then it sets bit 1 of
+// the status word and returns.  With arrive = 1 the barrier's phase completes
+// first (a plain arrive) and the wait succeeds.  Nothing faults and nothing
+// waits without a bound.
+__global__ void k_wait_selftest(long long polls, int arrive, unsigned* flag) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  n8::mbar_init(&bar, 1);
+  n8::fence_barrier_init();
+  if (arrive) n8::mbar_expect_tx(&bar, 0u);
+  for (long long it = 0; it < polls; ++it)
+    if (n8::mbar_try_wait(&bar, 0)) return;
+  atomicOr(flag, 2u);
+}
+
+int launch_wait_selftest(long long polls, int arrive, unsigned* flag, cudaStream_t s) {
+  k_wait_selftest<<<1, 32, 0, s>>>(polls, arrive, flag);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 // ---- work-list batching -------------------------------------------------------------
 size_t cons_n8_param_size(int precision, int which) {
   if (precision == 0) return which == 1 ? sizeof(K1N8<double>) : sizeof(K2N8<double>);

@@ -89,6 +89,7 @@ def library():
         "wt_ctx_create": [i, pvp], "wt_ctx_destroy": [vp], "wt_ctx_synchronize": [vp],
         "wt_ctx_get_stream": [vp, pvp], "wt_ctx_set_stream": [vp, vp],
         "wt_ctx_launch_count": [vp, C.POINTER(ll)], "wt_ctx_nonfinite": [vp, C.POINTER(i)],
+        "wt_ctx_selftest_wait": [vp, i, ll],
         "wt_mesh_create": [vp, C.POINTER(_MeshDesc), pvp],
         "wt_mesh_create_arrays": [vp, i, ll, vp, vp, vp, vp, vp, vp, i, pvp],
         "wt_mesh_create_patches": [vp, C.POINTER(_PatchDesc), pvp],
@@ -202,6 +203,11 @@ class Context:
         cnt = (C.c_longlong * 2)()
         self.check(library().wt_ctx_profile_read(self.h, C.byref(ms), C.byref(cnt)))
         return (ms[0], cnt[0]), (ms[1], cnt[1])
+
+    def selftest_wait(self, arrive: bool, polls: int = 1 << 16):
+        """Run the bounded-wait self-test (wt_ctx_selftest_wait): raises WaveToyError
+        (ETIMEOUT) when the wait gives up (arrive=False)."""
+        self.check(library().wt_ctx_selftest_wait(self.h, int(bool(arrive)), int(polls)), "wt_ctx_selftest_wait")
 
     def nonfinite(self) -> bool:
         f = C.c_int()
