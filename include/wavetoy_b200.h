@@ -406,6 +406,89 @@ int wt_batch_info(wt_batch* batch, int* nsolves, long long* nodes, int* ngroups)
 int wt_batch_group_info(wt_batch* batch, int group, int* N, int* precision, int* n8_path, int* epb_variant,
                         long long* tiles);
 
+/* ---- serving a stream of solve requests -------------------------------------
+ * No counterpart in the reference (one solve per evolve3d call,
+ * src/evolve.jl:1149-1358).  A server owns one batch on a context.  A request
+ * names an analytic mesh, a static background, initial data of Phi (Pi = 0), a
+ * CFL number and a step count, and arrives at a time on the server's clock
+ * (seconds since wt_serve_create).  Each scheduling round (wt_serve_poll):
+ *   1. requests whose arrival time has passed join the wait queue;
+ *   2. the queue is ordered (WT_SERVE_HRRN: highest response ratio
+ *      (wait + S) / S first, S = 2 nodes steps / rate + 0.05 s the estimated
+ *      service time; WT_SERVE_SJF: least nodes x steps first; WT_SERVE_FIFO:
+ *      arrival order; ties by arrival, then submission);
+ *   3. requests are admitted from the head of the queue while the admitted
+ *      ones' estimated device bytes fit hbm_budget, fewer than max_active run
+ *      and the running requests hold fewer than fill_nodes nodes; admission
+ *      builds the request's mesh, coefficients, workspace and state on the
+ *      device and adds it to the batch;
+ *   4. the batch advances by min(tick, the fewest steps any running request
+ *      has left) RK4 steps and the stream is synchronised; requests with no
+ *      steps left leave the batch (their finish time is taken here) and free
+ *      their memory (the final state stays while keep_results is set).
+ * A request's estimated bytes are nodes x (bytes per node of its running form +
+ * 272 for the FP64 set-up geometry held while it is built); the running form
+ * holds 520 (FP64, n = 8), 480 (FP64), 300 (FP32, n = 8) or 260 (FP32) bytes
+ * per node.  Results equal wt_step_rk4_curved on each request alone. */
+typedef struct wt_server wt_server;
+enum { WT_SERVE_HRRN = 0, WT_SERVE_SJF = 1, WT_SERVE_FIFO = 2 };
+#define WT_SERVE_AUTO (-1)  /* precision per request: FP32 when steps <= auto_fp32_max_steps, else FP64 */
+#define WT_SERVE_MAX_IC 128
+typedef struct {
+  double hbm_budget;         /* bytes the admitted requests may hold (estimate above) */
+  int tick;                  /* most RK4 steps per round, >= 1 */
+  int max_active;            /* most requests running together; 0 = no limit */
+  long long fill_nodes;      /* admit only while running requests hold fewer nodes; 0 = no limit */
+  int order;                 /* WT_SERVE_HRRN, WT_SERVE_SJF or WT_SERVE_FIFO */
+  int precision;             /* WT_F64, WT_F32 or WT_SERVE_AUTO */
+  int fp32_form;             /* wt_mesh_set_fp32_form of FP32 requests */
+  int auto_fp32_max_steps;   /* threshold of WT_SERVE_AUTO */
+  int keep_results;          /* keep each finished request's final state (wt_serve_result_state) */
+  double rate_f64, rate_f32; /* DOF-updates/s of the service estimate; <= 0: 3e9 and 6e9 */
+} wt_serve_desc;
+typedef struct {
+  double arrival;            /* seconds on the server's clock */
+  wt_mesh_desc mesh;         /* analytic mesh; precision is chosen by the server */
+  wt_background_desc bg;     /* static kinds only (the batch runs no time-dependent background) */
+  int ic_kind, nic;          /* wt_initial_data of Phi at t = 0 */
+  double ic[WT_SERVE_MAX_IC];
+  double cfl, max_speed;     /* dt = cfl * wt_mesh_min_spacing / max_speed */
+  int steps;                 /* RK4 steps, >= 1 */
+  wt_bc_desc bc;             /* data pointers must be NULL */
+} wt_serve_request;
+typedef struct {
+  int precision;             /* the form the request ran in */
+  long long nodes;
+  int steps;
+  double dt;
+  double arrival, admitted, finished;  /* server clock; latency = finished - arrival */
+} wt_serve_result;
+int wt_serve_create(wt_ctx* ctx, const wt_serve_desc* desc, wt_server** out);
+int wt_serve_destroy(wt_server* server);
+/* queue a request (WT_EINVAL when it can never fit the budget); rid numbers
+ * requests 0, 1, ... in submission order */
+int wt_serve_submit(wt_server* server, const wt_serve_request* req, int* rid);
+/* one scheduling round; *finished = requests that finished in it.  With nothing
+ * running and nothing arrived it sleeps until the next arrival (at most 10 ms). */
+int wt_serve_poll(wt_server* server, int* finished);
+/* rounds until every submitted request has finished; WT_ENONFINITE if a state
+ * became non-finite */
+int wt_serve_run(wt_server* server);
+/* WT_EINVAL until request rid has finished */
+int wt_serve_get_result(const wt_server* server, int rid, wt_serve_result* out);
+/* copy a finished request's kept final state into device buffers of its
+ * precision (nodes values each), on the context stream */
+int wt_serve_result_state(wt_server* server, int rid, void* Phi, void* Pi);
+int wt_serve_info(const wt_server* server, int* waiting, int* active, int* done, double* used_bytes,
+                  double* peak_bytes);
+/* the estimated device bytes and precision of a request under desc (host only) */
+int wt_serve_cost(const wt_serve_desc* desc, const wt_serve_request* req, double* bytes, int* precision);
+/* The admission order of step 2 as a permutation of count waiting requests
+ * (host only, no device): arrival times, estimated service seconds and work
+ * (nodes x steps) per request, listed in submission order. */
+int wt_serve_queue_order(int order, double now, int count, const double* arrival, const double* service,
+                         const double* work, int* perm);
+
 #ifdef __cplusplus
 }
 #endif

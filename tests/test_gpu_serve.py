@@ -69,3 +69,49 @@ def test_server_admission_respects_budget(wt, ctx):
     assert all(spans[i][1] <= spans[i + 1][0] + 1e-9 for i in range(len(spans) - 1))
     with pytest.raises(ValueError):
         S.Server(ctx, hbm_budget=1e3).run(reqs[:1])
+
+
+def test_engine_incremental_submission(wt, ctx):
+    """The native engine used directly: two requests start, two more are submitted
+    while they run (between polls) and join the same batch; every result equals
+    the request stepped alone (FP64, <= 1e-12); the error paths leave it usable."""
+    import dataclasses
+    import torch
+    S = wt.serve
+    reqs = requests(wt)[:4]
+    eng = wt.ServeEngine(ctx, wt.serve_desc(hbm_budget=4e9, tick=4, precision=wt.WT_F64, keep_results=True,
+                                            fill_nodes=None))
+    rids = [eng.submit(S.native_request(dataclasses.replace(q, arrival=0.0))) for q in reqs[:2]]
+    with pytest.raises(wt.WaveToyError):          # not finished yet
+        eng.result(rids[0])
+    assert eng.poll() == 0 and eng.info()["active"] == 2
+    eng.poll()
+    rids += [eng.submit(S.native_request(dataclasses.replace(q, arrival=0.0))) for q in reqs[2:]]
+    with pytest.raises(wt.WaveToyError):          # over the budget
+        big = dataclasses.replace(reqs[0], elements=40)
+        eng.submit(S.native_request(big, with_speed=False))
+    with pytest.raises(wt.WaveToyError):          # time-dependent backgrounds are not served
+        eng.submit(wt.serve_request(0.0, 6, 2, bg_kind=wt.BG_SINE_SHIFT, bg_params=(0.1, 1.0, 0.0), steps=2))
+    eng.run()
+    info = eng.info()
+    assert info["done"] == 4 and info["active"] == 0 and info["waiting"] == 0 and info["used_bytes"] == 0
+    res = [eng.result(r) for r in rids]
+    assert min(r["admitted"] for r in res[2:]) > max(r["admitted"] for r in res[:2])
+    assert any(b["admitted"] < a["finished"] for a in res[:2] for b in res[2:])   # joined running work
+    for q, rid, r in zip(reqs, rids, res):
+        assert r["precision"] == wt.WT_F64 and r["steps"] == q.steps and r["nodes"] == q.nodes
+        Phi_s, Pi_s = eng.state(rid)
+        mesh, coef, ws, Phi, Pi, dt = S.build_solve(ctx, q, wt.WT_F64, release=False)
+        assert dt == r["dt"]
+        wt.step_rk4_curved(Phi, Pi, coef, ws, dt, q.steps, bc3d=wt.make_bc3d([wt.BC_SOMMERFELD] * 6), metric=True)
+        a = torch.cat([Phi_s, Pi_s]).cpu().numpy()
+        b = torch.cat([Phi, Pi]).cpu().numpy()
+        assert rel(a, b) <= 1e-12, q.rid
+    eng.close()
+    eng2 = wt.ServeEngine(ctx, wt.serve_desc(tick=8))
+    rid = eng2.submit(S.native_request(dataclasses.replace(reqs[1], arrival=0.0)))
+    eng2.run()
+    with pytest.raises(wt.WaveToyError):          # no kept state without keep_results
+        eng2.state(rid)
+    eng2.close()
+    assert not ctx.nonfinite()

@@ -1,0 +1,83 @@
+"""Host logic of the native request server (wt_serve_*), on the CPU: the
+admission order of waiting requests (highest response ratio next, least work
+first, arrival order; ties by arrival, then submission) against a restatement
+of the three policies, and the per-request device-byte estimate and precision
+choice.  No device is touched."""
+import random
+
+import pytest
+
+from conftest import load_package
+
+
+def restated_order(order, now, arrival, service, work):
+    idx = list(range(len(arrival)))
+    if order == 0:
+        key = lambda k: (-(now - arrival[k] + service[k]) / service[k], arrival[k])
+    elif order == 1:
+        key = lambda k: (work[k], arrival[k])
+    else:
+        key = lambda k: arrival[k]
+    return sorted(idx, key=key)  # stable: ties keep submission order
+
+
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_queue_order_matches_policy(order):
+    wt = load_package()
+    rng = random.Random(7 + order)
+    for trial in range(200):
+        n = rng.randint(0, 12)
+        # coarse values so that ties in every key occur
+        arrival = [rng.choice([0.0, 0.25, 0.5, 1.0]) for _ in range(n)]
+        service = [rng.choice([0.1, 0.5, 2.0]) for _ in range(n)]
+        work = [float(rng.choice([1, 4, 9])) for _ in range(n)]
+        now = 1.5
+        assert wt.serve_queue_order(order, now, arrival, service, work) == \
+            restated_order(order, now, arrival, service, work), (trial, arrival, service, work)
+
+
+def test_hrrn_favours_short_then_ages_long():
+    wt = load_package()
+    # both waiting since t = 0: the short request's ratio (wait + S) / S grows faster
+    service, work = [20.0, 0.5], [1e12, 1e9]
+    assert wt.serve_queue_order(wt.SERVE_HRRN, 1.0, [0.0, 0.0], service, work) == [1, 0]
+    # a long request waiting since t = 0 against a short one waiting 0.1 s: the long
+    # one's ratio (6 + 20) / 20 = 1.3 beats (0.1 + 0.5) / 0.5 = 1.2, so it is not starved
+    assert wt.serve_queue_order(wt.SERVE_HRRN, 6.0, [0.0, 5.9], service, work) == [0, 1]
+    assert wt.serve_queue_order(wt.SERVE_HRRN, 3.0, [0.0, 2.9], service, work) == [1, 0]
+    arrival = [0.0, 2.9]
+    assert wt.serve_queue_order(wt.SERVE_SJF, 10.0, arrival, service, work) == [1, 0]
+    assert wt.serve_queue_order(wt.SERVE_FIFO, 10.0, arrival, service, work) == [0, 1]
+    with pytest.raises(wt.WaveToyError):
+        wt.serve_queue_order(3, 0.0, [0.0], [1.0], [1.0])
+    with pytest.raises(wt.WaveToyError):
+        wt.serve_queue_order(wt.SERVE_HRRN, 0.0, [0.0], [0.0], [1.0])
+
+
+@pytest.mark.parametrize("prec,n,steps,bpn,want_prec", [
+    (0, 8, 100, 520, 0), (0, 6, 100, 480, 0), (1, 8, 100, 300, 1), (1, 6, 900, 260, 1),
+    (-1, 8, 250, 300, 1), (-1, 8, 251, 520, 0), (-1, 6, 2000, 480, 0)])
+def test_cost_and_precision(prec, n, steps, bpn, want_prec):
+    wt = load_package()
+    d = wt.serve_desc(precision=prec, auto_fp32_max_steps=250)
+    q = wt.serve_request(0.0, n, (3, 4, 5), warp_A=0.05, outer_tag=7, bg_kind=wt.BG_ADM_PERTURBED,
+                         ic_params=wt.gaussian_params([(0.5, 0.5, 0.5)], [1.0], [0.1]), steps=steps,
+                         bc3d=wt.make_bc3d([wt.BC_SOMMERFELD] * 6))
+    nodes = 3 * 4 * 5 * n ** 3
+    assert wt.serve_cost(d, q) == (float(nodes * (bpn + 272)), want_prec)
+
+
+def test_request_validation():
+    wt = load_package()
+    d = wt.serve_desc()
+    good = dict(arrival=0.0, N=6, M=2, steps=10)
+    wt.serve_cost(d, wt.serve_request(**good))
+    for bad in (dict(steps=0), dict(N=9), dict(M=0), dict(arrival=float("nan"))):
+        with pytest.raises(wt.WaveToyError):
+            wt.serve_cost(d, wt.serve_request(**{**good, **bad}))
+    with pytest.raises(wt.WaveToyError):   # time-dependent backgrounds are not served
+        wt.serve_cost(d, wt.serve_request(**good, bg_kind=wt.BG_GAUGE_WAVE, bg_params=(0.1, 1.0, 0.0)))
+    with pytest.raises(wt.WaveToyError):
+        wt.serve_cost(wt.serve_desc(tick=0), wt.serve_request(**good))
+    with pytest.raises(ValueError):
+        wt.serve_request(**good, ic_params=[0.0] * 200)

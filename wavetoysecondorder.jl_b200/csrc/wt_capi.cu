@@ -422,6 +422,11 @@ int rhs_curved_impl(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi
 
 }  // namespace
 
+namespace wt {
+// error reporting on a context for the other host translation units (the server)
+int ctx_fail(wt_ctx* ctx, int code, const std::string& msg) { return fail(ctx, code, msg); }
+}  // namespace wt
+
 extern "C" {
 
 int wt_ctx_create(int device, wt_ctx** out) {

@@ -21,6 +21,8 @@
 
 #define WT_MAXN 8
 
+struct wt_ctx;  // the public context (include/wavetoy_b200.h)
+
 namespace wt {
 
 // ---- host-side GLL operators (product code, independent of the oracle) -----
@@ -138,6 +140,9 @@ __host__ __device__ inline int nbr_face_node(int fs, int p, int q, int N) {
   face_perm((fs >> 3) & 7, p, q, N, pn, qn);
   return face_node(faxis(fn), frow(fn, N), pn, qn, N);
 }
+
+// set the context's last-error message and return code (wt_capi.cu)
+int ctx_fail(::wt_ctx* ctx, int code, const std::string& msg);
 
 // ---- meshes built from node coordinates (wt_patches.cu, host) ----------------------
 // D4 orientation under which face (e,f)'s nodes coincide with face (en,fn)'s

@@ -4,6 +4,8 @@ solves advance together through one batch (wt_batch_*: the work-list kernels
 over (solve, element) tiles and a CUDA graph per RK4 step), so requests that
 arrive while others run join the work already on the GPU.  No counterpart in
 the reference, whose evolve3d (src/evolve.jl:1149-1358) runs one solve per call.
+The scheduling itself is native (wt_serve_*, wavetoy.ServeEngine); this module
+describes requests, builds single solves for comparison and summarises runs.
 
 A request is one warped-cube ADM solve (mesh size, order, background and
 initial-data seeds, step count at CFL 0.2).  Latency = finish - arrival, where
@@ -11,8 +13,6 @@ finish is when its last step has completed on the device.
 """
 from __future__ import annotations
 
-import time
-from collections import deque
 from dataclasses import dataclass
 from typing import List, Optional
 
@@ -83,15 +83,6 @@ def build_solve(ctx, req: Request, precision: int, fp32_form: int = wt.FP32_CUDA
     return mesh, coef, ws, Phi, Pi, dt
 
 
-def bytes_per_node(precision: int, n: int) -> int:
-    """Device bytes one node of a served solve holds while it runs (set-up
-    geometry released): coefficients, streamed metric, workspace and state;
-    a little above the sum of the arrays, for the allocator's rounding."""
-    if precision == wt.WT_F64:
-        return 520 if n == 8 else 480
-    return 300 if n == 8 else 260
-
-
 # Precision policy of the "auto" form.  FP32 state with FP32-rounded
 # coefficients perturbs the discrete operator by ~6e-8 relative, which shows
 # up as a phase error that grows about linearly with the step count: measured
@@ -100,7 +91,8 @@ def bytes_per_node(precision: int, n: int) -> int:
 # forms.  Requests whose step count keeps the FP32 error under 1e-5 run in
 # FP32, the others in FP64.
 AUTO_FP32_MAX_STEPS = 250
-AUTO = -1
+AUTO = wt.SERVE_AUTO
+ORDERS = {"hrrn": wt.SERVE_HRRN, "sjf": wt.SERVE_SJF, "fifo": wt.SERVE_FIFO}
 
 
 def request_precision(precision: int, req: Request) -> int:
@@ -109,10 +101,26 @@ def request_precision(precision: int, req: Request) -> int:
     return wt.WT_F32 if req.steps <= AUTO_FP32_MAX_STEPS else wt.WT_F64
 
 
+def native_request(req: Request, with_speed: bool = True):
+    """The wt_serve_request of a request: the warped cube of build_solve with its
+    seeded ADM background and Gaussian pulses, CFL 0.2 (the speed bound sampled on
+    24^3 points; with_speed=False leaves it 1, enough for the cost estimate)."""
+    p = W.adm_params(req.seed, req.scale)
+    c, a, w = W.pulses(req.seed, req.pulses, amp=(0.5, 1.0), width=(0.05, 0.15), centre=(0.25, 0.75))
+    return wt.serve_request(req.arrival, req.n, req.elements, 0.0, 1.0, 0.05, outer_tag=wt.SOMMERFELD_BDRY_TAG,
+                            bg_kind=wt.BG_ADM_PERTURBED, bg_params=p, ic_kind=wt.IC_GAUSSIANS,
+                            ic_params=wt.gaussian_params(c, a, w), cfl=0.2,
+                            max_speed=W.max_speed(p, 24) if with_speed else 1.0, steps=req.steps,
+                            bc3d=wt.make_bc3d([wt.BC_SOMMERFELD] * 6))
+
+
 class Server:
-    """Continuous-batching server over one context (one GPU).  precision:
-    wt.WT_F32, wt.WT_F64 or AUTO (per request, see request_precision); FP32 and
-    FP64 requests share the batch (they run as separate groups)."""
+    """Continuous-batching server over one context (one GPU): the Python face of
+    the native engine (wt_serve_*, wavetoy.ServeEngine), which does the
+    admission, the device set-up of each admitted request and the batched
+    stepping.  precision: wt.WT_F32, wt.WT_F64 or AUTO (per request, see
+    request_precision); FP32 and FP64 requests share the batch (they run as
+    separate groups)."""
 
     def __init__(self, ctx, precision: int = wt.WT_F32, hbm_budget: float = 150e9, tick: int = 50,
                  max_active: Optional[int] = None, fp32_form: int = wt.FP32_CUDA_CORES, keep_results: bool = False,
@@ -127,7 +135,7 @@ class Server:
         ahead under a backlog, and a long one's priority grows while it waits),
         "sjf" (least work first; long requests can wait until the backlog
         clears) or "fifo" (arrival order)."""
-        if order not in ("hrrn", "sjf", "fifo"):
+        if order not in ORDERS:
             raise ValueError("order must be 'hrrn', 'sjf' or 'fifo'")
         self.order = order
         self.ctx = ctx
@@ -138,73 +146,36 @@ class Server:
         self.max_active = max_active
         self.fp32_form = fp32_form
         self.keep = keep_results
+        self.peak_used = 0.0
 
-    def _service_s(self, req: Request) -> float:
-        # rough service time at the measured single-GPU rates (FP64 ~3e9, FP32 ~6e9 DOF-updates/s)
-        rate = 3e9 if request_precision(self.precision, req) == wt.WT_F64 else 6e9
-        return 2.0 * req.nodes * req.steps / rate + 0.05
+    def desc(self):
+        return wt.serve_desc(self.budget, self.tick, self.max_active, self.fill_nodes, ORDERS[self.order],
+                             self.precision, self.fp32_form, AUTO_FP32_MAX_STEPS, self.keep)
 
     def _cost(self, req: Request) -> float:
-        # running footprint plus the FP64 set-up geometry held while it is built
-        return req.nodes * (bytes_per_node(request_precision(self.precision, req), req.n) + 272)
+        """Estimated device bytes of a request (the engine's own estimate)."""
+        return wt.serve_cost(self.desc(), native_request(req, with_speed=False))[0]
 
     def run(self, requests: List[Request]) -> List[Result]:
         import torch
-        batch = wt.Batch(self.ctx)
-        pending = deque(sorted(requests, key=lambda r: r.arrival))
-        for r in pending:
+        for r in requests:
             if self._cost(r) > self.budget:
                 raise ValueError(f"request {r.rid} ({r.nodes} nodes) does not fit the HBM budget")
-        queue: deque = deque()
-        active = {}
-        used = 0.0
-        self.peak_used = 0.0
-        results: List[Result] = []
-        t0 = time.perf_counter()
-        while pending or queue or active:
-            now = time.perf_counter() - t0
-            while pending and pending[0].arrival <= now:
-                queue.append(pending.popleft())
-            if self.order == "sjf":
-                queue = deque(sorted(queue, key=lambda r: (r.nodes * r.steps, r.arrival)))
-            elif self.order == "hrrn":
-                queue = deque(sorted(queue, key=lambda r: (-(now - r.arrival + self._service_s(r)) / self._service_s(r),
-                                                           r.arrival)))
-            # admit in queue order while the budget (and the slot limit) allows
-            while queue and used + self._cost(queue[0]) <= self.budget and \
-                    (self.max_active is None or len(active) < self.max_active) and \
-                    (self.fill_nodes is None or not active or
-                     sum(a["req"].nodes for a in active.values()) < self.fill_nodes):
-                req = queue.popleft()
-                used += self._cost(req)
-                self.peak_used = max(self.peak_used, used)
-                mesh, coef, ws, Phi, Pi, dt = build_solve(self.ctx, req, request_precision(self.precision, req),
-                                                          self.fp32_form)
-                slot = batch.add(Phi, Pi, coef, ws, dt, wt.make_bc3d([wt.BC_SOMMERFELD] * 6))
-                active[slot] = {"req": req, "objs": (mesh, coef, ws), "Phi": Phi, "Pi": Pi, "dt": dt,
-                                "left": req.steps, "admitted": time.perf_counter() - t0}
-            if not active:
-                if pending:
-                    time.sleep(max(0.0, min(0.01, pending[0].arrival - (time.perf_counter() - t0))))
-                continue
-            k = min(self.tick, min(a["left"] for a in active.values()))
-            batch.step(k)
+        native = [(r, native_request(r)) for r in sorted(requests, key=lambda r: r.arrival)]
+        eng = wt.ServeEngine(self.ctx, self.desc())   # its clock starts here
+        try:
+            rids = [(eng.submit(q), r) for r, q in native]
+            eng.run()
+            self.peak_used = eng.info()["peak_bytes"]
+            results = []
+            for rid, req in rids:
+                x = eng.result(rid)
+                Phi, Pi = eng.state(rid) if self.keep else (None, None)
+                results.append(Result(req.rid, req.arrival, x["admitted"], x["finished"], x["nodes"], x["steps"],
+                                      x["dt"], Phi, Pi))
             torch.cuda.synchronize(self.ctx.device)
-            t_done = time.perf_counter() - t0
-            for slot in [s for s, a in active.items() if a["left"] - k <= 0]:
-                a = active.pop(slot)
-                batch.remove(slot)
-                req = a["req"]
-                results.append(Result(req.rid, req.arrival, a["admitted"], t_done, req.nodes, req.steps, a["dt"],
-                                      a["Phi"] if self.keep else None, a["Pi"] if self.keep else None))
-                for o in reversed(a["objs"]):
-                    o.close()
-                used -= self._cost(req)
-            for a in active.values():
-                a["left"] -= k
-        batch.close()
-        if self.ctx.nonfinite():
-            raise wt.WaveToyError(-5, "a served solve became non-finite")
+        finally:
+            eng.close()
         return sorted(results, key=lambda r: r.rid)
 
 

@@ -72,6 +72,28 @@ class _BcDesc(C.Structure):
                 ("gDz", C.c_void_p)]
 
 
+SERVE_HRRN, SERVE_SJF, SERVE_FIFO = 0, 1, 2
+SERVE_AUTO = -1
+SERVE_MAX_IC = 128
+
+
+class _ServeDesc(C.Structure):
+    _fields_ = [("hbm_budget", C.c_double), ("tick", C.c_int), ("max_active", C.c_int), ("fill_nodes", C.c_longlong),
+                ("order", C.c_int), ("precision", C.c_int), ("fp32_form", C.c_int), ("auto_fp32_max_steps", C.c_int),
+                ("keep_results", C.c_int), ("rate_f64", C.c_double), ("rate_f32", C.c_double)]
+
+
+class _ServeRequest(C.Structure):
+    _fields_ = [("arrival", C.c_double), ("mesh", _MeshDesc), ("bg", _BgDesc), ("ic_kind", C.c_int), ("nic", C.c_int),
+                ("ic", C.c_double * SERVE_MAX_IC), ("cfl", C.c_double), ("max_speed", C.c_double), ("steps", C.c_int),
+                ("bc", _BcDesc)]
+
+
+class _ServeResult(C.Structure):
+    _fields_ = [("precision", C.c_int), ("nodes", C.c_longlong), ("steps", C.c_int), ("dt", C.c_double),
+                ("arrival", C.c_double), ("admitted", C.c_double), ("finished", C.c_double)]
+
+
 _lib = None
 
 
@@ -130,6 +152,13 @@ def library():
         "wt_initial_data": [vp, vp, i, vp, i, d, vp, vp],
         "wt_gll_operators": [i, vp, vp, vp],
         "wt_ctx_profile": [vp, i], "wt_ctx_profile_read": [vp, C.POINTER(d * 2), C.POINTER(ll * 2)],
+        "wt_serve_create": [vp, C.POINTER(_ServeDesc), pvp], "wt_serve_destroy": [vp],
+        "wt_serve_submit": [vp, C.POINTER(_ServeRequest), C.POINTER(i)], "wt_serve_poll": [vp, C.POINTER(i)],
+        "wt_serve_run": [vp], "wt_serve_get_result": [vp, i, C.POINTER(_ServeResult)],
+        "wt_serve_result_state": [vp, i, vp, vp],
+        "wt_serve_info": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(d), C.POINTER(d)],
+        "wt_serve_cost": [C.POINTER(_ServeDesc), C.POINTER(_ServeRequest), C.POINTER(d), C.POINTER(i)],
+        "wt_serve_queue_order": [i, d, i, vp, vp, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -219,7 +248,7 @@ class Context:
         workspaces and coefficients, then meshes)."""
         if getattr(self, "h", None):
             alive = [r() for r in getattr(self, "_children", [])]
-            for kind in (Batch, Workspace, Coef, Mesh):
+            for kind in (ServeEngine, Batch, Workspace, Coef, Mesh):
                 for o in alive:
                     if isinstance(o, kind):
                         o.close()
@@ -514,6 +543,139 @@ class Batch(_Child):
     def close(self):
         if getattr(self, "h", None) and self._ctx_alive():
             library().wt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve_desc(hbm_budget: float = 150e9, tick: int = 50, max_active: Optional[int] = None,
+               fill_nodes: Optional[int] = 8_000_000, order: int = SERVE_HRRN, precision: int = WT_F32,
+               fp32_form: int = FP32_CUDA_CORES, auto_fp32_max_steps: int = 250, keep_results: bool = False,
+               rate_f64: float = 0.0, rate_f32: float = 0.0) -> _ServeDesc:
+    """wt_serve_desc: admission and stepping policy of a ServeEngine (None: no limit)."""
+    d = _ServeDesc()
+    d.hbm_budget = float(hbm_budget)
+    d.tick = int(tick)
+    d.max_active = 0 if max_active is None else int(max_active)
+    d.fill_nodes = 0 if fill_nodes is None else int(fill_nodes)
+    d.order, d.precision, d.fp32_form = int(order), int(precision), int(fp32_form)
+    d.auto_fp32_max_steps = int(auto_fp32_max_steps)
+    d.keep_results = int(bool(keep_results))
+    d.rate_f64, d.rate_f32 = float(rate_f64), float(rate_f32)
+    return d
+
+
+def serve_request(arrival: float, N: int, M, x0: float = 0.0, x1: float = 1.0, warp_A: float = 0.0,
+                  outer_tag: int = 0, bg_kind: int = BG_MINKOWSKI, bg_params: Sequence[float] = (),
+                  ic_kind: int = IC_GAUSSIANS, ic_params: Sequence[float] = (), cfl: float = 0.2,
+                  max_speed: float = 1.0, steps: int = 1, bc3d: Optional["BC3D"] = None) -> _ServeRequest:
+    """wt_serve_request: one solve (analytic mesh, static background, initial data
+    of Phi with Pi = 0, dt = cfl * min spacing / max_speed, RK4 steps)."""
+    q = _ServeRequest()
+    q.arrival = float(arrival)
+    M = (M, M, M) if isinstance(M, int) else tuple(M)
+    q.mesh.N = int(N)
+    for a in range(3):
+        q.mesh.M[a] = int(M[a])
+    q.mesh.x0, q.mesh.x1, q.mesh.warp_A = float(x0), float(x1), float(warp_A)
+    q.mesh.periodic, q.mesh.outer_tag = 0, int(outer_tag)
+    q.bg.kind = int(bg_kind)
+    if len(bg_params) > len(q.bg.p) or len(ic_params) > SERVE_MAX_IC:
+        raise ValueError("too many background or initial-data parameters")
+    for k, v in enumerate(bg_params):
+        q.bg.p[k] = float(v)
+    q.ic_kind, q.nic = int(ic_kind), len(ic_params)
+    for k, v in enumerate(ic_params):
+        q.ic[k] = float(v)
+    q.cfl, q.max_speed, q.steps = float(cfl), float(max_speed), int(steps)
+    if bc3d is not None:
+        if any(g is not None for g in (bc3d.gPhi, bc3d.gPi, bc3d.gDx, bc3d.gDy, bc3d.gDz)):
+            raise ValueError("served requests take no boundary data fields")
+        q.bc = bc3d.cstruct()
+    return q
+
+
+def serve_cost(desc: _ServeDesc, req: _ServeRequest):
+    """(estimated device bytes, precision) of a request under a policy (wt_serve_cost; host only)."""
+    b, p = C.c_double(), C.c_int()
+    rc = library().wt_serve_cost(C.byref(desc), C.byref(req), C.byref(b), C.byref(p))
+    if rc != 0:
+        raise WaveToyError(rc, "wt_serve_cost: bad descriptor or request")
+    return b.value, p.value
+
+
+def serve_queue_order(order: int, now: float, arrival, service, work):
+    """Admission order of waiting requests (wt_serve_queue_order; host only, no device)."""
+    import numpy as np
+    a = np.ascontiguousarray(arrival, dtype=np.float64)
+    s = np.ascontiguousarray(service, dtype=np.float64)
+    w = np.ascontiguousarray(work, dtype=np.float64)
+    n = a.size
+    if s.size != n or w.size != n:
+        raise ValueError("arrival, service and work must have the same length")
+    perm = np.zeros(n, dtype=np.int32)
+    rc = library().wt_serve_queue_order(int(order), float(now), int(n), a.ctypes.data, s.ctypes.data, w.ctypes.data,
+                                        perm.ctypes.data)
+    if rc != 0:
+        raise WaveToyError(rc, "wt_serve_queue_order: bad arguments")
+    return perm.tolist()
+
+
+class ServeEngine(_Child):
+    """The native request server (wt_serve_*; no counterpart in the reference):
+    requests arrive on the engine's clock (seconds since it was made), are
+    admitted by the descriptor's order within the HBM budget, built on the
+    device at admission and advanced together through one batch."""
+
+    def __init__(self, ctx: Context, desc: _ServeDesc):
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        self.desc = desc
+        ctx.check(library().wt_serve_create(ctx.h, C.byref(desc), C.byref(self.h)), "wt_serve_create")
+        ctx._adopt(self)
+
+    def submit(self, req: _ServeRequest) -> int:
+        rid = C.c_int()
+        self.ctx.check(library().wt_serve_submit(self.h, C.byref(req), C.byref(rid)), "wt_serve_submit")
+        return rid.value
+
+    def poll(self) -> int:
+        n = C.c_int()
+        self.ctx.check(library().wt_serve_poll(self.h, C.byref(n)), "wt_serve_poll")
+        return n.value
+
+    def run(self):
+        self.ctx.check(library().wt_serve_run(self.h), "wt_serve_run")
+
+    def result(self, rid: int) -> dict:
+        r = _ServeResult()
+        self.ctx.check(library().wt_serve_get_result(self.h, int(rid), C.byref(r)), "wt_serve_get_result")
+        return {k: getattr(r, k) for k, _ in _ServeResult._fields_}
+
+    def state(self, rid: int):
+        """(Phi, Pi) device tensors holding a finished request's kept final state."""
+        torch = _torch()
+        r = self.result(rid)
+        dt_ = torch.float64 if r["precision"] == WT_F64 else torch.float32
+        Phi = torch.empty(r["nodes"], dtype=dt_, device=f"cuda:{self.ctx.device}")
+        Pi = torch.empty_like(Phi)
+        self.ctx.check(library().wt_serve_result_state(self.h, int(rid), _ptr(Phi), _ptr(Pi)), "wt_serve_result_state")
+        return Phi, Pi
+
+    def info(self) -> dict:
+        w, a, dn, u, pk = C.c_int(), C.c_int(), C.c_int(), C.c_double(), C.c_double()
+        self.ctx.check(library().wt_serve_info(self.h, C.byref(w), C.byref(a), C.byref(dn), C.byref(u), C.byref(pk)),
+                       "wt_serve_info")
+        return {"waiting": w.value, "active": a.value, "done": dn.value, "used_bytes": u.value,
+                "peak_bytes": pk.value}
+
+    def close(self):
+        if getattr(self, "h", None) and self._ctx_alive():
+            library().wt_serve_destroy(self.h)
             self.h = None
 
     def __del__(self):
