@@ -149,6 +149,17 @@ typedef struct {
   int precision;  /* WT_F64 or WT_F32 */
 } wt_patch_desc;
 int wt_mesh_create_patches(wt_ctx* ctx, const wt_patch_desc* desc, wt_mesh** out);
+/* One z-slab of the analytic cube of desc, for a solve partitioned over GPUs
+ * (no counterpart in the reference, which runs one device per solve): the nz
+ * element layers z0 .. z0 + nz - 1 of the whole mesh (taken modulo M[2] when
+ * desc->periodic; there -M[2] <= z0 < M[2]), with the geometry, metric terms
+ * and face tags those elements have in the whole mesh.  A z face whose
+ * neighbour layer lies outside the slab gets no neighbour and no tag (a cut):
+ * a partition gives each slab one ghost layer beyond each cut and refreshes it
+ * with wt_halo_copy after the first part of every RK4 stage
+ * (wt_rk4_stage_curved), so that the slab's own layers advance exactly as in
+ * the whole mesh.  Elements are numbered as in wt_mesh_create with M[2] = nz. */
+int wt_mesh_create_slab(wt_ctx* ctx, const wt_mesh_desc* desc, int z0, int nz, wt_mesh** out);
 /* The same mesh as host arrays (host only, no device work): *Ne, and when
  * coords != NULL also coords (3,N,N,N,Ne), jac (9 per node, may be NULL),
  * neighbour / neighbour_face (6,Ne, 1-based, 0 = none), orientation (6,Ne, the
@@ -339,6 +350,24 @@ int wt_l2_diff(wt_ctx* ctx, wt_ws* ws, const void* a, const void* b, int use_met
  * (checked at the end; the reference asserts isfinite per sample). */
 int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
                        double eps_ko, const wt_bc_desc* bc, int use_metric);
+/* One half of RK4 stage `stage` (0..3) of wt_step_rk4_curved (eps_ko = 0),
+ * for callers that exchange halos between the halves (a z-slab partition):
+ * part 1 evaluates the gradient, the flux and the boundary terms and updates
+ * Phi's stage; part 2 the divergence and Pi's stage.  Calling parts 1, 2 of
+ * stages 0..3 in order is one wt_step_rk4_curved step, with the same kernels
+ * and results.  Time-dependent backgrounds are re-sampled at part 1 and their
+ * time advanced after stage 3. */
+int wt_rk4_stage_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int stage,
+                        int part, const wt_bc_desc* bc, int use_metric);
+/* Halo of a z-slab after part 1 of stage `stage`: the fields other elements read
+ * across a face before part 2 and the next stage -- the Phi that the next
+ * stage reads (the caller's Phi after stage 3) and the three flux components --
+ * restricted to element layer `layer` (M[0] M[1] consecutive elements), copied
+ * into buf (pack = 1) or from buf back into the fields (pack = 0), in the
+ * mesh's precision, asynchronously on the context stream.  buf holds
+ * wt_halo_size values (known once a first stage part has run on ws). */
+int wt_halo_size(const wt_ws* ws, long long* values);
+int wt_halo_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, void* buf, int pack);
 /* Fixed-step explicit Runge-Kutta methods of pick_integrator_first_order
  * (src/evolve.jl:43-48; evolve3d runs them with adaptive = false):
  * WT_ERK_RK4 (the fused low-storage RK4 above) and WT_ERK_TSIT5 (Tsitouras

@@ -1,0 +1,102 @@
+"""GPU: one solve split into z-slabs (wt_mesh_create_slab, wt_rk4_stage_curved,
+wt_halo_copy; slabs.py) advances its owned element layers exactly as the
+undivided mesh does -- bit for bit, since every element's arithmetic depends
+only on its own data and its neighbours' face traces, which the halo exchange
+supplies -- through the n = 8 FP64 tensor-core kernels, the generic kernels, the
+FP32 CUDA-core form, a periodic ring of slabs and a time-dependent background
+re-sampled at every stage.  The slabs share one device here (in-process
+exchange); between GPUs the same messages go through torch.distributed."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [  # N, M, slabs, periodic, precision, fp32 form, background
+    (8, (3, 2, 6), 2, False, 0, None, 2),
+    (8, (2, 3, 7), 3, True, 0, None, 2),
+    (5, (3, 3, 5), 2, False, 0, None, 2),
+    (8, (2, 2, 6), 3, False, 1, 0, 2),
+    (6, (2, 2, 6), 2, True, 0, None, 4),
+]
+
+
+@pytest.mark.parametrize("N,M,nslabs,periodic,prec,form,bg", CASES)
+def test_slab_solve_equals_whole_mesh(wt, ctx, N, M, nslabs, periodic, prec, form, bg):
+    import torch
+    S = wt.slabs
+    kw = dict(warp_A=0.05, periodic=periodic, outer_tag=0 if periodic else 7, precision=prec)
+    prm = wt.workloads.adm_params(5) if bg == 2 else (0.1, 1.0, 0.05)
+    speed = wt.workloads.max_speed(prm) if bg == 2 else 1.0
+    ic = wt.gaussian_params(*wt.workloads.pulses(5, 2))
+    bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+    whole = wt.Mesh.uniform_hex(ctx, N, M, **kw)
+    if form is not None:
+        whole.set_fp32_form(form)
+    coef = wt.sample_background3d(whole, bg, prm)
+    ws = wt.make_wave3d_workspace(whole)
+    P, Q = whole.zeros(), whole.zeros()
+    wt.initial_data(whole, wt.IC_GAUSSIANS, ic, P)
+    dt = 0.2 * whole.min_spacing() / speed
+    nsteps = 5
+    wt.step_rk4_curved(P, Q, coef, ws, dt, nsteps, bc3d=bc, metric=True)
+
+    slabs = [S.Slab(ctx, r, N, M, **kw, bg_kind=bg, bg_params=prm, fp32_form=form)
+             for r in S.partition(M[2], nslabs, periodic)]
+    for s in slabs:
+        wt.initial_data(s.mesh, wt.IC_GAUSSIANS, ic, s.Phi)
+    assert min(s.mesh.min_spacing() for s in slabs) == whole.min_spacing()
+    S.step(slabs, S.LocalHalo(slabs), dt, nsteps, bc)
+    Ps = torch.cat([s.owned(s.Phi) for s in slabs])
+    Qs = torch.cat([s.owned(s.Pi) for s in slabs])
+    assert torch.isfinite(Ps).all() and float(P.abs().max()) > 0
+    assert torch.equal(Ps, P) and torch.equal(Qs, Q), (float((Ps - P).abs().max()), float((Qs - Q).abs().max()))
+    if bg == 4:
+        assert all(abs(s.coef.time - coef.time) < 1e-15 for s in slabs)
+    for s in slabs:
+        s.close()
+    assert not ctx.nonfinite()
+
+
+def test_stage_halves_equal_fused_step(wt, ctx):
+    """Parts 1 and 2 of stages 0..3 called one by one are one wt_step_rk4_curved step."""
+    import torch
+    g = wt.Mesh.uniform_hex(ctx, 8, (2, 2, 3), warp_A=0.05, outer_tag=7)
+    prm = wt.workloads.adm_params(2)
+    c = wt.sample_background3d(g, wt.BG_ADM_PERTURBED, prm)
+    ws1, ws2 = wt.make_wave3d_workspace(g), wt.make_wave3d_workspace(g)
+    P1 = g.zeros()
+    wt.initial_data(g, wt.IC_GAUSSIANS, wt.gaussian_params(*wt.workloads.pulses(2, 2)), P1)
+    Q1 = 0.3 * P1
+    P2, Q2 = P1.clone(), Q1.clone()
+    bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+    dt = 1e-3
+    wt.step_rk4_curved(P1, Q1, c, ws1, dt, 2, bc3d=bc, metric=True)
+    for _ in range(2):
+        for st in range(4):
+            for part in (1, 2):
+                wt.rk4_stage_curved(P2, Q2, c, ws2, dt, st, part, bc3d=bc, metric=True)
+    assert torch.equal(P1, P2) and torch.equal(Q1, Q2)
+
+
+def test_slab_errors(wt, ctx):
+    with pytest.raises(wt.WaveToyError):          # layers outside a non-periodic mesh
+        wt.Mesh.slab(ctx, 6, 3, 2, 2)
+    with pytest.raises(wt.WaveToyError):
+        wt.Mesh.slab(ctx, 6, 3, 0, 4, periodic=True)
+    g = wt.Mesh.slab(ctx, 6, (2, 2, 5), -1, 3, periodic=True)
+    assert g.Ne == 12
+    ws = wt.make_wave3d_workspace(g)
+    with pytest.raises(wt.WaveToyError):          # nothing to size before a stage has run
+        wt.halo_size(ws)
+    c = wt.sample_background3d(g, wt.BG_MINKOWSKI)
+    P, Q = g.zeros(), g.zeros()
+    with pytest.raises(wt.WaveToyError):
+        wt.rk4_stage_curved(P, Q, c, ws, 1e-3, 4, 1, metric=True)
+    wt.rk4_stage_curved(P, Q, c, ws, 1e-3, 0, 1, metric=True)
+    n = wt.halo_size(ws)
+    assert n == 4 * 6 ** 3 * 4                    # Phi + three flux components of 4 elements
+    import torch
+    buf = torch.empty(n, dtype=torch.float64, device="cuda")
+    with pytest.raises(wt.WaveToyError):
+        wt.halo_copy(ws, P, 0, 3, buf, True)      # the slab has layers 0..2
+    wt.halo_copy(ws, P, 0, 2, buf, True)

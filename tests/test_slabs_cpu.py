@@ -1,0 +1,115 @@
+"""Host logic of the z-slab partition (slabs.py), on the CPU: the layer ranges,
+and the halo exchange -- every ghost layer receives the layer its neighbour owns
+there, also on a periodic ring of two slabs, where each slab is the other's
+upper and lower neighbour -- through a model of in-order point-to-point
+delivery and through real gloo ranks (world sizes 2 and 3)."""
+import os
+import socket
+import sys
+from collections import defaultdict, deque
+
+import pytest
+
+from conftest import load_package
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.parametrize("Mz,n,periodic", [(6, 1, False), (6, 2, False), (7, 3, False), (6, 2, True),
+                                            (7, 3, True), (9, 4, True), (5, 5, False)])
+def test_partition_covers_layers(Mz, n, periodic):
+    S = load_package().slabs
+    rs = S.partition(Mz, n, periodic)
+    owned = [z for r in rs for z in range(r.own0, r.own0 + r.nown)]
+    assert owned == list(range(Mz))
+    assert max(r.nown for r in rs) - min(r.nown for r in rs) <= 1
+    for r in rs:
+        assert r.nz <= Mz
+        if r.lower is not None:
+            lo = rs[r.lower]
+            assert (lo.own0 + lo.nown - 1) % Mz == r.z0 % Mz        # ghost below = neighbour's top layer
+        else:
+            assert r.own0 == 0 and not periodic or n == 1
+        if r.upper is not None:
+            up = rs[r.upper]
+            assert up.own0 == (r.z0 + r.nz - 1) % Mz                 # ghost above = neighbour's bottom layer
+    with pytest.raises(ValueError):
+        S.partition(3, 4)
+
+
+def _field(r, Mz, width=4):
+    # a slab's local layers: owned layers hold their whole-mesh layer number, ghosts -1
+    return [[float(r.own0 + k - r.ghost_lo) if r.ghost_lo <= k < r.ghost_lo + r.nown else -1.0] * width
+            for k in range(r.nz)]
+
+
+@pytest.mark.parametrize("Mz,n,periodic", [(6, 2, False), (6, 2, True), (7, 3, True), (8, 4, False)])
+def test_exchange_pairs_in_order(Mz, n, periodic):
+    """Every slab posts its messages; delivery is in order per (sender, receiver) pair,
+    as NCCL and gloo deliver point-to-point messages."""
+    S = load_package().slabs
+    rs = S.partition(Mz, n, periodic)
+    fields = [_field(r, Mz) for r in rs]
+    wires = defaultdict(deque)
+    posted = {}
+    for r in rs:   # phase 1: every slab posts its sends
+        def send_recv(sends, recvs, r=r):
+            for peer, buf in sends:
+                wires[(r.index, peer)].append(list(buf))
+            posted[r.index] = recvs
+        S.exchange(r, lambda layer, r=r: fields[r.index][layer], lambda layer, buf: None, send_recv, list)
+    for r in rs:   # phase 2: receives take messages in order
+        def send_recv(sends, recvs, r=r):
+            for peer, buf in recvs:
+                buf.extend(wires[(peer, r.index)].popleft())
+        def unpack(layer, buf, r=r):
+            fields[r.index][layer] = buf
+        S.exchange(r, lambda layer: None, unpack, send_recv, list)
+    assert all(len(q) == 0 for q in wires.values())
+    for r, f in zip(rs, fields):
+        want = [float((r.z0 + k) % Mz) for k in range(r.nz)]
+        assert [row[0] for row in f] == want
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, Mz, periodic, q):
+    import datetime
+    import importlib.util
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    from conftest import load_package as lp
+    S = lp().slabs
+    r = S.partition(Mz, world, periodic)[rank]
+    f = torch.tensor(_field(r, Mz, 5), dtype=torch.float64)
+    for _ in range(3):   # repeated exchanges stay paired
+        S.exchange(r, lambda layer: f[layer].clone(), lambda layer, buf: f[layer].copy_(buf),
+                   S.dist_send_recv(dist), lambda: torch.empty(5, dtype=torch.float64))
+    q.put((rank, f[:, 0].tolist(), [float((r.z0 + k) % Mz) for k in range(r.nz)]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,Mz,periodic", [(2, 6, False), (2, 6, True), (3, 7, True)])
+def test_exchange_over_gloo(world, Mz, periodic):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, Mz, periodic, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=180) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, got, want in out:
+        assert got == want, rank

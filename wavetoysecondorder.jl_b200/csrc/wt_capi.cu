@@ -86,6 +86,7 @@ struct wt_ws {
   void* compQ = nullptr;
   const void* comp_for[2] = {nullptr, nullptr};
   void* erk = nullptr;    // explicit RK stage slopes: 2 x 8 x nn (Phi slopes, then Pi slopes)
+  long long flux_block = 0;  // values per element block of F as the last fused stage wrote it (halo copies)
 };
 
 namespace {
@@ -553,22 +554,22 @@ int wt_gll_operators(int N, double* x, double* H, double* G) {
 }
 
 // ---- mesh -------------------------------------------------------------------
-int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* d, wt_mesh** out) {
-  if (!ctx) return WT_EINVAL;
-  if (!d || !out) return fail(ctx, WT_EINVAL, "wt_mesh_create: NULL argument");
-  *out = nullptr;
-  if (d->N < 2 || d->N > WT_MAXN) return fail(ctx, WT_EINVAL, "N must be in 2..8, got " + std::to_string(d->N));
-  if (d->M[0] < 1 || d->M[1] < 1 || d->M[2] < 1) return fail(ctx, WT_EINVAL, "element counts must be >= 1");
-  if (d->precision != WT_F64 && d->precision != WT_F32) return fail(ctx, WT_EINVAL, "precision must be WT_F64 or WT_F32");
-  if (!(d->x1 > d->x0)) return fail(ctx, WT_EINVAL, "x1 must exceed x0");
+// The analytic (warped) cube of desc, restricted to nz element layers along z
+// starting at layer z0 of the whole mesh (modulo M[2] for a periodic mesh).
+// Faces between layers of the slab couple as in the whole mesh; a z face whose
+// neighbour layer lies outside the slab gets no neighbour and no tag (a cut),
+// unless it is an outer face of the whole mesh.
+static int create_analytic(wt_ctx* ctx, const wt_mesh_desc* d, int z0, int nz, wt_mesh** out) {
   cudaSetDevice(ctx->device);
   auto* mh = new wt_mesh();
   mh->ctx = ctx;
   wt::DevMesh& m = mh->m;
   m.errflag = ctx->d_flag;
   m.N = d->N;
-  for (int a = 0; a < 3; ++a) m.M[a] = d->M[a];
-  m.Ne = (long long)d->M[0] * d->M[1] * d->M[2];
+  m.M[0] = d->M[0];
+  m.M[1] = d->M[1];
+  m.M[2] = nz;
+  m.Ne = (long long)d->M[0] * d->M[1] * nz;
   m.nn = m.Ne * d->N * d->N * d->N;
   m.precision = d->precision;
   m.affine = d->warp_A == 0.0;
@@ -576,18 +577,25 @@ int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* d, wt_mesh** out) {
   m.h_nbrf.assign(6 * m.Ne, 0);
   m.h_bdry.assign(6 * m.Ne, 0);
   const int Mx = d->M[0], My = d->M[1], Mz = d->M[2];
+  const int ML[3] = {Mx, My, nz};
   for (long long e = 0; e < m.Ne; ++e) {
     int c[3] = {(int)(e % Mx), (int)((e / Mx) % My), (int)(e / ((long long)Mx * My))};
     for (int f = 0; f < 6; ++f) {
       const int ax = f >> 1;
       int cc[3] = {c[0], c[1], c[2]};
       cc[ax] += (f & 1) ? 1 : -1;
-      if (cc[ax] < 0 || cc[ax] >= d->M[ax]) {
+      if (cc[ax] < 0 || cc[ax] >= ML[ax]) {
+        const bool whole = ax < 2 || nz == Mz;  // this axis spans the whole mesh
+        if (!whole) {
+          const int g = z0 + cc[2];  // the neighbour layer in the whole mesh
+          if (!d->periodic && (g < 0 || g >= Mz)) m.h_bdry[f + 6 * e] = d->outer_tag == 0 ? f + 1 : d->outer_tag;
+          continue;  // otherwise a cut face: no neighbour, no tag
+        }
         if (!d->periodic) {
           m.h_bdry[f + 6 * e] = d->outer_tag == 0 ? f + 1 : d->outer_tag;
           continue;
         }
-        cc[ax] = (cc[ax] + d->M[ax]) % d->M[ax];
+        cc[ax] = (cc[ax] + ML[ax]) % ML[ax];
       }
       m.h_nbr[f + 6 * e] = (int32_t)(cc[0] + (long long)Mx * (cc[1] + (long long)My * cc[2]));
       m.h_nbrf[f + 6 * e] = f ^ 1;
@@ -595,12 +603,41 @@ int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* d, wt_mesh** out) {
   }
   int rc = finish_topology(mh);
   if (!rc) rc = alloc_geometry(mh);
-  if (!rc) rc = lrc(ctx, wt::launch_geom_analytic(m, d->x0, d->x1, d->warp_A, ctx->stream), "geometry");
+  if (!rc) rc = lrc(ctx, wt::launch_geom_analytic(m, d->x0, d->x1, d->warp_A, ctx->stream, z0, Mz), "geometry");
   if (!rc) rc = derive_geometry(mh);
   if (rc) { free_mesh(mh); delete mh; return rc; }
   ctx->launches += 1;
   *out = mh;
   return 0;
+}
+
+static int check_mesh_desc(wt_ctx* ctx, const wt_mesh_desc* d) {
+  if (d->N < 2 || d->N > WT_MAXN) return fail(ctx, WT_EINVAL, "N must be in 2..8, got " + std::to_string(d->N));
+  if (d->M[0] < 1 || d->M[1] < 1 || d->M[2] < 1) return fail(ctx, WT_EINVAL, "element counts must be >= 1");
+  if (d->precision != WT_F64 && d->precision != WT_F32) return fail(ctx, WT_EINVAL, "precision must be WT_F64 or WT_F32");
+  if (!(d->x1 > d->x0)) return fail(ctx, WT_EINVAL, "x1 must exceed x0");
+  return 0;
+}
+
+int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* d, wt_mesh** out) {
+  if (!ctx) return WT_EINVAL;
+  if (!d || !out) return fail(ctx, WT_EINVAL, "wt_mesh_create: NULL argument");
+  *out = nullptr;
+  WT_TRY(check_mesh_desc(ctx, d));
+  return create_analytic(ctx, d, 0, d->M[2], out);
+}
+
+int wt_mesh_create_slab(wt_ctx* ctx, const wt_mesh_desc* d, int z0, int nz, wt_mesh** out) {
+  if (!ctx) return WT_EINVAL;
+  if (!d || !out) return fail(ctx, WT_EINVAL, "wt_mesh_create_slab: NULL argument");
+  *out = nullptr;
+  WT_TRY(check_mesh_desc(ctx, d));
+  const int Mz = d->M[2];
+  if (nz < 1 || nz > Mz) return fail(ctx, WT_EINVAL, "wt_mesh_create_slab: nz must be in 1..M[2]");
+  if (d->periodic ? (z0 < -Mz || z0 >= Mz) : (z0 < 0 || z0 + nz > Mz))
+    return fail(ctx, WT_EINVAL, "wt_mesh_create_slab: layers [z0, z0 + nz) outside the mesh (periodic meshes: "
+                                "-M[2] <= z0 < M[2])");
+  return create_analytic(ctx, d, z0, nz, out);
 }
 
 }  // extern "C"
@@ -1198,6 +1235,39 @@ static int coef_resample(wt_ctx* ctx, const wt_coef* coef, double toff, cudaStre
   return 0;
 }
 
+// One half of fused RK4 stage st (eps_ko = 0): part 1 launches K1 (flux, boundary
+// terms, the Phi stage update), part 2 K2 (divergence, the Pi stage update).
+static int rk4_stage_part(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int st,
+                          int part, const wt::ConsBC& b, int use_metric) {
+  const wt::DevMesh& m = ws->mesh->m;
+  cudaStream_t s = ctx->stream;
+  void* SP[2] = {ws->S0, ws->S1};
+  const void* inP = st == 0 ? Phi : SP[(st - 1) % 2];
+  const void* inQ = st == 0 ? Pi : ws->SQ;
+  wt::RKStage rkP, rkQ;
+  rkP.stage = rkQ.stage = st;
+  rkP.dt = rkQ.dt = dt;
+  rkP.y = Phi; rkP.acc = ws->accP; rkP.out = SP[st % 2]; rkP.comp = ws->compP;
+  rkQ.y = Pi; rkQ.acc = ws->accQ; rkQ.out = ws->SQ; rkQ.comp = ws->compQ;
+  rkP.nonfinite = rkQ.nonfinite = st == 3 ? ctx->d_flag : nullptr;
+  rkP.on = rkQ.on = 1;
+  const bool n8 = wt::cons_n8_path(m, coef->c, use_metric, b, rkP, rkQ, {inP, inQ, ws->F});
+  ws->flux_block = n8 ? wt::n8_flux_block(m) : (long long)m.N * m.N * m.N;
+  if (part == 1) {
+    prof_mark(ctx, 0);
+    WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, inP, inQ, ws->F, nullptr, ws->bbuf, nullptr, use_metric, b, rkP,
+                                       s, n8), "rk4 K1"));
+    prof_mark(ctx, 0);
+  } else {
+    prof_mark(ctx, 1);
+    WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, nullptr, ws->bbuf, use_metric, b, rkQ, rkQ.nonfinite, s, n8),
+               "rk4 K2"));
+    prof_mark(ctx, 1);
+  }
+  ctx->launches += 1;
+  return 0;
+}
+
 static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
                             double eps_ko, const wt::ConsBC& b, int use_metric) {
   const wt::DevMesh& m = ws->mesh->m;
@@ -1208,24 +1278,9 @@ static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* P
     if (coef->td) WT_TRY(coef_resample(ctx, coef, toff[st], s));
     const void* inP = st == 0 ? Phi : SP[(st - 1) % 2];
     const void* inQ = st == 0 ? Pi : ws->SQ;
-    wt::RKStage rkP, rkQ;
-    rkP.stage = rkQ.stage = st;
-    rkP.dt = rkQ.dt = dt;
-    rkP.y = Phi; rkP.acc = ws->accP; rkP.out = SP[st % 2]; rkP.comp = ws->compP;
-    rkQ.y = Pi; rkQ.acc = ws->accQ; rkQ.out = ws->SQ; rkQ.comp = ws->compQ;
-    rkP.nonfinite = rkQ.nonfinite = st == 3 ? ctx->d_flag : nullptr;
     if (eps_ko == 0.0) {
-      rkP.on = rkQ.on = 1;
-      const bool n8 = wt::cons_n8_path(m, coef->c, use_metric, b, rkP, rkQ, {inP, inQ, ws->F});
-      prof_mark(ctx, 0);
-      WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, inP, inQ, ws->F, nullptr, ws->bbuf, nullptr, use_metric, b, rkP,
-                                         s, n8), "rk4 K1"));
-      prof_mark(ctx, 0);
-      prof_mark(ctx, 1);
-      WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, nullptr, ws->bbuf, use_metric, b, rkQ, rkQ.nonfinite, s, n8),
-                 "rk4 K2"));
-      prof_mark(ctx, 1);
-      ctx->launches += 2;
+      WT_TRY(rk4_stage_part(ctx, ws, coef, Phi, Pi, dt, st, 1, b, use_metric));
+      WT_TRY(rk4_stage_part(ctx, ws, coef, Phi, Pi, dt, st, 2, b, use_metric));
     } else {
       WT_TRY(rhs_curved_impl(ctx, ws, coef, inP, inQ, ws->kP, ws->kQ, eps_ko, b, use_metric));
       WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, st, dt, Phi, ws->accP, SP[st % 2], ws->kP, s,
@@ -1381,6 +1436,67 @@ int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, v
   }
   if (!rc && coef->td) coef->t += nsteps * dt;  // the device copy was advanced step by step
   return rc;
+}
+
+int wt_rk4_stage_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int stage,
+                        int part, const wt_bc_desc* bc, int use_metric) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!coef || !Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved: NULL argument");
+  if (stage < 0 || stage > 3 || (part != 1 && part != 2))
+    return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved: stage must be 0..3 and part 1 or 2");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(ctx, WT_EINVAL, "dt must be positive and finite");
+  if (coef->mesh != ws->mesh) return fail(ctx, WT_EINVAL, "coefficients belong to another mesh");
+  wt::ConsBC b;
+  WT_TRY(make_bc(ctx, bc, use_metric, b));
+  WT_TRY(ws_step_buffers(ws));
+  if (coef->td) WT_TRY(need_setup_geometry(coef->mesh, "wt_rk4_stage_curved (time-dependent background)"));
+  comp_track(ws, Phi, Pi);
+  const double toff[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
+  if (coef->td && part == 1) WT_TRY(coef_resample(ctx, coef, toff[stage], ctx->stream));
+  WT_TRY(rk4_stage_part(ctx, ws, coef, Phi, Pi, dt, stage, part, b, use_metric));
+  if (coef->td && part == 2 && stage == 3) {
+    WT_TRY(lrc(ctx, wt::launch_advance_time(coef->d_t, dt, ctx->stream), "background time"));
+    ctx->launches += 1;
+    coef->t += dt;
+  }
+  return 0;
+}
+
+int wt_halo_size(const wt_ws* ws, long long* values) {
+  if (!ws || !values) return WT_EINVAL;
+  const wt::DevMesh& m = ws->mesh->m;
+  if (!ws->flux_block) return fail(ws->ctx, WT_EINVAL, "wt_halo_size: no fused stage has run on this workspace yet");
+  const long long L = (long long)m.M[0] * m.M[1];
+  *values = L * ((long long)m.N * m.N * m.N + 3 * ws->flux_block);
+  return 0;
+}
+
+int wt_halo_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, void* buf, int pack) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!Phi || !buf) return fail(ctx, WT_EINVAL, "wt_halo_copy: NULL argument");
+  const wt::DevMesh& m = ws->mesh->m;
+  if (stage < 0 || stage > 3) return fail(ctx, WT_EINVAL, "wt_halo_copy: stage must be 0..3");
+  if (layer < 0 || layer >= m.M[2]) return fail(ctx, WT_EINVAL, "wt_halo_copy: no such element layer");
+  if (!ws->flux_block) return fail(ctx, WT_EINVAL, "wt_halo_copy: no fused stage has run on this workspace yet");
+  const size_t es = rsize(m.precision);
+  const long long L = (long long)m.M[0] * m.M[1], N3 = (long long)m.N * m.N * m.N, B = ws->flux_block;
+  // the Phi the next stage reads (the caller's Phi after stage 3), then the three flux components
+  char* phi = (char*)(stage < 3 ? (stage % 2 ? ws->S1 : ws->S0) : Phi);
+  char* seg[4] = {phi + (size_t)(layer * L * N3) * es, nullptr, nullptr, nullptr};
+  size_t len[4] = {(size_t)(L * N3) * es, 0, 0, 0};
+  for (int c = 0; c < 3; ++c) {
+    seg[1 + c] = (char*)ws->F + (size_t)(c * m.Ne * B + layer * L * B) * es;
+    len[1 + c] = (size_t)(L * B) * es;
+  }
+  size_t off = 0;
+  for (int k = 0; k < 4; ++k) {
+    char* b = (char*)buf + off;
+    cudaError_t e = pack ? cudaMemcpyAsync(b, seg[k], len[k], cudaMemcpyDeviceToDevice, ctx->stream)
+                         : cudaMemcpyAsync(seg[k], b, len[k], cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "wt_halo_copy");
+    off += len[k];
+  }
+  return 0;
 }
 
 int wt_step_erk_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,

@@ -165,7 +165,9 @@ struct Status {
 
 // ---- launchers implemented in the .cu files -------------------------------------------
 // geometry (wt_geom.cu)
-int launch_geom_analytic(DevMesh& m, double x0, double x1, double A, cudaStream_t s);
+// analytic (warped) cube geometry; a z-slab mesh passes its first layer z0 within
+// the whole mesh of Mz layers (0: the mesh is the whole cube)
+int launch_geom_analytic(DevMesh& m, double x0, double x1, double A, cudaStream_t s, int z0 = 0, int Mz = 0);
 int launch_geom_derived(DevMesh& m, cudaStream_t s);
 int launch_metric(DevMesh& m, cudaStream_t s);
 int launch_dinvjac(DevMesh& m, cudaStream_t s);
@@ -227,6 +229,8 @@ int launch_wait_selftest(long long polls, int arrive, unsigned* flag, cudaStream
 // the split-form gradient of Phi through the n = 8 kernels (3 fields of nn words into grad)
 int launch_grad_n8(const DevMesh& m, const void* Phi, void* grad, unsigned* flag, cudaStream_t s);
 long long n8_padded_field_size(long long Ne);
+// values per element block of a flux component written by the n = 8 kernels (component c at F + c Ne block)
+long long n8_flux_block(const DevMesh& m);
 // True when an RHS evaluation takes the n = 8 pipelined path (both kernels take
 // the same path: K1 then writes F in the padded layout K2 reads).
 bool cons_n8_path(const DevMesh& m, const DevCoef& c, int use_metric, const ConsBC& bc, const RKStage& rkP,

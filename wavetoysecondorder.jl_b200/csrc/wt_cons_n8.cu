@@ -1652,6 +1652,7 @@ int launch_pad_metric_n8(DevMesh& m, cudaStream_t s) {
 // words per field of the element-block layouts (the larger, FP32, one: an
 // allocation of this size serves both precisions)
 long long n8_padded_field_size(long long Ne) { return Ne * n8::FS; }
+long long n8_flux_block(const DevMesh& m) { return n8_fs(m); }
 
 static int sm_count() {
   static int n = 0;

@@ -86,7 +86,10 @@ HostOps gll_operators(int N) {
 // ---------------------------------------------------------------------------
 // coords + analytic Jacobian of x = x0 + L (s + A P(s)), s the uniform
 // reference position, element numbering e = ex + Mx (ey + My ez).
-__global__ void k_geom_analytic(int N, int Mx, int My, int Mz, double x0, double L, double A,
+// Mz is the element count of the whole mesh along z; element layer ez of this
+// mesh is layer ez + z0 of the whole mesh (taken modulo Mz: a z-slab of a
+// periodic mesh may wrap around).
+__global__ void k_geom_analytic(int N, int Mx, int My, int Mz, int z0, double x0, double L, double A,
                                 const double* __restrict__ xg, long long nn, double* __restrict__ coords,
                                 double* __restrict__ jac) {
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -95,7 +98,9 @@ __global__ void k_geom_analytic(int N, int Mx, int My, int Mz, double x0, double
   long long e = n / N3;
   int t = (int)(n - e * N3);
   int i = t % N, j = (t / N) % N, k = t / (N * N);
-  int ex = (int)(e % Mx), ey = (int)((e / Mx) % My), ez = (int)(e / ((long long)Mx * My));
+  int ex = (int)(e % Mx), ey = (int)((e / Mx) % My), ez = (int)(e / ((long long)Mx * My)) + z0;
+  if (ez < 0) ez += Mz;
+  if (ez >= Mz) ez -= Mz;
   double s[3] = {(ex + xg[i]) / Mx, (ey + xg[j]) / My, (ez + xg[k]) / Mz};
   const double tp = 2.0 * M_PI;
   double sn[3], cs[3];
@@ -406,9 +411,9 @@ __global__ void k_min_spacing(int N, long long nn, const double* __restrict__ co
 // ---------------------------------------------------------------------------
 static inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
-int launch_geom_analytic(DevMesh& m, double x0, double x1, double A, cudaStream_t s) {
-  k_geom_analytic<<<nblk(m.nn, 256), 256, 0, s>>>(m.N, m.M[0], m.M[1], m.M[2], x0, x1 - x0, A, m.x, m.nn, m.coords,
-                                                  m.jac);
+int launch_geom_analytic(DevMesh& m, double x0, double x1, double A, cudaStream_t s, int z0, int Mz) {
+  k_geom_analytic<<<nblk(m.nn, 256), 256, 0, s>>>(m.N, m.M[0], m.M[1], Mz > 0 ? Mz : m.M[2], z0, x0, x1 - x0, A, m.x,
+                                                  m.nn, m.coords, m.jac);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

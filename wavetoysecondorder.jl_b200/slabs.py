@@ -1,0 +1,214 @@
+"""One solve of the analytic (warped) cube split into z-slabs of element layers.
+
+No counterpart in the reference, whose evolve3d (src/evolve.jl:1149-1358) runs a
+solve on one device.  Slab s owns a run of consecutive element layers and holds
+one ghost layer beyond each cut (the layer its neighbour slab owns there).  An
+RK4 stage is split in two halves (wt_rk4_stage_curved): after the first
+(gradient, flux, Phi stage update) every slab sends the layers next to its cuts
+-- the Phi the next stage reads and the three flux components, one packed
+buffer per layer (wt_halo_copy) -- to its neighbours, which unpack them into
+their ghost layers; the second half (divergence, Pi stage update) then reads
+correct neighbour traces, and so does the next stage's first half.  That is
+one halo exchange per RK4 stage.  The owned layers of every slab advance
+exactly as in the undivided mesh; ghost layers hold scratch values otherwise.
+
+Slabs live either all in one process on one device (LocalHalo: the exchange is
+a device copy per cut) or one per rank (DistHalo: torch.distributed point-to-
+point messages, NCCL between GPUs).  Kreiss-Oliger dissipation, whose line
+operators span the whole z extent, is not supported here (eps_KO = 0).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Callable, List, Optional, Sequence
+
+from . import wavetoy as wt
+
+
+@dataclass(frozen=True)
+class SlabRange:
+    """Layers of slab `index` in the whole mesh's numbering: it owns own0 .. own0 + nown - 1
+    and holds z0 .. z0 + nz - 1 (z0 may be negative for a periodic mesh: taken modulo Mz)."""
+    index: int
+    own0: int
+    nown: int
+    lower: Optional[int]   # slab owning the layer below (None: outer face or no neighbour)
+    upper: Optional[int]
+
+    @property
+    def ghost_lo(self) -> int:
+        return 0 if self.lower is None else 1
+
+    @property
+    def ghost_hi(self) -> int:
+        return 0 if self.upper is None else 1
+
+    @property
+    def z0(self) -> int:
+        return self.own0 - self.ghost_lo
+
+    @property
+    def nz(self) -> int:
+        return self.nown + self.ghost_lo + self.ghost_hi
+
+    # local layer numbers (0 .. nz - 1)
+    @property
+    def first_owned(self) -> int:
+        return self.ghost_lo
+
+    @property
+    def last_owned(self) -> int:
+        return self.ghost_lo + self.nown - 1
+
+
+def partition(Mz: int, nslabs: int, periodic: bool = False) -> List[SlabRange]:
+    """Split Mz element layers into nslabs runs as equal as possible (the first Mz mod
+    nslabs slabs get one more); periodic meshes close the ring of slabs."""
+    if nslabs < 1 or nslabs > Mz:
+        raise ValueError("need 1 <= nslabs <= Mz")
+    base, rem = divmod(Mz, nslabs)
+    out, z = [], 0
+    for r in range(nslabs):
+        n = base + (1 if r < rem else 0)
+        lower = r - 1 if r > 0 else (nslabs - 1 if periodic and nslabs > 1 else None)
+        upper = r + 1 if r < nslabs - 1 else (0 if periodic and nslabs > 1 else None)
+        rng = SlabRange(r, z, n, lower, upper)
+        if rng.nz > Mz:
+            raise ValueError(f"slab {r} would hold {rng.nz} layers of {Mz}: use fewer slabs")
+        out.append(rng)
+        z += n
+    return out
+
+
+def exchange(rng: SlabRange, pack: Callable[[int], object], unpack: Callable[[int, object], None],
+             send_recv: Callable[[list, list], None], empty: Callable[[], object]):
+    """One halo exchange of slab rng with its neighbours.  pack(layer) gives the packed
+    buffer of a local layer, unpack(layer, buf) writes one back, empty() a receive buffer;
+    send_recv(sends, recvs) moves [(slab, buffer)] pairs.  Messages are posted in two
+    phases -- every slab sends its top owned layer up while receiving its bottom ghost
+    from below, then its bottom owned layer down while receiving its top ghost from
+    above -- so that between any two slabs (two slabs of a periodic ring are each
+    other's upper and lower neighbour) sends and receives pair up in order."""
+    sends, recvs = [], []
+    if rng.upper is not None:
+        sends.append((rng.upper, pack(rng.last_owned)))
+    if rng.lower is not None:
+        recvs.append((rng.lower, 0, empty()))
+    if rng.lower is not None:
+        sends.append((rng.lower, pack(rng.first_owned)))
+    if rng.upper is not None:
+        recvs.append((rng.upper, rng.nz - 1, empty()))
+    send_recv(sends, [(peer, buf) for peer, _, buf in recvs])
+    for _, layer, buf in recvs:
+        unpack(layer, buf)
+
+
+def dist_send_recv(dist, group=None, rank_of: Callable[[int], int] = lambda s: s):
+    """send_recv for exchange() over torch.distributed: every send and receive as one
+    batch of point-to-point operations (NCCL runs a batch as one group), sends to a
+    peer in the order exchange() lists them and receives from a peer likewise."""
+    def go(sends, recvs):
+        ops = []
+        # interleave per exchange() phase: (send up, recv from below), (send down, recv from above)
+        order = []
+        for k in range(max(len(sends), len(recvs))):
+            if k < len(sends):
+                order.append(("s", sends[k]))
+            if k < len(recvs):
+                order.append(("r", recvs[k]))
+        for kind, (peer, buf) in order:
+            op = dist.isend if kind == "s" else dist.irecv
+            ops.append(dist.P2POp(op, buf, rank_of(peer), group))
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+    return go
+
+
+class Slab:
+    """One slab's device objects: mesh (wt_mesh_create_slab), static background,
+    workspace and state; ghost layers included."""
+
+    def __init__(self, ctx, rng: SlabRange, N: int, M, x0: float = 0.0, x1: float = 1.0, *, warp_A: float = 0.0,
+                 periodic: bool = False, outer_tag: int = 0, precision: int = wt.WT_F64,
+                 bg_kind: int = wt.BG_MINKOWSKI, bg_params: Sequence[float] = (), fp32_form: Optional[int] = None):
+        M = (M, M, M) if isinstance(M, int) else tuple(M)
+        self.rng = rng
+        self.ctx = ctx
+        self.mesh = wt.Mesh.slab(ctx, N, M, rng.z0, rng.nz, x0, x1, periodic=periodic, outer_tag=outer_tag,
+                                 warp_A=warp_A, precision=precision)
+        if precision == wt.WT_F32 and fp32_form is not None:
+            self.mesh.set_fp32_form(fp32_form)
+        self.coef = wt.sample_background3d(self.mesh, bg_kind, bg_params)
+        self.ws = wt.make_wave3d_workspace(self.mesh)
+        self.Phi, self.Pi = self.mesh.zeros(), self.mesh.zeros()
+        self.layer_nodes = M[0] * M[1] * N ** 3
+
+    def owned(self, field):
+        """The owned layers of a local field (a view)."""
+        a = self.rng.first_owned * self.layer_nodes
+        return field[a:a + self.rng.nown * self.layer_nodes]
+
+    def stage(self, dt: float, st: int, part: int, bc3d=None, metric: bool = True):
+        wt.rk4_stage_curved(self.Phi, self.Pi, self.coef, self.ws, dt, st, part, bc3d=bc3d, metric=metric)
+
+    def empty(self):
+        import torch
+        return torch.empty(wt.halo_size(self.ws), dtype=self.mesh.dtype, device=self.Phi.device)
+
+    def pack(self, st: int, layer: int):
+        buf = self.empty()
+        wt.halo_copy(self.ws, self.Phi, st, layer, buf, True)
+        return buf
+
+    def unpack(self, st: int, layer: int, buf):
+        wt.halo_copy(self.ws, self.Phi, st, layer, buf, False)
+
+    def close(self):
+        for o in (self.ws, self.coef, self.mesh):
+            o.close()
+
+
+class LocalHalo:
+    """All slabs in this process, on one device: each message is a device copy."""
+
+    def __init__(self, slabs: List[Slab]):
+        self.slabs = slabs
+
+    def __call__(self, st: int):
+        msgs = {}
+        for s in self.slabs:   # the layers next to each cut, packed ...
+            r = s.rng
+            if r.upper is not None:
+                msgs[(r.index, "up")] = s.pack(st, r.last_owned)
+            if r.lower is not None:
+                msgs[(r.index, "down")] = s.pack(st, r.first_owned)
+        for s in self.slabs:   # ... into the neighbours' ghost layers
+            r = s.rng
+            if r.lower is not None:
+                s.unpack(st, 0, msgs[(r.lower, "up")])
+            if r.upper is not None:
+                s.unpack(st, r.nz - 1, msgs[(r.upper, "down")])
+
+
+class DistHalo:
+    """One slab per rank (rank = slab index): torch.distributed point-to-point."""
+
+    def __init__(self, slab: Slab, dist, group=None):
+        self.slab, self.dist, self.group = slab, dist, group
+
+    def __call__(self, st: int):
+        s = self.slab
+        exchange(s.rng, lambda layer: s.pack(st, layer), lambda layer, buf: s.unpack(st, layer, buf),
+                 dist_send_recv(self.dist, self.group), s.empty)
+
+
+def step(slabs: List[Slab], halo, dt: float, nsteps: int, bc3d=None, metric: bool = True):
+    """nsteps RK4 steps of the partitioned solve (the slabs this process holds)."""
+    for _ in range(int(nsteps)):
+        for st in range(4):
+            for s in slabs:
+                s.stage(dt, st, 1, bc3d, metric)
+            halo(st)
+            for s in slabs:
+                s.stage(dt, st, 2, bc3d, metric)

@@ -152,6 +152,9 @@ def library():
         "wt_initial_data": [vp, vp, i, vp, i, d, vp, vp],
         "wt_gll_operators": [i, vp, vp, vp],
         "wt_ctx_profile": [vp, i], "wt_ctx_profile_read": [vp, C.POINTER(d * 2), C.POINTER(ll * 2)],
+        "wt_mesh_create_slab": [vp, C.POINTER(_MeshDesc), i, i, pvp],
+        "wt_rk4_stage_curved": [vp, vp, vp, vp, vp, d, i, i, C.POINTER(_BcDesc), i],
+        "wt_halo_size": [vp, C.POINTER(ll)], "wt_halo_copy": [vp, vp, vp, i, i, vp, i],
         "wt_serve_create": [vp, C.POINTER(_ServeDesc), pvp], "wt_serve_destroy": [vp],
         "wt_serve_submit": [vp, C.POINTER(_ServeRequest), C.POINTER(i)], "wt_serve_poll": [vp, C.POINTER(i)],
         "wt_serve_run": [vp], "wt_serve_get_result": [vp, i, C.POINTER(_ServeResult)],
@@ -296,6 +299,28 @@ class Mesh(_Child):
         ctx.check(library().wt_mesh_create(ctx.h, C.byref(d), C.byref(h)), "wt_mesh_create")
         m = cls(ctx, h, N, M[0] * M[1] * M[2], precision)
         m.M, m.x0, m.x1, m.warp_A, m.periodic = tuple(M), x0, x1, warp_A, periodic
+        return m
+
+    @classmethod
+    def slab(cls, ctx: Context, N: int, M, z0: int, nz: int, x0: float = 0.0, x1: float = 1.0, *,
+             periodic: bool = False, outer_tag: int = 0, warp_A: float = 0.0, precision: int = WT_F64) -> "Mesh":
+        """Element layers z0 .. z0 + nz - 1 of the analytic cube uniform_hex(N, M, ...) builds
+        (wt_mesh_create_slab): the same geometry, metric terms and tags per element; z faces
+        toward layers outside the slab are cuts (no neighbour, no tag)."""
+        if isinstance(M, int):
+            M = (M, M, M)
+        d = _MeshDesc()
+        d.N = N
+        for a in range(3):
+            d.M[a] = int(M[a])
+        d.x0, d.x1, d.warp_A = float(x0), float(x1), float(warp_A)
+        d.periodic, d.outer_tag, d.precision = int(periodic), int(outer_tag), int(precision)
+        h = C.c_void_p()
+        ctx.check(library().wt_mesh_create_slab(ctx.h, C.byref(d), int(z0), int(nz), C.byref(h)),
+                  "wt_mesh_create_slab")
+        m = cls(ctx, h, N, M[0] * M[1] * nz, precision)
+        m.M, m.x0, m.x1, m.warp_A, m.periodic = (M[0], M[1], nz), x0, x1, warp_A, periodic
+        m.z0, m.whole_M = int(z0), tuple(M)
         return m
 
     @classmethod
@@ -912,6 +937,29 @@ def l2_diff(a, b, ws: Workspace, metric: bool = False) -> float:
     out = C.c_double()
     ws.ctx.check(library().wt_l2_diff(ws.ctx.h, ws.h, _ptr(a), _ptr(b), int(metric), C.byref(out)), "l2")
     return out.value
+
+
+def rk4_stage_curved(Phi, Pi, coef: Coef, ws: Workspace, dt: float, stage: int, part: int,
+                     bc3d: Optional[BC3D] = None, metric: bool = False):
+    """Part 1 (gradient, flux, Phi stage) or 2 (divergence, Pi stage) of RK4 stage 0..3 of
+    step_rk4_curved with eps_KO = 0 (wt_rk4_stage_curved), for halo exchanges in between."""
+    p, keep = _bcptr(bc3d)
+    ws.ctx.check(library().wt_rk4_stage_curved(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt), int(stage),
+                                               int(part), p, int(bool(metric))), "wt_rk4_stage_curved")
+
+
+def halo_size(ws: Workspace) -> int:
+    """Values of one packed halo layer (wt_halo_size; after a first stage part on ws)."""
+    n = C.c_longlong()
+    ws.ctx.check(library().wt_halo_size(ws.h, C.byref(n)), "wt_halo_size")
+    return n.value
+
+
+def halo_copy(ws: Workspace, Phi, stage: int, layer: int, buf, pack: bool):
+    """Element layer `layer` of the fields read across faces after part 1 of `stage`
+    (the next stage's Phi and the three flux components) into buf (pack) or back (wt_halo_copy)."""
+    ws.ctx.check(library().wt_halo_copy(ws.ctx.h, ws.h, _ptr(Phi), int(stage), int(layer), _ptr(buf),
+                                        int(bool(pack))), "wt_halo_copy")
 
 
 def step_rk4_curved(Phi, Pi, coef: Coef, ws: Workspace, dt: float, nsteps: int, eps_KO: float = 0.0,
