@@ -353,6 +353,97 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_slab(args):
+    """One solve split across ranks: the --elements^3 warped ADM solve of the default
+    workload with its z element layers partitioned into one slab per rank
+    (slabs.py: a ghost layer beyond each cut, one halo exchange of the layers next
+    to the cuts per RK4 stage, NCCL point-to-point between GPUs; no exchange on
+    one GPU).  Strong scaling: the whole solve's DOF-updates over the maximum of
+    the ranks' device times."""
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    wt = package()
+    S = wt.slabs
+    ctx = wt.Context(local)
+    prec = wt.WT_F64 if args.precision == "f64" else wt.WT_F32
+    M, N = args.elements, args.n
+    form = {"bf16x3": wt.FP32_BF16X3, "bf16x2": wt.FP32_BF16X2, "cuda": wt.FP32_CUDA_CORES}[args.fp32_form]
+    # one slab per rank; on one GPU, --slabs slabs in this process (exchanged by device copies)
+    nslabs = world if world > 1 else max(1, args.slabs)
+    parts = S.partition(M, nslabs)
+    mine = [parts[rank]] if world > 1 else parts
+    p = wt.workloads.adm_params(args.seed)
+    c, a, w = wt.workloads.pulses(args.seed, 8, amp=(0.5, 1.0), width=(0.05, 0.15), centre=(0.25, 0.75))
+    slabs = []
+    for r in mine:
+        sl = S.Slab(ctx, r, N, M, warp_A=0.05, outer_tag=wt.SOMMERFELD_BDRY_TAG, precision=prec,
+                    bg_kind=wt.BG_ADM_PERTURBED, bg_params=p, fp32_form=form if prec == wt.WT_F32 else None)
+        wt.initial_data(sl.mesh, wt.IC_GAUSSIANS, wt.gaussian_params(c, a, w), sl.Phi)
+        slabs.append(sl)
+    h = torch.tensor([min(sl.mesh.min_spacing() for sl in slabs)], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(h, op=dist.ReduceOp.MIN)
+    dt = 0.2 * float(h.item()) / wt.workloads.max_speed(p)
+    bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+    halo = S.DistHalo(slabs[0], dist) if dist is not None else S.LocalHalo(slabs)
+    S.step(slabs, halo, dt, args.warmup, bc)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    n0 = ctx.launch_count()
+    stream = torch.cuda.current_stream()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    S.step(slabs, halo, dt, args.steps, bc)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = ctx.launch_count() - n0
+    clocks = sampler.stop()
+    t_ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        dist.barrier()
+    nodes = M ** 3 * N ** 3
+    _, t_max, _ = aggregate(dist, t_ms / 1000.0, 0.0, "cuda")
+    finite = not ctx.nonfinite()
+    wb = 8 if prec == wt.WT_F64 else 4
+    rng = mine[0]
+    halo_bytes = (wt.halo_size(slabs[0].ws) * wb) if nslabs > 1 else 0
+    line = {
+        "metric": "DOF-updates/s", "value": 2.0 * nodes * args.steps / t_max, "unit": "DOF-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": args.precision,
+        "data": "synthetic (seeded ADM background, 8 seeded Gaussian pulses; no dataset)",
+        "config": {**workload_desc(args, nodes),
+                   "parallelism": f"z-slabs x{nslabs}" + (" (one per rank)" if world > 1 else " in one process"),
+                   "layers_per_slab": [r.nown for r in parts],
+                   "ghost_layers_rank0": rng.ghost_lo + rng.ghost_hi,
+                   "halo_bytes_per_message": halo_bytes,
+                   "messages_per_stage_per_rank": (rng.ghost_lo + rng.ghost_hi) * 2},
+        "gpu_launches": launches, "clocks": clocks, "finite": finite,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for sl in slabs:
+        sl.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_batch(args):
     """Batched uneven solves: args.solves warped-cube solves (e ~ U{4..24}, n ~ {4,6,8},
     flat or perturbed ADM), FP32 form (CUDA-core n = 8 kernels), advanced together by the
@@ -508,9 +599,12 @@ def main():
                          "(three / two terms)")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["solve", "batch", "serve"], default="solve",
-                    help="solve: the large warped ADM solve (default); batch: batched uneven solves; "
-                         "serve: served Poisson request stream")
+    ap.add_argument("--workload", choices=["solve", "batch", "serve", "slab"], default="solve",
+                    help="solve: the large warped ADM solve (default; one independent solve per rank); "
+                         "batch: batched uneven solves; serve: served Poisson request stream; slab: the "
+                         "large solve split into one z-slab per rank with halo exchanges (strong scaling)")
+    ap.add_argument("--slabs", type=int, default=1,
+                    help="slab workload on one GPU: slabs held in one process (exchanged by device copies)")
     ap.add_argument("--solves", type=int, default=256, help="batch workload: number of solves")
     ap.add_argument("--batch-steps", type=int, default=300, help="batch workload: RK4 steps per solve")
     ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
@@ -524,6 +618,8 @@ def main():
         run_batch(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "slab":
+        run_slab(args)
     else:
         run_ours(args)
 
