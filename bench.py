@@ -305,6 +305,21 @@ def run_ours(args):
            "h2d_bytes_per_step": int(2 * nn * wb / args.steps), "d2h_bytes_per_step": int(2 * nn * wb + 8),
            "api": ("wt_evolve_curved_host" if prec == wt.WT_F64 else "wt_evolve_curved_host_f32")
            + " (evolve3d shape: state and energy copied to page-locked host buffers every step)"}
+    # the host link that bounds it: one device-to-host copy of both state fields into the
+    # page-locked buffers, timed with CUDA events on the current stream
+    hs = torch.cuda.current_stream()
+    l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    Ph.copy_(Phi, non_blocking=True)   # warm
+    torch.cuda.synchronize()
+    l0.record(hs)
+    Ph.copy_(Phi, non_blocking=True)
+    Qh.copy_(Pi, non_blocking=True)
+    l1.record(hs)
+    torch.cuda.synchronize()
+    link = 2 * nn * wb / (l0.elapsed_time(l1) / 1000.0) / 1e9
+    step_s = te / args.steps   # seconds per step end to end
+    e2e["d2h_link_GBps"] = link
+    e2e["d2h_bound_frac"] = (e2e["d2h_bytes_per_step"] / step_s / 1e9) / link
     del Ph, Qh
 
     # roofline of the dominant kernel (K1: gradient + flux + Phi stage update)
