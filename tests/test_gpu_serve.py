@@ -115,3 +115,29 @@ def test_engine_incremental_submission(wt, ctx):
         eng2.state(rid)
     eng2.close()
     assert not ctx.nonfinite()
+
+
+def test_auto_precision_mixes_forms_in_one_batch(wt, ctx):
+    """AUTO: requests with few steps run in FP32, the others in FP64, side by side in
+    one batch; each result equals its request stepped alone in its form."""
+    import dataclasses
+    import torch
+    S = wt.serve
+    base = requests(wt)[:4]
+    reqs = [dataclasses.replace(q, arrival=0.0, steps=st) for q, st in zip(base, (12, 30, 16, 28))]
+    eng = wt.ServeEngine(ctx, wt.serve_desc(hbm_budget=4e9, tick=4, precision=wt.SERVE_AUTO,
+                                            auto_fp32_max_steps=20, keep_results=True, fill_nodes=None))
+    rids = [eng.submit(S.native_request(q)) for q in reqs]
+    eng.run()
+    res = [eng.result(r) for r in rids]
+    assert [r["precision"] for r in res] == [wt.WT_F32, wt.WT_F64, wt.WT_F32, wt.WT_F64]
+    assert max(r["admitted"] for r in res) < min(r["finished"] for r in res)   # all four ran together
+    for q, rid, r in zip(reqs, rids, res):
+        Phi_s, Pi_s = eng.state(rid)
+        mesh, coef, ws, Phi, Pi, dt = S.build_solve(ctx, q, r["precision"], release=False)
+        wt.step_rk4_curved(Phi, Pi, coef, ws, dt, q.steps, bc3d=wt.make_bc3d([wt.BC_SOMMERFELD] * 6), metric=True)
+        tol = 1e-12 if r["precision"] == wt.WT_F64 else 1e-6
+        a = torch.cat([Phi_s, Pi_s]).double().cpu().numpy()
+        b = torch.cat([Phi, Pi]).double().cpu().numpy()
+        assert rel(a, b) <= tol, q.rid
+    eng.close()

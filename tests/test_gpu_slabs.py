@@ -3,7 +3,7 @@ wt_halo_copy; slabs.py) advances its owned element layers exactly as the
 undivided mesh does -- bit for bit, since every element's arithmetic depends
 only on its own data and its neighbours' face traces, which the halo exchange
 supplies -- through the n = 8 FP64 tensor-core kernels, the generic kernels, the
-FP32 CUDA-core form, a periodic ring of slabs and a time-dependent background
+FP32 CUDA-core and split-BF16 forms, a periodic ring of slabs and a time-dependent background
 re-sampled at every stage.  The slabs share one device here (in-process
 exchange); between GPUs the same messages go through torch.distributed."""
 import numpy as np
@@ -16,6 +16,7 @@ CASES = [  # N, M, slabs, periodic, precision, fp32 form, background
     (8, (2, 3, 7), 3, True, 0, None, 2),
     (5, (3, 3, 5), 2, False, 0, None, 2),
     (8, (2, 2, 6), 3, False, 1, 0, 2),
+    (8, (2, 2, 5), 2, False, 1, 1, 2),     # split-BF16 form: 544-word flux blocks
     (6, (2, 2, 6), 2, True, 0, None, 4),
 ]
 
