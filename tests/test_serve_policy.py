@@ -81,3 +81,27 @@ def test_request_validation():
         wt.serve_cost(wt.serve_desc(tick=0), wt.serve_request(**good))
     with pytest.raises(ValueError):
         wt.serve_request(**good, ic_params=[0.0] * 200)
+
+
+def test_native_request_describes_build_solve():
+    """serve.native_request carries the solve build_solve sets up: the warped cube
+    (A = 0.05, Sommerfeld tag on every outer face), the seeded ADM background, the
+    seeded Gaussian pulses of Phi, CFL 0.2 against the sampled speed bound."""
+    wt = load_package()
+    S, W = wt.serve, wt.workloads
+    q = S.Request(rid=3, arrival=1.25, elements=5, n=6, steps=77, seed=41, scale=0.5, pulses=3)
+    r = S.native_request(q)
+    assert r.arrival == 1.25 and r.steps == 77 and r.cfl == 0.2
+    assert (r.mesh.N, tuple(r.mesh.M), r.mesh.warp_A, r.mesh.outer_tag, r.mesh.periodic) == (6, (5, 5, 5), 0.05, 7, 0)
+    p = W.adm_params(41, 0.5)
+    assert r.bg.kind == wt.BG_ADM_PERTURBED and list(r.bg.p[:len(p)]) == [float(v) for v in p]
+    c, a, w = W.pulses(41, 3, amp=(0.5, 1.0), width=(0.05, 0.15), centre=(0.25, 0.75))
+    ic = wt.gaussian_params(c, a, w)
+    assert r.ic_kind == wt.IC_GAUSSIANS and r.nic == len(ic) == 16 and list(r.ic[:r.nic]) == ic
+    assert r.max_speed == W.max_speed(p, 24)
+    assert list(r.bc.kinds) == [wt.BC_SOMMERFELD] * 6 and not r.bc.gPhi
+    # the Python face of the engine charges what the engine's own estimate says
+    srv = S.Server.__new__(S.Server)
+    srv.budget, srv.tick, srv.max_active, srv.fill_nodes, srv.order = 1e12, 50, None, None, "hrrn"
+    srv.precision, srv.fp32_form, srv.keep = S.AUTO, wt.FP32_CUDA_CORES, False
+    assert srv._cost(q) == q.nodes * (260 + 272)      # 77 steps <= 250: FP32, n = 6
