@@ -254,6 +254,10 @@ int wt_initial_data(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, 
 int wt_workspace_create(wt_ctx* ctx, wt_mesh* mesh, wt_ws** out);
 int wt_workspace_destroy(wt_ws* ws);
 int wt_workspace_mu(wt_ws* ws, double* mu);
+/* Impose mu instead of estimating it (no counterpart in the reference): the
+ * slabs of a partitioned solve take the whole mesh's value, since each slab's
+ * own estimate differs from it. */
+int wt_workspace_set_mu(wt_ws* ws, double mu);
 
 /* ---- right-hand sides (device pointers, async) ------------------------------*/
 typedef struct {
@@ -366,6 +370,19 @@ int wt_rk4_stage_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, 
  * into buf (pack = 1) or from buf back into the fields (pack = 0), in the
  * mesh's precision, asynchronously on the context stream.  buf holds
  * wt_halo_size values (known once a first stage part has run on ws). */
+/* Kreiss-Oliger dissipation on a slab partition: its z passes reach six element
+ * layers, so such a partition keeps six ghost layers beyond each cut and
+ * refreshes them once per stage.  wt_rk4_stage_curved_ko runs one whole RK4
+ * stage of wt_step_rk4_curved with eps_ko != 0 (the RHS with dissipation, then
+ * both stage updates: the same kernels as that path).  wt_halo_state_copy then
+ * copies `count` element layers from `layer` of the state the next stage reads
+ * (the stage outputs; the caller's Phi and Pi after stage 3) into buf (pack = 1,
+ * Phi's layers then Pi's) or back (pack = 0), asynchronously on the context
+ * stream. */
+int wt_rk4_stage_curved_ko(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int stage,
+                           double eps_ko, const wt_bc_desc* bc, int use_metric);
+int wt_halo_state_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, void* Pi, int stage, int layer, int count, void* buf,
+                       int pack);
 int wt_halo_size(const wt_ws* ws, long long* values);
 int wt_halo_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, void* buf, int pack);
 /* Fixed-step explicit Runge-Kutta methods of pick_integrator_first_order

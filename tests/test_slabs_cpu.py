@@ -37,33 +37,47 @@ def test_partition_covers_layers(Mz, n, periodic):
         S.partition(3, 4)
 
 
+def test_partition_depth():
+    S = load_package().slabs
+    a, b = S.partition(14, 2, depth=6)
+    assert (a.z0, a.nz, a.top_block, a.first_owned) == (0, 13, 1, 0)
+    assert (b.z0, b.nz, b.top_block, b.first_owned) == (1, 13, 7, 6)
+    rs = S.partition(18, 3, periodic=True, depth=6)
+    assert [(r.z0, r.nz) for r in rs] == [(-6, 18), (0, 18), (6, 18)]
+    with pytest.raises(ValueError):          # a slab must own the layers it lends
+        S.partition(10, 2, depth=6)
+    with pytest.raises(ValueError):          # no more layers than the mesh has
+        S.partition(14, 2, periodic=True, depth=6)
+
+
 def _field(r, Mz, width=4):
     # a slab's local layers: owned layers hold their whole-mesh layer number, ghosts -1
     return [[float(r.own0 + k - r.ghost_lo) if r.ghost_lo <= k < r.ghost_lo + r.nown else -1.0] * width
             for k in range(r.nz)]
 
 
-@pytest.mark.parametrize("Mz,n,periodic", [(6, 2, False), (6, 2, True), (7, 3, True), (8, 4, False)])
-def test_exchange_pairs_in_order(Mz, n, periodic):
-    """Every slab posts its messages; delivery is in order per (sender, receiver) pair,
-    as NCCL and gloo deliver point-to-point messages."""
+@pytest.mark.parametrize("Mz,n,periodic,depth", [(6, 2, False, 1), (6, 2, True, 1), (7, 3, True, 1),
+                                                  (8, 4, False, 1), (14, 2, False, 6), (18, 3, True, 6),
+                                                  (9, 3, True, 2)])
+def test_exchange_pairs_in_order(Mz, n, periodic, depth):
+    """Every slab posts its messages (blocks of depth layers); delivery is in order per
+    (sender, receiver) pair, as NCCL and gloo deliver point-to-point messages."""
     S = load_package().slabs
-    rs = S.partition(Mz, n, periodic)
+    rs = S.partition(Mz, n, periodic, depth)
     fields = [_field(r, Mz) for r in rs]
     wires = defaultdict(deque)
-    posted = {}
     for r in rs:   # phase 1: every slab posts its sends
         def send_recv(sends, recvs, r=r):
             for peer, buf in sends:
                 wires[(r.index, peer)].append(list(buf))
-            posted[r.index] = recvs
-        S.exchange(r, lambda layer, r=r: fields[r.index][layer], lambda layer, buf: None, send_recv, list)
+        S.exchange(r, lambda layer, r=r: [row for row in fields[r.index][layer:layer + depth]],
+                   lambda layer, buf: None, send_recv, list)
     for r in rs:   # phase 2: receives take messages in order
         def send_recv(sends, recvs, r=r):
             for peer, buf in recvs:
                 buf.extend(wires[(peer, r.index)].popleft())
         def unpack(layer, buf, r=r):
-            fields[r.index][layer] = buf
+            fields[r.index][layer:layer + depth] = buf
         S.exchange(r, lambda layer: None, unpack, send_recv, list)
     assert all(len(q) == 0 for q in wires.values())
     for r, f in zip(rs, fields):
@@ -77,7 +91,7 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, Mz, periodic, q):
+def _worker(rank, world, port, Mz, periodic, depth, q):
     import datetime
     import importlib.util
     import torch
@@ -88,23 +102,25 @@ def _worker(rank, world, port, Mz, periodic, q):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     from conftest import load_package as lp
     S = lp().slabs
-    r = S.partition(Mz, world, periodic)[rank]
+    r = S.partition(Mz, world, periodic, depth)[rank]
     f = torch.tensor(_field(r, Mz, 5), dtype=torch.float64)
     for _ in range(3):   # repeated exchanges stay paired
-        S.exchange(r, lambda layer: f[layer].clone(), lambda layer, buf: f[layer].copy_(buf),
-                   S.dist_send_recv(dist), lambda: torch.empty(5, dtype=torch.float64))
+        S.exchange(r, lambda layer: f[layer:layer + depth].flatten().clone(),
+                   lambda layer, buf: f[layer:layer + depth].copy_(buf.view(depth, 5)),
+                   S.dist_send_recv(dist), lambda: torch.empty(depth * 5, dtype=torch.float64))
     q.put((rank, f[:, 0].tolist(), [float((r.z0 + k) % Mz) for k in range(r.nz)]))
     dist.barrier()
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,Mz,periodic", [(2, 6, False), (2, 6, True), (3, 7, True)])
-def test_exchange_over_gloo(world, Mz, periodic):
+@pytest.mark.parametrize("world,Mz,periodic,depth", [(2, 6, False, 1), (2, 6, True, 1), (3, 7, True, 1),
+                                                      (3, 18, True, 6)])
+def test_exchange_over_gloo(world, Mz, periodic, depth):
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, Mz, periodic, q)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, Mz, periodic, depth, q)) for r in range(world)]
     for p in procs:
         p.start()
     out = [q.get(timeout=180) for _ in procs]

@@ -1040,6 +1040,16 @@ int wt_workspace_mu(wt_ws* ws, double* mu) {
   return 0;
 }
 
+int wt_workspace_set_mu(wt_ws* ws, double mu) {
+  if (!ws) return WT_EINVAL;
+  if (!(mu > 0) || !std::isfinite(mu)) return fail(ws->ctx, WT_EINVAL, "wt_workspace_set_mu: mu must be positive");
+  WT_TRY(ws_k_buffers(ws));  // ensure_mu allocates these with the estimate; the RK4 paths rely on it
+  ws->mu = mu;
+  ws->inv_mu5 = std::pow(1.0 / mu, 5);
+  ws->mu_done = true;
+  return 0;
+}
+
 // ---- RHS ----------------------------------------------------------------------------
 int wt_rhs_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, void* Phidot,
                   void* Pidot, double eps_ko, const wt_bc_desc* bc, int use_metric) {
@@ -1458,6 +1468,67 @@ int wt_rk4_stage_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, 
     WT_TRY(lrc(ctx, wt::launch_advance_time(coef->d_t, dt, ctx->stream), "background time"));
     ctx->launches += 1;
     coef->t += dt;
+  }
+  return 0;
+}
+
+int wt_rk4_stage_curved_ko(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int stage,
+                           double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!coef || !Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved_ko: NULL argument");
+  if (stage < 0 || stage > 3) return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved_ko: stage must be 0..3");
+  if (eps_ko == 0.0 || !std::isfinite(eps_ko))
+    return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved_ko: eps_ko must be nonzero (eps_ko = 0: wt_rk4_stage_curved)");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(ctx, WT_EINVAL, "dt must be positive and finite");
+  if (coef->mesh != ws->mesh) return fail(ctx, WT_EINVAL, "coefficients belong to another mesh");
+  wt::ConsBC b;
+  WT_TRY(make_bc(ctx, bc, use_metric, b));
+  WT_TRY(ws_step_buffers(ws));
+  WT_TRY(ws_k_buffers(ws));
+  WT_TRY(ensure_mu(ws));
+  if (coef->td) WT_TRY(need_setup_geometry(coef->mesh, "wt_rk4_stage_curved_ko (time-dependent background)"));
+  comp_track(ws, Phi, Pi);
+  const wt::DevMesh& m = ws->mesh->m;
+  cudaStream_t s = ctx->stream;
+  void* SP[2] = {ws->S0, ws->S1};
+  const double toff[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
+  if (coef->td) WT_TRY(coef_resample(ctx, coef, toff[stage], s));
+  // the stage of step_curved_once with eps_ko != 0: RHS with dissipation, then both updates
+  const void* inP = stage == 0 ? Phi : SP[(stage - 1) % 2];
+  const void* inQ = stage == 0 ? Pi : ws->SQ;
+  WT_TRY(rhs_curved_impl(ctx, ws, coef, inP, inQ, ws->kP, ws->kQ, eps_ko, b, use_metric));
+  WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, stage, dt, Phi, ws->accP, SP[stage % 2], ws->kP, s,
+                                       ws->compP), "rk4"));
+  WT_TRY(lrc(ctx, wt::launch_rk_update(m.nn, m.precision, stage, dt, Pi, ws->accQ, ws->SQ, ws->kQ, s, ws->compQ),
+             "rk4"));
+  ctx->launches += 2;
+  if (coef->td && stage == 3) {
+    WT_TRY(lrc(ctx, wt::launch_advance_time(coef->d_t, dt, s), "background time"));
+    ctx->launches += 1;
+    coef->t += dt;
+  }
+  return 0;
+}
+
+int wt_halo_state_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, void* Pi, int stage, int layer, int count, void* buf,
+                       int pack) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!Phi || !Pi || !buf) return fail(ctx, WT_EINVAL, "wt_halo_state_copy: NULL argument");
+  const wt::DevMesh& m = ws->mesh->m;
+  if (stage < 0 || stage > 3) return fail(ctx, WT_EINVAL, "wt_halo_state_copy: stage must be 0..3");
+  if (count < 1 || layer < 0 || layer + count > m.M[2])
+    return fail(ctx, WT_EINVAL, "wt_halo_state_copy: layers outside the mesh");
+  WT_TRY(ws_step_buffers(ws));
+  const size_t es = rsize(m.precision);
+  const long long L = (long long)m.M[0] * m.M[1], N3 = (long long)m.N * m.N * m.N;
+  // the state the next stage reads: the stage outputs, or the caller's Phi and Pi after stage 3
+  char* f[2] = {(char*)(stage < 3 ? (stage % 2 ? ws->S1 : ws->S0) : Phi), (char*)(stage < 3 ? ws->SQ : Pi)};
+  const size_t off = (size_t)(layer * L * N3) * es, len = (size_t)(count * L * N3) * es;
+  for (int k = 0; k < 2; ++k) {
+    char* b = (char*)buf + k * len;
+    cudaError_t e = pack ? cudaMemcpyAsync(b, f[k] + off, len, cudaMemcpyDeviceToDevice, ctx->stream)
+                         : cudaMemcpyAsync(f[k] + off, b, len, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "wt_halo_state_copy");
   }
   return 0;
 }

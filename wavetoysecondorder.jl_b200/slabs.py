@@ -12,10 +12,15 @@ correct neighbour traces, and so does the next stage's first half.  That is
 one halo exchange per RK4 stage.  The owned layers of every slab advance
 exactly as in the undivided mesh; ghost layers hold scratch values otherwise.
 
+With Kreiss-Oliger dissipation (eps_KO != 0) the z passes of D^6 reach six
+element layers, so the partition keeps depth = 6 ghost layers beyond each cut.
+Every stage then runs whole on each slab (wt_rk4_stage_curved_ko), after which
+the state the next stage reads is exchanged, six layers per cut (step_ko).  The
+slabs take the whole mesh's mu (Workspace.set_mu).
+
 Slabs live either all in one process on one device (LocalHalo: the exchange is
 a device copy per cut) or one per rank (DistHalo: torch.distributed point-to-
-point messages, NCCL between GPUs).  Kreiss-Oliger dissipation, whose line
-operators span the whole z extent, is not supported here (eps_KO = 0).
+point messages, NCCL between GPUs).
 """
 from __future__ import annotations
 
@@ -32,16 +37,17 @@ class SlabRange:
     index: int
     own0: int
     nown: int
-    lower: Optional[int]   # slab owning the layer below (None: outer face or no neighbour)
+    lower: Optional[int]   # slab owning the layers below (None: outer face or no neighbour)
     upper: Optional[int]
+    depth: int = 1         # ghost layers beyond each cut
 
     @property
     def ghost_lo(self) -> int:
-        return 0 if self.lower is None else 1
+        return 0 if self.lower is None else self.depth
 
     @property
     def ghost_hi(self) -> int:
-        return 0 if self.upper is None else 1
+        return 0 if self.upper is None else self.depth
 
     @property
     def z0(self) -> int:
@@ -60,21 +66,32 @@ class SlabRange:
     def last_owned(self) -> int:
         return self.ghost_lo + self.nown - 1
 
+    @property
+    def top_block(self) -> int:
+        """First local layer of the depth owned layers its upper neighbour holds as ghosts."""
+        return self.ghost_lo + self.nown - self.depth
 
-def partition(Mz: int, nslabs: int, periodic: bool = False) -> List[SlabRange]:
+
+def partition(Mz: int, nslabs: int, periodic: bool = False, depth: int = 1) -> List[SlabRange]:
     """Split Mz element layers into nslabs runs as equal as possible (the first Mz mod
-    nslabs slabs get one more); periodic meshes close the ring of slabs."""
+    nslabs slabs get one more); periodic meshes close the ring of slabs.  depth ghost
+    layers beyond each cut (1 for the RHS alone, 6 with Kreiss-Oliger dissipation)
+    must come from the neighbour's own layers, so every slab owns at least depth."""
     if nslabs < 1 or nslabs > Mz:
         raise ValueError("need 1 <= nslabs <= Mz")
+    if depth < 1:
+        raise ValueError("depth must be >= 1")
     base, rem = divmod(Mz, nslabs)
     out, z = [], 0
     for r in range(nslabs):
         n = base + (1 if r < rem else 0)
         lower = r - 1 if r > 0 else (nslabs - 1 if periodic and nslabs > 1 else None)
         upper = r + 1 if r < nslabs - 1 else (0 if periodic and nslabs > 1 else None)
-        rng = SlabRange(r, z, n, lower, upper)
+        rng = SlabRange(r, z, n, lower, upper, depth)
         if rng.nz > Mz:
             raise ValueError(f"slab {r} would hold {rng.nz} layers of {Mz}: use fewer slabs")
+        if nslabs > 1 and n < depth:
+            raise ValueError(f"slab {r} owns {n} layers, fewer than the {depth} ghost layers it supplies")
         out.append(rng)
         z += n
     return out
@@ -83,7 +100,8 @@ def partition(Mz: int, nslabs: int, periodic: bool = False) -> List[SlabRange]:
 def exchange(rng: SlabRange, pack: Callable[[int], object], unpack: Callable[[int, object], None],
              send_recv: Callable[[list, list], None], empty: Callable[[], object]):
     """One halo exchange of slab rng with its neighbours.  pack(layer) gives the packed
-    buffer of a local layer, unpack(layer, buf) writes one back, empty() a receive buffer;
+    buffer of the rng.depth local layers from `layer`, unpack(layer, buf) writes one
+    back, empty() a receive buffer;
     send_recv(sends, recvs) moves [(slab, buffer)] pairs.  Messages are posted in two
     phases -- every slab sends its top owned layer up while receiving its bottom ghost
     from below, then its bottom owned layer down while receiving its top ghost from
@@ -91,13 +109,13 @@ def exchange(rng: SlabRange, pack: Callable[[int], object], unpack: Callable[[in
     other's upper and lower neighbour) sends and receives pair up in order."""
     sends, recvs = [], []
     if rng.upper is not None:
-        sends.append((rng.upper, pack(rng.last_owned)))
+        sends.append((rng.upper, pack(rng.top_block)))
     if rng.lower is not None:
         recvs.append((rng.lower, 0, empty()))
     if rng.lower is not None:
         sends.append((rng.lower, pack(rng.first_owned)))
     if rng.upper is not None:
-        recvs.append((rng.upper, rng.nz - 1, empty()))
+        recvs.append((rng.upper, rng.nz - rng.depth, empty()))
     send_recv(sends, [(peer, buf) for peer, _, buf in recvs])
     for _, layer, buf in recvs:
         unpack(layer, buf)
@@ -131,7 +149,8 @@ class Slab:
 
     def __init__(self, ctx, rng: SlabRange, N: int, M, x0: float = 0.0, x1: float = 1.0, *, warp_A: float = 0.0,
                  periodic: bool = False, outer_tag: int = 0, precision: int = wt.WT_F64,
-                 bg_kind: int = wt.BG_MINKOWSKI, bg_params: Sequence[float] = (), fp32_form: Optional[int] = None):
+                 bg_kind: int = wt.BG_MINKOWSKI, bg_params: Sequence[float] = (), fp32_form: Optional[int] = None,
+                 mu: Optional[float] = None):
         M = (M, M, M) if isinstance(M, int) else tuple(M)
         self.rng = rng
         self.ctx = ctx
@@ -141,6 +160,8 @@ class Slab:
             self.mesh.set_fp32_form(fp32_form)
         self.coef = wt.sample_background3d(self.mesh, bg_kind, bg_params)
         self.ws = wt.make_wave3d_workspace(self.mesh)
+        if mu is not None:
+            self.ws.set_mu(mu)
         self.Phi, self.Pi = self.mesh.zeros(), self.mesh.zeros()
         self.layer_nodes = M[0] * M[1] * N ** 3
 
@@ -163,6 +184,22 @@ class Slab:
 
     def unpack(self, st: int, layer: int, buf):
         wt.halo_copy(self.ws, self.Phi, st, layer, buf, False)
+
+    # the state halo of the dissipative stepping (depth layers of Phi and Pi)
+    def stage_ko(self, dt: float, st: int, eps_KO: float, bc3d=None, metric: bool = True):
+        wt.rk4_stage_curved_ko(self.Phi, self.Pi, self.coef, self.ws, dt, st, eps_KO, bc3d=bc3d, metric=metric)
+
+    def empty_state(self):
+        import torch
+        return torch.empty(2 * self.rng.depth * self.layer_nodes, dtype=self.mesh.dtype, device=self.Phi.device)
+
+    def pack_state(self, st: int, layer: int):
+        buf = self.empty_state()
+        wt.halo_state_copy(self.ws, self.Phi, self.Pi, st, layer, self.rng.depth, buf, True)
+        return buf
+
+    def unpack_state(self, st: int, layer: int, buf):
+        wt.halo_state_copy(self.ws, self.Phi, self.Pi, st, layer, self.rng.depth, buf, False)
 
     def close(self):
         for o in (self.ws, self.coef, self.mesh):
@@ -203,8 +240,59 @@ class DistHalo:
                  dist_send_recv(self.dist, self.group), s.empty)
 
 
+class LocalStateHalo:
+    """The state halo (depth layers of Phi and Pi) between slabs of this process."""
+
+    def __init__(self, slabs: List[Slab]):
+        self.slabs = slabs
+
+    def __call__(self, st: int):
+        msgs = {}
+        for s in self.slabs:
+            r = s.rng
+            if r.upper is not None:
+                msgs[(r.index, "up")] = s.pack_state(st, r.top_block)
+            if r.lower is not None:
+                msgs[(r.index, "down")] = s.pack_state(st, r.first_owned)
+        for s in self.slabs:
+            r = s.rng
+            if r.lower is not None:
+                s.unpack_state(st, 0, msgs[(r.lower, "up")])
+            if r.upper is not None:
+                s.unpack_state(st, r.nz - r.depth, msgs[(r.upper, "down")])
+
+
+class DistStateHalo:
+    """The state halo, one slab per rank, over torch.distributed."""
+
+    def __init__(self, slab: Slab, dist, group=None):
+        self.slab, self.dist, self.group = slab, dist, group
+
+    def __call__(self, st: int):
+        s = self.slab
+        exchange(s.rng, lambda layer: s.pack_state(st, layer), lambda layer, buf: s.unpack_state(st, layer, buf),
+                 dist_send_recv(self.dist, self.group), s.empty_state)
+
+
+def step_ko(slabs: List[Slab], halo, dt: float, nsteps: int, eps_KO: float, bc3d=None, metric: bool = True):
+    """nsteps RK4 steps with Kreiss-Oliger dissipation: every stage whole on each slab,
+    then the state halo (depth 6).  The ghost layers of the starting state are
+    exchanged first, so any state the owners hold can start it."""
+    if any(s.rng.depth < 6 for s in slabs if s.rng.lower is not None or s.rng.upper is not None):
+        raise ValueError("dissipation on slabs needs partition(..., depth=6)")
+    halo(3)
+    for _ in range(int(nsteps)):
+        for st in range(4):
+            for s in slabs:
+                s.stage_ko(dt, st, eps_KO, bc3d, metric)
+            halo(st)
+
+
 def step(slabs: List[Slab], halo, dt: float, nsteps: int, bc3d=None, metric: bool = True):
-    """nsteps RK4 steps of the partitioned solve (the slabs this process holds)."""
+    """nsteps RK4 steps of the partitioned solve (the slabs this process holds; depth-1
+    partitions, eps_KO = 0)."""
+    if any(s.rng.depth != 1 for s in slabs):
+        raise ValueError("the flux halo is one layer deep: use step_ko for a depth-6 partition")
     for _ in range(int(nsteps)):
         for st in range(4):
             for s in slabs:

@@ -155,6 +155,9 @@ def library():
         "wt_mesh_create_slab": [vp, C.POINTER(_MeshDesc), i, i, pvp],
         "wt_rk4_stage_curved": [vp, vp, vp, vp, vp, d, i, i, C.POINTER(_BcDesc), i],
         "wt_halo_size": [vp, C.POINTER(ll)], "wt_halo_copy": [vp, vp, vp, i, i, vp, i],
+        "wt_workspace_set_mu": [vp, d],
+        "wt_rk4_stage_curved_ko": [vp, vp, vp, vp, vp, d, i, d, C.POINTER(_BcDesc), i],
+        "wt_halo_state_copy": [vp, vp, vp, vp, i, i, i, vp, i],
         "wt_serve_create": [vp, C.POINTER(_ServeDesc), pvp], "wt_serve_destroy": [vp],
         "wt_serve_submit": [vp, C.POINTER(_ServeRequest), C.POINTER(i)], "wt_serve_poll": [vp, C.POINTER(i)],
         "wt_serve_run": [vp], "wt_serve_get_result": [vp, i, C.POINTER(_ServeResult)],
@@ -500,6 +503,11 @@ class Workspace(_Child):
             self.ctx.check(library().wt_workspace_mu(self.h, C.byref(mu)), "wt_workspace_mu")
             self._mu = mu.value
         return self._mu
+
+    def set_mu(self, mu: float):
+        """Impose mu (wt_workspace_set_mu): the slabs of a partitioned solve take the whole mesh's."""
+        self.ctx.check(library().wt_workspace_set_mu(self.h, float(mu)), "wt_workspace_set_mu")
+        self._mu = float(mu)
 
     @property
     def inv_mu5(self) -> float:
@@ -946,6 +954,22 @@ def rk4_stage_curved(Phi, Pi, coef: Coef, ws: Workspace, dt: float, stage: int, 
     p, keep = _bcptr(bc3d)
     ws.ctx.check(library().wt_rk4_stage_curved(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt), int(stage),
                                                int(part), p, int(bool(metric))), "wt_rk4_stage_curved")
+
+
+def rk4_stage_curved_ko(Phi, Pi, coef: Coef, ws: Workspace, dt: float, stage: int, eps_KO: float,
+                        bc3d: Optional[BC3D] = None, metric: bool = False):
+    """One whole RK4 stage 0..3 of step_rk4_curved with Kreiss-Oliger dissipation eps_KO != 0
+    (wt_rk4_stage_curved_ko), for halo exchanges between stages."""
+    p, keep = _bcptr(bc3d)
+    ws.ctx.check(library().wt_rk4_stage_curved_ko(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt), int(stage),
+                                                  float(eps_KO), p, int(bool(metric))), "wt_rk4_stage_curved_ko")
+
+
+def halo_state_copy(ws: Workspace, Phi, Pi, stage: int, layer: int, count: int, buf, pack: bool):
+    """count element layers from `layer` of the state the stage after `stage` reads (Phi's
+    layers, then Pi's) into buf (pack) or back (wt_halo_state_copy)."""
+    ws.ctx.check(library().wt_halo_state_copy(ws.ctx.h, ws.h, _ptr(Phi), _ptr(Pi), int(stage), int(layer), int(count),
+                                              _ptr(buf), int(bool(pack))), "wt_halo_state_copy")
 
 
 def halo_size(ws: Workspace) -> int:
