@@ -287,10 +287,14 @@ int wt_rhs_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, 
  * (8.4 MiB, held on every GPU that loads the library until exit), so the mesh
  * may have at most WT_NOALLOC_MAX_NODES nodes and WT_NOALLOC_MAX_BOUNDARY_NODES
  * boundary-face nodes; larger meshes are rejected with WT_EINVAL.  mu is the
- * workspace's KO normalisation (wt_workspace_mu), used only when eps_ko != 0.
- * The first call on a device looks up the array's device address (set-up);
- * make that first call before any stream capture.  All calls share the array:
- * calls whose kernels overlap on the GPU race and give wrong results. */
+ * KO normalisation that wt_workspace_mu returns for a workspace on the same
+ * mesh, used only when eps_ko != 0 (then a non-positive or non-finite mu is
+ * rejected with WT_EINVAL; nothing else ties mu to the mesh).  The first call
+ * through each wt_ctx looks up the array's device address on the context's
+ * device (set-up); make that first call before any stream capture.  The
+ * address belongs to the device's primary context: after cudaDeviceReset,
+ * create a new wt_ctx.  All calls share the array: calls whose kernels overlap
+ * on the GPU race and give wrong results. */
 #define WT_NOALLOC_MAX_NODES 262144
 #define WT_NOALLOC_MAX_BOUNDARY_NODES 262144
 int wt_rhs_curved_noalloc(wt_ctx* ctx, const wt_coef* coef, const void* Phi, const void* Pi, void* Phidot,

@@ -322,6 +322,64 @@ class OracleMesh:
         return lib().or_min_spacing(self.h)
 
 
+# ---- initial data and analytic references (numpy, Float64) --------------------
+# Restatements of the reference's closed-form fields, evaluated at node
+# coordinates x, y, z; each returns (u, u_t).
+
+def ic_eigenmode_cartesian(x, y, z, t, A, kx, ky, kz, om, x0, x1):
+    """eigenmode_cartesian! (src/wave.jl:163-185)."""
+    L = x1 - x0
+    s = np.sin(kx * (x - x0) / L) * np.sin(ky * (y - x0) / L) * np.sin(kz * (z - x0) / L)
+    return A * s * np.cos(om * t), -A * om * s * np.sin(om * t)
+
+
+def ic_gaussians(x, y, z, pulses):
+    """The :gaussian IC exp(-|x - c|^2 / (2 w^2)) (src/evolve.jl:1260-1263), one term per
+    (cx, cy, cz, A, w) in pulses, scaled by A and summed; u_t = 0."""
+    u = np.zeros_like(x)
+    for cx, cy, cz, A, w in pulses:
+        u = u + A * np.exp(-((x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2) / (2.0 * w * w))
+    return u, np.zeros_like(x)
+
+
+def _sinhc(v):
+    """sinh(v)/v with the reference's Taylor branch for v^2 < 1/1000 (src/wave.jl:242-250)."""
+    v = np.asarray(v, dtype=np.float64)
+    v2 = v * v
+    small = v2 < 1.0 / 1000.0
+    safe = np.where(small, 1.0, v)
+    return np.where(small, 1.0 + v2 * (1.0 / 6.0 + v2 * (1.0 / 120.0 + v2 * (1.0 / 5040.0))), np.sinh(safe) / safe)
+
+
+def ic_outgoing_pulse(x, y, z, t, A, s0, sigma, cx, cy, cz):
+    """outgoing_pulse! (src/wave.jl:292-323): u = 2A (b/s^2) sinhc(b r/s^2) exp(-(b^2 + r^2)/(2 s^2)),
+    b = t + s0, and its time derivative."""
+    is2 = 1.0 / (sigma * sigma)
+    be = t + s0
+    r2 = (x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2
+    r = np.sqrt(r2)
+    ex = np.exp(-0.5 * (be * be + r2) * is2)
+    u = 2.0 * A * be * is2 * _sinhc(be * r * is2) * ex
+    ut = -2.0 * A * is2 * ex * (be * be * is2 * _sinhc(be * r * is2) - np.cosh(be * r * is2))
+    return u, ut
+
+
+def ic_plane_wave(x, y, z, t, k, om, s):
+    """Phi_e, Pi_e of _background3d :minkowski / :constant_shift (src/evolve.jl:1119-1120):
+    Phi = sin(k (x + y + z) - om t), Pi = (-om - k s) cos(k (x + y + z) - om t)."""
+    ph = k * (x + y + z) - om * t
+    return np.sin(ph), (-om - k * s) * np.cos(ph)
+
+
+def ic_eigenmode_radial(x, y, z, t, A, R, n, cx, cy, cz):
+    """eigenmode_radial! (src/wave.jl:207-226): u = A sinc(n r / R) cos(om t), om = n pi / R,
+    sinc(v) = sin(pi v)/(pi v)."""
+    om = n * np.pi / R
+    r = np.sqrt((x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2)
+    sc = np.sinc(n * r / R)
+    return A * sc * np.cos(om * t), -A * om * sc * np.sin(om * t)
+
+
 def erk_tableau(method):
     """(c, A, b) of the oracle's Butcher tableau for method (1 Tsit5, 0 RK4)."""
     c, A, b = np.zeros(7), np.zeros(49), np.zeros(7)

@@ -270,6 +270,42 @@ def test_rk4_curved_with_ko(wt, ctx, O):
     assert rel(host(Pg), Po) < TOL64 and rel(host(Qg), Qo) < TOL64
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_ko_n8_warped_adm(wt, ctx, O, prec):
+    """Kreiss-Oliger dissipation at n = 8 (_ko_axis3!, src/wave3d_curved.jl:182-192, 241-248)
+    on the curvilinear warped ADM solve: the dissipative RHS (n = 8 K1/K2 plus the
+    line-local D^6 passes) and 20 RK4 steps with eps_KO = 0.1 (the stage path
+    wt_step_rk4_curved takes when eps_KO != 0), against the oracle.  FP64 <= 1e-12
+    (5e-12 for the one RHS through the tensor cores); FP32 <= 1e-5."""
+    import torch
+    g, o = pair(wt, ctx, O, 8, (3, 2, 3), A=0.05, outer_tag=7, precision=prec)
+    p = wt.workloads.adm_params(6)
+    cg, co = wt.sample_background3d(g, 2, p), o.background(2, p)
+    ws = wt.make_wave3d_workspace(g)
+    assert abs(ws.mu - o.mu()) <= (1e-10 if prec == 0 else 1e-6) * o.mu()
+    x, y, z = o.coords()
+    c, a, w = wt.workloads.pulses(6, 2, amp=(0.5, 1.0), width=(0.08, 0.15))
+    Phi = wt.workloads.gaussian_field(x, y, z, c, a, w)
+    Pi = 0.5 * np.sin(3 * x + 1) * np.cos(2 * y) * Phi
+    dt_ = torch.float64 if prec == 0 else torch.float32
+    bcg, bco = wt.make_bc3d([2] * 6), O.make_bc([2] * 6)
+    Pd, Qd = g.zeros(), g.zeros()
+    wt.wave3d_curved_rhs(Pd, Qd, dev(dt_, Phi), dev(dt_, Pi), cg, ws, eps_KO=0.1, bc3d=bcg, metric=True)
+    Po, Qo = o.rhs_curved(co, Phi, Pi, eps_ko=0.1, bc=bco, use_metric=True)
+    # the dissipation is a visible part of the RHS, not round-off
+    P0, Q0 = o.rhs_curved(co, Phi, Pi, eps_ko=0.0, bc=bco, use_metric=True)
+    assert rel(Po, P0) > 1e-6 and rel(Qo, Q0) > 1e-6
+    tol_rhs = TOL_TC if prec == 0 else 5e-5
+    assert rel(host(Pd), Po) < tol_rhs and rel(host(Qd), Qo) < tol_rhs, (rel(host(Pd), Po), rel(host(Qd), Qo))
+    dt = 0.2 * o.min_spacing() / wt.workloads.max_speed(p)
+    Pg, Qg = dev(dt_, Phi), dev(dt_, Pi)
+    wt.step_rk4_curved(Pg, Qg, cg, ws, dt, 20, eps_KO=0.1, bc3d=bcg, metric=True)
+    Po, Qo = o.evolve_curved(co, Phi, Pi, dt, 20, eps_ko=0.1, bc=bco, use_metric=True)
+    tol = TOL64 if prec == 0 else TOL32
+    assert rel(host(Pg), Po) < tol and rel(host(Qg), Qo) < tol, (rel(host(Pg), Po), rel(host(Qg), Qo))
+    assert not ctx.nonfinite()
+
+
 @pytest.mark.parametrize("tau", [37.5, 20.0])
 def test_sipg_standing_wave_100_steps(wt, ctx, O, tau):
     """The flat SIPG standing-wave workload (4^3 elements, n = 6, KO 0.1, RK4 CFL 0.25,

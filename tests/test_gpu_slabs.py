@@ -103,16 +103,18 @@ def test_slab_errors(wt, ctx):
     wt.halo_copy(ws, P, 0, 2, buf, True)
 
 
-@pytest.mark.parametrize("N,M,nslabs,periodic", [(5, (2, 2, 14), 2, False), (8, (2, 2, 14), 2, False),
-                                                 (6, (2, 2, 21), 3, True)])
-def test_dissipative_slab_solve_equals_whole_mesh(wt, ctx, N, M, nslabs, periodic):
+@pytest.mark.parametrize("N,M,nslabs,periodic,prec", [(5, (2, 2, 14), 2, False, 0), (8, (2, 2, 14), 2, False, 0),
+                                                      (6, (2, 2, 21), 3, True, 0), (8, (2, 2, 14), 2, False, 1)])
+def test_dissipative_slab_solve_equals_whole_mesh(wt, ctx, N, M, nslabs, periodic, prec):
     """Kreiss-Oliger dissipation on slabs: six ghost layers per cut (its z passes reach
     six elements), whole stages on each slab and a state halo after every stage, the
     whole mesh's mu imposed on every slab -- the owned layers match the undivided
-    solve to round-off (<= 1e-13 of the field's maximum)."""
+    solve to round-off (<= 1e-13 of the field's maximum in FP64; <= 1e-6 for the
+    FP32 form, whose Kahan compensation of the RK4 sums is also kept on the ghost
+    layers that the state halo overwrites)."""
     import torch
     S = wt.slabs
-    kw = dict(warp_A=0.05, periodic=periodic, outer_tag=0 if periodic else 7)
+    kw = dict(warp_A=0.05, periodic=periodic, outer_tag=0 if periodic else 7, precision=prec)
     prm = wt.workloads.adm_params(7)
     ic = wt.gaussian_params(*wt.workloads.pulses(7, 2))
     bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
@@ -135,7 +137,8 @@ def test_dissipative_slab_solve_equals_whole_mesh(wt, ctx, N, M, nslabs, periodi
     Qs = torch.cat([s.owned(s.Pi) for s in slabs])
     dP = float((Ps - P).abs().max()) / float(P.abs().max())
     dQ = float((Qs - Q).abs().max()) / float(Q.abs().max())
-    assert dP <= 1e-13 and dQ <= 1e-13, (dP, dQ)
+    tol = 1e-13 if prec == wt.WT_F64 else 1e-6
+    assert dP <= tol and dQ <= tol, (dP, dQ)
     for s in slabs:
         s.close()
     assert not ctx.nonfinite()

@@ -81,3 +81,14 @@ def test_noalloc_rejects_meshes_above_the_limit(wt, ctx):
         wt.wave3d_curved_rhs_noalloc(P, Q, P, Q, coef, metric=True)
     assert ei.value.code == -1
     assert "at most 262144" in str(ei.value)
+
+
+def test_noalloc_rejects_non_finite_mu(wt, ctx):
+    mesh = wt.Mesh.uniform_hex(ctx, 5, (2, 2, 2), 0.0, 1.0, outer_tag=0)
+    coef = wt.sample_background3d(mesh, wt.BG_ADM_PERTURBED, wt.workloads.adm_params(7))
+    P, Q = mesh.zeros(), mesh.zeros()
+    for mu in (float("inf"), float("nan"), 0.0, -1.0):
+        with pytest.raises(wt.WaveToyError) as ei:
+            wt.wave3d_curved_rhs_noalloc(P, Q, P, Q, coef, eps_KO=0.1, mu=mu)
+        assert ei.value.code == -1
+        assert "positive and finite" in str(ei.value)

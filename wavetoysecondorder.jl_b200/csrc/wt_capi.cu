@@ -30,6 +30,7 @@ struct wt_ctx {
   int prof_on = 0;
   std::vector<cudaEvent_t> prof_ev[2];  // [kernel] start/stop pairs
   cudaEvent_t ord_a = nullptr, ord_b = nullptr;  // order the graph stream with the caller's stream
+  double* noalloc_scratch = nullptr;  // device address of the wt_rhs_curved_noalloc array (first call)
 };
 
 static void prof_mark(wt_ctx* ctx, int which) {
@@ -2179,9 +2180,11 @@ int wt_batch_group_info(wt_batch* b, int group, int* N, int* precision, int* n8_
 // (8.4 MiB) until the process exits.
 //
 // The array's name is only a host-side stand-in for the symbol; its device
-// address is looked up once per device, with that device current, by
-// cudaGetSymbolAddress on the first call on that device, and that address is
-// what the kernels receive.
+// address is looked up by cudaGetSymbolAddress, with the context's device
+// current, on the first call made through each wt_ctx, and that address is
+// what the kernels receive.  Keeping it per context (not per device for the
+// whole process) means a context created after cudaDeviceReset looks the
+// address up again instead of reusing one from before the reset.
 //
 // Every call uses the same array and it keeps the contents of the last call.
 // Nothing in it has to start at zero: the gradient pass writes every flux
@@ -2199,16 +2202,9 @@ constexpr long long kNoallocDoubles = 3 * kNoallocFluxDoubles + kNoallocBdryDoub
 
 static __device__ __align__(256) double wt_noalloc_scratch[kNoallocDoubles];
 
-constexpr int kNoallocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-double* g_noalloc_ptr[kNoallocMaxDevices] = {};
-
-// Device address of the scratch array on ctx's device (set-up on first use).
+// Device address of the scratch array for ctx (set-up on the context's first call).
 int noalloc_scratch(wt_ctx* ctx, double** out) {
-  if (ctx->device < 0 || ctx->device >= kNoallocMaxDevices)
-    return fail(ctx, WT_ENOTSUP, "wt_rhs_curved_noalloc: device ordinal beyond the supported range");
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[ctx->device]) {
+  if (!ctx->noalloc_scratch) {
     int prev = 0;
     cudaError_t e = cudaGetDevice(&prev);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "wt_rhs_curved_noalloc set-up (cudaGetDevice)");
@@ -2221,9 +2217,9 @@ int noalloc_scratch(wt_ctx* ctx, double** out) {
       cudaGetLastError();
       return cuda_fail(ctx, e, "wt_rhs_curved_noalloc set-up (cudaGetSymbolAddress)");
     }
-    g_noalloc_ptr[ctx->device] = (double*)p;
+    ctx->noalloc_scratch = (double*)p;
   }
-  *out = g_noalloc_ptr[ctx->device];
+  *out = ctx->noalloc_scratch;
   return 0;
 }
 
@@ -2246,8 +2242,9 @@ int wt_rhs_curved_noalloc(wt_ctx* ctx, const wt_coef* coef, const void* Phi, con
     return fail(ctx, WT_EINVAL, "wt_rhs_curved_noalloc: mesh has " + std::to_string(bnodes) +
                                     " boundary-face nodes; the fixed scratch array holds at most " +
                                     std::to_string(kNoallocBdryDoubles) + " (use wt_rhs_curved)");
-  if (eps_ko != 0.0 && !(mu > 0.0))
-    return fail(ctx, WT_EINVAL, "wt_rhs_curved_noalloc: mu must be positive when eps_ko != 0");
+  if (eps_ko != 0.0 && !(mu > 0.0 && std::isfinite(mu)))
+    return fail(ctx, WT_EINVAL, "wt_rhs_curved_noalloc: mu must be positive and finite when eps_ko != 0 "
+                                "(pass wt_workspace_mu of a workspace on the same mesh)");
   wt::ConsBC b;
   WT_TRY(make_bc(ctx, bc, use_metric, b));
   double* scratch = nullptr;

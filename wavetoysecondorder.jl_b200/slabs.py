@@ -164,6 +164,12 @@ class Slab:
             self.ws.set_mu(mu)
         self.Phi, self.Pi = self.mesh.zeros(), self.mesh.zeros()
         self.layer_nodes = M[0] * M[1] * N ** 3
+        # halo buffers, allocated on first use and reused by every exchange: one
+        # send buffer per packed layer, two receive buffers used in turn
+        # (an exchange posts at most two receives and completes them before it returns)
+        self._send = {}
+        self._recv = {}
+        self._recv_turn = {}
 
     def owned(self, field):
         """The owned layers of a local field (a view)."""
@@ -173,12 +179,31 @@ class Slab:
     def stage(self, dt: float, st: int, part: int, bc3d=None, metric: bool = True):
         wt.rk4_stage_curved(self.Phi, self.Pi, self.coef, self.ws, dt, st, part, bc3d=bc3d, metric=metric)
 
-    def empty(self):
+    def _new(self, kind: str):
         import torch
-        return torch.empty(wt.halo_size(self.ws), dtype=self.mesh.dtype, device=self.Phi.device)
+        n = wt.halo_size(self.ws) if kind == "flux" else 2 * self.rng.depth * self.layer_nodes
+        return torch.empty(n, dtype=self.mesh.dtype, device=self.Phi.device)
+
+    def _send_buf(self, kind: str, layer: int):
+        key = (kind, layer)
+        if key not in self._send:
+            self._send[key] = self._new(kind)
+        return self._send[key]
+
+    def _recv_buf(self, kind: str):
+        if kind not in self._recv:
+            self._recv[kind] = (self._new(kind), self._new(kind))
+            self._recv_turn[kind] = 0
+        t = self._recv_turn[kind]
+        self._recv_turn[kind] = t ^ 1
+        return self._recv[kind][t]
+
+    def empty(self):
+        """A receive buffer of the flux halo (one of two reused in turn)."""
+        return self._recv_buf("flux")
 
     def pack(self, st: int, layer: int):
-        buf = self.empty()
+        buf = self._send_buf("flux", layer)
         wt.halo_copy(self.ws, self.Phi, st, layer, buf, True)
         return buf
 
@@ -190,11 +215,11 @@ class Slab:
         wt.rk4_stage_curved_ko(self.Phi, self.Pi, self.coef, self.ws, dt, st, eps_KO, bc3d=bc3d, metric=metric)
 
     def empty_state(self):
-        import torch
-        return torch.empty(2 * self.rng.depth * self.layer_nodes, dtype=self.mesh.dtype, device=self.Phi.device)
+        """A receive buffer of the state halo (one of two reused in turn)."""
+        return self._recv_buf("state")
 
     def pack_state(self, st: int, layer: int):
-        buf = self.empty_state()
+        buf = self._send_buf("state", layer)
         wt.halo_state_copy(self.ws, self.Phi, self.Pi, st, layer, self.rng.depth, buf, True)
         return buf
 

@@ -838,8 +838,9 @@ def wave3d_curved_rhs_noalloc(Phidot, Pidot, Phi, Pi, coef: Coef, eps_KO: float 
     library shared by all calls: meshes above NOALLOC_MAX_NODES nodes or
     NOALLOC_MAX_BOUNDARY_NODES boundary-face nodes raise WaveToyError (code
     WT_EINVAL), and calls
-    that overlap on the GPU race.  mu (Workspace.mu) is needed only when
-    eps_KO != 0.  No counterpart in the reference."""
+    that overlap on the GPU race.  mu (Workspace.mu of a workspace on the
+    same mesh) is needed only when eps_KO != 0, and must then be positive and
+    finite.  No counterpart in the reference."""
     p, keep = _bcptr(bc3d)
     ctx = coef.mesh.ctx
     ctx.check(library().wt_rhs_curved_noalloc(ctx.h, coef.h, _ptr(Phi), _ptr(Pi), _ptr(Phidot), _ptr(Pidot),
