@@ -119,6 +119,12 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+def FP32_FORMS(wt):
+    """--fp32-form names of the FP32 precision forms."""
+    return {"comp": wt.FP32_COMPENSATED, "bf16x3": wt.FP32_BF16X3, "bf16x2": wt.FP32_BF16X2,
+            "cuda": wt.FP32_CUDA_CORES}
+
+
 def rank_seed(seed: int, rank: int) -> int:
     """Seed of rank `rank`'s independent solve (weak scaling: one solve per rank)."""
     return seed + 7919 * rank
@@ -236,7 +242,7 @@ def run_ours(args):
     M, N = args.elements, args.n
     mesh = wt.Mesh.warped_uniform_hex(ctx, N, M, 0.0, 1.0, 0.05, outer_tag=wt.SOMMERFELD_BDRY_TAG, precision=prec)
     if prec == wt.WT_F32:
-        mesh.set_fp32_form({"bf16x3": wt.FP32_BF16X3, "bf16x2": wt.FP32_BF16X2, "cuda": wt.FP32_CUDA_CORES}[args.fp32_form])
+        mesh.set_fp32_form(FP32_FORMS(wt)[args.fp32_form])
     seed = rank_seed(args.seed, rank)
     p = wt.workloads.adm_params(seed)
     coef = wt.sample_background3d(mesh, wt.BG_ADM_PERTURBED, p)
@@ -391,7 +397,7 @@ def run_slab(args):
     ctx = wt.Context(local)
     prec = wt.WT_F64 if args.precision == "f64" else wt.WT_F32
     M, N = args.elements, args.n
-    form = {"bf16x3": wt.FP32_BF16X3, "bf16x2": wt.FP32_BF16X2, "cuda": wt.FP32_CUDA_CORES}[args.fp32_form]
+    form = FP32_FORMS(wt)[args.fp32_form]
     # one slab per rank; on one GPU, --slabs slabs in this process (exchanged by device copies)
     nslabs = world if world > 1 else max(1, args.slabs)
     parts = S.partition(M, nslabs)
@@ -609,8 +615,8 @@ def main():
     ap.add_argument("--elements", type=int, default=64, help="elements per axis")
     ap.add_argument("--n", type=int, default=8, help="GLL nodes per axis")
     ap.add_argument("--precision", choices=["f64", "f32"], default="f64")
-    ap.add_argument("--fp32-form", choices=["bf16x3", "bf16x2", "cuda"], default="cuda",
-                    help="FP32 n=8 contractions: CUDA cores (FFMA, default) or split BF16 tensor cores "
+    ap.add_argument("--fp32-form", choices=["comp", "bf16x3", "bf16x2", "cuda"], default="comp",
+                    help="FP32 form: compensated (default; FP64 gradient of the compensated Phi), plain CUDA cores, or split BF16 tensor cores "
                          "(three / two terms)")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")

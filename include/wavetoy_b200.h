@@ -41,11 +41,23 @@ enum {
 };
 
 enum { WT_F64 = 0, WT_F32 = 1 };
-/* How an FP32 mesh evaluates the n = 8 derivative contractions (the precision
- * forms of the large-solve study; other n always use CUDA cores): FP32 on
- * CUDA cores (default), split-precision BF16 on tensor cores with three-term
- * operands (FP32 accuracy), or the same with two-term hi + lo operands. */
-enum { WT_FP32_CUDA_CORES = 0, WT_FP32_BF16X3 = 1, WT_FP32_BF16X2 = 2 };
+/* How an FP32 mesh steps (the precision forms of the large-solve study):
+ *   WT_FP32_COMPENSATED (default): FP32 storage of the state, the RK4 stages,
+ *     the coefficients, the metric terms and the flux; the state Phi is held
+ *     as a compensated pair (the caller's FP32 array plus a low part the
+ *     workspace keeps, as for Pi), every RK4 stage carries that low part, and
+ *     K1 evaluates the split-form gradient of Phi in FP64 (CUDA cores) with the
+ *     metric terms split into an element-constant FP64 part and an FP32
+ *     deviation.  Rounding Phi to FP32 is what limits the plain forms: it is
+ *     amplified by the second derivative in Pi-dot.  Applies to the RK4
+ *     stepping without Kreiss-Oliger dissipation (eps_KO = 0), all n; the
+ *     other FP32 paths (dissipative stages, Tsit5) run as WT_FP32_CUDA_CORES.
+ *   WT_FP32_CUDA_CORES: FP32 everywhere, FFMA contractions (n = 8 kernels).
+ *   WT_FP32_BF16X3 / WT_FP32_BF16X2: n = 8 contractions as split-precision
+ *     BF16 on tensor cores with three-term operands (FP32 accuracy) or two-term
+ *     hi + lo operands.
+ * Other n use the generic CUDA-core kernels (compensated for the default). */
+enum { WT_FP32_CUDA_CORES = 0, WT_FP32_BF16X3 = 1, WT_FP32_BF16X2 = 2, WT_FP32_COMPENSATED = 3 };
 enum { WT_BC_DIRICHLET = 1, WT_BC_SOMMERFELD = 2, WT_BC_EXCISION = 3, WT_BC_FULL_DIRICHLET = 4 };
 enum { WT_BG_MINKOWSKI = 0, WT_BG_CONSTANT_SHIFT = 1, WT_BG_ADM_PERTURBED = 2, WT_BG_RADIAL_SHIFT = 3,
        WT_BG_GAUGE_WAVE = 4, WT_BG_SINE_SHIFT = 5 };
@@ -186,12 +198,10 @@ int wt_mesh_set_bdry(wt_mesh* mesh, const int32_t* bdry);
  * initial data, min spacing, the strong form and reading those arrays return
  * WT_EINVAL.  No counterpart in the reference (Julia's GC owns its arrays). */
 int wt_mesh_release_setup_geometry(wt_mesh* mesh);
-/* Precision form of an FP32 mesh's n = 8 contractions (WT_FP32_*; default
- * WT_FP32_CUDA_CORES: FFMA contractions, exact FP32, the fastest form; the
- * split-BF16 tensor-core forms are kept for the precision study).  Switching
- * between the CUDA-core and the BF16 forms re-lays the mesh's metric blocks
- * (synchronous).  No counterpart in the reference (its T = Float32 path uses
- * one form). */
+/* Precision form of an FP32 mesh (WT_FP32_*; default WT_FP32_COMPENSATED).
+ * Switching between the CUDA-core and the BF16 forms re-lays the mesh's
+ * n = 8 metric blocks (synchronous).  No counterpart in the reference (its
+ * T = Float32 path uses one form). */
 int wt_mesh_set_fp32_form(wt_mesh* mesh, int form);
 /* _min_node_spacing_3d (src/evolve.jl:60-69); synchronous. */
 int wt_mesh_min_spacing(wt_mesh* mesh, double* h);
@@ -244,6 +254,21 @@ enum { WT_IC_EIGENMODE_CARTESIAN = 0, WT_IC_GAUSSIANS = 1, WT_IC_OUTGOING_PULSE 
  *   EIGENMODE_RADIAL eigenmode_radial! (src/wave.jl:207-226): p = A, R, n, cx, cy, cz */
 int wt_initial_data(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, int nparams, double t, void* u,
                     void* ut);
+
+/* wt_initial_data of (Phi, Pi) = (u, u_t) for the solve that ws steps,
+ * evaluated in FP64: an FP32 mesh's state then starts as the compensated
+ * FP64 values (the rounded values in Phi, Pi, the low parts in the workspace),
+ * as wt_state_set_f64 does.  Synchronous. */
+int wt_initial_state(wt_ctx* ctx, wt_ws* ws, int kind, const double* params, int nparams, double t, void* Phi,
+                     void* Pi);
+/* Load a Float64 state (device arrays) into the state arrays a solve steps:
+ * for an FP64 mesh a copy; for an FP32 mesh the FP32 arrays Phi, Pi get the
+ * rounded values and the workspace keeps the low parts the rounding lost
+ * (the compensated state that WT_FP32_COMPENSATED and the Kahan-compensated
+ * RK4 sums carry), so that stepping Phi, Pi with this workspace starts from
+ * the Float64 state itself.  Replaces the host-side Float64 -> T conversion
+ * before the reference's evolve loop (src/evolve.jl:1270); asynchronous. */
+int wt_state_set_f64(wt_ctx* ctx, wt_ws* ws, const double* Phi64, const double* Pi64, void* Phi, void* Pi);
 
 /* ---- workspace ---------------------------------------------------------------*/
 /* Replaces make_wave3d_workspace (src/wave3d_curved.jl:158-178): device

@@ -301,6 +301,7 @@ def test_ko_n8_warped_adm(wt, ctx, O, prec):
     Pg, Qg = dev(dt_, Phi), dev(dt_, Pi)
     wt.step_rk4_curved(Pg, Qg, cg, ws, dt, 20, eps_KO=0.1, bc3d=bcg, metric=True)
     Po, Qo = o.evolve_curved(co, Phi, Pi, dt, 20, eps_ko=0.1, bc=bco, use_metric=True)
+    assert np.abs(Po).max() < 3.0 and np.abs(Qo).max() < 100.0  # a bounded solution, not a blow-up
     tol = TOL64 if prec == 0 else TOL32
     assert rel(host(Pg), Po) < tol and rel(host(Qg), Qo) < tol, (rel(host(Pg), Po), rel(host(Qg), Qo))
     assert not ctx.nonfinite()

@@ -103,8 +103,10 @@ def test_slab_errors(wt, ctx):
     wt.halo_copy(ws, P, 0, 2, buf, True)
 
 
-@pytest.mark.parametrize("N,M,nslabs,periodic,prec", [(5, (2, 2, 14), 2, False, 0), (8, (2, 2, 14), 2, False, 0),
-                                                      (6, (2, 2, 21), 3, True, 0), (8, (2, 2, 14), 2, False, 1)])
+# cubic elements: mu (the KO normalisation) is estimated along axis 1, so elements
+# much thinner along z than along x would make mu^-5 D_z^6 too stiff for the step
+@pytest.mark.parametrize("N,M,nslabs,periodic,prec", [(5, (12, 12, 12), 2, False, 0), (8, (12, 12, 12), 2, False, 0),
+                                                      (6, (18, 18, 18), 3, True, 0), (8, (12, 12, 12), 2, False, 1)])
 def test_dissipative_slab_solve_equals_whole_mesh(wt, ctx, N, M, nslabs, periodic, prec):
     """Kreiss-Oliger dissipation on slabs: six ghost layers per cut (its z passes reach
     six elements), whole stages on each slab and a state halo after every stage, the
@@ -135,6 +137,7 @@ def test_dissipative_slab_solve_equals_whole_mesh(wt, ctx, N, M, nslabs, periodi
     S.step_ko(slabs, S.LocalStateHalo(slabs), dt, nsteps, eps, bc)
     Ps = torch.cat([s.owned(s.Phi) for s in slabs])
     Qs = torch.cat([s.owned(s.Pi) for s in slabs])
+    assert float(P.abs().max()) < 3.0 and float(Q.abs().max()) < 50.0   # a bounded solution, not a blow-up
     dP = float((Ps - P).abs().max()) / float(P.abs().max())
     dQ = float((Qs - Q).abs().max()) / float(Q.abs().max())
     tol = 1e-13 if prec == wt.WT_F64 else 1e-6

@@ -81,13 +81,15 @@ struct wt_ws {
   void* trace = nullptr;  // 6 N^2 Ne
   void* zero = nullptr;   // nn zeros
   void* Lu = nullptr;     // nn
-  // FP32 state: Kahan compensation of the RK4 step sums of Phi and Pi, kept
+  // FP32 state: the low parts the FP32 state arrays lost (the state is
+  // Phi + compP, Pi + compQ): Kahan compensation of the RK4 step sums, kept
   // while the caller keeps stepping the same state buffers
   void* compP = nullptr;
   void* compQ = nullptr;
   const void* comp_for[2] = {nullptr, nullptr};
   void* erk = nullptr;    // explicit RK stage slopes: 2 x 8 x nn (Phi slopes, then Pi slopes)
   long long flux_block = 0;  // values per element block of F as the last fused stage wrote it (halo copies)
+  int halo_cp = 0;        // the last fused stage ran the compensated FP32 form (its halo adds Phit)
 };
 
 namespace {
@@ -264,6 +266,12 @@ int derive_geometry(wt_mesh* mh) {
     WT_TRY(dalloc(mh->ctx, &m.Ja_n8, 9 * (size_t)wt::n8_padded_field_size(m.Ne) * rsize(m.precision), &mh->owned));
     WT_TRY(lrc(mh->ctx, wt::launch_pad_metric_n8(m, s), "padded metric terms"));
   }
+  if (m.precision == WT_F32) {  // the compensated form's split metric terms
+    WT_TRY(dalloc(mh->ctx, &m.Ja0, 9 * (size_t)m.Ne * sizeof(double), &mh->owned));
+    const size_t nd = m.N == 8 ? (size_t)wt::n8_padded_field_size(m.Ne) : (size_t)m.nn;
+    WT_TRY(dalloc(mh->ctx, &m.dJa, 9 * nd * sizeof(float), &mh->owned));
+    WT_TRY(lrc(mh->ctx, wt::launch_split_metric(m, s), "split metric terms"));
+  }
   WT_TRY(lrc(mh->ctx, wt::launch_boundary_normals(m, s), "boundary normals"));
   mh->ctx->launches += 6;
   cudaError_t e = cudaStreamSynchronize(s);
@@ -303,6 +311,7 @@ int ws_step_buffers(wt_ws* ws) {
   if (m.precision == WT_F32) {
     WT_TRY(ensure(ws, &ws->compP, nb));
     WT_TRY(ensure(ws, &ws->compQ, nb));
+    WT_TRY(ensure(ws, &ws->kP, nb));  // the compensated form's copy of Phi's high part (stage 2 -> 3)
   }
   return 0;
 }
@@ -842,12 +851,12 @@ int wt_mesh_set_bdry(wt_mesh* mh, const int32_t* bdry) {
 
 int wt_mesh_set_fp32_form(wt_mesh* mh, int form) {
   if (!mh) return WT_EINVAL;
-  if (form != WT_FP32_CUDA_CORES && form != WT_FP32_BF16X3 && form != WT_FP32_BF16X2)
+  if (form != WT_FP32_CUDA_CORES && form != WT_FP32_BF16X3 && form != WT_FP32_BF16X2 && form != WT_FP32_COMPENSATED)
     return fail(mh->ctx, WT_EINVAL, "unknown FP32 form " + std::to_string(form));
   wt::DevMesh& m = mh->m;
   m.fp32_form = form;
   // the FP32 CUDA-core n = 8 kernels read the metric terms in their own layout
-  const int want = m.precision == WT_F32 && form == WT_FP32_CUDA_CORES ? 1 : 0;
+  const int want = m.precision == WT_F32 && (form == WT_FP32_CUDA_CORES || form == WT_FP32_COMPENSATED) ? 1 : 0;
   if (m.N == 8 && m.Ja_n8 && m.ja_n8_layout != want) {
     WT_TRY(lrc(mh->ctx, wt::launch_pad_metric_n8(m, mh->ctx->stream), "n = 8 metric layout"));
     cudaError_t e = cudaStreamSynchronize(mh->ctx->stream);
@@ -1011,6 +1020,43 @@ int wt_initial_data(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, 
   return rc;
 }
 
+int wt_initial_state(wt_ctx* ctx, wt_ws* ws, int kind, const double* params, int nparams, double t, void* Phi,
+                     void* Pi) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_initial_state: NULL argument");
+  wt_mesh* mesh = ws->mesh;
+  if (mesh->m.precision == WT_F64) return wt_initial_data(ctx, mesh, kind, params, nparams, t, Phi, Pi);
+  if (kind < 0 || kind > 4) return fail(ctx, WT_EINVAL, "wt_initial_state: unknown kind");
+  if (nparams < 0 || nparams > 4096 || (nparams > 0 && !params))
+    return fail(ctx, WT_EINVAL, "wt_initial_state: bad parameters");
+  if (kind == WT_IC_GAUSSIANS && (nparams < 1 || 1 + 5 * (int)params[0] > nparams))
+    return fail(ctx, WT_EINVAL, "wt_initial_state: Gaussian count does not match the parameters");
+  WT_TRY(need_setup_geometry(mesh, "wt_initial_state"));
+  WT_TRY(ws_step_buffers(ws));
+  const long long nn = mesh->m.nn;
+  double *dp = nullptr, *tmp = nullptr;
+  WT_TRY(dalloc(ctx, &dp, (nparams > 0 ? nparams : 1) * sizeof(double), nullptr));
+  if (dalloc(ctx, &tmp, 2 * (size_t)nn * sizeof(double), nullptr)) {
+    cudaFree(dp);
+    return WT_ENOMEM;
+  }
+  if (nparams > 0) cudaMemcpyAsync(dp, params, nparams * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  int rc = lrc(ctx, wt::launch_initial(mesh->m, kind, dp, nparams, t, tmp, tmp + nn, ctx->stream, true),
+               "initial state");
+  if (!rc) rc = lrc(ctx, wt::launch_split_f64(nn, tmp, (float*)Phi, (float*)ws->compP, ctx->stream), "state split");
+  if (!rc) rc = lrc(ctx, wt::launch_split_f64(nn, tmp + nn, (float*)Pi, (float*)ws->compQ, ctx->stream), "state split");
+  ctx->launches += 3;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(dp);
+  cudaFree(tmp);
+  if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "initial state");
+  if (!rc) {
+    ws->comp_for[0] = Phi;
+    ws->comp_for[1] = Pi;
+  }
+  return rc;
+}
+
 // ---- workspace ---------------------------------------------------------------------
 int wt_workspace_create(wt_ctx* ctx, wt_mesh* mesh, wt_ws** out) {
   if (!ctx) return WT_EINVAL;
@@ -1048,6 +1094,24 @@ int wt_workspace_set_mu(wt_ws* ws, double mu) {
   ws->mu = mu;
   ws->inv_mu5 = std::pow(1.0 / mu, 5);
   ws->mu_done = true;
+  return 0;
+}
+
+int wt_state_set_f64(wt_ctx* ctx, wt_ws* ws, const double* Phi64, const double* Pi64, void* Phi, void* Pi) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!Phi64 || !Pi64 || !Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_state_set_f64: NULL argument");
+  const wt::DevMesh& m = ws->mesh->m;
+  if (m.precision == WT_F64) {
+    cudaMemcpyAsync(Phi, Phi64, (size_t)m.nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+    cudaError_t e = cudaMemcpyAsync(Pi, Pi64, (size_t)m.nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "wt_state_set_f64");
+  }
+  WT_TRY(ws_step_buffers(ws));
+  WT_TRY(lrc(ctx, wt::launch_split_f64(m.nn, Phi64, (float*)Phi, (float*)ws->compP, ctx->stream), "state split"));
+  WT_TRY(lrc(ctx, wt::launch_split_f64(m.nn, Pi64, (float*)Pi, (float*)ws->compQ, ctx->stream), "state split"));
+  ctx->launches += 2;
+  ws->comp_for[0] = Phi;  // the low parts belong to this state pair: stepping it keeps them
+  ws->comp_for[1] = Pi;
   return 0;
 }
 
@@ -1246,6 +1310,29 @@ static int coef_resample(wt_ctx* ctx, const wt_coef* coef, double toff, cudaStre
   return 0;
 }
 
+// The Phi side of fused RK4 stage st (eps_ko = 0).  Plain forms: K1 reads the
+// state at stage 0 and the previous stage's output after it.  Compensated FP32
+// form: K1 reads the state's high part (stage 3: the copy stage 2 made of it,
+// since stage 3 overwrites the state while neighbours still read it) plus a
+// small part -- the state's low part at stage 0, the previous stage's output
+// (low part + increment) after it.
+struct PhiStage {
+  const void* in;
+  const void* phit;
+  void* hcopy;
+};
+static PhiStage phi_stage(const wt_ws* ws, void* Phi, int st, bool cp) {
+  void* SP[2] = {ws->S0, ws->S1};
+  if (!cp) return {st == 0 ? Phi : SP[(st - 1) % 2], nullptr, nullptr};
+  return {st == 3 ? ws->kP : Phi, st == 0 ? ws->compP : SP[(st - 1) % 2], st == 2 ? ws->kP : nullptr};
+}
+
+// Whether the fused stages of this mesh run the compensated FP32 form: the
+// default FP32 form, through the kernels that implement it.
+static bool compensated(const wt::DevMesh& m, bool n8) {
+  return m.precision == WT_F32 && m.fp32_form == WT_FP32_COMPENSATED && (n8 || wt::cons_gen_cp_supported(m));
+}
+
 // One half of fused RK4 stage st (eps_ko = 0): part 1 launches K1 (flux, boundary
 // terms, the Phi stage update), part 2 K2 (divergence, the Pi stage update).
 static int rk4_stage_part(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int st,
@@ -1253,7 +1340,6 @@ static int rk4_stage_part(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi
   const wt::DevMesh& m = ws->mesh->m;
   cudaStream_t s = ctx->stream;
   void* SP[2] = {ws->S0, ws->S1};
-  const void* inP = st == 0 ? Phi : SP[(st - 1) % 2];
   const void* inQ = st == 0 ? Pi : ws->SQ;
   wt::RKStage rkP, rkQ;
   rkP.stage = rkQ.stage = st;
@@ -1262,7 +1348,13 @@ static int rk4_stage_part(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi
   rkQ.y = Pi; rkQ.acc = ws->accQ; rkQ.out = ws->SQ; rkQ.comp = ws->compQ;
   rkP.nonfinite = rkQ.nonfinite = st == 3 ? ctx->d_flag : nullptr;
   rkP.on = rkQ.on = 1;
-  const bool n8 = wt::cons_n8_path(m, coef->c, use_metric, b, rkP, rkQ, {inP, inQ, ws->F});
+  const bool n8 = wt::cons_n8_path(m, coef->c, use_metric, b, rkP, rkQ, {Phi, inQ, ws->F});
+  const bool cp = compensated(m, n8);  // its buffers (kP: the high-part copy) come with ws_step_buffers
+  const PhiStage ps = phi_stage(ws, Phi, st, cp);
+  const void* inP = ps.in;
+  rkP.phit = ps.phit;
+  rkP.hcopy = ps.hcopy;
+  ws->halo_cp = cp ? 1 : 0;
   ws->flux_block = n8 ? wt::n8_flux_block(m) : (long long)m.N * m.N * m.N;
   if (part == 1) {
     prof_mark(ctx, 0);
@@ -1539,7 +1631,7 @@ int wt_halo_size(const wt_ws* ws, long long* values) {
   const wt::DevMesh& m = ws->mesh->m;
   if (!ws->flux_block) return fail(ws->ctx, WT_EINVAL, "wt_halo_size: no fused stage has run on this workspace yet");
   const long long L = (long long)m.M[0] * m.M[1];
-  *values = L * ((long long)m.N * m.N * m.N + 3 * ws->flux_block);
+  *values = L * ((ws->halo_cp ? 2 : 1) * (long long)m.N * m.N * m.N + 3 * ws->flux_block);
   return 0;
 }
 
@@ -1552,16 +1644,24 @@ int wt_halo_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, void* 
   if (!ws->flux_block) return fail(ctx, WT_EINVAL, "wt_halo_copy: no fused stage has run on this workspace yet");
   const size_t es = rsize(m.precision);
   const long long L = (long long)m.M[0] * m.M[1], N3 = (long long)m.N * m.N * m.N, B = ws->flux_block;
-  // the Phi the next stage reads (the caller's Phi after stage 3), then the three flux components
-  char* phi = (char*)(stage < 3 ? (stage % 2 ? ws->S1 : ws->S0) : Phi);
-  char* seg[4] = {phi + (size_t)(layer * L * N3) * es, nullptr, nullptr, nullptr};
-  size_t len[4] = {(size_t)(L * N3) * es, 0, 0, 0};
+  // the Phi the next stage reads (the caller's Phi after stage 3) -- for the
+  // compensated FP32 form its high part and its small part -- then the three
+  // flux components
+  const PhiStage ps = phi_stage(ws, Phi, (stage + 1) % 4, ws->halo_cp != 0);
+  std::vector<char*> seg;
+  std::vector<size_t> len;
+  seg.push_back((char*)ps.in + (size_t)(layer * L * N3) * es);
+  len.push_back((size_t)(L * N3) * es);
+  if (ws->halo_cp) {
+    seg.push_back((char*)ps.phit + (size_t)(layer * L * N3) * es);
+    len.push_back((size_t)(L * N3) * es);
+  }
   for (int c = 0; c < 3; ++c) {
-    seg[1 + c] = (char*)ws->F + (size_t)(c * m.Ne * B + layer * L * B) * es;
-    len[1 + c] = (size_t)(L * B) * es;
+    seg.push_back((char*)ws->F + (size_t)(c * m.Ne * B + layer * L * B) * es);
+    len.push_back((size_t)(L * B) * es);
   }
   size_t off = 0;
-  for (int k = 0; k < 4; ++k) {
+  for (size_t k = 0; k < seg.size(); ++k) {
     char* b = (char*)buf + off;
     cudaError_t e = pack ? cudaMemcpyAsync(b, seg[k], len[k], cudaMemcpyDeviceToDevice, ctx->stream)
                          : cudaMemcpyAsync(seg[k], b, len[k], cudaMemcpyDeviceToDevice, ctx->stream);
@@ -1861,6 +1961,7 @@ struct wt_batch {
     void* Pi = nullptr;
     double dt = 0.0;
     wt::ConsBC bc;
+    bool cp = false;  // the member's stages run the compensated FP32 form
   };
   std::vector<Member> members;
   struct Group {
@@ -1905,7 +2006,8 @@ wt::SolveStage batch_stage(wt_batch* b, const wt_batch::Member& mb, int st) {
   ss.m = &ws->mesh->m;
   ss.c = &mb.coef->c;
   void* SP[2] = {ws->S0, ws->S1};
-  ss.Phi = st == 0 ? mb.Phi : SP[(st - 1) % 2];
+  const PhiStage ps = phi_stage(ws, mb.Phi, st, mb.cp);
+  ss.Phi = ps.in;
   ss.Pi = st == 0 ? mb.Pi : ws->SQ;
   ss.F = ws->F;
   ss.bbuf = ws->bbuf;
@@ -1914,6 +2016,7 @@ wt::SolveStage batch_stage(wt_batch* b, const wt_batch::Member& mb, int st) {
   ss.rkP.stage = ss.rkQ.stage = st;
   ss.rkP.dt = ss.rkQ.dt = mb.dt;
   ss.rkP.y = mb.Phi; ss.rkP.acc = ws->accP; ss.rkP.out = SP[st % 2]; ss.rkP.comp = ws->compP;
+  ss.rkP.phit = ps.phit; ss.rkP.hcopy = ps.hcopy;
   ss.rkQ.y = mb.Pi; ss.rkQ.acc = ws->accQ; ss.rkQ.out = ws->SQ; ss.rkQ.comp = ws->compQ;
   ss.rkP.nonfinite = ss.rkQ.nonfinite = st == 3 ? b->ctx->d_flag : nullptr;
   return ss;
@@ -1929,7 +2032,8 @@ int batch_launch(wt_batch* b, wt_batch::Group& g, int which, int st, cudaStream_
   }
   const size_t sz = which == 1 ? g.k1sz : g.k2sz;
   const char* d = (which == 1 ? g.d_k1 : g.d_k2) + st * ns * sz;
-  return wt::launch_cons_gen_batch(which, g.N, g.precision, g.epb_variant, d, g.d_tiles, g.ntiles, s);
+  const int cp = g.precision == WT_F32 && g.fp32_form == WT_FP32_COMPENSATED;
+  return wt::launch_cons_gen_batch(which, g.N, g.precision, g.epb_variant, cp, d, g.d_tiles, g.ntiles, s);
 }
 
 int batch_one_step(wt_batch* b, cudaStream_t s) {
@@ -1981,14 +2085,17 @@ int batch_rebuild(wt_batch* b) {
   for (int slot = 0; slot < (int)b->members.size(); ++slot) {
     const auto& mb = b->members[slot];
     if (!mb.active) continue;
+    auto& mbw = b->members[slot];
     const wt::DevMesh& m = mb.ws->mesh->m;
+    mbw.cp = false;
     const wt::SolveStage s0 = batch_stage(b, mb, 0);
     const bool n8 = wt::cons_n8_path(m, mb.coef->c, 1, mb.bc, s0.rkP, s0.rkQ,
                                      {mb.Phi, mb.Pi, mb.ws->F, mb.ws->S0, mb.ws->S1, mb.ws->SQ});
+    mbw.cp = compensated(m, n8);
     const int form = m.precision == WT_F32 ? m.fp32_form : 0;
     wt_batch::Group* g = nullptr;
     for (auto& x : b->groups)
-      if (x.N == m.N && x.precision == m.precision && x.n8 == n8 && (!n8 || x.fp32_form == form)) g = &x;
+      if (x.N == m.N && x.precision == m.precision && x.n8 == n8 && x.fp32_form == form) g = &x;
     if (!g) {
       b->groups.emplace_back();
       g = &b->groups.back();

@@ -19,6 +19,8 @@
 #include <vector>
 #include <initializer_list>
 
+#include "../../include/wavetoy_b200.h"
+
 #define WT_MAXN 8
 
 struct wt_ctx;  // the public context (include/wavetoy_b200.h)
@@ -37,7 +39,7 @@ struct DevMesh {
   int N = 0;
   long long Ne = 0, nn = 0;
   int precision = 0;   // 0 = double, 1 = float
-  int fp32_form = 0;   // FP32 meshes, n = 8: WT_FP32_* of include/wavetoy_b200.h (default CUDA cores)
+  int fp32_form = WT_FP32_COMPENSATED;  // FP32 meshes: WT_FP32_* of include/wavetoy_b200.h
   int ja_n8_layout = 0;  // layout Ja_n8 holds (0: Lay<real>, 1: LayC of the FP32 CUDA-core form)
   int affine = 1;      // 1 if every Jacobian is diagonal and constant per element
   int M[3] = {0, 0, 0};
@@ -67,6 +69,11 @@ struct DevMesh {
   void* invdetJ_r = nullptr;
   void* sdiag = nullptr;     // [3e + d] element-constant axis scale invjac[d,d] at node 0
   void* Ja_n8 = nullptr;     // n = 8: metric terms in the n8 element-block layout (FP64 512, FP32 544 words per element), state precision
+  // FP32 meshes (the compensated form's gradient): Ja split into an element-constant
+  // FP64 part Ja0 [9e + c] (the element's mean) and an FP32 deviation dJa
+  // (9 fields; n = 8: LayC element blocks, otherwise node order)
+  double* Ja0 = nullptr;
+  void* dJa = nullptr;
   // per element: bits 0-5 faces that get the centred-flux SAT (interior face with a
   // neighbour), bit 6 element has an outer face
   int32_t* emask = nullptr;
@@ -183,7 +190,7 @@ int launch_erk_combine(long long n, int precision, double dt, const void* y, voi
 int launch_coef_combine(const DevMesh& m, DevCoef& c, cudaStream_t s);
 int launch_min_spacing(const DevMesh& m, double* out, cudaStream_t s);
 int launch_initial(const DevMesh& m, int kind, const double* dparams, int np, double t, void* u, void* ut,
-                   cudaStream_t s);
+                   cudaStream_t s, bool f64 = false);  // f64: evaluate in FP64 whatever the mesh precision
 
 // conservative first-order system (wt_cons.cu)
 struct ConsBC {
@@ -209,6 +216,11 @@ struct RKStage {
   // (Kahan); with it, acc holds the step increment alone
   void* comp = nullptr;
   unsigned int* nonfinite = nullptr;  // set to 1 if the stage-3 update is not finite
+  // compensated FP32 form (WT_FP32_COMPENSATED): the small part K1 adds to its
+  // Phi input (the state's low part at stage 0, the previous stage's output
+  // after it), and the copy of the state's high part stage 2 writes for stage 3
+  const void* phit = nullptr;
+  void* hcopy = nullptr;
 };
 // K1: gradient, flux F, Phidot (+ affine/curv BC increments), optional RK epilogue for Phi.
 int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
@@ -224,6 +236,10 @@ int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
                       const RKStage& rk, unsigned* flag, cudaStream_t s);
 int launch_pad_metric_n8(DevMesh& m, cudaStream_t s);
+// FP32 meshes: m.Ja0 (element means of the FP64 metric terms) and m.dJa (FP32 deviations)
+int launch_split_metric(const DevMesh& m, cudaStream_t s);
+// whether the generic (any n) kernels run the compensated FP32 form on this mesh
+bool cons_gen_cp_supported(const DevMesh& m);
 // bounded-wait self-test (see k_wait_selftest)
 int launch_wait_selftest(long long polls, int arrive, unsigned* flag, cudaStream_t s);
 // the split-form gradient of Phi through the n = 8 kernels (3 fields of nn words into grad)
@@ -260,7 +276,7 @@ int launch_cons_n8_batch(int which, int precision, int fp32_form, const void* hP
 // per CTA, 1 = twice that (when it fits 1024 threads); chosen by the autotuner
 size_t cons_gen_param_size(int precision, int which);
 void cons_gen_fill_params(int which, const SolveStage& ss, unsigned* flag, void* dst);
-int launch_cons_gen_batch(int which, int N, int precision, int epb_variant, const void* plist, const int2* tiles,
+int launch_cons_gen_batch(int which, int N, int precision, int epb_variant, int cp, const void* plist, const int2* tiles,
                           long long ntiles, cudaStream_t s);
 // dst += koT * sum_d D_d^6 field; scratch (2 nn words, may be NULL when every
 // axis has straight element lines) serves meshes without them
@@ -289,6 +305,8 @@ int launch_scale(long long n, int precision, void* a, double s, cudaStream_t st)
 int launch_fill(long long n, int precision, void* a, double v, cudaStream_t st);
 int launch_copy(long long n, int precision, void* dst, const void* src, cudaStream_t st);
 int launch_gather(int precision, int count, const void* field, const int64_t* nodes, double* out, cudaStream_t s);
+// hi = (float)a, lo = (float)(a - hi)
+int launch_split_f64(long long n, const double* a, float* hi, float* lo, cudaStream_t st);
 int launch_rk_update(long long n, int precision, int stage, double dt, void* y, void* acc, void* out,
                      const void* k, cudaStream_t st, void* comp = nullptr);
 int launch_axpy(long long n, int precision, void* y, double a, const void* x, cudaStream_t st);

@@ -22,6 +22,7 @@
 #include "wt_common.cuh"
 
 #include <initializer_list>
+#include <type_traits>
 
 namespace wt {
 
@@ -70,13 +71,21 @@ struct K1P {
   real* out;
   real* comp;
   unsigned int* nonfinite;
+  // compensated FP32 form (CP instantiation): the Phi the stage reads is Phi +
+  // Phit (Phit: the state's low part at stage 0, the previous stage's small
+  // output after it; NULL = zero); Ja = Ja0 [9e + c] (FP64, element constant)
+  // + dJa (FP32, node order); stage 2 copies Phi into hcopy for stage 3
+  const real* Phit;
+  const real* dJa;
+  const double* Ja0;
+  real* hcopy;
 };
 
 // Low-storage classic RK4 stage update.  Without compensation acc holds
 // y + partial increments.  With compensation (FP32 state) acc holds the
-// increment of the step alone and the final y + increment is a Kahan sum whose
-// running error term lives in comp, so that small increments are not lost to
-// the rounding of y over many steps.
+// increment of the step alone and the final y + increment is a Kahan sum; comp
+// holds the low part the FP32 y lost (the state is y + comp), so that small
+// increments are not lost to the rounding of y over many steps.
 template <typename real>
 __device__ __forceinline__ void rk_epilogue(int stage, double dt, real k, real yin, real* y, real* acc, real* out,
                                             real* comp, long long n, unsigned int* nonfinite) {
@@ -93,9 +102,9 @@ __device__ __forceinline__ void rk_epilogue(int stage, double dt, real k, real y
     } else {
       const real inc = acc[n] + (real)(dt / 6.0) * k;
       const real yv = y[n];
-      const real t = inc - comp[n];
+      const real t = inc + comp[n];
       const real v = yv + t;
-      comp[n] = (v - yv) - t;
+      comp[n] = t - (v - yv);
       y[n] = v;
       if (nonfinite && !isfinite((double)v)) atomicOr(nonfinite, 1u);
     }
@@ -114,6 +123,34 @@ __device__ __forceinline__ void rk_epilogue(int stage, double dt, real k, real y
     real v = acc[n] + (real)(dt / 6.0) * k;
     y[n] = v;
     if (nonfinite && !isfinite((double)v)) atomicOr(nonfinite, 1u);
+  }
+}
+
+// RK4 stage update of the compensated FP32 form (the Phi side, K1): the state
+// is (y, comp) = (high, low part) and the stage the next K1 reads is its high
+// part plus out = low part + c dt k; the step's final sum is formed in FP64 and
+// split again.  hi: this node's high part of the state (the K1 input).
+__device__ __forceinline__ void rk_epilogue_cp(int stage, double dt, float k, float hi, float* y, float* acc,
+                                               float* out, float* comp, float* hcopy, long long n,
+                                               unsigned int* nonfinite) {
+  const float lo = comp[n];
+  if (stage == 0) {
+    out[n] = lo + (float)(0.5 * dt) * k;
+    acc[n] = (float)(dt / 6.0) * k;
+  } else if (stage == 1) {
+    out[n] = lo + (float)(0.5 * dt) * k;
+    acc[n] = acc[n] + (float)(dt / 3.0) * k;
+  } else if (stage == 2) {
+    out[n] = lo + (float)dt * k;
+    acc[n] = acc[n] + (float)(dt / 3.0) * k;
+    hcopy[n] = hi;
+  } else {
+    const float inc = acc[n] + (float)(dt / 6.0) * k;
+    const double v = (double)hi + ((double)lo + (double)inc);
+    const float h = (float)v;
+    y[n] = h;
+    comp[n] = (float)(v - (double)h);
+    if (nonfinite && !isfinite(h)) atomicOr(nonfinite, 1u);
   }
 }
 
@@ -138,14 +175,17 @@ __device__ __forceinline__ real contract(const real* __restrict__ f, const real*
 // BATCH: the CTA's elements come from a work list of (solve, element) tiles
 // and each tile reads the parameter block of its solve (plist); otherwise
 // element blockIdx.x * EPB + le of the single solve P0.  EPB_: elements per CTA.
-template <int N, typename real, bool CURV, bool BATCH, int EPB_>
+// CP (real = float): the compensated form -- the Phi the stage reads (high
+// plus small part) and the split-form gradient of it in FP64.
+template <int N, typename real, bool CURV, bool BATCH, int EPB_, bool CP = false>
 __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0, const K1P<real>* __restrict__ plist,
                                                             const int2* __restrict__ tiles, long long ntiles) {
   constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = EPB_;
-  __shared__ real GT[N2];
-  __shared__ real su[EPB][N3];
-  __shared__ real sun[EPB][6][N2];
-  __shared__ real sw[CURV ? EPB : 1][CURV ? 9 : 1][CURV ? N3 : 1];
+  using gt = typename std::conditional<CP, double, real>::type;  // precision of the gradient
+  __shared__ gt GT[N2];
+  __shared__ gt su[EPB][N3];
+  __shared__ gt sun[EPB][6][N2];
+  __shared__ gt sw[CURV ? EPB : 1][CURV ? 9 : 1][CURV ? N3 : 1];
   const int tid = threadIdx.x;
   const int le = tid / N3, t = tid - le * N3;
   const int i = t % N, j = (t / N) % N, k = t / N2;
@@ -166,18 +206,26 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
   const long long ec = valid ? e : 0;  // clamp for address arithmetic
   const long long n = ec * N3 + t;
   const long long nn = P.nn;
-  if (tid < N2) GT[(tid % N) * N + tid / N] = (real)P.G[tid];
-  const real u = valid ? P.Phi[n] : (real)0;
-  su[le][t] = u;
+  if (tid < N2) GT[(tid % N) * N + tid / N] = (gt)P.G[tid];
+  const real u = valid ? P.Phi[n] : (real)0;  // CP: the high part
+  gt ug = u;                                   // the value the gradient differentiates
+  if constexpr (CP) {
+    if (valid && P.Phit) ug += (gt)P.Phit[n];
+  }
+  su[le][t] = ug;
   // element tables: SAT mask / outer-face flag, and the neighbour face sources
   const int emask = valid ? P.emask[ec] : 0;
   // neighbour Phi face traces
   for (int idx = t; idx < 6 * N2; idx += N3) {
     const int f = idx / N2, pq = idx - f * N2;
-    real v = 0;
+    gt v = 0;
     if ((emask >> f) & 1) {
       const int src = P.fsrc[f + 6 * ec];
-      v = P.Phi[(long long)(src >> 6) * N3 + nbr_face_node(src, pq % N, pq / N, N)];
+      const long long nb = (long long)(src >> 6) * N3 + nbr_face_node(src, pq % N, pq / N, N);
+      v = P.Phi[nb];
+      if constexpr (CP) {
+        if (P.Phit) v += (gt)P.Phit[nb];
+      }
     }
     sun[le][f][pq] = v;
   }
@@ -191,38 +239,43 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
     for (int c = 0; c < 6; ++c) K[c] = P.c10[(4 + c) * nn + n];
     Pi = P.Pi[n];
   }
-  real m[CURV ? 9 : 1];
+  gt m[CURV ? 9 : 1];
   real invJ = 0, sd[3];
   if (CURV) {
 #pragma unroll
-    for (int c = 0; c < 9; ++c) m[c] = valid ? P.Ja[c * nn + n] : (real)0;
+    for (int c = 0; c < 9; ++c) {
+      if constexpr (CP)
+        m[c] = valid ? P.Ja0[9 * ec + c] + (gt)P.dJa[c * nn + n] : (gt)0;
+      else
+        m[c] = valid ? P.Ja[c * nn + n] : (real)0;
+    }
     invJ = valid ? P.invdetJ[n] : (real)0;
   } else {
 #pragma unroll
     for (int d = 0; d < 3; ++d) sd[d] = P.sdiag[3 * ec + d];
   }
-  const real Hend = (real)P.H[0];
+  const gt Hend = (gt)P.H[0];
   if (CURV) {
 #pragma unroll
-    for (int c = 0; c < 9; ++c) sw[le][c][t] = m[c] * u;
+    for (int c = 0; c < 9; ++c) sw[le][c][t] = m[c] * ug;
   }
   __syncthreads();
-  real du[3];
+  gt du[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) du[d] = contract<N>(su[le], GT, i, j, k, d);
-  real g[3];
+  gt gg[3];
   if (CURV) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      real acc = 0;
+      gt acc = 0;
 #pragma unroll
       for (int al = 0; al < 3; ++al)
-        acc += (real)0.5 * contract<N>(sw[le][al * 3 + c], GT, i, j, k, al) + (real)0.5 * m[al * 3 + c] * du[al];
-      g[c] = acc;
+        acc += (gt)0.5 * contract<N>(sw[le][al * 3 + c], GT, i, j, k, al) + (gt)0.5 * m[al * 3 + c] * du[al];
+      gg[c] = acc;
     }
   } else {
 #pragma unroll
-    for (int d = 0; d < 3; ++d) g[d] = sd[d] * du[d];
+    for (int d = 0; d < 3; ++d) gg[d] = (gt)sd[d] * du[d];
   }
   // centred-flux SAT on interior faces through this node
   if (valid) {
@@ -233,20 +286,21 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
       if (idx3[ax] != frow(f, N)) continue;
       if (!((emask >> f) & 1)) continue;
       const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
-      const real jump = sun[le][f][p + N * q] - u;
-      const real nh = (f & 1) ? (real)1 : (real)-1;
+      const gt jump = sun[le][f][p + N * q] - ug;
+      const gt nh = (f & 1) ? (gt)1 : (gt)-1;
       if (CURV) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) g[c] += nh * m[ax * 3 + c] * jump / ((real)2 * Hend);
+        for (int c = 0; c < 3; ++c) gg[c] += nh * m[ax * 3 + c] * jump / ((gt)2 * Hend);
       } else {
-        g[ax] += nh * sd[ax] / ((real)2 * Hend) * jump;
+        gg[ax] += nh * (gt)sd[ax] / ((gt)2 * Hend) * jump;
       }
     }
   }
   if (CURV) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) g[c] *= invJ;
+    for (int c = 0; c < 3; ++c) gg[c] *= (gt)invJ;
   }
+  const real g[3] = {(real)gg[0], (real)gg[1], (real)gg[2]};
   if (!valid) return;
   if (P.grad_out) {
 #pragma unroll
@@ -281,7 +335,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
           if (kind == 4) {
             const real tau = P.sigma * (fabs(a_n - bax) + fabs(a_n + bax)) * wt;
             const real gp = P.gPhi ? P.gPhi[n] : (real)0, gq = P.gPi ? P.gPi[n] : (real)0;
-            dF = -tau * (u - gp);
+            dF = -tau * ((real)ug - gp);
             dP = -tau * (Pi - gq);
           } else {
             const real qv = nh * g[ax];
@@ -302,7 +356,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
         if (kind == 4) {
           const real tau = P.sigma * (fabs(a_n - bn) + fabs(a_n + bn)) * wt;
           const real gp = P.gPhi ? P.gPhi[n] : (real)0, gq = P.gPi ? P.gPi[n] : (real)0;
-          dF = -tau * (u - gp);
+          dF = -tau * ((real)ug - gp);
           dP = -tau * (Pi - gq);
         } else {
           const real qv = nx * g[0] + ny * g[1] + nz * g[2];
@@ -324,10 +378,17 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
   P.F[n] = F0;
   P.F[nn + n] = F1;
   P.F[2 * nn + n] = F2;
-  if (P.epi)
-    rk_epilogue<real>(P.stage, P.dt, phid, u, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
-  else
-    P.Phidot[n] = phid;
+  if constexpr (CP) {
+    if (P.epi)
+      rk_epilogue_cp(P.stage, P.dt, phid, u, P.y, P.acc, P.out, P.comp, P.hcopy, n, P.nonfinite);
+    else
+      P.Phidot[n] = phid;
+  } else {
+    if (P.epi)
+      rk_epilogue<real>(P.stage, P.dt, phid, u, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
+    else
+      P.Phidot[n] = phid;
+  }
 }
 
 template <typename real>
@@ -605,7 +666,14 @@ static K1P<real> k1p_params(const DevMesh& m, const DevCoef& c, const void* Phi,
   P.gDx = (const real*)bc.gDx; P.gDy = (const real*)bc.gDy; P.gDz = (const real*)bc.gDz;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.nonfinite = rk.nonfinite;
+  P.Phit = (const real*)rk.phit; P.dJa = (const real*)m.dJa; P.Ja0 = m.Ja0; P.hcopy = (real*)rk.hcopy;
   return P;
+}
+
+// the generic K1 runs the compensated instantiation for the default FP32 form
+// (not for the gradient-only launches of the energy)
+static bool gen_cp(const DevMesh& m, const void* grad_out) {
+  return m.precision == WT_F32 && m.fp32_form == WT_FP32_COMPENSATED && grad_out == nullptr && m.Ja0 && m.dJa;
 }
 
 template <typename real>
@@ -633,10 +701,17 @@ static int k1_dispatch(const DevMesh& m, const DevCoef& c, const void* Phi, cons
                        cudaStream_t s) {
   const K1P<real> P = k1p_params<real>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, bc, rk);
   const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
-  if (use_metric)
+  constexpr bool F32 = std::is_same<real, float>::value;
+  if (F32 && gen_cp(m, grad_out)) {
+    if (use_metric)
+      k_cons_k1<N, real, true, false, Ep<N>::EPB, F32><<<blocks, Ep<N>::T, 0, s>>>(P, nullptr, nullptr, 0);
+    else
+      k_cons_k1<N, real, false, false, Ep<N>::EPB, F32><<<blocks, Ep<N>::T, 0, s>>>(P, nullptr, nullptr, 0);
+  } else if (use_metric) {
     k_cons_k1<N, real, true, false, Ep<N>::EPB><<<blocks, Ep<N>::T, 0, s>>>(P, nullptr, nullptr, 0);
-  else
+  } else {
     k_cons_k1<N, real, false, false, Ep<N>::EPB><<<blocks, Ep<N>::T, 0, s>>>(P, nullptr, nullptr, 0);
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -664,10 +739,14 @@ struct EpAlt {
 };
 
 template <int N, typename real, int EPB>
-static int gen_batch(int which, const void* plist, const int2* tiles, long long ntiles, cudaStream_t s) {
+static int gen_batch(int which, bool cp, const void* plist, const int2* tiles, long long ntiles, cudaStream_t s) {
   const unsigned blocks = (unsigned)((ntiles + EPB - 1) / EPB);
   if (blocks == 0) return 0;
-  if (which == 1)
+  constexpr bool F32 = std::is_same<real, float>::value;
+  if (which == 1 && F32 && cp)
+    k_cons_k1<N, real, true, true, EPB, F32><<<blocks, Ep<N>::N3 * EPB, 0, s>>>(K1P<real>(), (const K1P<real>*)plist,
+                                                                               tiles, ntiles);
+  else if (which == 1)
     k_cons_k1<N, real, true, true, EPB><<<blocks, Ep<N>::N3 * EPB, 0, s>>>(K1P<real>(), (const K1P<real>*)plist, tiles,
                                                                           ntiles);
   else
@@ -677,13 +756,13 @@ static int gen_batch(int which, const void* plist, const int2* tiles, long long 
 }
 
 template <int N>
-static int gen_batch_n(int which, int precision, int variant, const void* plist, const int2* tiles, long long ntiles,
-                       cudaStream_t s) {
+static int gen_batch_n(int which, int precision, int variant, bool cp, const void* plist, const int2* tiles,
+                       long long ntiles, cudaStream_t s) {
   if (precision == 0)
-    return variant ? gen_batch<N, double, EpAlt<N>::V1>(which, plist, tiles, ntiles, s)
-                   : gen_batch<N, double, Ep<N>::EPB>(which, plist, tiles, ntiles, s);
-  return variant ? gen_batch<N, float, EpAlt<N>::V1>(which, plist, tiles, ntiles, s)
-                 : gen_batch<N, float, Ep<N>::EPB>(which, plist, tiles, ntiles, s);
+    return variant ? gen_batch<N, double, EpAlt<N>::V1>(which, false, plist, tiles, ntiles, s)
+                   : gen_batch<N, double, Ep<N>::EPB>(which, false, plist, tiles, ntiles, s);
+  return variant ? gen_batch<N, float, EpAlt<N>::V1>(which, cp, plist, tiles, ntiles, s)
+                 : gen_batch<N, float, Ep<N>::EPB>(which, cp, plist, tiles, ntiles, s);
 }
 
 size_t cons_gen_param_size(int precision, int which) {
@@ -733,6 +812,8 @@ bool cons_n8_path(const DevMesh& m, const DevCoef& c, int use_metric, const Cons
     if (!a16(p)) return false;
   return a16(c.c10) && a16(m.invdetJ_r);
 }
+
+bool cons_gen_cp_supported(const DevMesh& m) { return gen_cp(m, nullptr); }
 
 int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
                    void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
@@ -829,9 +910,9 @@ int launch_ko_add(const DevMesh& m, void* dst, const void* field, double koT, cu
   }
 }
 
-int launch_cons_gen_batch(int which, int N, int precision, int epb_variant, const void* plist, const int2* tiles,
+int launch_cons_gen_batch(int which, int N, int precision, int epb_variant, int cp, const void* plist, const int2* tiles,
                           long long ntiles, cudaStream_t s) {
-  WT_DISPATCH_N(N, (gen_batch_n<NN>(which, precision, epb_variant, plist, tiles, ntiles, s)));
+  WT_DISPATCH_N(N, (gen_batch_n<NN>(which, precision, epb_variant, cp != 0, plist, tiles, ntiles, s)));
 }
 
 }  // namespace wt

@@ -242,7 +242,8 @@ struct StageCoef {
 
 // RK4 stage update shared by both kernels (see rk_epilogue in wt_cons.cu):
 // with comp (FP32 state) acc holds the step increment and the final sum is
-// Kahan-compensated; yv, accv, compv are this node's prefetched values.
+// Kahan-compensated, comp holding the low part the FP32 state lost (the state
+// is y + comp); yv, accv, compv are this node's prefetched values.
 template <typename real>
 __device__ __forceinline__ void n8_rk(int stage, double dt, real k, real yin, real yv, real accv, real compv,
                                       long long n, real* y, real* acc, real* out, real* comp, unsigned* flag) {
@@ -258,9 +259,9 @@ __device__ __forceinline__ void n8_rk(int stage, double dt, real k, real yin, re
       acc[n] = accv + (real)(dt / 3.0) * k;
     } else {
       const real inc = accv + (real)(dt / 6.0) * k;
-      const real t = inc - compv;
+      const real t = inc + compv;
       const real v = yv + t;
-      comp[n] = (v - yv) - t;
+      comp[n] = t - (v - yv);
       y[n] = v;
       if (flag && !isfinite(v)) atomicOr(flag, 1u);
     }
@@ -279,6 +280,35 @@ __device__ __forceinline__ void n8_rk(int stage, double dt, real k, real yin, re
     const real v = accv + (real)(dt / 6.0) * k;
     y[n] = v;
     if (flag && !isfinite(v)) atomicOr(flag, 1u);
+  }
+}
+
+// RK4 stage update of the compensated FP32 form (Phi in K1, CP): the state is
+// the pair (y, lo) = (high, low part); the stage the next K1 reads is y + out
+// with out = lo + c dt k, so the stage value keeps the state's low part and
+// rounds only the small increment; acc holds the step increment; the step's
+// final sum is formed in FP64 and split again into y and lo.  Stage 2 also
+// copies y into hcopy, which stage 3 reads in place of y.  hi, accv, lov:
+// this node's y, acc and lo.
+__device__ __forceinline__ void n8_rk_cp(int stage, double dt, float k, float hi, float accv, float lov, long long n,
+                                         float* y, float* acc, float* out, float* lo, float* hcopy, unsigned* flag) {
+  if (stage == 0) {
+    out[n] = lov + (float)(0.5 * dt) * k;
+    acc[n] = (float)(dt / 6.0) * k;
+  } else if (stage == 1) {
+    out[n] = lov + (float)(0.5 * dt) * k;
+    acc[n] = accv + (float)(dt / 3.0) * k;
+  } else if (stage == 2) {
+    out[n] = lov + (float)dt * k;
+    acc[n] = accv + (float)(dt / 3.0) * k;
+    hcopy[n] = hi;
+  } else {
+    const float inc = accv + (float)(dt / 6.0) * k;
+    const double v = (double)hi + ((double)lov + (double)inc);
+    const float h = (float)v;
+    y[n] = h;
+    lo[n] = (float)(v - (double)h);
+    if (flag && !isfinite(h)) atomicOr(flag, 1u);
   }
 }
 
@@ -319,6 +349,19 @@ struct K1N8 {
   unsigned* flag;
   float Gh[64];  // 0.5 G in FP32 (the CUDA-core form reads it from the constant bank)
   real* gout;    // gradient-only launches (GR): the three components of the split-form gradient
+  // Compensated FP32 form (cp = 1, CUDA-core kernels): the Phi the stage reads is
+  // Phi + Phit, with Phit the low part of the state at stage 0 and the previous
+  // stage's small output after it (NULL: zero); the split-form gradient of it is
+  // evaluated in FP64 with the metric terms split into an element-constant FP64
+  // part Ja0 [9e + al*3 + c] and an FP32 deviation dJa (LayC blocks).
+  // Stage 3 reads a copy of the state's high part that stage 2 writes (hcopy),
+  // so that stage 3 may overwrite the state while neighbours still read it.
+  int cp;
+  const real* Phit;
+  const real* dJa;
+  const double* Ja0;
+  real* hcopy;
+  double Gd[64];  // 0.5 G in FP64
 };
 
 // Boundary terms of K1 at a node on an outer face (the curvilinear boundary
@@ -1135,20 +1178,29 @@ __device__ __forceinline__ void contract8(const float* G, const float v[8], floa
 // each single-buffered and bulk-copied as soon as the pass that reads it is done,
 // so that three CTAs fit on an SM.
 constexpr size_t K1C_STAGE = 9 * (size_t)n8::LayC::FS;
-constexpr size_t K1C_B = 15 * (size_t)n8::N3;
+// node-pass buffer: c10 (10), Pi, invJ, [y], acc, comp -- the compensated form
+// reads the state's high part from the Phi pencils and holds no y
+template <bool CP>
+constexpr size_t k1c_b() { return (CP ? 14 : 15) * (size_t)n8::N3; }
 constexpr size_t K2C_STAGE = (size_t)K2_NF * n8::LayC::FS;
 constexpr int K1C_OCC = 3, K2C_OCC = 3;
 constexpr int K2C_NS = 2;  // K2c flux + Ja stages (one stage at four CTAs per SM leaves 80 registers: spills)
+template <bool CP = false>
 constexpr size_t k1c_smem() {
-  return (K1C_STAGE + K1C_B + 9 * n8::LayC::FS + 2 * 6 * n8::N2 + 2 * n8::N3) * sizeof(float) + 64;
+  // CP adds one (single-buffered) copy of the small parts Phit: pencils and face traces
+  return (K1C_STAGE + k1c_b<CP>() + 9 * n8::LayC::FS + 2 * 6 * n8::N2 + 2 * n8::N3 +
+          (CP ? 6 * n8::N2 + n8::N3 : 0)) * sizeof(float) + 64;
 }
+static_assert(3 * (k1c_smem<true>() + 1024) <= 233472, "three compensated K1c CTAs must fit an SM");
 // K2c node-pass fields (1/J and the RK state: invJ, y, acc, comp), one bulk-copied buffer
 constexpr size_t K2C_B = 4 * (size_t)n8::N3;
 constexpr size_t k2c_smem() {
   return (K2C_NS * K2C_STAGE + 3 * n8::LayC::FS + 2 * 6 * 3 * n8::N2 + K2C_B) * sizeof(float) + 64;
 }
 
-template <bool BATCH, bool GR = false>  // GR: gradient only (see k_cons_k1_n8)
+// CP: the compensated FP32 form (see K1N8::cp): Phi + Phit in FP64 through the
+// contractions, the RK4 epilogue of n8_rk_cp.
+template <bool BATCH, bool GR = false, bool CP = false>  // GR: gradient only (see k_cons_k1_n8)
 __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
     k_cons_k1_n8c(const __grid_constant__ K1N8<float> P, const K1N8<float>* __restrict__ plist,
                   const int2* __restrict__ tiles, long long ntiles) {
@@ -1158,24 +1210,30 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
   constexpr int NPT = (N3 + THR - 1) / THR;   // node slots per thread (3, the last one partly)
   constexpr int NFT = 6 * N2;                 // 384 neighbour Phi face values
   constexpr int NFR = (NFT + THR - 1) / THR;  // 2 per thread
+  // node-pass buffer fields (sB)
+  constexpr int IY = 12, IACC = CP ? 12 : 13, ICOMP = CP ? 13 : 14;
   extern __shared__ __align__(128) unsigned char smraw[];
   real* sJa = reinterpret_cast<real*>(smraw);  // 9 fields (LayC), index al*3 + c
-  real* sB = sJa + K1C_STAGE;                  // node order: c10 (10), Pi, invJ, y, acc, comp
-  real* sg = sB + K1C_B;                       // 9 partial gradients [al*3 + c] (LayC)
+  real* sB = sJa + K1C_STAGE;                  // node order: c10 (10), Pi, invJ, [y], acc, comp
+  real* sg = sB + k1c_b<CP>();                 // 9 partial gradients [al*3 + c] (LayC)
   real* sface = sg + 9 * FSC;                  // 2 x 384
   real* sphi = sface + 2 * NFT;                // 2 x 512 (LayC)
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sphi + 2 * N3);  // [0] Ja stage, [1] sB
+  real* sfaceT = sphi + 2 * N3;                // CP: 384 small parts of the face traces
+  real* sphiT = sfaceT + (CP ? NFT : 0);       // CP: 512 small parts (LayC)
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sphiT + (CP ? N3 : 0));  // [0] Ja stage, [1] sB
   __shared__ int abort_flag;
   __shared__ short ftab[6 * N2];  // node of face-trace point pq on face fn of an element block
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int al = tid >> 6, pc = tid & 63;  // contraction: axis (warp-uniform) and pencil
   const real inv2H = (real)(1.0 / (2.0 * P.H[0]));
   const bool comp_on = P.epi && P.comp != nullptr;
-  const bool need_y = P.epi && (P.stage == 1 || P.stage == 2 || (comp_on && P.stage == 3));
+  // the compensated form reads the state's high part from the Phi pencils and the low part at every stage
+  const bool need_y = !CP && P.epi && (P.stage == 1 || P.stage == 2 || (comp_on && P.stage == 3));
   const bool need_acc = P.epi && P.stage >= 1;
-  const bool need_comp = comp_on && P.stage == 3;
+  const bool need_comp = comp_on && (CP || P.stage == 3);
   const unsigned txA = (unsigned)(K1C_STAGE * sizeof(real));
   const unsigned txB = (unsigned)((GR ? 1 : 12 + need_y + need_acc + need_comp) * N3 * sizeof(real));
+  const double inv2Hd = 1.0 / (2.0 * P.H[0]);
   const long long T = BATCH ? ntiles : P.Ne;
   const long long GS = gridDim.x;
   auto tile_at = [&](long long t) -> int2 {
@@ -1209,8 +1267,9 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
       mbar_expect_tx(&bar[0], txA);
     }
     __syncwarp();
+    const real* ja = CP ? Q.dJa : Q.Ja;
     if (lane < 9)
-      bulk_g2s(sJa + lane * FSC, Q.Ja + ((long long)lane * Q.Ne + tl.y) * FSC, FSC * (unsigned)sizeof(real), &bar[0]);
+      bulk_g2s(sJa + lane * FSC, ja + ((long long)lane * Q.Ne + tl.y) * FSC, FSC * (unsigned)sizeof(real), &bar[0]);
   };
   auto issueB = [&](int2 tl) {
     const K1N8<real>& Q = prm(tl.x);
@@ -1227,9 +1286,9 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
     } else if (lane < 10) src = Q.c10 + lane * Q.nn + o;
     else if (lane == 10) src = Q.Pi + o;
     else if (lane == 11) src = Q.invdetJ + o;
-    else if (lane == 12 && need_y) src = Q.y + o;
-    else if (lane == 13 && need_acc) src = Q.acc + o;
-    else if (lane == 14 && need_comp) src = Q.comp + o;
+    else if (lane == IY && !CP && need_y) src = Q.y + o;
+    else if (lane == IACC && need_acc) src = Q.acc + o;
+    else if (lane == ICOMP && need_comp) src = Q.comp + o;
     if (src) bulk_g2s(sB + lane * N3, src, nb, &bar[1]);
   };
   // face-trace slot r of this thread: value tid + r * THR = (face, pq) of the 384
@@ -1259,6 +1318,27 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
       if (node < N3) cp_async4(sphi + b * N3 + LayC::at(node), Q.Phi + (long long)tl.y * N3 + node, true);
     }
   };
+  // CP: the small parts Phit of the same values into the single buffers sfaceT, sphiT
+  // (zero-filled where there is no neighbour or no Phit)
+  auto async_loadT = [&](int2 tl, const int src[NFR]) {
+    const K1N8<real>& Q = prm(tl.x);
+    const bool have = Q.Phit != nullptr;
+    const real* base = have ? Q.Phit : Q.Phi;
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = tid + r * THR;
+      if (idx < NFT) {
+        const bool ok = have && src[r] >= 0;
+        const real* g = ok ? base + (long long)(src[r] >> 6) * N3 + ftab[face_slot(src[r], idx & 63)] : base;
+        cp_async4(sfaceT + idx, g, ok);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < NPT; ++r) {
+      const int node = tid + r * THR;
+      if (node < N3) cp_async4(sphiT + LayC::at(node), base + (long long)tl.y * N3 + node, have);
+    }
+  };
   auto emask_at = [&](int2 tl) -> int { return tl.x >= 0 ? prm(tl.x).emask[tl.y] : 0; };
 
   int2 t0 = tile_at(blockIdx.x), t1 = tile_at(blockIdx.x + GS), t2 = tile_at(blockIdx.x + 2 * GS);
@@ -1271,6 +1351,7 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
     int src0[NFR];
     src_load(t0, src0);
     async_load(t0, src0, 0);
+    if constexpr (CP) async_loadT(t0, src0);
     src_load(t1, src1);
     cp_async_wait_all();
   }
@@ -1305,7 +1386,58 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
     const int bnd = emcur >> 6;
     // ---- contractions: thread (al, pc); the operator in the constant bank is
     // 0.5 G (scaling by 1/2 is exact) ----
-    {
+    if constexpr (CP) {
+      // The state u = Phi + Phit enters the derivative in FP64: FP32 rounding of
+      // it, or of the contraction of it, would be amplified by the second
+      // derivative in Pi-dot.  With Ja = Ja0 + dJa (Ja0 element-constant, FP64):
+      //   0.5 D(Ja u) = Ja0 (0.5 D u) + 0.5 D(dJa u),
+      // so the only contraction left in FP32 acts on dJa u, which is as small as
+      // the metric terms' variation over the element; its rounding error is
+      // that much smaller than the one of 0.5 D(Ja u) in FP32.
+      const real* sPhiT = sphiT;
+      double cu[8];
+      float uf[8];
+      {
+        double u[8];
+#pragma unroll
+        for (int pos = 0; pos < 8; ++pos) u[pos] = (double)sPhi[addr[pos]] + (double)sPhiT[addr[pos]];
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+          double acc = P.Gd[l * 8] * u[0];
+#pragma unroll
+          for (int m = 1; m < 8; ++m) acc = fma(P.Gd[l * 8 + m], u[m], acc);
+          cu[l] = acc;  // 0.5 D u
+        }
+        // centred-flux SAT of an interior al-face: jump on the face row
+        const bool sat0 = (mask >> (2 * al)) & 1, sat1 = (mask >> (2 * al + 1)) & 1;
+        const int f0 = (2 * al) * N2 + pc, f1 = (2 * al + 1) * N2 + pc;
+        const double jmp0 = sat0 ? -inv2Hd * (((double)sfc[f0] + (double)sfaceT[f0]) - u[0]) : 0.0;
+        const double jmp1 = sat1 ? inv2Hd * (((double)sfc[f1] + (double)sfaceT[f1]) - u[7]) : 0.0;
+#pragma unroll
+        for (int pos = 0; pos < 8; ++pos) uf[pos] = (float)u[pos];
+        // rows 0 and 7 also get the SAT, Ja times the jump
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const real* mc = sJa + (al * 3 + c) * FSC;
+          const double m0 = Q.Ja0[9 * e + al * 3 + c];
+          float w[8];
+#pragma unroll
+          for (int pos = 0; pos < 8; ++pos) w[pos] = mc[addr[pos]] * uf[pos];
+          real* gout = sg + (al * 3 + c) * FSC;
+#pragma unroll
+          for (int l = 0; l < 8; ++l) {
+            float o = P.Gh[l * 8] * w[0];
+#pragma unroll
+            for (int m = 1; m < 8; ++m) o = fmaf(P.Gh[l * 8 + m], w[m], o);  // 0.5 D(dJa u)
+            const double dl = (double)mc[addr[l]];
+            double r = fma(2.0 * m0 + dl, cu[l], (double)o);
+            if (l == 0) r = fma(m0 + dl, jmp0, r);
+            if (l == 7) r = fma(m0 + dl, jmp1, r);
+            gout[addr[l]] = (real)r;
+          }
+        }
+      }
+    } else {
       float u[8], cu[8], w[8], o[8];
 #pragma unroll
       for (int pos = 0; pos < 8; ++pos) u[pos] = sPhi[addr[pos]];
@@ -1338,6 +1470,9 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
     __syncthreads();  // partial gradients and sB complete; the Ja stage is free
     if (abort_flag) return;
     if (warp == 0 && has_next) issueA(t1);  // lands while the node pass runs
+    if constexpr (CP) {
+      if (has_next) async_loadT(t1, src1);  // the small parts are read by the contraction pass only
+    }
     // ---- node phase ----
 #pragma unroll
     for (int rr = 0; rr < NPT; ++rr) {
@@ -1346,7 +1481,7 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
       const int ti = node & 7, tj = (node >> 3) & 7, tk = node >> 6;
       const int at = LayC::at(node);
       const long long n = e * N3 + node;
-      const real u = sPhi[at];
+      const real u = sPhi[at];  // CP: the state's high part
       const real invJ = sB[11 * N3 + node];
       real g0 = (sg[at] + sg[3 * FSC + at]) + sg[6 * FSC + at];
       real g1 = (sg[FSC + at] + sg[4 * FSC + at]) + sg[7 * FSC + at];
@@ -1369,19 +1504,32 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
       const real F1 = b1 * Pi + (K1v * g0 + K3 * g1 + K4 * g2);
       const real F2 = b2 * Pi + (K2 * g0 + K4 * g1 + K5 * g2);
       real phid = b0 * g0 + b1 * g1 + b2 * g2 + a * Pi;
-      if (bnd && Q.bc_on) k1_boundary<real>(Q, e, ti, tj, tk, n, u, Pi, g0, g1, g2, cc, phid);
+      if (bnd && Q.bc_on) {
+        // the whole stage value where a boundary term reads Phi itself
+        const real uf = CP && Q.Phit ? u + Q.Phit[n] : u;
+        k1_boundary<real>(Q, e, ti, tj, tk, n, uf, Pi, g0, g1, g2, cc, phid);
+      }
       {  // flux in the LayC element-block layout read by K2
         const long long fo = e * FSC + at, fstr = Q.Ne * FSC;
         Q.F[fo] = F0;
         Q.F[fstr + fo] = F1;
         Q.F[2 * fstr + fo] = F2;
       }
-      const real yv = need_y ? sB[12 * N3 + node] : (real)0, accv = need_acc ? sB[13 * N3 + node] : (real)0;
-      const real compv = need_comp ? sB[14 * N3 + node] : (real)0;
-      if (P.epi)
-        n8_rk<real>(P.stage, Q.dt, phid, u, yv, accv, compv, n, Q.y, Q.acc, Q.out, comp_on ? Q.comp : nullptr, P.flag);
-      else
-        Q.Phidot[n] = phid;
+      const real accv = need_acc ? sB[IACC * N3 + node] : (real)0;
+      const real compv = need_comp ? sB[ICOMP * N3 + node] : (real)0;
+      if constexpr (CP) {
+        if (P.epi)
+          n8_rk_cp(P.stage, Q.dt, phid, u, accv, compv, n, Q.y, Q.acc, Q.out, Q.comp, Q.hcopy, P.flag);
+        else
+          Q.Phidot[n] = phid;
+      } else {
+        const real yv = need_y ? sB[IY * N3 + node] : (real)0;
+        if (P.epi)
+          n8_rk<real>(P.stage, Q.dt, phid, u, yv, accv, compv, n, Q.y, Q.acc, Q.out, comp_on ? Q.comp : nullptr,
+                      P.flag);
+        else
+          Q.Phidot[n] = phid;
+      }
     }
     cp_async_wait_all();  // this thread's copies into buffers fb^1 (the barrier above the next element publishes them)
     emcur = emnext;
@@ -1632,8 +1780,55 @@ __global__ void k_pad_fields(long long Ne, int nf, const real* __restrict__ src,
   }
 }
 
+// Split of the FP64 metric terms for the compensated FP32 form: per element
+// the mean of each of the nine fields (FP64), and every node's deviation from
+// it rounded to FP32 (n = 8: in the LayC element blocks of the CUDA-core
+// kernels; otherwise node order).  FP32 rounding then perturbs the metric
+// terms by the deviation's ulp, not the field's.
+__global__ void k_split_metric_mean(int N3, long long Ne, long long nn, const double* __restrict__ Ja,
+                                    double* __restrict__ Ja0) {
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;  // one warp per (element, field)
+  const int lane = threadIdx.x & 31;
+  if (w >= 9 * Ne) return;  // whole warps leave together
+  const long long e = w / 9;
+  const int c = (int)(w - 9 * e);
+  const double* src = Ja + c * nn + e * N3;
+  double sum = 0.0;
+  for (int t = lane; t < N3; t += 32) sum += src[t];
+  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if (lane == 0) Ja0[9 * e + c] = sum / N3;
+}
+
+template <bool LAYC>
+__global__ void k_split_metric_dev(int N3, long long Ne, long long nn, const double* __restrict__ Ja,
+                                   const double* __restrict__ Ja0, float* __restrict__ dJa) {
+  const long long total = 9 * nn;
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
+    const long long c = x / nn, r = x - c * nn, e = r / N3;
+    const int t = (int)(r - e * N3);
+    const float v = (float)(Ja[x] - Ja0[9 * e + c]);
+    if (LAYC)
+      dJa[(c * Ne + e) * n8::LayC::FS + n8::LayC::at(t)] = v;
+    else
+      dJa[x] = v;
+  }
+}
+
+int launch_split_metric(const DevMesh& m, cudaStream_t s) {
+  const int N3 = m.N * m.N * m.N;
+  const long long warps = 9 * m.Ne;
+  k_split_metric_mean<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(N3, m.Ne, m.nn, m.Ja, m.Ja0);
+  if (m.N == 8)
+    k_split_metric_dev<true><<<4096, 256, 0, s>>>(N3, m.Ne, m.nn, m.Ja, m.Ja0, (float*)m.dJa);
+  else
+    k_split_metric_dev<false><<<4096, 256, 0, s>>>(N3, m.Ne, m.nn, m.Ja, m.Ja0, (float*)m.dJa);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 // element-block layout of the mesh's n = 8 kernels: 0 = Lay<real>, 1 = LayC (FP32 CUDA-core form)
-static int n8_layout(const DevMesh& m) { return m.precision == 1 && m.fp32_form == WT_FP32_CUDA_CORES ? 1 : 0; }
+static int n8_layout(const DevMesh& m) {
+  return m.precision == 1 && (m.fp32_form == WT_FP32_CUDA_CORES || m.fp32_form == WT_FP32_COMPENSATED) ? 1 : 0;
+}
 static long long n8_fs(const DevMesh& m) {
   return m.precision == 0 ? n8::Lay<double>::FS : n8_layout(m) ? n8::LayC::FS : n8::Lay<float>::FS;
 }
@@ -1683,6 +1878,12 @@ static K1N8<real> k1n8_params(const DevMesh& m, const DevCoef& c, const void* Ph
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
   for (int i = 0; i < 64; ++i) P.Gh[i] = (float)(0.5 * m.ops.G[i]);
   P.gout = nullptr;
+  P.cp = m.precision == WT_F32 && m.fp32_form == WT_FP32_COMPENSATED ? 1 : 0;
+  P.Phit = (const real*)rk.phit;
+  P.dJa = (const real*)m.dJa;
+  P.Ja0 = m.Ja0;
+  P.hcopy = (real*)rk.hcopy;
+  for (int i = 0; i < 64; ++i) P.Gd[i] = 0.5 * m.ops.G[i];
   return P;
 }
 
@@ -1737,7 +1938,7 @@ static int n8_launch(int which, const void* hP, const void* plist, const int2* t
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-template <bool BATCH>
+template <bool BATCH, bool CP>
 static int n8c_launch(int which, const void* hP, const void* plist, const int2* tiles, long long ntiles,
                       cudaStream_t s) {
   static bool attr1 = false, attr2 = false;
@@ -1745,18 +1946,19 @@ static int n8c_launch(int which, const void* hP, const void* plist, const int2* 
   const long long cap = (long long)sm_count() * occ;
   const long long grid = ntiles < cap ? ntiles : cap;
   if (which == 1) {
+    constexpr size_t smem = k1c_smem<CP>();
     if (!attr1) {
       // three CTAs per SM need (nearly) all of the SM's shared memory
-      if (cudaFuncSetAttribute(k_cons_k1_n8c<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k1c_smem()) !=
-              cudaSuccess ||
-          cudaFuncSetAttribute(k_cons_k1_n8c<BATCH>, cudaFuncAttributePreferredSharedMemoryCarveout,
+      if (cudaFuncSetAttribute(k_cons_k1_n8c<BATCH, false, CP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem) != cudaSuccess ||
+          cudaFuncSetAttribute(k_cons_k1_n8c<BATCH, false, CP>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
         return -2;
       attr1 = true;
     }
     if (grid <= 0) return 0;
-    k_cons_k1_n8c<BATCH><<<(unsigned)grid, n8::CTHR, k1c_smem(), s>>>(*(const K1N8<float>*)hP,
-                                                                       (const K1N8<float>*)plist, tiles, ntiles);
+    k_cons_k1_n8c<BATCH, false, CP><<<(unsigned)grid, n8::CTHR, smem, s>>>(
+        *(const K1N8<float>*)hP, (const K1N8<float>*)plist, tiles, ntiles);
   } else {
     if (!attr2) {
       if (cudaFuncSetAttribute(k_cons_k2_n8c<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k2c_smem()) !=
@@ -1777,7 +1979,8 @@ template <bool BATCH>
 static int n8_dispatch(int which, int precision, int fp32_form, const void* hP, const void* plist, const int2* tiles,
                        long long ntiles, cudaStream_t s) {
   if (precision == 0) return n8_launch<double, 0, BATCH>(which, hP, plist, tiles, ntiles, s);
-  if (fp32_form == WT_FP32_CUDA_CORES) return n8c_launch<BATCH>(which, hP, plist, tiles, ntiles, s);
+  if (fp32_form == WT_FP32_COMPENSATED) return n8c_launch<BATCH, true>(which, hP, plist, tiles, ntiles, s);
+  if (fp32_form == WT_FP32_CUDA_CORES) return n8c_launch<BATCH, false>(which, hP, plist, tiles, ntiles, s);
   if (fp32_form == WT_FP32_BF16X2) return n8_launch<float, 2, BATCH>(which, hP, plist, tiles, ntiles, s);
   return n8_launch<float, 3, BATCH>(which, hP, plist, tiles, ntiles, s);
 }
@@ -1846,7 +2049,7 @@ int launch_grad_n8(const DevMesh& m, const void* Phi, void* grad, unsigned* flag
   K1N8<float> P = k1n8_params<float>(m, none, Phi, nullptr, nullptr, nullptr, nullptr, bc, rk, flag);
   P.gout = (float*)grad;
   if (m.fp32_form == WT_FP32_BF16X2) return launch_grad_n8_t<float, 2>(P, false, s);
-  return launch_grad_n8_t<float, 3>(P, m.fp32_form == WT_FP32_CUDA_CORES, s);
+  return launch_grad_n8_t<float, 3>(P, m.fp32_form == WT_FP32_CUDA_CORES || m.fp32_form == WT_FP32_COMPENSATED, s);
 }
 
 // Self-test of the bounded-wait failure path: one thread polls an mbarrier the

@@ -561,9 +561,9 @@ __global__ void k_initial(long long nn, int kind, const double* __restrict__ coo
 }
 
 int launch_initial(const DevMesh& m, int kind, const double* dparams, int np, double t, void* u, void* ut,
-                   cudaStream_t s) {
+                   cudaStream_t s, bool f64) {
   const unsigned b = (unsigned)((m.nn + 255) / 256);
-  if (m.precision == 0)
+  if (m.precision == 0 || f64)
     k_initial<double><<<b, 256, 0, s>>>(m.nn, kind, m.coords, dparams, np, t, (double*)u, (double*)ut);
   else
     k_initial<float><<<b, 256, 0, s>>>(m.nn, kind, m.coords, dparams, np, t, (float*)u, (float*)ut);

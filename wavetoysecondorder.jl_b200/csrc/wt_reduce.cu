@@ -132,9 +132,9 @@ __global__ void k_rk_update(long long n, int stage, double dt, real* __restrict_
       } else {
         const real inc = acc[i] + (real)(dt / 6.0) * kv;
         const real yv = y[i];
-        const real t = inc - comp[i];
+        const real t = inc + comp[i];
         const real v = yv + t;
-        comp[i] = (v - yv) - t;
+        comp[i] = t - (v - yv);
         y[i] = v;
       }
       continue;
@@ -221,6 +221,21 @@ int launch_copy(long long n, int precision, void* d, const void* s, cudaStream_t
   else k_copy<float><<<gblocks(n), RB, 0, st>>>(n, (float*)d, (const float*)s);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
+// FP64 values -> FP32 high part + FP32 low part (hi + lo carries ~48 bits)
+__global__ void k_split_f64(long long n, const double* __restrict__ a, float* __restrict__ hi, float* __restrict__ lo) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = a[i];
+    const float h = (float)v;
+    hi[i] = h;
+    lo[i] = (float)(v - (double)h);
+  }
+}
+
+int launch_split_f64(long long n, const double* a, float* hi, float* lo, cudaStream_t st) {
+  k_split_f64<<<gblocks(n), RB, 0, st>>>(n, a, hi, lo);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 int launch_rk_update(long long n, int precision, int stage, double dt, void* y, void* acc, void* out, const void* k,
                      cudaStream_t st, void* comp) {
   if (precision == 0)

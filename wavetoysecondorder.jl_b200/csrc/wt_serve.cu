@@ -76,7 +76,7 @@ int check_desc(const wt_serve_desc* d) {
   if (!(d->hbm_budget > 0) || d->tick < 1 || d->max_active < 0 || d->fill_nodes < 0) return -1;
   if (d->order < WT_SERVE_HRRN || d->order > WT_SERVE_FIFO) return -1;
   if (d->precision != WT_F64 && d->precision != WT_F32 && d->precision != WT_SERVE_AUTO) return -1;
-  if (d->fp32_form < WT_FP32_CUDA_CORES || d->fp32_form > WT_FP32_BF16X2) return -1;
+  if (d->fp32_form < WT_FP32_CUDA_CORES || d->fp32_form > WT_FP32_COMPENSATED) return -1;
   return 0;
 }
 
@@ -144,13 +144,8 @@ struct wt_server {
     }
     void* Phi = r.state;
     void* Pi = r.state ? (void*)((char*)r.state + fb) : nullptr;
-    if (!rc) rc = wt_initial_data(ctx, r.mesh, r.q.ic_kind, r.q.nic ? r.q.ic : nullptr, r.q.nic, 0.0, Phi, nullptr);
-    if (!rc) {
-      void* s = nullptr;
-      rc = wt_ctx_get_stream(ctx, &s);
-      if (!rc && cudaMemsetAsync(Pi, 0, fb, (cudaStream_t)s) != cudaSuccess)
-        rc = wt::ctx_fail(ctx, WT_ECUDA, "wt_serve: clearing Pi failed");
-    }
+    // (u, u_t) in FP64; an FP32 request keeps the low parts in its workspace
+    if (!rc) rc = wt_initial_state(ctx, r.ws, r.q.ic_kind, r.q.nic ? r.q.ic : nullptr, r.q.nic, 0.0, Phi, Pi);
     double h = 0;
     if (!rc) rc = wt_mesh_min_spacing(r.mesh, &h);
     if (!rc) {

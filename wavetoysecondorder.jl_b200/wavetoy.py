@@ -32,7 +32,7 @@ BG_GAUGE_WAVE, BG_SINE_SHIFT = 4, 5
 ERK_RK4, ERK_TSIT5 = 0, 1
 IC_EIGENMODE_CARTESIAN, IC_GAUSSIANS, IC_OUTGOING_PULSE, IC_PLANE_WAVE, IC_EIGENMODE_RADIAL = 0, 1, 2, 3, 4
 # precision forms of an FP32 mesh (n = 8 contractions): CUDA cores, split BF16 three-term / two-term
-FP32_CUDA_CORES, FP32_BF16X3, FP32_BF16X2 = 0, 1, 2
+FP32_CUDA_CORES, FP32_BF16X3, FP32_BF16X2, FP32_COMPENSATED = 0, 1, 2, 3
 # multi-patch mesh kinds (evolve3d mesh_kind :cubed_cube, :inflated_cube, :radial_shell)
 MESH_CUBED_CUBE, MESH_INFLATED_CUBE, MESH_RADIAL_SHELL = 1, 2, 3
 # prescribed 4-metrics of the fully second-order curved path
@@ -150,6 +150,7 @@ def library():
         "wt_evolve_curved_host": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i, vp],
         "wt_evolve_curved_host_f32": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i, vp],
         "wt_initial_data": [vp, vp, i, vp, i, d, vp, vp],
+        "wt_initial_state": [vp, vp, i, vp, i, d, vp, vp], "wt_state_set_f64": [vp, vp, vp, vp, vp, vp],
         "wt_gll_operators": [i, vp, vp, vp],
         "wt_ctx_profile": [vp, i], "wt_ctx_profile_read": [vp, C.POINTER(d * 2), C.POINTER(ll * 2)],
         "wt_mesh_create_slab": [vp, C.POINTER(_MeshDesc), i, i, pvp],
@@ -390,7 +391,7 @@ class Mesh(_Child):
         self.ctx.check(library().wt_mesh_release_setup_geometry(self.h), "wt_mesh_release_setup_geometry")
 
     def set_fp32_form(self, form: int):
-        """Select how an FP32 mesh evaluates the n = 8 contractions (FP32_* constants)."""
+        """Select the precision form of an FP32 mesh (FP32_* constants; default FP32_COMPENSATED)."""
         self.ctx.check(library().wt_mesh_set_fp32_form(self.h, int(form)), "wt_mesh_set_fp32_form")
 
     def min_spacing(self) -> float:
@@ -587,7 +588,7 @@ class Batch(_Child):
 
 def serve_desc(hbm_budget: float = 150e9, tick: int = 50, max_active: Optional[int] = None,
                fill_nodes: Optional[int] = 8_000_000, order: int = SERVE_HRRN, precision: int = WT_F32,
-               fp32_form: int = FP32_CUDA_CORES, auto_fp32_max_steps: int = 250, keep_results: bool = False,
+               fp32_form: int = FP32_COMPENSATED, auto_fp32_max_steps: int = 2000, keep_results: bool = False,
                rate_f64: float = 0.0, rate_f32: float = 0.0) -> _ServeDesc:
     """wt_serve_desc: admission and stepping policy of a ServeEngine (None: no limit)."""
     d = _ServeDesc()
@@ -1157,6 +1158,24 @@ def initial_data(mesh: Mesh, kind: int, params: Sequence[float], u, ut=None, t: 
     mesh.ctx.check(library().wt_initial_data(mesh.ctx.h, mesh.h, int(kind), p.ctypes.data if p.size else None,
                                              int(p.size), float(t), _ptr(u), _ptr(ut)), "initial_data")
     return u, ut
+
+
+def initial_state(ws: "Workspace", kind: int, params: Sequence[float], Phi, Pi, t: float = 0.0):
+    """initial_data of (Phi, Pi) = (u, u_t) for the solve ws steps, evaluated in FP64; on an FP32
+    mesh the workspace keeps the low parts the FP32 arrays lose (wt_initial_state)."""
+    import numpy as np
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    ws.ctx.check(library().wt_initial_state(ws.ctx.h, ws.h, int(kind), p.ctypes.data if p.size else None,
+                                            int(p.size), float(t), _ptr(Phi), _ptr(Pi)), "initial_state")
+    return Phi, Pi
+
+
+def state_from_f64(ws: "Workspace", Phi64, Pi64, Phi, Pi):
+    """Load a Float64 device state into the state arrays ws steps (wt_state_set_f64): FP32 meshes keep
+    the rounded values in Phi, Pi and the lost low parts in the workspace."""
+    ws.ctx.check(library().wt_state_set_f64(ws.ctx.h, ws.h, _ptr(Phi64), _ptr(Pi64), _ptr(Phi), _ptr(Pi)),
+                 "state_from_f64")
+    return Phi, Pi
 
 
 def gaussian_params(centres, amps, widths):
