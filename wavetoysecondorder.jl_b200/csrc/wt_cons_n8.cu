@@ -1147,6 +1147,9 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src, bool valid
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 4 : 0)
                : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 // index into a per-CTA table of the 6 x 64 face nodes for face source fs and
 // this face's point pq: the neighbour face's point after the orientation
@@ -1191,7 +1194,8 @@ constexpr size_t k1c_smem() {
   return (K1C_STAGE + k1c_b<CP>() + 9 * n8::LayC::FS + 2 * 6 * n8::N2 + 2 * n8::N3 +
           (CP ? 6 * n8::N2 + n8::N3 : 0)) * sizeof(float) + 64;
 }
-static_assert(3 * (k1c_smem<true>() + 1024) <= 233472, "three compensated K1c CTAs must fit an SM");
+// per CTA: dynamic + static (a few words) + the 1 KB the SM reserves; 228 KB per SM
+static_assert(3 * (k1c_smem<true>() + 64 + 1024) <= 233472, "three compensated K1c CTAs must fit an SM");
 // K2c node-pass fields (1/J and the RK state: invJ, y, acc, comp), one bulk-copied buffer
 constexpr size_t K2C_B = 4 * (size_t)n8::N3;
 constexpr size_t k2c_smem() {
@@ -1222,9 +1226,16 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
   real* sphiT = sfaceT + (CP ? NFT : 0);       // CP: 512 small parts (LayC)
   uint64_t* bar = reinterpret_cast<uint64_t*>(sphiT + (CP ? N3 : 0));  // [0] Ja stage, [1] sB
   __shared__ int abort_flag;
-  __shared__ short ftab[6 * N2];  // node of face-trace point pq on face fn of an element block
+  __shared__ __align__(16) double sJa0[2][9];  // CP: the element-constant metric part, double-buffered
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int al = tid >> 6, pc = tid & 63;  // contraction: axis (warp-uniform) and pencil
+  // node of the neighbour's face-trace point for face source fs and this face's point pq
+  // (computed, not tabled: three compensated CTAs need the table's shared memory)
+  auto fnode = [](int fs, int pq) -> int {
+    const int slot = face_slot(fs, pq);
+    const int fn = slot >> 6;
+    return face_node(faxis(fn), frow(fn, N), slot & 7, (slot >> 3) & 7, N);
+  };
   const real inv2H = (real)(1.0 / (2.0 * P.H[0]));
   const bool comp_on = P.epi && P.comp != nullptr;
   // the compensated form reads the state's high part from the Phi pencils and the low part at every stage
@@ -1249,8 +1260,6 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
 #pragma unroll
   for (int pos = 0; pos < 8; ++pos) addr[pos] = LayC::at(pnode(al, pc, pos));
 
-  for (int i = tid; i < 6 * N2; i += THR)
-    ftab[i] = (short)face_node(faxis(i >> 6), frow(i >> 6, N), i & 7, (i >> 3) & 7, N);
   if (tid == 0) {
     abort_flag = 0;
     mbar_init(&bar[0], 1);
@@ -1308,7 +1317,7 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
       const int idx = tid + r * THR;
       if (idx < NFT) {
         const bool ok = src[r] >= 0;
-        const real* g = ok ? Q.Phi + (long long)(src[r] >> 6) * N3 + ftab[face_slot(src[r], idx & 63)] : Q.Phi;
+        const real* g = ok ? Q.Phi + (long long)(src[r] >> 6) * N3 + fnode(src[r], idx & 63) : Q.Phi;
         cp_async4(sface + b * NFT + idx, g, ok);
       }
     }
@@ -1316,6 +1325,9 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
     for (int r = 0; r < NPT; ++r) {
       const int node = tid + r * THR;
       if (node < N3) cp_async4(sphi + b * N3 + LayC::at(node), Q.Phi + (long long)tl.y * N3 + node, true);
+    }
+    if constexpr (CP) {
+      if (tid < 9) cp_async8(&sJa0[b][tid], Q.Ja0 + 9 * (long long)tl.y + tid);
     }
   };
   // CP: the small parts Phit of the same values into the single buffers sfaceT, sphiT
@@ -1329,7 +1341,7 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
       const int idx = tid + r * THR;
       if (idx < NFT) {
         const bool ok = have && src[r] >= 0;
-        const real* g = ok ? base + (long long)(src[r] >> 6) * N3 + ftab[face_slot(src[r], idx & 63)] : base;
+        const real* g = ok ? base + (long long)(src[r] >> 6) * N3 + fnode(src[r], idx & 63) : base;
         cp_async4(sfaceT + idx, g, ok);
       }
     }
@@ -1419,7 +1431,7 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const real* mc = sJa + (al * 3 + c) * FSC;
-          const double m0 = Q.Ja0[9 * e + al * 3 + c];
+          const double m0 = sJa0[fb][al * 3 + c];
           float w[8];
 #pragma unroll
           for (int pos = 0; pos < 8; ++pos) w[pos] = mc[addr[pos]] * uf[pos];
