@@ -251,9 +251,12 @@ def run_ours(args):
     Phi = mesh.zeros()
     Pi = mesh.zeros()
     c, a, w = wt.workloads.pulses(seed, 8, amp=(0.5, 1.0), width=(0.05, 0.15), centre=(0.25, 0.75))
-    wt.initial_data(mesh, wt.IC_GAUSSIANS, wt.gaussian_params(c, a, w), Phi)
+    ic = wt.gaussian_params(c, a, w)
+    wt.initial_state(ws, wt.IC_GAUSSIANS, ic, Phi, Pi)
     dt = 0.2 * mesh.min_spacing() / wt.workloads.max_speed(p)
     bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+    study = args.precision == "f64" and world == 1 and not args.no_precision_study
+    E_0 = wt.wave3d_energy(Phi, Pi, coef, ws, metric=True) if study else None
 
     def step():
         wt.step_rk4_curved(Phi, Pi, coef, ws, dt, 1, eps_KO=0.0, bc3d=bc, metric=True)
@@ -286,6 +289,9 @@ def run_ours(args):
         dist.barrier()
     value, t_max, _ = aggregate(dist, t_ms / 1000.0, 2.0 * nn * args.steps, "cuda")
     finite = not ctx.nonfinite()
+    ref = None
+    if study:  # the FP64 state after warmup + timed steps: the reference of the FP32 forms
+        ref = (torch.cat([Phi, Pi]), wt.wave3d_energy(Phi, Pi, coef, ws, metric=True))
 
     # end to end through the host-buffer API (wt_evolve_curved_host, the shape of
     # evolve3d): page-locked host state in, one RK4 step per sample, state and
@@ -360,6 +366,20 @@ def run_ours(args):
                           "definition": "w (34 + 4 C) bytes per node per RK4 step, C = 20 streamed coefficient words"},
         "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "finite": finite,
     }
+    if study:
+        # the precision study of the large solve: every FP32 form on the same workload,
+        # timed like the FP64 form and compared with its state after the same steps
+        ws.close(); coef.close(); mesh.close()
+        del Phi, Pi
+        torch.cuda.empty_cache()
+        line["precision_forms"] = precision_study(wt, ctx, args, seed, p, ic, dt, ref, E_0, value, hbm)
+        comp = line["precision_forms"]["fp32_compensated"]
+        line["north_star"] = {
+            "form": "fp32_compensated (the chosen split-precision form: FP32 storage, compensated Phi, "
+                    "FP64 gradient of Phi)",
+            "dof_updates_per_s": comp["value"], "speedup_vs_plain_f64": comp["speedup_vs_f64"],
+            "rel_l2_vs_f64": comp["rel_l2_vs_f64"], "step_roofline_frac": comp["step_roofline"]["frac"],
+            "target": "speedup >= 3 at step_roofline_frac >= 0.7, rel_l2_vs_f64 <= 1e-5"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, ROOT)
         from oracle import oracle as O
@@ -372,6 +392,64 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def precision_study(wt, ctx, args, seed, p, ic, dt64, ref, E64_0, value64, hbm):
+    """The FP32 forms on the large solve (same mesh, background, initial data and
+    steps as the FP64 form): per form DOF-updates/s over the timed steps, the step
+    roofline against w (34 + 4 C) bytes with w = 4, the speed-up over the FP64
+    form, and the relative L2 / max error against the FP64 state and the energy
+    drift after warmup + timed steps."""
+    import torch
+    M, N = args.elements, args.n
+    mesh = wt.Mesh.warped_uniform_hex(ctx, N, M, 0.0, 1.0, 0.05, outer_tag=wt.SOMMERFELD_BDRY_TAG, precision=wt.WT_F32)
+    coef = wt.sample_background3d(mesh, wt.BG_ADM_PERTURBED, p)
+    ws = wt.make_wave3d_workspace(mesh)
+    nn = mesh.nn
+    dt = 0.2 * mesh.min_spacing() / wt.workloads.max_speed(p)
+    assert dt == dt64
+    bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+    Phi, Pi = mesh.zeros(), mesh.zeros()
+    refv, E64 = ref
+    out = {}
+    for name, form in (("fp32_compensated", wt.FP32_COMPENSATED), ("fp32_cuda_cores", wt.FP32_CUDA_CORES),
+                       ("fp32_bf16x3", wt.FP32_BF16X3)):
+        mesh.set_fp32_form(form)
+        wt.initial_state(ws, wt.IC_GAUSSIANS, ic, Phi, Pi)
+        E0 = wt.wave3d_energy(Phi, Pi, coef, ws, metric=True)
+        for _ in range(args.warmup):
+            wt.step_rk4_curved(Phi, Pi, coef, ws, dt, 1, bc3d=bc, metric=True)
+        torch.cuda.synchronize()
+        ctx.profile(True)
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            wt.step_rk4_curved(Phi, Pi, coef, ws, dt, 1, bc3d=bc, metric=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ctx.profile(False)
+        (k1_ms, k1_n), (k2_ms, k2_n) = ctx.profile_read()
+        t_s = e0.elapsed_time(e1) / 1000.0
+        v = 2.0 * nn * args.steps / t_s
+        step_bytes = 4 * (34 + 4 * 20) * nn
+        x = torch.cat([Phi, Pi]).double()
+        d = x - refv
+        E = wt.wave3d_energy(Phi, Pi, coef, ws, metric=True)
+        out[name] = {
+            "value": v, "unit": "DOF-updates/s", "ms_per_step": 1000.0 * t_s / args.steps,
+            "speedup_vs_f64": v / value64,
+            "step_roofline": {"algorithmic_bytes_per_step": step_bytes,
+                              "frac": step_bytes / (t_s / args.steps) / 1e9 / hbm},
+            "kernels_ms_per_launch": {"k1": k1_ms / max(k1_n, 1), "k2": k2_ms / max(k2_n, 1)},
+            "rel_l2_vs_f64": float(torch.linalg.norm(d) / torch.linalg.norm(refv)),
+            "max_err_vs_f64": float(d.abs().max() / refv.abs().max()),
+            "energy_drift": E / E0 - 1.0, "steps_compared": args.warmup + args.steps,
+            "finite": not ctx.nonfinite()}
+    out["f64_energy_drift"] = E64 / E64_0 - 1.0
+    ws.close(); coef.close(); mesh.close()
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_slab(args):
@@ -620,6 +698,8 @@ def main():
                          "(three / two terms)")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision-study", action="store_true",
+                    help="skip the FP32 forms run after the FP64 line (default workload, one GPU)")
     ap.add_argument("--workload", choices=["solve", "batch", "serve", "slab"], default="solve",
                     help="solve: the large warped ADM solve (default; one independent solve per rank); "
                          "batch: batched uneven solves; serve: served Poisson request stream; slab: the "

@@ -433,9 +433,13 @@ int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int n
  * run steps_per_sample RK4 steps, copy the state back into Phi_host/Pi_host
  * and the energy into energy[s] (may be NULL).  Phi_host/Pi_host hold the
  * final state on return.  Each sample is copied device to device into a
- * staging pair and from there to the host on a second stream, so the copy
+ * staging pair and from there to the host on two copy streams, so the copy
  * overlaps the next sample's steps (page-locked host buffers make it
- * asynchronous); four state-sized device buffers are allocated per call. */
+ * asynchronous).  The host does not wait inside the loop: energies are
+ * collected on the device and summed at the end, and the non-finite check
+ * (WT_ENONFINITE) runs every 16 samples and at the end.  The four state-sized
+ * device buffers it needs are allocated on the first call and kept by the
+ * workspace. */
 int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* Phi_host, double* Pi_host,
                           double dt, int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc,
                           int use_metric, double* energy);

@@ -90,6 +90,11 @@ struct wt_ws {
   void* erk = nullptr;    // explicit RK stage slopes: 2 x 8 x nn (Phi slopes, then Pi slopes)
   long long flux_block = 0;  // values per element block of F as the last fused stage wrote it (halo copies)
   int halo_cp = 0;        // the last fused stage ran the compensated FP32 form (its halo adds Phit)
+  // host-buffer evolution (evolve_host): device state, staging pair for the
+  // copies to the host, per-sample energy partial sums -- kept between calls
+  void* evo[4] = {nullptr, nullptr, nullptr, nullptr};
+  double* evoE = nullptr;
+  size_t evoE_len = 0;
 };
 
 namespace {
@@ -1073,7 +1078,8 @@ int wt_workspace_destroy(wt_ws* ws) {
   if (!ws) return WT_EINVAL;
   cudaStreamSynchronize(ws->ctx->stream);
   void* bufs[] = {ws->F, ws->bbuf, ws->grad, ws->kP, ws->kQ, ws->S0, ws->S1, ws->SQ, ws->accP, ws->accQ,
-                  ws->trace, ws->zero, ws->Lu, ws->compP, ws->compQ, ws->erk};
+                  ws->trace, ws->zero, ws->Lu, ws->compP, ws->compQ, ws->erk, ws->evo[0], ws->evo[1],
+                  ws->evo[2], ws->evo[3], ws->evoE};
   for (void* p : bufs)
     if (p) cudaFree(p);
   delete ws;
@@ -1243,10 +1249,9 @@ int wt_rhs_curved4(wt_ctx* ctx, wt_ws* ws, const void* phi, const void* phidot, 
                                      ctx->stream), "rhs_curved4");
 }
 
-int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, int use_metric,
-              double* E) {
-  WT_TRY(check_ws(ctx, ws));
-  if (!coef || !Phi || !Pi || !E) return fail(ctx, WT_EINVAL, "wt_energy: NULL argument");
+// The energy's per-block partial sums into ctx->d_partial (asynchronous).
+static int energy_partials(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi,
+                           int use_metric) {
   const wt::DevMesh& m = ws->mesh->m;
   WT_TRY(ensure(ws, &ws->grad, 3 * (size_t)m.nn * rsize(m.precision)));
   wt::DevCoef nocoef;
@@ -1261,6 +1266,14 @@ int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, cons
   WT_TRY(lrc(ctx, wt::launch_energy(m, coef->c, Pi, ws->grad, use_metric, ctx->d_partial, ctx->nblocks, ctx->stream),
              "energy"));
   ctx->launches += 2;
+  return 0;
+}
+
+int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, int use_metric,
+              double* E) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!coef || !Phi || !Pi || !E) return fail(ctx, WT_EINVAL, "wt_energy: NULL argument");
+  WT_TRY(energy_partials(ctx, ws, coef, Phi, Pi, use_metric));
   return reduce_to_host(ctx, E);
 }
 
@@ -1862,17 +1875,24 @@ static int evolve_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi_ho
   if (steps_per_sample < 1 || nsamples < 1) return fail(ctx, WT_EINVAL, "steps_per_sample, nsamples must be >= 1");
   const wt::DevMesh& m = ws->mesh->m;
   const size_t nb = (size_t)m.nn * rsize(prec);
-  // device state (dP, dQ) and a staging copy of the last sample (sP, sQ): each
-  // sample is copied device to device on the compute stream and from the
-  // staging pair to the host on a second stream, so the device-to-host copy of
-  // sample s overlaps the steps of sample s + 1
-  void* buf[4] = {nullptr, nullptr, nullptr, nullptr};
-  for (void*& p : buf)
-    if (dalloc(ctx, &p, nb, nullptr)) {
-      for (void* q : buf) cudaFree(q);
-      return WT_ENOMEM;
-    }
-  void *dP = buf[0], *dQ = buf[1], *sP = buf[2], *sQ = buf[3];
+  // device state (dP, dQ) and a staging copy of the last sample (sP, sQ), kept
+  // in the workspace between calls: each sample is copied device to device on
+  // the compute stream and from the staging pair to the host on two copy
+  // streams, so the device-to-host copy of sample s overlaps the steps of
+  // sample s + 1.  Nothing in the loop waits on the host: the energies go to a
+  // device array (per-block partial sums, summed on the host at the end in the
+  // order wt_energy sums them) and the non-finite flag is read every 16
+  // samples and at the end.
+  for (void*& p : ws->evo) WT_TRY(ensure(ws, &p, nb));
+  const size_t elen = energy ? (size_t)nsamples * ctx->nblocks : 0;
+  if (elen > ws->evoE_len) {
+    cudaFree(ws->evoE);
+    ws->evoE = nullptr;
+    ws->evoE_len = 0;
+    WT_TRY(dalloc(ctx, &ws->evoE, elen * sizeof(double), nullptr));
+    ws->evoE_len = elen;
+  }
+  void *dP = ws->evo[0], *dQ = ws->evo[1], *sP = ws->evo[2], *sQ = ws->evo[3];
   // one copy stream per field, so that the two device-to-host copies can run on
   // separate copy engines at the same time
   cudaStream_t cs = nullptr, cs2 = nullptr;
@@ -1888,14 +1908,22 @@ static int evolve_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi_ho
     cudaMemcpyAsync(dP, Phi_host, nb, cudaMemcpyHostToDevice, ctx->stream);
     cudaMemcpyAsync(dQ, Pi_host, nb, cudaMemcpyHostToDevice, ctx->stream);
   }
+  auto check_finite = [&]() -> int {
+    int bad = 0;
+    int r = wt_ctx_nonfinite(ctx, &bad);
+    if (!r && bad) r = fail(ctx, WT_ENONFINITE, "state became non-finite during evolution");
+    return r;
+  };
   for (int sidx = 0; sidx < nsamples && !rc; ++sidx) {
     rc = wt_step_rk4_curved(ctx, ws, coef, dP, dQ, dt, steps_per_sample, eps_ko, bc, use_metric);
     if (rc) break;
-    if (energy) rc = wt_energy(ctx, ws, coef, dP, dQ, use_metric, &energy[sidx]);
-    int bad = 0;
-    if (!rc) rc = wt_ctx_nonfinite(ctx, &bad);
-    if (!rc && bad) rc = fail(ctx, WT_ENONFINITE, "state became non-finite during evolution");
-    if (rc) break;
+    if (energy) {
+      rc = energy_partials(ctx, ws, coef, dP, dQ, use_metric);
+      if (rc) break;
+      cudaMemcpyAsync(ws->evoE + (size_t)sidx * ctx->nblocks, ctx->d_partial, ctx->nblocks * sizeof(double),
+                      cudaMemcpyDeviceToDevice, ctx->stream);
+    }
+    if (sidx % 16 == 15 && (rc = check_finite())) break;
     if (sidx > 0) {  // the previous sample has left the staging pair
       cudaStreamWaitEvent(ctx->stream, copied, 0);
       cudaStreamWaitEvent(ctx->stream, copied2, 0);
@@ -1915,13 +1943,24 @@ static int evolve_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi_ho
       cudaError_t e = cudaStreamSynchronize(c);
       if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, name);
     }
-  cudaStreamSynchronize(ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, name);
+  if (!rc) rc = check_finite();
+  if (!rc && energy) {
+    std::vector<double> h(elen);
+    e = cudaMemcpy(h.data(), ws->evoE, elen * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, name);
+    for (int sidx = 0; sidx < nsamples && !rc; ++sidx) {
+      double sum = 0.0;
+      for (int k = 0; k < ctx->nblocks; ++k) sum += h[(size_t)sidx * ctx->nblocks + k];
+      energy[sidx] = sum;
+    }
+  }
   if (staged) cudaEventDestroy(staged);
   if (copied) cudaEventDestroy(copied);
   if (copied2) cudaEventDestroy(copied2);
   if (cs) cudaStreamDestroy(cs);
   if (cs2) cudaStreamDestroy(cs2);
-  for (void* p : buf) cudaFree(p);
   return rc;
 }
 
