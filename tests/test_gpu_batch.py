@@ -105,3 +105,39 @@ def test_batch_rejects_bad_members(wt, ctx):
         batch.add(s.Pa, s.Qa, s.coef, s.ws, s.dt, s.bc)
     with pytest.raises(wt.WaveToyError):
         batch.remove(7)
+
+
+def test_batch_members_against_oracle(wt, ctx, O):
+    """Members of one mixed batch (n = 4, 6, 8; FP64 and the default compensated FP32
+    form; groups running as parallel graph branches) against the Float64 oracle after
+    60 steps: FP64 <= 1e-12, compensated FP32 <= 1e-5 relative L2."""
+    import torch
+    W = wt.workloads
+    specs = [(4, 3, 41, 0), (6, 2, 42, 1), (8, 2, 43, 1), (8, 2, 44, 0), (6, 2, 45, 0), (4, 3, 46, 1)]
+    members = []
+    batch = wt.Batch(ctx)
+    bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+    for N, M, seed, prec in specs:
+        g = wt.Mesh.uniform_hex(ctx, N, M, outer_tag=7, warp_A=0.05, precision=prec)
+        p = W.adm_params(seed, 1.0)
+        coef = wt.sample_background3d(g, wt.BG_ADM_PERTURBED, p)
+        ws = wt.make_wave3d_workspace(g)
+        c, a, w = W.pulses(seed, 2, amp=(0.5, 1.0), width=(0.08, 0.15))
+        Phi, Pi = g.zeros(), g.zeros()
+        wt.initial_state(ws, wt.IC_GAUSSIANS, wt.gaussian_params(c, a, w), Phi, Pi)
+        dt = 0.2 * g.min_spacing() / W.max_speed(p)
+        batch.add(Phi, Pi, coef, ws, dt, bc)
+        members.append((N, M, seed, prec, p, (c, a, w), dt, g, coef, ws, Phi, Pi))
+    assert batch.info()[2] == 6  # one group per (n, precision)
+    batch.step(60)
+    for N, M, seed, prec, p, pul, dt, g, coef, ws, Phi, Pi in members:
+        o = O.OracleMesh(N, M, A=0.05, outer_tag=7)
+        x, y, z = o.coords()
+        P0 = W.gaussian_field(x, y, z, *pul)
+        Po, Qo = o.evolve_curved(o.background(2, p), P0, np.zeros_like(P0), dt, 60, bc=O.make_bc([2] * 6),
+                                 use_metric=True)
+        err = np.linalg.norm(np.concatenate([Phi.double().cpu().numpy(), Pi.double().cpu().numpy()]) -
+                             np.concatenate([Po, Qo])) / np.linalg.norm(np.concatenate([Po, Qo]))
+        assert err <= (1e-12 if prec == 0 else 1e-5), (N, M, prec, err)
+    assert not ctx.nonfinite()
+    batch.close()

@@ -2021,6 +2021,11 @@ struct wt_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   long long launches_per_step = 0;
+  // one stream per group inside the captured step: the groups share no buffer,
+  // so their launches form parallel branches of the graph and run side by side
+  std::vector<cudaStream_t> gstreams;
+  std::vector<cudaEvent_t> gjoin;
+  cudaEvent_t fork = nullptr;
 };
 
 namespace {
@@ -2030,6 +2035,12 @@ void batch_release(wt_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
+  for (cudaStream_t st : b->gstreams) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : b->gjoin) cudaEventDestroy(ev);
+  if (b->fork) cudaEventDestroy(b->fork);
+  b->gstreams.clear();
+  b->gjoin.clear();
+  b->fork = nullptr;
   for (auto& g : b->groups) {
     cudaFree(g.d_tiles);
     cudaFree(g.d_k1);
@@ -2076,9 +2087,24 @@ int batch_launch(wt_batch* b, wt_batch::Group& g, int which, int st, cudaStream_
 }
 
 int batch_one_step(wt_batch* b, cudaStream_t s) {
-  for (int st = 0; st < 4; ++st) {
-    for (auto& g : b->groups) WT_TRY(lrc(b->ctx, batch_launch(b, g, 1, st, s), "batch K1"));
-    for (auto& g : b->groups) WT_TRY(lrc(b->ctx, batch_launch(b, g, 2, st, s), "batch K2"));
+  if (b->groups.size() <= 1 || b->gstreams.size() != b->groups.size()) {
+    for (int st = 0; st < 4; ++st) {
+      for (auto& g : b->groups) WT_TRY(lrc(b->ctx, batch_launch(b, g, 1, st, s), "batch K1"));
+      for (auto& g : b->groups) WT_TRY(lrc(b->ctx, batch_launch(b, g, 2, st, s), "batch K2"));
+    }
+    return 0;
+  }
+  // fork: each group's eight launches in order on its own stream, joined at the end
+  if (cudaEventRecord(b->fork, s) != cudaSuccess) return fail(b->ctx, WT_ECUDA, "batch fork");
+  for (size_t k = 0; k < b->groups.size(); ++k) {
+    cudaStream_t gs = b->gstreams[k];
+    cudaStreamWaitEvent(gs, b->fork, 0);
+    for (int st = 0; st < 4; ++st) {
+      WT_TRY(lrc(b->ctx, batch_launch(b, b->groups[k], 1, st, gs), "batch K1"));
+      WT_TRY(lrc(b->ctx, batch_launch(b, b->groups[k], 2, st, gs), "batch K2"));
+    }
+    cudaEventRecord(b->gjoin[k], gs);
+    cudaStreamWaitEvent(s, b->gjoin[k], 0);
   }
   return 0;
 }
@@ -2180,8 +2206,21 @@ int batch_rebuild(wt_batch* b) {
     for (auto& g : b->groups)
       if (!g.n8) WT_TRY(batch_tune_group(b, g));
   }
-  // capture one RK4 step of every group
+  // capture one RK4 step of every group (several groups: parallel branches)
   cudaStream_t own = ctx->own_stream;
+  if (b->groups.size() > 1) {
+    if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+      return fail(ctx, WT_ECUDA, "batch: event creation failed");
+    for (size_t k = 0; k < b->groups.size(); ++k) {
+      cudaStream_t gs = nullptr;
+      cudaEvent_t ev = nullptr;
+      if (cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+        return fail(ctx, WT_ECUDA, "batch: stream or event creation failed");
+      b->gstreams.push_back(gs);
+      b->gjoin.push_back(ev);
+    }
+  }
   cudaError_t e = cudaStreamBeginCapture(own, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph capture");
   int rc = batch_one_step(b, own);

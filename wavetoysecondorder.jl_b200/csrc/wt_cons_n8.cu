@@ -1402,13 +1402,13 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
       // The state u = Phi + Phit enters the derivative in FP64: FP32 rounding of
       // it, or of the contraction of it, would be amplified by the second
       // derivative in Pi-dot.  With Ja = Ja0 + dJa (Ja0 element-constant, FP64):
-      //   0.5 D(Ja u) = Ja0 (0.5 D u) + 0.5 D(dJa u),
+      //   0.5 D(Ja u) + 0.5 Ja D u = (2 Ja0 + dJa) (0.5 D u) + 0.5 D(dJa u),
       // so the only contraction left in FP32 acts on dJa u, which is as small as
-      // the metric terms' variation over the element; its rounding error is
-      // that much smaller than the one of 0.5 D(Ja u) in FP32.
+      // the metric terms' variation over the element; its rounding error is that
+      // much smaller than the one of 0.5 D(Ja u) in FP32.  Once 0.5 D u has been
+      // formed in FP64 it is a gradient-sized value, and FP32 suffices for the rest.
       const real* sPhiT = sphiT;
-      double cu[8];
-      float uf[8];
+      float cu[8], uf[8], jmp0, jmp1;
       {
         double u[8];
 #pragma unroll
@@ -1418,35 +1418,34 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
           double acc = P.Gd[l * 8] * u[0];
 #pragma unroll
           for (int m = 1; m < 8; ++m) acc = fma(P.Gd[l * 8 + m], u[m], acc);
-          cu[l] = acc;  // 0.5 D u
+          cu[l] = (float)acc;  // 0.5 D u
         }
-        // centred-flux SAT of an interior al-face: jump on the face row
+        // centred-flux SAT of an interior al-face: jump on the face row (formed in FP64)
         const bool sat0 = (mask >> (2 * al)) & 1, sat1 = (mask >> (2 * al + 1)) & 1;
         const int f0 = (2 * al) * N2 + pc, f1 = (2 * al + 1) * N2 + pc;
-        const double jmp0 = sat0 ? -inv2Hd * (((double)sfc[f0] + (double)sfaceT[f0]) - u[0]) : 0.0;
-        const double jmp1 = sat1 ? inv2Hd * (((double)sfc[f1] + (double)sfaceT[f1]) - u[7]) : 0.0;
+        jmp0 = sat0 ? (float)(-inv2Hd * (((double)sfc[f0] + (double)sfaceT[f0]) - u[0])) : 0.f;
+        jmp1 = sat1 ? (float)(inv2Hd * (((double)sfc[f1] + (double)sfaceT[f1]) - u[7])) : 0.f;
 #pragma unroll
         for (int pos = 0; pos < 8; ++pos) uf[pos] = (float)u[pos];
-        // rows 0 and 7 also get the SAT, Ja times the jump
+      }
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const real* mc = sJa + (al * 3 + c) * FSC;
-          const double m0 = sJa0[fb][al * 3 + c];
-          float w[8];
+      for (int c = 0; c < 3; ++c) {
+        const real* mc = sJa + (al * 3 + c) * FSC;
+        const float m0 = (float)sJa0[fb][al * 3 + c];
+        float w[8];
 #pragma unroll
-          for (int pos = 0; pos < 8; ++pos) w[pos] = mc[addr[pos]] * uf[pos];
-          real* gout = sg + (al * 3 + c) * FSC;
+        for (int pos = 0; pos < 8; ++pos) w[pos] = mc[addr[pos]] * uf[pos];
+        real* gout = sg + (al * 3 + c) * FSC;
 #pragma unroll
-          for (int l = 0; l < 8; ++l) {
-            float o = P.Gh[l * 8] * w[0];
+        for (int l = 0; l < 8; ++l) {
+          float o = P.Gh[l * 8] * w[0];
 #pragma unroll
-            for (int m = 1; m < 8; ++m) o = fmaf(P.Gh[l * 8 + m], w[m], o);  // 0.5 D(dJa u)
-            const double dl = (double)mc[addr[l]];
-            double r = fma(2.0 * m0 + dl, cu[l], (double)o);
-            if (l == 0) r = fma(m0 + dl, jmp0, r);
-            if (l == 7) r = fma(m0 + dl, jmp1, r);
-            gout[addr[l]] = (real)r;
-          }
+          for (int m = 1; m < 8; ++m) o = fmaf(P.Gh[l * 8 + m], w[m], o);  // 0.5 D(dJa u)
+          const float dl = mc[addr[l]];
+          float r = fmaf(2.f * m0 + dl, cu[l], o);
+          if (l == 0) r = fmaf(m0 + dl, jmp0, r);
+          if (l == 7) r = fmaf(m0 + dl, jmp1, r);
+          gout[addr[l]] = r;
         }
       }
     } else {

@@ -15,7 +15,8 @@ Workloads (sizes as named in the benchmark configuration):
     elements per axis and n ~ {4, 6, 8}, flat or perturbed ADM backgrounds
     with metric-perturbation amplitude U(0, 0.15), seeded pulses;
   * served solves (serve_requests): Poisson arrivals, e log-uniform in
-    [4, 32], n ~ {6, 8}, 200..2000 RK4 steps.
+    [4, 32], n ~ {6, 8}, final time U(0.5, 2) light-crossing times as a step
+    count clamped to 200..2000 RK4 steps.
 """
 from __future__ import annotations
 
@@ -127,11 +128,22 @@ def batch_specs(seed: int, count: int = 256, e_range=(4, 24), orders=(4, 6, 8)):
     return out
 
 
-def serve_requests(seed: int, count: int, rate: float, e_range=(4, 32), orders=(6, 8), steps=(200, 2000)):
+def gll_min_gap(n: int) -> float:
+    """Smallest gap between the n Gauss-Lobatto-Legendre nodes on [0, 1]
+    (the end nodes and the roots of P'_{n-1})."""
+    inner = np.polynomial.legendre.Legendre.basis(n - 1).deriv().roots()
+    x = np.sort(np.concatenate([[-1.0], inner.real, [1.0]]))
+    return float(np.min(np.diff(x)) / 2.0)
+
+
+def serve_requests(seed: int, count: int, rate: float, e_range=(4, 32), orders=(6, 8), steps=(200, 2000),
+                   final_time=(0.5, 2.0)):
     """Served-solve requests: Poisson arrivals at `rate` per second (exponential
-    gaps), e log-uniform in e_range, n ~ U(orders), ADM scale U(0, 1.5), the
-    final time as a step count U{steps} at CFL 0.2 (the U(0.5, 2) light-crossing
-    span mapped onto the step range), and seeds for background and pulses."""
+    gaps), e log-uniform in e_range, n ~ U(orders), ADM scale U(0, 1.5), a final
+    time t ~ U(final_time) light-crossing times of the unit cube and its RK4 step
+    count t / dt at CFL 0.2 (dt from the unwarped node spacing h * gll_min_gap(n)
+    and the background's speed bound), clamped to the step range; and seeds for
+    background and pulses."""
     r = SplitMix64(seed ^ 0x5E7E)
     t = 0.0
     out = []
@@ -140,7 +152,11 @@ def serve_requests(seed: int, count: int, rate: float, e_range=(4, 32), orders=(
         t += -math.log(1.0 - r.uniform()) / rate
         e = int(round(math.exp(lo + (hi - lo) * r.uniform())))
         n = orders[min(int(r.uniform() * len(orders)), len(orders) - 1)]
-        st = steps[0] + min(int(r.uniform() * (steps[1] - steps[0] + 1)), steps[1] - steps[0])
-        out.append({"rid": k, "arrival": t, "elements": e, "n": n, "scale": r.uniform(0.0, 1.5), "steps": st,
-                    "seed": seed * 100000 + k})
+        tf = r.uniform(*final_time)
+        scale = r.uniform(0.0, 1.5)
+        rseed = seed * 100000 + k
+        dt = 0.2 * gll_min_gap(n) / e / max_speed(adm_params(rseed, scale), 24)
+        st = int(min(max(round(tf / dt), steps[0]), steps[1]))
+        out.append({"rid": k, "arrival": t, "elements": e, "n": n, "scale": scale, "steps": st,
+                    "final_time": tf, "seed": rseed})
     return out
