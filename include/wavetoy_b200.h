@@ -470,10 +470,12 @@ int wt_snapshot_load(wt_ctx* ctx, wt_mesh* mesh, void* Phi, void* Pi, double* t,
  * boundary data; they are grouped by (n, precision, kernel path), each group
  * is one work list of (solve, element) tiles run by one kernel launch per RK4
  * stage, and one RK4 step of all groups is a CUDA graph, captured when the
- * membership changes and replayed by wt_batch_step.  The first step after a
- * change also picks the elements per CTA of the generic kernels by timing
- * (autotuner, on by default).  Every member advances by the same number of
- * steps per call; results equal wt_step_rk4_curved on each member alone. */
+ * membership changes and replayed by wt_batch_step; the groups' launches are
+ * parallel branches of that graph.  The first step after a change also picks
+ * the elements per CTA of the generic kernels, K1 and K2 separately, by
+ * timing (autotuner, on by default; wt_batch_group_info's epb_variant: bit 0
+ * K1, bit 1 K2).  Every member advances by the same number of steps per call;
+ * results equal wt_step_rk4_curved on each member alone. */
 int wt_batch_create(wt_ctx* ctx, wt_batch** out);
 int wt_batch_destroy(wt_batch* batch);
 int wt_batch_add(wt_batch* batch, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,

@@ -2083,7 +2083,8 @@ int batch_launch(wt_batch* b, wt_batch::Group& g, int which, int st, cudaStream_
   const size_t sz = which == 1 ? g.k1sz : g.k2sz;
   const char* d = (which == 1 ? g.d_k1 : g.d_k2) + st * ns * sz;
   const int cp = g.precision == WT_F32 && g.fp32_form == WT_FP32_COMPENSATED;
-  return wt::launch_cons_gen_batch(which, g.N, g.precision, g.epb_variant, cp, d, g.d_tiles, g.ntiles, s);
+  const int variant = (g.epb_variant >> (which - 1)) & 1;  // bit 0: K1, bit 1: K2
+  return wt::launch_cons_gen_batch(which, g.N, g.precision, variant, cp, d, g.d_tiles, g.ntiles, s);
 }
 
 int batch_one_step(wt_batch* b, cudaStream_t s) {
@@ -2109,37 +2110,36 @@ int batch_one_step(wt_batch* b, cudaStream_t s) {
   return 0;
 }
 
-// Time stage 0 of a generic group in both elements-per-CTA variants and keep
-// the faster (stage 0 writes only stage scratch, never the solution state).
+// Time K1 and K2 of stage 0 of a generic group, each in both elements-per-CTA
+// variants, and keep the faster of each (stage 0 writes only stage scratch,
+// never the solution state).  epb_variant: bit 0 K1's choice, bit 1 K2's.
 int batch_tune_group(wt_batch* b, wt_batch::Group& g) {
   cudaStream_t s = b->ctx->own_stream;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  float best = 1e30f;
-  int best_v = 0;
-  for (int v = 0; v < 2; ++v) {
-    g.epb_variant = v;
-    int rc = 0;
-    for (int rep = 0; rep < 2 && !rc; ++rep) {  // warm up
-      rc = batch_launch(b, g, 1, 0, s);
-      if (!rc) rc = batch_launch(b, g, 2, 0, s);
+  int choice = 0, rc = 0;
+  for (int which = 1; which <= 2 && !rc; ++which) {
+    float best = 1e30f;
+    int best_v = 0;
+    for (int v = 0; v < 2 && !rc; ++v) {
+      g.epb_variant = (choice & ~(1 << (which - 1))) | (v << (which - 1));
+      for (int rep = 0; rep < 2 && !rc; ++rep) rc = batch_launch(b, g, which, 0, s);  // warm up
+      cudaEventRecord(e0, s);
+      for (int rep = 0; rep < 4 && !rc; ++rep) rc = batch_launch(b, g, which, 0, s);
+      cudaEventRecord(e1, s);
+      if (rc) break;
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) { best = ms; best_v = v; }
     }
-    cudaEventRecord(e0, s);
-    for (int rep = 0; rep < 3 && !rc; ++rep) {
-      rc = batch_launch(b, g, 1, 0, s);
-      if (!rc) rc = batch_launch(b, g, 2, 0, s);
-    }
-    cudaEventRecord(e1, s);
-    if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return lrc(b->ctx, rc, "batch autotune"); }
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (ms < best) { best = ms; best_v = v; }
+    choice |= best_v << (which - 1);
   }
-  g.epb_variant = best_v;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (rc) return lrc(b->ctx, rc, "batch autotune");
+  g.epb_variant = choice;
   return 0;
 }
 

@@ -172,20 +172,31 @@ __device__ __forceinline__ real contract(const real* __restrict__ f, const real*
   return s;
 }
 
+// resident CTAs per SM the generic kernels are compiled for: about 1024 threads
+template <int T>
+struct GenOcc {
+  static constexpr int value = T >= 1024 ? 1 : 1024 / T;
+};
+
 // BATCH: the CTA's elements come from a work list of (solve, element) tiles
 // and each tile reads the parameter block of its solve (plist); otherwise
 // element blockIdx.x * EPB + le of the single solve P0.  EPB_: elements per CTA.
 // CP (real = float): the compensated form -- the Phi the stage reads (high
 // plus small part) and the split-form gradient of it in FP64.
 template <int N, typename real, bool CURV, bool BATCH, int EPB_, bool CP = false>
-__global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0, const K1P<real>* __restrict__ plist,
+__global__ void __launch_bounds__(Ep<N>::N3 * EPB_, GenOcc<Ep<N>::N3 * EPB_>::value) k_cons_k1(const K1P<real> P0, const K1P<real>* __restrict__ plist,
                                                             const int2* __restrict__ tiles, long long ntiles) {
   constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = EPB_;
-  using gt = typename std::conditional<CP, double, real>::type;  // precision of the gradient
+  // CP: u = Phi + Phit and its derivative D u in FP64; with Ja = Ja0 + dJa
+  // (Ja0 element-constant, FP64) the split form is
+  //   0.5 D(Ja u) + 0.5 Ja D u = (Ja0 + 0.5 dJa) D u + 0.5 D(dJa u),
+  // and only the last contraction, of the small dJa u, runs in FP32
+  using gt = typename std::conditional<CP, double, real>::type;  // precision of u and D u
   __shared__ gt GT[N2];
+  __shared__ real GTr[CP ? N2 : 1];  // CP: the operator in FP32 for D(dJa u)
   __shared__ gt su[EPB][N3];
   __shared__ gt sun[EPB][6][N2];
-  __shared__ gt sw[CURV ? EPB : 1][CURV ? 9 : 1][CURV ? N3 : 1];
+  __shared__ real sw[CURV ? EPB : 1][CURV ? 9 : 1][CURV ? N3 : 1];
   const int tid = threadIdx.x;
   const int le = tid / N3, t = tid - le * N3;
   const int i = t % N, j = (t / N) % N, k = t / N2;
@@ -207,6 +218,9 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
   const long long n = ec * N3 + t;
   const long long nn = P.nn;
   if (tid < N2) GT[(tid % N) * N + tid / N] = (gt)P.G[tid];
+  if constexpr (CP) {
+    if (tid < N2) GTr[(tid % N) * N + tid / N] = (real)P.G[tid];
+  }
   const real u = valid ? P.Phi[n] : (real)0;  // CP: the high part
   gt ug = u;                                   // the value the gradient differentiates
   if constexpr (CP) {
@@ -229,55 +243,53 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
     }
     sun[le][f][pq] = v;
   }
-  const bool grad_only = P.c10 == nullptr;
-  real a = 0, b[3] = {0, 0, 0}, K[6] = {0, 0, 0, 0, 0, 0}, Pi = 0;
-  if (!grad_only && valid) {
-    a = P.c10[n];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) b[c] = P.c10[(1 + c) * nn + n];
-#pragma unroll
-    for (int c = 0; c < 6; ++c) K[c] = P.c10[(4 + c) * nn + n];
-    Pi = P.Pi[n];
-  }
-  gt m[CURV ? 9 : 1];
+  real m[CURV ? 9 : 1];   // Ja (CP: its deviation dJa)
+  real m0[CP && CURV ? 9 : 1];  // CP: the element-constant part Ja0
   real invJ = 0, sd[3];
   if (CURV) {
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
-      if constexpr (CP)
-        m[c] = valid ? P.Ja0[9 * ec + c] + (gt)P.dJa[c * nn + n] : (gt)0;
-      else
+      if constexpr (CP) {
+        m[c] = valid ? P.dJa[c * nn + n] : (real)0;
+        m0[c] = valid ? (real)P.Ja0[9 * ec + c] : (real)0;
+      } else {
         m[c] = valid ? P.Ja[c * nn + n] : (real)0;
+      }
     }
     invJ = valid ? P.invdetJ[n] : (real)0;
   } else {
 #pragma unroll
     for (int d = 0; d < 3; ++d) sd[d] = P.sdiag[3 * ec + d];
   }
-  const gt Hend = (gt)P.H[0];
+  const real Hend = (real)P.H[0];
   if (CURV) {
 #pragma unroll
-    for (int c = 0; c < 9; ++c) sw[le][c][t] = m[c] * ug;
+    for (int c = 0; c < 9; ++c) sw[le][c][t] = m[c] * (real)ug;  // CP: dJa u
   }
   __syncthreads();
-  gt du[3];
+  real du[3];  // D u (CP: formed in FP64, then a gradient-sized value)
 #pragma unroll
-  for (int d = 0; d < 3; ++d) du[d] = contract<N>(su[le], GT, i, j, k, d);
-  gt gg[3];
+  for (int d = 0; d < 3; ++d) du[d] = (real)contract<N>(su[le], GT, i, j, k, d);
+  real g[3];
   if (CURV) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      gt acc = 0;
+      real acc = 0;
 #pragma unroll
-      for (int al = 0; al < 3; ++al)
-        acc += (gt)0.5 * contract<N>(sw[le][al * 3 + c], GT, i, j, k, al) + (gt)0.5 * m[al * 3 + c] * du[al];
-      gg[c] = acc;
+      for (int al = 0; al < 3; ++al) {
+        if constexpr (CP)
+          acc += (real)0.5 * contract<N>(sw[le][al * 3 + c], GTr, i, j, k, al) +
+                 (m0[al * 3 + c] + (real)0.5 * m[al * 3 + c]) * du[al];
+        else
+          acc += (real)0.5 * contract<N>(sw[le][al * 3 + c], GT, i, j, k, al) + (real)0.5 * m[al * 3 + c] * du[al];
+      }
+      g[c] = acc;
     }
   } else {
 #pragma unroll
-    for (int d = 0; d < 3; ++d) gg[d] = (gt)sd[d] * du[d];
+    for (int d = 0; d < 3; ++d) g[d] = sd[d] * du[d];
   }
-  // centred-flux SAT on interior faces through this node
+  // centred-flux SAT on interior faces through this node (CP: the jump formed in FP64)
   if (valid) {
     const int idx3[3] = {i, j, k};
 #pragma unroll
@@ -286,22 +298,37 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k1(const K1P<real> P0
       if (idx3[ax] != frow(f, N)) continue;
       if (!((emask >> f) & 1)) continue;
       const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
-      const gt jump = sun[le][f][p + N * q] - ug;
-      const gt nh = (f & 1) ? (gt)1 : (gt)-1;
+      const real jump = (real)(sun[le][f][p + N * q] - ug);
+      const real nh = (f & 1) ? (real)1 : (real)-1;
       if (CURV) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) gg[c] += nh * m[ax * 3 + c] * jump / ((gt)2 * Hend);
+        for (int c = 0; c < 3; ++c) {
+          real mc = m[ax * 3 + c];
+          if constexpr (CP) mc += m0[ax * 3 + c];
+          g[c] += nh * mc * jump / ((real)2 * Hend);
+        }
       } else {
-        gg[ax] += nh * (gt)sd[ax] / ((gt)2 * Hend) * jump;
+        g[ax] += nh * sd[ax] / ((real)2 * Hend) * jump;
       }
     }
   }
   if (CURV) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) gg[c] *= (gt)invJ;
+    for (int c = 0; c < 3; ++c) g[c] *= invJ;
   }
-  const real g[3] = {(real)gg[0], (real)gg[1], (real)gg[2]};
   if (!valid) return;
+  // the node's coefficients and Pi, loaded only now: held across the contraction
+  // they would cost the registers that keep more CTAs resident
+  const bool grad_only = P.c10 == nullptr;
+  real a = 0, b[3] = {0, 0, 0}, K[6] = {0, 0, 0, 0, 0, 0}, Pi = 0;
+  if (!grad_only) {
+    a = P.c10[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) b[c] = P.c10[(1 + c) * nn + n];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) K[c] = P.c10[(4 + c) * nn + n];
+    Pi = P.Pi[n];
+  }
   if (P.grad_out) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) P.grad_out[c * nn + n] = g[c];
