@@ -712,6 +712,11 @@ def run_serve(args):
             out[name]["max_rel_l2_vs_fp64"] = max(errs)
             out[name]["median_rel_l2_vs_fp64"] = sorted(errs)[len(errs) // 2]
             out[name]["requests_within_1e-5"] = int(sum(e <= 1e-5 for e in errs))
+            byrid = {q.rid: q for q in reqs}
+            out[name]["over_1e-5"] = [
+                {"rid": r.rid, "elements": byrid[r.rid].elements, "n": byrid[r.rid].n, "steps": byrid[r.rid].steps,
+                 "final_time": round(r.dt * byrid[r.rid].steps, 3), "rel_l2": e}
+                for r, e in zip(res, errs) if e > 1e-5]
         del res
         torch.cuda.empty_cache()
     main_ = out["served_fp32_compensated"]
