@@ -18,6 +18,8 @@ CASES = [  # N, M, slabs, periodic, precision, fp32 form, background
     (8, (2, 2, 6), 3, False, 1, 0, 2),
     (8, (2, 2, 5), 2, False, 1, 1, 2),     # split-BF16 form: 544-word flux blocks
     (6, (2, 2, 6), 2, True, 0, None, 4),
+    (8, (2, 2, 6), 3, False, 1, 3, 2),     # compensated FP32 form: the halo also carries Phi's small part
+    (6, (2, 3, 6), 2, True, 1, 3, 2),      # compensated, generic kernels, periodic ring
 ]
 
 
