@@ -125,6 +125,20 @@ def FP32_FORMS(wt):
             "cuda": wt.FP32_CUDA_CORES}
 
 
+def cpu_model() -> str:
+    """The host CPU's model name and logical core count (for the CPU baseline's record)."""
+    name = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    name = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return f"{name}, {os.cpu_count()} logical cores"
+
+
 def rank_seed(seed: int, rank: int) -> int:
     """Seed of rank `rank`'s independent solve (weak scaling: one solve per rank)."""
     return seed + 7919 * rank
@@ -216,6 +230,7 @@ def run_reference(args):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ADM background, 8 Gaussian pulses)",
             "config": workload_desc(args, nn_full),
             "cpu_baseline": {"value": value, "unit": "DOF-updates/s", "cores": O.num_threads(), "kind": "port",
+                             "cpu": cpu_model(), "sample_is_full_config": M == args.elements,
                              "sample": sample},
             "e2e": {"value": value, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference is Julia with unvendored dependencies (no toolchain here); its CPU path is "
@@ -386,6 +401,7 @@ def run_ours(args):
         O.build()
         v, cores, sample = cpu_sample(wt, O, args)
         line["cpu_baseline"] = {"value": v, "unit": "DOF-updates/s", "cores": cores, "kind": "port",
+                                "cpu": cpu_model(), "sample_is_full_config": args.elements <= 16,
                                 "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
