@@ -474,8 +474,10 @@ int wt_snapshot_load(wt_ctx* ctx, wt_mesh* mesh, void* Phi, void* Pi, double* t,
  * parallel branches of that graph.  The first step after a change also picks
  * the elements per CTA of the generic kernels, K1 and K2 separately, by
  * timing (autotuner, on by default; wt_batch_group_info's epb_variant: bit 0
- * K1, bit 1 K2).  Every member advances by the same number of steps per call;
- * results equal wt_step_rk4_curved on each member alone. */
+ * K1, bit 1 K2).  A member with a time-dependent background is re-sampled at
+ * every stage time inside the graph (its mesh must keep the set-up geometry).
+ * Every member advances by the same number of steps per call; results equal
+ * wt_step_rk4_curved on each member alone. */
 int wt_batch_create(wt_ctx* ctx, wt_batch** out);
 int wt_batch_destroy(wt_batch* batch);
 int wt_batch_add(wt_batch* batch, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
@@ -490,7 +492,8 @@ int wt_batch_group_info(wt_batch* batch, int group, int* N, int* precision, int*
 /* ---- serving a stream of solve requests -------------------------------------
  * No counterpart in the reference (one solve per evolve3d call,
  * src/evolve.jl:1149-1358).  A server owns one batch on a context.  A request
- * names an analytic mesh, a static background, initial data of Phi (Pi = 0), a
+ * names an analytic mesh, a background (static, or time-dependent and then
+ * re-sampled at every RK4 stage inside the batch), initial data of Phi (Pi = 0), a
  * CFL number and a step count, and arrives at a time on the server's clock
  * (seconds since wt_serve_create).  Each scheduling round (wt_serve_poll):
  *   1. requests whose arrival time has passed join the wait queue;
@@ -530,7 +533,7 @@ typedef struct {
 typedef struct {
   double arrival;            /* seconds on the server's clock */
   wt_mesh_desc mesh;         /* analytic mesh; precision is chosen by the server */
-  wt_background_desc bg;     /* static kinds only (the batch runs no time-dependent background) */
+  wt_background_desc bg;     /* any kind; a time-dependent one (gauge wave, sine shift) keeps its mesh's set-up geometry and is re-sampled at every RK4 stage */
   int ic_kind, nic;          /* wt_initial_data of Phi at t = 0 */
   double ic[WT_SERVE_MAX_IC];
   double cfl, max_speed;     /* dt = cfl * wt_mesh_min_spacing / max_speed */

@@ -141,3 +141,49 @@ def test_batch_members_against_oracle(wt, ctx, O):
         assert err <= (1e-12 if prec == 0 else 1e-5), (N, M, prec, err)
     assert not ctx.nonfinite()
     batch.close()
+
+
+@pytest.mark.parametrize("branches", [True, False])
+def test_batch_time_dependent_backgrounds(wt, ctx, branches):
+    """Gauge-wave and sine-shift members (re-sampled at every stage inside the batch
+    graph) beside a static member: each matches its solve stepped alone with
+    wt_step_rk4_curved, and each background's time advances with the steps.  Both with
+    the groups as parallel graph branches and with one group (FP64 members only)."""
+    specs = [(6, 2, wt.BG_GAUGE_WAVE, 0), (8, 2, wt.BG_SINE_SHIFT, 1), (4, 3, None, 0)]
+    if not branches:
+        specs = [(6, 2, wt.BG_GAUGE_WAVE, 0), (6, 3, wt.BG_SINE_SHIFT, 0)]
+    batch = wt.Batch(ctx)
+    bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+    members = []
+    for k, (N, M, kind, prec) in enumerate(specs):
+        g = wt.Mesh.uniform_hex(ctx, N, M, outer_tag=7, warp_A=0.05, precision=prec)
+        if kind is None:
+            prm = wt.workloads.adm_params(50 + k)
+            mk = lambda: wt.sample_background3d(g, wt.BG_ADM_PERTURBED, prm)
+            speed = wt.workloads.max_speed(prm)
+        else:
+            A, t0 = 0.1 + 0.02 * k, 0.03 * k
+            mk = lambda: wt.sample_background3d(g, kind, (A, 1.0, t0))
+            speed = (1 + A) / (1 - A)
+        cb, ca = mk(), mk()
+        ws, ws_alone = wt.make_wave3d_workspace(g), wt.make_wave3d_workspace(g)
+        c, a, w = wt.workloads.pulses(60 + k, 2, amp=(0.5, 1.0), width=(0.08, 0.15))
+        P, Q = g.zeros(), g.zeros()
+        wt.initial_state(ws, wt.IC_GAUSSIANS, wt.gaussian_params(c, a, w), P, Q)
+        Pa, Qa = P.clone(), Q.clone()
+        dt = 0.2 * g.min_spacing() / speed
+        batch.add(P, Q, cb, ws, dt, bc)
+        members.append((kind, prec, cb, ca, ws_alone, P, Q, Pa, Qa, dt))
+    assert (batch.info()[2] > 1) == branches
+    for n in (3, 5):
+        batch.step(n)
+        for kind, prec, cb, ca, wsa, P, Q, Pa, Qa, dt in members:
+            wt.step_rk4_curved(Pa, Qa, ca, wsa, dt, n, bc3d=bc, metric=True)
+    for kind, prec, cb, ca, wsa, P, Q, Pa, Qa, dt in members:
+        tol = 1e-12 if prec == 0 else 1e-6
+        assert rel(P, Pa) <= tol and rel(Q, Qa) <= tol, (kind, rel(P, Pa), rel(Q, Qa))
+        if kind is not None:
+            assert abs(cb.time - ca.time) < 1e-14 and cb.time > 0.2 * dt
+            np.testing.assert_allclose(cb.get(), ca.get(), rtol=0, atol=1e-13)
+    assert not ctx.nonfinite()
+    batch.close()

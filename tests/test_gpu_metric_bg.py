@@ -86,7 +86,14 @@ def test_plane_wave_on_device(wt, ctx, kind):
     wt.step_rk4_curved(P, Q, c, ws, t1 / nst, nst)
     Pe, _ = exact(kind, A, d, k0, t1, x)
     assert np.sqrt(np.mean((P.cpu().numpy() - Pe) ** 2)) < 1e-5
+    # the same solve as a batch member (background re-sampled inside the batch graph)
+    c2 = wt.sample_background3d(g, kind, (A, d, 0.0))
+    ws2 = wt.make_wave3d_workspace(g)
+    P2 = torch.tensor(P0, dtype=torch.float64, device="cuda")
+    Q2 = torch.tensor(Q0, dtype=torch.float64, device="cuda")
     batch = wt.Batch(ctx)
-    with pytest.raises(wt.WaveToyError):  # time-dependent backgrounds are not batched
-        batch.add(P, Q, c, ws, 1e-3, wt.make_bc3d([2] * 6))
+    batch.add(P2, Q2, c2, ws2, t1 / nst)
+    batch.step(nst)
+    assert abs(c2.time - t1) < 1e-13
+    assert np.sqrt(np.mean((P2.cpu().numpy() - Pe) ** 2)) < 1e-5
     batch.close()

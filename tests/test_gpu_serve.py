@@ -2,6 +2,8 @@
 every served result equals the same request stepped alone (<= 1e-6 relative
 L2, FP32 state), and the split-precision results stay within 1e-5 of the
 Float64 oracle."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -90,8 +92,6 @@ def test_engine_incremental_submission(wt, ctx):
     with pytest.raises(wt.WaveToyError):          # over the budget
         big = dataclasses.replace(reqs[0], elements=40)
         eng.submit(S.native_request(big, with_speed=False))
-    with pytest.raises(wt.WaveToyError):          # time-dependent backgrounds are not served
-        eng.submit(wt.serve_request(0.0, 6, 2, bg_kind=wt.BG_SINE_SHIFT, bg_params=(0.1, 1.0, 0.0), steps=2))
     eng.run()
     info = eng.info()
     assert info["done"] == 4 and info["active"] == 0 and info["waiting"] == 0 and info["used_bytes"] == 0
@@ -114,6 +114,43 @@ def test_engine_incremental_submission(wt, ctx):
     with pytest.raises(wt.WaveToyError):          # no kept state without keep_results
         eng2.state(rid)
     eng2.close()
+    assert not ctx.nonfinite()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_engine_serves_time_dependent_background(wt, ctx, precision):
+    """A sine-shift request (its background re-sampled at every RK4 stage inside the
+    batch) served beside a static one: the result equals the same solve stepped alone
+    (FP64 <= 1e-12, compensated FP32 <= 1e-6)."""
+    import torch
+    S = wt.serve
+    bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
+    c, a, w = wt.workloads.pulses(71, 2, amp=(0.5, 1.0), width=(0.08, 0.15))
+    icp = wt.gaussian_params(c, a, w)
+    A, t0, speed = 0.1, 0.02, 1.1 / 0.9
+    q = wt.serve_request(0.0, 6, 2, warp_A=0.05, outer_tag=wt.SOMMERFELD_BDRY_TAG, bg_kind=wt.BG_SINE_SHIFT,
+                         bg_params=(A, 1.0, t0), ic_params=icp, max_speed=speed, steps=9, bc3d=bc)
+    eng = wt.ServeEngine(ctx, wt.serve_desc(hbm_budget=4e9, tick=4, precision=precision, keep_results=True,
+                                            fill_nodes=None))
+    rid = eng.submit(q)
+    other = eng.submit(S.native_request(dataclasses.replace(requests(wt)[0], arrival=0.0)))
+    eng.run()
+    r = eng.result(rid)
+    assert r["steps"] == 9 and eng.result(other)["steps"] > 0
+    mesh = wt.Mesh.warped_uniform_hex(ctx, 6, 2, 0.0, 1.0, 0.05, outer_tag=wt.SOMMERFELD_BDRY_TAG,
+                                      precision=precision)
+    coef = wt.sample_background3d(mesh, wt.BG_SINE_SHIFT, (A, 1.0, t0))
+    ws = wt.make_wave3d_workspace(mesh)
+    Phi, Pi = mesh.zeros(), mesh.zeros()
+    wt.initial_state(ws, wt.IC_GAUSSIANS, icp, Phi, Pi)
+    dt = 0.2 * mesh.min_spacing() / speed
+    assert abs(dt - r["dt"]) <= 1e-15 * dt
+    wt.step_rk4_curved(Phi, Pi, coef, ws, r["dt"], 9, bc3d=bc, metric=True)
+    Phi_s, Pi_s = eng.state(rid)
+    got = torch.cat([Phi_s, Pi_s]).double().cpu().numpy()
+    want = torch.cat([Phi, Pi]).double().cpu().numpy()
+    assert rel(got, want) <= (1e-12 if precision == 0 else 1e-6)
+    eng.close()
     assert not ctx.nonfinite()
 
 

@@ -55,8 +55,8 @@ def test_hrrn_favours_short_then_ages_long():
 
 
 @pytest.mark.parametrize("prec,n,steps,bpn,want_prec", [
-    (0, 8, 100, 520, 0), (0, 6, 100, 480, 0), (1, 8, 100, 300, 1), (1, 6, 900, 260, 1),
-    (-1, 8, 250, 300, 1), (-1, 8, 251, 520, 0), (-1, 6, 2000, 480, 0)])
+    (0, 8, 100, 520, 0), (0, 6, 100, 480, 0), (1, 8, 100, 340, 1), (1, 6, 900, 300, 1),
+    (-1, 8, 250, 340, 1), (-1, 8, 251, 520, 0), (-1, 6, 2000, 480, 0)])
 def test_cost_and_precision(prec, n, steps, bpn, want_prec):
     wt = load_package()
     d = wt.serve_desc(precision=prec, auto_fp32_max_steps=250)
@@ -75,8 +75,8 @@ def test_request_validation():
     for bad in (dict(steps=0), dict(N=9), dict(M=0), dict(arrival=float("nan"))):
         with pytest.raises(wt.WaveToyError):
             wt.serve_cost(d, wt.serve_request(**{**good, **bad}))
-    with pytest.raises(wt.WaveToyError):   # time-dependent backgrounds are not served
-        wt.serve_cost(d, wt.serve_request(**good, bg_kind=wt.BG_GAUGE_WAVE, bg_params=(0.1, 1.0, 0.0)))
+    # time-dependent backgrounds are served (re-sampled every stage inside the batch)
+    wt.serve_cost(d, wt.serve_request(**good, bg_kind=wt.BG_GAUGE_WAVE, bg_params=(0.1, 1.0, 0.0)))
     with pytest.raises(wt.WaveToyError):
         wt.serve_cost(wt.serve_desc(tick=0), wt.serve_request(**good))
     with pytest.raises(ValueError):
@@ -104,4 +104,4 @@ def test_native_request_describes_build_solve():
     srv = S.Server.__new__(S.Server)
     srv.budget, srv.tick, srv.max_active, srv.fill_nodes, srv.order = 1e12, 50, None, None, "hrrn"
     srv.precision, srv.fp32_form, srv.keep = S.AUTO, wt.FP32_CUDA_CORES, False
-    assert srv._cost(q) == q.nodes * (260 + 272)      # 77 steps <= 250: FP32, n = 6
+    assert srv._cost(q) == q.nodes * (300 + 272)      # 77 steps <= the FP32 limit: FP32, n = 6

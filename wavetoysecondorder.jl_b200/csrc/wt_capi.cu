@@ -2087,12 +2087,34 @@ int batch_launch(wt_batch* b, wt_batch::Group& g, int which, int st, cudaStream_
   return wt::launch_cons_gen_batch(which, g.N, g.precision, variant, cp, d, g.d_tiles, g.ntiles, s);
 }
 
+// Members of a group with a time-dependent background: re-sample it at the stage
+// time before the group's K1 of stage st (as step_curved_once does), and after
+// stage 3 advance the time it holds by the member's dt.
+int batch_group_td(wt_batch* b, const wt_batch::Group& g, int st, bool after, cudaStream_t s) {
+  for (int slot : g.slots) {
+    const auto& mb = b->members[slot];
+    if (!mb.coef->td) continue;
+    if (!after) {
+      const double toff[4] = {0.0, 0.5 * mb.dt, 0.5 * mb.dt, mb.dt};
+      WT_TRY(coef_resample(b->ctx, mb.coef, toff[st], s));
+    } else {
+      WT_TRY(lrc(b->ctx, wt::launch_advance_time(mb.coef->d_t, mb.dt, s), "background time"));
+      b->ctx->launches += 1;
+    }
+  }
+  return 0;
+}
+
 int batch_one_step(wt_batch* b, cudaStream_t s) {
   if (b->groups.size() <= 1 || b->gstreams.size() != b->groups.size()) {
     for (int st = 0; st < 4; ++st) {
-      for (auto& g : b->groups) WT_TRY(lrc(b->ctx, batch_launch(b, g, 1, st, s), "batch K1"));
+      for (auto& g : b->groups) {
+        WT_TRY(batch_group_td(b, g, st, false, s));
+        WT_TRY(lrc(b->ctx, batch_launch(b, g, 1, st, s), "batch K1"));
+      }
       for (auto& g : b->groups) WT_TRY(lrc(b->ctx, batch_launch(b, g, 2, st, s), "batch K2"));
     }
+    for (auto& g : b->groups) WT_TRY(batch_group_td(b, g, 3, true, s));
     return 0;
   }
   // fork: each group's eight launches in order on its own stream, joined at the end
@@ -2101,9 +2123,11 @@ int batch_one_step(wt_batch* b, cudaStream_t s) {
     cudaStream_t gs = b->gstreams[k];
     cudaStreamWaitEvent(gs, b->fork, 0);
     for (int st = 0; st < 4; ++st) {
+      WT_TRY(batch_group_td(b, b->groups[k], st, false, gs));
       WT_TRY(lrc(b->ctx, batch_launch(b, b->groups[k], 1, st, gs), "batch K1"));
       WT_TRY(lrc(b->ctx, batch_launch(b, b->groups[k], 2, st, gs), "batch K2"));
     }
+    WT_TRY(batch_group_td(b, b->groups[k], 3, true, gs));
     cudaEventRecord(b->gjoin[k], gs);
     cudaStreamWaitEvent(s, b->gjoin[k], 0);
   }
@@ -2230,6 +2254,8 @@ int batch_rebuild(wt_batch* b) {
   e = cudaGraphInstantiate(&b->exec, b->graph, 0);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph instantiate");
   b->launches_per_step = 8 * (long long)b->groups.size();
+  for (const auto& mb : b->members)
+    if (mb.active && mb.coef->td) b->launches_per_step += 9;  // 4 re-samplings of 2 launches + the time step
   b->dirty = false;
   return 0;
 }
@@ -2264,7 +2290,8 @@ int wt_batch_add(wt_batch* b, wt_ws* ws, const wt_coef* coef, void* Phi, void* P
   if (!coef || !Phi || !Pi || !slot) return fail(ctx, WT_EINVAL, "wt_batch_add: NULL argument");
   if (coef->mesh != ws->mesh) return fail(ctx, WT_EINVAL, "coefficients belong to another mesh");
   if (!(dt > 0) || !std::isfinite(dt)) return fail(ctx, WT_EINVAL, "dt must be positive and finite");
-  if (coef->td) return fail(ctx, WT_ENOTSUP, "wt_batch_add: time-dependent backgrounds are not batched");
+  // a time-dependent background is re-sampled at every stage inside the batch's graph
+  if (coef->td) WT_TRY(need_setup_geometry(coef->mesh, "wt_batch_add (time-dependent background)"));
   wt_batch::Member mb;
   WT_TRY(make_bc(ctx, bc, 1, mb.bc));
   WT_TRY(ws_step_buffers(ws));
@@ -2307,6 +2334,10 @@ int wt_batch_step(wt_batch* b, int nsteps) {
   if (!b) return WT_EINVAL;
   wt_ctx* ctx = b->ctx;
   if (nsteps < 0) return fail(ctx, WT_EINVAL, "nsteps must be >= 0");
+  // re-sampling a time-dependent background reads the set-up coordinates: refuse
+  // before any launch if a member's mesh released them after it joined
+  for (const auto& mb : b->members)
+    if (mb.active && mb.coef->td) WT_TRY(need_setup_geometry(mb.coef->mesh, "wt_batch_step (time-dependent background)"));
   if (b->dirty) WT_TRY(batch_rebuild(b));
   if (nsteps == 0 || b->groups.empty()) return 0;
   cudaStream_t user = ctx->stream, own = ctx->own_stream;
@@ -2317,6 +2348,8 @@ int wt_batch_step(wt_batch* b, int nsteps) {
   cudaEventRecord(ctx->ord_b, own);
   cudaStreamWaitEvent(user, ctx->ord_b, 0);
   ctx->launches += b->launches_per_step * nsteps;
+  for (const auto& mb : b->members)  // the host copy of a time-dependent background's time
+    if (mb.active && mb.coef->td) mb.coef->t += nsteps * mb.dt;
   return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "batch graph launch");
 }
 

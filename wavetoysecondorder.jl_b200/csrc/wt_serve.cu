@@ -26,9 +26,10 @@ using Clock = std::chrono::steady_clock;
 // coefficients and metric, workspace and state, with the allocator's rounding
 int bytes_per_node(int precision, int n) {
   if (precision == WT_F64) return n == 8 ? 520 : 480;
-  return n == 8 ? 300 : 260;
+  return n == 8 ? 340 : 300;  // FP32: with the compensated form's split metric terms and Phi copy
 }
-constexpr int kSetupBytesPerNode = 272;  // FP64 set-up geometry held while a request is built
+constexpr int kSetupBytesPerNode = 272;  // FP64 set-up geometry: held while a request is built, and
+                                          // while it runs if its background is time-dependent
 
 struct Req {
   wt_serve_request q{};
@@ -90,8 +91,6 @@ std::string check_request(const wt_serve_request* q) {
   if (!(q->cfl > 0) || !(q->max_speed > 0) || !std::isfinite(q->cfl) || !std::isfinite(q->max_speed))
     return "cfl and max_speed must be positive and finite";
   if (q->nic < 0 || q->nic > WT_SERVE_MAX_IC) return "nic must be in 0..WT_SERVE_MAX_IC";
-  if (q->bg.kind == WT_BG_GAUGE_WAVE || q->bg.kind == WT_BG_SINE_SHIFT)
-    return "time-dependent backgrounds are not served (the batch runs static coefficients)";
   if (q->bc.gPhi || q->bc.gPi || q->bc.gDx || q->bc.gDy || q->bc.gDz) return "boundary data pointers must be NULL";
   return "";
 }
@@ -150,7 +149,9 @@ struct wt_server {
     if (!rc) rc = wt_mesh_min_spacing(r.mesh, &h);
     if (!rc) {
       r.dt = r.q.cfl * h / r.q.max_speed;
-      rc = wt_mesh_release_setup_geometry(r.mesh);
+      // a time-dependent background is re-sampled on the mesh every stage: keep its geometry
+      const bool td = r.q.bg.kind == WT_BG_GAUGE_WAVE || r.q.bg.kind == WT_BG_SINE_SHIFT;
+      if (!td) rc = wt_mesh_release_setup_geometry(r.mesh);
     }
     if (!rc) rc = wt_batch_add(batch, r.ws, r.coef, Phi, Pi, r.dt, &r.q.bc, &r.slot);
     if (rc) {

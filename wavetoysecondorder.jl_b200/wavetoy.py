@@ -607,8 +607,9 @@ def serve_request(arrival: float, N: int, M, x0: float = 0.0, x1: float = 1.0, w
                   outer_tag: int = 0, bg_kind: int = BG_MINKOWSKI, bg_params: Sequence[float] = (),
                   ic_kind: int = IC_GAUSSIANS, ic_params: Sequence[float] = (), cfl: float = 0.2,
                   max_speed: float = 1.0, steps: int = 1, bc3d: Optional["BC3D"] = None) -> _ServeRequest:
-    """wt_serve_request: one solve (analytic mesh, static background, initial data
-    of Phi with Pi = 0, dt = cfl * min spacing / max_speed, RK4 steps)."""
+    """wt_serve_request: one solve (analytic mesh; background, a time-dependent one
+    re-sampled at every RK4 stage; initial data of Phi with Pi = 0; dt = cfl * min
+    spacing / max_speed; RK4 steps)."""
     q = _ServeRequest()
     q.arrival = float(arrival)
     M = (M, M, M) if isinstance(M, int) else tuple(M)
