@@ -262,6 +262,8 @@ def run_ours(args):
     p = wt.workloads.adm_params(seed)
     coef = wt.sample_background3d(mesh, wt.BG_ADM_PERTURBED, p)
     ws = wt.make_wave3d_workspace(mesh)
+    if args.unfused:
+        ws.set_fused(False)
     nn = mesh.nn
     Phi = mesh.zeros()
     Pi = mesh.zeros()
@@ -296,7 +298,7 @@ def run_ours(args):
     ev1.record(stream)
     torch.cuda.synchronize()
     ctx.profile(False)
-    (k1_ms, k1_n), (k2_ms, k2_n) = ctx.profile_read()
+    (k1_ms, k1_n), (k2_ms, k2_n), (fk_ms, fk_n) = ctx.profile_read()
     launches = ctx.launch_count() - n0
     clocks = sampler.stop()
     t_ms = ev0.elapsed_time(ev1)
@@ -349,16 +351,37 @@ def run_ours(args):
     e2e["d2h_bound_frac"] = (e2e["d2h_bytes_per_step"] / step_s / 1e9) / link
     del Ph, Qh
 
-    # roofline of the dominant kernel (K1: gradient + flux + Phi stage update)
+    # roofline of the dominant kernel: the fused stage kernel (FP64 n = 8: three of
+    # its launches per step), else K1 (gradient + flux + Phi stage update)
     hbm, src = peaks()
     wbytes = 8 if prec == wt.WT_F64 else 4
-    k1_words = 1 + 1 + 20 + 3 + 3   # Phi, Pi, 20 coefficient words, F (3), Phi RK stage words (stage mean)
+    fused = fk_n > 0
+    # K1 in the two-kernel step: Phi, Pi, 20 coefficient words, F (3), Phi RK stage
+    # words (3, the mean over the four stages); the fused step's K1_0 (stage 0)
+    # reads no RK state: Phi, Pi, 20 coefficient words, F (3), stage value, acc
+    k1_words = 1 + 1 + 20 + 3 + (2 if fused else 3)
     k1_avg_s = (k1_ms / max(k1_n, 1)) / 1000.0
     k1_achieved = k1_words * wbytes * nn / k1_avg_s / 1e9 if k1_n else None
-    traffic_pn = profiled_traffic(f"k1_curv_{args.precision}" if args.precision == "f64" or args.fp32_form == "cuda"
-                                  else f"k1_curv_f32_{args.fp32_form}")
+    # fused stage FK_s, s = 0, 1, 2 (mean): K2 half F_s (3), Ja (9), 1/J, Pi state y and acc
+    # read (5/3), acc written (1); K1 half Phi_{s+1} (1), ten coefficients, Phi y and acc read
+    # (5/3), F_{s+1} (3) and the Phi stage value or state (1) written, acc written (2/3)
+    fk_words = 3 + 9 + 1 + 5 / 3 + 1 + 1 + 10 + 5 / 3 + 3 + 1 + 2 / 3
+    fk_avg_s = (fk_ms / max(fk_n, 1)) / 1000.0
+    fk_achieved = fk_words * wbytes * nn / fk_avg_s / 1e9 if fk_n else None
     k2_avg_s = (k2_ms / max(k2_n, 1)) / 1000.0
-    k2_words = 3 + 10 + 3
+    # K2: F (3), Ja (9), 1/J, Pi RK stage words (3, four-stage mean; the fused step's
+    # K2_3 reads acc and writes the state: 2)
+    k2_words = 3 + 10 + (2 if fused else 3)
+    if fused:
+        traffic_pn = profiled_traffic("fk_curv_f64")
+        rl_kernel, rl_words, rl_achieved, rl_avg_s = (
+            "k_cons_fk_n8 (fused stage: divergence + Pi stage s, gradient + flux + Phi stage s + 1)", fk_words,
+            fk_achieved, fk_avg_s)
+    else:
+        traffic_pn = profiled_traffic(f"k1_curv_{args.precision}" if args.precision == "f64" or args.fp32_form == "cuda"
+                                      else f"k1_curv_f32_{args.fp32_form}")
+        rl_kernel, rl_words, rl_achieved, rl_avg_s = (
+            "k_cons_k1 (split-form gradient + flux + Phi RK4 stage)", k1_words, k1_achieved, k1_avg_s)
     step_bytes = wbytes * (34 + 4 * 20) * nn
     line = {
         "metric": "DOF-updates/s", "value": value, "unit": "DOF-updates/s", "n_gpus": world, "steps": args.steps,
@@ -366,15 +389,17 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
         "data": "synthetic (seeded ADM background, 8 seeded Gaussian pulses; no dataset)",
         "config": workload_desc(args, nn),
-        "roofline": {"bound": "hbm", "kernel": "k_cons_k1 (split-form gradient + flux + Phi RK4 stage)",
-                     "achieved": k1_achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": (k1_achieved / hbm) if k1_achieved else None,
+        "roofline": {"bound": "hbm", "kernel": rl_kernel,
+                     "achieved": rl_achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (rl_achieved / hbm) if rl_achieved else None,
                      "traffic": (traffic_pn * nn) if traffic_pn else None,
-                     "algorithmic_bytes_per_launch": k1_words * wbytes * nn,
-                     "avg_launch_ms": 1000.0 * k1_avg_s, "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)"},
-        "kernels": {"k_cons_k1": {"launches": k1_n, "ms": k1_ms},
+                     "algorithmic_bytes_per_launch": rl_words * wbytes * nn,
+                     "avg_launch_ms": 1000.0 * rl_avg_s, "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)"},
+        "kernels": {"k_cons_k1": {"launches": k1_n, "ms": k1_ms,
+                                  "achieved_GBps": k1_achieved},
                     "k_cons_k2": {"launches": k2_n, "ms": k2_ms,
-                                  "achieved_GBps": k2_words * wbytes * nn / k2_avg_s / 1e9 if k2_n else None}},
+                                  "achieved_GBps": k2_words * wbytes * nn / k2_avg_s / 1e9 if k2_n else None},
+                    "k_cons_fk_n8": {"launches": fk_n, "ms": fk_ms, "achieved_GBps": fk_achieved}},
         "step_roofline": {"algorithmic_bytes_per_step": step_bytes,
                           "achieved_GBps": step_bytes / (t_max / args.steps) / 1e9,
                           "frac": step_bytes / (t_max / args.steps) / 1e9 / hbm,
@@ -445,7 +470,7 @@ def precision_study(wt, ctx, args, seed, p, ic, dt64, ref, E64_0, value64, hbm):
         e1.record(stream)
         torch.cuda.synchronize()
         ctx.profile(False)
-        (k1_ms, k1_n), (k2_ms, k2_n) = ctx.profile_read()
+        (k1_ms, k1_n), (k2_ms, k2_n), _ = ctx.profile_read()
         t_s = e0.elapsed_time(e1) / 1000.0
         v = 2.0 * nn * args.steps / t_s
         step_bytes = 4 * (34 + 4 * 20) * nn
@@ -765,6 +790,8 @@ def main():
                          "(three / two terms)")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--unfused", action="store_true",
+                    help="FP64 n = 8: step through the two-kernel stages instead of the fused stage kernel")
     ap.add_argument("--no-precision-study", action="store_true",
                     help="skip the FP32 forms run after the FP64 line (default workload, one GPU)")
     ap.add_argument("--workload", choices=["solve", "batch", "serve", "slab"], default="solve",

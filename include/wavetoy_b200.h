@@ -96,11 +96,12 @@ int wt_ctx_nonfinite(wt_ctx* ctx, int* flag);
  * WT_ETIMEOUT); the context stays usable.  Nothing faults or waits unbounded. */
 int wt_ctx_selftest_wait(wt_ctx* ctx, int arrive, long long polls);
 /* Per-kernel timing for measurement: while enabled, the fused RK4 step records
- * CUDA events around each launch of its two kernels (gradient/flux and
- * divergence) on the launching stream; wt_ctx_profile_read synchronises and
- * returns the summed milliseconds and launch counts {K1, K2}, then clears. */
+ * CUDA events around each launch of its kernels (gradient/flux K1, divergence
+ * K2, and the fused stage kernel of FP64 n = 8 solves) on the launching
+ * stream; wt_ctx_profile_read synchronises and returns the summed milliseconds
+ * and launch counts {K1, K2, fused stage}, then clears. */
 int wt_ctx_profile(wt_ctx* ctx, int enable);
-int wt_ctx_profile_read(wt_ctx* ctx, double ms[2], long long count[2]);
+int wt_ctx_profile_read(wt_ctx* ctx, double ms[3], long long count[3]);
 
 /* ---- reference element ----------------------------------------------------- */
 /* HexSBPSAT.make_element(T, N) + make_operators(elem) (src/evolve.jl:1189):
@@ -283,6 +284,15 @@ int wt_workspace_mu(wt_ws* ws, double* mu);
  * slabs of a partitioned solve take the whole mesh's value, since each slab's
  * own estimate differs from it. */
 int wt_workspace_set_mu(wt_ws* ws, double mu);
+/* Fused RK4 stages (the integrator-in-RHS idea of the reference's IDEAS.md:48-50;
+ * no entry point of its own there): with on = 1 (the default) an FP64 n = 8
+ * solve without Kreiss-Oliger dissipation steps through the fused stage kernel,
+ * which runs the divergence half of stage s and the gradient half of stage
+ * s + 1 in one launch (five launches per RK4 step instead of eight, a quarter
+ * fewer bytes).  The results equal the two-kernel stages' bit for bit; on = 0
+ * selects the two-kernel stages (for comparison).  Takes effect at the next
+ * step call; the second flux buffer (3 x 8 bytes per node) is allocated then. */
+int wt_workspace_set_fused(wt_ws* ws, int on);
 
 /* ---- right-hand sides (device pointers, async) ------------------------------*/
 typedef struct {

@@ -28,7 +28,7 @@ struct wt_ctx {
   int nblocks = 0;
   // per-kernel timing (CUDA events around K1/K2 launches on the launching stream)
   int prof_on = 0;
-  std::vector<cudaEvent_t> prof_ev[2];  // [kernel] start/stop pairs
+  std::vector<cudaEvent_t> prof_ev[3];  // [kernel: K1, K2, fused stage] start/stop pairs
   cudaEvent_t ord_a = nullptr, ord_b = nullptr;  // order the graph stream with the caller's stream
   double* noalloc_scratch = nullptr;  // device address of the wt_rhs_curved_noalloc array (first call)
 };
@@ -69,6 +69,8 @@ struct wt_ws {
   double mu = 0.0, inv_mu5 = 0.0;
   bool mu_done = false;  // mu is computed on first use (Kreiss-Oliger or wt_workspace_mu)
   void* F = nullptr;      // 3 nn
+  void* F2 = nullptr;     // FP64 n = 8 fused stages: the second flux buffer (F ping-pongs between launches)
+  int fused = 1;          // FP64 n = 8 RK4 steps through the fused stage kernel (wt_workspace_set_fused)
   void* bbuf = nullptr;   // nbf N^2
   void* grad = nullptr;   // 3 nn
   void* kP = nullptr;     // nn (Phidot / u_t slope)
@@ -518,11 +520,11 @@ int wt_ctx_profile(wt_ctx* ctx, int enable) {
   return 0;
 }
 
-int wt_ctx_profile_read(wt_ctx* ctx, double ms[2], long long count[2]) {
+int wt_ctx_profile_read(wt_ctx* ctx, double ms[3], long long count[3]) {
   if (!ctx || !ms || !count) return WT_EINVAL;
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "profile");
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < 3; ++k) {
     ms[k] = 0.0;
     count[k] = 0;
     auto& v = ctx->prof_ev[k];
@@ -1077,12 +1079,18 @@ int wt_workspace_create(wt_ctx* ctx, wt_mesh* mesh, wt_ws** out) {
 int wt_workspace_destroy(wt_ws* ws) {
   if (!ws) return WT_EINVAL;
   cudaStreamSynchronize(ws->ctx->stream);
-  void* bufs[] = {ws->F, ws->bbuf, ws->grad, ws->kP, ws->kQ, ws->S0, ws->S1, ws->SQ, ws->accP, ws->accQ,
+  void* bufs[] = {ws->F, ws->F2, ws->bbuf, ws->grad, ws->kP, ws->kQ, ws->S0, ws->S1, ws->SQ, ws->accP, ws->accQ,
                   ws->trace, ws->zero, ws->Lu, ws->compP, ws->compQ, ws->erk, ws->evo[0], ws->evo[1],
                   ws->evo[2], ws->evo[3], ws->evoE};
   for (void* p : bufs)
     if (p) cudaFree(p);
   delete ws;
+  return 0;
+}
+
+int wt_workspace_set_fused(wt_ws* ws, int on) {
+  if (!ws) return WT_EINVAL;
+  ws->fused = on ? 1 : 0;
   return 0;
 }
 
@@ -1384,8 +1392,74 @@ static int rk4_stage_part(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi
   return 0;
 }
 
+// The RK4 step of an FP64 n = 8 solve through the fused stage kernel: K1_0,
+// FK_0, FK_1, FK_2 (each the K2 half of stage s and the K1 half of stage s + 1),
+// K2_3 -- five launches instead of eight, the flux ping-ponging between ws->F
+// and ws->F2.  Time-dependent backgrounds are re-sampled before the launch
+// whose K1 half reads them (the K2 halves read no coefficients).  The results
+// equal those of the two-kernel stages bit for bit.
+static bool fused_path(const wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double eps_ko,
+                       const wt::ConsBC& b, int use_metric) {
+  const wt::DevMesh& m = ws->mesh->m;
+  if (!ws->fused || eps_ko != 0.0 || m.precision != WT_F64 || m.N != 8 || !ws->F2) return false;
+  wt::RKStage r;
+  r.on = 1;
+  r.y = Phi; r.acc = ws->accP; r.out = ws->S0;
+  wt::RKStage q = r;
+  q.y = Pi; q.acc = ws->accQ; q.out = ws->SQ;
+  return wt::cons_n8_path(m, coef->c, use_metric, b, r, q, {Phi, Pi, ws->F, ws->F2, ws->S1});
+}
+
+static int step_curved_fused(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
+                             const wt::ConsBC& b, int use_metric) {
+  const wt::DevMesh& m = ws->mesh->m;
+  cudaStream_t s = ctx->stream;
+  void* SP[2] = {ws->S0, ws->S1};
+  void* FB[2] = {ws->F, ws->F2};
+  const double toff[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};  // RK4 stage times
+  auto rkP = [&](int st) {
+    wt::RKStage r;
+    r.on = 1; r.stage = st; r.dt = dt;
+    r.y = Phi; r.acc = ws->accP; r.out = SP[st % 2];
+    return r;
+  };
+  auto rkQ = [&](int st) {
+    wt::RKStage r;
+    r.on = 1; r.stage = st; r.dt = dt;
+    r.y = Pi; r.acc = ws->accQ; r.out = nullptr;  // Pi's stage value stays in the fused kernel's registers
+    return r;
+  };
+  ws->halo_cp = 0;
+  ws->flux_block = wt::n8_flux_block(m);
+  if (coef->td) WT_TRY(coef_resample(ctx, coef, toff[0], s));
+  prof_mark(ctx, 0);
+  WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, Phi, Pi, FB[0], nullptr, ws->bbuf, nullptr, use_metric, b, rkP(0), s,
+                                     true), "rk4 K1"));
+  prof_mark(ctx, 0);
+  ctx->launches += 1;
+  for (int st = 0; st < 3; ++st) {
+    if (coef->td) WT_TRY(coef_resample(ctx, coef, toff[st + 1], s));
+    prof_mark(ctx, 2);
+    WT_TRY(lrc(ctx, wt::launch_cons_fk_n8(m, coef->c, FB[st % 2], FB[(st + 1) % 2], SP[st % 2], ws->bbuf, b, rkQ(st),
+                                          rkP(st + 1), s), "rk4 fused stage"));
+    prof_mark(ctx, 2);
+    ctx->launches += 1;
+  }
+  prof_mark(ctx, 1);
+  WT_TRY(lrc(ctx, wt::launch_cons_k2(m, FB[1], nullptr, ws->bbuf, use_metric, b, rkQ(3), nullptr, s, true), "rk4 K2"));
+  prof_mark(ctx, 1);
+  ctx->launches += 1;
+  if (coef->td) {
+    WT_TRY(lrc(ctx, wt::launch_advance_time(coef->d_t, dt, s), "background time"));
+    ctx->launches += 1;
+  }
+  return 0;
+}
+
 static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
                             double eps_ko, const wt::ConsBC& b, int use_metric) {
+  if (fused_path(ws, coef, Phi, Pi, eps_ko, b, use_metric))
+    return step_curved_fused(ctx, ws, coef, Phi, Pi, dt, b, use_metric);
   const wt::DevMesh& m = ws->mesh->m;
   cudaStream_t s = ctx->stream;
   void* SP[2] = {ws->S0, ws->S1};
@@ -1539,6 +1613,11 @@ int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, v
   wt::ConsBC b;
   WT_TRY(make_bc(ctx, bc, use_metric, b));
   WT_TRY(ws_step_buffers(ws));
+  {  // the fused stages' second flux buffer (FP64 n = 8 whole-step calls only)
+    const wt::DevMesh& m = ws->mesh->m;
+    if (m.precision == WT_F64 && m.N == 8 && ws->fused && eps_ko == 0.0)
+      WT_TRY(ensure(ws, &ws->F2, 3 * (size_t)wt::n8_padded_field_size(m.Ne) * sizeof(double)));
+  }
   if (eps_ko != 0.0) WT_TRY(ensure_mu(ws));
   if (coef->td) WT_TRY(need_setup_geometry(coef->mesh, "wt_step_rk4_curved (time-dependent background)"));
   comp_track(ws, Phi, Pi);

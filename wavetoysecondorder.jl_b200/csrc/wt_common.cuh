@@ -235,6 +235,12 @@ int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const
                       void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s);
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
                       const RKStage& rk, unsigned* flag, cudaStream_t s);
+// Fused RK4 stage (FP64): K2 of stage rkQ.stage (0..2, F_s in Fin) and K1 of
+// stage rkP.stage = rkQ.stage + 1 (Phi_{s+1} in Phi, F_{s+1} into Fout) in one
+// launch; Fin and Fout must differ.  rkQ.out may be NULL (Pi's stage value is
+// then not stored).
+int launch_cons_fk_n8(const DevMesh& m, const DevCoef& c, const void* Fin, void* Fout, const void* Phi, void* bbuf,
+                      const ConsBC& bc, const RKStage& rkQ, const RKStage& rkP, cudaStream_t s);
 int launch_pad_metric_n8(DevMesh& m, cudaStream_t s);
 // FP32 meshes: m.Ja0 (element means of the FP64 metric terms) and m.dJa (FP32 deviations)
 int launch_split_metric(const DevMesh& m, cudaStream_t s);

@@ -1122,6 +1122,380 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
 }
 
 // ---------------------------------------------------------------------------
+// Fused RK4 stage kernel FK_s (FP64, n = 8): on each element, the K2 half of
+// stage s (split-form divergence of F_s, centred-flux SAT, boundary terms, the
+// Pi stage update) and the K1 half of stage s + 1 (split-form gradient of
+// Phi_{s+1}, flux F_{s+1}, boundary terms, the Phi stage update) -- the
+// integrator fused into the right-hand side (IDEAS.md:48-50 of the reference;
+// the arithmetic is that of wave3d_curved_rhs!, src/wave3d_curved.jl:205-258).
+// No grid-wide barrier is needed between the halves:
+//   * K2_s of element e reads F_s of e and of its neighbours' faces: all of F_s
+//     was written by the previous launch (F ping-pongs: this launch writes
+//     F_{s+1} into the other buffer while neighbours still read F_s);
+//   * K1_{s+1} of e reads Phi_{s+1} of e and of its neighbours' faces (written
+//     by the previous launch) and Pi_{s+1} of e only, which its own K2 half has
+//     just formed -- it stays in a register (one node per thread in both node
+//     passes), so Pi_{s+1} is never stored;
+//   * the boundary buffer: each thread reads its node's slots in the K2 half
+//     before the K1 half rewrites them.
+// Only the node passes depend on each other, so the two contraction passes run
+// side by side: warps 0-7 contract the divergence (tile w, both halves of its
+// fields, as the 256-thread k_cons_k2_n8<double>), warps 8-15 the gradient
+// (tile w - 8, all nine components); one barrier later every thread does the
+// divergence node pass and then the gradient node pass of its node.  Two CTA
+// barriers per element, as in one of the two-kernel launches.  The metric terms
+// Ja staged for the divergence are read by the gradient too, and 1/J once.  Per
+// node and stage the fused kernel moves 33 words against 44 for the two
+// kernels (F 3 + Ja 9 + 1/J 1 + Pi RK 3 + Phi 1 + coefficients 10 + Phi RK 3 +
+// F_{s+1} 3).
+// CTA: 512 threads, one per SM (217 KB of shared memory); the flux and metric
+// terms (12 blocks) in a two-stage ring, issued one element ahead; the ten
+// coefficient blocks (read only by the node pass) single-buffered, issued once
+// the previous element's node pass is done; neighbour face traces of F_s and
+// Phi_{s+1}, Phi_{s+1} itself, 1/J and the RK states are prefetched into
+// registers one element ahead.  Each partial sum is formed by the instructions
+// k_cons_k2_n8<double> and k_cons_k1_n8<double> use and added in their order,
+// so the fused step equals the two-kernel step bit for bit.
+struct FKN8 {
+  K2N8<double> a;  // stage s: F_s in (a.F0..F2), the Pi stage update
+  K1N8<double> b;  // stage s + 1: Phi_{s+1} in (b.Phi), F_{s+1} out (b.F), the Phi stage update
+};
+constexpr int FK_NA = 12;  // ring stage: F (3) + Ja (9) blocks
+constexpr size_t fk_smem() {
+  return (2 * FK_NA * 512 + 10 * 512 + 12 * 512 + 2 * 6 * 3 * 64 + 2 * 6 * 64 + 2 * 512) * sizeof(double) +
+         64 * sizeof(double) + 64;
+}
+static_assert(fk_smem() + 64 + 1024 <= 233472, "the fused stage kernel's CTA must fit an SM");
+
+// RK4 stage update of an FP64 field for stages 0..2 (n8_rk without the FP32
+// compensation) returning the stage value; it is also written to out unless out
+// is NULL (the fused step keeps Pi's stage value in a register and never reads
+// it back).
+__device__ __forceinline__ double n8_rk_out(int stage, double dt, double k, double yv, double accv, long long n,
+                                            double* acc, double* out) {
+  double o;
+  if (stage == 0) {
+    o = yv + (0.5 * dt) * k;
+    acc[n] = yv + (dt / 6.0) * k;
+  } else if (stage == 1) {
+    o = yv + (0.5 * dt) * k;
+    acc[n] = accv + (dt / 3.0) * k;
+  } else {
+    o = yv + dt * k;
+    acc[n] = accv + (dt / 3.0) * k;
+  }
+  if (out) out[n] = o;
+  return o;
+}
+
+__global__ void __launch_bounds__(n8::THREADS, 1) k_cons_fk_n8(const FKN8 P) {
+  using namespace n8;
+  using real = double;
+  constexpr int FS = Lay<double>::FS;
+  constexpr int NFACE = 6 * 3 * N2;                     // flux face values
+  constexpr int NFR = (NFACE + THREADS - 1) / THREADS;  // per thread
+  constexpr int NPF = 6 * N2;                           // Phi face values
+  const K2N8<double>& A = P.a;
+  const K1N8<double>& B = P.b;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  double* sG = reinterpret_cast<double*>(smraw);  // 64
+  double* stg = sG + N2;                          // 2 x 12 blocks: F (3), Ja (9)
+  double* sC = stg + 2 * FK_NA * FS;              // 10 coefficient blocks (node order)
+  double* sdiv = sC + 10 * N3;                    // 3 partial divergences [al] (Lay)
+  double* sg = sdiv + 3 * FS;                     // 9 partial gradients [al * 3 + c] (Lay)
+  double* sfF = sg + 9 * FS;                      // 2 x 1152 flux face traces [f][c][pq]
+  double* sfP = sfF + 2 * NFACE;                  // 2 x 384 Phi face traces [f][pq]
+  double* sphi = sfP + 2 * NPF;                   // 2 x 512 Phi_{s+1} (Lay)
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sphi + 2 * N3);  // [0], [1] ring, [2] coefficients
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gq = lane >> 2, tig = lane & 3, wt8 = warp & 7;
+  const bool divw = warp < 8;  // divergence-contraction warp (else gradient)
+  const real inv2H = (real)(1.0 / (2.0 * A.H[0]));
+  const int sa = A.stage, sb = B.stage;  // sb = sa + 1
+  const bool needQy = sa <= 2, needQacc = sa >= 1;
+  const bool needPy = sb == 1 || sb == 2;
+  const unsigned txA = (unsigned)(FK_NA * FS * sizeof(real)), txC = (unsigned)(10 * N3 * sizeof(real));
+  const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
+  const int tpad = Lay<real>::at(tid);
+  const long long T = A.Ne, GS = gridDim.x;
+
+  if (tid < N2) sG[tid] = A.G[tid];
+  if (tid == 0) {
+    abort_flag = 0;
+    for (int k = 0; k < 3; ++k) mbar_init(&bar[k], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  // warp 0: F_s and Ja of element e into ring stage s
+  auto issueA = [&](long long e, int s) {
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&bar[s], txA);
+    }
+    __syncwarp();
+    real* d = stg + s * FK_NA * FS;
+    if (lane < FK_NA) {
+      const real* src = lane < 3 ? (lane == 0 ? A.F0 : lane == 1 ? A.F1 : A.F2) + e * FS
+                                 : A.Ja + ((long long)(lane - 3) * A.Ne + e) * FS;
+      bulk_g2s(d + lane * FS, src, FS * (unsigned)sizeof(real), &bar[s]);
+    }
+  };
+  // warp 0: the ten coefficient blocks of element e
+  auto issueC = [&](long long e) {
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&bar[2], txC);
+    }
+    __syncwarp();
+    if (lane < 10) bulk_g2s(sC + lane * N3, B.c10 + lane * B.nn + e * N3, N3 * (unsigned)sizeof(real), &bar[2]);
+  };
+  // face sources of element e (-1: none or past the end), loaded one iteration
+  // before the traces they address
+  auto srcF_load = [&](long long e, int src[NFR]) {
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = tid + r * THREADS;
+      src[r] = (e < T && idx < NFACE) ? A.fsrc[idx / (3 * N2) + 6 * e] : -1;
+    }
+  };
+  auto srcP_load = [&](long long e) -> int { return (e < T && tid < NPF) ? B.fsrc[(tid >> 6) + 6 * e] : -1; };
+  auto faceF_load = [&](const int src[NFR], real fv[NFR]) {
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = tid + r * THREADS;
+      real v = 0;
+      if (src[r] >= 0) {
+        const int rem = idx % (3 * N2), c = rem >> 6, pq = rem & 63;
+        const real* Fc = c == 0 ? A.F0 : c == 1 ? A.F1 : A.F2;
+        v = Fc[(long long)(src[r] >> 6) * FS + Lay<real>::at(nbr_face_node(src[r], pq & 7, pq >> 3, N))];
+      }
+      fv[r] = v;
+    }
+  };
+  auto faceP_load = [&](int src) -> real {
+    if (src < 0) return (real)0;
+    const int pq = tid & 63;
+    return B.Phi[(long long)(src >> 6) * N3 + nbr_face_node(src, pq & 7, pq >> 3, N)];
+  };
+  struct PW {
+    real invJ, Qy, Qacc, phi, Py, Pacc;
+  };
+  auto pw_load = [&](long long e, PW& w) {
+    const long long n = e * N3 + tid;
+    w.invJ = A.invdetJ[n];
+    w.Qy = needQy ? A.y[n] : (real)0;
+    w.Qacc = needQacc ? A.acc[n] : (real)0;
+    w.phi = B.Phi[n];
+    w.Py = needPy ? B.y[n] : (real)0;
+    w.Pacc = B.acc[n];  // stage s + 1 >= 1 reads the accumulator
+  };
+
+  PW cur;
+  int emcur = 0, srcF1[NFR], srcP1 = -1;
+#pragma unroll
+  for (int r = 0; r < NFR; ++r) srcF1[r] = -1;
+  {
+    const long long t0 = blockIdx.x;
+    if (t0 < T) {
+      if (warp == 0) issueA(t0, 0);
+      emcur = A.emask[t0];
+      int s0[NFR];
+      srcF_load(t0, s0);
+      real fv[NFR];
+      faceF_load(s0, fv);
+#pragma unroll
+      for (int r = 0; r < NFR; ++r)
+        if (tid + r * THREADS < NFACE) sfF[tid + r * THREADS] = fv[r];
+      const real pv = faceP_load(srcP_load(t0));
+      if (tid < NPF) sfP[tid] = pv;
+      pw_load(t0, cur);
+      sphi[tpad] = cur.phi;
+      srcF_load(t0 + GS, srcF1);
+      srcP1 = srcP_load(t0 + GS);
+    }
+  }
+  __syncthreads();
+  const double aG0 = sG[gq * 8 + tig], aG1 = sG[gq * 8 + 4 + tig];
+
+  int it = 0;
+  for (long long t = blockIdx.x; t < T; t += GS, ++it) {
+    const int s = it & 1, fb = it & 1;
+    const unsigned parity = (it >> 1) & 1;
+    const long long t1 = t + GS;
+    const bool has_next = t1 < T;
+    const int emnext = has_next ? A.emask[t1] : 0;
+    int srcF2[NFR];
+    srcF_load(t + 2 * GS, srcF2);
+    const int srcP2 = srcP_load(t + 2 * GS);
+    real fnext[NFR];
+    faceF_load(srcF1, fnext);  // srcF1 is -1 everywhere past the end
+    const real pnext = faceP_load(srcP1);
+    PW nxt;
+    if (has_next) pw_load(t1, nxt);
+    if (tid == 0 && !wait_phase(&bar[s], parity, A.flag)) abort_flag = 1;
+    // every thread has finished the previous element: ring stage s ^ 1, the
+    // coefficient buffer and the face / Phi buffers fb ^ 1 are free
+    __syncthreads();
+    if (abort_flag) return;  // no copy of this CTA is in flight (the coefficient copy was waited for)
+    if (warp == 0) {
+      issueC(t);
+      if (has_next) issueA(t1, s ^ 1);
+    }
+    const long long e = t;
+    const real* d = stg + s * FK_NA * FS;
+    const real* sF = d;
+    const real* sJa = d + 3 * FS;
+    const int mask = emcur & 63, bnd = emcur >> 6;
+
+    if (divw) {
+      // ---- divergence of F_s (K2 half), tile wt8: per axis the two halves of its
+      // fields, added in registers into sdiv[al] ----
+      const real* sfc = sfF + fb * NFACE;
+#pragma unroll
+      for (int al = 0; al < 3; ++al) {
+        const real* m0 = sJa + (al * 3 + 0) * FS;
+        const real* m1 = sJa + (al * 3 + 1) * FS;
+        const real* m2 = sJa + (al * 3 + 2) * FS;
+        real rsum[2] = {0, 0};
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
+          double dx[2] = {0, 0}, dy[2] = {0, 0};
+#pragma unroll
+          for (int kc = 0; kc < 2; ++kc) {
+            const int nd = Lay<real>::at(bnode(al, wt8, kc, gq, tig));
+            const double a = kc ? aG1 : aG0;
+            if (hh == 0) {
+              const double f0 = sF[nd];
+              const double ft = m0[nd] * f0 + m1[nd] * sF[FS + nd] + m2[nd] * sF[2 * FS + nd];
+              dmma(dx[0], dx[1], a, ft);
+              dmma(dy[0], dy[1], a, f0);
+            } else {
+              dmma(dx[0], dx[1], a, sF[FS + nd]);
+              dmma(dy[0], dy[1], a, sF[2 * FS + nd]);
+            }
+          }
+          const int sface_f = gq == 0 ? 2 * al : gq == 7 ? 2 * al + 1 : -1;
+          const bool sat = hh == 1 && sface_f >= 0 && ((mask >> sface_f) & 1);
+#pragma unroll
+          for (int b = 0; b < 2; ++b) {
+            const int no = Lay<real>::at(onode(al, wt8, b, gq, tig));
+            real r;
+            if (hh == 0) {
+              r = (real)0.5 * dx[b] + (real)0.5 * m0[no] * dy[b];
+            } else {
+              r = (real)0.5 * m1[no] * dx[b] + (real)0.5 * m2[no] * dy[b];
+            }
+            if (sat) {
+              const int pq = opq(al, wt8, b, tig);
+              const real sacc = m0[no] * (sfc[(sface_f * 3 + 0) * N2 + pq] - sF[no]) +
+                                m1[no] * (sfc[(sface_f * 3 + 1) * N2 + pq] - sF[FS + no]) +
+                                m2[no] * (sfc[(sface_f * 3 + 2) * N2 + pq] - sF[2 * FS + no]);
+              r += (gq ? inv2H : -inv2H) * sacc;
+            }
+            rsum[b] = hh ? rsum[b] + r : r;
+          }
+        }
+#pragma unroll
+        for (int b = 0; b < 2; ++b) sdiv[al * FS + Lay<real>::at(onode(al, wt8, b, gq, tig))] = rsum[b];
+      }
+    } else {
+      // ---- split-form gradient of Phi_{s+1} (K1 half), tile wt8: all nine partials ----
+      const real* sPhi = sphi + fb * N3;
+      const real* sfc = sfP + fb * NPF;
+#pragma unroll 1
+      for (int al = 0; al < 3; ++al) {
+        double du[2] = {0, 0}, dm[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+#pragma unroll
+        for (int kc = 0; kc < 2; ++kc) {
+          const int nd = Lay<real>::at(bnode(al, wt8, kc, gq, tig));
+          const double u = sPhi[nd];
+          const double a = kc ? aG1 : aG0;
+          dmma(du[0], du[1], a, u);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) dmma(dm[c][0], dm[c][1], a, sJa[(al * 3 + c) * FS + nd] * u);
+        }
+        const int sface_f = gq == 0 ? 2 * al : gq == 7 ? 2 * al + 1 : -1;
+        const bool sat = sface_f >= 0 && ((mask >> sface_f) & 1);
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          const int no = Lay<real>::at(onode(al, wt8, b, gq, tig));
+          real jump = 0;
+          if (sat) jump = (gq ? inv2H : -inv2H) * (sfc[sface_f * N2 + opq(al, wt8, b, tig)] - sPhi[no]);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const real m = sJa[(al * 3 + c) * FS + no];
+            real r = (real)0.5 * dm[c][b] + (real)0.5 * m * du[b];
+            if (sat) r += m * jump;
+            sg[(al * 3 + c) * FS + no] = r;
+          }
+        }
+      }
+    }
+    if (tid == 0 && !wait_phase(&bar[2], (unsigned)(it & 1), A.flag)) abort_flag = 1;
+    __syncthreads();
+    if (abort_flag) {  // wait (bounded) for the next element's ring copy, then leave
+      if (tid == 0 && has_next) wait_phase(&bar[s ^ 1], ((it + 1) >> 1) & 1, nullptr);
+      return;
+    }
+    {
+      const long long n = e * N3 + tid;
+      // ---- divergence node pass: boundary terms, Pi stage update (K2 half) ----
+      real dv = (sdiv[tpad] + sdiv[FS + tpad]) + sdiv[2 * FS + tpad];
+      dv *= cur.invJ;
+      if (bnd && A.bc_on) {
+        const int idx3[3] = {ti, tj, tk};
+        for (int f = 0; f < 6; ++f) {
+          if (A.bdry[f + 6 * e] == 0) continue;
+          const int ax = f >> 1;
+          if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
+          const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
+          dv += A.bbuf[(long long)A.bslot[f + 6 * e] * N2 + p + 8 * q];
+        }
+      }
+      const real Pi = n8_rk_out(sa, A.dt, dv, cur.Qy, cur.Qacc, n, A.acc, A.out);  // Pi_{s+1}
+      // ---- gradient node pass: flux F_{s+1}, Phidot, boundary terms, Phi stage update (K1 half) ----
+      const real u = cur.phi;
+      real g0 = (sg[tpad] + sg[3 * FS + tpad]) + sg[6 * FS + tpad];
+      real g1 = (sg[FS + tpad] + sg[4 * FS + tpad]) + sg[7 * FS + tpad];
+      real g2 = (sg[2 * FS + tpad] + sg[5 * FS + tpad]) + sg[8 * FS + tpad];
+      g0 *= cur.invJ; g1 *= cur.invJ; g2 *= cur.invJ;
+      real cc[10];
+#pragma unroll
+      for (int c = 0; c < 10; ++c) cc[c] = sC[c * N3 + tid];
+      const real a = cc[0];
+      const real b0 = cc[1], b1 = cc[2], b2 = cc[3];
+      const real K0 = cc[4], K1v = cc[5], K2 = cc[6], K3 = cc[7], K4 = cc[8], K5 = cc[9];
+      const real F0 = b0 * Pi + (K0 * g0 + K1v * g1 + K2 * g2);
+      const real F1 = b1 * Pi + (K1v * g0 + K3 * g1 + K4 * g2);
+      const real F2 = b2 * Pi + (K2 * g0 + K4 * g1 + K5 * g2);
+      real phid = b0 * g0 + b1 * g1 + b2 * g2 + a * Pi;
+      if (bnd && B.bc_on) k1_boundary<real>(B, e, ti, tj, tk, n, u, Pi, g0, g1, g2, cc, phid);
+      {
+        const long long fo = e * FS + tpad, fstr = B.Ne * FS;
+        B.F[fo] = F0;
+        B.F[fstr + fo] = F1;
+        B.F[2 * fstr + fo] = F2;
+      }
+      n8_rk<real>(sb, B.dt, phid, u, cur.Py, cur.Pacc, (real)0, n, B.y, B.acc, B.out, nullptr, B.flag);
+    }
+    if (has_next) {
+#pragma unroll
+      for (int r = 0; r < NFR; ++r)
+        if (tid + r * THREADS < NFACE) sfF[(fb ^ 1) * NFACE + tid + r * THREADS] = fnext[r];
+      if (tid < NPF) sfP[(fb ^ 1) * NPF + tid] = pnext;
+      sphi[(fb ^ 1) * N3 + tpad] = nxt.phi;
+    }
+    cur = nxt;
+    emcur = emnext;
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) srcF1[r] = srcF2[r];
+    srcP1 = srcP2;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // FP32 CUDA-core form (WT_FP32_CUDA_CORES) of the two n = 8 kernels: one
 // thread per (axis, pencil) -- 3 x 64 = 192 threads -- does the 8x8
 // contractions of its pencil as FFMAs whose operator entries come from the
@@ -2004,6 +2378,25 @@ int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const
   }
   const K1N8<float> P = k1n8_params<float>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag);
   return n8_dispatch<false>(1, 1, m.fp32_form, &P, nullptr, nullptr, m.Ne, s);
+}
+
+int launch_cons_fk_n8(const DevMesh& m, const DevCoef& c, const void* Fin, void* Fout, const void* Phi, void* bbuf,
+                      const ConsBC& bc, const RKStage& rkQ, const RKStage& rkP, cudaStream_t s) {
+  if (m.precision != 0 || rkQ.stage < 0 || rkQ.stage > 2 || rkP.stage != rkQ.stage + 1 || !rkQ.on || !rkP.on)
+    return -4;
+  FKN8 P;
+  P.a = k2n8_params<double>(m, Fin, nullptr, bbuf, bc, rkQ, m.errflag);
+  P.b = k1n8_params<double>(m, c, Phi, nullptr, Fout, nullptr, bbuf, bc, rkP, m.errflag);
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_cons_fk_n8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fk_smem()) != cudaSuccess)
+      return -2;
+    attr = true;
+  }
+  const long long cap = sm_count(), grid = m.Ne < cap ? m.Ne : cap;
+  if (grid <= 0) return 0;
+  k_cons_fk_n8<<<(unsigned)grid, n8::THREADS, fk_smem(), s>>>(P);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,

@@ -152,11 +152,11 @@ def library():
         "wt_initial_data": [vp, vp, i, vp, i, d, vp, vp],
         "wt_initial_state": [vp, vp, i, vp, i, d, vp, vp], "wt_state_set_f64": [vp, vp, vp, vp, vp, vp],
         "wt_gll_operators": [i, vp, vp, vp],
-        "wt_ctx_profile": [vp, i], "wt_ctx_profile_read": [vp, C.POINTER(d * 2), C.POINTER(ll * 2)],
+        "wt_ctx_profile": [vp, i], "wt_ctx_profile_read": [vp, C.POINTER(d * 3), C.POINTER(ll * 3)],
         "wt_mesh_create_slab": [vp, C.POINTER(_MeshDesc), i, i, pvp],
         "wt_rk4_stage_curved": [vp, vp, vp, vp, vp, d, i, i, C.POINTER(_BcDesc), i],
         "wt_halo_size": [vp, C.POINTER(ll)], "wt_halo_copy": [vp, vp, vp, i, i, vp, i],
-        "wt_workspace_set_mu": [vp, d],
+        "wt_workspace_set_mu": [vp, d], "wt_workspace_set_fused": [vp, i],
         "wt_rk4_stage_curved_ko": [vp, vp, vp, vp, vp, d, i, d, C.POINTER(_BcDesc), i],
         "wt_halo_state_copy": [vp, vp, vp, vp, i, i, i, vp, i],
         "wt_serve_create": [vp, C.POINTER(_ServeDesc), pvp], "wt_serve_destroy": [vp],
@@ -234,11 +234,11 @@ class Context:
         self.check(library().wt_ctx_profile(self.h, int(enable)))
 
     def profile_read(self):
-        """((K1 ms, K1 launches), (K2 ms, K2 launches)) since the last read."""
-        ms = (C.c_double * 2)()
-        cnt = (C.c_longlong * 2)()
+        """((K1 ms, K1 launches), (K2 ms, K2 launches), (fused-stage ms, launches)) since the last read."""
+        ms = (C.c_double * 3)()
+        cnt = (C.c_longlong * 3)()
         self.check(library().wt_ctx_profile_read(self.h, C.byref(ms), C.byref(cnt)))
-        return (ms[0], cnt[0]), (ms[1], cnt[1])
+        return (ms[0], cnt[0]), (ms[1], cnt[1]), (ms[2], cnt[2])
 
     def selftest_wait(self, arrive: bool, polls: int = 1 << 16):
         """Run the bounded-wait self-test (wt_ctx_selftest_wait): raises WaveToyError
@@ -509,6 +509,11 @@ class Workspace(_Child):
         """Impose mu (wt_workspace_set_mu): the slabs of a partitioned solve take the whole mesh's."""
         self.ctx.check(library().wt_workspace_set_mu(self.h, float(mu)), "wt_workspace_set_mu")
         self._mu = float(mu)
+
+    def set_fused(self, on: bool = True):
+        """FP64 n = 8 RK4 steps through the fused stage kernel (wt_workspace_set_fused; the
+        default) or through the two-kernel stages (on=False); the results are equal bit for bit."""
+        self.ctx.check(library().wt_workspace_set_fused(self.h, int(bool(on))), "wt_workspace_set_fused")
 
     @property
     def inv_mu5(self) -> float:
