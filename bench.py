@@ -309,6 +309,38 @@ def run_ours(args):
     ref = None
     if study:  # the FP64 state after warmup + timed steps: the reference of the FP32 forms
         ref = (torch.cat([Phi, Pi]), wt.wave3d_energy(Phi, Pi, coef, ws, metric=True))
+    alt = None
+    if prec == wt.WT_F64 and N == 8:
+        # the other stage form of the FP64 n = 8 step (fused stage kernel <-> two-kernel
+        # stages), timed right after on copies of the state, so that both forms are
+        # measured on the same GPU at nearly the same clocks
+        P2, Q2 = Phi.clone(), Pi.clone()
+        ws.set_fused(args.unfused)
+        for _ in range(args.warmup):
+            wt.step_rk4_curved(P2, Q2, coef, ws, dt, 1, eps_KO=0.0, bc3d=bc, metric=True)
+        torch.cuda.synchronize()
+        asampler = ClockSampler(local)
+        asampler.start()
+        time.sleep(0.3)
+        ctx.profile(True)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(args.steps):
+            wt.step_rk4_curved(P2, Q2, coef, ws, dt, 1, eps_KO=0.0, bc3d=bc, metric=True)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ctx.profile(False)
+        aclocks = asampler.stop()
+        pa = ctx.profile_read()
+        ta = a0.elapsed_time(a1) / 1000.0
+        alt = {"form": "fused stage kernel (wt_workspace_set_fused)" if args.unfused else "two-kernel stages",
+               "value": 2.0 * nn * args.steps / ta, "unit": "DOF-updates/s", "ms_per_step": 1000.0 * ta / args.steps,
+               "ratio_to_value": (2.0 * nn * args.steps / ta) / (2.0 * nn * args.steps / (t_ms / 1000.0)),
+               "kernels_ms_per_launch": {k: (m / n if n else None) for k, (m, n) in
+                                         zip(("k_cons_k1", "k_cons_k2", "k_cons_fk_n8"), pa)},
+               "clocks": aclocks}
+        ws.set_fused(not args.unfused)
+        del P2, Q2
 
     # end to end through the host-buffer API (wt_evolve_curved_host, the shape of
     # evolve3d): page-locked host state in, one RK4 step per sample, state and
@@ -406,6 +438,8 @@ def run_ours(args):
                           "definition": "w (34 + 4 C) bytes per node per RK4 step, C = 20 streamed coefficient words"},
         "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "finite": finite,
     }
+    if alt is not None:
+        line["other_stage_form"] = alt
     if study:
         # the precision study of the large solve: every FP32 form on the same workload,
         # timed like the FP64 form and compared with its state after the same steps

@@ -288,10 +288,10 @@ int wt_workspace_set_mu(wt_ws* ws, double mu);
  * no entry point of its own there): with on = 1 (the default) an FP64 n = 8
  * solve without Kreiss-Oliger dissipation steps through the fused stage kernel,
  * which runs the divergence half of stage s and the gradient half of stage
- * s + 1 in one launch (five launches per RK4 step instead of eight, a quarter
- * fewer bytes).  The results equal the two-kernel stages' bit for bit; on = 0
- * selects the two-kernel stages (for comparison).  Takes effect at the next
- * step call; the second flux buffer (3 x 8 bytes per node) is allocated then. */
+ * s + 1 in one launch (five launches per RK4 step instead of eight, 28 % fewer
+ * DRAM bytes).  The results equal the two-kernel stages' bit for bit; on = 0
+ * selects the two-kernel stages.  Takes effect at the next step call; the
+ * second flux buffer (3 x 8 bytes per node) is allocated then. */
 int wt_workspace_set_fused(wt_ws* ws, int on);
 
 /* ---- right-hand sides (device pointers, async) ------------------------------*/

@@ -6,9 +6,9 @@ of stage s and the gradient half of stage s + 1 on every element, then K2_3
 (the integrator fused into the right-hand side, the reference's IDEAS.md:48-50;
 arithmetic of wave3d_curved_rhs!, src/wave3d_curved.jl:205-258).  Each half
 repeats the arithmetic of its two-kernel counterpart in the same order, so the
-fused and the two-kernel steps must agree bit for bit; both are held to the
-oracle at <= 1e-12 (the default path, which is the fused one, is also what the
-other FP64 n = 8 stepping tests run).
+fused and the two-kernel steps must agree bit for bit; the fused step (the
+default, so also what the other FP64 n = 8 stepping tests run) is held to the
+oracle at <= 1e-12.
 """
 import numpy as np
 import pytest

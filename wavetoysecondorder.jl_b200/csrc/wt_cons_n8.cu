@@ -1152,10 +1152,16 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
 // terms (12 blocks) in a two-stage ring, issued one element ahead; the ten
 // coefficient blocks (read only by the node pass) single-buffered, issued once
 // the previous element's node pass is done; neighbour face traces of F_s and
-// Phi_{s+1}, Phi_{s+1} itself, 1/J and the RK states are prefetched into
-// registers one element ahead.  Each partial sum is formed by the instructions
-// k_cons_k2_n8<double> and k_cons_k1_n8<double> use and added in their order,
-// so the fused step equals the two-kernel step bit for bit.
+// Phi_{s+1} and Phi_{s+1} itself by per-thread cp.async one element ahead; 1/J
+// and the RK states prefetched into registers one element ahead.  Each partial
+// sum is formed by the instructions k_cons_k2_n8<double> and
+// k_cons_k1_n8<double> use and added in their order, so the fused step equals
+// the two-kernel step bit for bit.
+// Measured on the 64^3 x 8^3 solve: 262 DRAM bytes per node and launch (the two
+// kernels: 364); the RK4 step 5-7 % faster than the two-kernel step timed right
+// after it on the same GPU.  The kernels are bound by latency and issue (16
+// warps per SM, about 41 % issue active) rather than by DRAM bandwidth, so
+// the gain is smaller than the bytes saved.
 struct FKN8 {
   K2N8<double> a;  // stage s: F_s in (a.F0..F2), the Pi stage update
   K1N8<double> b;  // stage s + 1: Phi_{s+1} in (b.Phi), F_{s+1} out (b.F), the Phi stage update
@@ -1166,6 +1172,19 @@ constexpr size_t fk_smem() {
          64 * sizeof(double) + 64;
 }
 static_assert(fk_smem() + 64 + 1024 <= 233472, "the fused stage kernel's CTA must fit an SM");
+
+namespace n8 {
+// per-thread 8-byte asynchronous copy global -> shared, zero-filled when !valid
+// (src must still be a valid address); commit / wait for all groups but the
+// newest / wait for all (cp_async_wait_all)
+__device__ __forceinline__ void cp_async8z(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+}  // namespace n8
 
 // RK4 stage update of an FP64 field for stages 0..2 (n8_rk without the FP32
 // compensation) returning the stage value; it is also written to out unless out
@@ -1280,14 +1299,13 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_fk_n8(const FKN8 P) {
     return B.Phi[(long long)(src >> 6) * N3 + nbr_face_node(src, pq & 7, pq >> 3, N)];
   };
   struct PW {
-    real invJ, Qy, Qacc, phi, Py, Pacc;
+    real invJ, Qy, Qacc, Py, Pacc;
   };
   auto pw_load = [&](long long e, PW& w) {
     const long long n = e * N3 + tid;
     w.invJ = A.invdetJ[n];
     w.Qy = needQy ? A.y[n] : (real)0;
     w.Qacc = needQacc ? A.acc[n] : (real)0;
-    w.phi = B.Phi[n];
     w.Py = needPy ? B.y[n] : (real)0;
     w.Pacc = B.acc[n];  // stage s + 1 >= 1 reads the accumulator
   };
@@ -1311,7 +1329,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_fk_n8(const FKN8 P) {
       const real pv = faceP_load(srcP_load(t0));
       if (tid < NPF) sfP[tid] = pv;
       pw_load(t0, cur);
-      sphi[tpad] = cur.phi;
+      sphi[tpad] = B.Phi[t0 * N3 + tid];
       srcF_load(t0 + GS, srcF1);
       srcP1 = srcP_load(t0 + GS);
     }
@@ -1329,16 +1347,48 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_fk_n8(const FKN8 P) {
     int srcF2[NFR];
     srcF_load(t + 2 * GS, srcF2);
     const int srcP2 = srcP_load(t + 2 * GS);
-    real fnext[NFR];
-    faceF_load(srcF1, fnext);  // srcF1 is -1 everywhere past the end
-    const real pnext = faceP_load(srcP1);
+    // the next element's neighbour face traces and its Phi_{s+1} go straight into
+    // the buffers fb ^ 1 by per-thread asynchronous copies (zero-filled where a
+    // face has no neighbour; srcF1, srcP1 are -1 past the end); the previous
+    // group -- this element's -- is complete after the wait, and visible to
+    // every thread after the barrier below
+    {
+      double* dF = sfF + (fb ^ 1) * NFACE;
+#pragma unroll
+      for (int r = 0; r < NFR; ++r) {
+        const int idx = tid + r * THREADS;
+        if (idx < NFACE) {
+          const real* g = A.F0;
+          if (srcF1[r] >= 0) {
+            const int rem = idx % (3 * N2), c = rem >> 6, pq = rem & 63;
+            const real* Fc = c == 0 ? A.F0 : c == 1 ? A.F1 : A.F2;
+            g = Fc + (long long)(srcF1[r] >> 6) * FS + Lay<real>::at(nbr_face_node(srcF1[r], pq & 7, pq >> 3, N));
+          }
+          cp_async8z(dF + idx, g, srcF1[r] >= 0);
+        }
+      }
+      if (tid < NPF) {
+        const real* g = B.Phi;
+        if (srcP1 >= 0) {
+          const int pq = tid & 63;
+          g = B.Phi + (long long)(srcP1 >> 6) * N3 + nbr_face_node(srcP1, pq & 7, pq >> 3, N);
+        }
+        cp_async8z(sfP + (fb ^ 1) * NPF + tid, g, srcP1 >= 0);
+      }
+      cp_async8z(sphi + (fb ^ 1) * N3 + tpad, B.Phi + (has_next ? t1 : t) * N3 + tid, has_next);
+      cp_async_commit();
+      cp_async_wait_prior();
+    }
     PW nxt;
     if (has_next) pw_load(t1, nxt);
     if (tid == 0 && !wait_phase(&bar[s], parity, A.flag)) abort_flag = 1;
     // every thread has finished the previous element: ring stage s ^ 1, the
     // coefficient buffer and the face / Phi buffers fb ^ 1 are free
     __syncthreads();
-    if (abort_flag) return;  // no copy of this CTA is in flight (the coefficient copy was waited for)
+    if (abort_flag) {  // no bulk copy of this CTA is in flight (the coefficient copy was waited for)
+      cp_async_wait_all();
+      return;
+    }
     if (warp == 0) {
       issueC(t);
       if (has_next) issueA(t1, s ^ 1);
@@ -1404,7 +1454,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_fk_n8(const FKN8 P) {
       // ---- split-form gradient of Phi_{s+1} (K1 half), tile wt8: all nine partials ----
       const real* sPhi = sphi + fb * N3;
       const real* sfc = sfP + fb * NPF;
-#pragma unroll 1
+#pragma unroll
       for (int al = 0; al < 3; ++al) {
         double du[2] = {0, 0}, dm[3][2] = {{0, 0}, {0, 0}, {0, 0}};
 #pragma unroll
@@ -1437,6 +1487,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_fk_n8(const FKN8 P) {
     __syncthreads();
     if (abort_flag) {  // wait (bounded) for the next element's ring copy, then leave
       if (tid == 0 && has_next) wait_phase(&bar[s ^ 1], ((it + 1) >> 1) & 1, nullptr);
+      cp_async_wait_all();
       return;
     }
     {
@@ -1456,7 +1507,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_fk_n8(const FKN8 P) {
       }
       const real Pi = n8_rk_out(sa, A.dt, dv, cur.Qy, cur.Qacc, n, A.acc, A.out);  // Pi_{s+1}
       // ---- gradient node pass: flux F_{s+1}, Phidot, boundary terms, Phi stage update (K1 half) ----
-      const real u = cur.phi;
+      const real u = sphi[fb * N3 + tpad];
       real g0 = (sg[tpad] + sg[3 * FS + tpad]) + sg[6 * FS + tpad];
       real g1 = (sg[FS + tpad] + sg[4 * FS + tpad]) + sg[7 * FS + tpad];
       real g2 = (sg[2 * FS + tpad] + sg[5 * FS + tpad]) + sg[8 * FS + tpad];
@@ -1479,13 +1530,6 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_fk_n8(const FKN8 P) {
         B.F[2 * fstr + fo] = F2;
       }
       n8_rk<real>(sb, B.dt, phid, u, cur.Py, cur.Pacc, (real)0, n, B.y, B.acc, B.out, nullptr, B.flag);
-    }
-    if (has_next) {
-#pragma unroll
-      for (int r = 0; r < NFR; ++r)
-        if (tid + r * THREADS < NFACE) sfF[(fb ^ 1) * NFACE + tid + r * THREADS] = fnext[r];
-      if (tid < NPF) sfP[(fb ^ 1) * NPF + tid] = pnext;
-      sphi[(fb ^ 1) * N3 + tpad] = nxt.phi;
     }
     cur = nxt;
     emcur = emnext;
@@ -1524,7 +1568,6 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src, bool valid
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 // index into a per-CTA table of the 6 x 64 face nodes for face source fs and
 // this face's point pq: the neighbour face's point after the orientation
 __device__ __forceinline__ int face_slot(int fs, int pq) {

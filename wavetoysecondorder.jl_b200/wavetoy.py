@@ -511,8 +511,8 @@ class Workspace(_Child):
         self._mu = float(mu)
 
     def set_fused(self, on: bool = True):
-        """FP64 n = 8 RK4 steps through the fused stage kernel (wt_workspace_set_fused; the
-        default) or through the two-kernel stages (on=False); the results are equal bit for bit."""
+        """FP64 n = 8 RK4 steps through the fused stage kernel (wt_workspace_set_fused; the default)
+        or through the two-kernel stages (on=False); the results are equal bit for bit."""
         self.ctx.check(library().wt_workspace_set_fused(self.h, int(bool(on))), "wt_workspace_set_fused")
 
     @property
