@@ -154,6 +154,89 @@ __device__ __forceinline__ void rk_epilogue_cp(int stage, double dt, float k, fl
   }
 }
 
+// Per-thread asynchronous copy of one word (4 or 8 bytes) global -> shared,
+// and the wait for all of this thread's copies.  The generic kernels copy the
+// words their node pass reads at their own node (coefficients, Pi, RK state)
+// at kernel start, so that those loads run under the contraction; each thread
+// reads back only its own words, so the wait needs no CTA barrier.
+template <typename T>
+__device__ __forceinline__ void cp_async_word(T* dst, const T* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_own() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// The RK4 stage updates above with the words they read at node n passed in
+// (yv = y[n], accv = acc[n], compv = comp[n]; only those the stage reads need
+// to be valid): the same arithmetic in the same order.
+template <typename real>
+__device__ __forceinline__ void rk_epilogue_v(int stage, double dt, real k, real yin, real yv, real accv, real compv,
+                                              real* y, real* acc, real* out, real* comp, long long n,
+                                              unsigned int* nonfinite) {
+  if (comp) {
+    if (stage == 0) {
+      out[n] = yin + (real)(0.5 * dt) * k;
+      acc[n] = (real)(dt / 6.0) * k;
+    } else if (stage == 1) {
+      out[n] = yv + (real)(0.5 * dt) * k;
+      acc[n] = accv + (real)(dt / 3.0) * k;
+    } else if (stage == 2) {
+      out[n] = yv + (real)dt * k;
+      acc[n] = accv + (real)(dt / 3.0) * k;
+    } else {
+      const real inc = accv + (real)(dt / 6.0) * k;
+      const real t = inc + compv;
+      const real v = yv + t;
+      comp[n] = t - (v - yv);
+      y[n] = v;
+      if (nonfinite && !isfinite((double)v)) atomicOr(nonfinite, 1u);
+    }
+    return;
+  }
+  if (stage == 0) {
+    out[n] = yin + (real)(0.5 * dt) * k;
+    acc[n] = yin + (real)(dt / 6.0) * k;
+  } else if (stage == 1) {
+    out[n] = yv + (real)(0.5 * dt) * k;
+    acc[n] = accv + (real)(dt / 3.0) * k;
+  } else if (stage == 2) {
+    out[n] = yv + (real)dt * k;
+    acc[n] = accv + (real)(dt / 3.0) * k;
+  } else {
+    real v = accv + (real)(dt / 6.0) * k;
+    y[n] = v;
+    if (nonfinite && !isfinite((double)v)) atomicOr(nonfinite, 1u);
+  }
+}
+
+// rk_epilogue_cp with lov = comp[n] and accv = acc[n] passed in
+__device__ __forceinline__ void rk_epilogue_cp_v(int stage, double dt, float k, float hi, float lov, float accv,
+                                                 float* y, float* acc, float* out, float* comp, float* hcopy,
+                                                 long long n, unsigned int* nonfinite) {
+  const float lo = lov;
+  if (stage == 0) {
+    out[n] = lo + (float)(0.5 * dt) * k;
+    acc[n] = (float)(dt / 6.0) * k;
+  } else if (stage == 1) {
+    out[n] = lo + (float)(0.5 * dt) * k;
+    acc[n] = accv + (float)(dt / 3.0) * k;
+  } else if (stage == 2) {
+    out[n] = lo + (float)dt * k;
+    acc[n] = accv + (float)(dt / 3.0) * k;
+    hcopy[n] = hi;
+  } else {
+    const float inc = accv + (float)(dt / 6.0) * k;
+    const double v = (double)hi + ((double)lo + (double)inc);
+    const float h = (float)v;
+    y[n] = h;
+    comp[n] = (float)(v - (double)h);
+    if (nonfinite && !isfinite(h)) atomicOr(nonfinite, 1u);
+  }
+}
+
 // contraction along axis d of a smem field f (N^3) with transposed G (GT[p*N+i] = G[i][p])
 template <int N, typename real>
 __device__ __forceinline__ real contract(const real* __restrict__ f, const real* __restrict__ GT, int i, int j, int k,
@@ -221,6 +304,25 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_, GenOcc<Ep<N>::N3 * EPB_>::va
   if constexpr (CP) {
     if (tid < N2) GTr[(tid % N) * N + tid / N] = (real)P.G[tid];
   }
+  // the node pass's own-node words, copied now (cp.async) so that their loads run
+  // under the contraction: c10 [0..9], Pi [10], RK state y [11], acc [12],
+  // comp [13] (only the words this stage's update reads)
+  constexpr bool PF = 14 * N3 * EPB * sizeof(real) <= 24576;
+  __shared__ real spf[PF ? EPB : 1][PF ? 14 : 1][PF ? N3 : 1];
+  const bool grad_only = P.c10 == nullptr;
+  const bool pf_y = P.epi && (P.stage == 1 || P.stage == 2 || (!CP && P.comp && P.stage == 3));
+  const bool pf_acc = P.epi && P.stage >= 1;
+  const bool pf_comp = P.epi && (CP || (P.comp && P.stage == 3));
+  if constexpr (PF) {
+    if (valid && !grad_only) {
+#pragma unroll
+      for (int c = 0; c < 10; ++c) cp_async_word(&spf[le][c][t], P.c10 + c * nn + n);
+      cp_async_word(&spf[le][10][t], P.Pi + n);
+      if (pf_y) cp_async_word(&spf[le][11][t], P.y + n);
+      if (pf_acc) cp_async_word(&spf[le][12][t], P.acc + n);
+      if (pf_comp) cp_async_word(&spf[le][13][t], P.comp + n);
+    }
+  }
   const real u = valid ? P.Phi[n] : (real)0;  // CP: the high part
   gt ug = u;                                   // the value the gradient differentiates
   if constexpr (CP) {
@@ -229,12 +331,13 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_, GenOcc<Ep<N>::N3 * EPB_>::va
   su[le][t] = ug;
   // element tables: SAT mask / outer-face flag, and the neighbour face sources
   const int emask = valid ? P.emask[ec] : 0;
-  // neighbour Phi face traces
+  // neighbour Phi face traces (fsrc is -1 exactly where the SAT mask bit is 0,
+  // so the trace loads need not wait for the mask)
   for (int idx = t; idx < 6 * N2; idx += N3) {
     const int f = idx / N2, pq = idx - f * N2;
     gt v = 0;
-    if ((emask >> f) & 1) {
-      const int src = P.fsrc[f + 6 * ec];
+    const int src = valid ? P.fsrc[f + 6 * ec] : -1;
+    if (src >= 0) {
       const long long nb = (long long)(src >> 6) * N3 + nbr_face_node(src, pq % N, pq / N, N);
       v = P.Phi[nb];
       if constexpr (CP) {
@@ -317,17 +420,27 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_, GenOcc<Ep<N>::N3 * EPB_>::va
     for (int c = 0; c < 3; ++c) g[c] *= invJ;
   }
   if (!valid) return;
-  // the node's coefficients and Pi, loaded only now: held across the contraction
-  // they would cost the registers that keep more CTAs resident
-  const bool grad_only = P.c10 == nullptr;
+  // the node's coefficients and Pi: from the words copied at kernel start, or
+  // (no room for them) loaded only now -- held in registers across the
+  // contraction they would cost the registers that keep more CTAs resident
   real a = 0, b[3] = {0, 0, 0}, K[6] = {0, 0, 0, 0, 0, 0}, Pi = 0;
   if (!grad_only) {
-    a = P.c10[n];
+    if constexpr (PF) {
+      cp_async_wait_own();
+      a = spf[le][0][t];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) b[c] = P.c10[(1 + c) * nn + n];
+      for (int c = 0; c < 3; ++c) b[c] = spf[le][1 + c][t];
 #pragma unroll
-    for (int c = 0; c < 6; ++c) K[c] = P.c10[(4 + c) * nn + n];
-    Pi = P.Pi[n];
+      for (int c = 0; c < 6; ++c) K[c] = spf[le][4 + c][t];
+      Pi = spf[le][10][t];
+    } else {
+      a = P.c10[n];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) b[c] = P.c10[(1 + c) * nn + n];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) K[c] = P.c10[(4 + c) * nn + n];
+      Pi = P.Pi[n];
+    }
   }
   if (P.grad_out) {
 #pragma unroll
@@ -405,7 +518,21 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_, GenOcc<Ep<N>::N3 * EPB_>::va
   P.F[n] = F0;
   P.F[nn + n] = F1;
   P.F[2 * nn + n] = F2;
-  if constexpr (CP) {
+  if constexpr (PF) {
+    const real yv = pf_y ? spf[le][11][t] : (real)0, accv = pf_acc ? spf[le][12][t] : (real)0,
+               compv = pf_comp ? spf[le][13][t] : (real)0;
+    if constexpr (CP) {
+      if (P.epi)
+        rk_epilogue_cp_v(P.stage, P.dt, phid, u, compv, accv, P.y, P.acc, P.out, P.comp, P.hcopy, n, P.nonfinite);
+      else
+        P.Phidot[n] = phid;
+    } else {
+      if (P.epi)
+        rk_epilogue_v<real>(P.stage, P.dt, phid, u, yv, accv, compv, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
+      else
+        P.Phidot[n] = phid;
+    }
+  } else if constexpr (CP) {
     if (P.epi)
       rk_epilogue_cp(P.stage, P.dt, phid, u, P.y, P.acc, P.out, P.comp, P.hcopy, n, P.nonfinite);
     else
@@ -476,6 +603,20 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
   const long long n = ec * N3 + t;
   const long long nn = P.nn;
   if (tid < N2) GT[(tid % N) * N + tid / N] = (real)P.G[tid];
+  // the RK state words the stage update reads at this node, copied now (see K1):
+  // y [0], acc [1], comp [2]
+  constexpr bool PF = 3 * N3 * EPB * sizeof(real) <= 12288;
+  __shared__ real spf[PF ? EPB : 1][PF ? 3 : 1][PF ? N3 : 1];
+  const bool pf_y = P.epi && (P.stage <= 2 || (P.comp && P.stage == 3));
+  const bool pf_acc = P.epi && P.stage >= 1;
+  const bool pf_comp = P.epi && P.comp && P.stage == 3;
+  if constexpr (PF) {
+    if (valid) {
+      if (pf_y) cp_async_word(&spf[le][0][t], P.y + n);
+      if (pf_acc) cp_async_word(&spf[le][1][t], P.acc + n);
+      if (pf_comp) cp_async_word(&spf[le][2][t], P.comp + n);
+    }
+  }
   const real* Fp[3] = {P.F0, P.F1, P.F2};
   real Fv[3];
 #pragma unroll
@@ -487,10 +628,8 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
   for (int idx = t; idx < 6 * N2; idx += N3) {
     const int f = idx / N2, pq = idx - f * N2;
     long long src = -1;
-    if ((emask >> f) & 1) {
-      const int fs = P.fsrc[f + 6 * ec];
-      src = (long long)(fs >> 6) * N3 + nbr_face_node(fs, pq % N, pq / N, N);
-    }
+    const int fs = valid ? P.fsrc[f + 6 * ec] : -1;  // -1 exactly where the SAT mask bit is 0
+    if (fs >= 0) src = (long long)(fs >> 6) * N3 + nbr_face_node(fs, pq % N, pq / N, N);
     if (CURV) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) sFn[le][f][c][pq] = src >= 0 ? Fp[c][src] : (real)0;
@@ -553,8 +692,16 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
     }
   }
   if (P.epi) {
-    const real yin = P.stage == 0 ? P.y[n] : (real)0;
-    rk_epilogue<real>(P.stage, P.dt, dv, yin, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
+    if constexpr (PF) {
+      cp_async_wait_own();
+      const real yv = pf_y ? spf[le][0][t] : (real)0, accv = pf_acc ? spf[le][1][t] : (real)0,
+                 compv = pf_comp ? spf[le][2][t] : (real)0;
+      rk_epilogue_v<real>(P.stage, P.dt, dv, P.stage == 0 ? yv : (real)0, yv, accv, compv, P.y, P.acc, P.out, P.comp,
+                          n, P.nonfinite);
+    } else {
+      const real yin = P.stage == 0 ? P.y[n] : (real)0;
+      rk_epilogue<real>(P.stage, P.dt, dv, yin, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
+    }
   } else {
     P.Pidot[n] = dv;
   }
