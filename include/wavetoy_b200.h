@@ -482,9 +482,12 @@ int wt_snapshot_load(wt_ctx* ctx, wt_mesh* mesh, void* Phi, void* Pi, double* t,
  * stage, and one RK4 step of all groups is a CUDA graph, captured when the
  * membership changes and replayed by wt_batch_step; the groups' launches are
  * parallel branches of that graph.  The first step after a change also picks
- * the elements per CTA of the generic kernels, K1 and K2 separately, by
- * timing (autotuner, on by default; wt_batch_group_info's epb_variant: bit 0
- * K1, bit 1 K2).  A member with a time-dependent background is re-sampled at
+ * the launch variant of the generic (n != 8) kernels, K1 and K2 separately, by
+ * timing (autotuner, on by default): 0 the generic kernels at their default
+ * elements per CTA, 1 at the alternative count, 2 (n = 4 and 6) the persistent
+ * kernels that copy the next group of tiles into shared memory by cp.async
+ * while they compute the current one; all three give the same bits
+ * (wt_batch_group_info's epb_variant: bits 0-1 K1's variant, bits 2-3 K2's).  A member with a time-dependent background is re-sampled at
  * every stage time inside the graph (its mesh must keep the set-up geometry).
  * Every member advances by the same number of steps per call; results equal
  * wt_step_rk4_curved on each member alone. */
@@ -494,6 +497,10 @@ int wt_batch_add(wt_batch* batch, wt_ws* ws, const wt_coef* coef, void* Phi, voi
                  const wt_bc_desc* bc, int* slot);
 int wt_batch_remove(wt_batch* batch, int slot);
 int wt_batch_set_autotune(wt_batch* batch, int on);
+/* Fix the launch variants of the generic groups' K1 and K2 (0, 1, 2 as above;
+ * -1, the default, leaves the choice to the autotuner; 2 falls back to 0 where
+ * a group's order has no pipelined kernels).  Takes effect at the next step. */
+int wt_batch_set_variant(wt_batch* batch, int k1, int k2);
 int wt_batch_step(wt_batch* batch, int nsteps);
 int wt_batch_info(wt_batch* batch, int* nsolves, long long* nodes, int* ngroups);
 int wt_batch_group_info(wt_batch* batch, int group, int* N, int* precision, int* n8_path, int* epb_variant,

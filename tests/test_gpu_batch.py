@@ -107,15 +107,18 @@ def test_batch_rejects_bad_members(wt, ctx):
         batch.remove(7)
 
 
-def test_batch_members_against_oracle(wt, ctx, O):
+@pytest.mark.parametrize("variant", [-1, 2])
+def test_batch_members_against_oracle(wt, ctx, O, variant):
     """Members of one mixed batch (n = 4, 6, 8; FP64 and the default compensated FP32
     form; groups running as parallel graph branches) against the Float64 oracle after
-    60 steps: FP64 <= 1e-12, compensated FP32 <= 1e-5 relative L2."""
+    60 steps: FP64 <= 1e-12, compensated FP32 <= 1e-5 relative L2.  variant: the
+    autotuner's choice (-1) or the pipelined n = 4, 6 kernels (2)."""
     import torch
     W = wt.workloads
     specs = [(4, 3, 41, 0), (6, 2, 42, 1), (8, 2, 43, 1), (8, 2, 44, 0), (6, 2, 45, 0), (4, 3, 46, 1)]
     members = []
     batch = wt.Batch(ctx)
+    batch.set_variant(variant, variant)
     bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
     for N, M, seed, prec in specs:
         g = wt.Mesh.uniform_hex(ctx, N, M, outer_tag=7, warp_A=0.05, precision=prec)
@@ -187,3 +190,29 @@ def test_batch_time_dependent_backgrounds(wt, ctx, branches):
             np.testing.assert_allclose(cb.get(), ca.get(), rtol=0, atol=1e-13)
     assert not ctx.nonfinite()
     batch.close()
+
+
+@pytest.mark.parametrize("prec,form", [(0, None), (1, None), (1, "cuda")])
+def test_batch_pipelined_kernels_bitwise(wt, ctx, prec, form):
+    """The persistent cp.async-pipelined n = 4, 6 kernels (launch variant 2) against the generic
+    kernels (variant 0): bit-identical states after 7 steps, for FP64, the compensated FP32 form and
+    plain FP32; the 512- and 2197-element members make each persistent CTA loop over several
+    groups of tiles, the small ones leave most of the grid idle."""
+    import torch
+    specs = [(6, 8, 51, 0.1), (4, 13, 52, 0.05), (6, 3, 53, 0.15), (4, 2, 54, 0.0)]
+    fform = {None: None, "cuda": wt.FP32_CUDA_CORES}[form]
+    runs = []
+    for var in (0, 2):
+        solves = [Solve(wt, ctx, N, M, seed, prec, fform if prec else None, amp) for N, M, seed, amp in specs]
+        b = wt.Batch(ctx)
+        b.set_variant(var, var)
+        for s in solves:
+            b.add(s.Phi, s.Pi, s.coef, s.ws, s.dt, s.bc)
+        b.step(2)
+        b.step(5)
+        assert all(g[3] == var | (var << 2) for g in b.groups() if not g[2])
+        runs.append(solves)
+        b.close()
+    for a, c in zip(*runs):
+        assert torch.equal(a.Phi, c.Phi) and torch.equal(a.Pi, c.Pi)
+    assert not ctx.nonfinite()

@@ -2097,6 +2097,7 @@ struct wt_batch {
   std::vector<Group> groups;
   bool dirty = true;
   int autotune = 1;
+  int force_var[2] = {-1, -1};  // wt_batch_set_variant: fixed launch variants of K1 / K2 (-1: tuned)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   long long launches_per_step = 0;
@@ -2162,7 +2163,7 @@ int batch_launch(wt_batch* b, wt_batch::Group& g, int which, int st, cudaStream_
   const size_t sz = which == 1 ? g.k1sz : g.k2sz;
   const char* d = (which == 1 ? g.d_k1 : g.d_k2) + st * ns * sz;
   const int cp = g.precision == WT_F32 && g.fp32_form == WT_FP32_COMPENSATED;
-  const int variant = (g.epb_variant >> (which - 1)) & 1;  // bit 0: K1, bit 1: K2
+  const int variant = (g.epb_variant >> (2 * (which - 1))) & 3;  // bits 0-1: K1, bits 2-3: K2
   return wt::launch_cons_gen_batch(which, g.N, g.precision, variant, cp, d, g.d_tiles, g.ntiles, s);
 }
 
@@ -2213,20 +2214,28 @@ int batch_one_step(wt_batch* b, cudaStream_t s) {
   return 0;
 }
 
-// Time K1 and K2 of stage 0 of a generic group, each in both elements-per-CTA
-// variants, and keep the faster of each (stage 0 writes only stage scratch,
-// never the solution state).  epb_variant: bit 0 K1's choice, bit 1 K2's.
+// Time K1 and K2 of stage 0 of a generic group in each launch variant -- the
+// generic kernels at two elements-per-CTA counts and, for n = 4 and 6, the
+// pipelined kernels -- and keep the fastest of each (stage 0 writes only stage
+// scratch, never the solution state).  epb_variant: bits 0-1 K1's choice, bits
+// 2-3 K2's.  A variant fixed by wt_batch_set_variant is kept untimed.
 int batch_tune_group(wt_batch* b, wt_batch::Group& g) {
   cudaStream_t s = b->ctx->own_stream;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   int choice = 0, rc = 0;
+  const int nvar = wt::cons_gen_pipe_available(g.N) ? 3 : 2;
   for (int which = 1; which <= 2 && !rc; ++which) {
+    const int sh = 2 * (which - 1);
+    if (b->force_var[which - 1] >= 0) {
+      choice |= (b->force_var[which - 1] < nvar ? b->force_var[which - 1] : 0) << sh;
+      continue;
+    }
     float best = 1e30f;
     int best_v = 0;
-    for (int v = 0; v < 2 && !rc; ++v) {
-      g.epb_variant = (choice & ~(1 << (which - 1))) | (v << (which - 1));
+    for (int v = 0; v < nvar && !rc; ++v) {
+      g.epb_variant = (choice & ~(3 << sh)) | (v << sh);
       for (int rep = 0; rep < 2 && !rc; ++rep) rc = batch_launch(b, g, which, 0, s);  // warm up
       cudaEventRecord(e0, s);
       for (int rep = 0; rep < 4 && !rc; ++rep) rc = batch_launch(b, g, which, 0, s);
@@ -2237,7 +2246,7 @@ int batch_tune_group(wt_batch* b, wt_batch::Group& g) {
       cudaEventElapsedTime(&ms, e0, e1);
       if (ms < best) { best = ms; best_v = v; }
     }
-    choice |= best_v << (which - 1);
+    choice |= best_v << sh;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -2308,6 +2317,13 @@ int batch_rebuild(wt_batch* b) {
     cudaStreamSynchronize(ctx->stream);  // the tuning launches run on the context's own stream
     for (auto& g : b->groups)
       if (!g.n8) WT_TRY(batch_tune_group(b, g));
+  } else {
+    for (auto& g : b->groups) {  // untuned: the fixed variants, else the default one
+      const int nvar = wt::cons_gen_pipe_available(g.N) ? 3 : 2;
+      int v[2];
+      for (int w = 0; w < 2; ++w) v[w] = b->force_var[w] >= 0 && b->force_var[w] < nvar ? b->force_var[w] : 0;
+      g.epb_variant = g.n8 ? 0 : v[0] | (v[1] << 2);
+    }
   }
   // capture one RK4 step of every group (several groups: parallel branches)
   cudaStream_t own = ctx->own_stream;
@@ -2405,6 +2421,16 @@ int wt_batch_remove(wt_batch* b, int slot) {
 int wt_batch_set_autotune(wt_batch* b, int on) {
   if (!b) return WT_EINVAL;
   b->autotune = on ? 1 : 0;
+  b->dirty = true;
+  return 0;
+}
+
+int wt_batch_set_variant(wt_batch* b, int k1, int k2) {
+  if (!b) return WT_EINVAL;
+  if (k1 < -1 || k1 > 2 || k2 < -1 || k2 > 2)
+    return fail(b->ctx, WT_EINVAL, "wt_batch_set_variant: variants are -1 (tuned), 0, 1 or 2");
+  b->force_var[0] = k1;
+  b->force_var[1] = k2;
   b->dirty = true;
   return 0;
 }

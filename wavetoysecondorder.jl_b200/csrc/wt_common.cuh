@@ -246,6 +246,8 @@ int launch_pad_metric_n8(DevMesh& m, cudaStream_t s);
 int launch_split_metric(const DevMesh& m, cudaStream_t s);
 // whether the generic (any n) kernels run the compensated FP32 form on this mesh
 bool cons_gen_cp_supported(const DevMesh& m);
+// whether the batch has pipelined kernels (launch variant 2) for order N
+bool cons_gen_pipe_available(int N);
 // bounded-wait self-test (see k_wait_selftest)
 int launch_wait_selftest(long long polls, int arrive, unsigned* flag, cudaStream_t s);
 // the split-form gradient of Phi through the n = 8 kernels (3 fields of nn words into grad)

@@ -261,6 +261,115 @@ struct GenOcc {
   static constexpr int value = T >= 1024 ? 1 : 1024 / T;
 };
 
+// The node pass of K1 at node n (element ec, node (i, j, k)): flux, Phidot,
+// boundary terms (into bbuf) and the RK4 stage update or Phidot.  g: the
+// gradient; u: the stage input (CP: its high part), ug: the value the gradient
+// differentiated; sd: the affine axis scales; a, b, K, Pi: the node's
+// coefficients and Pi.  PRE: the RK words the update reads (yv, accv, compv)
+// were loaded by the caller; otherwise the update reads them itself.
+template <int N, typename real, bool CP, bool PRE, typename gt>
+__device__ __forceinline__ void k1_finish(const K1P<real>& P, long long ec, long long n, int i, int j, int k,
+                                          int emask, const real g[3], real u, gt ug, const real sd[3], real Hend,
+                                          real a, const real b[3], const real K[6], real Pi, real yv, real accv,
+                                          real compv) {
+  constexpr int N2 = Ep<N>::N2;
+  const long long nn = P.nn;
+  // flux and Phidot
+  const real F0 = b[0] * Pi + (K[0] * g[0] + K[1] * g[1] + K[2] * g[2]);
+  const real F1 = b[1] * Pi + (K[1] * g[0] + K[3] * g[1] + K[4] * g[2]);
+  const real F2 = b[2] * Pi + (K[2] * g[0] + K[4] * g[1] + K[5] * g[2]);
+  real phid = b[0] * g[0] + b[1] * g[1] + b[2] * g[2] + a * Pi;
+  // boundary increments (per boundary face of the node; Pi parts go to the face slot)
+  if (P.bc_on && (emask >> 6)) {
+    const int idx3[3] = {i, j, k};
+    for (int f = 0; f < 6; ++f) {
+      const int tag = P.bdry[f + 6 * ec];
+      if (tag == 0) continue;
+      const int ax = f >> 1;
+      if (idx3[ax] != frow(f, N)) continue;
+      const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
+      const int slot = P.bslot[f + 6 * ec];
+      real dF = 0, dP = 0;
+      if (!P.bc_curv) {
+        const int kind = P.kinds[f];
+        if (kind != 3) {
+          const real nh = (f & 1) ? (real)1 : (real)-1;
+          const real Kdd = ax == 0 ? K[0] : ax == 1 ? K[3] : K[5];
+          const real a_n = sqrt(a * Kdd);
+          const real bax = b[ax];
+          const real bn = nh * bax;
+          const real wt = sd[ax] / Hend;
+          if (kind == 4) {
+            const real tau = P.sigma * (fabs(a_n - bax) + fabs(a_n + bax)) * wt;
+            const real gp = P.gPhi ? P.gPhi[n] : (real)0, gq = P.gPi ? P.gPi[n] : (real)0;
+            dF = -tau * ((real)ug - gp);
+            dP = -tau * (Pi - gq);
+          } else {
+            const real qv = nh * g[ax];
+            const real r = Pi + ((bn + a_n) / a) * qv;
+            const real gv = kind == 2 ? (real)0 : (P.gPhi ? P.gPhi[n] : (real)0);
+            dP = -P.sigma * fabs(a_n + bn) * wt * (r - gv);
+          }
+        }
+      } else if (tag != P.exc_tag) {
+        const int kind = P.kinds[0];
+        const long long nb = (long long)P.nbf * N2;
+        const long long bi = (long long)slot * N2 + p + N * q;
+        const real nx = P.bnorm[bi], ny = P.bnorm[nb + bi], nz = P.bnorm[2 * nb + bi], wt = P.bnorm[3 * nb + bi];
+        const real Kn = K[0] * nx * nx + K[3] * ny * ny + K[5] * nz * nz +
+                        (real)2 * (K[1] * nx * ny + K[2] * nx * nz + K[4] * ny * nz);
+        const real a_n = sqrt(a * Kn);
+        const real bn = b[0] * nx + b[1] * ny + b[2] * nz;
+        if (kind == 4) {
+          const real tau = P.sigma * (fabs(a_n - bn) + fabs(a_n + bn)) * wt;
+          const real gp = P.gPhi ? P.gPhi[n] : (real)0, gq = P.gPi ? P.gPi[n] : (real)0;
+          dF = -tau * ((real)ug - gp);
+          dP = -tau * (Pi - gq);
+        } else {
+          const real qv = nx * g[0] + ny * g[1] + nz * g[2];
+          const real r = Pi + ((bn + a_n) / a) * qv;
+          real gv = 0;
+          if (kind != 2) {
+            const real gq = P.gPi ? P.gPi[n] : (real)0;
+            const real gx = P.gDx ? P.gDx[n] : (real)0, gy = P.gDy ? P.gDy[n] : (real)0,
+                       gz = P.gDz ? P.gDz[n] : (real)0;
+            gv = gq + ((bn + a_n) / a) * (nx * gx + ny * gy + nz * gz);
+          }
+          dP = -P.sigma * fabs(a_n + bn) * wt * (r - gv);
+        }
+      }
+      phid += dF;
+      P.bbuf[(long long)slot * N2 + p + N * q] = dP;
+    }
+  }
+  P.F[n] = F0;
+  P.F[nn + n] = F1;
+  P.F[2 * nn + n] = F2;
+  if constexpr (PRE) {
+    if constexpr (CP) {
+      if (P.epi)
+        rk_epilogue_cp_v(P.stage, P.dt, phid, u, compv, accv, P.y, P.acc, P.out, P.comp, P.hcopy, n, P.nonfinite);
+      else
+        P.Phidot[n] = phid;
+    } else {
+      if (P.epi)
+        rk_epilogue_v<real>(P.stage, P.dt, phid, u, yv, accv, compv, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
+      else
+        P.Phidot[n] = phid;
+    }
+  } else if constexpr (CP) {
+    if (P.epi)
+      rk_epilogue_cp(P.stage, P.dt, phid, u, P.y, P.acc, P.out, P.comp, P.hcopy, n, P.nonfinite);
+    else
+      P.Phidot[n] = phid;
+  } else {
+    if (P.epi)
+      rk_epilogue<real>(P.stage, P.dt, phid, u, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
+    else
+      P.Phidot[n] = phid;
+  }
+}
+
 // BATCH: the CTA's elements come from a work list of (solve, element) tiles
 // and each tile reads the parameter block of its solve (plist); otherwise
 // element blockIdx.x * EPB + le of the single solve P0.  EPB_: elements per CTA.
@@ -447,102 +556,236 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_, GenOcc<Ep<N>::N3 * EPB_>::va
     for (int c = 0; c < 3; ++c) P.grad_out[c * nn + n] = g[c];
   }
   if (grad_only) return;
-  // flux and Phidot
-  const real F0 = b[0] * Pi + (K[0] * g[0] + K[1] * g[1] + K[2] * g[2]);
-  const real F1 = b[1] * Pi + (K[1] * g[0] + K[3] * g[1] + K[4] * g[2]);
-  const real F2 = b[2] * Pi + (K[2] * g[0] + K[4] * g[1] + K[5] * g[2]);
-  real phid = b[0] * g[0] + b[1] * g[1] + b[2] * g[2] + a * Pi;
-  // boundary increments (per boundary face of the node; Pi parts go to the face slot)
-  if (P.bc_on && (emask >> 6)) {
-    const int idx3[3] = {i, j, k};
-    for (int f = 0; f < 6; ++f) {
-      const int tag = P.bdry[f + 6 * ec];
-      if (tag == 0) continue;
-      const int ax = f >> 1;
-      if (idx3[ax] != frow(f, N)) continue;
-      const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
-      const int slot = P.bslot[f + 6 * ec];
-      real dF = 0, dP = 0;
-      if (!P.bc_curv) {
-        const int kind = P.kinds[f];
-        if (kind != 3) {
-          const real nh = (f & 1) ? (real)1 : (real)-1;
-          const real Kdd = ax == 0 ? K[0] : ax == 1 ? K[3] : K[5];
-          const real a_n = sqrt(a * Kdd);
-          const real bax = b[ax];
-          const real bn = nh * bax;
-          const real wt = sd[ax] / Hend;
-          if (kind == 4) {
-            const real tau = P.sigma * (fabs(a_n - bax) + fabs(a_n + bax)) * wt;
-            const real gp = P.gPhi ? P.gPhi[n] : (real)0, gq = P.gPi ? P.gPi[n] : (real)0;
-            dF = -tau * ((real)ug - gp);
-            dP = -tau * (Pi - gq);
-          } else {
-            const real qv = nh * g[ax];
-            const real r = Pi + ((bn + a_n) / a) * qv;
-            const real gv = kind == 2 ? (real)0 : (P.gPhi ? P.gPhi[n] : (real)0);
-            dP = -P.sigma * fabs(a_n + bn) * wt * (r - gv);
-          }
+  k1_finish<N, real, CP, PF>(P, ec, n, i, j, k, emask, g, u, ug, sd, Hend, a, b, K, Pi,
+                             PF && pf_y ? spf[le][11][t] : (real)0, PF && pf_acc ? spf[le][12][t] : (real)0,
+                             PF && pf_comp ? spf[le][13][t] : (real)0);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent, cp.async-pipelined K1 for work lists of n < 8 solves (the batch's
+// and the server's n = 4 and n = 6 groups).  The generic K1 above loads its
+// inputs when its one element starts (the face traces behind two dependent
+// loads), so it waits on global memory: about 0.2 of DRAM throughput, long-
+// scoreboard stalls.  Here a CTA loops over groups of EPB tiles and copies
+// everything group g + 1 reads at its own nodes -- Phi (and Phit), the metric
+// terms, 1/J, the ten coefficients, Pi, the RK words, the neighbour face
+// traces (sources loaded one group earlier) and Ja0 -- into the second of two
+// shared buffers while it computes group g.  The arithmetic is the generic
+// K1's (same contractions, same order, k1_finish for the node pass), so both
+// give the same bits.
+template <int N, typename real, bool CP>
+struct PipeK1 {
+  static constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = Ep<N>::EPB, T = N3 * EPB;
+  // own-node word planes of an element block in a buffer
+  static constexpr int PHI = 0, PHIT = 1, JA = CP ? 2 : 1, INVJ = JA + 9, C10 = INVJ + 1, PI = C10 + 10,
+                       Y = PI + 1, ACC = Y + 1, COMP = ACC + 1, NW = COMP + 1;
+  static constexpr int NF = CP ? 12 : 6;               // face-trace planes: Phi [+ Phit] on the 6 faces
+  static constexpr int NFR = (6 * N2 + N3 - 1) / N3;  // face entries per thread
+  // words of one element block (padded to 16 bytes) and of one buffer
+  static constexpr size_t EW = ((NW * N3 + NF * N2) * sizeof(real) + (CP ? 9 * sizeof(double) : 0) + 15) / 16 * 16;
+  static constexpr size_t BUF = EPB * EW;
+  using gt = typename std::conditional<CP, double, real>::type;
+  static constexpr size_t SU = ((size_t)EPB * N3 * sizeof(gt) + 15) / 16 * 16;
+  static constexpr size_t SW = ((size_t)EPB * 9 * N3 * sizeof(real) + 15) / 16 * 16;
+  static constexpr size_t SMEM = 2 * BUF + SU + SW + N2 * sizeof(gt) + N2 * sizeof(real) + 16;
+  // resident CTAs per SM the registers are sized for: as many as the shared memory
+  // allows, up to 1024 threads
+  static constexpr int OCC_SM = (int)(220000 / SMEM) > 0 ? (int)(220000 / SMEM) : 1;
+  static constexpr int OCC = OCC_SM < 1024 / T ? OCC_SM : 1024 / T;
+  static_assert(!CP || ((NW * N3 + NF * N2) * sizeof(real)) % 8 == 0, "Ja0 must be 8-byte aligned in a block");
+};
+
+// 4- or 8-byte cp.async, zero-filled (src not read) when !valid
+template <typename T>
+__device__ __forceinline__ void cp_async_word_z(T* dst, const T* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+
+template <int N, typename real, bool CP>
+__global__ void __launch_bounds__(PipeK1<N, real, CP>::T, PipeK1<N, real, CP>::OCC)
+    k_cons_k1_pipe(const K1P<real>* __restrict__ plist, const int2* __restrict__ tiles, long long ntiles) {
+  using L = PipeK1<N, real, CP>;
+  using gt = typename L::gt;
+  constexpr int N3 = L::N3, N2 = L::N2, EPB = L::EPB, NFR = L::NFR;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  gt* su = reinterpret_cast<gt*>(smraw + 2 * L::BUF);                   // [EPB][N3]
+  real* sw = reinterpret_cast<real*>(smraw + 2 * L::BUF + L::SU);       // [EPB][9][N3]
+  gt* GT = reinterpret_cast<gt*>(smraw + 2 * L::BUF + L::SU + L::SW);   // transposed G
+  real* GTr = reinterpret_cast<real*>(GT + N2);                         // CP: G in FP32
+  const int tid = threadIdx.x;
+  const int le = tid / N3, t = tid - le * N3;
+  const int i = t % N, j = (t / N) % N, k = t / N2;
+  const long long ngroups = (ntiles + EPB - 1) / EPB;
+  const long long GS = gridDim.x;
+  auto blk = [&](int bb) -> real* { return reinterpret_cast<real*>(smraw + bb * L::BUF + le * L::EW); };
+  // this thread's tile in group gg (x = -1: none)
+  auto tile_of = [&](long long gg) -> int2 {
+    const long long ti = gg * EPB + le;
+    return (gg < ngroups && ti < ntiles) ? tiles[ti] : make_int2(-1, -1);
+  };
+  auto src_load = [&](int2 tl, int src[NFR]) {
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = t + r * N3;
+      src[r] = (tl.x >= 0 && idx < 6 * N2) ? plist[tl.x].fsrc[idx / N2 + 6 * tl.y] : -1;
+    }
+  };
+  // copy what tile tl reads at this thread's node, and this thread's face-trace
+  // entries, into buffer bb
+  auto issue = [&](int2 tl, const int src[NFR], int bb) {
+    if (tl.x < 0) return;
+    const K1P<real>& P = plist[tl.x];
+    const long long e = tl.y, n = e * N3 + t, nn = P.nn;
+    real* w = blk(bb);
+    cp_async_word(w + L::PHI * N3 + t, P.Phi + n);
+    if constexpr (CP) cp_async_word_z(w + L::PHIT * N3 + t, P.Phit ? P.Phit + n : P.Phi + n, P.Phit != nullptr);
+    const real* ja = CP ? P.dJa : P.Ja;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) cp_async_word(w + (L::JA + c) * N3 + t, ja + c * nn + n);
+    cp_async_word(w + L::INVJ * N3 + t, P.invdetJ + n);
+    if (P.c10) {
+#pragma unroll
+      for (int c = 0; c < 10; ++c) cp_async_word(w + (L::C10 + c) * N3 + t, P.c10 + c * nn + n);
+      cp_async_word(w + L::PI * N3 + t, P.Pi + n);
+    }
+    if (P.epi && (P.stage == 1 || P.stage == 2 || (!CP && P.comp && P.stage == 3)))
+      cp_async_word(w + L::Y * N3 + t, P.y + n);
+    if (P.epi && P.stage >= 1) cp_async_word(w + L::ACC * N3 + t, P.acc + n);
+    if (P.epi && (CP || (P.comp && P.stage == 3))) cp_async_word(w + L::COMP * N3 + t, P.comp + n);
+    real* fc = w + L::NW * N3;
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = t + r * N3;
+      if (idx < 6 * N2) {
+        const int f = idx / N2, pq = idx - f * N2, sr = src[r];
+        const long long nb = sr >= 0 ? (long long)(sr >> 6) * N3 + nbr_face_node(sr, pq % N, pq / N, N) : 0;
+        cp_async_word_z(fc + f * N2 + pq, P.Phi + nb, sr >= 0);
+        if constexpr (CP) cp_async_word_z(fc + (6 + f) * N2 + pq, (P.Phit ? P.Phit : P.Phi) + nb, sr >= 0 && P.Phit);
+      }
+    }
+    if constexpr (CP) {
+      if (t < 9) cp_async_word(reinterpret_cast<double*>(fc + L::NF * N2) + t, P.Ja0 + 9 * e + t);
+    }
+  };
+
+  if (tid < N2) {
+    GT[(tid % N) * N + tid / N] = (gt)plist[0].G[tid];  // every solve of a group has the same N, hence G
+    if constexpr (CP) GTr[(tid % N) * N + tid / N] = (real)plist[0].G[tid];
+  }
+  long long g = blockIdx.x;
+  int2 tcur = tile_of(g), tnext = tile_of(g + GS);
+  int src[NFR];
+  src_load(tcur, src);
+  issue(tcur, src, 0);
+  src_load(tnext, src);
+  int emcur = tcur.x >= 0 ? plist[tcur.x].emask[tcur.y] : 0;
+  for (int it = 0; g < ngroups; g += GS, ++it) {
+    const int bb = it & 1;
+    const int2 tn2 = tile_of(g + 2 * GS);
+    const int emnext = tnext.x >= 0 ? plist[tnext.x].emask[tnext.y] : 0;
+    cp_async_wait_own();
+    // this group's words are visible to every thread, and every thread is done
+    // with the previous group: the other buffer, su and sw are free
+    __syncthreads();
+    issue(tnext, src, bb ^ 1);
+    src_load(tn2, src);
+    const bool valid = tcur.x >= 0;
+    const K1P<real>& P = plist[valid ? tcur.x : 0];
+    const long long ec = valid ? tcur.y : 0, n = ec * N3 + t;
+    const real* w = blk(bb);
+    const real* fc = w + L::NW * N3;
+    const int emask = emcur;
+    const real u = valid ? w[L::PHI * N3 + t] : (real)0;  // CP: the high part
+    gt ug = u;
+    if constexpr (CP) {
+      if (valid && P.Phit) ug += (gt)w[L::PHIT * N3 + t];
+    }
+    su[le * N3 + t] = ug;
+    real m[9], m0[CP ? 9 : 1];
+    const double* ja0 = reinterpret_cast<const double*>(fc + L::NF * N2);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      m[c] = valid ? w[(L::JA + c) * N3 + t] : (real)0;
+      if constexpr (CP) m0[c] = valid ? (real)ja0[c] : (real)0;
+    }
+    const real invJ = valid ? w[L::INVJ * N3 + t] : (real)0;
+    const real Hend = (real)P.H[0];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) sw[(le * 9 + c) * N3 + t] = m[c] * (real)ug;
+    __syncthreads();
+    real du[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) du[d] = (real)contract<N>(su + le * N3, GT, i, j, k, d);
+    real g3[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      real acc = 0;
+#pragma unroll
+      for (int al = 0; al < 3; ++al) {
+        if constexpr (CP)
+          acc += (real)0.5 * contract<N>(sw + (le * 9 + al * 3 + c) * N3, GTr, i, j, k, al) +
+                 (m0[al * 3 + c] + (real)0.5 * m[al * 3 + c]) * du[al];
+        else
+          acc += (real)0.5 * contract<N>(sw + (le * 9 + al * 3 + c) * N3, GT, i, j, k, al) +
+                 (real)0.5 * m[al * 3 + c] * du[al];
+      }
+      g3[c] = acc;
+    }
+    if (valid) {
+      const int idx3[3] = {i, j, k};
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        const int ax = f >> 1;
+        if (idx3[ax] != frow(f, N)) continue;
+        if (!((emask >> f) & 1)) continue;
+        const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
+        gt sv = fc[f * N2 + p + N * q];
+        if constexpr (CP) {
+          if (P.Phit) sv += (gt)fc[(6 + f) * N2 + p + N * q];
         }
-      } else if (tag != P.exc_tag) {
-        const int kind = P.kinds[0];
-        const long long nb = (long long)P.nbf * N2;
-        const long long bi = (long long)slot * N2 + p + N * q;
-        const real nx = P.bnorm[bi], ny = P.bnorm[nb + bi], nz = P.bnorm[2 * nb + bi], wt = P.bnorm[3 * nb + bi];
-        const real Kn = K[0] * nx * nx + K[3] * ny * ny + K[5] * nz * nz +
-                        (real)2 * (K[1] * nx * ny + K[2] * nx * nz + K[4] * ny * nz);
-        const real a_n = sqrt(a * Kn);
-        const real bn = b[0] * nx + b[1] * ny + b[2] * nz;
-        if (kind == 4) {
-          const real tau = P.sigma * (fabs(a_n - bn) + fabs(a_n + bn)) * wt;
-          const real gp = P.gPhi ? P.gPhi[n] : (real)0, gq = P.gPi ? P.gPi[n] : (real)0;
-          dF = -tau * ((real)ug - gp);
-          dP = -tau * (Pi - gq);
-        } else {
-          const real qv = nx * g[0] + ny * g[1] + nz * g[2];
-          const real r = Pi + ((bn + a_n) / a) * qv;
-          real gv = 0;
-          if (kind != 2) {
-            const real gq = P.gPi ? P.gPi[n] : (real)0;
-            const real gx = P.gDx ? P.gDx[n] : (real)0, gy = P.gDy ? P.gDy[n] : (real)0,
-                       gz = P.gDz ? P.gDz[n] : (real)0;
-            gv = gq + ((bn + a_n) / a) * (nx * gx + ny * gy + nz * gz);
-          }
-          dP = -P.sigma * fabs(a_n + bn) * wt * (r - gv);
+        const real jump = (real)(sv - ug);
+        const real nh = (f & 1) ? (real)1 : (real)-1;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          real mc = m[ax * 3 + c];
+          if constexpr (CP) mc += m0[ax * 3 + c];
+          g3[c] += nh * mc * jump / ((real)2 * Hend);
         }
       }
-      phid += dF;
-      P.bbuf[(long long)slot * N2 + p + N * q] = dP;
     }
-  }
-  P.F[n] = F0;
-  P.F[nn + n] = F1;
-  P.F[2 * nn + n] = F2;
-  if constexpr (PF) {
-    const real yv = pf_y ? spf[le][11][t] : (real)0, accv = pf_acc ? spf[le][12][t] : (real)0,
-               compv = pf_comp ? spf[le][13][t] : (real)0;
-    if constexpr (CP) {
-      if (P.epi)
-        rk_epilogue_cp_v(P.stage, P.dt, phid, u, compv, accv, P.y, P.acc, P.out, P.comp, P.hcopy, n, P.nonfinite);
-      else
-        P.Phidot[n] = phid;
-    } else {
-      if (P.epi)
-        rk_epilogue_v<real>(P.stage, P.dt, phid, u, yv, accv, compv, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
-      else
-        P.Phidot[n] = phid;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g3[c] *= invJ;
+    if (valid) {
+      if (P.grad_out) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) P.grad_out[c * P.nn + n] = g3[c];
+      }
+      if (P.c10) {
+        const real a = w[L::C10 * N3 + t];
+        real b[3], K[6];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) b[c] = w[(L::C10 + 1 + c) * N3 + t];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) K[c] = w[(L::C10 + 4 + c) * N3 + t];
+        const real Pi = w[L::PI * N3 + t];
+        const bool pf_y = P.epi && (P.stage == 1 || P.stage == 2 || (!CP && P.comp && P.stage == 3));
+        const bool pf_acc = P.epi && P.stage >= 1;
+        const bool pf_comp = P.epi && (CP || (P.comp && P.stage == 3));
+        const real sd[3] = {0, 0, 0};
+        k1_finish<N, real, CP, true>(P, ec, n, i, j, k, emask, g3, u, ug, sd, Hend, a, b, K, Pi,
+                                     pf_y ? w[L::Y * N3 + t] : (real)0, pf_acc ? w[L::ACC * N3 + t] : (real)0,
+                                     pf_comp ? w[L::COMP * N3 + t] : (real)0);
+      }
     }
-  } else if constexpr (CP) {
-    if (P.epi)
-      rk_epilogue_cp(P.stage, P.dt, phid, u, P.y, P.acc, P.out, P.comp, P.hcopy, n, P.nonfinite);
-    else
-      P.Phidot[n] = phid;
-  } else {
-    if (P.epi)
-      rk_epilogue<real>(P.stage, P.dt, phid, u, P.y, P.acc, P.out, P.comp, n, P.nonfinite);
-    else
-      P.Phidot[n] = phid;
+    tcur = tnext;
+    tnext = tn2;
+    emcur = emnext;
   }
+  cp_async_wait_own();
 }
 
 template <typename real>
@@ -705,6 +948,157 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
   } else {
     P.Pidot[n] = dv;
   }
+}
+
+// Persistent, cp.async-pipelined K2 for work lists of n < 8 solves (see
+// k_cons_k1_pipe): group g + 1's F, metric terms, 1/J, RK words and neighbour
+// flux face traces are copied into the second shared buffer while group g is
+// computed with the generic K2's arithmetic.
+template <int N, typename real>
+struct PipeK2 {
+  static constexpr int N3 = Ep<N>::N3, N2 = Ep<N>::N2, EPB = Ep<N>::EPB, T = N3 * EPB;
+  static constexpr int F = 0, JA = 3, INVJ = 12, Y = 13, ACC = 14, COMP = 15, NW = 16;
+  static constexpr int NF = 18;                        // face-trace planes: F_c on the 6 faces
+  static constexpr int NFR = (6 * N2 + N3 - 1) / N3;  // face points per thread (3 components each)
+  static constexpr size_t EW = ((NW * N3 + NF * N2) * sizeof(real) + 15) / 16 * 16;
+  static constexpr size_t BUF = EPB * EW;
+  static constexpr size_t SW = ((size_t)EPB * 3 * N3 * sizeof(real) + 15) / 16 * 16;
+  static constexpr size_t SMEM = 2 * BUF + SW + N2 * sizeof(real) + 16;
+  static constexpr int OCC_SM = (int)(220000 / SMEM) > 0 ? (int)(220000 / SMEM) : 1;
+  static constexpr int OCC = OCC_SM < 1024 / T ? OCC_SM : 1024 / T;
+};
+
+template <int N, typename real>
+__global__ void __launch_bounds__(PipeK2<N, real>::T, PipeK2<N, real>::OCC)
+    k_cons_k2_pipe(const K2P<real>* __restrict__ plist, const int2* __restrict__ tiles, long long ntiles) {
+  using L = PipeK2<N, real>;
+  constexpr int N3 = L::N3, N2 = L::N2, EPB = L::EPB, NFR = L::NFR;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  real* sw = reinterpret_cast<real*>(smraw + 2 * L::BUF);              // [EPB][3][N3]
+  real* GT = reinterpret_cast<real*>(smraw + 2 * L::BUF + L::SW);      // transposed G
+  const int tid = threadIdx.x;
+  const int le = tid / N3, t = tid - le * N3;
+  const int i = t % N, j = (t / N) % N, k = t / N2;
+  const long long ngroups = (ntiles + EPB - 1) / EPB;
+  const long long GS = gridDim.x;
+  auto blk = [&](int bb) -> real* { return reinterpret_cast<real*>(smraw + bb * L::BUF + le * L::EW); };
+  auto tile_of = [&](long long gg) -> int2 {
+    const long long ti = gg * EPB + le;
+    return (gg < ngroups && ti < ntiles) ? tiles[ti] : make_int2(-1, -1);
+  };
+  auto src_load = [&](int2 tl, int src[NFR]) {
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = t + r * N3;
+      src[r] = (tl.x >= 0 && idx < 6 * N2) ? plist[tl.x].fsrc[idx / N2 + 6 * tl.y] : -1;
+    }
+  };
+  auto issue = [&](int2 tl, const int src[NFR], int bb) {
+    if (tl.x < 0) return;
+    const K2P<real>& P = plist[tl.x];
+    const long long e = tl.y, n = e * N3 + t, nn = P.nn;
+    const real* Fp[3] = {P.F0, P.F1, P.F2};
+    real* w = blk(bb);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) cp_async_word(w + (L::F + c) * N3 + t, Fp[c] + n);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) cp_async_word(w + (L::JA + c) * N3 + t, P.Ja + c * nn + n);
+    cp_async_word(w + L::INVJ * N3 + t, P.invdetJ + n);
+    if (P.epi && (P.stage <= 2 || (P.comp && P.stage == 3))) cp_async_word(w + L::Y * N3 + t, P.y + n);
+    if (P.epi && P.stage >= 1) cp_async_word(w + L::ACC * N3 + t, P.acc + n);
+    if (P.epi && P.comp && P.stage == 3) cp_async_word(w + L::COMP * N3 + t, P.comp + n);
+    real* fc = w + L::NW * N3;
+#pragma unroll
+    for (int r = 0; r < NFR; ++r) {
+      const int idx = t + r * N3;
+      if (idx < 6 * N2) {
+        const int f = idx / N2, pq = idx - f * N2, sr = src[r];
+        const long long nb = sr >= 0 ? (long long)(sr >> 6) * N3 + nbr_face_node(sr, pq % N, pq / N, N) : 0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) cp_async_word_z(fc + (f * 3 + c) * N2 + pq, Fp[c] + nb, sr >= 0);
+      }
+    }
+  };
+  if (tid < N2) GT[(tid % N) * N + tid / N] = (real)plist[0].G[tid];
+  long long g = blockIdx.x;
+  int2 tcur = tile_of(g), tnext = tile_of(g + GS);
+  int src[NFR];
+  src_load(tcur, src);
+  issue(tcur, src, 0);
+  src_load(tnext, src);
+  int emcur = tcur.x >= 0 ? plist[tcur.x].emask[tcur.y] : 0;
+  for (int it = 0; g < ngroups; g += GS, ++it) {
+    const int bb = it & 1;
+    const int2 tn2 = tile_of(g + 2 * GS);
+    const int emnext = tnext.x >= 0 ? plist[tnext.x].emask[tnext.y] : 0;
+    cp_async_wait_own();
+    __syncthreads();  // see k_cons_k1_pipe
+    issue(tnext, src, bb ^ 1);
+    src_load(tn2, src);
+    const bool valid = tcur.x >= 0;
+    const K2P<real>& P = plist[valid ? tcur.x : 0];
+    const long long ec = valid ? tcur.y : 0, n = ec * N3 + t;
+    const real* w = blk(bb);
+    const real* fc = w + L::NW * N3;
+    const int emask = emcur;
+    real Fv[3], m[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Fv[c] = valid ? w[(L::F + c) * N3 + t] : (real)0;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) m[c] = valid ? w[(L::JA + c) * N3 + t] : (real)0;
+    const real invJ = valid ? w[L::INVJ * N3 + t] : (real)0;
+#pragma unroll
+    for (int al = 0; al < 3; ++al)
+      sw[(le * 3 + al) * N3 + t] = m[al * 3] * Fv[0] + m[al * 3 + 1] * Fv[1] + m[al * 3 + 2] * Fv[2];
+    const real Hend = (real)P.H[0];
+    __syncthreads();
+    real dv = 0;
+#pragma unroll
+    for (int al = 0; al < 3; ++al) {
+      dv += (real)0.5 * contract<N>(sw + (le * 3 + al) * N3, GT, i, j, k, al);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dv += (real)0.5 * m[al * 3 + c] * contract<N>(w + (L::F + c) * N3, GT, i, j, k, al);
+    }
+    if (valid) {
+      const int idx3[3] = {i, j, k};
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        const int ax = f >> 1;
+        if (idx3[ax] != frow(f, N)) continue;
+        if (!((emask >> f) & 1)) continue;
+        const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
+        const real nh = (f & 1) ? (real)1 : (real)-1;
+        real sacc = 0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sacc += m[ax * 3 + c] * (fc[(f * 3 + c) * N2 + p + N * q] - Fv[c]);
+        dv += nh * sacc / ((real)2 * Hend);
+      }
+      dv *= invJ;
+      if (P.bc_on && (emask >> 6)) {
+        for (int f = 0; f < 6; ++f) {
+          if (P.bdry[f + 6 * ec] == 0) continue;
+          const int ax = f >> 1;
+          if (idx3[ax] != frow(f, N)) continue;
+          const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
+          dv += P.bbuf[(long long)P.bslot[f + 6 * ec] * N2 + p + N * q];
+        }
+      }
+      if (P.epi) {
+        const bool pf_y = P.stage <= 2 || (P.comp && P.stage == 3);
+        const real yv = pf_y ? w[L::Y * N3 + t] : (real)0;
+        const real accv = P.stage >= 1 ? w[L::ACC * N3 + t] : (real)0;
+        const real compv = P.comp && P.stage == 3 ? w[L::COMP * N3 + t] : (real)0;
+        rk_epilogue_v<real>(P.stage, P.dt, dv, P.stage == 0 ? yv : (real)0, yv, accv, compv, P.y, P.acc, P.out,
+                            P.comp, n, P.nonfinite);
+      } else {
+        P.Pidot[n] = dv;
+      }
+    }
+    tcur = tnext;
+    tnext = tn2;
+    emcur = emnext;
+  }
+  cp_async_wait_own();
 }
 
 // ---------------------------------------------------------------------------
@@ -929,15 +1323,69 @@ static int gen_batch(int which, bool cp, const void* plist, const int2* tiles, l
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+static int gen_sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+// the pipelined kernels: a persistent grid of up to OCC CTAs per SM
+template <int N, typename real, bool CP>
+static int pipe_batch(int which, const void* plist, const int2* tiles, long long ntiles, cudaStream_t s) {
+  static bool attr1 = false, attr2 = false;
+  if (which == 1) {
+    using L = PipeK1<N, real, CP>;
+    if (!attr1) {
+      if (cudaFuncSetAttribute(k_cons_k1_pipe<N, real, CP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)L::SMEM) != cudaSuccess)
+        return -2;
+      attr1 = true;
+    }
+    const long long ng = (ntiles + L::EPB - 1) / L::EPB, cap = (long long)gen_sm_count() * L::OCC;
+    const long long grid = ng < cap ? ng : cap;
+    if (grid <= 0) return 0;
+    k_cons_k1_pipe<N, real, CP><<<(unsigned)grid, L::T, L::SMEM, s>>>((const K1P<real>*)plist, tiles, ntiles);
+  } else {
+    using L = PipeK2<N, real>;
+    if (!attr2) {
+      if (cudaFuncSetAttribute(k_cons_k2_pipe<N, real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::SMEM) !=
+          cudaSuccess)
+        return -2;
+      attr2 = true;
+    }
+    const long long ng = (ntiles + L::EPB - 1) / L::EPB, cap = (long long)gen_sm_count() * L::OCC;
+    const long long grid = ng < cap ? ng : cap;
+    if (grid <= 0) return 0;
+    k_cons_k2_pipe<N, real><<<(unsigned)grid, L::T, L::SMEM, s>>>((const K2P<real>*)plist, tiles, ntiles);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// variant: 0 the generic kernels at Ep<N>::EPB elements per CTA, 1 at the
+// alternative EPB, 2 the pipelined kernels (n = 4 and 6; otherwise as 0)
 template <int N>
 static int gen_batch_n(int which, int precision, int variant, bool cp, const void* plist, const int2* tiles,
                        long long ntiles, cudaStream_t s) {
+  if constexpr (N == 4 || N == 6) {
+    if (variant == 2) {
+      if (precision == 0) return pipe_batch<N, double, false>(which, plist, tiles, ntiles, s);
+      return cp ? pipe_batch<N, float, true>(which, plist, tiles, ntiles, s)
+                : pipe_batch<N, float, false>(which, plist, tiles, ntiles, s);
+    }
+  }
   if (precision == 0)
-    return variant ? gen_batch<N, double, EpAlt<N>::V1>(which, false, plist, tiles, ntiles, s)
-                   : gen_batch<N, double, Ep<N>::EPB>(which, false, plist, tiles, ntiles, s);
-  return variant ? gen_batch<N, float, EpAlt<N>::V1>(which, cp, plist, tiles, ntiles, s)
-                 : gen_batch<N, float, Ep<N>::EPB>(which, cp, plist, tiles, ntiles, s);
+    return variant == 1 ? gen_batch<N, double, EpAlt<N>::V1>(which, false, plist, tiles, ntiles, s)
+                        : gen_batch<N, double, Ep<N>::EPB>(which, false, plist, tiles, ntiles, s);
+  return variant == 1 ? gen_batch<N, float, EpAlt<N>::V1>(which, cp, plist, tiles, ntiles, s)
+                      : gen_batch<N, float, Ep<N>::EPB>(which, cp, plist, tiles, ntiles, s);
 }
+
+bool cons_gen_pipe_available(int N) { return N == 4 || N == 6; }
 
 size_t cons_gen_param_size(int precision, int which) {
   if (precision == 0) return which == 1 ? sizeof(K1P<double>) : sizeof(K2P<double>);

@@ -134,7 +134,8 @@ def library():
         "wt_mesh_release_setup_geometry": [vp],
         "wt_batch_create": [vp, C.POINTER(vp)], "wt_batch_destroy": [vp],
         "wt_batch_add": [vp, vp, vp, vp, vp, d, C.POINTER(_BcDesc), C.POINTER(i)],
-        "wt_batch_remove": [vp, i], "wt_batch_set_autotune": [vp, i], "wt_batch_step": [vp, i],
+        "wt_batch_remove": [vp, i], "wt_batch_set_autotune": [vp, i], "wt_batch_set_variant": [vp, i, i],
+        "wt_batch_step": [vp, i],
         "wt_batch_info": [vp, C.POINTER(i), C.POINTER(ll), C.POINTER(i)],
         "wt_batch_group_info": [vp, i, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(ll)],
         "wt_apply_D": [vp, vp, vp, vp, i], "wt_ko_add": [vp, vp, vp, vp, d],
@@ -538,8 +539,9 @@ class Batch(_Child):
     Members are (workspace, coefficients, Phi, Pi, dt, bc) sets on curvilinear
     meshes of any order and size.  Solves of one (n, precision, path) group run
     as one work list of (solve, element) tiles per kernel launch, one RK4 step
-    of all groups is a CUDA graph, and the elements per CTA of the generic
-    kernels are picked by timing when the membership changes."""
+    of all groups is a CUDA graph, and the launch variant of the generic
+    kernels (elements per CTA, or the pipelined kernels for n = 4, 6) is picked
+    by timing when the membership changes."""
 
     def __init__(self, ctx: Context, autotune: bool = True):
         self.ctx = ctx
@@ -561,6 +563,12 @@ class Batch(_Child):
     def remove(self, slot: int):
         self.ctx.check(library().wt_batch_remove(self.h, int(slot)), "wt_batch_remove")
         self._keep.pop(slot, None)
+
+    def set_variant(self, k1: int = -1, k2: int = -1):
+        """Fix the launch variants of the generic groups' K1 and K2 (wt_batch_set_variant): 0 / 1 the
+        generic kernels at the default / alternative elements per CTA, 2 the pipelined kernels
+        (n = 4, 6); -1 leaves the choice to the autotuner."""
+        self.ctx.check(library().wt_batch_set_variant(self.h, int(k1), int(k2)), "wt_batch_set_variant")
 
     def step(self, nsteps: int = 1):
         self.ctx.check(library().wt_batch_step(self.h, int(nsteps)), "wt_batch_step")
