@@ -1158,7 +1158,7 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
 // k_cons_k1_n8<double> use and added in their order, so the fused step equals
 // the two-kernel step bit for bit.
 // Measured on the 64^3 x 8^3 solve: 262 DRAM bytes per node and launch (the two
-// kernels: 364); the RK4 step 5-7 % faster than the two-kernel step timed right
+// kernels: 364); the RK4 step 1-7 % faster than the two-kernel step timed right
 // after it on the same GPU.  The kernels are bound by latency and issue (16
 // warps per SM, about 41 % issue active) rather than by DRAM bandwidth, so
 // the gain is smaller than the bytes saved.
