@@ -341,6 +341,28 @@ def run_ours(args):
                "clocks": aclocks}
         ws.set_fused(not args.unfused)
         del P2, Q2
+    ko = None
+    if prec == wt.WT_F64 and N == 8 and world == 1:
+        # Kreiss-Oliger dissipation on (eps_KO = 0.1, the reference's wave3d_curved_rhs!
+        # with the line-local D^6 passes): RK4 steps of the same solve on copies of the
+        # state; mu (the power iteration) is computed before the timed steps
+        P2, Q2 = Phi.clone(), Pi.clone()
+        _ = ws.mu
+        for _ in range(2):
+            wt.step_rk4_curved(P2, Q2, coef, ws, dt, 1, eps_KO=0.1, bc3d=bc, metric=True)
+        torch.cuda.synchronize()
+        kst = max(3, args.steps // 4)
+        k0, k1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        for _ in range(kst):
+            wt.step_rk4_curved(P2, Q2, coef, ws, dt, 1, eps_KO=0.1, bc3d=bc, metric=True)
+        k1e.record(stream)
+        torch.cuda.synchronize()
+        tk = k0.elapsed_time(k1e) / 1000.0
+        ko = {"eps_KO": 0.1, "steps": kst, "value": 2.0 * nn * kst / tk, "unit": "DOF-updates/s",
+              "ms_per_step": 1000.0 * tk / kst, "ratio_to_value": (2.0 * nn * kst / tk) / value,
+              "finite": bool(torch.isfinite(P2).all() and torch.isfinite(Q2).all())}
+        del P2, Q2
 
     # end to end through the host-buffer API (wt_evolve_curved_host, the shape of
     # evolve3d): page-locked host state in, one RK4 step per sample, state and
@@ -440,6 +462,8 @@ def run_ours(args):
     }
     if alt is not None:
         line["other_stage_form"] = alt
+    if ko is not None:
+        line["ko_step"] = ko
     if study:
         # the precision study of the large solve: every FP32 form on the same workload,
         # timed like the FP64 form and compared with its state after the same steps

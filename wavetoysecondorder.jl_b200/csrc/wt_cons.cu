@@ -1146,37 +1146,61 @@ __global__ void __launch_bounds__(Ep<N>::T) k_apply_D(long long Ne, const real* 
 // on the same axis-d grid line (METHODS.md:151-155), so a CTA loads N pencils
 // of one whole element line (N * len * N values) into smem and applies D_d six
 // times there; one thread per (pencil, element segment) keeps its N values in
-// registers.  Arithmetic is that of six apply_D! calls.
+// registers.  The line's values come in and go out by cooperative loads and
+// stores in node order (consecutive threads, consecutive addresses), staged
+// through the same shared buffer; a thread loading its own pencil directly
+// would read N consecutive words with a stride of N words between threads (the
+// kernel then ran at 0.14 of DRAM bandwidth).  Arithmetic is that of six
+// apply_D! calls.
 template <int N, typename real>
 __global__ void k_ko_line(int d, int len, int closed, const int32_t* __restrict__ lines, real* __restrict__ dst,
                           const real* __restrict__ field, real koT, const real* __restrict__ sdiag,
                           const double* __restrict__ G, const double* __restrict__ H) {
   extern __shared__ unsigned char smraw[];
-  real* buf = reinterpret_cast<real*>(smraw);  // [N pencils][len*N]
+  // [N pencils][len*N], pencil stride len*N + 1: the N pencils a warp touches at
+  // once fall into different banks (with stride len*N they all share one)
+  const int PS = len * N + 1;
+  real* buf = reinterpret_cast<real*>(smraw);
+  int* se = reinterpret_cast<int*>(buf + N * PS);  // the line's elements
   __shared__ real Gs[N * N];
-  constexpr int N3 = N * N * N;
+  constexpr int N2 = N * N, N3 = N * N * N;
   const int line = blockIdx.x;
   const int g = blockIdx.y;       // pencil group (second tangential index)
   const int tid = threadIdx.x;
   const int pb = tid % N;         // pencil within group (fastest tangential index)
   const int sg = tid / N;         // element segment along the line
   for (int idx = tid; idx < N * N; idx += blockDim.x) Gs[idx] = (real)G[idx];
+  for (int q = tid; q < len; q += blockDim.x) se[q] = lines[(long long)line * len + q];
   const bool act = sg < len;
-  const int e = act ? lines[(long long)line * len + sg] : 0;
-  // node index of position l along axis d for this pencil
-  auto node = [&](int l) -> long long {
+  // node of position l along axis d of pencil p in the element of segment sq
+  auto node = [&](int sq, int p, int l) -> long long {
     int ii, jj, kk;
-    if (d == 0) { ii = l; jj = pb; kk = g; }
-    else if (d == 1) { ii = pb; jj = l; kk = g; }
-    else { ii = pb; jj = g; kk = l; }
-    return (long long)e * N3 + ii + N * (jj + N * kk);
+    if (d == 0) { ii = l; jj = p; kk = g; }
+    else if (d == 1) { ii = p; jj = l; kk = g; }
+    else { ii = p; jj = g; kk = l; }
+    return (long long)se[sq] * N3 + ii + N * (jj + N * kk);
   };
+  // (pencil, position) of the w-th of an element's N^2 nodes in this group, w in
+  // increasing node order: the cooperative loads and stores below run over
+  // (segment, w), so that consecutive threads touch consecutive addresses
+  auto split = [&](int w, int& p, int& l) {
+    if (d == 0) { l = w % N; p = w / N; }
+    else { p = w % N; l = w / N; }
+  };
+  __syncthreads();
+  for (int q = tid; q < len * N2; q += blockDim.x) {
+    const int sq = q / N2;
+    int p, l;
+    split(q - sq * N2, p, l);
+    buf[p * PS + sq * N + l] = field[node(sq, p, l)];
+  }
+  __syncthreads();
   real v[N];
   if (act) {
 #pragma unroll
-    for (int l = 0; l < N; ++l) v[l] = field[node(l)];
+    for (int l = 0; l < N; ++l) v[l] = buf[pb * PS + sg * N + l];
   }
-  const real s = act ? sdiag[3 * e + d] : (real)0;
+  const real s = act ? sdiag[3 * se[sg] + d] : (real)0;
   const real Hend = (real)H[0];
   const bool has_prev = closed || sg > 0;
   const bool has_next = closed || sg < len - 1;
@@ -1185,7 +1209,7 @@ __global__ void k_ko_line(int d, int len, int closed, const int32_t* __restrict_
   for (int it = 0; it < 6; ++it) {
     if (act) {
 #pragma unroll
-      for (int l = 0; l < N; ++l) buf[pb * len * N + sg * N + l] = v[l];
+      for (int l = 0; l < N; ++l) buf[pb * PS + sg * N + l] = v[l];
     }
     __syncthreads();
     if (act) {
@@ -1197,8 +1221,8 @@ __global__ void k_ko_line(int d, int len, int closed, const int32_t* __restrict_
         for (int p = 0; p < N; ++p) acc += Gs[l * N + p] * v[p];
         w[l] = s * acc;
       }
-      if (has_prev) w[0] += -s / ((real)2 * Hend) * (buf[pb * len * N + sp * N + (N - 1)] - v[0]);
-      if (has_next) w[N - 1] += s / ((real)2 * Hend) * (buf[pb * len * N + sn * N + 0] - v[N - 1]);
+      if (has_prev) w[0] += -s / ((real)2 * Hend) * (buf[pb * PS + sp * N + (N - 1)] - v[0]);
+      if (has_next) w[N - 1] += s / ((real)2 * Hend) * (buf[pb * PS + sn * N + 0] - v[N - 1]);
 #pragma unroll
       for (int l = 0; l < N; ++l) v[l] = w[l];
     }
@@ -1206,10 +1230,15 @@ __global__ void k_ko_line(int d, int len, int closed, const int32_t* __restrict_
   }
   if (act) {
 #pragma unroll
-    for (int l = 0; l < N; ++l) {
-      long long nd = node(l);
-      dst[nd] = dst[nd] + koT * v[l];
-    }
+    for (int l = 0; l < N; ++l) buf[pb * PS + sg * N + l] = v[l];
+  }
+  __syncthreads();
+  for (int q = tid; q < len * N2; q += blockDim.x) {
+    const int sq = q / N2;
+    int p, l;
+    split(q - sq * N2, p, l);
+    const long long nd = node(sq, p, l);
+    dst[nd] = dst[nd] + koT * buf[p * PS + sq * N + l];
   }
 }
 
@@ -1514,7 +1543,7 @@ static int ko_dispatch(const DevMesh& m, void* dst, const void* field, double ko
       continue;
     }
     dim3 grid((unsigned)m.nlines[d], N);
-    size_t smem = (size_t)N * len * N * sizeof(real);
+    size_t smem = (size_t)N * (len * N + 1) * sizeof(real) + (size_t)len * sizeof(int);
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(k_ko_line<N, real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_ko_line<N, real><<<grid, len * N, smem, s>>>(d, len, m.line_closed[d], m.lines[d], (real*)dst,
