@@ -554,9 +554,10 @@ def precision_study(wt, ctx, args, seed, p, ic, dt64, ref, E64_0, value64, hbm):
 def run_slab(args):
     """One solve split across ranks: the --elements^3 warped ADM solve of the default
     workload with its z element layers partitioned into one slab per rank
-    (slabs.py: a ghost layer beyond each cut, one halo exchange of the layers next
-    to the cuts per RK4 stage, NCCL point-to-point between GPUs; no exchange on
-    one GPU).  Strong scaling: the whole solve's DOF-updates over the maximum of
+    (slabs.py: a ghost layer beyond each cut, one halo exchange per RK4 stage of
+    the face planes the owned elements read across each cut -- or, with
+    --layer-halo, of whole layers -- NCCL point-to-point between GPUs; device
+    copies between slabs on one GPU).  Strong scaling: the whole solve's DOF-updates over the maximum of
     the ranks' device times."""
     import torch
 
@@ -592,8 +593,13 @@ def run_slab(args):
         dist.all_reduce(h, op=dist.ReduceOp.MIN)
     dt = 0.2 * float(h.item()) / wt.workloads.max_speed(p)
     bc = wt.make_bc3d([wt.BC_SOMMERFELD] * 6)
-    halo = S.DistHalo(slabs[0], dist) if dist is not None else S.LocalHalo(slabs)
-    S.step(slabs, halo, dt, args.warmup, bc)
+    if args.layer_halo:   # every slab layer computed, whole layers exchanged after the first half
+        halo = S.DistHalo(slabs[0], dist) if dist is not None else S.LocalHalo(slabs)
+        stepper = S.step
+    else:                 # owned layers only, face planes exchanged under the interior's first half
+        halo = S.DistFaceHalo(slabs[0], dist) if dist is not None else S.LocalFaceHalo(slabs)
+        stepper = S.step_faces
+    stepper(slabs, halo, dt, args.warmup, bc)
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
@@ -606,7 +612,7 @@ def run_slab(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    S.step(slabs, halo, dt, args.steps, bc)
+    stepper(slabs, halo, dt, args.steps, bc)
     ev1.record(stream)
     torch.cuda.synchronize()
     launches = ctx.launch_count() - n0
@@ -619,7 +625,8 @@ def run_slab(args):
     finite = not ctx.nonfinite()
     wb = 8 if prec == wt.WT_F64 else 4
     rng = mine[0]
-    halo_bytes = (wt.halo_size(slabs[0].ws) * wb) if nslabs > 1 else 0
+    halo_bytes = ((wt.halo_size(slabs[0].ws) if args.layer_halo else wt.halo_face_size(slabs[0].ws)) * wb
+                  if nslabs > 1 else 0)
     line = {
         "metric": "DOF-updates/s", "value": 2.0 * nodes * args.steps / t_max, "unit": "DOF-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps,
@@ -627,6 +634,8 @@ def run_slab(args):
         "data": "synthetic (seeded ADM background, 8 seeded Gaussian pulses; no dataset)",
         "config": {**workload_desc(args, nodes),
                    "parallelism": f"z-slabs x{nslabs}" + (" (one per rank)" if world > 1 else " in one process"),
+                   "halo": ("whole ghost layers, every slab layer computed" if args.layer_halo else
+                            "shared face planes, owned layers only, exchange under the interior layers' first half"),
                    "layers_per_slab": [r.nown for r in parts],
                    "ghost_layers_rank0": rng.ghost_lo + rng.ghost_hi,
                    "halo_bytes_per_message": halo_bytes,
@@ -856,6 +865,8 @@ def main():
                     help="solve: the large warped ADM solve (default; one independent solve per rank); "
                          "batch: batched uneven solves; serve: served Poisson request stream; slab: the "
                          "large solve split into one z-slab per rank with halo exchanges (strong scaling)")
+    ap.add_argument("--layer-halo", action="store_true",
+                    help="slab workload: exchange whole ghost layers and compute them (instead of face planes)")
     ap.add_argument("--slabs", type=int, default=1,
                     help="slab workload on one GPU: slabs held in one process (exchanged by device copies)")
     ap.add_argument("--solves", type=int, default=256, help="batch workload: number of solves")

@@ -424,6 +424,27 @@ int wt_halo_state_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, void* Pi, int stage, i
                        int pack);
 int wt_halo_size(const wt_ws* ws, long long* values);
 int wt_halo_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, void* buf, int pack);
+/* The face-plane exchange of a z-slab partition (no counterpart in the
+ * reference).  An owned element next to a cut reads, of the ghost element
+ * across it, only the face plane they share: the Phi trace its gradient's
+ * SAT reads and the flux trace its divergence's SAT reads.  So a partition
+ * may run both stage halves on its owned layers only
+ * (wt_rk4_stage_curved_layers: the elements of layers layer0 ..
+ * layer0 + nlayers - 1; an analytic cube's layer is M[0] M[1] consecutive
+ * elements) and exchange just those planes: wt_halo_face_copy packs (pack = 1)
+ * or unpacks (pack = 0) face `face` (4: -z, 5: +z) of element layer `layer` --
+ * per element the n^2 face values of the Phi the next stage reads (and, for
+ * the compensated FP32 form, its small part) and of the three flux
+ * components -- wt_halo_face_size values, asynchronously on the context
+ * stream.  The sender packs its boundary layer's face toward the cut, the
+ * receiver unpacks the same face of its ghost layer (the same element).
+ * Ghost layers are then never computed.  A time-dependent background is
+ * re-sampled at every part-1 call and its time advanced at the part-2 call of
+ * stage 3, so make one such call per step. */
+int wt_rk4_stage_curved_layers(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
+                               int stage, int part, int layer0, int nlayers, const wt_bc_desc* bc, int use_metric);
+int wt_halo_face_size(const wt_ws* ws, long long* values);
+int wt_halo_face_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, int face, void* buf, int pack);
 /* Fixed-step explicit Runge-Kutta methods of pick_integrator_first_order
  * (src/evolve.jl:43-48; evolve3d runs them with adaptive = false):
  * WT_ERK_RK4 (the fused low-storage RK4 above) and WT_ERK_TSIT5 (Tsitouras

@@ -1,5 +1,6 @@
 """GPU: one solve split into z-slabs (wt_mesh_create_slab, wt_rk4_stage_curved,
-wt_halo_copy; slabs.py) advances its owned element layers exactly as the
+wt_halo_copy; or wt_rk4_stage_curved_layers and wt_halo_face_copy; slabs.py)
+advances its owned element layers exactly as the
 undivided mesh does -- bit for bit, since every element's arithmetic depends
 only on its own data and its neighbours' face traces, which the halo exchange
 supplies -- through the n = 8 FP64 tensor-core kernels, the generic kernels, the
@@ -20,11 +21,16 @@ CASES = [  # N, M, slabs, periodic, precision, fp32 form, background
     (6, (2, 2, 6), 2, True, 0, None, 4),
     (8, (2, 2, 6), 3, False, 1, 3, 2),     # compensated FP32 form: the halo also carries Phi's small part
     (6, (2, 3, 6), 2, True, 1, 3, 2),      # compensated, generic kernels, periodic ring
+    (6, (2, 2, 4), 3, False, 0, None, 2),  # slabs of 2, 1 and 1 layers: a one-layer slab between two cuts
 ]
 
 
+@pytest.mark.parametrize("halo", ["layers", "faces"])
 @pytest.mark.parametrize("N,M,nslabs,periodic,prec,form,bg", CASES)
-def test_slab_solve_equals_whole_mesh(wt, ctx, N, M, nslabs, periodic, prec, form, bg):
+def test_slab_solve_equals_whole_mesh(wt, ctx, N, M, nslabs, periodic, prec, form, bg, halo):
+    """halo "layers": every slab layer computed, whole ghost layers exchanged after the first
+    stage half (step, LocalHalo); "faces": owned layers only, the shared face planes exchanged
+    while the interior layers' first half runs (step_faces, LocalFaceHalo)."""
     import torch
     S = wt.slabs
     kw = dict(warp_A=0.05, periodic=periodic, outer_tag=0 if periodic else 7, precision=prec)
@@ -48,7 +54,10 @@ def test_slab_solve_equals_whole_mesh(wt, ctx, N, M, nslabs, periodic, prec, for
     for s in slabs:
         wt.initial_data(s.mesh, wt.IC_GAUSSIANS, ic, s.Phi)
     assert min(s.mesh.min_spacing() for s in slabs) == whole.min_spacing()
-    S.step(slabs, S.LocalHalo(slabs), dt, nsteps, bc)
+    if halo == "layers":
+        S.step(slabs, S.LocalHalo(slabs), dt, nsteps, bc)
+    else:
+        S.step_faces(slabs, S.LocalFaceHalo(slabs), dt, nsteps, bc)
     Ps = torch.cat([s.owned(s.Phi) for s in slabs])
     Qs = torch.cat([s.owned(s.Pi) for s in slabs])
     assert torch.isfinite(Ps).all() and float(P.abs().max()) > 0
@@ -147,3 +156,24 @@ def test_dissipative_slab_solve_equals_whole_mesh(wt, ctx, N, M, nslabs, periodi
     for s in slabs:
         s.close()
     assert not ctx.nonfinite()
+
+
+def test_face_halo_errors_and_size(wt, ctx):
+    import torch
+    g = wt.Mesh.slab(ctx, 6, (2, 3, 5), 1, 3)
+    ws = wt.make_wave3d_workspace(g)
+    c = wt.sample_background3d(g, wt.BG_MINKOWSKI)
+    P, Q = g.zeros(), g.zeros()
+    with pytest.raises(wt.WaveToyError):          # nothing to size before a stage has run
+        wt.halo_face_size(ws)
+    with pytest.raises(wt.WaveToyError):          # the slab has layers 0..2
+        wt.rk4_stage_curved_layers(P, Q, c, ws, 1e-3, 0, 1, 2, 2, metric=True)
+    wt.rk4_stage_curved_layers(P, Q, c, ws, 1e-3, 0, 1, 1, 1, metric=True)
+    n = wt.halo_face_size(ws)
+    assert n == 6 * 6 ** 2 * 4                    # Phi + three flux components on the faces of 6 elements
+    buf = torch.empty(n, dtype=torch.float64, device="cuda")
+    with pytest.raises(wt.WaveToyError):
+        wt.halo_face_copy(ws, P, 0, 1, 3, buf, True)   # faces 4 (-z) and 5 (+z) only
+    with pytest.raises(wt.WaveToyError):
+        wt.halo_face_copy(ws, P, 0, 3, 5, buf, True)
+    wt.halo_face_copy(ws, P, 0, 1, 5, buf, True)

@@ -129,3 +129,71 @@ def test_exchange_over_gloo(world, Mz, periodic, depth):
         assert p.exitcode == 0
     for rank, got, want in out:
         assert got == want, rank
+
+
+class _FaceSlab:
+    """Stands in for slabs.Slab in DistFaceHalo: per local layer the two face planes
+    (-z, +z) as one value each, owned layers holding 10 * global layer + face."""
+
+    def __init__(self, r, Mz):
+        import torch
+        self.rng = r
+        self.f = torch.full((r.nz, 2), -1.0, dtype=torch.float64)
+        for z in range(r.first_owned, r.last_owned + 1):
+            for k in range(2):
+                self.f[z, k] = 10.0 * ((r.z0 + z) % Mz) + 4 + k
+        self.bufs = {}
+
+    def pack_face(self, st, layer, face):
+        return self.f[layer, face - 4].reshape(1).clone()
+
+    def unpack_face(self, st, layer, face, buf):
+        self.f[layer, face - 4] = buf[0]
+
+    def empty_face(self, which):
+        import torch
+        return self.bufs.setdefault(which, torch.empty(1, dtype=torch.float64))
+
+
+def _face_worker(rank, world, port, Mz, periodic, q):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    from conftest import load_package as lp
+    S = lp().slabs
+    r = S.partition(Mz, world, periodic)[rank]
+    s = _FaceSlab(r, Mz)
+    halo = S.DistFaceHalo(s, dist)
+    for st in range(3):   # repeated exchanges stay paired
+        halo.start(st)
+        halo.finish(st)
+    lo = float(s.f[0, 1]) if r.lower is not None else None
+    hi = float(s.f[r.nz - 1, 0]) if r.upper is not None else None
+    want_lo = 10.0 * ((r.z0) % Mz) + 5 if r.lower is not None else None
+    want_hi = 10.0 * ((r.z0 + r.nz - 1) % Mz) + 4 if r.upper is not None else None
+    q.put((rank, (lo, hi), (want_lo, want_hi)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,Mz,periodic", [(2, 6, False), (3, 7, True), (2, 4, True)])
+def test_face_halo_over_gloo(world, Mz, periodic):
+    """DistFaceHalo: the +z face of every slab's top owned layer lands in the +z face of its
+    upper neighbour's lower ghost layer, the -z face of its bottom owned layer in the -z face
+    of its lower neighbour's upper ghost layer (the same elements), over gloo ranks."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_face_worker, args=(r, world, port, Mz, periodic, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=180) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, got, want in out:
+        assert got == want, rank

@@ -91,6 +91,7 @@ struct wt_ws {
   const void* comp_for[2] = {nullptr, nullptr};
   void* erk = nullptr;    // explicit RK stage slopes: 2 x 8 x nn (Phi slopes, then Pi slopes)
   long long flux_block = 0;  // values per element block of F as the last fused stage wrote it (halo copies)
+  int flux_lay = 0;          // and its element-block layout (wt::n8_flux_layout; 0: node order)
   int halo_cp = 0;        // the last fused stage ran the compensated FP32 form (its halo adds Phit)
   // host-buffer evolution (evolve_host): device state, staging pair for the
   // copies to the host, per-sample energy partial sums -- kept between calls
@@ -1357,7 +1358,7 @@ static bool compensated(const wt::DevMesh& m, bool n8) {
 // One half of fused RK4 stage st (eps_ko = 0): part 1 launches K1 (flux, boundary
 // terms, the Phi stage update), part 2 K2 (divergence, the Pi stage update).
 static int rk4_stage_part(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int st,
-                          int part, const wt::ConsBC& b, int use_metric) {
+                          int part, const wt::ConsBC& b, int use_metric, long long e0 = 0, long long e1 = -1) {
   const wt::DevMesh& m = ws->mesh->m;
   cudaStream_t s = ctx->stream;
   void* SP[2] = {ws->S0, ws->S1};
@@ -1377,14 +1378,15 @@ static int rk4_stage_part(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi
   rkP.hcopy = ps.hcopy;
   ws->halo_cp = cp ? 1 : 0;
   ws->flux_block = n8 ? wt::n8_flux_block(m) : (long long)m.N * m.N * m.N;
+  ws->flux_lay = n8 ? wt::n8_flux_layout(m) : 0;
   if (part == 1) {
     prof_mark(ctx, 0);
     WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, inP, inQ, ws->F, nullptr, ws->bbuf, nullptr, use_metric, b, rkP,
-                                       s, n8), "rk4 K1"));
+                                       s, n8, e0, e1), "rk4 K1"));
     prof_mark(ctx, 0);
   } else {
     prof_mark(ctx, 1);
-    WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, nullptr, ws->bbuf, use_metric, b, rkQ, rkQ.nonfinite, s, n8),
+    WT_TRY(lrc(ctx, wt::launch_cons_k2(m, ws->F, nullptr, ws->bbuf, use_metric, b, rkQ, rkQ.nonfinite, s, n8, e0, e1),
                "rk4 K2"));
     prof_mark(ctx, 1);
   }
@@ -1431,6 +1433,7 @@ static int step_curved_fused(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* 
   };
   ws->halo_cp = 0;
   ws->flux_block = wt::n8_flux_block(m);
+  ws->flux_lay = wt::n8_flux_layout(m);
   if (coef->td) WT_TRY(coef_resample(ctx, coef, toff[0], s));
   prof_mark(ctx, 0);
   WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, Phi, Pi, FB[0], nullptr, ws->bbuf, nullptr, use_metric, b, rkP(0), s,
@@ -1633,9 +1636,11 @@ int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, v
   return rc;
 }
 
-int wt_rk4_stage_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int stage,
-                        int part, const wt_bc_desc* bc, int use_metric) {
-  WT_TRY(check_ws(ctx, ws));
+}  // extern "C"
+
+// One half of RK4 stage `stage` on the elements [e0, e1) (e1 < 0: all).
+static int stage_curved_range(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
+                              int stage, int part, long long e0, long long e1, const wt_bc_desc* bc, int use_metric) {
   if (!coef || !Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved: NULL argument");
   if (stage < 0 || stage > 3 || (part != 1 && part != 2))
     return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved: stage must be 0..3 and part 1 or 2");
@@ -1648,13 +1653,34 @@ int wt_rk4_stage_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, 
   comp_track(ws, Phi, Pi);
   const double toff[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};
   if (coef->td && part == 1) WT_TRY(coef_resample(ctx, coef, toff[stage], ctx->stream));
-  WT_TRY(rk4_stage_part(ctx, ws, coef, Phi, Pi, dt, stage, part, b, use_metric));
+  WT_TRY(rk4_stage_part(ctx, ws, coef, Phi, Pi, dt, stage, part, b, use_metric, e0, e1));
   if (coef->td && part == 2 && stage == 3) {
     WT_TRY(lrc(ctx, wt::launch_advance_time(coef->d_t, dt, ctx->stream), "background time"));
     ctx->launches += 1;
     coef->t += dt;
   }
   return 0;
+}
+
+extern "C" {
+
+int wt_rk4_stage_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int stage,
+                        int part, const wt_bc_desc* bc, int use_metric) {
+  WT_TRY(check_ws(ctx, ws));
+  return stage_curved_range(ctx, ws, coef, Phi, Pi, dt, stage, part, 0, -1, bc, use_metric);
+}
+
+int wt_rk4_stage_curved_layers(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
+                               int stage, int part, int layer0, int nlayers, const wt_bc_desc* bc, int use_metric) {
+  WT_TRY(check_ws(ctx, ws));
+  const wt::DevMesh& m = ws->mesh->m;
+  if (m.M[2] <= 0 || (long long)m.M[0] * m.M[1] * m.M[2] != m.Ne)
+    return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved_layers: the mesh has no element layers (analytic cubes only)");
+  if (layer0 < 0 || nlayers < 0 || layer0 + nlayers > m.M[2])
+    return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved_layers: layers outside the mesh");
+  const long long L = (long long)m.M[0] * m.M[1];
+  return stage_curved_range(ctx, ws, coef, Phi, Pi, dt, stage, part, layer0 * L, (layer0 + nlayers) * L, bc,
+                            use_metric);
 }
 
 int wt_rk4_stage_curved_ko(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int stage,
@@ -1761,6 +1787,32 @@ int wt_halo_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, void* 
     off += len[k];
   }
   return 0;
+}
+
+int wt_halo_face_size(const wt_ws* ws, long long* values) {
+  if (!ws || !values) return WT_EINVAL;
+  const wt::DevMesh& m = ws->mesh->m;
+  if (!ws->flux_block)
+    return fail(ws->ctx, WT_EINVAL, "wt_halo_face_size: no fused stage has run on this workspace yet");
+  *values = (long long)m.M[0] * m.M[1] * m.N * m.N * (ws->halo_cp ? 5 : 4);
+  return 0;
+}
+
+int wt_halo_face_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, int face, void* buf, int pack) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!Phi || !buf) return fail(ctx, WT_EINVAL, "wt_halo_face_copy: NULL argument");
+  const wt::DevMesh& m = ws->mesh->m;
+  if (stage < 0 || stage > 3) return fail(ctx, WT_EINVAL, "wt_halo_face_copy: stage must be 0..3");
+  if (layer < 0 || layer >= m.M[2]) return fail(ctx, WT_EINVAL, "wt_halo_face_copy: no such element layer");
+  if (face != 4 && face != 5) return fail(ctx, WT_EINVAL, "wt_halo_face_copy: face must be 4 (-z) or 5 (+z)");
+  if (!ws->flux_block) return fail(ctx, WT_EINVAL, "wt_halo_face_copy: no fused stage has run on this workspace yet");
+  // the Phi the next stage reads (compensated FP32 form: its high part and its
+  // small part) and the three flux components, on the face plane only
+  const PhiStage ps = phi_stage(ws, Phi, (stage + 1) % 4, ws->halo_cp != 0);
+  const long long L = (long long)m.M[0] * m.M[1];
+  return lrc(ctx, wt::launch_halo_face(m, layer * L, L, face == 5 ? m.N - 1 : 0, (void*)ps.in,
+                                       ws->halo_cp ? (void*)ps.phit : nullptr, ws->F, ws->flux_block, ws->flux_lay,
+                                       buf, pack, ctx->stream), "wt_halo_face_copy");
 }
 
 int wt_step_erk_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,

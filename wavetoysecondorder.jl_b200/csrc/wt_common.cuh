@@ -223,18 +223,22 @@ struct RKStage {
   void* hcopy = nullptr;
 };
 // K1: gradient, flux F, Phidot (+ affine/curv BC increments), optional RK epilogue for Phi.
+// e0, e1: the elements [e0, e1) the launch covers (e1 < 0: to the last element)
 int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
                    void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
-                   cudaStream_t s, bool n8 = false);
+                   cudaStream_t s, bool n8 = false, long long e0 = 0, long long e1 = -1);
 // K2: divergence of F (+ boundary increments), optional RK epilogue for Pi.
 int launch_cons_k2(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
-                   const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s, bool n8 = false);
+                   const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s, bool n8 = false,
+                   long long e0 = 0, long long e1 = -1);
 int launch_apply_D(const DevMesh& m, const void* u, void* out, int d, cudaStream_t s);
 // n = 8 curvilinear path: persistent, bulk-copy-pipelined, tensor cores (wt_cons_n8.cu)
+// [e0, e1): the elements the launch covers (e1 < 0: to the last element)
 int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
-                      void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s);
+                      void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s,
+                      long long e0 = 0, long long e1 = -1);
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
-                      const RKStage& rk, unsigned* flag, cudaStream_t s);
+                      const RKStage& rk, unsigned* flag, cudaStream_t s, long long e0 = 0, long long e1 = -1);
 // Fused RK4 stage (FP64): K2 of stage rkQ.stage (0..2, F_s in Fin) and K1 of
 // stage rkP.stage = rkQ.stage + 1 (Phi_{s+1} in Phi, F_{s+1} into Fout) in one
 // launch; Fin and Fout must differ.  rkQ.out may be NULL (Pi's stage value is
@@ -255,6 +259,12 @@ int launch_grad_n8(const DevMesh& m, const void* Phi, void* grad, unsigned* flag
 long long n8_padded_field_size(long long Ne);
 // values per element block of a flux component written by the n = 8 kernels (component c at F + c Ne block)
 long long n8_flux_block(const DevMesh& m);
+// its element-block layout: 1 Lay<double>, 2 Lay<float>, 3 LayC (0: node order, the generic kernels)
+int n8_flux_layout(const DevMesh& m);
+// face plane `row` of the L elements from e0 (Phi stage input, [small part], three flux
+// components) into buf (pack = 1) or back (pack = 0); see k_halo_face
+int launch_halo_face(const DevMesh& m, long long e0, long long L, int row, void* phi, void* phit, void* F, long long B,
+                     int lay, void* buf, int pack, cudaStream_t s);
 // True when an RHS evaluation takes the n = 8 pipelined path (both kernels take
 // the same path: K1 then writes F in the padded layout K2 reads).
 bool cons_n8_path(const DevMesh& m, const DevCoef& c, int use_metric, const ConsBC& bc, const RKStage& rkP,

@@ -37,6 +37,7 @@ struct Ep {
 template <typename real>
 struct K1P {
   long long Ne, nn;
+  long long e0, e1;  // single-solve launches: the elements [e0, e1) the launch covers
   const real* Phi;
   const real* Pi;
   const real* c10;  // a, b1, b2, b3, K11, K12, K13, K22, K23, K33 (nullptr: gradient only)
@@ -392,7 +393,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_, GenOcc<Ep<N>::N3 * EPB_>::va
   const int tid = threadIdx.x;
   const int le = tid / N3, t = tid - le * N3;
   const int i = t % N, j = (t / N) % N, k = t / N2;
-  long long e = (long long)blockIdx.x * EPB + le;
+  long long e = (BATCH ? 0 : P0.e0) + (long long)blockIdx.x * EPB + le;
   int sid = 0;
   bool valid;
   if constexpr (BATCH) {
@@ -403,7 +404,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_, GenOcc<Ep<N>::N3 * EPB_>::va
       e = tl.y;
     }
   } else {
-    valid = e < P0.Ne;
+    valid = e < P0.e1;
   }
   const K1P<real>& P = BATCH ? plist[sid] : P0;
   const long long ec = valid ? e : 0;  // clamp for address arithmetic
@@ -791,6 +792,7 @@ __global__ void __launch_bounds__(PipeK1<N, real, CP>::T, PipeK1<N, real, CP>::O
 template <typename real>
 struct K2P {
   long long Ne, nn;
+  long long e0, e1;  // single-solve launches: the elements [e0, e1) the launch covers
   const real* F0;
   const real* F1;
   const real* F2;
@@ -828,7 +830,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
   const int tid = threadIdx.x;
   const int le = tid / N3, t = tid - le * N3;
   const int i = t % N, j = (t / N) % N, k = t / N2;
-  long long e = (long long)blockIdx.x * EPB + le;
+  long long e = (BATCH ? 0 : P0.e0) + (long long)blockIdx.x * EPB + le;
   int sid = 0;
   bool valid;
   if constexpr (BATCH) {
@@ -839,7 +841,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
       e = tl.y;
     }
   } else {
-    valid = e < P0.Ne;
+    valid = e < P0.e1;
   }
   const K2P<real>& P = BATCH ? plist[sid] : P0;
   const long long ec = valid ? e : 0;
@@ -1248,7 +1250,7 @@ template <typename real>
 static K1P<real> k1p_params(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
                             void* bbuf, void* grad_out, const ConsBC& bc, const RKStage& rk) {
   K1P<real> P;
-  P.Ne = m.Ne; P.nn = m.nn;
+  P.Ne = m.Ne; P.nn = m.nn; P.e0 = 0; P.e1 = m.Ne;
   P.Phi = (const real*)Phi; P.Pi = (const real*)Pi;
   P.c10 = (const real*)c.c10;
   P.Ja = (const real*)m.Ja_r; P.invdetJ = (const real*)m.invdetJ_r; P.sdiag = (const real*)m.sdiag;
@@ -1277,7 +1279,7 @@ template <typename real>
 static K2P<real> k2p_params(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
                             const RKStage& rk, unsigned int* nonfinite, const void* F1, const void* F2) {
   K2P<real> P;
-  P.Ne = m.Ne; P.nn = m.nn;
+  P.Ne = m.Ne; P.nn = m.nn; P.e0 = 0; P.e1 = m.Ne;
   P.F0 = (const real*)F;
   P.F1 = F1 ? (const real*)F1 : (const real*)F + m.nn;
   P.F2 = F2 ? (const real*)F2 : (const real*)F + 2 * m.nn;
@@ -1295,9 +1297,12 @@ static K2P<real> k2p_params(const DevMesh& m, const void* F, void* Pidot, const 
 template <int N, typename real>
 static int k1_dispatch(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
                        void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
-                       cudaStream_t s) {
-  const K1P<real> P = k1p_params<real>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, bc, rk);
-  const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
+                       cudaStream_t s, long long e0 = 0, long long e1 = -1) {
+  K1P<real> P = k1p_params<real>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, bc, rk);
+  P.e0 = e0;
+  P.e1 = e1 < 0 ? m.Ne : e1;
+  const unsigned blocks = (unsigned)((P.e1 - P.e0 + Ep<N>::EPB - 1) / Ep<N>::EPB);
+  if (blocks == 0) return 0;
   constexpr bool F32 = std::is_same<real, float>::value;
   if (F32 && gen_cp(m, grad_out)) {
     if (use_metric)
@@ -1315,9 +1320,12 @@ static int k1_dispatch(const DevMesh& m, const DevCoef& c, const void* Phi, cons
 template <int N, typename real>
 static int k2_dispatch(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
                        const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s,
-                       const void* F1 = nullptr, const void* F2 = nullptr) {
-  const K2P<real> P = k2p_params<real>(m, F, Pidot, bbuf, bc, rk, nonfinite, F1, F2);
-  const unsigned blocks = (unsigned)((m.Ne + Ep<N>::EPB - 1) / Ep<N>::EPB);
+                       const void* F1 = nullptr, const void* F2 = nullptr, long long e0 = 0, long long e1 = -1) {
+  K2P<real> P = k2p_params<real>(m, F, Pidot, bbuf, bc, rk, nonfinite, F1, F2);
+  P.e0 = e0;
+  P.e1 = e1 < 0 ? m.Ne : e1;
+  const unsigned blocks = (unsigned)((P.e1 - P.e0 + Ep<N>::EPB - 1) / Ep<N>::EPB);
+  if (blocks == 0) return 0;
   if (use_metric)
     k_cons_k2<N, real, true, false, Ep<N>::EPB><<<blocks, Ep<N>::T, 0, s>>>(P, nullptr, nullptr, 0);
   else
@@ -1468,22 +1476,28 @@ bool cons_gen_cp_supported(const DevMesh& m) { return gen_cp(m, nullptr); }
 
 int launch_cons_k1(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
                    void* bbuf, void* grad_out, int use_metric, const ConsBC& bc, const RKStage& rk,
-                   cudaStream_t s, bool n8) {
-  if (n8 && grad_out == nullptr) return launch_cons_k1_n8(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, m.errflag, s);
+                   cudaStream_t s, bool n8, long long e0, long long e1) {
+  if (n8 && grad_out == nullptr)
+    return launch_cons_k1_n8(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, m.errflag, s, e0, e1);
   if (m.precision == 0) {
-    WT_DISPATCH_N(m.N, (k1_dispatch<NN, double>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, use_metric, bc, rk, s)));
+    WT_DISPATCH_N(m.N, (k1_dispatch<NN, double>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, use_metric, bc, rk, s, e0,
+                                                e1)));
   } else {
-    WT_DISPATCH_N(m.N, (k1_dispatch<NN, float>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, use_metric, bc, rk, s)));
+    WT_DISPATCH_N(m.N, (k1_dispatch<NN, float>(m, c, Phi, Pi, F, Phidot, bbuf, grad_out, use_metric, bc, rk, s, e0,
+                                               e1)));
   }
 }
 
 int launch_cons_k2(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, int use_metric,
-                   const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s, bool n8) {
-  if (n8) return launch_cons_k2_n8(m, F, Pidot, bbuf, bc, rk, m.errflag, s);
+                   const ConsBC& bc, const RKStage& rk, unsigned int* nonfinite, cudaStream_t s, bool n8,
+                   long long e0, long long e1) {
+  if (n8) return launch_cons_k2_n8(m, F, Pidot, bbuf, bc, rk, m.errflag, s, e0, e1);
   if (m.precision == 0) {
-    WT_DISPATCH_N(m.N, (k2_dispatch<NN, double>(m, F, Pidot, bbuf, use_metric, bc, rk, nonfinite, s)));
+    WT_DISPATCH_N(m.N, (k2_dispatch<NN, double>(m, F, Pidot, bbuf, use_metric, bc, rk, nonfinite, s, nullptr,
+                                                nullptr, e0, e1)));
   } else {
-    WT_DISPATCH_N(m.N, (k2_dispatch<NN, float>(m, F, Pidot, bbuf, use_metric, bc, rk, nonfinite, s)));
+    WT_DISPATCH_N(m.N, (k2_dispatch<NN, float>(m, F, Pidot, bbuf, use_metric, bc, rk, nonfinite, s, nullptr,
+                                               nullptr, e0, e1)));
   }
 }
 

@@ -316,6 +316,7 @@ __device__ __forceinline__ void n8_rk_cp(int stage, double dt, float k, float hi
 template <typename real>
 struct K1N8 {
   long long Ne, nn;
+  long long e0;  // single-solve launches: the first element (the launch covers ntiles elements from it)
   const real* Phi;
   const real* Pi;
   const real* c10;
@@ -468,13 +469,13 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
   // node-phase coordinates of this thread
   const int ti = tid & 7, tj = (tid >> 3) & 7, tk = tid >> 6;
   const int tpad = Lay<real>::at(tid), tphi = PhiLay<real>::at(tid);
-  const long long T = BATCH ? ntiles : P.Ne;
+  const long long T = ntiles;
   const long long GS = gridDim.x;
   // tile t = (solve, element); (-1, -1) past the end
   auto tile_at = [&](long long t) -> int2 {
     if (t >= T) return make_int2(-1, -1);
     if constexpr (BATCH) return tiles[t];
-    else return make_int2(0, (int)t);
+    else return make_int2(0, (int)(P.e0 + t));
   };
   auto prm = [&](int sidx) -> const K1N8<real>& {
     if constexpr (BATCH) return plist[sidx];
@@ -758,6 +759,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
 template <typename real>
 struct K2N8 {
   long long Ne, nn;
+  long long e0;  // single-solve launches: the first element (see K1N8)
   const real* F0;
   const real* F1;
   const real* F2;
@@ -836,12 +838,12 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
   const bool need_acc = P.epi && P.stage >= 1;
   const bool need_comp = comp_on && P.stage == 3;
   const unsigned tx_bytes = (unsigned)(K2_NF * FS * sizeof(real));
-  const long long T = BATCH ? ntiles : P.Ne;
+  const long long T = ntiles;
   const long long GS = gridDim.x;
   auto tile_at = [&](long long t) -> int2 {
     if (t >= T) return make_int2(-1, -1);
     if constexpr (BATCH) return tiles[t];
-    else return make_int2(0, (int)t);
+    else return make_int2(0, (int)(P.e0 + t));
   };
   auto prm = [&](int sidx) -> const K2N8<real>& {
     if constexpr (BATCH) return plist[sidx];
@@ -1662,12 +1664,12 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
   const unsigned txA = (unsigned)(K1C_STAGE * sizeof(real));
   const unsigned txB = (unsigned)((GR ? 1 : 12 + need_y + need_acc + need_comp) * N3 * sizeof(real));
   const double inv2Hd = 1.0 / (2.0 * P.H[0]);
-  const long long T = BATCH ? ntiles : P.Ne;
+  const long long T = ntiles;
   const long long GS = gridDim.x;
   auto tile_at = [&](long long t) -> int2 {
     if (t >= T) return make_int2(-1, -1);
     if constexpr (BATCH) return tiles[t];
-    else return make_int2(0, (int)t);
+    else return make_int2(0, (int)(P.e0 + t));
   };
   auto prm = [&](int sidx) -> const K1N8<real>& {
     if constexpr (BATCH) return plist[sidx];
@@ -1998,12 +2000,12 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
   const bool need_comp = comp_on && P.stage == 3;
   const unsigned tx_bytes = (unsigned)(K2C_STAGE * sizeof(real));
   const unsigned txB = (unsigned)((1 + need_y + need_acc + need_comp) * N3 * sizeof(real));
-  const long long T = BATCH ? ntiles : P.Ne;
+  const long long T = ntiles;
   const long long GS = gridDim.x;
   auto tile_at = [&](long long t) -> int2 {
     if (t >= T) return make_int2(-1, -1);
     if constexpr (BATCH) return tiles[t];
-    else return make_int2(0, (int)t);
+    else return make_int2(0, (int)(P.e0 + t));
   };
   auto prm = [&](int sidx) -> const K2N8<real>& {
     if constexpr (BATCH) return plist[sidx];
@@ -2292,7 +2294,7 @@ template <typename real>
 static K1N8<real> k1n8_params(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F,
                               void* Phidot, void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag) {
   K1N8<real> P;
-  P.Ne = m.Ne; P.nn = m.nn;
+  P.Ne = m.Ne; P.nn = m.nn; P.e0 = 0;
   P.Phi = (const real*)Phi; P.Pi = (const real*)Pi; P.c10 = (const real*)c.c10;
   P.Ja = (const real*)m.Ja_n8; P.invdetJ = (const real*)m.invdetJ_r;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
@@ -2319,7 +2321,7 @@ template <typename real>
 static K2N8<real> k2n8_params(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
                               const RKStage& rk, unsigned* flag) {
   K2N8<real> P;
-  P.Ne = m.Ne; P.nn = m.nn;
+  P.Ne = m.Ne; P.nn = m.nn; P.e0 = 0;
   const long long fs = m.Ne * n8_fs(m);
   P.F0 = (const real*)F; P.F1 = (const real*)F + fs; P.F2 = (const real*)F + 2 * fs;
   P.Ja = (const real*)m.Ja_n8; P.invdetJ = (const real*)m.invdetJ_r;
@@ -2414,13 +2416,17 @@ static int n8_dispatch(int which, int precision, int fp32_form, const void* hP, 
 }
 
 int launch_cons_k1_n8(const DevMesh& m, const DevCoef& c, const void* Phi, const void* Pi, void* F, void* Phidot,
-                      void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s) {
+                      void* bbuf, const ConsBC& bc, const RKStage& rk, unsigned* flag, cudaStream_t s, long long e0,
+                      long long e1) {
+  if (e1 < 0) e1 = m.Ne;
   if (m.precision == 0) {
-    const K1N8<double> P = k1n8_params<double>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag);
-    return n8_dispatch<false>(1, 0, m.fp32_form, &P, nullptr, nullptr, m.Ne, s);
+    K1N8<double> P = k1n8_params<double>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag);
+    P.e0 = e0;
+    return n8_dispatch<false>(1, 0, m.fp32_form, &P, nullptr, nullptr, e1 - e0, s);
   }
-  const K1N8<float> P = k1n8_params<float>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag);
-  return n8_dispatch<false>(1, 1, m.fp32_form, &P, nullptr, nullptr, m.Ne, s);
+  K1N8<float> P = k1n8_params<float>(m, c, Phi, Pi, F, Phidot, bbuf, bc, rk, flag);
+  P.e0 = e0;
+  return n8_dispatch<false>(1, 1, m.fp32_form, &P, nullptr, nullptr, e1 - e0, s);
 }
 
 int launch_cons_fk_n8(const DevMesh& m, const DevCoef& c, const void* Fin, void* Fout, const void* Phi, void* bbuf,
@@ -2443,13 +2449,16 @@ int launch_cons_fk_n8(const DevMesh& m, const DevCoef& c, const void* Fin, void*
 }
 
 int launch_cons_k2_n8(const DevMesh& m, const void* F, void* Pidot, const void* bbuf, const ConsBC& bc,
-                      const RKStage& rk, unsigned* flag, cudaStream_t s) {
+                      const RKStage& rk, unsigned* flag, cudaStream_t s, long long e0, long long e1) {
+  if (e1 < 0) e1 = m.Ne;
   if (m.precision == 0) {
-    const K2N8<double> P = k2n8_params<double>(m, F, Pidot, bbuf, bc, rk, flag);
-    return n8_dispatch<false>(2, 0, m.fp32_form, &P, nullptr, nullptr, m.Ne, s);
+    K2N8<double> P = k2n8_params<double>(m, F, Pidot, bbuf, bc, rk, flag);
+    P.e0 = e0;
+    return n8_dispatch<false>(2, 0, m.fp32_form, &P, nullptr, nullptr, e1 - e0, s);
   }
-  const K2N8<float> P = k2n8_params<float>(m, F, Pidot, bbuf, bc, rk, flag);
-  return n8_dispatch<false>(2, 1, m.fp32_form, &P, nullptr, nullptr, m.Ne, s);
+  K2N8<float> P = k2n8_params<float>(m, F, Pidot, bbuf, bc, rk, flag);
+  P.e0 = e0;
+  return n8_dispatch<false>(2, 1, m.fp32_form, &P, nullptr, nullptr, e1 - e0, s);
 }
 
 // Gradient-only launch (the energy's split-form gradient, apply_gradient3d! with the
@@ -2519,6 +2528,54 @@ int launch_wait_selftest(long long polls, int arrive, unsigned* flag, cudaStream
   k_wait_selftest<<<1, 32, 0, s>>>(polls, arrive, flag);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
+
+// ---- face-plane halo of a z-slab partition ---------------------------------------------
+// Pack (pack = 1) or unpack (pack = 0) the face plane `row` (0: the -z face, N - 1:
+// the +z face) of the L elements from e0: per element and face point pq = p + N q,
+// the Phi the next stage reads, its small part (phit != NULL: the compensated FP32
+// form), then the three flux components (element blocks of B words in layout lay:
+// 0 node order, 1 Lay<double>, 2 Lay<float>, 3 LayC).  buf: [component][element][pq].
+template <typename real>
+__global__ void k_halo_face(int N, long long e0, long long L, int row, real* phi, real* phit, real* F, long long Ne,
+                            long long B, int lay, real* buf, int pack) {
+  const long long N2 = (long long)N * N, N3 = N2 * N, tot = L * N2;
+  const int nc = phit ? 5 : 4;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < tot; v += (long long)gridDim.x * blockDim.x) {
+    const long long l = v / N2;
+    const int pq = (int)(v - l * N2), p = pq % N, q = pq / N;
+    const long long e = e0 + l;
+    const int node = p + N * (q + N * row);
+    const int fo = lay == 1 ? n8::Lay<double>::at(node) : lay == 2 ? n8::Lay<float>::at(node)
+                 : lay == 3 ? n8::LayC::at(node) : node;
+    real* ptr[5];
+    int c = 0;
+    ptr[c++] = phi + e * N3 + node;
+    if (phit) ptr[c++] = phit + e * N3 + node;
+    for (int k = 0; k < 3; ++k) ptr[c++] = F + (long long)k * Ne * B + e * B + fo;
+    for (int k = 0; k < nc; ++k) {
+      real* b = buf + (long long)k * tot + v;
+      if (pack) *b = *ptr[k];
+      else *ptr[k] = *b;
+    }
+  }
+}
+
+int launch_halo_face(const DevMesh& m, long long e0, long long L, int row, void* phi, void* phit, void* F, long long B,
+                     int lay, void* buf, int pack, cudaStream_t s) {
+  const long long tot = L * m.N * m.N;
+  if (tot <= 0) return 0;
+  const unsigned blocks = (unsigned)((tot + 255) / 256 < 4096 ? (tot + 255) / 256 : 4096);
+  if (m.precision == 0)
+    k_halo_face<double><<<blocks, 256, 0, s>>>(m.N, e0, L, row, (double*)phi, (double*)phit, (double*)F, m.Ne, B, lay,
+                                               (double*)buf, pack);
+  else
+    k_halo_face<float><<<blocks, 256, 0, s>>>(m.N, e0, L, row, (float*)phi, (float*)phit, (float*)F, m.Ne, B, lay,
+                                              (float*)buf, pack);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// element-block layout of the flux the n = 8 kernels of this mesh write (see k_halo_face)
+int n8_flux_layout(const DevMesh& m) { return m.precision == 0 ? 1 : n8_layout(m) ? 3 : 2; }
 
 // ---- work-list batching -------------------------------------------------------------
 size_t cons_n8_param_size(int precision, int which) {

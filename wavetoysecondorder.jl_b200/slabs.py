@@ -210,6 +210,54 @@ class Slab:
     def unpack(self, st: int, layer: int, buf):
         wt.halo_copy(self.ws, self.Phi, st, layer, buf, False)
 
+    # the face-plane halo (step_faces): both stage halves run on the owned layers only
+    def stage_layers(self, dt: float, st: int, part: int, layer0: int, nlayers: int, bc3d=None,
+                     metric: bool = True):
+        if nlayers > 0:
+            wt.rk4_stage_curved_layers(self.Phi, self.Pi, self.coef, self.ws, dt, st, part, layer0, nlayers,
+                                       bc3d=bc3d, metric=metric)
+
+    def boundary_layers(self):
+        """The owned layers next to a cut (their face planes are sent)."""
+        r = self.rng
+        out = []
+        if r.lower is not None:
+            out.append(r.first_owned)
+        if r.upper is not None and r.last_owned not in out:
+            out.append(r.last_owned)
+        return out
+
+    def interior_runs(self):
+        """(layer0, nlayers) runs of the owned layers not next to a cut."""
+        b = set(self.boundary_layers())
+        runs, start = [], None
+        for z in range(self.rng.first_owned, self.rng.last_owned + 2):
+            inside = z <= self.rng.last_owned and z not in b
+            if inside and start is None:
+                start = z
+            elif not inside and start is not None:
+                runs.append((start, z - start))
+                start = None
+        return runs
+
+    def _face_buf(self, key):
+        import torch
+        if key not in self._send:
+            self._send[key] = torch.empty(wt.halo_face_size(self.ws), dtype=self.mesh.dtype, device=self.Phi.device)
+        return self._send[key]
+
+    def pack_face(self, st: int, layer: int, face: int):
+        buf = self._face_buf(("face", layer, face))
+        wt.halo_face_copy(self.ws, self.Phi, st, layer, face, buf, True)
+        return buf
+
+    def unpack_face(self, st: int, layer: int, face: int, buf):
+        wt.halo_face_copy(self.ws, self.Phi, st, layer, face, buf, False)
+
+    def empty_face(self, which: str):
+        """The receive buffer of the face halo from below ("lo") or above ("hi")."""
+        return self._face_buf(("recv", which))
+
     # the state halo of the dissipative stepping (depth layers of Phi and Pi)
     def stage_ko(self, dt: float, st: int, eps_KO: float, bc3d=None, metric: bool = True):
         wt.rk4_stage_curved_ko(self.Phi, self.Pi, self.coef, self.ws, dt, st, eps_KO, bc3d=bc3d, metric=metric)
@@ -297,6 +345,114 @@ class DistStateHalo:
         s = self.slab
         exchange(s.rng, lambda layer: s.pack_state(st, layer), lambda layer, buf: s.unpack_state(st, layer, buf),
                  dist_send_recv(self.dist, self.group), s.empty_state)
+
+
+def exchange_faces(rng: SlabRange, pack_up: Callable[[], object], pack_down: Callable[[], object],
+                   recv_lo: object, recv_hi: object, send_recv: Callable[[list, list], None]):
+    """Post the face-plane messages of slab rng in exchange()'s two-phase order: the +z face
+    of its top owned layer up while receiving its lower ghost's face from below, then the
+    -z face of its bottom owned layer down while receiving its upper ghost's face from above."""
+    sends, recvs = [], []
+    if rng.upper is not None:
+        sends.append((rng.upper, pack_up()))
+    if rng.lower is not None:
+        recvs.append((rng.lower, recv_lo))
+    if rng.lower is not None:
+        sends.append((rng.lower, pack_down()))
+    if rng.upper is not None:
+        recvs.append((rng.upper, recv_hi))
+    return send_recv(sends, recvs)
+
+
+class LocalFaceHalo:
+    """The face-plane halo between slabs of this process (device copies).  start()
+    packs every slab's boundary faces and unpacks them into the neighbours' ghost
+    faces; finish() has nothing left to do."""
+
+    def __init__(self, slabs: List[Slab]):
+        self.slabs = slabs
+
+    def start(self, st: int):
+        msgs = {}
+        for s in self.slabs:
+            r = s.rng
+            if r.upper is not None:
+                msgs[(r.index, "up")] = s.pack_face(st, r.last_owned, 5)
+            if r.lower is not None:
+                msgs[(r.index, "down")] = s.pack_face(st, r.first_owned, 4)
+        for s in self.slabs:
+            r = s.rng
+            if r.lower is not None:
+                s.unpack_face(st, 0, 5, msgs[(r.lower, "up")])
+            if r.upper is not None:
+                s.unpack_face(st, r.nz - 1, 4, msgs[(r.upper, "down")])
+
+    def finish(self, st: int):
+        pass
+
+
+class DistFaceHalo:
+    """The face-plane halo, one slab per rank, over torch.distributed.  start() packs and
+    posts the messages as one batch of point-to-point operations (NCCL runs them on its
+    own stream, after the packs); finish() makes the current stream wait for them and
+    unpacks -- so that work enqueued in between (the interior layers' first stage half)
+    overlaps the transfer."""
+
+    def __init__(self, slab: Slab, dist, group=None, rank_of: Callable[[int], int] = lambda s: s):
+        self.slab, self.dist, self.group, self.rank_of = slab, dist, group, rank_of
+        self._works = []
+
+    def start(self, st: int):
+        s, r = self.slab, self.slab.rng
+
+        def post(sends, recvs):
+            order = []
+            for k in range(max(len(sends), len(recvs))):
+                if k < len(sends):
+                    order.append((self.dist.isend, sends[k]))
+                if k < len(recvs):
+                    order.append((self.dist.irecv, recvs[k]))
+            ops = [self.dist.P2POp(op, buf, self.rank_of(peer), self.group) for op, (peer, buf) in order]
+            self._works = self.dist.batch_isend_irecv(ops) if ops else []
+
+        self._lo = s.empty_face("lo") if r.lower is not None else None
+        self._hi = s.empty_face("hi") if r.upper is not None else None
+        exchange_faces(r, lambda: s.pack_face(st, r.last_owned, 5), lambda: s.pack_face(st, r.first_owned, 4),
+                       self._lo, self._hi, post)
+
+    def finish(self, st: int):
+        for w in self._works:
+            w.wait()
+        self._works = []
+        s, r = self.slab, self.slab.rng
+        if r.lower is not None:
+            s.unpack_face(st, 0, 5, self._lo)
+        if r.upper is not None:
+            s.unpack_face(st, r.nz - 1, 4, self._hi)
+
+
+def step_faces(slabs: List[Slab], halo, dt: float, nsteps: int, bc3d=None, metric: bool = True):
+    """nsteps RK4 steps of the partitioned solve with the face-plane halo (depth-1
+    partitions, eps_KO = 0): per stage the first half on the owned layers next to a cut,
+    the exchange started, the first half on the other owned layers (overlapping the
+    transfer when the halo is asynchronous), the exchange finished, the second half on
+    the owned layers.  Ghost layers are never computed: only the face planes the owned
+    elements read are written into them.  The ghost layers of the starting state must
+    hold the state (as after set-up from the analytic initial data on the whole slab)."""
+    if any(s.rng.depth != 1 for s in slabs):
+        raise ValueError("the face halo serves depth-1 partitions")
+    for _ in range(int(nsteps)):
+        for st in range(4):
+            for s in slabs:
+                for z in s.boundary_layers():
+                    s.stage_layers(dt, st, 1, z, 1, bc3d, metric)
+            halo.start(st)
+            for s in slabs:
+                for z0, nz in s.interior_runs():
+                    s.stage_layers(dt, st, 1, z0, nz, bc3d, metric)
+            halo.finish(st)
+            for s in slabs:
+                s.stage_layers(dt, st, 2, s.rng.first_owned, s.rng.nown, bc3d, metric)
 
 
 def step_ko(slabs: List[Slab], halo, dt: float, nsteps: int, eps_KO: float, bc3d=None, metric: bool = True):

@@ -157,6 +157,8 @@ def library():
         "wt_mesh_create_slab": [vp, C.POINTER(_MeshDesc), i, i, pvp],
         "wt_rk4_stage_curved": [vp, vp, vp, vp, vp, d, i, i, C.POINTER(_BcDesc), i],
         "wt_halo_size": [vp, C.POINTER(ll)], "wt_halo_copy": [vp, vp, vp, i, i, vp, i],
+        "wt_rk4_stage_curved_layers": [vp, vp, vp, vp, vp, d, i, i, i, i, C.POINTER(_BcDesc), i],
+        "wt_halo_face_size": [vp, C.POINTER(ll)], "wt_halo_face_copy": [vp, vp, vp, i, i, i, vp, i],
         "wt_workspace_set_mu": [vp, d], "wt_workspace_set_fused": [vp, i],
         "wt_rk4_stage_curved_ko": [vp, vp, vp, vp, vp, d, i, d, C.POINTER(_BcDesc), i],
         "wt_halo_state_copy": [vp, vp, vp, vp, i, i, i, vp, i],
@@ -970,6 +972,30 @@ def rk4_stage_curved(Phi, Pi, coef: Coef, ws: Workspace, dt: float, stage: int, 
     p, keep = _bcptr(bc3d)
     ws.ctx.check(library().wt_rk4_stage_curved(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt), int(stage),
                                                int(part), p, int(bool(metric))), "wt_rk4_stage_curved")
+
+
+def rk4_stage_curved_layers(Phi, Pi, coef: Coef, ws: Workspace, dt: float, stage: int, part: int, layer0: int,
+                            nlayers: int, bc3d: Optional[BC3D] = None, metric: bool = False):
+    """rk4_stage_curved on the element layers layer0 .. layer0 + nlayers - 1 only
+    (wt_rk4_stage_curved_layers; analytic cubes and slabs)."""
+    p, keep = _bcptr(bc3d)
+    ws.ctx.check(library().wt_rk4_stage_curved_layers(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt),
+                                                      int(stage), int(part), int(layer0), int(nlayers), p,
+                                                      int(bool(metric))), "wt_rk4_stage_curved_layers")
+
+
+def halo_face_size(ws: Workspace) -> int:
+    """Values of one packed face-plane halo (wt_halo_face_size; after a first stage part on ws)."""
+    n = C.c_longlong()
+    ws.ctx.check(library().wt_halo_face_size(ws.h, C.byref(n)), "wt_halo_face_size")
+    return n.value
+
+
+def halo_face_copy(ws: Workspace, Phi, stage: int, layer: int, face: int, buf, pack: bool):
+    """Face `face` (4: -z, 5: +z) of element layer `layer`: the next stage's Phi and the three flux
+    components on that face plane, into buf (pack) or back (wt_halo_face_copy)."""
+    ws.ctx.check(library().wt_halo_face_copy(ws.ctx.h, ws.h, _ptr(Phi), int(stage), int(layer), int(face),
+                                             _ptr(buf), int(bool(pack))), "wt_halo_face_copy")
 
 
 def rk4_stage_curved_ko(Phi, Pi, coef: Coef, ws: Workspace, dt: float, stage: int, eps_KO: float,
