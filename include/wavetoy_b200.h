@@ -379,6 +379,15 @@ int wt_rhs_curved4(wt_ctx* ctx, wt_ws* ws, const void* phi, const void* phidot, 
 /* wave3d_energy (src/wave3d_curved.jl:268-287). */
 int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, int use_metric,
               double* E);
+/* The lapse-weighted energy (no counterpart in the reference):
+ * E_alpha = sum 1/2 [(alpha/sqrt(gamma)) Pi^2 + alpha sqrt(gamma) gamma^{ij} dPhi_i dPhi_j] H,
+ * the reference energy's integrand times the lapse.  wave3d_energy is exactly
+ * conserved only for alpha = 1 (src/wave3d_curved.jl:263-266); for a static
+ * background with zero shift the split-form semi-discretisation conserves
+ * E_alpha instead (its gradient / divergence pair is skew-adjoint in Hd), so it
+ * is the drift monitor for alpha != 1.  Same arguments as wt_energy. */
+int wt_energy_lapse(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, int use_metric,
+                    double* E);
 /* SIPG Hamiltonian 1/2<ut,ut>_H - 1/2<u, L_SAT u>_H (test/kernels3d_tests.jl:39-47). */
 int wt_energy_sipg(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, double tau, double* E);
 /* sqrt(sum (a-b)^2 H), H = Hphys (use_metric 0) or Hd (1) (src/evolve.jl:1353-1354);

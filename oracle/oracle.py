@@ -73,6 +73,8 @@ def lib():
         L.or_rhs_curved.argtypes = [vp, vp, vp, vp, vp, vp, d, C.POINTER(_BC), i, vp]
         L.or_energy.restype = d
         L.or_energy.argtypes = [vp, vp, vp, vp, i]
+        L.or_energy_w.restype = d
+        L.or_energy_w.argtypes = [vp, vp, vp, vp, i, i]
         L.or_rhs_sipg.argtypes = [vp, vp, vp, vp, vp, d, d]
         L.or_rhs_strong.argtypes = [vp, vp, vp, vp, d, d]
         L.or_lap_strong_cons.argtypes = [vp, vp, vp, d, d]
@@ -219,9 +221,10 @@ class OracleMesh:
                             int(use_metric), _p(D))
         return (Phid, Pid, D) if want_grad else (Phid, Pid)
 
-    def energy(self, coef, Phi, Pi, use_metric=False):
-        return lib().or_energy(self.h, _p(coef), _p(np.ascontiguousarray(Phi)), _p(np.ascontiguousarray(Pi)),
-                               int(use_metric))
+    def energy(self, coef, Phi, Pi, use_metric=False, lapse=False):
+        """wave3d_energy; lapse=True: the alpha-weighted norm (see or_energy_w)."""
+        return lib().or_energy_w(self.h, _p(coef), _p(np.ascontiguousarray(Phi)), _p(np.ascontiguousarray(Pi)),
+                                 int(use_metric), int(bool(lapse)))
 
     def rhs_sipg(self, u, ut, bdry_values=(0,) * 6, tau=20.0, R=np.inf):
         out = np.zeros(self.nn)

@@ -906,7 +906,12 @@ void or_rhs_curved(void* h, const double* coef, const double* Phi, const double*
 
 // wave3d_energy (src/wave3d_curved.jl:268-287):
 // E = sum 1/2 [Pi^2/sqrtg + sqrtg gu^{ij} dPhi_i dPhi_j] H.
-double or_energy(void* h, const double* coef, const double* Phi, const double* Pi, int use_metric) {
+// lapse = 1: the same integrand times alpha (coef field 0),
+// E_alpha = sum 1/2 [(alpha/sqrtg) Pi^2 + alpha sqrtg gu^{ij} dPhi_i dPhi_j] H -- the
+// norm the first-order system conserves for a static background with zero
+// shift (the reference's wave3d_energy is exactly conserved only for alpha = 1,
+// src/wave3d_curved.jl:263-266).
+double or_energy_w(void* h, const double* coef, const double* Phi, const double* Pi, int use_metric, int lapse) {
   Mesh& m = *static_cast<Mesh*>(h);
   const long nn = m.nn();
   std::vector<double> D1(nn), D2(nn), D3(nn);
@@ -919,11 +924,15 @@ double or_energy(void* h, const double* coef, const double* Phi, const double* P
   double E = 0.0;
   for (long n = 0; n < nn; ++n) {
     double d1 = D1[n], d2 = D2[n], d3 = D3[n];
-    E += (Pi[n] * Pi[n] / sg[n] +
-          sg[n] * (g11[n] * d1 * d1 + g22[n] * d2 * d2 + g33[n] * d3 * d3 + 2 * g12[n] * d1 * d2 +
-                   2 * g13[n] * d1 * d3 + 2 * g23[n] * d2 * d3)) * H[n] / 2;
+    const double w = lapse ? coef[n] : 1.0;
+    E += w * (Pi[n] * Pi[n] / sg[n] +
+              sg[n] * (g11[n] * d1 * d1 + g22[n] * d2 * d2 + g33[n] * d3 * d3 + 2 * g12[n] * d1 * d2 +
+                       2 * g13[n] * d1 * d3 + 2 * g23[n] * d2 * d3)) * H[n] / 2;
   }
   return E;
+}
+double or_energy(void* h, const double* coef, const double* Phi, const double* Pi, int use_metric) {
+  return or_energy_w(h, coef, Phi, Pi, use_metric, 0);
 }
 
 // ---------------------------------------------------------------------------

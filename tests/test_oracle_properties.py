@@ -301,3 +301,46 @@ def test_classify_face(O):
         wt.validate_bc1d(wt.FACE_OUTFLOW, wt.BC_SOMMERFELD, "-x side")
     with pytest.raises(ValueError):
         wt.bc1d_kind("bogus")
+
+
+def adm_no_shift(wt, seed, scale=1.0):
+    """The perturbed ADM background's parameters with zero shift (beta = 0)."""
+    p = list(wt.workloads.adm_params(seed, scale))
+    p[1] = 0.0
+    return p
+
+
+def test_lapse_weighted_energy_is_conserved_without_shift(O, wt):
+    """The reference's wave3d_energy is exactly conserved only for alpha = 1
+    (src/wave3d_curved.jl:263-266).  With a static lapse alpha != 1 and zero shift,
+    the semi-discrete split-form system conserves the alpha-weighted norm
+    E_a = 1/2 sum [(alpha/sqrtg) Pi^2 + alpha sqrtg gu^{ij} dPhi_i dPhi_j] Hd (the
+    gradient/divergence pair is skew-adjoint in Hd): dE_a/dt = 0 to round-off on a
+    periodic warped mesh, while d/dt of the reference energy is not."""
+    N, M = 5, 2
+    m = O.OracleMesh(N, M, A=0.05, periodic=True)
+    coef = m.background(2, adm_no_shift(wt, 7, 2.0))
+    nn = m.nn
+    rng = np.random.default_rng(3)
+    x, y, z = m.coords()
+    Phi = np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y) + 0.3 * np.sin(2 * np.pi * (y + z))
+    Pi = 0.5 * np.cos(2 * np.pi * (x - z)) + 0.1 * rng.standard_normal(nn)
+    Phid, Pid, D = m.rhs_curved(coef, Phi, Pi, eps_ko=0.0, use_metric=True, want_grad=True)
+    _, _, Dd = m.rhs_curved(coef, Phid, Pi, eps_ko=0.0, use_metric=True, want_grad=True)
+    Hd = m.get("Hd")
+    al, sg = coef[:nn], coef[nn:2 * nn]
+    gu = [coef[(5 + c) * nn:(6 + c) * nn] for c in range(6)]   # g11 g12 g13 g22 g23 g33
+    K = np.array([[gu[0], gu[1], gu[2]], [gu[1], gu[3], gu[4]], [gu[2], gu[4], gu[5]]])
+    g = D.reshape(3, nn)
+    gd = Dd.reshape(3, nn)
+    Kg = np.einsum("ijn,jn->in", K, g)
+
+    def rate(w):  # d/dt of 1/2 sum w [Pi^2/sqrtg + sqrtg g.gu.g] Hd along the RHS
+        return np.sum(Hd * w * (Pi * Pid / sg + sg * np.sum(gd * Kg, axis=0)))
+
+    scale = np.sum(Hd * al * (np.abs(Pi * Pid) / sg + sg * np.abs(np.sum(gd * Kg, axis=0))))
+    assert abs(rate(al)) < 1e-12 * scale
+    assert abs(rate(np.ones(nn))) > 1e-6 * scale
+    # the oracle's weighted energy is that norm
+    Ea = 0.5 * np.sum(Hd * al * (Pi ** 2 / sg + sg * np.sum(g * Kg, axis=0)))
+    assert abs(m.energy(coef, Phi, Pi, use_metric=True, lapse=True) - Ea) < 1e-13 * Ea

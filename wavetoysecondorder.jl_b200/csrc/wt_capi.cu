@@ -1260,7 +1260,7 @@ int wt_rhs_curved4(wt_ctx* ctx, wt_ws* ws, const void* phi, const void* phidot, 
 
 // The energy's per-block partial sums into ctx->d_partial (asynchronous).
 static int energy_partials(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi,
-                           int use_metric) {
+                           int use_metric, int lapse = 0) {
   const wt::DevMesh& m = ws->mesh->m;
   WT_TRY(ensure(ws, &ws->grad, 3 * (size_t)m.nn * rsize(m.precision)));
   wt::DevCoef nocoef;
@@ -1272,8 +1272,8 @@ static int energy_partials(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const vo
   else
     WT_TRY(lrc(ctx, wt::launch_cons_k1(m, nocoef, Phi, nullptr, nullptr, nullptr, nullptr, ws->grad, use_metric, bc,
                                        rk, ctx->stream), "energy gradient"));
-  WT_TRY(lrc(ctx, wt::launch_energy(m, coef->c, Pi, ws->grad, use_metric, ctx->d_partial, ctx->nblocks, ctx->stream),
-             "energy"));
+  WT_TRY(lrc(ctx, wt::launch_energy(m, coef->c, Pi, ws->grad, use_metric, ctx->d_partial, ctx->nblocks, ctx->stream,
+                                     lapse), "energy"));
   ctx->launches += 2;
   return 0;
 }
@@ -1283,6 +1283,15 @@ int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, cons
   WT_TRY(check_ws(ctx, ws));
   if (!coef || !Phi || !Pi || !E) return fail(ctx, WT_EINVAL, "wt_energy: NULL argument");
   WT_TRY(energy_partials(ctx, ws, coef, Phi, Pi, use_metric));
+  return reduce_to_host(ctx, E);
+}
+
+int wt_energy_lapse(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, int use_metric,
+                    double* E) {
+  WT_TRY(check_ws(ctx, ws));
+  if (!coef || !Phi || !Pi || !E) return fail(ctx, WT_EINVAL, "wt_energy_lapse: NULL argument");
+  if (coef->mesh != ws->mesh) return fail(ctx, WT_EINVAL, "coefficients belong to another mesh");
+  WT_TRY(energy_partials(ctx, ws, coef, Phi, Pi, use_metric, 1));
   return reduce_to_host(ctx, E);
 }
 

@@ -315,7 +315,7 @@ int launch_curved4_background(const DevMesh& m, int kind, const double* p, doubl
 
 // reductions and vector updates (wt_reduce.cu)
 int launch_energy(const DevMesh& m, const DevCoef& c, const void* Pi, const void* grad, int use_metric,
-                  double* partial, int nblocks, cudaStream_t s);
+                  double* partial, int nblocks, cudaStream_t s, int lapse = 0);
 int launch_dot_weighted(const DevMesh& m, const void* a, const void* b, const void* c, const void* d,
                         int weight_kind, int mode, double* partial, int nblocks, cudaStream_t s);
 int launch_sumsq(long long n, int precision, const void* a, double* partial, int nblocks, cudaStream_t s);

@@ -25,17 +25,22 @@ __device__ inline double block_sum(double v, double* red) {
   return s;
 }
 
-// wave3d_energy: sum 1/2 [Pi^2/sqrtg + sqrtg gu^{ij} D_i D_j] H
+// wave3d_energy: sum 1/2 [Pi^2/sqrtg + sqrtg gu^{ij} D_i D_j] H; lapse = 1: the
+// integrand times alpha (the norm the system conserves for a static background
+// without shift)
 template <typename real>
 __global__ void k_energy(long long nn, const double* __restrict__ c11, const real* __restrict__ Pi,
-                         const real* __restrict__ g, const double* __restrict__ H, double* __restrict__ partial) {
+                         const real* __restrict__ g, const double* __restrict__ H, double* __restrict__ partial,
+                         int lapse) {
   __shared__ double red[32];
   double acc = 0.0;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nn; n += (long long)gridDim.x * blockDim.x) {
     const double sg = c11[nn + n];
     const double d1 = g[n], d2 = g[nn + n], d3 = g[2 * nn + n];
     const double p = Pi[n];
-    acc += (p * p / sg + sg * (c11[5 * nn + n] * d1 * d1 + c11[8 * nn + n] * d2 * d2 + c11[10 * nn + n] * d3 * d3 +
+    const double w = lapse ? c11[n] : 1.0;
+    acc += w *
+           (p * p / sg + sg * (c11[5 * nn + n] * d1 * d1 + c11[8 * nn + n] * d2 * d2 + c11[10 * nn + n] * d3 * d3 +
                                2 * c11[6 * nn + n] * d1 * d2 + 2 * c11[7 * nn + n] * d1 * d3 +
                                2 * c11[9 * nn + n] * d2 * d3)) *
            H[n] / 2;
@@ -179,12 +184,12 @@ static inline unsigned gblocks(long long n) {
 }
 
 int launch_energy(const DevMesh& m, const DevCoef& c, const void* Pi, const void* grad, int use_metric,
-                  double* partial, int nblocks, cudaStream_t s) {
+                  double* partial, int nblocks, cudaStream_t s, int lapse) {
   const double* H = use_metric ? m.Hd : m.Hphys;
   if (m.precision == 0)
-    k_energy<double><<<nblocks, RB, 0, s>>>(m.nn, c.c11, (const double*)Pi, (const double*)grad, H, partial);
+    k_energy<double><<<nblocks, RB, 0, s>>>(m.nn, c.c11, (const double*)Pi, (const double*)grad, H, partial, lapse);
   else
-    k_energy<float><<<nblocks, RB, 0, s>>>(m.nn, c.c11, (const float*)Pi, (const float*)grad, H, partial);
+    k_energy<float><<<nblocks, RB, 0, s>>>(m.nn, c.c11, (const float*)Pi, (const float*)grad, H, partial, lapse);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

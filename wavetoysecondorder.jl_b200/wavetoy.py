@@ -142,7 +142,8 @@ def library():
         "wt_gradient3d": [vp, vp, vp, vp, vp, vp], "wt_divergence3d": [vp, vp, vp, vp, vp, vp],
         "wt_rhs_sipg": [vp, vp, vp, vp, vp, C.POINTER(C.c_double * 6), d, d],
         "wt_rhs_strong": [vp, vp, vp, vp, vp, d, d], "wt_lap_strong_cons": [vp, vp, vp, vp, d, d],
-        "wt_energy": [vp, vp, vp, vp, vp, i, C.POINTER(d)], "wt_energy_sipg": [vp, vp, vp, vp, d, C.POINTER(d)],
+        "wt_energy": [vp, vp, vp, vp, vp, i, C.POINTER(d)],
+        "wt_energy_lapse": [vp, vp, vp, vp, vp, i, C.POINTER(d)], "wt_energy_sipg": [vp, vp, vp, vp, d, C.POINTER(d)],
         "wt_l2_diff": [vp, vp, vp, vp, i, C.POINTER(d)],
         "wt_step_rk4_curved": [vp, vp, vp, vp, vp, d, i, d, C.POINTER(_BcDesc), i],
         "wt_step_erk_curved": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i],
@@ -890,11 +891,13 @@ def apply_divergence3d(out, F1, F2, F3, ws: Workspace):
     return out
 
 
-def wave3d_energy(Phi, Pi, coef: Coef, ws: Workspace, metric: bool = False) -> float:
-    """wave3d_energy(Φ, Π, coef; geom, ops, ws, metric) (src/wave3d_curved.jl:268-287)."""
+def wave3d_energy(Phi, Pi, coef: Coef, ws: Workspace, metric: bool = False, lapse: bool = False) -> float:
+    """wave3d_energy(Φ, Π, coef; geom, ops, ws, metric) (src/wave3d_curved.jl:268-287); lapse=True:
+    the lapse-weighted energy (wt_energy_lapse), the norm conserved for a static background
+    without shift when α != 1."""
     E = C.c_double()
-    ws.ctx.check(library().wt_energy(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), int(metric), C.byref(E)),
-                 "wave3d_energy")
+    fn = library().wt_energy_lapse if lapse else library().wt_energy
+    ws.ctx.check(fn(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), int(metric), C.byref(E)), "wave3d_energy")
     return E.value
 
 
