@@ -139,3 +139,19 @@ def test_fused_path_taken(wt, ctx, O):
         counts.append((ctx.launch_count() - n0, [n for _, n in prof]))
     assert counts[0] == (5, [1, 1, 3])
     assert counts[1] == (8, [4, 4, 0])
+
+
+@pytest.mark.parametrize("M,periodic", [((1, 1, 1), False), ((1, 1, 1), True), ((1, 3, 2), False), ((2, 1, 3), True)])
+def test_fused_degenerate_meshes(wt, ctx, O, M, periodic):
+    """One element (every face outer, or its own neighbour on every face of a periodic cube) and
+    one-element-thick meshes: fused = two-kernel bit for bit, and the fused step against the oracle."""
+    import torch
+    g, o, p, Phi, Pi = _setup(wt, ctx, O, M, periodic=periodic, outer_tag=0 if periodic else 7, seed=13)
+    bc = None if periodic else wt.make_bc3d([2] * 6)
+    dt = 0.2 * o.min_spacing() / wt.workloads.max_speed(p)
+    Pf, Qf, _ = _run(wt, ctx, g, 2, p, Phi, Pi, dt, 5, bc, True)
+    Pu, Qu, _ = _run(wt, ctx, g, 2, p, Phi, Pi, dt, 5, bc, False)
+    assert torch.equal(Pf, Pu) and torch.equal(Qf, Qu)
+    Po, Qo = o.evolve_curved(o.background(2, p), Phi, Pi, dt, 5, bc=None if periodic else O.make_bc([2] * 6),
+                             use_metric=True)
+    assert rel(host(Pf), Po) < TOL64 and rel(host(Qf), Qo) < TOL64
