@@ -307,8 +307,15 @@ def run_ours(args):
     value, t_max, _ = aggregate(dist, t_ms / 1000.0, 2.0 * nn * args.steps, "cuda")
     finite = not ctx.nonfinite()
     ref = None
-    if study:  # the FP64 state after warmup + timed steps: the reference of the FP32 forms
-        ref = (torch.cat([Phi, Pi]), wt.wave3d_energy(Phi, Pi, coef, ws, metric=True))
+    if study:
+        # the reference of the FP32 forms: the FP64 state after the study's step count
+        # (config C3: 200 steps), continued from the timed steps on a copy of the state
+        Pr, Qr = Phi.clone(), Pi.clone()
+        extra = max(0, args.study_steps - args.warmup - args.steps)
+        if extra:
+            wt.step_rk4_curved(Pr, Qr, coef, ws, dt, extra, eps_KO=0.0, bc3d=bc, metric=True)
+        ref = (torch.cat([Pr, Qr]), wt.wave3d_energy(Pr, Qr, coef, ws, metric=True))
+        del Pr, Qr
     alt = None
     if prec == wt.WT_F64 and N == 8:
         # the other stage form of the FP64 n = 8 step (fused stage kernel <-> two-kernel
@@ -498,7 +505,7 @@ def precision_study(wt, ctx, args, seed, p, ic, dt64, ref, E64_0, value64, hbm):
     steps as the FP64 form): per form DOF-updates/s over the timed steps, the step
     roofline against w (34 + 4 C) bytes with w = 4, the speed-up over the FP64
     form, and the relative L2 / max error against the FP64 state and the energy
-    drift after warmup + timed steps."""
+    drift after --study-steps steps (the timed ones included)."""
     import torch
     M, N = args.elements, args.n
     mesh = wt.Mesh.warped_uniform_hex(ctx, N, M, 0.0, 1.0, 0.05, outer_tag=wt.SOMMERFELD_BDRY_TAG, precision=wt.WT_F32)
@@ -531,6 +538,9 @@ def precision_study(wt, ctx, args, seed, p, ic, dt64, ref, E64_0, value64, hbm):
         (k1_ms, k1_n), (k2_ms, k2_n), _ = ctx.profile_read()
         t_s = e0.elapsed_time(e1) / 1000.0
         v = 2.0 * nn * args.steps / t_s
+        extra = max(0, args.study_steps - args.warmup - args.steps)   # untimed, up to the study's step count
+        if extra:
+            wt.step_rk4_curved(Phi, Pi, coef, ws, dt, extra, bc3d=bc, metric=True)
         step_bytes = 4 * (34 + 4 * 20) * nn
         x = torch.cat([Phi, Pi]).double()
         d = x - refv
@@ -543,7 +553,7 @@ def precision_study(wt, ctx, args, seed, p, ic, dt64, ref, E64_0, value64, hbm):
             "kernels_ms_per_launch": {"k1": k1_ms / max(k1_n, 1), "k2": k2_ms / max(k2_n, 1)},
             "rel_l2_vs_f64": float(torch.linalg.norm(d) / torch.linalg.norm(refv)),
             "max_err_vs_f64": float(d.abs().max() / refv.abs().max()),
-            "energy_drift": E / E0 - 1.0, "steps_compared": args.warmup + args.steps,
+            "energy_drift": E / E0 - 1.0, "steps_compared": max(args.study_steps, args.warmup + args.steps),
             "finite": not ctx.nonfinite()}
     out["f64_energy_drift"] = E64 / E64_0 - 1.0
     ws.close(); coef.close(); mesh.close()
@@ -859,6 +869,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--unfused", action="store_true",
                     help="FP64 n = 8: step through the two-kernel stages instead of the fused stage kernel")
+    ap.add_argument("--study-steps", type=int, default=200,
+                    help="precision study: RK4 steps after which each FP32 form is compared with FP64 (config C3: 200)")
     ap.add_argument("--no-precision-study", action="store_true",
                     help="skip the FP32 forms run after the FP64 line (default workload, one GPU)")
     ap.add_argument("--workload", choices=["solve", "batch", "serve", "slab"], default="solve",
