@@ -197,3 +197,25 @@ def test_face_halo_over_gloo(world, Mz, periodic):
         assert p.exitcode == 0
     for rank, got, want in out:
         assert got == want, rank
+
+
+@pytest.mark.parametrize("Mz,n,periodic", [(6, 2, False), (7, 3, True), (4, 3, False), (5, 1, False), (9, 4, True)])
+def test_boundary_and_interior_layers_cover_owned(Mz, n, periodic):
+    """The first stage half of step_faces runs on boundary_layers() then interior_runs(): together
+    they cover every owned layer exactly once, the boundary ones are those next to a cut."""
+    S = load_package().slabs
+
+    for r in S.partition(Mz, n, periodic):
+        s = object.__new__(S.Slab)  # the two methods need only .rng (no device objects)
+        s.rng = r
+        b = s.boundary_layers()
+        runs = s.interior_runs()
+        covered = list(b) + [z for z0, k in runs for z in range(z0, z0 + k)]
+        assert sorted(covered) == list(range(r.first_owned, r.last_owned + 1))
+        want = set()
+        if r.lower is not None:
+            want.add(r.first_owned)
+        if r.upper is not None:
+            want.add(r.last_owned)
+        assert set(b) == want
+        assert all(k > 0 for _, k in runs)
