@@ -479,7 +479,7 @@ def run_ours(args):
         torch.cuda.empty_cache()
         line["precision_forms"] = precision_study(wt, ctx, args, seed, p, ic, dt, ref, E_0, value, hbm)
         comp = line["precision_forms"]["fp32_compensated"]
-        line["north_star"] = {
+        line["chosen_form"] = {
             "form": "fp32_compensated (the chosen split-precision form: FP32 storage, compensated Phi, "
                     "FP64 gradient of Phi)",
             "dof_updates_per_s": comp["value"], "speedup_vs_plain_f64": comp["speedup_vs_f64"],
