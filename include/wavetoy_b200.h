@@ -85,6 +85,17 @@ int wt_ctx_get_stream(wt_ctx* ctx, void** stream);
 int wt_ctx_set_stream(wt_ctx* ctx, void* stream);
 /* number of kernel launches this context has issued (evidence counter) */
 int wt_ctx_launch_count(const wt_ctx* ctx, long long* count);
+/* Device memory held by the objects of this context (meshes, coefficients,
+ * workspaces, batches, served requests): live bytes, live allocations, and
+ * the allocations made since the context was created (any may be NULL).
+ * Host only.  No counterpart in the reference (Julia's GC owns its arrays). */
+int wt_ctx_memory(const wt_ctx* ctx, long long* live_bytes, long long* live_allocs, long long* total_allocs);
+/* Host-side fault injection: the device allocation `after` allocations from
+ * now (0: the next one) fails once with WT_ENOMEM, as if cudaMalloc had
+ * failed, without calling it; after < 0 cancels a pending injection.  The
+ * failing call releases what it had allocated, and the context stays usable.
+ * No device fault is involved.  No counterpart in the reference. */
+int wt_ctx_inject_alloc_failure(wt_ctx* ctx, long long after);
 /* Read and clear the device non-finite flag that fused RK4 steps set when the
  * state stops being finite (the reference asserts all(isfinite, ...) per
  * sample, src/evolve.jl:1344); synchronous. */
@@ -270,6 +281,18 @@ int wt_initial_state(wt_ctx* ctx, wt_ws* ws, int kind, const double* params, int
  * the Float64 state itself.  Replaces the host-side Float64 -> T conversion
  * before the reference's evolve loop (src/evolve.jl:1270); asynchronous. */
 int wt_state_set_f64(wt_ctx* ctx, wt_ws* ws, const double* Phi64, const double* Pi64, void* Phi, void* Pi);
+/* Host checkpoints of a stepped state, word for word: Phi and Pi in the mesh
+ * precision and, for an FP32 mesh, the low parts the workspace keeps for that
+ * pair (zeros if it keeps none).  Loading a checkpoint into the state arrays of
+ * a workspace on a mesh of the same N, Ne and precision, then stepping, gives
+ * the values that stepping the saved solve gives, bit for bit.  bytes must equal
+ * wt_state_checkpoint_size.  The serving engine's preemption keeps a
+ * preempted request's state this way.  No counterpart in the reference, whose
+ * evolve3d returns its final state only (src/evolve.jl:1361-1365).
+ * Synchronous. */
+int wt_state_checkpoint_size(const wt_ws* ws, long long* bytes);
+int wt_state_checkpoint_save(wt_ctx* ctx, wt_ws* ws, const void* Phi, const void* Pi, void* host, long long bytes);
+int wt_state_checkpoint_load(wt_ctx* ctx, wt_ws* ws, void* Phi, void* Pi, const void* host, long long bytes);
 
 /* ---- workspace ---------------------------------------------------------------*/
 /* Replaces make_wave3d_workspace (src/wave3d_curved.jl:158-178): device
@@ -607,6 +630,24 @@ int wt_serve_poll(wt_server* server, int* finished);
 int wt_serve_run(wt_server* server);
 /* WT_EINVAL until request rid has finished */
 int wt_serve_get_result(const wt_server* server, int rid, wt_serve_result* out);
+/* A request's state: WAITING (submitted, not running; PREEMPTED if it ran and
+ * waits with a host checkpoint), RUNNING, FINISHED or CANCELLED, with the steps
+ * it has left and how often it was preempted (any pointer may be NULL). */
+enum { WT_REQ_WAITING = 0, WT_REQ_RUNNING = 1, WT_REQ_FINISHED = 2, WT_REQ_CANCELLED = 3, WT_REQ_PREEMPTED = 4 };
+int wt_serve_status(const wt_server* server, int rid, int* status, int* steps_left, int* preemptions);
+/* Cancel a request that has not finished: a waiting one leaves the queue, a
+ * running one leaves the batch and its device memory (and its share of the
+ * budget) is released at once.  WT_EINVAL if it finished or was cancelled. */
+int wt_serve_cancel(wt_server* server, int rid);
+/* Preempt a running request: its state is saved to a host checkpoint
+ * (wt_state_checkpoint_save), it leaves the batch, its device memory and budget
+ * share are released, and it waits again with the steps it has left, in the
+ * admission order of those.  When admitted again it is rebuilt and resumes from
+ * the checkpoint; with a static background its final state equals the one of
+ * an uninterrupted run, bit for bit (a time-dependent background resumes at the
+ * time the host recorded, which may differ from the device's in the last bit).
+ * WT_EINVAL unless the request is running. */
+int wt_serve_preempt(wt_server* server, int rid);
 /* copy a finished request's kept final state into device buffers of its
  * precision (nodes values each), on the context stream */
 int wt_serve_result_state(wt_server* server, int rid, void* Phi, void* Pi);

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -31,6 +32,11 @@ struct wt_ctx {
   std::vector<cudaEvent_t> prof_ev[3];  // [kernel: K1, K2, fused stage] start/stop pairs
   cudaEvent_t ord_a = nullptr, ord_b = nullptr;  // order the graph stream with the caller's stream
   double* noalloc_scratch = nullptr;  // device address of the wt_rhs_curved_noalloc array (first call)
+  // device memory of the objects the context owns (meshes, coefficients,
+  // workspaces, batches, served requests): live allocations by address
+  std::unordered_map<void*, size_t> live;
+  long long live_bytes = 0, total_allocs = 0;
+  long long fail_after = -1;  // host-side fault injection: allocations left before one fails (< 0: none)
 };
 
 static void prof_mark(wt_ctx* ctx, int which) {
@@ -116,14 +122,31 @@ size_t rsize(int precision) { return precision == 0 ? sizeof(double) : sizeof(fl
 template <typename T>
 int dalloc(wt_ctx* ctx, T** p, size_t bytes, std::vector<void*>* owner) {
   if (bytes == 0) bytes = 16;
+  if (ctx->fail_after >= 0 && ctx->fail_after-- == 0)  // wt_ctx_inject_alloc_failure: fail as cudaMalloc would
+    return fail(ctx, WT_ENOMEM, std::string("device allocation of ") + std::to_string(bytes) +
+                                    " bytes failed: injected failure");
   cudaError_t e = cudaMalloc((void**)p, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return fail(ctx, WT_ENOMEM, std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
                                     cudaGetErrorString(e));
   }
+  ctx->live[(void*)*p] = bytes;
+  ctx->live_bytes += (long long)bytes;
+  ctx->total_allocs += 1;
   if (owner) owner->push_back((void*)*p);
   return 0;
+}
+
+// free an allocation of dalloc (NULL: nothing)
+void dfree(wt_ctx* ctx, void* p) {
+  if (!p) return;
+  auto it = ctx->live.find(p);
+  if (it != ctx->live.end()) {
+    ctx->live_bytes -= (long long)it->second;
+    ctx->live.erase(it);
+  }
+  cudaFree(p);
 }
 
 #define WT_TRY(x)            \
@@ -288,7 +311,7 @@ int derive_geometry(wt_mesh* mh) {
 }
 
 void free_mesh(wt_mesh* mh) {
-  for (void* p : mh->owned) cudaFree(p);
+  for (void* p : mh->owned) dfree(mh->ctx, p);
   mh->owned.clear();
 }
 
@@ -444,6 +467,9 @@ int rhs_curved_impl(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi
 namespace wt {
 // error reporting on a context for the other host translation units (the server)
 int ctx_fail(wt_ctx* ctx, int code, const std::string& msg) { return fail(ctx, code, msg); }
+// tracked device allocations for the other host translation units (the server's state buffers)
+int ctx_alloc(wt_ctx* ctx, void** p, size_t bytes) { return dalloc(ctx, p, bytes, nullptr); }
+void ctx_free(wt_ctx* ctx, void* p) { dfree(ctx, p); }
 }  // namespace wt
 
 extern "C" {
@@ -465,6 +491,9 @@ int wt_ctx_create(int device, wt_ctx** out) {
   c->nblocks = wt::reduce_blocks();
   if (cudaMalloc(&c->d_flag, sizeof(unsigned int)) != cudaSuccess ||
       cudaMalloc(&c->d_partial, c->nblocks * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(c->d_flag);
+    cudaStreamDestroy(c->own_stream);
     delete c;
     return WT_ENOMEM;
   }
@@ -512,6 +541,20 @@ int wt_ctx_set_stream(wt_ctx* ctx, void* stream) {
 int wt_ctx_launch_count(const wt_ctx* ctx, long long* count) {
   if (!ctx || !count) return WT_EINVAL;
   *count = ctx->launches;
+  return 0;
+}
+
+int wt_ctx_memory(const wt_ctx* ctx, long long* live_bytes, long long* live_allocs, long long* total_allocs) {
+  if (!ctx) return WT_EINVAL;
+  if (live_bytes) *live_bytes = ctx->live_bytes;
+  if (live_allocs) *live_allocs = (long long)ctx->live.size();
+  if (total_allocs) *total_allocs = ctx->total_allocs;
+  return 0;
+}
+
+int wt_ctx_inject_alloc_failure(wt_ctx* ctx, long long after) {
+  if (!ctx) return WT_EINVAL;
+  ctx->fail_after = after < 0 ? -1 : after;
   return 0;
 }
 
@@ -638,6 +681,7 @@ static int check_mesh_desc(wt_ctx* ctx, const wt_mesh_desc* d) {
 }
 
 int wt_mesh_create(wt_ctx* ctx, const wt_mesh_desc* d, wt_mesh** out) {
+  wt::NvtxRange nvtx_("wt_mesh_create");
   if (!ctx) return WT_EINVAL;
   if (!d || !out) return fail(ctx, WT_EINVAL, "wt_mesh_create: NULL argument");
   *out = nullptr;
@@ -886,7 +930,7 @@ int wt_mesh_release_setup_geometry(wt_mesh* mh) {
     if (!p) continue;
     auto it = std::find(mh->owned.begin(), mh->owned.end(), p);
     if (it != mh->owned.end()) mh->owned.erase(it);
-    cudaFree(p);
+    dfree(mh->ctx, p);
   }
   m.coords = m.jac = m.invjac = m.detjac = nullptr;
   if (m.precision != WT_F64) m.Ja = m.invdetJ = nullptr;
@@ -908,7 +952,7 @@ static int coef_alloc(wt_ctx* ctx, wt_mesh* mesh, wt_coef** out) {
   c->c.precision = mesh->m.precision;
   if (dalloc(ctx, &c->c.c11, 11 * c->c.nn * sizeof(double), nullptr) ||
       dalloc(ctx, &c->c.c10, 10 * c->c.nn * rsize(c->c.precision), nullptr)) {
-    cudaFree(c->c.c11);
+    dfree(ctx, c->c.c11);
     delete c;
     return WT_ENOMEM;
   }
@@ -917,6 +961,7 @@ static int coef_alloc(wt_ctx* ctx, wt_mesh* mesh, wt_coef** out) {
 }
 
 int wt_background_set(wt_ctx* ctx, wt_mesh* mesh, const wt_background_desc* desc, wt_coef** out) {
+  wt::NvtxRange nvtx_("wt_background_set");
   if (!ctx) return WT_EINVAL;
   if (!mesh || !desc || !out) return fail(ctx, WT_EINVAL, "wt_background_set: NULL argument");
   if (desc->kind < 0 || desc->kind > 5) return fail(ctx, WT_EINVAL, "unknown background kind");
@@ -976,9 +1021,9 @@ int wt_coef_get(const wt_coef* c, double* coef11) {
 int wt_coef_destroy(wt_coef* c) {
   if (!c) return WT_EINVAL;
   cudaStreamSynchronize(c->ctx->stream);
-  cudaFree(c->c.c11);
-  cudaFree(c->c.c10);
-  if (c->d_t) cudaFree(c->d_t);
+  dfree(c->ctx, c->c.c11);
+  dfree(c->ctx, c->c.c10);
+  dfree(c->ctx, c->d_t);
   delete c;
   return 0;
 }
@@ -1010,6 +1055,7 @@ int wt_coef_get_time(const wt_coef* c, double* t) {
 // ---- initial data ---------------------------------------------------------------
 int wt_initial_data(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, int nparams, double t, void* u,
                     void* ut) {
+  wt::NvtxRange nvtx_("wt_initial_data");
   if (!ctx) return WT_EINVAL;
   if (!mesh || !u || (nparams > 0 && !params)) return fail(ctx, WT_EINVAL, "wt_initial_data: NULL argument");
   if (kind < 0 || kind > 4) return fail(ctx, WT_EINVAL, "wt_initial_data: unknown kind");
@@ -1023,13 +1069,14 @@ int wt_initial_data(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* params, 
   int rc = lrc(ctx, wt::launch_initial(mesh->m, kind, dp, nparams, t, u, ut, ctx->stream), "initial data");
   ctx->launches += 1;
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
-  cudaFree(dp);
+  dfree(ctx, dp);
   if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "initial data");
   return rc;
 }
 
 int wt_initial_state(wt_ctx* ctx, wt_ws* ws, int kind, const double* params, int nparams, double t, void* Phi,
                      void* Pi) {
+  wt::NvtxRange nvtx_("wt_initial_state");
   WT_TRY(check_ws(ctx, ws));
   if (!Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_initial_state: NULL argument");
   wt_mesh* mesh = ws->mesh;
@@ -1045,7 +1092,7 @@ int wt_initial_state(wt_ctx* ctx, wt_ws* ws, int kind, const double* params, int
   double *dp = nullptr, *tmp = nullptr;
   WT_TRY(dalloc(ctx, &dp, (nparams > 0 ? nparams : 1) * sizeof(double), nullptr));
   if (dalloc(ctx, &tmp, 2 * (size_t)nn * sizeof(double), nullptr)) {
-    cudaFree(dp);
+    dfree(ctx, dp);
     return WT_ENOMEM;
   }
   if (nparams > 0) cudaMemcpyAsync(dp, params, nparams * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
@@ -1055,8 +1102,8 @@ int wt_initial_state(wt_ctx* ctx, wt_ws* ws, int kind, const double* params, int
   if (!rc) rc = lrc(ctx, wt::launch_split_f64(nn, tmp + nn, (float*)Pi, (float*)ws->compQ, ctx->stream), "state split");
   ctx->launches += 3;
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
-  cudaFree(dp);
-  cudaFree(tmp);
+  dfree(ctx, dp);
+  dfree(ctx, tmp);
   if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "initial state");
   if (!rc) {
     ws->comp_for[0] = Phi;
@@ -1083,8 +1130,7 @@ int wt_workspace_destroy(wt_ws* ws) {
   void* bufs[] = {ws->F, ws->F2, ws->bbuf, ws->grad, ws->kP, ws->kQ, ws->S0, ws->S1, ws->SQ, ws->accP, ws->accQ,
                   ws->trace, ws->zero, ws->Lu, ws->compP, ws->compQ, ws->erk, ws->evo[0], ws->evo[1],
                   ws->evo[2], ws->evo[3], ws->evoE};
-  for (void* p : bufs)
-    if (p) cudaFree(p);
+  for (void* p : bufs) dfree(ws->ctx, p);
   delete ws;
   return 0;
 }
@@ -1130,9 +1176,72 @@ int wt_state_set_f64(wt_ctx* ctx, wt_ws* ws, const double* Phi64, const double* 
   return 0;
 }
 
+// ---- host checkpoints of a stepped state ----------------------------------------------
+// Layout: Phi, Pi in the mesh precision, then (FP32 meshes) the low parts compP,
+// compQ as float -- zeros when the workspace holds none for this state pair.
+int wt_state_checkpoint_size(const wt_ws* ws, long long* bytes) {
+  if (!ws || !bytes) return WT_EINVAL;
+  const wt::DevMesh& m = ws->mesh->m;
+  *bytes = (long long)m.nn * (long long)(m.precision == WT_F64 ? 2 * sizeof(double) : 4 * sizeof(float));
+  return 0;
+}
+
+int wt_state_checkpoint_save(wt_ctx* ctx, wt_ws* ws, const void* Phi, const void* Pi, void* host, long long bytes) {
+  wt::NvtxRange nvtx_("wt_state_checkpoint_save");
+  WT_TRY(check_ws(ctx, ws));
+  if (!Phi || !Pi || !host) return fail(ctx, WT_EINVAL, "wt_state_checkpoint_save: NULL argument");
+  long long need = 0;
+  wt_state_checkpoint_size(ws, &need);
+  if (bytes != need)
+    return fail(ctx, WT_EINVAL, "wt_state_checkpoint_save: the buffer must hold " + std::to_string(need) + " bytes");
+  const wt::DevMesh& m = ws->mesh->m;
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  char* h = (char*)host;
+  cudaMemcpyAsync(h, Phi, nb, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(h + nb, Pi, nb, cudaMemcpyDeviceToHost, ctx->stream);
+  if (m.precision != WT_F64) {
+    const size_t cb = (size_t)m.nn * sizeof(float);
+    const bool held = ws->compP && ws->comp_for[0] == Phi && ws->comp_for[1] == Pi;
+    if (held) {
+      cudaMemcpyAsync(h + 2 * nb, ws->compP, cb, cudaMemcpyDeviceToHost, ctx->stream);
+      cudaMemcpyAsync(h + 2 * nb + cb, ws->compQ, cb, cudaMemcpyDeviceToHost, ctx->stream);
+    } else {
+      std::memset(h + 2 * nb, 0, 2 * cb);  // stepping this pair would start from zero low parts
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "wt_state_checkpoint_save");
+}
+
+int wt_state_checkpoint_load(wt_ctx* ctx, wt_ws* ws, void* Phi, void* Pi, const void* host, long long bytes) {
+  wt::NvtxRange nvtx_("wt_state_checkpoint_load");
+  WT_TRY(check_ws(ctx, ws));
+  if (!Phi || !Pi || !host) return fail(ctx, WT_EINVAL, "wt_state_checkpoint_load: NULL argument");
+  long long need = 0;
+  wt_state_checkpoint_size(ws, &need);
+  if (bytes != need)
+    return fail(ctx, WT_EINVAL, "wt_state_checkpoint_load: the buffer must hold " + std::to_string(need) + " bytes");
+  const wt::DevMesh& m = ws->mesh->m;
+  const size_t nb = (size_t)m.nn * rsize(m.precision);
+  const char* h = (const char*)host;
+  if (m.precision != WT_F64) WT_TRY(ws_step_buffers(ws));  // the low parts' home
+  cudaMemcpyAsync(Phi, h, nb, cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(Pi, h + nb, nb, cudaMemcpyHostToDevice, ctx->stream);
+  if (m.precision != WT_F64) {
+    const size_t cb = (size_t)m.nn * sizeof(float);
+    cudaMemcpyAsync(ws->compP, h + 2 * nb, cb, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(ws->compQ, h + 2 * nb + cb, cb, cudaMemcpyHostToDevice, ctx->stream);
+    ws->comp_for[0] = Phi;  // the low parts belong to this state pair: stepping it keeps them
+    ws->comp_for[1] = Pi;
+  }
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "wt_state_checkpoint_load");
+}
+
 // ---- RHS ----------------------------------------------------------------------------
 int wt_rhs_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, void* Phidot,
                   void* Pidot, double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  wt::NvtxRange nvtx_("wt_rhs_curved");
   WT_TRY(check_ws(ctx, ws));
   if (!coef || !Phi || !Pi || !Phidot || !Pidot) return fail(ctx, WT_EINVAL, "wt_rhs_curved: NULL argument");
   if (coef->mesh != ws->mesh) return fail(ctx, WT_EINVAL, "coefficients belong to another mesh");
@@ -1143,6 +1252,7 @@ int wt_rhs_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, 
 }
 
 int wt_apply_D(wt_ctx* ctx, wt_ws* ws, const void* u, void* Du, int d) {
+  wt::NvtxRange nvtx_("wt_apply_D");
   WT_TRY(check_ws(ctx, ws));
   if (!u || !Du) return fail(ctx, WT_EINVAL, "wt_apply_D: NULL argument");
   if (d < 1 || d > 3) return fail(ctx, WT_EINVAL, "wt_apply_D: d must be 1, 2 or 3");
@@ -1192,6 +1302,7 @@ int wt_divergence3d(wt_ctx* ctx, wt_ws* ws, const void* F1, const void* F2, cons
 
 int wt_rhs_sipg(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, void* utt, const double bdry_values[6],
                 double tau, double sommerfeld_R) {
+  wt::NvtxRange nvtx_("wt_rhs_sipg");
   WT_TRY(check_ws(ctx, ws));
   if (!u || !ut || !utt || !bdry_values) return fail(ctx, WT_EINVAL, "wt_rhs_sipg: NULL argument");
   const wt::DevMesh& m = ws->mesh->m;
@@ -1204,6 +1315,7 @@ int wt_rhs_sipg(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, void* utt
 
 int wt_rhs_strong(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, void* utt, double tau,
                   double sommerfeld_R) {
+  wt::NvtxRange nvtx_("wt_rhs_strong");
   WT_TRY(check_ws(ctx, ws));
   if (!u || !ut || !utt) return fail(ctx, WT_EINVAL, "wt_rhs_strong: NULL argument");
   WT_TRY(need_setup_geometry(ws->mesh, "wt_rhs_strong"));
@@ -1249,6 +1361,7 @@ int wt_curved4_background(wt_ctx* ctx, wt_mesh* mesh, int kind, const double* pa
 
 int wt_rhs_curved4(wt_ctx* ctx, wt_ws* ws, const void* phi, const void* phidot, void* phiddot, const void* ginv,
                    const void* gamma, double h, int conservative, double tau) {
+  wt::NvtxRange nvtx_("wt_rhs_curved4");
   WT_TRY(check_ws(ctx, ws));
   if (!phi || !phidot || !phiddot || !ginv || !gamma) return fail(ctx, WT_EINVAL, "wt_rhs_curved4: NULL argument");
   if (!(h > 0)) return fail(ctx, WT_EINVAL, "wt_rhs_curved4: h must be positive");
@@ -1280,6 +1393,7 @@ static int energy_partials(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const vo
 
 int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, int use_metric,
               double* E) {
+  wt::NvtxRange nvtx_("wt_energy");
   WT_TRY(check_ws(ctx, ws));
   if (!coef || !Phi || !Pi || !E) return fail(ctx, WT_EINVAL, "wt_energy: NULL argument");
   WT_TRY(energy_partials(ctx, ws, coef, Phi, Pi, use_metric));
@@ -1288,6 +1402,7 @@ int wt_energy(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, cons
 
 int wt_energy_lapse(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi, const void* Pi, int use_metric,
                     double* E) {
+  wt::NvtxRange nvtx_("wt_energy_lapse");
   WT_TRY(check_ws(ctx, ws));
   if (!coef || !Phi || !Pi || !E) return fail(ctx, WT_EINVAL, "wt_energy_lapse: NULL argument");
   if (coef->mesh != ws->mesh) return fail(ctx, WT_EINVAL, "coefficients belong to another mesh");
@@ -1296,6 +1411,7 @@ int wt_energy_lapse(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, const void* Phi
 }
 
 int wt_energy_sipg(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, double tau, double* E) {
+  wt::NvtxRange nvtx_("wt_energy_sipg");
   WT_TRY(check_ws(ctx, ws));
   if (!u || !ut || !E) return fail(ctx, WT_EINVAL, "wt_energy_sipg: NULL argument");
   const wt::DevMesh& m = ws->mesh->m;
@@ -1320,6 +1436,7 @@ int wt_energy_sipg(wt_ctx* ctx, wt_ws* ws, const void* u, const void* ut, double
 }
 
 int wt_l2_diff(wt_ctx* ctx, wt_ws* ws, const void* a, const void* b, int use_metric, double* out) {
+  wt::NvtxRange nvtx_("wt_l2_diff");
   WT_TRY(check_ws(ctx, ws));
   if (!a || !out) return fail(ctx, WT_EINVAL, "wt_l2_diff: NULL argument");
   double s = 0;
@@ -1388,6 +1505,9 @@ static int rk4_stage_part(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi
   ws->halo_cp = cp ? 1 : 0;
   ws->flux_block = n8 ? wt::n8_flux_block(m) : (long long)m.N * m.N * m.N;
   ws->flux_lay = n8 ? wt::n8_flux_layout(m) : 0;
+  static const char* kNames[2][4] = {{"rk4 stage 0 K1", "rk4 stage 1 K1", "rk4 stage 2 K1", "rk4 stage 3 K1"},
+                                     {"rk4 stage 0 K2", "rk4 stage 1 K2", "rk4 stage 2 K2", "rk4 stage 3 K2"}};
+  wt::NvtxRange nv(kNames[part - 1][st]);
   if (part == 1) {
     prof_mark(ctx, 0);
     WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, inP, inQ, ws->F, nullptr, ws->bbuf, nullptr, use_metric, b, rkP,
@@ -1444,22 +1564,31 @@ static int step_curved_fused(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* 
   ws->flux_block = wt::n8_flux_block(m);
   ws->flux_lay = wt::n8_flux_layout(m);
   if (coef->td) WT_TRY(coef_resample(ctx, coef, toff[0], s));
-  prof_mark(ctx, 0);
-  WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, Phi, Pi, FB[0], nullptr, ws->bbuf, nullptr, use_metric, b, rkP(0), s,
-                                     true), "rk4 K1"));
-  prof_mark(ctx, 0);
+  {
+    wt::NvtxRange nv("rk4 stage 0 K1");
+    prof_mark(ctx, 0);
+    WT_TRY(lrc(ctx, wt::launch_cons_k1(m, coef->c, Phi, Pi, FB[0], nullptr, ws->bbuf, nullptr, use_metric, b, rkP(0),
+                                       s, true), "rk4 K1"));
+    prof_mark(ctx, 0);
+  }
   ctx->launches += 1;
+  static const char* kNames[3] = {"rk4 fused stage 0-1", "rk4 fused stage 1-2", "rk4 fused stage 2-3"};
   for (int st = 0; st < 3; ++st) {
     if (coef->td) WT_TRY(coef_resample(ctx, coef, toff[st + 1], s));
+    wt::NvtxRange nv(kNames[st]);
     prof_mark(ctx, 2);
     WT_TRY(lrc(ctx, wt::launch_cons_fk_n8(m, coef->c, FB[st % 2], FB[(st + 1) % 2], SP[st % 2], ws->bbuf, b, rkQ(st),
                                           rkP(st + 1), s), "rk4 fused stage"));
     prof_mark(ctx, 2);
     ctx->launches += 1;
   }
-  prof_mark(ctx, 1);
-  WT_TRY(lrc(ctx, wt::launch_cons_k2(m, FB[1], nullptr, ws->bbuf, use_metric, b, rkQ(3), nullptr, s, true), "rk4 K2"));
-  prof_mark(ctx, 1);
+  {
+    wt::NvtxRange nv("rk4 stage 3 K2");
+    prof_mark(ctx, 1);
+    WT_TRY(lrc(ctx, wt::launch_cons_k2(m, FB[1], nullptr, ws->bbuf, use_metric, b, rkQ(3), nullptr, s, true),
+               "rk4 K2"));
+    prof_mark(ctx, 1);
+  }
   ctx->launches += 1;
   if (coef->td) {
     WT_TRY(lrc(ctx, wt::launch_advance_time(coef->d_t, dt, s), "background time"));
@@ -1594,10 +1723,15 @@ static int replay_graph(wt_ctx* ctx, int nsteps, F&& one_step) {
   cudaGraphExec_t exec = nullptr;
   const long long before = ctx->launches;
   ctx->stream = own;
-  cudaError_t e = cudaStreamBeginCapture(own, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) { ctx->stream = user; return cuda_fail(ctx, e, "graph capture"); }
-  int rc = one_step();
-  e = cudaStreamEndCapture(own, &graph);
+  int rc = 0;
+  cudaError_t e;
+  {
+    wt::NvtxRange nv("graph capture");
+    e = cudaStreamBeginCapture(own, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) { ctx->stream = user; return cuda_fail(ctx, e, "graph capture"); }
+    rc = one_step();
+    e = cudaStreamEndCapture(own, &graph);
+  }
   ctx->stream = user;
   if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
   if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
@@ -1605,7 +1739,10 @@ static int replay_graph(wt_ctx* ctx, int nsteps, F&& one_step) {
   if (e != cudaSuccess) { cudaGraphDestroy(graph); return cuda_fail(ctx, e, "graph instantiate"); }
   const long long per = ctx->launches - before;
   ctx->launches = before;
-  for (int i = 0; i < nsteps && e == cudaSuccess; ++i) e = cudaGraphLaunch(exec, own);
+  {
+    wt::NvtxRange nv("graph replay");
+    for (int i = 0; i < nsteps && e == cudaSuccess; ++i) e = cudaGraphLaunch(exec, own);
+  }
   ctx->launches += per * nsteps;
   cudaEventRecord(ctx->ord_b, own);
   cudaStreamWaitEvent(user, ctx->ord_b, 0);
@@ -1618,6 +1755,7 @@ extern "C" {
 
 int wt_step_rk4_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
                        double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  wt::NvtxRange nvtx_("wt_step_rk4_curved");
   WT_TRY(check_ws(ctx, ws));
   if (!coef || !Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_step_rk4_curved: NULL argument");
   if (nsteps < 0) return fail(ctx, WT_EINVAL, "nsteps must be >= 0");
@@ -1675,12 +1813,14 @@ extern "C" {
 
 int wt_rk4_stage_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int stage,
                         int part, const wt_bc_desc* bc, int use_metric) {
+  wt::NvtxRange nvtx_("wt_rk4_stage_curved");
   WT_TRY(check_ws(ctx, ws));
   return stage_curved_range(ctx, ws, coef, Phi, Pi, dt, stage, part, 0, -1, bc, use_metric);
 }
 
 int wt_rk4_stage_curved_layers(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
                                int stage, int part, int layer0, int nlayers, const wt_bc_desc* bc, int use_metric) {
+  wt::NvtxRange nvtx_("wt_rk4_stage_curved_layers");
   WT_TRY(check_ws(ctx, ws));
   const wt::DevMesh& m = ws->mesh->m;
   if (m.M[2] <= 0 || (long long)m.M[0] * m.M[1] * m.M[2] != m.Ne)
@@ -1694,6 +1834,7 @@ int wt_rk4_stage_curved_layers(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void
 
 int wt_rk4_stage_curved_ko(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int stage,
                            double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  wt::NvtxRange nvtx_("wt_rk4_stage_curved_ko");
   WT_TRY(check_ws(ctx, ws));
   if (!coef || !Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved_ko: NULL argument");
   if (stage < 0 || stage > 3) return fail(ctx, WT_EINVAL, "wt_rk4_stage_curved_ko: stage must be 0..3");
@@ -1732,6 +1873,7 @@ int wt_rk4_stage_curved_ko(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Ph
 
 int wt_halo_state_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, void* Pi, int stage, int layer, int count, void* buf,
                        int pack) {
+  wt::NvtxRange nvtx_("wt_halo_state_copy");
   WT_TRY(check_ws(ctx, ws));
   if (!Phi || !Pi || !buf) return fail(ctx, WT_EINVAL, "wt_halo_state_copy: NULL argument");
   const wt::DevMesh& m = ws->mesh->m;
@@ -1763,6 +1905,7 @@ int wt_halo_size(const wt_ws* ws, long long* values) {
 }
 
 int wt_halo_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, void* buf, int pack) {
+  wt::NvtxRange nvtx_("wt_halo_copy");
   WT_TRY(check_ws(ctx, ws));
   if (!Phi || !buf) return fail(ctx, WT_EINVAL, "wt_halo_copy: NULL argument");
   const wt::DevMesh& m = ws->mesh->m;
@@ -1808,6 +1951,7 @@ int wt_halo_face_size(const wt_ws* ws, long long* values) {
 }
 
 int wt_halo_face_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, int face, void* buf, int pack) {
+  wt::NvtxRange nvtx_("wt_halo_face_copy");
   WT_TRY(check_ws(ctx, ws));
   if (!Phi || !buf) return fail(ctx, WT_EINVAL, "wt_halo_face_copy: NULL argument");
   const wt::DevMesh& m = ws->mesh->m;
@@ -1826,6 +1970,7 @@ int wt_halo_face_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, i
 
 int wt_step_erk_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
                        int method, double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  wt::NvtxRange nvtx_("wt_step_erk_curved");
   WT_TRY(check_ws(ctx, ws));
   const ErkTableau* T = erk_tableau(method);
   if (!T) return fail(ctx, WT_EINVAL, "wt_step_erk_curved: unknown method " + std::to_string(method));
@@ -1890,6 +2035,7 @@ static int step_sipg_once(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, 
 
 int wt_step_rk4_sipg(wt_ctx* ctx, wt_ws* ws, void* u, void* ut, double dt, int nsteps, const double bdry_values[6],
                      double tau, double sommerfeld_R, double eps_ko) {
+  wt::NvtxRange nvtx_("wt_step_rk4_sipg");
   WT_TRY(check_ws(ctx, ws));
   if (!u || !ut || !bdry_values) return fail(ctx, WT_EINVAL, "wt_step_rk4_sipg: NULL argument");
   if (nsteps < 0 || !(dt > 0)) return fail(ctx, WT_EINVAL, "bad nsteps/dt");
@@ -1920,14 +2066,14 @@ int wt_gather_nodes(wt_ctx* ctx, wt_mesh* mesh, const void* field, const int64_t
   int64_t* dn = nullptr;
   double* dv = nullptr;
   WT_TRY(dalloc(ctx, &dn, count * sizeof(int64_t), nullptr));
-  if (dalloc(ctx, &dv, count * sizeof(double), nullptr)) { cudaFree(dn); return WT_ENOMEM; }
+  if (dalloc(ctx, &dv, count * sizeof(double), nullptr)) { dfree(ctx, dn); return WT_ENOMEM; }
   cudaMemcpyAsync(dn, nodes, count * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream);
   int rc = lrc(ctx, wt::launch_gather(mesh->m.precision, count, field, dn, dv, ctx->stream), "gather");
   ctx->launches += 1;
   if (!rc) cudaMemcpyAsync(host_out, dv, count * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
-  cudaFree(dn);
-  cudaFree(dv);
+  dfree(ctx, dn);
+  dfree(ctx, dv);
   if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "gather");
   return rc;
 }
@@ -2026,7 +2172,7 @@ static int evolve_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi_ho
   for (void*& p : ws->evo) WT_TRY(ensure(ws, &p, nb));
   const size_t elen = energy ? (size_t)nsamples * ctx->nblocks : 0;
   if (elen > ws->evoE_len) {
-    cudaFree(ws->evoE);
+    dfree(ctx, ws->evoE);
     ws->evoE = nullptr;
     ws->evoE_len = 0;
     WT_TRY(dalloc(ctx, &ws->evoE, elen * sizeof(double), nullptr));
@@ -2109,6 +2255,7 @@ extern "C" {
 int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* Phi_host, double* Pi_host, double dt,
                           int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc, int use_metric,
                           double* energy) {
+  wt::NvtxRange nvtx_("wt_evolve_curved_host");
   return evolve_host(ctx, ws, coef, Phi_host, Pi_host, WT_F64, "wt_evolve_curved_host", dt, steps_per_sample,
                      nsamples, eps_ko, bc, use_metric, energy);
 }
@@ -2116,6 +2263,7 @@ int wt_evolve_curved_host(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, double* P
 int wt_evolve_curved_host_f32(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, float* Phi_host, float* Pi_host, double dt,
                               int steps_per_sample, int nsamples, double eps_ko, const wt_bc_desc* bc, int use_metric,
                               double* energy) {
+  wt::NvtxRange nvtx_("wt_evolve_curved_host_f32");
   return evolve_host(ctx, ws, coef, Phi_host, Pi_host, WT_F32, "wt_evolve_curved_host_f32", dt, steps_per_sample,
                      nsamples, eps_ko, bc, use_metric, energy);
 }
@@ -2183,9 +2331,9 @@ void batch_release(wt_batch* b) {
   b->gjoin.clear();
   b->fork = nullptr;
   for (auto& g : b->groups) {
-    cudaFree(g.d_tiles);
-    cudaFree(g.d_k1);
-    cudaFree(g.d_k2);
+    dfree(b->ctx, g.d_tiles);
+    dfree(b->ctx, g.d_k1);
+    dfree(b->ctx, g.d_k2);
   }
   b->groups.clear();
 }
@@ -2497,6 +2645,7 @@ int wt_batch_set_variant(wt_batch* b, int k1, int k2) {
 }
 
 int wt_batch_step(wt_batch* b, int nsteps) {
+  wt::NvtxRange nvtx_("wt_batch_step");
   if (!b) return WT_EINVAL;
   wt_ctx* ctx = b->ctx;
   if (nsteps < 0) return fail(ctx, WT_EINVAL, "nsteps must be >= 0");
@@ -2613,6 +2762,7 @@ extern "C" {
 
 int wt_rhs_curved_noalloc(wt_ctx* ctx, const wt_coef* coef, const void* Phi, const void* Pi, void* Phidot,
                           void* Pidot, double eps_ko, double mu, const wt_bc_desc* bc, int use_metric) {
+  wt::NvtxRange nvtx_("wt_rhs_curved_noalloc");
   if (!ctx) return WT_EINVAL;
   if (!coef || !Phi || !Pi || !Phidot || !Pidot) return fail(ctx, WT_EINVAL, "wt_rhs_curved_noalloc: NULL argument");
   if (coef->ctx != ctx) return fail(ctx, WT_EINVAL, "coefficients belong to another context");

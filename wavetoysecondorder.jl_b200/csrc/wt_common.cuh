@@ -21,11 +21,31 @@
 
 #include "../../include/wavetoy_b200.h"
 
+#ifndef WT_NO_NVTX
+#include <nvtx3/nvToolsExt.h>
+#endif
+
 #define WT_MAXN 8
 
 struct wt_ctx;  // the public context (include/wavetoy_b200.h)
 
 namespace wt {
+
+// ---- NVTX ranges (host side) ---------------------------------------------------------
+// The C entry points, the RK4 stages, graph captures and replays are named
+// ranges on an Nsight Systems timeline, and `ncu --nvtx --nvtx-include` can pick
+// kernels by them.  NVTX v3 is header-only: with no tool attached a range costs
+// a test of a null function pointer.  -DWT_NO_NVTX compiles them out.
+struct NvtxRange {
+#ifndef WT_NO_NVTX
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+#else
+  explicit NvtxRange(const char*) {}
+#endif
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // ---- host-side GLL operators (product code, independent of the oracle) -----
 struct HostOps {
@@ -150,6 +170,9 @@ __host__ __device__ inline int nbr_face_node(int fs, int p, int q, int N) {
 
 // set the context's last-error message and return code (wt_capi.cu)
 int ctx_fail(::wt_ctx* ctx, int code, const std::string& msg);
+// a device allocation the context tracks (and wt_ctx_inject_alloc_failure can fail), and its release
+int ctx_alloc(::wt_ctx* ctx, void** p, size_t bytes);
+void ctx_free(::wt_ctx* ctx, void* p);
 
 // ---- meshes built from node coordinates (wt_patches.cu, host) ----------------------
 // D4 orientation under which face (e,f)'s nodes coincide with face (en,fn)'s

@@ -44,6 +44,12 @@ struct Req {
   int slot = -1, left = 0;
   double dt = 0, admitted = 0, finished = 0;
   bool finished_flag = false;
+  int status = WT_REQ_WAITING;
+  // preemption: the host checkpoint of the state (wt_state_checkpoint_save) and
+  // the background time it was taken at; resumed from on the next admission
+  std::vector<char> ckpt;
+  double t_ckpt = 0;
+  int preemptions = 0;
 };
 
 int form_of(const wt_serve_desc& d, const wt_serve_request& q) {
@@ -95,6 +101,12 @@ std::string check_request(const wt_serve_request* q) {
   return "";
 }
 
+#define WT_TRY_SERVE(x)      \
+  do {                       \
+    int _rc = (x);           \
+    if (_rc != 0) return _rc; \
+  } while (0)
+
 }  // namespace
 
 struct wt_server {
@@ -107,9 +119,15 @@ struct wt_server {
   std::vector<int> queue;    // arrived, waiting for admission
   std::vector<int> active;   // running, in admission order
   double used = 0, peak = 0;
-  int done = 0;
+  int done = 0, cancelled = 0;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
+  // the admission keys of a request with `steps` left: work and estimated service time
+  void estimate(Req& r, int steps) const {
+    r.work = (double)r.nodes * steps;
+    r.service = 2.0 * r.work / (r.precision == WT_F64 ? d.rate_f64 : d.rate_f32) + 0.05;
+  }
 
   void release(Req& r, bool keep_state) {
     if (r.ws) wt_workspace_destroy(r.ws);
@@ -119,13 +137,14 @@ struct wt_server {
     r.coef = nullptr;
     r.mesh = nullptr;
     if (!keep_state && r.state) {
-      cudaFree(r.state);
+      wt::ctx_free(ctx, r.state);
       r.state = nullptr;
     }
   }
 
   // build request r on the device and add it to the batch
   int admit(Req& r) {
+    wt::NvtxRange nv("wt_serve admit");
     wt_mesh_desc md = r.q.mesh;
     md.precision = r.precision;
     int rc = wt_mesh_create(ctx, &md, &r.mesh);
@@ -133,18 +152,14 @@ struct wt_server {
     if (!rc) rc = wt_background_set(ctx, r.mesh, &r.q.bg, &r.coef);
     if (!rc) rc = wt_workspace_create(ctx, r.mesh, &r.ws);
     const size_t fb = (size_t)r.nodes * esize(r.precision);
-    if (!rc) {
-      cudaError_t e = cudaMalloc(&r.state, 2 * fb);
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        r.state = nullptr;
-        rc = wt::ctx_fail(ctx, WT_ENOMEM, "wt_serve: state allocation failed: " + std::string(cudaGetErrorString(e)));
-      }
-    }
+    if (!rc) rc = wt::ctx_alloc(ctx, &r.state, 2 * fb);
     void* Phi = r.state;
     void* Pi = r.state ? (void*)((char*)r.state + fb) : nullptr;
+    const bool resume = !r.ckpt.empty();
     // (u, u_t) in FP64; an FP32 request keeps the low parts in its workspace
-    if (!rc) rc = wt_initial_state(ctx, r.ws, r.q.ic_kind, r.q.nic ? r.q.ic : nullptr, r.q.nic, 0.0, Phi, Pi);
+    if (!rc && !resume)
+      rc = wt_initial_state(ctx, r.ws, r.q.ic_kind, r.q.nic ? r.q.ic : nullptr, r.q.nic, 0.0, Phi, Pi);
+    if (!rc && resume) rc = wt_state_checkpoint_load(ctx, r.ws, Phi, Pi, r.ckpt.data(), (long long)r.ckpt.size());
     double h = 0;
     if (!rc) rc = wt_mesh_min_spacing(r.mesh, &h);
     if (!rc) {
@@ -152,17 +167,71 @@ struct wt_server {
       // a time-dependent background is re-sampled on the mesh every stage: keep its geometry
       const bool td = r.q.bg.kind == WT_BG_GAUGE_WAVE || r.q.bg.kind == WT_BG_SINE_SHIFT;
       if (!td) rc = wt_mesh_release_setup_geometry(r.mesh);
+      else if (resume) rc = wt_coef_set_time(ctx, r.coef, r.t_ckpt);
     }
     if (!rc) rc = wt_batch_add(batch, r.ws, r.coef, Phi, Pi, r.dt, &r.q.bc, &r.slot);
     if (rc) {
       release(r, false);
       return rc;
     }
-    r.left = r.q.steps;
+    if (!resume) r.left = r.q.steps;
+    r.ckpt.clear();
+    r.ckpt.shrink_to_fit();
+    r.status = WT_REQ_RUNNING;
+    return 0;
+  }
+
+  // take running request rid out of the batch and release its device memory
+  int leave_batch(int rid, bool keep_state) {
+    Req& r = reqs[rid];
+    const int rc = wt_batch_remove(batch, r.slot);
+    if (rc) return rc;
+    release(r, keep_state);
+    used -= r.cost;
+    active.erase(std::find(active.begin(), active.end(), rid));
+    return 0;
+  }
+
+  int preempt(int rid) {
+    Req& r = reqs[rid];
+    long long nb = 0;
+    int rc = wt_state_checkpoint_size(r.ws, &nb);
+    if (rc) return rc;
+    std::vector<char> ck((size_t)nb);
+    const size_t fb = (size_t)r.nodes * esize(r.precision);
+    void* Phi = r.state;
+    void* Pi = (char*)r.state + fb;
+    rc = wt_state_checkpoint_save(ctx, r.ws, Phi, Pi, ck.data(), nb);  // synchronises: the steps so far are done
+    if (!rc && (r.q.bg.kind == WT_BG_GAUGE_WAVE || r.q.bg.kind == WT_BG_SINE_SHIFT))
+      rc = wt_coef_get_time(r.coef, &r.t_ckpt);
+    if (!rc) rc = leave_batch(rid, false);
+    if (rc) return rc;
+    r.ckpt.swap(ck);
+    r.status = WT_REQ_PREEMPTED;
+    r.preemptions += 1;
+    estimate(r, r.left);
+    queue.push_back(rid);  // ordered with the others at the next round
+    return 0;
+  }
+
+  int cancel(int rid) {
+    Req& r = reqs[rid];
+    if (r.status == WT_REQ_RUNNING) {
+      WT_TRY_SERVE(wt_ctx_synchronize(ctx));
+      WT_TRY_SERVE(leave_batch(rid, false));
+    } else {
+      pending.erase(std::remove(pending.begin(), pending.end(), rid), pending.end());
+      queue.erase(std::remove(queue.begin(), queue.end(), rid), queue.end());
+      r.ckpt.clear();
+      r.ckpt.shrink_to_fit();
+    }
+    r.status = WT_REQ_CANCELLED;
+    ++cancelled;
     return 0;
   }
 
   int poll(int* nfin) {
+    wt::NvtxRange nv("wt_serve_poll");
     int fin = 0;
     const double t = now();
     while (!pending.empty() && reqs[pending.front()].q.arrival <= t) {
@@ -197,12 +266,12 @@ struct wt_server {
       used += r.cost;
       peak = std::max(peak, used);
       const int rid = queue.front();
-      queue.erase(queue.begin());
       const int rc = admit(r);
-      if (rc) {
+      if (rc) {  // the request stays at the head of the queue; a later round retries it
         used -= r.cost;
         return rc;
       }
+      queue.erase(queue.begin());
       r.admitted = now();
       active.push_back(rid);
     }
@@ -232,6 +301,7 @@ struct wt_server {
       if (rc) return rc;
       r.finished = t_done;
       r.finished_flag = true;
+      r.status = WT_REQ_FINISHED;
       release(r, d.keep_results != 0);
       used -= r.cost;
       ++done;
@@ -295,8 +365,8 @@ int wt_serve_submit(wt_server* s, const wt_serve_request* req, int* rid) {
   if (r.cost > s->d.hbm_budget)
     return wt::ctx_fail(s->ctx, WT_EINVAL, "wt_serve_submit: the request (" + std::to_string(r.nodes) +
                                                " nodes) does not fit the HBM budget");
-  r.work = (double)r.nodes * req->steps;
-  r.service = 2.0 * r.work / (r.precision == WT_F64 ? s->d.rate_f64 : s->d.rate_f32) + 0.05;
+  r.left = req->steps;
+  s->estimate(r, req->steps);
   const int id = (int)s->reqs.size();
   s->reqs.push_back(r);
   // pending stays ordered by (arrival, rid)
@@ -356,6 +426,37 @@ int wt_serve_result_state(wt_server* s, int rid, void* Phi, void* Pi) {
       cudaMemcpyAsync(Pi, (char*)r.state + fb, fb, cudaMemcpyDeviceToDevice, (cudaStream_t)st) != cudaSuccess)
     return wt::ctx_fail(s->ctx, WT_ECUDA, "wt_serve_result_state: copy failed");
   return 0;
+}
+
+int wt_serve_status(const wt_server* s, int rid, int* status, int* steps_left, int* preemptions) {
+  if (!s) return WT_EINVAL;
+  if (rid < 0 || rid >= (int)s->reqs.size())
+    return wt::ctx_fail(s->ctx, WT_EINVAL, "wt_serve_status: no request " + std::to_string(rid));
+  const Req& r = s->reqs[rid];
+  if (status) *status = r.status;
+  if (steps_left) *steps_left = r.left;
+  if (preemptions) *preemptions = r.preemptions;
+  return 0;
+}
+
+int wt_serve_cancel(wt_server* s, int rid) {
+  if (!s) return WT_EINVAL;
+  wt::NvtxRange nv("wt_serve_cancel");
+  if (rid < 0 || rid >= (int)s->reqs.size())
+    return wt::ctx_fail(s->ctx, WT_EINVAL, "wt_serve_cancel: no request " + std::to_string(rid));
+  const int st = s->reqs[rid].status;
+  if (st == WT_REQ_FINISHED || st == WT_REQ_CANCELLED)
+    return wt::ctx_fail(s->ctx, WT_EINVAL, "wt_serve_cancel: request " + std::to_string(rid) + " has " +
+                                               (st == WT_REQ_FINISHED ? "finished" : "been cancelled"));
+  return s->cancel(rid);
+}
+
+int wt_serve_preempt(wt_server* s, int rid) {
+  if (!s) return WT_EINVAL;
+  wt::NvtxRange nv("wt_serve_preempt");
+  if (rid < 0 || rid >= (int)s->reqs.size() || s->reqs[rid].status != WT_REQ_RUNNING)
+    return wt::ctx_fail(s->ctx, WT_EINVAL, "wt_serve_preempt: request " + std::to_string(rid) + " is not running");
+  return s->preempt(rid);
 }
 
 int wt_serve_info(const wt_server* s, int* waiting, int* active, int* done, double* used_bytes, double* peak_bytes) {

@@ -74,6 +74,8 @@ class _BcDesc(C.Structure):
 
 SERVE_HRRN, SERVE_SJF, SERVE_FIFO = 0, 1, 2
 SERVE_AUTO = -1
+# wt_serve_status
+REQ_WAITING, REQ_RUNNING, REQ_FINISHED, REQ_CANCELLED, REQ_PREEMPTED = 0, 1, 2, 3, 4
 SERVE_MAX_IC = 128
 
 
@@ -112,6 +114,8 @@ def library():
         "wt_ctx_get_stream": [vp, pvp], "wt_ctx_set_stream": [vp, vp],
         "wt_ctx_launch_count": [vp, C.POINTER(ll)], "wt_ctx_nonfinite": [vp, C.POINTER(i)],
         "wt_ctx_selftest_wait": [vp, i, ll],
+        "wt_ctx_memory": [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)],
+        "wt_ctx_inject_alloc_failure": [vp, ll],
         "wt_mesh_create": [vp, C.POINTER(_MeshDesc), pvp],
         "wt_mesh_create_arrays": [vp, i, ll, vp, vp, vp, vp, vp, vp, i, pvp],
         "wt_mesh_create_patches": [vp, C.POINTER(_PatchDesc), pvp],
@@ -167,6 +171,10 @@ def library():
         "wt_serve_submit": [vp, C.POINTER(_ServeRequest), C.POINTER(i)], "wt_serve_poll": [vp, C.POINTER(i)],
         "wt_serve_run": [vp], "wt_serve_get_result": [vp, i, C.POINTER(_ServeResult)],
         "wt_serve_result_state": [vp, i, vp, vp],
+        "wt_serve_status": [vp, i, C.POINTER(i), C.POINTER(i), C.POINTER(i)], "wt_serve_cancel": [vp, i],
+        "wt_serve_preempt": [vp, i],
+        "wt_state_checkpoint_size": [vp, C.POINTER(ll)], "wt_state_checkpoint_save": [vp, vp, vp, vp, vp, ll],
+        "wt_state_checkpoint_load": [vp, vp, vp, vp, vp, ll],
         "wt_serve_info": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(d), C.POINTER(d)],
         "wt_serve_cost": [C.POINTER(_ServeDesc), C.POINTER(_ServeRequest), C.POINTER(d), C.POINTER(i)],
         "wt_serve_queue_order": [i, d, i, vp, vp, vp, vp],
@@ -253,6 +261,18 @@ class Context:
         f = C.c_int()
         self.check(library().wt_ctx_nonfinite(self.h, C.byref(f)))
         return bool(f.value)
+
+    def memory(self):
+        """(live bytes, live allocations, allocations so far) of the device memory
+        this context's objects hold."""
+        v = [C.c_longlong() for _ in range(3)]
+        self.check(library().wt_ctx_memory(self.h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def inject_alloc_failure(self, after: int):
+        """Make the device allocation `after` allocations from now fail once with
+        WT_ENOMEM (host side; after < 0 cancels)."""
+        self.check(library().wt_ctx_inject_alloc_failure(self.h, int(after)))
 
     def close(self):
         """Destroy the context after every object made on it (children first:
@@ -716,6 +736,20 @@ class ServeEngine(_Child):
         Pi = torch.empty_like(Phi)
         self.ctx.check(library().wt_serve_result_state(self.h, int(rid), _ptr(Phi), _ptr(Pi)), "wt_serve_result_state")
         return Phi, Pi
+
+    def status(self, rid: int) -> dict:
+        """{"status": REQ_*, "steps_left": ..., "preemptions": ...} of a request."""
+        st, left, pre = C.c_int(), C.c_int(), C.c_int()
+        self.ctx.check(library().wt_serve_status(self.h, int(rid), C.byref(st), C.byref(left), C.byref(pre)),
+                       "wt_serve_status")
+        return {"status": st.value, "steps_left": left.value, "preemptions": pre.value}
+
+    def cancel(self, rid: int):
+        self.ctx.check(library().wt_serve_cancel(self.h, int(rid)), "wt_serve_cancel")
+
+    def preempt(self, rid: int):
+        """Checkpoint a running request to host memory and put it back in the queue."""
+        self.ctx.check(library().wt_serve_preempt(self.h, int(rid)), "wt_serve_preempt")
 
     def info(self) -> dict:
         w, a, dn, u, pk = C.c_int(), C.c_int(), C.c_int(), C.c_double(), C.c_double()
@@ -1218,6 +1252,27 @@ def state_from_f64(ws: "Workspace", Phi64, Pi64, Phi, Pi):
     the rounded values in Phi, Pi and the lost low parts in the workspace."""
     ws.ctx.check(library().wt_state_set_f64(ws.ctx.h, ws.h, _ptr(Phi64), _ptr(Pi64), _ptr(Phi), _ptr(Pi)),
                  "state_from_f64")
+    return Phi, Pi
+
+
+def checkpoint_save(ws: "Workspace", Phi, Pi):
+    """The stepped state (Phi, Pi) as a host checkpoint (numpy uint8), word for word, the FP32 low
+    parts included (wt_state_checkpoint_save); synchronous."""
+    import numpy as np
+    n = C.c_longlong()
+    ws.ctx.check(library().wt_state_checkpoint_size(ws.h, C.byref(n)), "wt_state_checkpoint_size")
+    buf = np.empty(n.value, dtype=np.uint8)
+    ws.ctx.check(library().wt_state_checkpoint_save(ws.ctx.h, ws.h, _ptr(Phi), _ptr(Pi), buf.ctypes.data, n.value),
+                 "wt_state_checkpoint_save")
+    return buf
+
+
+def checkpoint_load(ws: "Workspace", Phi, Pi, buf):
+    """Restore a checkpoint into the state arrays (Phi, Pi) that ws steps (wt_state_checkpoint_load)."""
+    import numpy as np
+    buf = np.ascontiguousarray(buf, dtype=np.uint8)
+    ws.ctx.check(library().wt_state_checkpoint_load(ws.ctx.h, ws.h, _ptr(Phi), _ptr(Pi), buf.ctypes.data,
+                                                    int(buf.size)), "wt_state_checkpoint_load")
     return Phi, Pi
 
 
