@@ -96,6 +96,25 @@ int wt_ctx_memory(const wt_ctx* ctx, long long* live_bytes, long long* live_allo
  * failing call releases what it had allocated, and the context stays usable.
  * No device fault is involved.  No counterpart in the reference. */
 int wt_ctx_inject_alloc_failure(wt_ctx* ctx, long long after);
+/* How this library was built: WT_BUILD_BOUNDS_CHECK (compiled with
+ * -DWT_BOUNDS_CHECK: every index a kernel reads from the mesh's neighbour,
+ * face-source and boundary-slot tables is checked against the table's range
+ * before use) and WT_BUILD_NVTX (NVTX ranges on the entry points).  Host only. */
+enum { WT_BUILD_BOUNDS_CHECK = 1, WT_BUILD_NVTX = 2 };
+int wt_build_flags(int* flags);
+/* Synchronise, then read and clear the bounds word of the bounds-check build:
+ * bit 0 = a neighbour element index out of range was read, bit 1 = a boundary
+ * slot out of range.  The kernel replaced the value by "no neighbour" / slot 0
+ * and made no access outside its buffers.  Always 0 in the normal build.  No
+ * counterpart in the reference (its kernels run with @inbounds). */
+int wt_ctx_bounds_status(wt_ctx* ctx, unsigned int* word);
+/* Bounds-check build only (WT_ENOTSUP otherwise): overwrite entry (e, f) of a
+ * mesh's device face-source table (64 * neighbour + 8 * orientation +
+ * neighbour face, -1 = none) or boundary-slot table, so that a test can plant
+ * an out-of-range index and see wt_ctx_bounds_status report it while every
+ * access stays inside its buffer.  Synchronous. */
+enum { WT_TABLE_FACE_SOURCE = 0, WT_TABLE_BOUNDARY_SLOT = 1 };
+int wt_mesh_debug_set_table(wt_mesh* mesh, int table, long long e, int f, int value);
 /* Read and clear the device non-finite flag that fused RK4 steps set when the
  * state stops being finite (the reference asserts all(isfinite, ...) per
  * sample, src/evolve.jl:1344); synchronous. */

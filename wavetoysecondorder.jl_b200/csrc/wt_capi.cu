@@ -552,6 +552,44 @@ int wt_ctx_memory(const wt_ctx* ctx, long long* live_bytes, long long* live_allo
   return 0;
 }
 
+int wt_build_flags(int* flags) {
+  if (!flags) return WT_EINVAL;
+  *flags = 0;
+#ifdef WT_BOUNDS_CHECK
+  *flags |= WT_BUILD_BOUNDS_CHECK;
+#endif
+#ifndef WT_NO_NVTX
+  *flags |= WT_BUILD_NVTX;
+#endif
+  return 0;
+}
+
+int wt_mesh_debug_set_table(wt_mesh* mesh, int table, long long e, int f, int value) {
+  if (!mesh) return WT_EINVAL;
+#ifndef WT_BOUNDS_CHECK
+  (void)table; (void)e; (void)f; (void)value;
+  return fail(mesh->ctx, WT_ENOTSUP, "wt_mesh_debug_set_table: only in the bounds-check build (-DWT_BOUNDS_CHECK)");
+#else
+  const wt::DevMesh& m = mesh->m;
+  if (e < 0 || e >= m.Ne || f < 0 || f > 5 || (table != WT_TABLE_FACE_SOURCE && table != WT_TABLE_BOUNDARY_SLOT))
+    return fail(mesh->ctx, WT_EINVAL, "wt_mesh_debug_set_table: bad table, element or face");
+  int32_t* t = table == WT_TABLE_FACE_SOURCE ? m.fsrc : m.bslot;
+  if (!t) return fail(mesh->ctx, WT_EINVAL, "wt_mesh_debug_set_table: the mesh has no such table");
+  const int32_t v = value;
+  cudaError_t err = cudaMemcpyAsync(t + f + 6 * e, &v, sizeof(v), cudaMemcpyHostToDevice, mesh->ctx->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(mesh->ctx->stream);
+  return err == cudaSuccess ? 0 : cuda_fail(mesh->ctx, err, "wt_mesh_debug_set_table");
+#endif
+}
+
+int wt_ctx_bounds_status(wt_ctx* ctx, unsigned int* word) {
+  if (!ctx || !word) return WT_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "wt_ctx_bounds_status");
+  *word = wt::bounds_take_cons() | wt::bounds_take_n8() | wt::bounds_take_second() | wt::bounds_take_geom();
+  return 0;
+}
+
 int wt_ctx_inject_alloc_failure(wt_ctx* ctx, long long after) {
   if (!ctx) return WT_EINVAL;
   ctx->fail_after = after < 0 ? -1 : after;

@@ -47,6 +47,56 @@ struct NvtxRange {
   NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
+// ---- bounds-check build (-DWT_BOUNDS_CHECK) ------------------------------------------
+// The kernels index memory through four host-built tables: face sources
+// (fsrc: 64 * neighbour element + 8 * orientation + neighbour face), neighbour
+// elements (nbr), boundary slots (bslot) and, for batches, (solve, element)
+// tiles built from the member list.  Every value read from the first three
+// passes through one of these checks where it is loaded, so every access that
+// depends on it is covered.  In the bounds-check build a value outside its
+// table's range sets a bit of this translation unit's bounds word (1:
+// element, 2: boundary slot) and is replaced by "no neighbour" (-1) or slot
+// 0, which every buffer holds; the kernel goes on and no access leaves its
+// buffer.  wt_ctx_bounds_status reads and clears the words.  In the normal
+// build the checks compile to nothing.
+#ifdef WT_BOUNDS_CHECK
+static __device__ unsigned int wt_bounds_word;  // one per translation unit
+__device__ __forceinline__ int bc_src(int v, long long Ne) {
+  if (v < 0 || (long long)(v >> 6) < Ne) return v;
+  atomicOr(&wt_bounds_word, 1u);
+  return -1;
+}
+__device__ __forceinline__ int bc_elem(int v, long long Ne) {
+  if (v < Ne) return v;
+  atomicOr(&wt_bounds_word, 1u);
+  return -1;
+}
+__device__ __forceinline__ int bc_slot(int v, int nbf) {
+  if (v >= 0 && v < (nbf > 0 ? nbf : 1)) return v;
+  atomicOr(&wt_bounds_word, 2u);
+  return 0;
+}
+// defines `unsigned int fn()`: this translation unit's bounds word, cleared
+#define WT_BOUNDS_TAKE(fn)                                              \
+  unsigned int fn() {                                                   \
+    unsigned int v = 0, z = 0;                                          \
+    cudaMemcpyFromSymbol(&v, wt::wt_bounds_word, sizeof(v));            \
+    cudaMemcpyToSymbol(wt::wt_bounds_word, &z, sizeof(z));              \
+    return v;                                                           \
+  }
+#else
+__device__ __forceinline__ int bc_src(int v, long long) { return v; }
+__device__ __forceinline__ int bc_elem(int v, long long) { return v; }
+__device__ __forceinline__ int bc_slot(int v, int) { return v; }
+#define WT_BOUNDS_TAKE(fn) \
+  unsigned int fn() { return 0; }
+#endif
+// the bounds words of the kernel translation units (wt_cons.cu, wt_cons_n8.cu, wt_second.cu, wt_geom.cu)
+unsigned int bounds_take_cons();
+unsigned int bounds_take_n8();
+unsigned int bounds_take_second();
+unsigned int bounds_take_geom();
+
 // ---- host-side GLL operators (product code, independent of the oracle) -----
 struct HostOps {
   int N = 0;

@@ -289,7 +289,7 @@ __device__ __forceinline__ void k1_finish(const K1P<real>& P, long long ec, long
       const int ax = f >> 1;
       if (idx3[ax] != frow(f, N)) continue;
       const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
-      const int slot = P.bslot[f + 6 * ec];
+      const int slot = ::wt::bc_slot(P.bslot[f + 6 * ec], P.nbf);
       real dF = 0, dP = 0;
       if (!P.bc_curv) {
         const int kind = P.kinds[f];
@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_, GenOcc<Ep<N>::N3 * EPB_>::va
   for (int idx = t; idx < 6 * N2; idx += N3) {
     const int f = idx / N2, pq = idx - f * N2;
     gt v = 0;
-    const int src = valid ? P.fsrc[f + 6 * ec] : -1;
+    const int src = valid ? ::wt::bc_src(P.fsrc[f + 6 * ec], P.Ne) : -1;
     if (src >= 0) {
       const long long nb = (long long)(src >> 6) * N3 + nbr_face_node(src, pq % N, pq / N, N);
       v = P.Phi[nb];
@@ -632,7 +632,7 @@ __global__ void __launch_bounds__(PipeK1<N, real, CP>::T, PipeK1<N, real, CP>::O
 #pragma unroll
     for (int r = 0; r < NFR; ++r) {
       const int idx = t + r * N3;
-      src[r] = (tl.x >= 0 && idx < 6 * N2) ? plist[tl.x].fsrc[idx / N2 + 6 * tl.y] : -1;
+      src[r] = (tl.x >= 0 && idx < 6 * N2) ? ::wt::bc_src(plist[tl.x].fsrc[idx / N2 + 6 * tl.y], plist[tl.x].Ne) : -1;
     }
   };
   // copy what tile tl reads at this thread's node, and this thread's face-trace
@@ -808,7 +808,7 @@ struct K2P {
   const double* G;
   const double* H;
   const real* bbuf;
-  int bc_on;
+  int bc_on, nbf;
   real* Pidot;
   int epi, stage;
   double dt;
@@ -873,7 +873,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
   for (int idx = t; idx < 6 * N2; idx += N3) {
     const int f = idx / N2, pq = idx - f * N2;
     long long src = -1;
-    const int fs = valid ? P.fsrc[f + 6 * ec] : -1;  // -1 exactly where the SAT mask bit is 0
+    const int fs = valid ? ::wt::bc_src(P.fsrc[f + 6 * ec], P.Ne) : -1;  // -1 exactly where the SAT mask bit is 0
     if (fs >= 0) src = (long long)(fs >> 6) * N3 + nbr_face_node(fs, pq % N, pq / N, N);
     if (CURV) {
 #pragma unroll
@@ -933,7 +933,7 @@ __global__ void __launch_bounds__(Ep<N>::N3 * EPB_) k_cons_k2(const K2P<real> P0
       const int ax = f >> 1;
       if (idx3[ax] != frow(f, N)) continue;
       const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
-      dv += P.bbuf[(long long)P.bslot[f + 6 * ec] * N2 + p + N * q];
+      dv += P.bbuf[(long long)::wt::bc_slot(P.bslot[f + 6 * ec], P.nbf) * N2 + p + N * q];
     }
   }
   if (P.epi) {
@@ -992,7 +992,7 @@ __global__ void __launch_bounds__(PipeK2<N, real>::T, PipeK2<N, real>::OCC)
 #pragma unroll
     for (int r = 0; r < NFR; ++r) {
       const int idx = t + r * N3;
-      src[r] = (tl.x >= 0 && idx < 6 * N2) ? plist[tl.x].fsrc[idx / N2 + 6 * tl.y] : -1;
+      src[r] = (tl.x >= 0 && idx < 6 * N2) ? ::wt::bc_src(plist[tl.x].fsrc[idx / N2 + 6 * tl.y], plist[tl.x].Ne) : -1;
     }
   };
   auto issue = [&](int2 tl, const int src[NFR], int bb) {
@@ -1082,7 +1082,7 @@ __global__ void __launch_bounds__(PipeK2<N, real>::T, PipeK2<N, real>::OCC)
           const int ax = f >> 1;
           if (idx3[ax] != frow(f, N)) continue;
           const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
-          dv += P.bbuf[(long long)P.bslot[f + 6 * ec] * N2 + p + N * q];
+          dv += P.bbuf[(long long)::wt::bc_slot(P.bslot[f + 6 * ec], P.nbf) * N2 + p + N * q];
         }
       }
       if (P.epi) {
@@ -1133,7 +1133,7 @@ __global__ void __launch_bounds__(Ep<N>::T) k_apply_D(long long Ne, const real* 
   for (int f = 2 * d; f < 2 * d + 2; ++f) {
     if (idx3[d] != frow(f, N)) continue;
     if (bdry[f + 6 * ec] != 0) continue;
-    const int en = nbr[f + 6 * ec];
+    const int en = ::wt::bc_elem(nbr[f + 6 * ec], Ne);
     if (en < 0) continue;
     const int p = d == 0 ? j : i, q = d == 2 ? j : k;
     const real un = u[(long long)en * N3 + nbr_face_node(nbrf[f + 6 * ec], p, q, N)];
@@ -1287,7 +1287,7 @@ static K2P<real> k2p_params(const DevMesh& m, const void* F, void* Pidot, const 
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot;
   P.emask = m.emask; P.fsrc = m.fsrc;
   P.G = m.G; P.H = m.H;
-  P.bbuf = (const real*)bbuf; P.bc_on = bc.on;
+  P.bbuf = (const real*)bbuf; P.bc_on = bc.on; P.nbf = m.nbf;
   P.Pidot = (real*)Pidot;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.nonfinite = nonfinite;
@@ -1579,5 +1579,8 @@ int launch_cons_gen_batch(int which, int N, int precision, int epb_variant, int 
                           long long ntiles, cudaStream_t s) {
   WT_DISPATCH_N(N, (gen_batch_n<NN>(which, precision, epb_variant, cp != 0, plist, tiles, ntiles, s)));
 }
+
+// this file's bounds word (bounds-check build; 0 otherwise)
+WT_BOUNDS_TAKE(bounds_take_cons)
 
 }  // namespace wt

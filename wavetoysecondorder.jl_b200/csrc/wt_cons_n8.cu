@@ -383,7 +383,7 @@ __device__ __forceinline__ void k1_boundary(const K1N8<real>& Q, long long e, in
     const int ax = f >> 1;
     if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
     const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
-    const int slot = Q.bslot[f + 6 * e];
+    const int slot = ::wt::bc_slot(Q.bslot[f + 6 * e], Q.nbf);
     real dF = 0, dP = 0;
     if (tag != Q.exc_tag) {
       const long long nb = (long long)Q.nbf * N2;
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(n8::THREADS, n8::Occ<real>::k1)
   // the trace itself, and the tile two iterations before, so no load waits on
   // another inside the loop.
   const int my_f = tid >> 6, my_pq = tid & 63;
-  auto src_load = [&](int2 tl) -> int { return (tl.x >= 0 && tid < 6 * N2) ? prm(tl.x).fsrc[my_f + 6 * tl.y] : -1; };
+  auto src_load = [&](int2 tl) -> int { return (tl.x >= 0 && tid < 6 * N2) ? ::wt::bc_src(prm(tl.x).fsrc[my_f + 6 * tl.y], prm(tl.x).Ne) : -1; };
   auto face_load = [&](int src, int sidx) -> real {
     if (src < 0) return (real)0;
     return prm(sidx).Phi[(long long)(src >> 6) * N3 + nbr_face_node(src, my_pq & 7, my_pq >> 3, N)];
@@ -774,7 +774,7 @@ struct K2N8 {
   const double* G;
   const double* H;
   const real* bbuf;
-  int bc_on;
+  int bc_on, nbf;
   real* Pidot;
   int epi, stage;
   double dt;
@@ -879,7 +879,7 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
 #pragma unroll
     for (int r = 0; r < NFR; ++r) {
       const int idx = tid + r * THR;
-      src[r] = (tl.x >= 0 && idx < NFACE) ? prm(tl.x).fsrc[idx / (3 * N2) + 6 * tl.y] : -1;
+      src[r] = (tl.x >= 0 && idx < NFACE) ? ::wt::bc_src(prm(tl.x).fsrc[idx / (3 * N2) + 6 * tl.y], prm(tl.x).Ne) : -1;
     }
   };
   auto face_load = [&](const int src[NFR], int sidx, real fv[NFR]) {
@@ -1096,7 +1096,7 @@ __global__ void __launch_bounds__(K2Shape<real>::THR, K2Shape<real>::OCC)
           const int ax = f >> 1;
           if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
           const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
-          dv += Q.bbuf[(long long)Q.bslot[f + 6 * e] * N2 + p + 8 * q];
+          dv += Q.bbuf[(long long)::wt::bc_slot(Q.bslot[f + 6 * e], Q.nbf) * N2 + p + 8 * q];
         }
       }
       if (P.epi)
@@ -1278,10 +1278,10 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_fk_n8(const FKN8 P) {
 #pragma unroll
     for (int r = 0; r < NFR; ++r) {
       const int idx = tid + r * THREADS;
-      src[r] = (e < T && idx < NFACE) ? A.fsrc[idx / (3 * N2) + 6 * e] : -1;
+      src[r] = (e < T && idx < NFACE) ? ::wt::bc_src(A.fsrc[idx / (3 * N2) + 6 * e], A.Ne) : -1;
     }
   };
-  auto srcP_load = [&](long long e) -> int { return (e < T && tid < NPF) ? B.fsrc[(tid >> 6) + 6 * e] : -1; };
+  auto srcP_load = [&](long long e) -> int { return (e < T && tid < NPF) ? ::wt::bc_src(B.fsrc[(tid >> 6) + 6 * e], B.Ne) : -1; };
   auto faceF_load = [&](const int src[NFR], real fv[NFR]) {
 #pragma unroll
     for (int r = 0; r < NFR; ++r) {
@@ -1504,7 +1504,7 @@ __global__ void __launch_bounds__(n8::THREADS, 1) k_cons_fk_n8(const FKN8 P) {
           const int ax = f >> 1;
           if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
           const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
-          dv += A.bbuf[(long long)A.bslot[f + 6 * e] * N2 + p + 8 * q];
+          dv += A.bbuf[(long long)::wt::bc_slot(A.bslot[f + 6 * e], A.nbf) * N2 + p + 8 * q];
         }
       }
       const real Pi = n8_rk_out(sa, A.dt, dv, cur.Qy, cur.Qacc, n, A.acc, A.out);  // Pi_{s+1}
@@ -1724,7 +1724,7 @@ __global__ void __launch_bounds__(n8::CTHR, K1C_OCC)
 #pragma unroll
     for (int r = 0; r < NFR; ++r) {
       const int idx = tid + r * THR;
-      src[r] = (tl.x >= 0 && idx < NFT) ? prm(tl.x).fsrc[(idx >> 6) + 6 * tl.y] : -1;
+      src[r] = (tl.x >= 0 && idx < NFT) ? ::wt::bc_src(prm(tl.x).fsrc[(idx >> 6) + 6 * tl.y], prm(tl.x).Ne) : -1;
     }
   };
   // neighbour Phi face traces and this element's Phi of tile tl straight into
@@ -2043,7 +2043,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
   // uniform), point tid & 63: sface[(r * 3 + c) * 64 + pq] = sface[r * THR + tid]
   auto src_load = [&](int2 tl, int src[NFR]) {
 #pragma unroll
-    for (int r = 0; r < NFR; ++r) src[r] = tl.x >= 0 ? prm(tl.x).fsrc[r + 6 * tl.y] : -1;
+    for (int r = 0; r < NFR; ++r) src[r] = tl.x >= 0 ? ::wt::bc_src(prm(tl.x).fsrc[r + 6 * tl.y], prm(tl.x).Ne) : -1;
   };
   // neighbour flux face traces of tile tl straight into shared buffer b
   auto async_faces = [&](int2 tl, const int src[NFR], int b) {
@@ -2175,7 +2175,7 @@ __global__ void __launch_bounds__(n8::CTHR, K2C_OCC)
           const int ax = f >> 1;
           if (idx3[ax] != ((f & 1) ? 7 : 0)) continue;
           const int p = ax == 0 ? tj : ti, q = ax == 2 ? tj : tk;
-          dv += Q.bbuf[(long long)Q.bslot[f + 6 * e] * N2 + p + 8 * q];
+          dv += Q.bbuf[(long long)::wt::bc_slot(Q.bslot[f + 6 * e], Q.nbf) * N2 + p + 8 * q];
         }
       }
       const real yv = need_y ? sB[N3 + node] : (real)0, accv = need_acc ? sB[2 * N3 + node] : (real)0;
@@ -2327,7 +2327,7 @@ static K2N8<real> k2n8_params(const DevMesh& m, const void* F, void* Pidot, cons
   P.Ja = (const real*)m.Ja_n8; P.invdetJ = (const real*)m.invdetJ_r;
   P.nbr = m.nbr; P.nbrf = m.nbrf; P.bdry = m.bdry; P.bslot = m.bslot; P.G = m.G; P.H = m.H;
   P.emask = m.emask; P.fsrc = m.fsrc;
-  P.bbuf = (const real*)bbuf; P.bc_on = bc.on;
+  P.bbuf = (const real*)bbuf; P.bc_on = bc.on; P.nbf = m.nbf;
   P.Pidot = (real*)Pidot;
   P.epi = rk.on; P.stage = rk.stage; P.dt = rk.dt;
   P.y = (real*)rk.y; P.acc = (real*)rk.acc; P.out = (real*)rk.out; P.comp = (real*)rk.comp; P.flag = flag;
@@ -2602,5 +2602,8 @@ int launch_cons_n8_batch(int which, int precision, int fp32_form, const void* hP
                          long long ntiles, cudaStream_t s) {
   return n8_dispatch<true>(which, precision, fp32_form, hP0, plist, tiles, ntiles, s);
 }
+
+// this file's bounds word (bounds-check build; 0 otherwise)
+WT_BOUNDS_TAKE(bounds_take_n8)
 
 }  // namespace wt

@@ -281,7 +281,7 @@ __global__ void k_bnorm(int N, long long Ne, const int32_t* __restrict__ bslot, 
   const long long fe = gid / (N * N);
   const int f = (int)(fe % 6);
   const long long e = fe / 6;
-  const int slot = bslot[f + 6 * e];
+  const int slot = bslot[f + 6 * e] < 0 ? -1 : ::wt::bc_slot(bslot[f + 6 * e], nbf);
   if (slot < 0) return;
   const int p = pq % N, q = pq / N;
   const int ai = faxis(f), row = frow(f, N);
@@ -569,5 +569,8 @@ int launch_initial(const DevMesh& m, int kind, const double* dparams, int np, do
     k_initial<float><<<b, 256, 0, s>>>(m.nn, kind, m.coords, dparams, np, t, (float*)u, (float*)ut);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
+
+// this file's bounds word (bounds-check build; 0 otherwise)
+WT_BOUNDS_TAKE(bounds_take_geom)
 
 }  // namespace wt

@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(Sp<N>::T) k_sipg_rhs(const SipgP<real> P) {
     real du = 0;
     if (valid) {
       const int tag = P.bdry[f + 6 * ec];
-      const int en = P.nbr[f + 6 * ec];
+      const int en = ::wt::bc_elem(P.nbr[f + 6 * ec], P.Ne);
       const int ax = f >> 1;
       const int fl = face_node(ax, frow(f, N), pq % N, pq / N, N);
       if (tag == 0 && en >= 0) {
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(Sp<N>::T) k_sipg_rhs(const SipgP<real> P) {
   const int idx3[3] = {i, j, k};
   for (int f = 0; f < 6; ++f) {
     const int tag = P.bdry[f + 6 * ec];
-    const int en = P.nbr[f + 6 * ec];
+    const int en = ::wt::bc_elem(P.nbr[f + 6 * ec], P.Ne);
     const bool interior = tag == 0 && en >= 0;
     const bool dir = tag >= 1 && tag <= 6;
     if (!interior && !dir) continue;
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(Sp<N>::T) k_sipg_rhs(const SipgP<real> P) {
     if (idx3[ax] != frow(f, N)) continue;
     const int p = ax == 0 ? j : i, q = ax == 2 ? j : k;
     const long long nb = (long long)P.nbf * N2;
-    const long long bi = (long long)P.bslot[f + 6 * ec] * N2 + p + N * q;
+    const long long bi = (long long)::wt::bc_slot(P.bslot[f + 6 * ec], P.nbf) * N2 + p + N * q;
     const real nx = P.bnorm[bi], ny = P.bnorm[nb + bi], nz = P.bnorm[2 * nb + bi], wFH = P.bnorm[4 * nb + bi];
     const real Gn = nx * D[0] + ny * D[1] + nz * D[2];
     acc -= wFH * (P.ut[n] + Gn + P.inv_R * uv);
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(Sp<N>::T) k_strong(const StrongP<real> P) {
     const int f = idx / N2, pq = idx - f * N2;
     double v = 0.0;
     if (valid) {
-      const int en = P.nbr[f + 6 * ec];
+      const int en = ::wt::bc_elem(P.nbr[f + 6 * ec], P.Ne);
       if (en >= 0) {
         const int fs = P.nbrf[f + 6 * ec];  // fn | ori << 3
         v = (double)P.u[(long long)en * N3 + nbr_face_node(fs, pq % N, pq / N, N)];
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(Sp<N>::T) k_lap_strong_cons(long long Ne, cons
     const double coef_dir = -tau * inv_h / H[fr];
     const int p = al == 0 ? j : i, q = al == 2 ? j : k;
     double uf = 0.0;
-    const int en = nbr[f + 6 * ec];
+    const int en = ::wt::bc_elem(nbr[f + 6 * ec], Ne);
     if (en >= 0) {
       const int fs = nbrf[f + 6 * ec];  // fn | ori << 3
       uf = (double)u[(long long)en * N3 + nbr_face_node(fs, p, q, N)];
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(Sp<N>::T) k_curved4(long long Ne, const real* 
     vf[f] = 0.0;
     const int al = f >> 1;
     if (!valid || idx3[al] != frow(f, N)) continue;
-    const int en = nbr[f + 6 * ec];
+    const int en = ::wt::bc_elem(nbr[f + 6 * ec], Ne);
     if (en < 0) continue;
     const int fs = nbrf[f + 6 * ec];  // fn | ori << 3
     const int p = al == 0 ? j : i, q = al == 2 ? j : k;
@@ -584,5 +584,8 @@ int launch_curved4_background(const DevMesh& m, int kind, const double* p, doubl
     k_curved4_bg<float><<<blocks, 256, 0, s>>>(m.nn, m.coords, kind, p[0], p[1], t, (float*)ginv, (float*)gam);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
+
+// this file's bounds word (bounds-check build; 0 otherwise)
+WT_BOUNDS_TAKE(bounds_take_second)
 
 }  // namespace wt

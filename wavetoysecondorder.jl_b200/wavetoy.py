@@ -18,7 +18,9 @@ from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libwavetoy_b200.so")
+# WAVETOY_B200_LIB selects another build of the library, e.g. the bounds-check
+# variant libwavetoy_b200_bc.so (build.py --bounds-check)
+LIB_PATH = os.environ.get("WAVETOY_B200_LIB") or os.path.join(_HERE, "libwavetoy_b200.so")
 
 WT_F64, WT_F32 = 0, 1
 BC_DIRICHLET, BC_SOMMERFELD, BC_EXCISION, BC_FULL_DIRICHLET = 1, 2, 3, 4
@@ -115,6 +117,8 @@ def library():
         "wt_ctx_launch_count": [vp, C.POINTER(ll)], "wt_ctx_nonfinite": [vp, C.POINTER(i)],
         "wt_ctx_selftest_wait": [vp, i, ll],
         "wt_ctx_memory": [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)],
+        "wt_build_flags": [C.POINTER(i)], "wt_ctx_bounds_status": [vp, C.POINTER(C.c_uint)],
+        "wt_mesh_debug_set_table": [vp, i, ll, i, i],
         "wt_ctx_inject_alloc_failure": [vp, ll],
         "wt_mesh_create": [vp, C.POINTER(_MeshDesc), pvp],
         "wt_mesh_create_arrays": [vp, i, ll, vp, vp, vp, vp, vp, vp, i, pvp],
@@ -268,6 +272,13 @@ class Context:
         v = [C.c_longlong() for _ in range(3)]
         self.check(library().wt_ctx_memory(self.h, *[C.byref(x) for x in v]))
         return tuple(x.value for x in v)
+
+    def bounds_status(self) -> int:
+        """Read and clear the bounds word of the bounds-check build (bit 0: an element index
+        out of range, bit 1: a boundary slot); always 0 in the normal build."""
+        w = C.c_uint()
+        self.check(library().wt_ctx_bounds_status(self.h, C.byref(w)))
+        return w.value
 
     def inject_alloc_failure(self, after: int):
         """Make the device allocation `after` allocations from now fail once with
@@ -1253,6 +1264,25 @@ def state_from_f64(ws: "Workspace", Phi64, Pi64, Phi, Pi):
     ws.ctx.check(library().wt_state_set_f64(ws.ctx.h, ws.h, _ptr(Phi64), _ptr(Pi64), _ptr(Phi), _ptr(Pi)),
                  "state_from_f64")
     return Phi, Pi
+
+
+BUILD_BOUNDS_CHECK, BUILD_NVTX = 1, 2
+TABLE_FACE_SOURCE, TABLE_BOUNDARY_SLOT = 0, 1
+
+
+def build_flags() -> int:
+    """BUILD_* bits of the loaded library (wt_build_flags)."""
+    f = C.c_int()
+    if library().wt_build_flags(C.byref(f)) != 0:
+        raise WaveToyError(-1, "wt_build_flags")
+    return f.value
+
+
+def debug_set_table(mesh: "Mesh", table: int, e: int, f: int, value: int):
+    """Overwrite entry (e, f) of a mesh's device face-source or boundary-slot table
+    (bounds-check build only: wt_mesh_debug_set_table)."""
+    mesh.ctx.check(library().wt_mesh_debug_set_table(mesh.h, int(table), int(e), int(f), int(value)),
+                   "wt_mesh_debug_set_table")
 
 
 def checkpoint_save(ws: "Workspace", Phi, Pi):
