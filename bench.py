@@ -908,6 +908,18 @@ def main():
     ap.add_argument("--serve-chosen-only", action="store_true",
                     help="serve workload: only the compensated FP32 served form (a longer stream), with every k-th "
                          "request re-solved alone in FP64 (50 of them) as the accuracy check")
+    ap.add_argument("--config", default=None,
+                    help="JSON file of option values (keys: the option names, e.g. {\"workload\": \"serve\", "
+                         "\"rate\": 0.6}); options given on the command line take precedence")
+    first, _ = ap.parse_known_args()
+    if first.config:
+        with open(first.config) as f:
+            cfg = {k.replace("-", "_"): v for k, v in json.load(f).items()}
+        known = {a.dest for a in ap._actions}
+        bad = sorted(set(cfg) - known)
+        if bad:
+            ap.error(f"--config: unknown options {bad}")
+        ap.set_defaults(**cfg)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -680,6 +680,60 @@ int wt_serve_cost(const wt_serve_desc* desc, const wt_serve_request* req, double
 int wt_serve_queue_order(int order, double now, int count, const double* arrival, const double* service,
                          const double* work, int* perm);
 
+/* ---- evolve3d in one call ------------------------------------------------------
+ * The keyword set of evolve3d(formulation = :conservative; T, N, M, mesh_kind,
+ * background, ic, bc, eps_KO, t0, t1, Nt, cfl) (src/evolve.jl:1149-1166) as one
+ * descriptor, over this library's mesh, background and initial-data
+ * descriptors.  wt_evolve3d builds the mesh, coefficients and workspace,
+ * fills the initial state at t0, and integrates to t1 with the reference's
+ * time sampling (src/evolve.jl:1209-1213, 1311-1352):
+ *   dt = cfl * (smallest node spacing) / max_speed, and with eps_ko != 0 at
+ *   most 1.4 / (eps_ko mu); the samples are range(t0, t1, nt); before sample n
+ *   the solve takes RK4 steps of dt while its time is below ts[n], the time
+ *   accumulated in the mesh precision, and a step that would pass t1 is
+ *   shortened to end on t1 (the integrator's stop at the end of its span).
+ * At each sample it records the time reached, the energy (wt_energy) and the
+ * L2 distance (Hd-weighted with use_metric, else Hphys) of Phi to the initial
+ * data family at that time when ic_exact = 1 (ic = :exact), else the L2 norm
+ * of Phi.  The final state goes to Phi_host, Pi_host (nodes values of the mesh
+ * precision; wt_solve_nodes gives the count).  A non-finite state ends it with
+ * WT_ENONFINITE.  Every device object is released before it returns. */
+typedef struct {
+  int mesh_kind;              /* 0: analytic hex (mesh); WT_MESH_CUBED_CUBE / _INFLATED_CUBE / _RADIAL_SHELL (patch) */
+  wt_mesh_desc mesh;          /* mesh_kind 0 */
+  wt_patch_desc patch;        /* mesh_kind > 0 */
+  int precision;              /* T: WT_F64 or WT_F32 (overrides the mesh descriptors') */
+  wt_background_desc bg;
+  int ic_kind, nic;           /* wt_initial_state at t0 */
+  double ic[WT_SERVE_MAX_IC];
+  int ic_exact;               /* 1: the initial-data family is the exact solution (ic = :exact) */
+  wt_bc_desc bc;              /* data pointers must be NULL; all kinds 0: none (bc3d = nothing) */
+  int use_metric;             /* 1: curvilinear split form (the reference passes the metric bundle) */
+  double eps_ko;
+  double t0, t1;
+  int nt;                     /* samples, >= 1 */
+  double cfl, max_speed;
+} wt_solve_desc;
+typedef struct {
+  double dt;                  /* the step */
+  double dx;                  /* the smallest node spacing */
+  double mu;                  /* the Kreiss-Oliger spectral radius (0 without dissipation) */
+  long long steps;            /* RK4 steps taken, the shortened last one included */
+} wt_solve_info;
+/* why desc is not a valid solve ("" if it is), written to msg (host only, no device) */
+int wt_solve_desc_check(const wt_solve_desc* desc, char* msg, int msglen);
+/* nodes of the mesh desc describes (host only) */
+int wt_solve_nodes(const wt_solve_desc* desc, long long* nodes);
+/* The sampling schedule (host only): steps[n] = RK4 steps before sample n,
+ * after steps[n - 1]; the last step taken is shortened to dt_last (dt if no
+ * step is shortened); ts_actual[n] = the time at sample n.  precision: the
+ * type the time accumulates in. */
+int wt_solve_schedule(double t0, double t1, int nt, double dt, int precision, long long* steps, double* dt_last,
+                      double* ts_actual);
+/* Any of ts_actual, energy, l2 (nt values each), info may be NULL. */
+int wt_evolve3d(wt_ctx* ctx, const wt_solve_desc* desc, void* Phi_host, void* Pi_host, double* ts_actual,
+                double* energy, double* l2, wt_solve_info* info);
+
 #ifdef __cplusplus
 }
 #endif

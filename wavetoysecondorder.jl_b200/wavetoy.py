@@ -93,6 +93,18 @@ class _ServeRequest(C.Structure):
                 ("bc", _BcDesc)]
 
 
+class _SolveDesc(C.Structure):
+    _fields_ = [("mesh_kind", C.c_int), ("mesh", _MeshDesc), ("patch", _PatchDesc), ("precision", C.c_int),
+                ("bg", _BgDesc), ("ic_kind", C.c_int), ("nic", C.c_int), ("ic", C.c_double * SERVE_MAX_IC),
+                ("ic_exact", C.c_int), ("bc", _BcDesc), ("use_metric", C.c_int), ("eps_ko", C.c_double),
+                ("t0", C.c_double), ("t1", C.c_double), ("nt", C.c_int), ("cfl", C.c_double),
+                ("max_speed", C.c_double)]
+
+
+class _SolveInfo(C.Structure):
+    _fields_ = [("dt", C.c_double), ("dx", C.c_double), ("mu", C.c_double), ("steps", C.c_longlong)]
+
+
 class _ServeResult(C.Structure):
     _fields_ = [("precision", C.c_int), ("nodes", C.c_longlong), ("steps", C.c_int), ("dt", C.c_double),
                 ("arrival", C.c_double), ("admitted", C.c_double), ("finished", C.c_double)]
@@ -179,6 +191,10 @@ def library():
         "wt_serve_preempt": [vp, i],
         "wt_state_checkpoint_size": [vp, C.POINTER(ll)], "wt_state_checkpoint_save": [vp, vp, vp, vp, vp, ll],
         "wt_state_checkpoint_load": [vp, vp, vp, vp, vp, ll],
+        "wt_solve_desc_check": [C.POINTER(_SolveDesc), C.c_char_p, i],
+        "wt_solve_nodes": [C.POINTER(_SolveDesc), C.POINTER(ll)],
+        "wt_solve_schedule": [d, d, i, d, i, vp, C.POINTER(d), vp],
+        "wt_evolve3d": [vp, C.POINTER(_SolveDesc), vp, vp, vp, vp, vp, C.POINTER(_SolveInfo)],
         "wt_serve_info": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(d), C.POINTER(d)],
         "wt_serve_cost": [C.POINTER(_ServeDesc), C.POINTER(_ServeRequest), C.POINTER(d), C.POINTER(i)],
         "wt_serve_queue_order": [i, d, i, vp, vp, vp, vp],
@@ -648,6 +664,125 @@ def serve_desc(hbm_budget: float = 150e9, tick: int = 50, max_active: Optional[i
     d.keep_results = int(bool(keep_results))
     d.rate_f64, d.rate_f32 = float(rate_f64), float(rate_f32)
     return d
+
+
+# ---- evolve3d in one call (wt_solve_desc, wt_evolve3d) ------------------------------
+MESH_KINDS = {"cubical": 0, "cubed_cube": MESH_CUBED_CUBE, "inflated_cube": MESH_INFLATED_CUBE,
+              "radial_shell": MESH_RADIAL_SHELL}
+BG_KINDS = {"minkowski": BG_MINKOWSKI, "constant_shift": BG_CONSTANT_SHIFT, "adm_perturbed": BG_ADM_PERTURBED,
+            "radial_shift": BG_RADIAL_SHIFT, "gauge_wave": BG_GAUGE_WAVE, "sine_shift": BG_SINE_SHIFT}
+IC_KINDS = {"eigenmode_cartesian": IC_EIGENMODE_CARTESIAN, "gaussians": IC_GAUSSIANS,
+            "outgoing_pulse": IC_OUTGOING_PULSE, "plane_wave": IC_PLANE_WAVE, "eigenmode_radial": IC_EIGENMODE_RADIAL}
+
+
+def solve_desc(N: int = 4, M=8, *, T: int = WT_F64, mesh_kind: int = 0, x0: float = 0.0, x1: float = 1.0,
+               warp_A: float = 0.0, periodic: bool = False, outer_tag: int = SOMMERFELD_BDRY_TAG,
+               patch_params: Sequence[float] = (), inner_tag: int = 8, background: int = BG_MINKOWSKI,
+               bg_params: Sequence[float] = (), ic: int = IC_GAUSSIANS, ic_params: Sequence[float] = (),
+               ic_exact: bool = False, bc3d: Optional["BC3D"] = None, metric: bool = True, eps_KO: float = 0.0,
+               t0: float = 0.0, t1: float = 1.0, Nt: int = 200, cfl: float = 0.1,
+               max_speed: float = 1.0) -> _SolveDesc:
+    """wt_solve_desc: the keywords of evolve3d(formulation = :conservative; T, N, M, mesh_kind,
+    background, ic, bc, eps_KO, t0, t1, Nt, cfl) (src/evolve.jl:1149-1166) over this library's
+    mesh, background and initial-data descriptors (defaults as the reference's: N = 4, M = 8,
+    t1 = 1, Nt = 200, cfl = 1/10)."""
+    d = _SolveDesc()
+    d.mesh_kind, d.precision = int(mesh_kind), int(T)
+    if d.mesh_kind == 0:
+        Ms = (M, M, M) if isinstance(M, int) else tuple(M)
+        d.mesh.N = int(N)
+        for a in range(3):
+            d.mesh.M[a] = int(Ms[a])
+        d.mesh.x0, d.mesh.x1, d.mesh.warp_A = float(x0), float(x1), float(warp_A)
+        d.mesh.periodic, d.mesh.outer_tag = int(bool(periodic)), 0 if periodic else int(outer_tag)
+    else:
+        if not isinstance(M, int) or len(patch_params) > 3:
+            raise ValueError("patch meshes take one M and at most 3 parameters")
+        d.patch.kind, d.patch.N, d.patch.M = int(mesh_kind), int(N), int(M)
+        for k, v in enumerate(patch_params):
+            d.patch.p[k] = float(v)
+        d.patch.outer_tag, d.patch.inner_tag = int(outer_tag), int(inner_tag)
+    if len(bg_params) > 16 or len(ic_params) > SERVE_MAX_IC:
+        raise ValueError("too many background or initial-data parameters")
+    d.bg.kind = int(background)
+    for k, v in enumerate(bg_params):
+        d.bg.p[k] = float(v)
+    d.ic_kind, d.nic, d.ic_exact = int(ic), len(ic_params), int(bool(ic_exact))
+    for k, v in enumerate(ic_params):
+        d.ic[k] = float(v)
+    if bc3d is not None:
+        if any(g is not None for g in (bc3d.gPhi, bc3d.gPi, bc3d.gDx, bc3d.gDy, bc3d.gDz)):
+            raise ValueError("evolve3d takes no boundary data fields")
+        d.bc = bc3d.cstruct()
+    d.use_metric, d.eps_ko = int(bool(metric)), float(eps_KO)
+    d.t0, d.t1, d.nt, d.cfl, d.max_speed = float(t0), float(t1), int(Nt), float(cfl), float(max_speed)
+    return d
+
+
+def solve_config(cfg: dict) -> _SolveDesc:
+    """A wt_solve_desc from a JSON-style dict: the keyword names of solve_desc; kinds may be
+    given by name ("mesh_kind": "cubed_cube", "background": "adm_perturbed", "ic": "gaussians"),
+    T as "Float64" / "Float32", the boundary as "bc": {"kinds": [...], "sigma": 1, "excision_tag": 0}."""
+    kw = dict(cfg)
+    for key, table in (("mesh_kind", MESH_KINDS), ("background", BG_KINDS), ("ic", IC_KINDS)):
+        if isinstance(kw.get(key), str):
+            if kw[key] not in table:
+                raise ValueError(f"unknown {key} {kw[key]!r}: one of {sorted(table)}")
+            kw[key] = table[kw[key]]
+    if isinstance(kw.get("T"), str):
+        kw["T"] = {"Float64": WT_F64, "Float32": WT_F32}[kw["T"]]
+    if "bc" in kw:
+        b = kw.pop("bc")
+        kw["bc3d"] = make_bc3d(b["kinds"], sigma=b.get("sigma", 1.0), excision_tag=b.get("excision_tag", 0))
+    if "M" in kw and isinstance(kw["M"], list):
+        kw["M"] = tuple(kw["M"])
+    return solve_desc(**kw)
+
+
+def load_solve_config(path: str) -> _SolveDesc:
+    """solve_config of a JSON file."""
+    import json
+    with open(path) as f:
+        return solve_config(json.load(f))
+
+
+def solve_desc_check(desc: _SolveDesc) -> str:
+    """Why desc is not a valid solve ("" if it is); host only."""
+    buf = C.create_string_buffer(256)
+    library().wt_solve_desc_check(C.byref(desc), buf, 256)
+    return buf.value.decode()
+
+
+def solve_schedule(t0: float, t1: float, nt: int, dt: float, precision: int = WT_F64):
+    """(steps before each sample, the last step's length, the sample times) of evolve3d's
+    loop (wt_solve_schedule; host only)."""
+    import numpy as np
+    steps = np.zeros(max(int(nt), 1), dtype=np.int64)
+    ts = np.zeros(max(int(nt), 1))
+    last = C.c_double()
+    rc = library().wt_solve_schedule(float(t0), float(t1), int(nt), float(dt), int(precision), steps.ctypes.data,
+                                     C.byref(last), ts.ctypes.data)
+    if rc != 0:
+        raise WaveToyError(rc, "wt_solve_schedule: bad arguments")
+    return steps, last.value, ts
+
+
+def evolve3d(ctx: Context, desc: _SolveDesc) -> dict:
+    """evolve3d(formulation = :conservative; ...) (src/evolve.jl:1149-1366) in one call
+    (wt_evolve3d): the sample times reached, energy and l2_err per sample, the final
+    state (host arrays of the solve's precision), dt, dx, mu and the steps taken."""
+    import numpy as np
+    nn = C.c_longlong()
+    if library().wt_solve_nodes(C.byref(desc), C.byref(nn)) != 0:
+        raise WaveToyError(-1, "evolve3d: " + solve_desc_check(desc))
+    dt_ = np.float64 if desc.precision == WT_F64 else np.float32
+    Phi, Pi = np.empty(nn.value, dtype=dt_), np.empty(nn.value, dtype=dt_)
+    ts, E, L = (np.empty(desc.nt) for _ in range(3))
+    info = _SolveInfo()
+    ctx.check(library().wt_evolve3d(ctx.h, C.byref(desc), Phi.ctypes.data, Pi.ctypes.data, ts.ctypes.data,
+                                    E.ctypes.data, L.ctypes.data, C.byref(info)), "evolve3d")
+    return {"ts_actual": ts, "energy": E, "l2_err": L, "Phi_final": Phi, "Pi_final": Pi, "dt": info.dt,
+            "dx": info.dx, "mu": info.mu, "steps": info.steps}
 
 
 def serve_request(arrival: float, N: int, M, x0: float = 0.0, x1: float = 1.0, warp_A: float = 0.0,
