@@ -46,3 +46,17 @@ def ctx(wt):
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     return wt.Context(0)
+
+
+@pytest.fixture(autouse=True)
+def _bounds_words_clear(request):
+    """With the bounds-check library loaded (WAVETOY_B200_LIB=.../libwavetoy_b200_bc.so), every GPU
+    test must leave the bounds words clear: no kernel read a table index out of range."""
+    checked = None
+    if "gpu" in request.keywords and os.environ.get("WAVETOY_B200_LIB"):
+        wt = load_package()
+        if wt.build_flags() & wt.BUILD_BOUNDS_CHECK:
+            checked = request.getfixturevalue("ctx")
+    yield
+    if checked is not None:
+        assert checked.bounds_status() == 0, "a kernel read a table index out of range"
