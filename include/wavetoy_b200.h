@@ -730,9 +730,25 @@ int wt_solve_nodes(const wt_solve_desc* desc, long long* nodes);
  * type the time accumulates in. */
 int wt_solve_schedule(double t0, double t1, int nt, double dt, int precision, long long* steps, double* dt_last,
                       double* ts_actual);
-/* Any of ts_actual, energy, l2 (nt values each), info may be NULL. */
+/* The diagnostic 1-D slice evolve3d records (src/evolve.jl:104-123, 1322-1349):
+ * the nodes whose y and z lie strictly within atol of (y, z), in storage order,
+ * keeping the first node at each x (within atol), then sorted by x (stable).
+ * evolve3d takes atol = sqrt(eps(T)) and (y, z) = the mid-plane (x0 + x1) / 2. */
+typedef struct {
+  double y, z;          /* the line; NaN: the mid-plane of the mesh's extent */
+  long long capacity;   /* room in xs, and per sample in Phi and Pi */
+  long long count;      /* out: nodes on the line (nothing is written past capacity) */
+  long long* nodes;     /* out: their node indices (capacity; may be NULL) */
+  double* xs;           /* out: their x, ascending (capacity) */
+  double* Phi;          /* out: [sample][node], nt x capacity values, FP64 */
+  double* Pi;
+} wt_solve_slice;
+/* The slice selection on node-major coordinates xyz[3 * node + c] (host only). */
+int wt_slice_select(const double* xyz, long long nodes, double y, double z, double atol, long long capacity,
+                    long long* node_out, double* xs_out, long long* count);
+/* Any of ts_actual, energy, l2 (nt values each), slice, info may be NULL. */
 int wt_evolve3d(wt_ctx* ctx, const wt_solve_desc* desc, void* Phi_host, void* Pi_host, double* ts_actual,
-                double* energy, double* l2, wt_solve_info* info);
+                double* energy, double* l2, wt_solve_slice* slice, wt_solve_info* info);
 
 #ifdef __cplusplus
 }

@@ -62,6 +62,15 @@ def test_evolve3d_equals_the_manual_solve(wt, ctx, prec):
         E.append(wt.wave3d_energy(P, Q, c, ws, metric=True))
     assert np.array_equal(r["Phi_final"], P.cpu().numpy()) and np.array_equal(r["Pi_final"], Q.cpu().numpy())
     assert np.array_equal(r["energy"], np.array(E))
+    # the 1-D slice at the mid-plane: the rule of the reference's _build_slice_3d on the mesh
+    # coordinates, and at the last sample the final state's values there
+    xyz = g.get("coords").reshape(-1, 3)
+    atol = float(np.sqrt(np.finfo(np.float64 if prec == 0 else np.float32).eps))
+    nodes, xs = wt.slice_select(xyz, 0.5, 0.5, atol)
+    assert len(nodes) > 0 and np.array_equal(r["slice_nodes"], nodes) and np.array_equal(r["xs_line"], xs)
+    assert r["Phis"].shape == (len(nodes), 4)
+    assert np.array_equal(r["Phis"][:, -1], r["Phi_final"][nodes].astype(np.float64))
+    assert np.array_equal(r["Pis"][:, -1], r["Pi_final"][nodes].astype(np.float64))
 
 
 def test_evolve3d_exact_solution_and_energy(wt, ctx):

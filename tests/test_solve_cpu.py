@@ -105,3 +105,29 @@ def test_bench_config_rejects_unknown_options(tmp_path):
     r = subprocess.run([sys.executable, os.path.join(conftest.ROOT, "bench.py"), "--config", str(cfg)],
                        capture_output=True, text=True, timeout=120)
     assert r.returncode == 2 and "no_such_option" in r.stderr
+
+
+def build_slice_reference(x, y, z, yt, zt, atol):
+    """_build_slice_3d (src/evolve.jl:104-123), restated: nodes strictly within atol of the line,
+    in storage order, the first at each x kept, then sorted by x (stable)."""
+    idx, xs = [], []
+    for n in range(len(x)):
+        if abs(y[n] - yt) < atol and abs(z[n] - zt) < atol:
+            if not any(abs(x0 - x[n]) < atol for x0 in xs):
+                idx.append(n)
+                xs.append(x[n])
+    perm = sorted(range(len(xs)), key=lambda q: xs[q])
+    return [idx[q] for q in perm], [xs[q] for q in perm]
+
+
+@pytest.mark.parametrize("N,M,A,atol", [(6, 4, 0.05, 1.4901161193847656e-08), (8, 2, 0.0, 1.4901161193847656e-08),
+                                        (5, (4, 2, 2), 0.05, 3.4526698e-4)])
+def test_slice_selection_equals_the_reference_rule(wt, O, N, M, A, atol):
+    o = O.OracleMesh(N, M, A=A, outer_tag=7)
+    x, y, z = o.coords()
+    nodes, xs = wt.slice_select(np.stack([x, y, z], axis=1), 0.5, 0.5, atol)
+    rn, rx = build_slice_reference(x, y, z, 0.5, 0.5, atol)
+    assert list(nodes) == rn and list(xs) == rx
+    assert len(rn) > 0 and np.all(np.diff(xs) > 0)
+    raw = int(np.sum((np.abs(y - 0.5) < atol) & (np.abs(z - 0.5) < atol)))
+    assert raw > len(rn)                       # shared face nodes appear once

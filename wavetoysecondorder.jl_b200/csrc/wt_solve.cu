@@ -9,10 +9,14 @@
 #include "wavetoy_b200.h"
 #include "wt_common.cuh"
 
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
+#include <numeric>
 #include <string>
+#include <vector>
 
 namespace {
 
@@ -118,8 +122,34 @@ int wt_solve_schedule(double t0, double t1, int nt, double dt, int precision, lo
                              : schedule_t<double>(t0, t1, nt, dt, steps, dt_last, ts_actual);
 }
 
+int wt_slice_select(const double* xyz, long long nodes, double y, double z, double atol, long long capacity,
+                    long long* node_out, double* xs_out, long long* count) {
+  if (!xyz || nodes < 0 || !count || capacity < 0 || !(atol > 0)) return WT_EINVAL;
+  std::vector<long long> idx;
+  std::vector<double> xs;
+  for (long long n = 0; n < nodes; ++n) {  // storage order: node i fastest, then j, k, element
+    const double* p = xyz + 3 * n;
+    if (!(std::fabs(p[1] - y) < atol && std::fabs(p[2] - z) < atol)) continue;
+    bool isnew = true;
+    for (double x0 : xs)
+      if (std::fabs(x0 - p[0]) < atol) { isnew = false; break; }
+    if (!isnew) continue;
+    idx.push_back(n);
+    xs.push_back(p[0]);
+  }
+  std::vector<size_t> perm(xs.size());
+  std::iota(perm.begin(), perm.end(), 0);
+  std::stable_sort(perm.begin(), perm.end(), [&](size_t a, size_t b) { return xs[a] < xs[b]; });
+  *count = (long long)xs.size();
+  for (size_t q = 0; q < perm.size() && (long long)q < capacity; ++q) {
+    if (node_out) node_out[q] = idx[perm[q]];
+    if (xs_out) xs_out[q] = xs[perm[q]];
+  }
+  return 0;
+}
+
 int wt_evolve3d(wt_ctx* ctx, const wt_solve_desc* d, void* Phi_host, void* Pi_host, double* ts_actual,
-                double* energy, double* l2, wt_solve_info* info) {
+                double* energy, double* l2, wt_solve_slice* slice, wt_solve_info* info) {
   if (!ctx) return WT_EINVAL;
   wt::NvtxRange nv("wt_evolve3d");
   const std::string why = check_desc(d);
@@ -166,6 +196,23 @@ int wt_evolve3d(wt_ctx* ctx, const wt_solve_desc* d, void* Phi_host, void* Pi_ho
     const double lim = prec == WT_F32 ? (double)(1.4f / ((float)d->eps_ko * (float)mu)) : 1.4 / (d->eps_ko * mu);
     dt = std::fmin(dt, lim);
   }
+  // the 1-D slice (src/evolve.jl:1322-1334): atol = sqrt(eps(T)), the mid-plane by default
+  std::vector<int64_t> snodes;
+  if (slice) {
+    if (slice->capacity < 0 || (slice->capacity > 0 && (!slice->xs || !slice->Phi || !slice->Pi)))
+      return wt::ctx_fail(ctx, WT_EINVAL, "wt_evolve3d: slice buffers missing for its capacity");
+    const double mid = d->mesh_kind == 0 ? 0.5 * (d->mesh.x0 + d->mesh.x1) : 0.0;  // patch meshes are centred
+    const double ys = std::isnan(slice->y) ? mid : slice->y, zs = std::isnan(slice->z) ? mid : slice->z;
+    const double atol = prec == WT_F32 ? (double)std::sqrt(FLT_EPSILON) : std::sqrt(DBL_EPSILON);
+    std::vector<double> xyz(3 * (size_t)nn);
+    WT_TRY_SOLVE(wt_mesh_get(S.mesh, "coords", xyz.data()));
+    std::vector<long long> sel((size_t)std::max<long long>(slice->capacity, 0));
+    WT_TRY_SOLVE(wt_slice_select(xyz.data(), nn, ys, zs, atol, slice->capacity, sel.data(), slice->xs,
+                                 &slice->count));
+    if (slice->nodes)
+      for (long long q = 0; q < std::min(slice->count, slice->capacity); ++q) slice->nodes[q] = sel[q];
+    if (slice->count <= slice->capacity) snodes.assign(sel.begin(), sel.begin() + slice->count);
+  }
   // no boundary conditions (bc3d = nothing, e.g. a periodic mesh) when every kind is 0
   bool any_kind = false;
   for (int f = 0; f < 6; ++f) any_kind = any_kind || d->bc.kinds[f] != 0;
@@ -198,6 +245,11 @@ int wt_evolve3d(wt_ctx* ctx, const wt_solve_desc* d, void* Phi_host, void* Pi_ho
                                                          std::to_string(n));
     if (ts_actual) ts_actual[n] = ts[n];
     if (energy) WT_TRY_SOLVE(wt_energy(ctx, S.ws, S.coef, Phi, Pi, d->use_metric, &energy[n]));
+    if (!snodes.empty()) {
+      const int cnt = (int)snodes.size();
+      WT_TRY_SOLVE(wt_gather_nodes(ctx, S.mesh, Phi, snodes.data(), cnt, slice->Phi + n * slice->capacity));
+      WT_TRY_SOLVE(wt_gather_nodes(ctx, S.mesh, Pi, snodes.data(), cnt, slice->Pi + n * slice->capacity));
+    }
     if (l2) {
       if (d->ic_exact) WT_TRY_SOLVE(wt_initial_data(ctx, S.mesh, d->ic_kind, icp, d->nic, ts[n], S.ref, nullptr));
       WT_TRY_SOLVE(wt_l2_diff(ctx, S.ws, Phi, d->ic_exact ? S.ref : nullptr, d->use_metric, &l2[n]));

@@ -101,6 +101,11 @@ class _SolveDesc(C.Structure):
                 ("max_speed", C.c_double)]
 
 
+class _SolveSlice(C.Structure):
+    _fields_ = [("y", C.c_double), ("z", C.c_double), ("capacity", C.c_longlong), ("count", C.c_longlong),
+                ("nodes", C.c_void_p), ("xs", C.c_void_p), ("Phi", C.c_void_p), ("Pi", C.c_void_p)]
+
+
 class _SolveInfo(C.Structure):
     _fields_ = [("dt", C.c_double), ("dx", C.c_double), ("mu", C.c_double), ("steps", C.c_longlong)]
 
@@ -194,7 +199,9 @@ def library():
         "wt_solve_desc_check": [C.POINTER(_SolveDesc), C.c_char_p, i],
         "wt_solve_nodes": [C.POINTER(_SolveDesc), C.POINTER(ll)],
         "wt_solve_schedule": [d, d, i, d, i, vp, C.POINTER(d), vp],
-        "wt_evolve3d": [vp, C.POINTER(_SolveDesc), vp, vp, vp, vp, vp, C.POINTER(_SolveInfo)],
+        "wt_evolve3d": [vp, C.POINTER(_SolveDesc), vp, vp, vp, vp, vp, C.POINTER(_SolveSlice),
+                        C.POINTER(_SolveInfo)],
+        "wt_slice_select": [vp, ll, d, d, d, ll, vp, vp, C.POINTER(ll)],
         "wt_serve_info": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(d), C.POINTER(d)],
         "wt_serve_cost": [C.POINTER(_ServeDesc), C.POINTER(_ServeRequest), C.POINTER(d), C.POINTER(i)],
         "wt_serve_queue_order": [i, d, i, vp, vp, vp, vp],
@@ -767,10 +774,27 @@ def solve_schedule(t0: float, t1: float, nt: int, dt: float, precision: int = WT
     return steps, last.value, ts
 
 
-def evolve3d(ctx: Context, desc: _SolveDesc) -> dict:
+def slice_select(xyz, y: float, z: float, atol: float):
+    """The 1-D slice rule of evolve3d (_build_slice_3d, src/evolve.jl:104-123) on node-major
+    coordinates (wt_slice_select; host only): (node indices, x) sorted by x."""
+    import numpy as np
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    cnt = C.c_longlong()
+    nodes = np.zeros(len(xyz), dtype=np.int64)
+    xs = np.zeros(len(xyz))
+    rc = library().wt_slice_select(xyz.ctypes.data, len(xyz), float(y), float(z), float(atol), len(xyz),
+                                   nodes.ctypes.data, xs.ctypes.data, C.byref(cnt))
+    if rc != 0:
+        raise WaveToyError(rc, "wt_slice_select: bad arguments")
+    return nodes[:cnt.value], xs[:cnt.value]
+
+
+def evolve3d(ctx: Context, desc: _SolveDesc, slice_yz=(math.nan, math.nan), slice_capacity: int = 4096) -> dict:
     """evolve3d(formulation = :conservative; ...) (src/evolve.jl:1149-1366) in one call
-    (wt_evolve3d): the sample times reached, energy and l2_err per sample, the final
-    state (host arrays of the solve's precision), dt, dx, mu and the steps taken."""
+    (wt_evolve3d): the sample times reached, energy and l2_err per sample, the 1-D slice
+    (xs_line, Phis and Pis as [node, sample] like the reference's), the final state (host
+    arrays of the solve's precision), dt, dx, mu and the steps taken.  slice_yz: the
+    line (NaN: the mid-plane); slice_capacity: room for its nodes."""
     import numpy as np
     nn = C.c_longlong()
     if library().wt_solve_nodes(C.byref(desc), C.byref(nn)) != 0:
@@ -778,11 +802,20 @@ def evolve3d(ctx: Context, desc: _SolveDesc) -> dict:
     dt_ = np.float64 if desc.precision == WT_F64 else np.float32
     Phi, Pi = np.empty(nn.value, dtype=dt_), np.empty(nn.value, dtype=dt_)
     ts, E, L = (np.empty(desc.nt) for _ in range(3))
+    cap = int(slice_capacity)
+    nodes, xs = np.zeros(cap, dtype=np.int64), np.zeros(cap)
+    Ps, Qs = np.zeros((desc.nt, cap)), np.zeros((desc.nt, cap))
+    sl = _SolveSlice(float(slice_yz[0]), float(slice_yz[1]), cap, 0, nodes.ctypes.data, xs.ctypes.data,
+                     Ps.ctypes.data, Qs.ctypes.data)
     info = _SolveInfo()
     ctx.check(library().wt_evolve3d(ctx.h, C.byref(desc), Phi.ctypes.data, Pi.ctypes.data, ts.ctypes.data,
-                                    E.ctypes.data, L.ctypes.data, C.byref(info)), "evolve3d")
-    return {"ts_actual": ts, "energy": E, "l2_err": L, "Phi_final": Phi, "Pi_final": Pi, "dt": info.dt,
-            "dx": info.dx, "mu": info.mu, "steps": info.steps}
+                                    E.ctypes.data, L.ctypes.data, C.byref(sl), C.byref(info)), "evolve3d")
+    k = sl.count
+    if k > cap:
+        raise WaveToyError(-1, f"evolve3d: the slice has {k} nodes; raise slice_capacity")
+    return {"ts_actual": ts, "energy": E, "l2_err": L, "xs_line": xs[:k], "slice_nodes": nodes[:k],
+            "Phis": Ps[:, :k].T.copy(), "Pis": Qs[:, :k].T.copy(), "Phi_final": Phi, "Pi_final": Pi,
+            "dt": info.dt, "dx": info.dx, "mu": info.mu, "steps": info.steps}
 
 
 def serve_request(arrival: float, N: int, M, x0: float = 0.0, x1: float = 1.0, warp_A: float = 0.0,
