@@ -500,10 +500,22 @@ int wt_halo_face_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, i
  * (src/evolve.jl:43-48; evolve3d runs them with adaptive = false):
  * WT_ERK_RK4 (the fused low-storage RK4 above) and WT_ERK_TSIT5 (Tsitouras
  * 2011, fifth order).  Time-dependent backgrounds are re-sampled at every
- * stage time.  Vern7 (N >= 7 in the reference) is not provided. */
+ * stage time.  Vern7 (N >= 7 in the reference) has no built-in tableau: a caller
+ * passes its published coefficients to wt_step_erk_curved_tableau. */
 enum { WT_ERK_RK4 = 0, WT_ERK_TSIT5 = 1 };
+#define WT_ERK_MAX_STAGES 16
 int wt_step_erk_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
                        int method, double eps_ko, const wt_bc_desc* bc, int use_metric);
+/* The same with the caller's explicit Butcher tableau: stages s (1..WT_ERK_MAX_STAGES),
+ * c[s], A[s*s] row major with A[i*s + j] = 0 for j >= i, b[s], all finite
+ * (WT_EINVAL otherwise).  It runs any explicit method with its published
+ * coefficients, e.g. Verner's 7(6) pair, which pick_integrator_first_order
+ * chooses for N >= 7 (Vern7, 10 stages; its 7th-order weights).  The workspace
+ * holds 2 s state-sized slope buffers.  No counterpart in the reference as an
+ * entry point (OrdinaryDiffEq takes the method as a type). */
+int wt_step_erk_curved_tableau(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
+                               int nsteps, int stages, const double* c, const double* A, const double* b,
+                               double eps_ko, const wt_bc_desc* bc, int use_metric);
 /* The method's Butcher tableau (host only): stages, c[s], A[s*s] (row major), b[s]. */
 int wt_erk_tableau(int method, int* stages, double* c, double* A, double* b);
 /* RK4 of the SIPG system as first-order (u, ut):

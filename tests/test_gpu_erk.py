@@ -60,3 +60,39 @@ def test_erk_rk4_is_the_fused_step(wt, ctx):
     assert torch.equal(P, P2) and torch.equal(Q, Q2)
     with pytest.raises(wt.WaveToyError):
         wt.step_erk_curved(P, Q, c, ws, 1e-3, 1, 7)
+
+
+def test_caller_tableau(wt, ctx, O):
+    """wt_step_erk_curved_tableau: Tsit5's own tableau gives the built-in method's bits; a
+    12-stage method (three RK4 steps of dt/3 as one tableau, more slopes than the built-in
+    methods use) equals the oracle's RK4 at dt/3; a non-explicit or oversized tableau is
+    refused."""
+    import torch
+    g = wt.Mesh.uniform_hex(ctx, 6, 2, outer_tag=7, warp_A=0.05)
+    o = O.OracleMesh(6, 2, A=0.05, outer_tag=7)
+    p = wt.workloads.adm_params(5)
+    c, co = wt.sample_background3d(g, wt.BG_ADM_PERTURBED, p), o.background(2, p)
+    ws = wt.make_wave3d_workspace(g)
+    x, y, z = o.coords()
+    P0 = np.sin(2 * np.pi * x) * np.cos(np.pi * (y - z))
+    Q0 = 0.3 * np.cos(np.pi * (x + 2 * z))
+    dt = 0.2 * o.min_spacing() / wt.workloads.max_speed(p)
+    bc = wt.make_bc3d([2] * 6)
+    P1, Q1 = torch.tensor(P0, device="cuda"), torch.tensor(Q0, device="cuda")
+    P2, Q2 = P1.clone(), Q1.clone()
+    wt.step_erk_curved(P1, Q1, c, ws, dt, 4, wt.ERK_TSIT5, bc3d=bc, metric=True)
+    wt.step_erk_curved_tableau(P2, Q2, c, ws, dt, 4, *wt.erk_tableau(wt.ERK_TSIT5), bc3d=bc, metric=True)
+    assert torch.equal(P1, P2) and torch.equal(Q1, Q2)
+    C2, A2, B2 = wt.composed_tableau(*wt.erk_tableau(wt.ERK_RK4), 3)
+    P3, Q3 = torch.tensor(P0, device="cuda"), torch.tensor(Q0, device="cuda")
+    wt.step_erk_curved_tableau(P3, Q3, c, ws, dt, 5, C2, A2, B2, bc3d=bc, metric=True)
+    Po, Qo = o.evolve_curved(co, P0, Q0, dt / 3, 15, bc=O.make_bc([2] * 6), use_metric=True)
+    assert rel(P3.cpu().numpy(), Po) < 1e-12 and rel(Q3.cpu().numpy(), Qo) < 1e-12
+    bad = A2.copy()
+    bad[3, 5] = 0.1                                   # an implicit coupling
+    with pytest.raises(wt.WaveToyError):
+        wt.step_erk_curved_tableau(P3, Q3, c, ws, dt, 1, C2, bad, B2, bc3d=bc, metric=True)
+    C4, A4, B4 = wt.composed_tableau(*wt.erk_tableau(wt.ERK_RK4), 5)   # 20 stages
+    with pytest.raises(wt.WaveToyError):
+        wt.step_erk_curved_tableau(P3, Q3, c, ws, dt, 1, C4, A4, B4, bc3d=bc, metric=True)
+    assert not ctx.nonfinite()

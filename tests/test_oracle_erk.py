@@ -47,3 +47,15 @@ def test_time_convergence(O, method, order, td):
     ref = run(96)
     e1, e2 = np.linalg.norm(run(6) - ref), np.linalg.norm(run(12) - ref)
     assert e1 / e2 > 2 ** order * 0.8, (e1, e2, e1 / e2)
+
+
+def test_composed_tableau_keeps_the_order(wt):
+    """Three RK4 steps of dt/3 written as one 12-stage explicit method: its Butcher
+    tableau meets the order conditions up to 4 (the composition has RK4's order), it
+    is strictly lower triangular, and its stage times are the substep times."""
+    c, A, b = wt.erk_tableau(wt.ERK_RK4)
+    C2, A2, B2 = wt.composed_tableau(c, A, b, 3)
+    assert len(C2) == 12 <= wt.ERK_MAX_STAGES
+    assert np.all(np.triu(A2) == 0)
+    assert max(abs(r) for r in order_conditions(C2, A2, B2)[:8]) < 1e-15
+    assert np.allclose(A2.sum(axis=1), C2, atol=1e-15)

@@ -95,7 +95,8 @@ struct wt_ws {
   void* compP = nullptr;
   void* compQ = nullptr;
   const void* comp_for[2] = {nullptr, nullptr};
-  void* erk = nullptr;    // explicit RK stage slopes: 2 x 8 x nn (Phi slopes, then Pi slopes)
+  void* erk = nullptr;    // explicit RK stage slopes: 2 x erk_stages x nn (Phi slopes, then Pi slopes)
+  int erk_stages = 0;
   long long flux_block = 0;  // values per element block of F as the last fused stage wrote it (halo copies)
   int flux_lay = 0;          // and its element-block layout (wt::n8_flux_layout; 0: node order)
   int halo_cp = 0;        // the last fused stage ran the compensated FP32 form (its halo adds Phit)
@@ -1676,9 +1677,9 @@ static int step_curved_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* P
 // step evaluates six stages.
 struct ErkTableau {
   int s = 0;
-  double c[8] = {};
-  double A[8][8] = {};
-  double b[8] = {};
+  double c[WT_ERK_MAX_STAGES] = {};
+  double A[WT_ERK_MAX_STAGES][WT_ERK_MAX_STAGES] = {};
+  double b[WT_ERK_MAX_STAGES] = {};
 };
 
 static const ErkTableau* erk_tableau(int method) {
@@ -1718,10 +1719,10 @@ static int step_erk_once(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi,
   const wt::DevMesh& m = ws->mesh->m;
   cudaStream_t s = ctx->stream;
   const size_t nb = (size_t)m.nn * rsize(m.precision);
-  char* base = static_cast<char*>(ws->erk);
-  const void* kP[8];
-  const void* kQ[8];
-  for (int j = 0; j < 8; ++j) { kP[j] = base + j * nb; kQ[j] = base + (8 + j) * nb; }
+  char* base = static_cast<char*>(ws->erk);  // the Phi slopes of the T.s stages, then the Pi slopes
+  const void* kP[WT_ERK_MAX_STAGES];
+  const void* kQ[WT_ERK_MAX_STAGES];
+  for (int j = 0; j < T.s; ++j) { kP[j] = base + j * nb; kQ[j] = base + (T.s + j) * nb; }
   int last = T.s - 1;
   while (last > 0 && T.b[last] == 0.0) --last;  // stages past the last nonzero weight do not contribute
   for (int st = 0; st <= last; ++st) {
@@ -2006,14 +2007,12 @@ int wt_halo_face_copy(wt_ctx* ctx, wt_ws* ws, void* Phi, int stage, int layer, i
                                        buf, pack, ctx->stream), "wt_halo_face_copy");
 }
 
-int wt_step_erk_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
-                       int method, double eps_ko, const wt_bc_desc* bc, int use_metric) {
-  wt::NvtxRange nvtx_("wt_step_erk_curved");
-  WT_TRY(check_ws(ctx, ws));
-  const ErkTableau* T = erk_tableau(method);
-  if (!T) return fail(ctx, WT_EINVAL, "wt_step_erk_curved: unknown method " + std::to_string(method));
-  if (method == WT_ERK_RK4)  // the fused low-storage stages
-    return wt_step_rk4_curved(ctx, ws, coef, Phi, Pi, dt, nsteps, eps_ko, bc, use_metric);
+}  // extern "C"
+
+// nsteps steps of the explicit tableau T (wt_step_erk_curved and _tableau)
+static int erk_run(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
+                   const ErkTableau& Tab, double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  const ErkTableau* T = &Tab;
   if (!coef || !Phi || !Pi) return fail(ctx, WT_EINVAL, "wt_step_erk_curved: NULL argument");
   if (nsteps < 0) return fail(ctx, WT_EINVAL, "nsteps must be >= 0");
   if (!(dt > 0) || !std::isfinite(dt)) return fail(ctx, WT_EINVAL, "dt must be positive and finite");
@@ -2021,7 +2020,13 @@ int wt_step_erk_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, v
   WT_TRY(make_bc(ctx, bc, use_metric, b));
   WT_TRY(ws_step_buffers(ws));
   const wt::DevMesh& m = ws->mesh->m;
-  WT_TRY(ensure(ws, &ws->erk, 16 * (size_t)m.nn * rsize(m.precision)));
+  if (ws->erk_stages < T->s) {  // room for this tableau's slopes
+    dfree(ctx, ws->erk);
+    ws->erk = nullptr;
+    ws->erk_stages = 0;
+    WT_TRY(dalloc(ctx, &ws->erk, 2 * (size_t)T->s * (size_t)m.nn * rsize(m.precision), nullptr));
+    ws->erk_stages = T->s;
+  }
   if (eps_ko != 0.0) WT_TRY(ensure_mu(ws));
   if (coef->td) WT_TRY(need_setup_geometry(coef->mesh, "wt_step_erk_curved (time-dependent background)"));
   int rc = 0;
@@ -2033,6 +2038,44 @@ int wt_step_erk_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, v
   }
   if (!rc && coef->td) coef->t += nsteps * dt;
   return rc;
+}
+
+extern "C" {
+
+int wt_step_erk_curved(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt, int nsteps,
+                       int method, double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  wt::NvtxRange nvtx_("wt_step_erk_curved");
+  WT_TRY(check_ws(ctx, ws));
+  const ErkTableau* T = erk_tableau(method);
+  if (!T) return fail(ctx, WT_EINVAL, "wt_step_erk_curved: unknown method " + std::to_string(method));
+  if (method == WT_ERK_RK4)  // the fused low-storage stages
+    return wt_step_rk4_curved(ctx, ws, coef, Phi, Pi, dt, nsteps, eps_ko, bc, use_metric);
+  return erk_run(ctx, ws, coef, Phi, Pi, dt, nsteps, *T, eps_ko, bc, use_metric);
+}
+
+int wt_step_erk_curved_tableau(wt_ctx* ctx, wt_ws* ws, const wt_coef* coef, void* Phi, void* Pi, double dt,
+                               int nsteps, int stages, const double* c, const double* A, const double* b,
+                               double eps_ko, const wt_bc_desc* bc, int use_metric) {
+  wt::NvtxRange nvtx_("wt_step_erk_curved_tableau");
+  WT_TRY(check_ws(ctx, ws));
+  if (stages < 1 || stages > WT_ERK_MAX_STAGES || !c || !A || !b)
+    return fail(ctx, WT_EINVAL, "wt_step_erk_curved_tableau: stages must be in 1..16, c, A, b not NULL");
+  auto T = std::make_unique<ErkTableau>();
+  T->s = stages;
+  for (int i = 0; i < stages; ++i) {
+    T->c[i] = c[i];
+    T->b[i] = b[i];
+    if (!std::isfinite(c[i]) || !std::isfinite(b[i]))
+      return fail(ctx, WT_EINVAL, "wt_step_erk_curved_tableau: c and b must be finite");
+    for (int j = 0; j < stages; ++j) {
+      const double a = A[i * stages + j];
+      if (!std::isfinite(a) || (j >= i && a != 0.0))
+        return fail(ctx, WT_EINVAL, "wt_step_erk_curved_tableau: A must be finite and strictly lower triangular "
+                                    "(an explicit method)");
+      T->A[i][j] = a;
+    }
+  }
+  return erk_run(ctx, ws, coef, Phi, Pi, dt, nsteps, *T, eps_ko, bc, use_metric);
 }
 
 int wt_erk_tableau(int method, int* stages, double* c, double* A, double* b) {

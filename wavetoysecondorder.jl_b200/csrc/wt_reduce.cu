@@ -89,8 +89,8 @@ __global__ void k_axpy(long long n, real* __restrict__ y, real a, const real* __
 // Explicit RK stage/step combination: out = y + dt * sum_j a_j k_j (j < nk),
 // summed in j order.
 struct ErkSum {
-  const void* k[8];
-  double a[8];
+  const void* k[WT_ERK_MAX_STAGES];
+  double a[WT_ERK_MAX_STAGES];
   int nk;
 };
 template <typename real>
@@ -104,10 +104,10 @@ __global__ void k_erk_combine(long long n, double dt, const real* __restrict__ y
 
 int launch_erk_combine(long long n, int precision, double dt, const void* y, void* out, int nk, const void* const* k,
                        const double* a, cudaStream_t s) {
-  if (nk < 0 || nk > 8) return -1;
+  if (nk < 0 || nk > WT_ERK_MAX_STAGES) return -1;
   ErkSum S;
   S.nk = nk;
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < WT_ERK_MAX_STAGES; ++j) {
     S.k[j] = j < nk ? k[j] : nullptr;
     S.a[j] = j < nk ? a[j] : 0.0;
   }

@@ -32,6 +32,7 @@ BG_MINKOWSKI, BG_CONSTANT_SHIFT, BG_ADM_PERTURBED, BG_RADIAL_SHIFT = 0, 1, 2, 3
 BG_GAUGE_WAVE, BG_SINE_SHIFT = 4, 5
 # fixed-step explicit Runge-Kutta methods (pick_integrator_first_order)
 ERK_RK4, ERK_TSIT5 = 0, 1
+ERK_MAX_STAGES = 16
 IC_EIGENMODE_CARTESIAN, IC_GAUSSIANS, IC_OUTGOING_PULSE, IC_PLANE_WAVE, IC_EIGENMODE_RADIAL = 0, 1, 2, 3, 4
 # precision forms of an FP32 mesh (n = 8 contractions): CUDA cores, split BF16 three-term / two-term
 FP32_CUDA_CORES, FP32_BF16X3, FP32_BF16X2, FP32_COMPENSATED = 0, 1, 2, 3
@@ -172,6 +173,7 @@ def library():
         "wt_l2_diff": [vp, vp, vp, vp, i, C.POINTER(d)],
         "wt_step_rk4_curved": [vp, vp, vp, vp, vp, d, i, d, C.POINTER(_BcDesc), i],
         "wt_step_erk_curved": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i],
+        "wt_step_erk_curved_tableau": [vp, vp, vp, vp, vp, d, i, i, vp, vp, vp, d, C.POINTER(_BcDesc), i],
         "wt_erk_tableau": [i, C.POINTER(i), vp, vp, vp],
         "wt_step_rk4_sipg": [vp, vp, vp, vp, d, i, C.POINTER(C.c_double * 6), d, d, d],
         "wt_evolve_curved_host": [vp, vp, vp, vp, vp, d, i, i, d, C.POINTER(_BcDesc), i, vp],
@@ -1261,6 +1263,39 @@ def step_erk_curved(Phi, Pi, coef: Coef, ws: Workspace, dt: float, nsteps: int, 
     ws.ctx.check(library().wt_step_erk_curved(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt), int(nsteps),
                                               int(method), float(eps_KO), p, int(metric)), "step_erk_curved")
     return Phi, Pi
+
+
+def step_erk_curved_tableau(Phi, Pi, coef: Coef, ws: Workspace, dt: float, nsteps: int, c, A, b,
+                            eps_KO: float = 0.0, bc3d: Optional[BC3D] = None, metric: bool = False):
+    """nsteps fixed-dt steps of the caller's explicit Butcher tableau (c, A, b) with at most
+    ERK_MAX_STAGES stages (wt_step_erk_curved_tableau), e.g. Vern7 with its published
+    coefficients."""
+    import numpy as np
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    A = np.ascontiguousarray(A, dtype=np.float64).reshape(len(c), len(c))
+    p, keep = _bcptr(bc3d)
+    ws.ctx.check(library().wt_step_erk_curved_tableau(ws.ctx.h, ws.h, coef.h, _ptr(Phi), _ptr(Pi), float(dt),
+                                                      int(nsteps), len(c), c.ctypes.data, A.ctypes.data,
+                                                      b.ctypes.data, float(eps_KO), p, int(metric)),
+                 "step_erk_curved_tableau")
+    return Phi, Pi
+
+
+def composed_tableau(c, A, b, m: int):
+    """The explicit tableau of m consecutive steps of (c, A, b), each of length dt / m, as one
+    method with m s stages."""
+    import numpy as np
+    c, b, A = np.asarray(c, float), np.asarray(b, float), np.asarray(A, float).reshape(len(c), len(c))
+    s = len(c)
+    C2, B2, A2 = np.zeros(m * s), np.zeros(m * s), np.zeros((m * s, m * s))
+    for p in range(m):
+        C2[p * s:(p + 1) * s] = (p + c) / m
+        B2[p * s:(p + 1) * s] = b / m
+        A2[p * s:(p + 1) * s, p * s:(p + 1) * s] = A / m
+        for q in range(p):
+            A2[p * s:(p + 1) * s, q * s:(q + 1) * s] = b / m
+    return C2, A2, B2
 
 
 def erk_tableau(method: int):
