@@ -739,7 +739,7 @@ int wt_solve_nodes(const wt_solve_desc* desc, long long* nodes);
 /* The sampling schedule (host only): steps[n] = RK4 steps before sample n,
  * after steps[n - 1]; the last step taken is shortened to dt_last (dt if no
  * step is shortened); ts_actual[n] = the time at sample n.  precision: the
- * type the time accumulates in. */
+ * type the time accumulates in.  WT_EINVAL above 1e9 steps. */
 int wt_solve_schedule(double t0, double t1, int nt, double dt, int precision, long long* steps, double* dt_last,
                       double* ts_actual);
 /* The diagnostic 1-D slice evolve3d records (src/evolve.jl:104-123, 1322-1349):

@@ -46,7 +46,7 @@ template <typename T>
 int schedule_t(double t0d, double t1d, int nt, double dtd, long long* steps, double* dt_last, double* ts_actual) {
   const T t0 = (T)t0d, t1 = (T)t1d, dt = (T)dtd;
   if (!(dt > 0)) return WT_EINVAL;
-  if ((t1d - t0d) / dtd > 1e12) return WT_EINVAL;  // more steps than any solve takes
+  if ((t1d - t0d) / dtd > 1e9) return WT_EINVAL;  // more steps than any solve takes (a host loop of them)
   T t = t0, last = dt;
   for (int n = 0; n < nt; ++n) {
     // the range's end points are exact; the points between them rounded once to T
