@@ -630,7 +630,15 @@ typedef struct {
   int auto_fp32_max_steps;   /* threshold of WT_SERVE_AUTO */
   int keep_results;          /* keep each finished request's final state (wt_serve_result_state) */
   double rate_f64, rate_f32; /* DOF-updates/s of the service estimate; <= 0: 3e9 and 6e9 */
+  int preempt;               /* 1: preemptive admission (below); 0: none */
 } wt_serve_desc;
+/* Preemptive admission (preempt = 1): when the request at the head of the
+ * queue cannot start (budget, max_active or fill_nodes), running requests with
+ * at least twice its remaining work (nodes x steps left) are preempted
+ * (wt_serve_preempt), the one with the most remaining work first, until it
+ * can -- but only if preempting the eligible ones makes room at all.  A request
+ * is preempted this way at most once, so no two requests trade places forever;
+ * a preempted request resumes from its host checkpoint, to the same bits. */
 typedef struct {
   double arrival;            /* seconds on the server's clock */
   wt_mesh_desc mesh;         /* analytic mesh; precision is chosen by the server */

@@ -223,3 +223,37 @@ def test_checkpoint_roundtrip_is_bitwise(wt, ctx, prec):
         assert not torch.equal(P3, P)
     with pytest.raises(wt.WaveToyError):
         wt.checkpoint_load(ws2, P2, Q2, ck[:-1])
+
+
+@pytest.mark.parametrize("preempt", [False, True])
+def test_preemptive_admission(wt, ctx, preempt):
+    """One slot (max_active = 1): a long request runs, a short one arrives.  With preemptive
+    admission the long one is checkpointed, the short one runs and finishes first, and the
+    long one resumes to the bits of its uninterrupted run; without it the short one waits."""
+    import torch
+    S = wt.serve
+    long_q, short_q = _requests(wt)[0], _requests(wt)[1]
+    long_q = dataclasses.replace(long_q, steps=60)
+    short_q = dataclasses.replace(short_q, steps=8)
+    alone = {}
+    for q in (long_q, short_q):
+        eng = wt.ServeEngine(ctx, wt.serve_desc(**_engine(wt, wt.WT_F64)))
+        rid = eng.submit(S.native_request(q))
+        eng.run()
+        alone[q.rid] = tuple(t.clone() for t in eng.state(rid))
+        eng.close()
+    eng = wt.ServeEngine(ctx, wt.serve_desc(**_engine(wt, wt.WT_F64, max_active=1, preempt=preempt)))
+    rl = eng.submit(S.native_request(long_q))
+    eng.poll()
+    eng.poll()
+    rs = eng.submit(S.native_request(short_q))
+    eng.run()
+    L, Sh = eng.result(rl), eng.result(rs)
+    if preempt:
+        assert eng.status(rl)["preemptions"] == 1 and Sh["finished"] < L["finished"]
+    else:
+        assert eng.status(rl)["preemptions"] == 0 and Sh["admitted"] >= L["finished"]
+    for rid, q in ((rl, long_q), (rs, short_q)):
+        P, Q = eng.state(rid)
+        assert torch.equal(P, alone[q.rid][0]) and torch.equal(Q, alone[q.rid][1]), (preempt, rid)
+    eng.close()

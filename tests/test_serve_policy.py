@@ -79,6 +79,11 @@ def test_request_validation():
     wt.serve_cost(d, wt.serve_request(**good, bg_kind=wt.BG_GAUGE_WAVE, bg_params=(0.1, 1.0, 0.0)))
     with pytest.raises(wt.WaveToyError):
         wt.serve_cost(wt.serve_desc(tick=0), wt.serve_request(**good))
+    wt.serve_cost(wt.serve_desc(preempt=True), wt.serve_request(**good))
+    bad_desc = wt.serve_desc(preempt=True)
+    bad_desc.preempt = 2
+    with pytest.raises(wt.WaveToyError):
+        wt.serve_cost(bad_desc, wt.serve_request(**good))
     with pytest.raises(ValueError):
         wt.serve_request(**good, ic_params=[0.0] * 200)
 

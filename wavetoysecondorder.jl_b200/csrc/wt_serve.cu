@@ -84,6 +84,7 @@ int check_desc(const wt_serve_desc* d) {
   if (d->order < WT_SERVE_HRRN || d->order > WT_SERVE_FIFO) return -1;
   if (d->precision != WT_F64 && d->precision != WT_F32 && d->precision != WT_SERVE_AUTO) return -1;
   if (d->fp32_form < WT_FP32_CUDA_CORES || d->fp32_form > WT_FP32_COMPENSATED) return -1;
+  if (d->preempt != 0 && d->preempt != 1) return -1;
   return 0;
 }
 
@@ -192,6 +193,44 @@ struct wt_server {
     return 0;
   }
 
+  // whether request r could start with `u` bytes used, `na` requests running on `run` nodes
+  bool fits(const Req& r, double u, int na, long long run) const {
+    if (u + r.cost > d.hbm_budget) return false;
+    if (d.max_active > 0 && na >= d.max_active) return false;
+    if (d.fill_nodes > 0 && na > 0 && run >= d.fill_nodes) return false;
+    return true;
+  }
+  long long running_nodes() const {
+    long long run = 0;
+    for (int k : active) run += reqs[k].nodes;
+    return run;
+  }
+
+  // preemptive admission for the queue head r: the running requests with at least twice
+  // its remaining work, most work first, if preempting them lets r start
+  int make_room(const Req& r) {
+    std::vector<int> cand;
+    for (int k : active)
+      if (reqs[k].preemptions == 0 && (double)reqs[k].nodes * reqs[k].left >= 2.0 * (double)r.nodes * r.left)
+        cand.push_back(k);
+    std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) {
+      return (double)reqs[a].nodes * reqs[a].left > (double)reqs[b].nodes * reqs[b].left;
+    });
+    double u = used;
+    int na = (int)active.size();
+    long long run = running_nodes();
+    size_t n = 0;
+    while (!fits(r, u, na, run) && n < cand.size()) {
+      const Req& v = reqs[cand[n++]];
+      u -= v.cost;
+      na -= 1;
+      run -= v.nodes;
+    }
+    if (!fits(r, u, na, run)) return 0;  // no room even without them: preempt nothing
+    for (size_t k = 0; k < n; ++k) WT_TRY_SERVE(preempt(cand[k]));
+    return 0;
+  }
+
   int preempt(int rid) {
     Req& r = reqs[rid];
     long long nb = 0;
@@ -256,13 +295,8 @@ struct wt_server {
     // admission from the head of the queue
     while (!queue.empty()) {
       Req& r = reqs[queue.front()];
-      if (used + r.cost > d.hbm_budget) break;
-      if (d.max_active > 0 && (int)active.size() >= d.max_active) break;
-      if (d.fill_nodes > 0 && !active.empty()) {
-        long long running = 0;
-        for (int k : active) running += reqs[k].nodes;
-        if (running >= d.fill_nodes) break;
-      }
+      if (d.preempt && !fits(r, used, (int)active.size(), running_nodes())) WT_TRY_SERVE(make_room(r));
+      if (!fits(r, used, (int)active.size(), running_nodes())) break;
       used += r.cost;
       peak = std::max(peak, used);
       const int rid = queue.front();
@@ -320,7 +354,7 @@ int wt_serve_create(wt_ctx* ctx, const wt_serve_desc* desc, wt_server** out) {
   *out = nullptr;
   if (check_desc(desc))
     return wt::ctx_fail(ctx, WT_EINVAL, "wt_serve_create: bad descriptor (budget > 0, tick >= 1, "
-                                        "max_active >= 0, fill_nodes >= 0, order, precision, fp32_form)");
+                                        "max_active >= 0, fill_nodes >= 0, order, precision, fp32_form, preempt 0 or 1)");
   auto* s = new wt_server();
   s->ctx = ctx;
   s->d = *desc;

@@ -85,7 +85,8 @@ SERVE_MAX_IC = 128
 class _ServeDesc(C.Structure):
     _fields_ = [("hbm_budget", C.c_double), ("tick", C.c_int), ("max_active", C.c_int), ("fill_nodes", C.c_longlong),
                 ("order", C.c_int), ("precision", C.c_int), ("fp32_form", C.c_int), ("auto_fp32_max_steps", C.c_int),
-                ("keep_results", C.c_int), ("rate_f64", C.c_double), ("rate_f32", C.c_double)]
+                ("keep_results", C.c_int), ("rate_f64", C.c_double), ("rate_f32", C.c_double),
+                ("preempt", C.c_int)]
 
 
 class _ServeRequest(C.Structure):
@@ -661,8 +662,9 @@ class Batch(_Child):
 def serve_desc(hbm_budget: float = 150e9, tick: int = 50, max_active: Optional[int] = None,
                fill_nodes: Optional[int] = 8_000_000, order: int = SERVE_HRRN, precision: int = WT_F32,
                fp32_form: int = FP32_COMPENSATED, auto_fp32_max_steps: int = 2000, keep_results: bool = False,
-               rate_f64: float = 0.0, rate_f32: float = 0.0) -> _ServeDesc:
-    """wt_serve_desc: admission and stepping policy of a ServeEngine (None: no limit)."""
+               rate_f64: float = 0.0, rate_f32: float = 0.0, preempt: bool = False) -> _ServeDesc:
+    """wt_serve_desc: admission and stepping policy of a ServeEngine (None: no limit; preempt:
+    preemptive admission of short requests, wt_serve_desc.preempt)."""
     d = _ServeDesc()
     d.hbm_budget = float(hbm_budget)
     d.tick = int(tick)
@@ -672,6 +674,7 @@ def serve_desc(hbm_budget: float = 150e9, tick: int = 50, max_active: Optional[i
     d.auto_fp32_max_steps = int(auto_fp32_max_steps)
     d.keep_results = int(bool(keep_results))
     d.rate_f64, d.rate_f32 = float(rate_f64), float(rate_f32)
+    d.preempt = int(bool(preempt))
     return d
 
 
