@@ -809,21 +809,32 @@ def run_serve(args):
     out = {}
     # the served forms admit by response ratio (Server's default); the plain form runs
     # one request at a time in arrival order
-    forms = (("plain_fp64_per_request", wt.WT_F64, 1, "fifo"),
-             ("served_fp32_compensated", wt.WT_F32, None, "hrrn"),
-             ("served_fp64", wt.WT_F64, None, "hrrn"))
+    forms = (("plain_fp64_per_request", wt.WT_F64, 1, "fifo", False),
+             ("served_fp32_compensated", wt.WT_F32, None, "hrrn", False),
+             ("served_fp64", wt.WT_F64, None, "hrrn", False))
     if args.serve_chosen_only:   # a longer stream: the chosen form alone, FP64 checks on a sample
         forms = forms[1:2]
+    if args.preempt:   # the chosen form without and with preemptive admission, compared bit for bit
+        forms = forms[1:2] + (("served_fp32_compensated_preemptive", wt.WT_F32, None, "hrrn", True),)
     ref = {}
-    for name, prec, max_active, order in forms:
+    first = {}
+    for name, prec, max_active, order, preempt in forms:
         server = S.Server(ctx, precision=prec, hbm_budget=150e9, tick=50, max_active=max_active, keep_results=True,
-                          order=order, fp32_form=wt.FP32_COMPENSATED)
+                          order=order, fp32_form=wt.FP32_COMPENSATED, preempt=preempt)
         t0 = time.perf_counter()
         res = server.run(reqs)
         makespan = time.perf_counter() - t0
         out[name] = S.summary(res, makespan)
         if name == "plain_fp64_per_request":
             ref = {r.rid: torch.cat([r.Phi, r.Pi]).double() for r in res}
+        elif args.preempt:
+            # preemption changes when a request runs, not what it computes
+            if not preempt:
+                first = {r.rid: torch.cat([r.Phi, r.Pi]) for r in res}
+            else:
+                out[name]["bitwise_equal_to_non_preemptive"] = int(
+                    sum(bool(torch.equal(torch.cat([r.Phi, r.Pi]), first[r.rid])) for r in res))
+                out[name]["preempted_requests"] = int(sum(r.preemptions > 0 for r in res))
         elif args.serve_chosen_only:
             # every k-th request solved again alone in FP64 (the same set-up and steps)
             k = max(1, len(res) // 50)
@@ -905,6 +916,9 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=300, help="batch workload: RK4 steps per solve")
     ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
     ap.add_argument("--rate", type=float, default=1.5, help="serve workload: Poisson arrival rate (1/s)")
+    ap.add_argument("--preempt", action="store_true",
+                    help="serve workload: the chosen form without and with preemptive admission (results compared "
+                         "bit for bit, p50/p99 of both)")
     ap.add_argument("--serve-chosen-only", action="store_true",
                     help="serve workload: only the compensated FP32 served form (a longer stream), with every k-th "
                          "request re-solved alone in FP64 (50 of them) as the accuracy check")

@@ -108,5 +108,5 @@ def test_native_request_describes_build_solve():
     # the Python face of the engine charges what the engine's own estimate says
     srv = S.Server.__new__(S.Server)
     srv.budget, srv.tick, srv.max_active, srv.fill_nodes, srv.order = 1e12, 50, None, None, "hrrn"
-    srv.precision, srv.fp32_form, srv.keep = S.AUTO, wt.FP32_CUDA_CORES, False
+    srv.precision, srv.fp32_form, srv.keep, srv.preempt = S.AUTO, wt.FP32_CUDA_CORES, False, False
     assert srv._cost(q) == q.nodes * (300 + 272)      # 77 steps <= the FP32 limit: FP32, n = 6

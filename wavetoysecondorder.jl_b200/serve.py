@@ -52,6 +52,7 @@ class Result:
     dt: float
     Phi: Optional[object] = None   # final state (device tensors) when keep_results
     Pi: Optional[object] = None
+    preemptions: int = 0           # times the request was preempted (preemptive admission)
 
     @property
     def latency(self) -> float:
@@ -125,7 +126,7 @@ class Server:
 
     def __init__(self, ctx, precision: int = wt.WT_F32, hbm_budget: float = 150e9, tick: int = 50,
                  max_active: Optional[int] = None, fp32_form: int = wt.FP32_COMPENSATED, keep_results: bool = False,
-                 fill_nodes: Optional[int] = 8_000_000, order: str = "hrrn"):
+                 fill_nodes: Optional[int] = 8_000_000, order: str = "hrrn", preempt: bool = False):
         """fill_nodes: admit further requests only while the running ones hold fewer
         nodes than this (about what keeps the GPU busy); beyond it, new requests
         wait, so large requests are not slowed down by sharing the GPU with many
@@ -135,7 +136,9 @@ class Server:
         service time estimated from the request's DOF-updates: short requests go
         ahead under a backlog, and a long one's priority grows while it waits),
         "sjf" (least work first; long requests can wait until the backlog
-        clears) or "fifo" (arrival order)."""
+        clears) or "fifo" (arrival order).  preempt: preemptive admission -- a
+        request that blocks a much shorter one is checkpointed to host memory and
+        resumes later (wt_serve_desc.preempt)."""
         if order not in ORDERS:
             raise ValueError("order must be 'hrrn', 'sjf' or 'fifo'")
         self.order = order
@@ -148,10 +151,11 @@ class Server:
         self.fp32_form = fp32_form
         self.keep = keep_results
         self.peak_used = 0.0
+        self.preempt = bool(preempt)
 
     def desc(self):
         return wt.serve_desc(self.budget, self.tick, self.max_active, self.fill_nodes, ORDERS[self.order],
-                             self.precision, self.fp32_form, AUTO_FP32_MAX_STEPS, self.keep)
+                             self.precision, self.fp32_form, AUTO_FP32_MAX_STEPS, self.keep, preempt=self.preempt)
 
     def _cost(self, req: Request) -> float:
         """Estimated device bytes of a request (the engine's own estimate)."""
@@ -173,7 +177,7 @@ class Server:
                 x = eng.result(rid)
                 Phi, Pi = eng.state(rid) if self.keep else (None, None)
                 results.append(Result(req.rid, req.arrival, x["admitted"], x["finished"], x["nodes"], x["steps"],
-                                      x["dt"], Phi, Pi))
+                                      x["dt"], Phi, Pi, eng.status(rid)["preemptions"]))
             torch.cuda.synchronize(self.ctx.device)
         finally:
             eng.close()
