@@ -699,6 +699,14 @@ int wt_serve_cost(const wt_serve_desc* desc, const wt_serve_request* req, double
  * (nodes x steps) per request, listed in submission order. */
 int wt_serve_queue_order(int order, double now, int count, const double* arrival, const double* service,
                          const double* work, int* perm);
+/* The requests preemptive admission would preempt for a head request (host only,
+ * no device): count running requests (nodes, steps left, estimated bytes, times
+ * preempted), the bytes in use and the head's nodes, steps left and bytes.
+ * victims (count entries of room) gets their indices in preemption order,
+ * *nvictims their number (0: preempt nothing). */
+int wt_serve_preempt_choice(const wt_serve_desc* desc, double used, int count, const long long* nodes,
+                            const int* steps_left, const double* cost, const int* preemptions, long long head_nodes,
+                            int head_steps_left, double head_cost, int* victims, int* nvictims);
 
 /* ---- evolve3d in one call ------------------------------------------------------
  * The keyword set of evolve3d(formulation = :conservative; T, N, M, mesh_kind,

@@ -1,9 +1,12 @@
 """Host logic of the native request server (wt_serve_*), on the CPU: the
 admission order of waiting requests (highest response ratio next, least work
 first, arrival order; ties by arrival, then submission) against a restatement
-of the three policies, and the per-request device-byte estimate and precision
-choice.  No device is touched."""
+of the three policies, the per-request device-byte estimate and precision
+choice, and the victims of preemptive admission against a restatement of
+that rule.  No device is touched."""
 import random
+
+import numpy as np
 
 import pytest
 
@@ -110,3 +113,44 @@ def test_native_request_describes_build_solve():
     srv.budget, srv.tick, srv.max_active, srv.fill_nodes, srv.order = 1e12, 50, None, None, "hrrn"
     srv.precision, srv.fp32_form, srv.keep, srv.preempt = S.AUTO, wt.FP32_CUDA_CORES, False, False
     assert srv._cost(q) == q.nodes * (300 + 272)      # 77 steps <= the FP32 limit: FP32, n = 6
+
+
+def preempt_choice_reference(budget, max_active, fill_nodes, used, nodes, left, cost, pre, hn, hl, hc):
+    """Preemptive admission's victim rule, restated: running requests never preempted with at least
+    twice the head's remaining work, most work first, as many as make room -- none if all do not."""
+    def fits(u, na, run):
+        return (u + hc <= budget and (max_active == 0 or na < max_active)
+                and (fill_nodes == 0 or na == 0 or run < fill_nodes))
+    work = [n * l for n, l in zip(nodes, left)]
+    cand = sorted([k for k in range(len(nodes)) if pre[k] == 0 and work[k] >= 2.0 * hn * hl],
+                  key=lambda k: -work[k])
+    u, na, run, chosen = used, len(nodes), sum(nodes), []
+    for k in cand:
+        if fits(u, na, run):
+            break
+        u, na, run = u - cost[k], na - 1, run - nodes[k]
+        chosen.append(k)
+    return chosen if fits(u, na, run) else []
+
+
+def test_preempt_choice_equals_the_rule():
+    wt = load_package()
+    rng = np.random.default_rng(11)
+    picked = 0
+    for _ in range(400):
+        n = int(rng.integers(0, 7))
+        nodes = [int(v) for v in rng.integers(1_000, 2_000_000, n)]
+        left = [int(v) for v in rng.integers(1, 2000, n)]
+        cost = [v * 600.0 for v in nodes]
+        pre = [int(v) for v in rng.integers(0, 2, n)]
+        budget = float(rng.uniform(1e9, 6e9))
+        max_active = int(rng.integers(0, 5))
+        fill = int(rng.choice([0, 1_000_000, 4_000_000]))
+        used = float(sum(cost))
+        hn, hl = int(rng.integers(1_000, 500_000)), int(rng.integers(1, 400))
+        d = wt.serve_desc(hbm_budget=budget, max_active=max_active or None, fill_nodes=fill or None, preempt=True)
+        got = wt.serve_preempt_choice(d, used, nodes, left, cost, pre, hn, hl, hn * 600.0)
+        want = preempt_choice_reference(budget, max_active, fill, used, nodes, left, cost, pre, hn, hl, hn * 600.0)
+        assert got == want
+        picked += bool(got)
+    assert picked > 20

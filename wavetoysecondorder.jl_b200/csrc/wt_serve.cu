@@ -102,6 +102,42 @@ std::string check_request(const wt_serve_request* q) {
   return "";
 }
 
+// whether a request of `cost` bytes could start with `u` bytes used and `na` requests
+// running on `run` nodes, under desc's limits
+bool fits_desc(const wt_serve_desc& d, double cost, double u, int na, long long run) {
+  if (u + cost > d.hbm_budget) return false;
+  if (d.max_active > 0 && na >= d.max_active) return false;
+  if (d.fill_nodes > 0 && na > 0 && run >= d.fill_nodes) return false;
+  return true;
+}
+
+// The victims of preemptive admission for a head request (head_work = nodes x steps
+// left): the running requests never preempted before with at least twice its remaining
+// work, most work first, as many as it takes to make room -- none if even all of them
+// do not.  Indices into the running lists.
+std::vector<int> choose_victims(const wt_serve_desc& d, double used, const std::vector<long long>& nodes,
+                                const std::vector<double>& work, const std::vector<double>& cost,
+                                const std::vector<int>& preemptions, double head_cost, double head_work) {
+  std::vector<int> cand;
+  for (size_t k = 0; k < nodes.size(); ++k)
+    if (preemptions[k] == 0 && work[k] >= 2.0 * head_work) cand.push_back((int)k);
+  std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) { return work[a] > work[b]; });
+  double u = used;
+  int na = (int)nodes.size();
+  long long run = 0;
+  for (long long v : nodes) run += v;
+  size_t n = 0;
+  while (!fits_desc(d, head_cost, u, na, run) && n < cand.size()) {
+    u -= cost[cand[n]];
+    na -= 1;
+    run -= nodes[cand[n]];
+    ++n;
+  }
+  if (!fits_desc(d, head_cost, u, na, run)) return {};
+  cand.resize(n);
+  return cand;
+}
+
 #define WT_TRY_SERVE(x)      \
   do {                       \
     int _rc = (x);           \
@@ -194,12 +230,7 @@ struct wt_server {
   }
 
   // whether request r could start with `u` bytes used, `na` requests running on `run` nodes
-  bool fits(const Req& r, double u, int na, long long run) const {
-    if (u + r.cost > d.hbm_budget) return false;
-    if (d.max_active > 0 && na >= d.max_active) return false;
-    if (d.fill_nodes > 0 && na > 0 && run >= d.fill_nodes) return false;
-    return true;
-  }
+  bool fits(const Req& r, double u, int na, long long run) const { return fits_desc(d, r.cost, u, na, run); }
   long long running_nodes() const {
     long long run = 0;
     for (int k : active) run += reqs[k].nodes;
@@ -209,25 +240,18 @@ struct wt_server {
   // preemptive admission for the queue head r: the running requests with at least twice
   // its remaining work, most work first, if preempting them lets r start
   int make_room(const Req& r) {
-    std::vector<int> cand;
-    for (int k : active)
-      if (reqs[k].preemptions == 0 && (double)reqs[k].nodes * reqs[k].left >= 2.0 * (double)r.nodes * r.left)
-        cand.push_back(k);
-    std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) {
-      return (double)reqs[a].nodes * reqs[a].left > (double)reqs[b].nodes * reqs[b].left;
-    });
-    double u = used;
-    int na = (int)active.size();
-    long long run = running_nodes();
-    size_t n = 0;
-    while (!fits(r, u, na, run) && n < cand.size()) {
-      const Req& v = reqs[cand[n++]];
-      u -= v.cost;
-      na -= 1;
-      run -= v.nodes;
+    std::vector<long long> nodes;
+    std::vector<double> work, cost;
+    std::vector<int> pre;
+    for (int k : active) {
+      nodes.push_back(reqs[k].nodes);
+      work.push_back((double)reqs[k].nodes * reqs[k].left);
+      cost.push_back(reqs[k].cost);
+      pre.push_back(reqs[k].preemptions);
     }
-    if (!fits(r, u, na, run)) return 0;  // no room even without them: preempt nothing
-    for (size_t k = 0; k < n; ++k) WT_TRY_SERVE(preempt(cand[k]));
+    const std::vector<int> running = active;  // preempt() edits active
+    for (int k : choose_victims(d, used, nodes, work, cost, pre, r.cost, (double)r.nodes * r.left))
+      WT_TRY_SERVE(preempt(running[k]));
     return 0;
   }
 
@@ -500,6 +524,22 @@ int wt_serve_info(const wt_server* s, int* waiting, int* active, int* done, doub
   if (done) *done = s->done;
   if (used_bytes) *used_bytes = s->used;
   if (peak_bytes) *peak_bytes = s->peak;
+  return 0;
+}
+
+int wt_serve_preempt_choice(const wt_serve_desc* desc, double used, int count, const long long* nodes,
+                            const int* steps_left, const double* cost, const int* preemptions, long long head_nodes,
+                            int head_steps_left, double head_cost, int* victims, int* nvictims) {
+  if (check_desc(desc) || count < 0 || !nvictims) return WT_EINVAL;
+  if (count > 0 && (!nodes || !steps_left || !cost || !preemptions || !victims)) return WT_EINVAL;
+  std::vector<long long> nv(nodes, nodes + count);
+  std::vector<double> work(count), cv(cost, cost + count);
+  std::vector<int> pre(preemptions, preemptions + count);
+  for (int k = 0; k < count; ++k) work[k] = (double)nodes[k] * steps_left[k];
+  const std::vector<int> v =
+      choose_victims(*desc, used, nv, work, cv, pre, head_cost, (double)head_nodes * head_steps_left);
+  std::copy(v.begin(), v.end(), victims);
+  *nvictims = (int)v.size();
   return 0;
 }
 

@@ -208,6 +208,7 @@ def library():
         "wt_serve_info": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(d), C.POINTER(d)],
         "wt_serve_cost": [C.POINTER(_ServeDesc), C.POINTER(_ServeRequest), C.POINTER(d), C.POINTER(i)],
         "wt_serve_queue_order": [i, d, i, vp, vp, vp, vp],
+        "wt_serve_preempt_choice": [C.POINTER(_ServeDesc), d, i, vp, vp, vp, vp, ll, i, d, vp, C.POINTER(i)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -861,6 +862,26 @@ def serve_cost(desc: _ServeDesc, req: _ServeRequest):
     if rc != 0:
         raise WaveToyError(rc, "wt_serve_cost: bad descriptor or request")
     return b.value, p.value
+
+
+def serve_preempt_choice(desc: _ServeDesc, used: float, nodes, steps_left, cost, preemptions, head_nodes: int,
+                         head_steps_left: int, head_cost: float):
+    """The running requests (indices) that preemptive admission would preempt for the head request,
+    in order (wt_serve_preempt_choice; host only)."""
+    import numpy as np
+    n = len(nodes)
+    nodes = np.ascontiguousarray(nodes, dtype=np.int64)
+    left = np.ascontiguousarray(steps_left, dtype=np.int32)
+    cost = np.ascontiguousarray(cost, dtype=np.float64)
+    pre = np.ascontiguousarray(preemptions, dtype=np.int32)
+    out = np.zeros(max(n, 1), dtype=np.int32)
+    cnt = C.c_int()
+    rc = library().wt_serve_preempt_choice(C.byref(desc), float(used), n, nodes.ctypes.data, left.ctypes.data,
+                                           cost.ctypes.data, pre.ctypes.data, int(head_nodes), int(head_steps_left),
+                                           float(head_cost), out.ctypes.data, C.byref(cnt))
+    if rc != 0:
+        raise WaveToyError(rc, "wt_serve_preempt_choice: bad arguments")
+    return [int(v) for v in out[:cnt.value]]
 
 
 def serve_queue_order(order: int, now: float, arrival, service, work):
