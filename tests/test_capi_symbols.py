@@ -28,6 +28,18 @@ def test_library_exports_every_declared_symbol(wt):
     assert not missing, missing
 
 
+def test_bounds_check_library_exports_every_symbol_and_says_so(wt):
+    """The debug variant (build.py --bounds-check) has the same ABI; wt_build_flags (host only)
+    tells the two builds apart."""
+    wt.build.build(bounds_check=True)
+    for path, want in ((wt.LIB_PATH, wt.BUILD_NVTX), (wt.build.LIB_BC, wt.BUILD_NVTX | wt.BUILD_BOUNDS_CHECK)):
+        lib = ctypes.CDLL(path)
+        missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+        assert not missing, (path, missing)
+        flags = ctypes.c_int()
+        assert lib.wt_build_flags(ctypes.byref(flags)) == 0 and flags.value == want, path
+
+
 def test_python_mirror_binds_every_symbol(wt):
     lib = wt.library()
     for n in declared_symbols():
