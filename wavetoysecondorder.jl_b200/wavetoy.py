@@ -1354,14 +1354,11 @@ def gather_nodes(field, nodes, mesh: Mesh):
 
 
 def slice_nodes(mesh: Mesh, y_target: float, z_target: float, atol: float = 1.4901161193847656e-08):
-    """The 1-D diagnostic slice of evolve3d (_build_slice_3d): nodes with y, z within atol
-    of (y_target, z_target), sorted by x.  Returns (node indices, x).  Reads the set-up
-    coordinates once."""
-    import numpy as np
-    xyz = mesh.get("coords").reshape(-1, 3)
-    sel = np.nonzero((np.abs(xyz[:, 1] - y_target) <= atol) & (np.abs(xyz[:, 2] - z_target) <= atol))[0]
-    order = np.argsort(xyz[sel, 0], kind="stable")
-    return sel[order], xyz[sel[order], 0]
+    """The 1-D diagnostic slice of evolve3d (_build_slice_3d, src/evolve.jl:104-123): nodes with
+    y, z strictly within atol of (y_target, z_target), the first node at each x (a node shared
+    by two elements appears once), sorted by x (wt_slice_select).  Returns (node indices, x).
+    Reads the set-up coordinates once."""
+    return slice_select(mesh.get("coords"), y_target, z_target, atol)
 
 
 def snapshot_save(path: str, Phi, Pi, mesh: Mesh, t: float = 0.0):
