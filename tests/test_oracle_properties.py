@@ -344,3 +344,25 @@ def test_lapse_weighted_energy_is_conserved_without_shift(O, wt):
     # the oracle's weighted energy is that norm
     Ea = 0.5 * np.sum(Hd * al * (Pi ** 2 / sg + sg * np.sum(g * Kg, axis=0)))
     assert abs(m.energy(coef, Phi, Pi, use_metric=True, lapse=True) - Ea) < 1e-13 * Ea
+
+
+@pytest.mark.parametrize("N", [4, 5])
+def test_sommerfeld_faces_absorb_an_outgoing_pulse(O, N):
+    """The reference's absorption check (test/sommerfeld_tests.jl:132-154: an outgoing pulse
+    loses >= 95 % of its SIPG energy through Sommerfeld faces by t = 1.5, tau = 1.5 (N-1)^2),
+    on the unit cube, where this SIPG path runs (the reference runs it on the inflated cube).
+    With Dirichlet faces instead, the energy stays (the pulse is reflected)."""
+    tau = 1.5 * (N - 1) ** 2
+    ratio = {}
+    for tag in (7, 1):
+        o = O.OracleMesh(N, 4, A=0.0, outer_tag=tag)
+        x, y, z = o.coords()
+        u, v = O.ic_outgoing_pulse(x, y, z, 0.0, 1.0, 0.2, 0.07, 0.5, 0.5, 0.5)
+        dt = 0.2 * o.min_spacing()
+        ue, ve = o.evolve_sipg(u, v, dt, int(np.ceil(1.5 / dt)), tau=tau)
+        assert np.all(np.isfinite(ue))
+        if tag == 7:
+            assert np.abs(ue).max() < 1.0                # no blow-up; the initial peak is about 5.3
+        ratio[tag] = o.energy_sipg(ue, ve, tau) / o.energy_sipg(u, v, tau)
+    assert ratio[7] < 0.05
+    assert ratio[1] > 0.95
