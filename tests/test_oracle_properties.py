@@ -348,10 +348,11 @@ def test_lapse_weighted_energy_is_conserved_without_shift(O, wt):
 
 @pytest.mark.parametrize("N", [4, 5])
 def test_sommerfeld_faces_absorb_an_outgoing_pulse(O, N):
-    """The reference's absorption check (test/sommerfeld_tests.jl:132-154: an outgoing pulse
-    loses >= 95 % of its SIPG energy through Sommerfeld faces by t = 1.5, tau = 1.5 (N-1)^2),
-    on the unit cube, where this SIPG path runs (the reference runs it on the inflated cube).
-    With Dirichlet faces instead, the energy stays (the pulse is reflected)."""
+    """The reference's absorption checks (test/sommerfeld_tests.jl:132-176: an outgoing pulse
+    loses >= 95 % of its SIPG energy through Sommerfeld faces by t = 1.5, tau = 1.5 (N-1)^2,
+    and BGT-1 leaves a smaller residual than BGT-0), on the unit cube, where this SIPG path
+    runs (the reference runs them on the inflated cube).  With Dirichlet faces instead, the
+    energy stays (the pulse is reflected)."""
     tau = 1.5 * (N - 1) ** 2
     ratio = {}
     for tag in (7, 1):
@@ -366,3 +367,11 @@ def test_sommerfeld_faces_absorb_an_outgoing_pulse(O, N):
         ratio[tag] = o.energy_sipg(ue, ve, tau) / o.energy_sipg(u, v, tau)
     assert ratio[7] < 0.05
     assert ratio[1] > 0.95
+    # T3 (test/sommerfeld_tests.jl:155-176): BGT-1's +u/R term (R = 0.5, the faces' distance
+    # from the pulse centre) leaves under 0.7 of BGT-0's largest residual value
+    o = O.OracleMesh(N, 4, A=0.0, outer_tag=7)
+    x, y, z = o.coords()
+    u, v = O.ic_outgoing_pulse(x, y, z, 0.0, 1.0, 0.2, 0.07, 0.5, 0.5, 0.5)
+    dt = 0.2 * o.min_spacing()
+    mx = {R: np.abs(o.evolve_sipg(u, v, dt, int(np.ceil(1.5 / dt)), tau=tau, R=R)[0]).max() for R in (np.inf, 0.5)}
+    assert mx[0.5] < 0.7 * mx[np.inf]
