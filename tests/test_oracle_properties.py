@@ -288,6 +288,26 @@ def test_lap_strong_cons_H_symmetric(O):
     assert np.linalg.eigvalsh(0.5 * (HL + HL.T)).max() < 1e-10
 
 
+def test_lap_strong_cons_constants_and_rayleigh_convergence(O):
+    """The periodic conservative strong Laplacian (test/wave_lap_strong_mesh_tests.jl:45-135):
+    a constant is in its kernel, and the H_phys-weighted Rayleigh quotient of
+    sin(2 pi x) sin(2 pi y) sin(2 pi z) converges to the eigenvalue 3 (2 pi)^2 at N = 4 with
+    error ratios of at least 5, 50 and 10 from M = 1 to 2, 4 and 8, ending below 1e-3."""
+    m = O.OracleMesh(3, 2, periodic=True)
+    assert np.abs(m.lap_strong_cons(np.ones(m.nn), 0.5)).max() < 1e-12
+    lam = 3 * (2 * np.pi) ** 2
+    errs = []
+    for M in (1, 2, 4, 8):
+        m = O.OracleMesh(4, M, periodic=True)
+        x, y, z = m.coords()
+        u = np.sin(2 * np.pi * x) * np.sin(2 * np.pi * y) * np.sin(2 * np.pi * z)
+        Hp = m.get("Hphys")
+        errs.append(abs(-np.dot(u, Hp * m.lap_strong_cons(u, 1.0 / M)) / np.dot(u, Hp * u) - lam))
+    assert all(e > 0 for e in errs)
+    assert errs[1] < errs[0] / 5 and errs[2] < errs[1] / 50 and errs[3] < errs[2] / 10
+    assert errs[3] < 1e-3
+
+
 def test_classify_face(O):
     """classify_face3d flat => subluminal (test/wave3d_tests.jl:103-107)."""
     import conftest
