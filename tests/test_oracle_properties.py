@@ -308,6 +308,42 @@ def test_lap_strong_cons_constants_and_rayleigh_convergence(O):
     assert errs[3] < 1e-3
 
 
+def test_lap_strong_cons_leapfrog_energy_is_second_order(O):
+    """Leapfrog on the periodic 2x2x2, N = 3 conservative strong Laplacian
+    (test/wave_lap_strong_mesh_tests.jl:138-189): the discrete energy's oscillation stays
+    below 0.5 at dt = 0.5 * 2 / omega_max over 2000 steps and shrinks more than 3 times when
+    dt halves (O(dt^2))."""
+    m = O.OracleMesh(3, 2, periodic=True)
+    L = dense(lambda v: m.lap_strong_cons(v, 0.5), m.nn)
+    Hp = m.get("Hphys")
+    w_max = np.sqrt(-np.linalg.eigvals(L).real.min())
+    x, y, z = m.coords()
+    u0 = np.sin(2 * np.pi * x) * np.sin(2 * np.pi * y) * np.sin(2 * np.pi * z)
+
+    def energy(u, v):
+        return 0.5 * v @ (Hp * v) + 0.5 * u @ (Hp * -(L @ u))
+
+    def envelope(factor, nsteps):
+        dt = factor * 2 / w_max
+        u = u0.copy()
+        Lu = L @ u
+        v = 0.5 * dt * Lu
+        E0 = energy(u, v - 0.5 * dt * Lu)
+        lo = hi = E0
+        for _ in range(nsteps):
+            u = u + dt * v
+            Lu = L @ u
+            v = v + dt * Lu
+            E = energy(u, v - 0.5 * dt * Lu)
+            lo, hi = min(lo, E), max(hi, E)
+        assert np.isfinite(E)
+        return E0, (hi - lo) / E0
+
+    E0a, env_a = envelope(0.5, 2000)
+    _, env_b = envelope(0.25, 4000)
+    assert E0a > 0 and env_a < 0.5 and env_b < env_a / 3
+
+
 def test_classify_face(O):
     """classify_face3d flat => subluminal (test/wave3d_tests.jl:103-107)."""
     import conftest
