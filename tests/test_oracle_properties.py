@@ -270,6 +270,28 @@ def test_strong_warped_dirichlet_rayleigh(O):
     assert (errs[0] / errs[-1]) ** 0.5 > 4 and errs[-1] < 1e-3
 
 
+def test_strong_periodic_warped_rayleigh(O):
+    """The periodic warped cube (test/periodic_warped_tests.jl:56-92): the H_phys-weighted
+    Rayleigh quotient of the strong-form RHS on sin(2 pi x) sin(2 pi y) sin(2 pi z) (physical
+    coordinates, N = 4) is continuous in the warp A (A = 0 within 0.01 of 3 (2 pi)^2, larger at
+    A = 0.1, below 5 there) and converges at A = 0.05 (errors shrink at least 3 and 50 times
+    from M = 2 to 4 and 8, ending below 1e-2)."""
+    lam = 3 * (2 * np.pi) ** 2
+
+    def ray(A, M):
+        o = O.OracleMesh(4, M, A=A, periodic=True, outer_tag=0)
+        x, y, z = o.coords()
+        u = np.sin(2 * np.pi * x) * np.sin(2 * np.pi * y) * np.sin(2 * np.pi * z)
+        H = o.get("Hphys")
+        return -np.dot(u, H * o.rhs_strong(u, np.zeros_like(u))) / np.dot(u, H * u)
+
+    errs = [abs(ray(A, 4) - lam) for A in (0.0, 0.01, 0.05, 0.1)]
+    assert errs[0] < 0.01 and errs[3] > errs[0] and errs[3] < 5
+    errs = [abs(ray(0.05, M) - lam) for M in (2, 4, 8)]
+    assert all(e > 0 for e in errs)
+    assert errs[1] < errs[0] / 3 and errs[2] < errs[1] / 50 and errs[2] < 1e-2
+
+
 def test_strong_dirichlet_spectrum_flat(O):
     """Flat Dirichlet cube: spectrum real and negative (test/dirichlet_cube_tests.jl:110-130)."""
     m = O.OracleMesh(3, 2, outer_tag=0)
