@@ -203,3 +203,25 @@ def test_oracle_turned_elements_match(wt, O):
     P1, Q1 = o1.rhs_curved(o1.background(2, p), Phi0[gidx], Pi0[gidx], eps_ko=0.0, bc=bc, use_metric=True)
     for a, b in ((P1, P0[gidx]), (Q1, Q0[gidx])):
         assert np.linalg.norm(a - b) <= 1e-11 * np.linalg.norm(b)
+
+
+def test_oracle_radial_shell_excision_drains_noise(wt, O):
+    """The reference's radial-shell excision check (test/evolve3d_curv_tests.jl:46-60): flat
+    space with a radial shift ramping from V = 2 at R1 = 0.5 (superluminal: the inner sphere
+    is excised, tag 8) to 1/20 at R2 = 1 (Sommerfeld), sqrt(eps) noise, eps_KO = 0.1, CFL 1/10
+    with max speed V + 1, to t = 1: the energy never grows (here at every RK4 step, not only at
+    the samples) and the noise drains out."""
+    N, M, V = 4, 2, 2.0
+    a = wt.patch_mesh_arrays(wt.MESH_RADIAL_SHELL, N, M, (0.5, 1.0))
+    o = oracle_from(O, N, a)
+    assert sorted(set(a["bdry"].tolist())) == [0, 7, 8]
+    co = o.background(3, [V, 1.0 / 20, 0.5, 1.0])
+    rng = np.random.default_rng(20260604)
+    amp = np.sqrt(np.finfo(float).eps)
+    P0, Q0 = amp * rng.standard_normal(o.nn), amp * rng.standard_normal(o.nn)
+    dt = min(0.1 * o.min_spacing() / (V + 1), 1.4 / (0.1 * o.mu()))
+    P, Q, E = o.evolve_curved(co, P0, Q0, dt, int(np.ceil(1.0 / dt)), eps_ko=0.1,
+                              bc=O.make_bc([2] * 6, excision_tag=8), use_metric=True, record_energy=True)
+    assert np.all(np.isfinite(P)) and np.all(np.isfinite(Q))
+    assert np.all(np.diff(E) <= 1e-6 * E[0])
+    assert E[-1] < 0.5 * E[0]
