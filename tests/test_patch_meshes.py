@@ -225,3 +225,21 @@ def test_oracle_radial_shell_excision_drains_noise(wt, O):
     assert np.all(np.isfinite(P)) and np.all(np.isfinite(Q))
     assert np.all(np.diff(E) <= 1e-6 * E[0])
     assert E[-1] < 0.5 * E[0]
+
+
+def test_oracle_cubed_cube_sommerfeld_noise_energy(wt, O):
+    """The reference's cubed-cube Sommerfeld check (test/evolve3d_curv_tests.jl:36-44): N = 4,
+    M = 1, R = 0.3, Minkowski, sqrt(eps) noise, eps_KO = 0.1, CFL 1/10, to t = 0.5: the energy
+    never exceeds its start by more than 1e-6 (checked at every RK4 step)."""
+    N = 4
+    a = wt.patch_mesh_arrays(wt.MESH_CUBED_CUBE, N, 1, (0.3,))
+    o = oracle_from(O, N, a)
+    co = o.background(0)
+    rng = np.random.default_rng(20260604)
+    amp = np.sqrt(np.finfo(float).eps)
+    P0, Q0 = amp * rng.standard_normal(o.nn), amp * rng.standard_normal(o.nn)
+    dt = min(0.1 * o.min_spacing(), 1.4 / (0.1 * o.mu()))
+    P, Q, E = o.evolve_curved(co, P0, Q0, dt, int(np.ceil(0.5 / dt)), eps_ko=0.1, bc=O.make_bc([2] * 6),
+                              use_metric=True, record_energy=True)
+    assert np.all(np.isfinite(P)) and np.all(np.isfinite(Q))
+    assert E.max() <= E[0] * (1 + 1e-6)
