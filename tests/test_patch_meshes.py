@@ -243,3 +243,29 @@ def test_oracle_cubed_cube_sommerfeld_noise_energy(wt, O):
                               use_metric=True, record_energy=True)
     assert np.all(np.isfinite(P)) and np.all(np.isfinite(Q))
     assert E.max() <= E[0] * (1 + 1e-6)
+
+
+@pytest.mark.parametrize("noise", [False, True])
+def test_oracle_strong_form_inflated_cube_stays_bounded(wt, O, noise):
+    """The reference's strong-form (full chain rule) checks on the inflated cube
+    (test/wave_strong_rhs_tests.jl:89-151): N = 3, M = 4, L = 0.1, R1 = 0.3, R2 = 1, an outgoing
+    pulse (A = 1, s0 = 0.5, sigma = 0.15), with sqrt(eps) noise added in the second case,
+    leapfrog at dt = 5e-4 with BGT-1 at R = 1: finite after 1500 (1000 with noise) steps and
+    below 20 (20 times the initial maximum with noise)."""
+    N = 3
+    a = wt.patch_mesh_arrays(wt.MESH_INFLATED_CUBE, N, 4, (0.1, 0.3, 1.0))
+    o = oracle_from(O, N, a)
+    x, y, z = o.coords()
+    u, ud = O.ic_outgoing_pulse(x, y, z, 0.0, 1.0, 0.5, 0.15, 0.0, 0.0, 0.0)
+    if noise:
+        rng = np.random.default_rng(20260602)
+        amp = np.sqrt(np.finfo(float).eps)
+        u, ud = u + amp * rng.standard_normal(o.nn), ud + amp * rng.standard_normal(o.nn)
+    bound = 20 * np.abs(u).max() if noise else 20.0
+    dt = 5e-4
+    ud = ud + 0.5 * dt * o.rhs_strong(u, ud, R=1.0)
+    for _ in range(1000 if noise else 1500):
+        u = u + dt * ud
+        ud = ud + dt * o.rhs_strong(u, ud, R=1.0)
+    assert np.all(np.isfinite(u)) and np.all(np.isfinite(ud))
+    assert np.abs(u).max() < bound
