@@ -269,3 +269,32 @@ def test_oracle_strong_form_inflated_cube_stays_bounded(wt, O, noise):
         ud = ud + dt * o.rhs_strong(u, ud, R=1.0)
     assert np.all(np.isfinite(u)) and np.all(np.isfinite(ud))
     assert np.abs(u).max() < bound
+
+
+def test_oracle_strong_form_cubed_cube_dirichlet(wt, O):
+    """The reference's cubed-cube Dirichlet checks of the strong form
+    (test/dirichlet_cubed_cube_tests.jl:54-109), on the oracle: the H_phys-weighted Rayleigh
+    quotient of cos(pi x/2) cos(pi y/2) cos(pi z/2) on [-1, 1]^3 (N = 4, R = 0.3, zero
+    Dirichlet faces) converges to 3 pi^2 / 4 with a geometric-mean ratio above 4 over
+    M = 2, 4, 8, ending below 1e-3; at N = 3, M = 2 the spectrum has no growing mode
+    (max Re < 1), is non-trivial (min Re < -1) and has bounded imaginary parts (< 100)."""
+    lam = 3 * np.pi ** 2 / 4
+    errs = []
+    for M in (2, 4, 8):
+        o = oracle_from(O, 4, wt.patch_mesh_arrays(wt.MESH_CUBED_CUBE, 4, M, (0.3,), outer_tag=1))
+        x, y, z = o.coords()
+        u = np.cos(np.pi * x / 2) * np.cos(np.pi * y / 2) * np.cos(np.pi * z / 2)
+        H = o.get("Hphys")
+        errs.append(abs(-np.dot(u, H * o.rhs_strong(u, np.zeros_like(u))) / np.dot(u, H * u) - lam))
+    assert all(e > 0 for e in errs) and errs[-1] < errs[0]
+    assert (errs[0] / errs[-1]) ** 0.5 > 4 and errs[-1] < 1e-3
+    o = oracle_from(O, 3, wt.patch_mesh_arrays(wt.MESH_CUBED_CUBE, 3, 2, (0.3,), outer_tag=1))
+    n = o.nn
+    L = np.zeros((n, n))
+    e, zero = np.zeros(n), np.zeros(n)
+    for k in range(n):
+        e[k] = 1.0
+        L[:, k] = o.rhs_strong(e, zero)
+        e[k] = 0.0
+    ev = np.linalg.eigvals(L)
+    assert ev.real.max() < 1.0 and ev.real.min() < -1.0 and np.abs(ev.imag).max() < 100.0
