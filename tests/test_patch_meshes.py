@@ -298,3 +298,22 @@ def test_oracle_strong_form_cubed_cube_dirichlet(wt, O):
         e[k] = 0.0
     ev = np.linalg.eigvals(L)
     assert ev.real.max() < 1.0 and ev.real.min() < -1.0 and np.abs(ev.imag).max() < 100.0
+
+
+def test_oracle_strong_form_inflated_cube_dirichlet_j0(wt, O):
+    """The reference's cubed-sphere Dirichlet checks of the strong form
+    (test/dirichlet_cubed_sphere_tests.jl:84-128), on this library's inflated cube
+    (L = 0.1, R1 = 0.3, R2 = 1, zero Dirichlet outer faces, N = 4): the H_phys-weighted
+    Rayleigh quotient of j0(pi r) = sin(pi r) / (pi r) is within 1e-3 of pi^2 at M = 4, and
+    its error shrinks more than 10 times from M = 2 to 4."""
+    def rq(M):
+        o = oracle_from(O, 4, wt.patch_mesh_arrays(wt.MESH_INFLATED_CUBE, 4, M, (0.1, 0.3, 1.0), outer_tag=1))
+        x, y, z = o.coords()
+        r = np.sqrt(x * x + y * y + z * z)
+        u = np.where(r > 0, np.sin(np.pi * r) / np.where(r > 0, np.pi * r, 1.0), 1.0)
+        H = o.get("Hphys")
+        return -np.dot(u, H * o.rhs_strong(u, np.zeros_like(u))) / np.dot(u, H * u)
+
+    errs = [abs(rq(M) - np.pi ** 2) for M in (2, 4)]
+    assert all(e > 0 for e in errs)
+    assert errs[1] / np.pi ** 2 < 1e-3 and errs[1] < errs[0] / 10
