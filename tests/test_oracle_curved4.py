@@ -76,3 +76,17 @@ def test_leapfrog_on_gauge_wave_bounded(O, cons):
         phid += dt * o.rhs_curved4(phi, phid, ginv, gam, 0.5, conservative=cons)
         bound = max(bound, np.max(np.abs(phi - 1)))
     assert np.all(np.isfinite(phi)) and bound < 0.1
+
+
+def test_conservative_and_centred_flux_differ_on_gauge_wave(O):
+    """test/wave_curved_tests.jl:354-375: on the gauge wave (A = 0.1, d = 1; N = 4, periodic
+    2x2x2) the conservative (Mattsson-Nordstrom) and centred-flux forms give different but
+    comparable RHS on random data (relative difference between 1e-6 and 10)."""
+    o = O.OracleMesh(4, 2, periodic=True)
+    ginv, gam = o.curved4_background(1, (0.1, 1.0), 0.0)
+    rng = np.random.default_rng(20260601)
+    phi, phid = rng.standard_normal(o.nn), rng.standard_normal(o.nn)
+    cf = o.rhs_curved4(phi, phid, ginv, gam, 0.5, conservative=False)
+    cons = o.rhs_curved4(phi, phid, ginv, gam, 0.5, conservative=True)
+    rel = np.max(np.abs(cons - cf)) / np.max(np.abs(cf))
+    assert 1e-6 < rel < 10.0
